@@ -1,0 +1,216 @@
+/*
+ * kestrel_gpu.h — C ABI of the B200 all-pairs maximum-likelihood Jacquard
+ * estimator (libkestrel_gpu.so).
+ *
+ * This is the drop-in boundary for the path the reference (malariagen/kestrel
+ * v0.1.2, Rust) runs from its CLI and Python module:
+ *   src/wrapper.rs:89-96   calculate_relatedness_coefficients_gl(...)
+ *   src/wrapper.rs:22-29   calculate_relatedness_coefficients_gt(...)
+ *   src/coefficients.rs:40-141  the per-pair SQP driver they call
+ *   src/coefficients.rs:143-151 struct Output
+ * Every entry point takes plain pointers and sizes, returns a kg_status, and
+ * never lets a C++ exception or a CUDA error escape; kg_last_error() gives the
+ * message.  Buffers are caller-owned.  One context per host thread, except the
+ * serving calls (kg_panel_*, kg_submit/kg_poll/kg_wait/kg_cancel), which are
+ * thread-safe.
+ *
+ * Genotype codes are the reference's unphased triangular index
+ * (src/coefficients.rs:19-38): 0 = 0/0, 1 = 0/1, 2 = 1/1; KG_MISSING (3) marks
+ * a missing call, which the reference turns into a NaN likelihood row
+ * (src/vcf.rs:397) and drops for that pair only (src/lanevector.rs:99-104).
+ * Codes are sample-major: codes[sample * row_stride + site].
+ */
+#ifndef KESTREL_GPU_H
+#define KESTREL_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define KG_MISSING 3
+
+/* One estimated pair; the reference's Output (src/coefficients.rs:143-151).
+ * jacquard[0..8] = Delta1..Delta9; cond is the raw condition estimate (the CLI
+ * prints log10(cond), src/cli.rs:170); cond = NaN when the SQP ran out of
+ * iterations (src/sqp.rs:92). */
+typedef struct {
+    uint64_t x;
+    uint64_t y;
+    double jacquard[9];
+    double obj;
+    uint64_t iters;
+    double cond;
+} kg_output;
+
+typedef enum {
+    KG_OK = 0,
+    KG_EINVAL = 1,      /* bad argument (the reference panics/asserts here) */
+    KG_ENOMEM = 2,      /* device or host allocation failed / over budget */
+    KG_ECUDA = 3,       /* CUDA runtime or kernel error */
+    KG_ETIMEOUT = 4,    /* kg_wait timed out, or a bounded device wait gave up */
+    KG_ENOSITES = 5,    /* no segregating site, or a pair with no jointly
+                           observed site (the reference asserts,
+                           src/lanevector.rs:133-138) */
+    KG_ENOTREADY = 6,   /* request still running */
+    KG_ENOTFOUND = 7,   /* unknown request id */
+    KG_ECANCELED = 8    /* request was cancelled */
+} kg_status;
+
+typedef enum {
+    KG_PREC_FP32C = 0,  /* FP32 site sums with compensation; FP64 solver (default) */
+    KG_PREC_FP64 = 1    /* FP64 throughout (the plain FP64 GPU form) */
+} kg_precision;
+
+typedef struct kg_ctx kg_ctx;
+
+/* Context on CUDA device `device`.  mem_budget = 0 means no limit beyond the
+ * device's free memory. */
+int kg_create(kg_ctx **ctx, int device, size_t mem_budget);
+int kg_destroy(kg_ctx *ctx);
+const char *kg_last_error(const kg_ctx *ctx);
+const char *kg_version(void);
+
+/* Arithmetic of the per-site sums (kg_precision). */
+int kg_set_precision(kg_ctx *ctx, int precision);
+
+/* Launch shape: warps per block and blocks per SM of the persistent pair
+ * kernel (0 = autotuned choice).  Exposed for the autotuner and tests. */
+int kg_set_launch(kg_ctx *ctx, int warps_per_block, int blocks_per_sm);
+
+/* Runs the autotuner on a sample of the loaded cohort and keeps the fastest
+ * launch shape; writes it to *warps_per_block / *blocks_per_sm if non-NULL. */
+int kg_autotune(kg_ctx *ctx, int *warps_per_block, int *blocks_per_sm);
+
+/* ---------------------------------------------------------------- cohort */
+
+/* Loads a cohort (all n_samples rows feed the allele frequencies). */
+int kg_load_genotypes(kg_ctx *ctx, const uint8_t *codes, int64_t n_samples,
+                      int64_t n_sites, int64_t row_stride);
+
+/* Same cohort from the host VCF parser's packed form: 2-bit genotype codes,
+ * 16 sites per uint32 (site s at bits 2*(s%16) of word s/16, values 0..2), and
+ * an observed mask, 32 sites per uint32 (bit s%32 of word s/32 set = called).
+ * Rows are ceil(n_sites/16) and ceil(n_sites/32) words long. */
+int kg_load_genotypes_2bit(kg_ctx *ctx, const uint32_t *codes2,
+                           const uint32_t *observed, int64_t n_samples,
+                           int64_t n_sites);
+
+/* Pre-computed allele frequencies, n_sites x 2 ([REF, ALT]) or NULL to estimate
+ * them from the samples (the reference's -a estimate). */
+int kg_set_allele_frequencies(kg_ctx *ctx, const double *af);
+
+/* All pairs (x, y), 0 <= x <= y < num_samples, in the reference's row order
+ * (outputs[x] then y = x..num_samples-1, src/coefficients.rs:77-136).
+ * num_samples < 0 means all samples; iterations is the SQP cap (-i, default
+ * 100); maf < 0 or NaN selects 1/(2 n_samples) (src/wrapper.rs:101).
+ * out_cap must be >= num_samples*(num_samples+1)/2. */
+int kg_relatedness(kg_ctx *ctx, int64_t num_samples, uint64_t iterations,
+                   double maf, kg_output *out, int64_t out_cap, int64_t *n_out);
+
+/* One-shot form of the reference's
+ * calculate_relatedness_coefficients_gl(genotype_likelihoods,
+ * allele_frequencies, threads, iterations, minimum_allele_frequency,
+ * num_samples) (src/wrapper.rs:89-96) on hard calls: creates a context on
+ * device 0, loads, runs and destroys it.  `threads` is accepted and ignored
+ * (there is no host thread pool on this path). */
+int kg_relatedness_coefficients(const uint8_t *codes, int64_t n_samples,
+                                int64_t n_sites, int64_t row_stride,
+                                const double *allele_frequencies,
+                                int64_t threads, uint64_t iterations,
+                                double maf, int64_t num_samples,
+                                kg_output *out, int64_t out_cap,
+                                int64_t *n_out);
+
+/* ------------------------------------------------------------ batching */
+
+/* Several independent cohorts (uneven N, M and missingness) in one persistent
+ * launch: each cohort gets its own allele frequencies and all its pairs. */
+typedef struct {
+    const uint8_t *codes;      /* sample-major, row_stride bytes per row */
+    int64_t n_samples;
+    int64_t n_sites;
+    int64_t row_stride;
+    const double *allele_frequencies; /* NULL = estimate */
+    int64_t num_samples;       /* < 0 = all */
+    kg_output *out;
+    int64_t out_cap;
+    int64_t n_out;             /* written by the call */
+    int32_t status;            /* per-cohort kg_status, written by the call */
+} kg_cohort;
+
+int kg_relatedness_batch(kg_ctx *ctx, kg_cohort *cohorts, int n_cohorts,
+                         uint64_t iterations, double maf);
+
+/* ------------------------------------------------------------- serving */
+
+/* Makes `codes` the resident reference panel (packed in HBM with its allele
+ * frequencies, estimated unless af is given).  Query requests are scored
+ * against it until the next kg_panel_load or kg_destroy. */
+int kg_panel_load(kg_ctx *ctx, const uint8_t *codes, int64_t n_samples,
+                  int64_t n_sites, int64_t row_stride, const double *af,
+                  double maf);
+
+/* Queues n_query new samples (codes over the panel's n_sites) for scoring
+ * against every panel sample.  site_mask (n_sites bytes, nonzero = use the
+ * site) restricts the request to a subset of sites; NULL uses all.  The call
+ * copies its inputs and returns at once with a request id. */
+int kg_submit(kg_ctx *ctx, const uint8_t *query_codes, int64_t n_query,
+              int64_t row_stride, const uint8_t *site_mask,
+              uint64_t iterations, int64_t *request_id);
+
+/* *done = 1 once the request has finished (or failed). */
+int kg_poll(kg_ctx *ctx, int64_t request_id, int *done);
+
+/* Waits up to timeout_ms (< 0 = forever) and copies the n_query*n_panel rows
+ * (x = query index, y = panel index, query-major) to out, then forgets the
+ * request.  Returns KG_ETIMEOUT if it is still running. */
+int kg_wait(kg_ctx *ctx, int64_t request_id, int64_t timeout_ms,
+            kg_output *out, int64_t out_cap, int64_t *n_out);
+
+/* Drops a queued request (a running one finishes but its rows are discarded). */
+int kg_cancel(kg_ctx *ctx, int64_t request_id);
+
+/* Serving counters: requests completed, pairs completed, device launches. */
+int kg_serving_stats(kg_ctx *ctx, int64_t *requests, int64_t *pairs,
+                     int64_t *launches);
+
+/* --------------------------------------------------------- diagnostics */
+
+/* Per-run counters of the last kg_relatedness / batch call: grad-Hessian and
+ * objective site passes (summed over pairs), pairs that escalated to FP64,
+ * kernel launches, and the device time of the pair kernel in milliseconds. */
+typedef struct {
+    uint64_t gh_passes;
+    uint64_t obj_passes;
+    uint64_t fp64_passes;
+    uint64_t fp64_pairs;
+    uint64_t pair_sites;       /* sum over pairs of jointly observed sites */
+    uint64_t work_units;       /* sum over passes of sites visited */
+    uint64_t launches;         /* kernels launched by the call */
+    uint64_t flops_fp32;       /* executed FP32 site arithmetic (FMA = 2) */
+    uint64_t flops_fp64;       /* executed FP64 site arithmetic */
+    uint64_t shape_sites[5];   /* pair-sites per genotype-pair shape A,B1,B2,C,D */
+    double pair_kernel_ms;     /* CUDA-event time of the pair kernel */
+    double device_ms;          /* CUDA-event time of preparation + pair kernel */
+    double total_ms;           /* host time of the call */
+} kg_run_stats;
+
+int kg_last_run_stats(kg_ctx *ctx, kg_run_stats *stats);
+
+/* Measured FP32 FMA throughput of `device` (TFLOP/s, FMA = 2 FLOP) from a
+ * register-resident FFMA loop over every SM; the roofline denominator of the
+ * FP32 pair kernel. */
+int kg_fp32_peak(int device, double *tflops);
+
+/* Runs the reference-compatible CLI (`kestrel input.vcf kinship.tsv [flags]`,
+ * src/cli.rs:12-127) in-process; argv[0] is the program name. */
+int kg_run_cli(int argc, const char *const *argv);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,282 @@
+"""kestrel_b200 — B200-native all-pairs maximum-likelihood Jacquard estimator.
+
+Python surface of the reference's `kestrel` module (src/lib.rs:26-161):
+`relatedness_coefficients_gt`, `relatedness_coefficients_gl`, `run_cli` and
+`Coefficients`, all running on libkestrel_gpu.so (sm_100a).  `Estimator` exposes
+the context API (precision, batching of several cohorts, serving a resident
+panel) of include/kestrel_gpu.h.
+"""
+from __future__ import annotations
+
+import ctypes
+import sys
+import warnings
+
+import numpy as np
+
+from ._lib import (KG_ENOSITES, KG_ETIMEOUT, KG_OK, KG_PREC_FP32C, KG_PREC_FP64, MISSING,
+                   OUTPUT_DTYPE, KestrelError, KgCohort, KgRunStats, lib, ptr)
+
+__all__ = ["Coefficients", "relatedness_coefficients_gt", "relatedness_coefficients_gl",
+           "run_cli", "Estimator", "genotype_codes", "build_arrays", "KestrelError",
+           "OUTPUT_DTYPE", "MISSING", "KINSHIP_VECTOR"]
+
+# Kinship as a linear function of Delta (src/cli.rs:150, src/lib.rs:127).
+KINSHIP_VECTOR = np.array([1.0, 0.0, 0.5, 0.0, 0.5, 0.0, 0.5, 0.25, 0.0])
+
+
+class Coefficients:
+    """Result arrays of the reference's Python API (src/lib.rs:36-44)."""
+
+    def __init__(self, jacquard, kinship, inbreeding):
+        self.jacquard = jacquard
+        self.kinship = kinship
+        self.inbreeding = inbreeding
+
+    def __repr__(self):
+        return f"Coefficients(samples={self.kinship.shape[0]})"
+
+
+def _check(status: int, ctx=None):
+    if status != KG_OK:
+        msg = lib().kg_last_error(ctx).decode() if ctx else ""
+        raise KestrelError(status, msg)
+
+
+def genotype_codes(genotypes: np.ndarray) -> np.ndarray:
+    """u8/int [V, S, 2] allele indices -> sample-major [S, V] codes 0/1/2, 3 = missing.
+
+    The unphased index j(j+1)/2 + i of the reference (src/coefficients.rs:19-38)
+    for biallelic sites; an allele < 0 or > 1 (e.g. -1 or 255) marks a missing call.
+    """
+    g = np.asarray(genotypes)
+    if g.ndim != 3 or g.shape[2] != 2:
+        raise ValueError("genotypes must have shape (variants, samples, 2)")
+    a = g.astype(np.int16)
+    if g.dtype == np.uint8:
+        a = np.where(g == 255, -1, a)
+    miss = (a < 0) | (a > 1)
+    codes = (a[..., 0] + a[..., 1]).astype(np.uint8)
+    codes[miss.any(axis=2)] = MISSING
+    return np.ascontiguousarray(codes.T)
+
+
+def build_arrays(rows: np.ndarray, num_samples: int):
+    """(jacquard N x N x 9, kinship N x N, inbreeding N) from output rows, with
+    the D3<->D5 and D4<->D6 swap for (y, x) (src/lib.rs:120-161)."""
+    jac = np.zeros((num_samples, num_samples, 9))
+    kin = np.zeros((num_samples, num_samples))
+    inb = np.zeros(num_samples)
+    x = rows["x"].astype(np.int64)
+    y = rows["y"].astype(np.int64)
+    d = rows["jacquard"]
+    k = d @ KINSHIP_VECTOR
+    jac[x, y] = d
+    off = x != y
+    jac[y[off], x[off]] = d[off][:, [0, 1, 4, 5, 2, 3, 6, 7, 8]]
+    kin[x, y] = k
+    kin[y[off], x[off]] = k[off]
+    self_ = ~off
+    inb[x[self_]] = 2.0 * k[self_] - 1.0
+    return jac, kin, inb
+
+
+class Estimator:
+    """A device context (kg_ctx) on one GPU."""
+
+    def __init__(self, device: int = 0, mem_budget: int = 0, precision: str = "fp32c"):
+        self._L = lib()
+        h = ctypes.c_void_p()
+        st = self._L.kg_create(ctypes.byref(h), device, mem_budget)
+        if st != KG_OK:
+            raise KestrelError(st, "kg_create failed (is a CUDA device present?)")
+        self._h = h
+        self.n_samples = 0
+        self.n_sites = 0
+        self.set_precision(precision)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._L.kg_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_precision(self, precision: str):
+        p = {"fp32c": KG_PREC_FP32C, "fp64": KG_PREC_FP64}[precision]
+        _check(self._L.kg_set_precision(self._h, p), self._h)
+
+    def set_launch(self, warps_per_block: int = 0, blocks_per_sm: int = 0):
+        _check(self._L.kg_set_launch(self._h, warps_per_block, blocks_per_sm), self._h)
+
+    def autotune(self):
+        w, b = ctypes.c_int(), ctypes.c_int()
+        _check(self._L.kg_autotune(self._h, ctypes.byref(w), ctypes.byref(b)), self._h)
+        return w.value, b.value
+
+    def load(self, codes: np.ndarray, allele_frequencies=None):
+        codes = np.ascontiguousarray(codes, dtype=np.uint8)
+        if codes.ndim != 2:
+            raise ValueError("codes must be (samples, sites)")
+        n, m = codes.shape
+        _check(self._L.kg_load_genotypes(self._h, ptr(codes), n, m, m), self._h)
+        self.n_samples, self.n_sites = n, m
+        if allele_frequencies is not None:
+            af = np.ascontiguousarray(allele_frequencies, dtype=np.float64)
+            if af.shape != (m, 2):
+                raise ValueError("allele_frequencies must be (sites, 2)")
+            _check(self._L.kg_set_allele_frequencies(self._h, ptr(af)), self._h)
+            self._af = af
+        return self
+
+    def relatedness(self, num_samples=None, iterations: int = 100, maf=None,
+                    out: np.ndarray | None = None, allow_nosites: bool = False) -> np.ndarray:
+        ns = self.n_samples if num_samples is None else int(num_samples)
+        np_ = ns * (ns + 1) // 2
+        if out is None:
+            out = np.empty(np_, OUTPUT_DTYPE)
+        nout = ctypes.c_int64()
+        st = self._L.kg_relatedness(self._h, ns, iterations,
+                                    float("nan") if maf is None else float(maf),
+                                    ptr(out), out.size, ctypes.byref(nout))
+        if st == KG_ENOSITES and allow_nosites and nout.value == np_:
+            return out
+        _check(st, self._h)
+        return out
+
+    def run_stats(self) -> dict:
+        s = KgRunStats()
+        _check(self._L.kg_last_run_stats(self._h, ctypes.byref(s)), self._h)
+        d = {f: getattr(s, f) for f, _ in KgRunStats._fields_}
+        d["shape_sites"] = list(s.shape_sites)
+        return d
+
+    def relatedness_batch(self, cohorts, iterations: int = 100, maf=None):
+        """cohorts: list of (codes[S, V] u8, allele_frequencies or None, num_samples or None).
+        Returns one row array per cohort, all from a single persistent launch."""
+        arr = (KgCohort * len(cohorts))()
+        keep = []
+        outs = []
+        for i, c in enumerate(cohorts):
+            codes, af, ns = (list(c) + [None, None])[:3]
+            codes = np.ascontiguousarray(codes, dtype=np.uint8)
+            n, m = codes.shape
+            ns = n if ns is None else int(ns)
+            out = np.empty(ns * (ns + 1) // 2, OUTPUT_DTYPE)
+            afa = None if af is None else np.ascontiguousarray(af, dtype=np.float64)
+            keep += [codes, afa, out]
+            arr[i].codes = codes.ctypes.data
+            arr[i].n_samples, arr[i].n_sites, arr[i].row_stride = n, m, m
+            arr[i].allele_frequencies = None if afa is None else afa.ctypes.data
+            arr[i].num_samples = ns
+            arr[i].out = out.ctypes.data
+            arr[i].out_cap = out.size
+            outs.append(out)
+        st = self._L.kg_relatedness_batch(self._h, arr, len(cohorts), iterations,
+                                          float("nan") if maf is None else float(maf))
+        _check(st, self._h)
+        return outs
+
+    # ---- serving
+    def panel_load(self, codes: np.ndarray, allele_frequencies=None, maf=None):
+        codes = np.ascontiguousarray(codes, dtype=np.uint8)
+        n, m = codes.shape
+        afa = None if allele_frequencies is None else np.ascontiguousarray(allele_frequencies, np.float64)
+        _check(self._L.kg_panel_load(self._h, ptr(codes), n, m, m, ptr(afa),
+                                     float("nan") if maf is None else float(maf)), self._h)
+        self.panel_samples, self.panel_sites = n, m
+
+    def submit(self, query_codes: np.ndarray, site_mask=None, iterations: int = 100) -> int:
+        q = np.ascontiguousarray(query_codes, dtype=np.uint8)
+        mask = None if site_mask is None else np.ascontiguousarray(site_mask, dtype=np.uint8)
+        rid = ctypes.c_int64()
+        _check(self._L.kg_submit(self._h, ptr(q), q.shape[0], q.shape[1], ptr(mask), iterations,
+                                 ctypes.byref(rid)), self._h)
+        self._pending = getattr(self, "_pending", {})
+        self._pending[rid.value] = q.shape[0]
+        return rid.value
+
+    def poll(self, request_id: int) -> bool:
+        done = ctypes.c_int()
+        _check(self._L.kg_poll(self._h, request_id, ctypes.byref(done)), self._h)
+        return bool(done.value)
+
+    def wait(self, request_id: int, timeout_ms: int = -1) -> np.ndarray | None:
+        nq = self._pending.get(request_id, 0)
+        out = np.empty(max(nq * self.panel_samples, 1), OUTPUT_DTYPE)
+        nout = ctypes.c_int64()
+        st = self._L.kg_wait(self._h, request_id, timeout_ms, ptr(out), out.size, ctypes.byref(nout))
+        if st == KG_ETIMEOUT:
+            return None
+        self._pending.pop(request_id, None)
+        _check(st, self._h)
+        return out[:nout.value]
+
+    def cancel(self, request_id: int):
+        _check(self._L.kg_cancel(self._h, request_id), self._h)
+
+    def serving_stats(self):
+        r, p, l_ = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64()
+        _check(self._L.kg_serving_stats(self._h, ctypes.byref(r), ctypes.byref(p), ctypes.byref(l_)),
+               self._h)
+        return {"requests": r.value, "pairs": p.value, "launches": l_.value}
+
+
+def relatedness_coefficients_gt(genotypes, allele_frequencies=None, threads=None, iterations=100):
+    """Jacquard, kinship and inbreeding for every pair of samples from hard
+    calls (the reference's signature, src/lib.rs:46-70).  genotypes: u8/int
+    [variants, samples, 2] allele indices; allele_frequencies: f64 [variants, 2]
+    ([REF, ALT]) or None to estimate.  `threads` is accepted and unused."""
+    del threads
+    codes = genotype_codes(genotypes)
+    with Estimator() as est:
+        est.load(codes, allele_frequencies)
+        rows = est.relatedness(iterations=iterations)
+    return Coefficients(*build_arrays(rows, codes.shape[0]))
+
+
+def relatedness_coefficients_gl(genotype_likelihoods, allele_frequencies=None, threads=None,
+                                iterations=100, minimum_allele_frequency=None):
+    """The GL/PL entry point (src/lib.rs:72-109) for biallelic one-hot
+    likelihoods [variants, samples, 3] (NaN = missing).  Each call is the most
+    likely genotype; non-one-hot rows are reduced the same way with a warning."""
+    del threads
+    gl = np.asarray(genotype_likelihoods, dtype=np.float64)
+    if gl.ndim != 3 or gl.shape[2] != 3:
+        raise ValueError("genotype_likelihoods must have shape (variants, samples, 3)")
+    miss = np.isnan(gl).any(axis=2)
+    g = np.where(miss[..., None], 0.0, gl)
+    best = np.argmax(g, axis=2)
+    top = np.take_along_axis(g, best[..., None], axis=2)[..., 0]
+    rest = np.sort(g, axis=2)[..., 1]
+    soft = (~miss) & (rest > top * 10 ** -25.5)
+    if soft.any():
+        warnings.warn(f"{int(soft.sum())} likelihood rows are not one-hot; using the most likely genotype")
+    codes = best.astype(np.uint8)
+    codes[miss] = MISSING
+    codes = np.ascontiguousarray(codes.T)
+    with Estimator() as est:
+        est.load(codes, allele_frequencies)
+        rows = est.relatedness(iterations=iterations, maf=minimum_allele_frequency)
+    return build_arrays(rows, codes.shape[0])
+
+
+def run_cli(argv=None) -> int:
+    """`kestrel input.vcf kinship.tsv [flags]` (src/lib.rs:112-117, src/cli.rs:67-127)."""
+    argv = list(sys.argv if argv is None else argv)
+    L = lib()
+    arr = (ctypes.c_char_p * len(argv))(*[a.encode() for a in argv])
+    st = L.kg_run_cli(len(argv), arr)
+    if st != 0:
+        raise RuntimeError(f"kestrel exited with status {st}")
+    return st

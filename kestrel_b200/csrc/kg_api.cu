@@ -1,0 +1,727 @@
+// kg_api.cu — extern "C" boundary of libkestrel_gpu.so (see include/kestrel_gpu.h).
+//
+// No exception or CUDA error crosses this boundary: every entry point returns a
+// kg_status and records a message for kg_last_error().
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <cmath>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <new>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "kestrel_gpu.h"
+#include "kg_engine.h"
+
+namespace {
+
+struct Request {
+    int64_t id = 0;
+    int64_t n_query = 0;
+    uint64_t iterations = 100;
+    std::vector<uint8_t> codes;   // n_query x n_sites
+    std::vector<uint8_t> mask;    // n_sites or empty
+    std::vector<kg_output> rows;
+    int status = KG_OK;
+    std::string err;
+    bool done = false;
+    bool cancelled = false;
+};
+
+struct Slot {
+    cudaStream_t stream = nullptr;
+    kg::Workspace ws;
+    kg::DevBuf out;
+    std::vector<std::unique_ptr<kg::QueryPlanes>> queries;
+    bool busy = false;
+};
+
+}  // namespace
+
+struct kg_ctx {
+    int device = 0;
+    size_t budget = 0;
+    int precision = KG_PREC_FP32C;
+    int wpb = 0, bps = 0;
+    std::string err;
+    cudaStream_t stream = nullptr;
+    // single cohort
+    kg::Cohort cohort;
+    bool loaded = false;
+    std::vector<double> af;
+    bool af_set = false;
+    kg::Workspace ws;
+    kg::DevBuf dout;
+    kg_run_stats last{};
+    // serving
+    std::mutex mu;
+    std::condition_variable cv;
+    std::thread server;
+    bool stop = false;
+    bool panel_ready = false;
+    kg::Cohort panel;
+    std::map<int64_t, std::shared_ptr<Request>> requests;
+    std::deque<int64_t> pending;
+    int64_t next_id = 1;
+    int64_t served_requests = 0, served_pairs = 0, served_launches = 0;
+    std::vector<Slot> slots;
+};
+
+namespace {
+
+int set_err(kg_ctx* c, int st, const std::string& msg) {
+    if (c) c->err = msg;
+    return st;
+}
+
+int use_device(kg_ctx* c) {
+    cudaError_t e = cudaSetDevice(c->device);
+    if (e != cudaSuccess) return set_err(c, KG_ECUDA, std::string("cudaSetDevice: ") + cudaGetErrorString(e));
+    return KG_OK;
+}
+
+bool budget_ok(kg_ctx* c, size_t extra) {
+    size_t fr = 0, tot = 0;
+    if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) return false;
+    if (extra > fr) return false;
+    if (c->budget) {
+        size_t used = tot - fr;
+        if (used + extra > c->budget) return false;
+    }
+    return true;
+}
+
+template <class F>
+int guarded(kg_ctx* c, F&& f) {
+    try {
+        return f();
+    } catch (const std::bad_alloc&) {
+        return set_err(c, KG_ENOMEM, "host allocation failed");
+    } catch (const std::exception& ex) {
+        return set_err(c, KG_ECUDA, ex.what());
+    } catch (...) {
+        return set_err(c, KG_ECUDA, "unknown error");
+    }
+}
+
+kg::RunConfig run_config(const kg_ctx* c, uint64_t iterations) {
+    kg::RunConfig cfg;
+    cfg.precision = c->precision;
+    cfg.iterations = iterations;
+    cfg.warps_per_block = c->wpb;
+    cfg.blocks_per_sm = c->bps;
+    return cfg;
+}
+
+int copy_rows_out(kg_ctx* c, const kg::DevBuf& d, int64_t n, kg_output* out, cudaStream_t st) {
+    cudaError_t e = cudaMemcpyAsync(out, d.p, sizeof(kg_output) * n, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return set_err(c, KG_ECUDA, std::string("copy rows: ") + cudaGetErrorString(e));
+    return KG_OK;
+}
+
+// ------------------------------------------------------------- serving loop
+
+void serve_batch(kg_ctx* c, Slot& slot, std::vector<std::shared_ptr<Request>>& batch) {
+    std::string err;
+    int st = KG_OK;
+    std::vector<kg::PairJob> jobs;
+    int64_t total = 0;
+    for (auto& r : batch) total += r->n_query * c->panel.n_samples;
+    slot.queries.clear();
+    int e = slot.out.reserve(sizeof(kg_output) * std::max<int64_t>(total, 1));
+    if (e != cudaSuccess) { st = KG_ENOMEM; err = "request outputs do not fit"; }
+    int64_t off = 0;
+    for (size_t i = 0; st == KG_OK && i < batch.size(); i++) {
+        auto q = std::make_unique<kg::QueryPlanes>();
+        st = kg::prepare_query(c->panel, *q, batch[i]->codes.data(), batch[i]->n_query,
+                               c->panel.n_sites, batch[i]->mask.empty() ? nullptr : batch[i]->mask.data(),
+                               slot.stream, err);
+        if (st != KG_OK) break;
+        kg::PairJob jb;
+        jb.panel = &c->panel;
+        jb.query = q.get();
+        jb.kind = 1;
+        jb.n_x = batch[i]->n_query;
+        jb.n_y = c->panel.n_samples;
+        jb.d_out = slot.out.as<kg_output>() + off;
+        off += jb.n_pairs();
+        jobs.push_back(jb);
+        slot.queries.push_back(std::move(q));
+    }
+    kg_run_stats stats{};
+    if (st == KG_OK) {
+        kg::RunConfig cfg = run_config(c, batch.empty() ? 100 : batch[0]->iterations);
+        uint64_t it = 1;
+        for (auto& r : batch) it = std::max<uint64_t>(it, r->iterations);
+        cfg.iterations = it;
+        cfg.max_warps = total;
+        st = kg::run_pairs(jobs, cfg, slot.ws, slot.stream, stats, err);
+        if (st == KG_ENOSITES) st = KG_OK;  // per-pair NaN rows; reported on the rows
+    }
+    off = 0;
+    for (auto& r : batch) {
+        int64_t np = r->n_query * c->panel.n_samples;
+        if (st == KG_OK) {
+            r->rows.resize(np);
+            cudaError_t ce = cudaMemcpyAsync(r->rows.data(), slot.out.as<kg_output>() + off,
+                                             sizeof(kg_output) * np, cudaMemcpyDeviceToHost, slot.stream);
+            if (ce == cudaSuccess) ce = cudaStreamSynchronize(slot.stream);
+            if (ce != cudaSuccess) { r->status = KG_ECUDA; r->err = cudaGetErrorString(ce); }
+        } else {
+            r->status = st;
+            r->err = err;
+        }
+        off += np;
+    }
+    std::lock_guard<std::mutex> lk(c->mu);
+    for (auto& r : batch) {
+        r->done = true;
+        c->served_requests++;
+        c->served_pairs += r->n_query * c->panel.n_samples;
+    }
+    c->served_launches++;
+    c->cv.notify_all();
+}
+
+// The scheduler: admits every queued request whose inputs fit the memory
+// budget into one batched launch (continuous batching); one batch per slot,
+// slots run concurrently on their own streams.
+void serve_loop(kg_ctx* c) {
+    cudaSetDevice(c->device);
+    std::vector<std::thread> workers;
+    const size_t kMaxPairs = (size_t)1 << 22;
+    for (;;) {
+        std::vector<std::shared_ptr<Request>> batch;
+        int slot_idx = -1;
+        {
+            std::unique_lock<std::mutex> lk(c->mu);
+            c->cv.wait(lk, [&] {
+                if (c->stop) return true;
+                if (c->pending.empty()) return false;
+                for (auto& s : c->slots)
+                    if (!s.busy) return true;
+                return false;
+            });
+            if (c->stop && c->pending.empty()) break;
+            if (c->stop) {
+                // drop what is still queued
+                for (int64_t id : c->pending) {
+                    auto it = c->requests.find(id);
+                    if (it != c->requests.end()) {
+                        it->second->status = KG_ECANCELED;
+                        it->second->done = true;
+                    }
+                }
+                c->pending.clear();
+                c->cv.notify_all();
+                break;
+            }
+            for (size_t i = 0; i < c->slots.size(); i++)
+                if (!c->slots[i].busy) { slot_idx = (int)i; break; }
+            size_t pairs = 0, bytes = 0;
+            while (!c->pending.empty()) {
+                int64_t id = c->pending.front();
+                auto it = c->requests.find(id);
+                if (it == c->requests.end() || it->second->cancelled) {
+                    c->pending.pop_front();
+                    continue;
+                }
+                auto& r = it->second;
+                size_t np = (size_t)(r->n_query * c->panel.n_samples);
+                size_t nb = np * sizeof(kg_output) +
+                            (size_t)r->n_query * (size_t)(c->panel.n_sites + c->panel.plane_stride * 8);
+                if (!batch.empty() && (pairs + np > kMaxPairs || !budget_ok(c, bytes + nb))) break;
+                batch.push_back(r);
+                pairs += np;
+                bytes += nb;
+                c->pending.pop_front();
+            }
+            if (batch.empty()) continue;
+            c->slots[slot_idx].busy = true;
+        }
+        workers.emplace_back([c, slot_idx, batch]() mutable {
+            cudaSetDevice(c->device);
+            serve_batch(c, c->slots[slot_idx], batch);
+            std::lock_guard<std::mutex> lk(c->mu);
+            c->slots[slot_idx].busy = false;
+            c->cv.notify_all();
+        });
+        // reap finished workers
+        if (workers.size() > 8) {
+            for (auto& w : workers) if (w.joinable()) w.join();
+            workers.clear();
+        }
+    }
+    for (auto& w : workers)
+        if (w.joinable()) w.join();
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* kg_version(void) { return kg::engine_version(); }
+
+int kg_create(kg_ctx** ctx, int device, size_t mem_budget) {
+    if (!ctx) return KG_EINVAL;
+    *ctx = nullptr;
+    kg_ctx* c = new (std::nothrow) kg_ctx();
+    if (!c) return KG_ENOMEM;
+    c->device = device;
+    c->budget = mem_budget;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || device < 0 || device >= n) {
+        delete c;
+        return KG_ECUDA;
+    }
+    if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete c;
+        return KG_ECUDA;
+    }
+    *ctx = c;
+    return KG_OK;
+}
+
+int kg_destroy(kg_ctx* c) {
+    if (!c) return KG_EINVAL;
+    cudaSetDevice(c->device);
+    {
+        std::lock_guard<std::mutex> lk(c->mu);
+        c->stop = true;
+        c->cv.notify_all();
+    }
+    if (c->server.joinable()) c->server.join();
+    for (auto& s : c->slots)
+        if (s.stream) {
+            cudaStreamSynchronize(s.stream);
+            cudaStreamDestroy(s.stream);
+        }
+    c->slots.clear();
+    if (c->stream) {
+        cudaStreamSynchronize(c->stream);
+        cudaStreamDestroy(c->stream);
+    }
+    delete c;
+    return KG_OK;
+}
+
+const char* kg_last_error(const kg_ctx* c) { return c ? c->err.c_str() : "null context"; }
+
+int kg_set_precision(kg_ctx* c, int precision) {
+    if (!c || (precision != KG_PREC_FP32C && precision != KG_PREC_FP64)) return set_err(c, KG_EINVAL, "precision must be KG_PREC_FP32C or KG_PREC_FP64");
+    c->precision = precision;
+    return KG_OK;
+}
+
+int kg_set_launch(kg_ctx* c, int warps_per_block, int blocks_per_sm) {
+    if (!c || warps_per_block < 0 || warps_per_block > 4 || blocks_per_sm < 0 || blocks_per_sm > 32)
+        return set_err(c, KG_EINVAL, "warps_per_block must be 0..4 and blocks_per_sm 0..32");
+    c->wpb = warps_per_block;
+    c->bps = blocks_per_sm;
+    return KG_OK;
+}
+
+int kg_load_genotypes(kg_ctx* c, const uint8_t* codes, int64_t n_samples, int64_t n_sites,
+                      int64_t row_stride) {
+    if (!c) return KG_EINVAL;
+    if (!codes || n_samples <= 0 || n_sites <= 0 || row_stride < n_sites)
+        return set_err(c, KG_EINVAL, "codes must be non-NULL with n_samples, n_sites > 0 and row_stride >= n_sites");
+    return guarded(c, [&]() -> int {
+        int st = use_device(c);
+        if (st) return st;
+        if (!budget_ok(c, (size_t)(n_samples * n_sites))) return set_err(c, KG_ENOMEM, "genotypes exceed the memory budget");
+        if (c->cohort.raw.reserve((size_t)(n_samples * n_sites)) != cudaSuccess)
+            return set_err(c, KG_ENOMEM, "cannot allocate device genotypes");
+        cudaError_t e = cudaMemcpy2DAsync(c->cohort.raw.p, (size_t)n_sites, codes, (size_t)row_stride,
+                                          (size_t)n_sites, (size_t)n_samples, cudaMemcpyHostToDevice, c->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+        if (e != cudaSuccess) return set_err(c, KG_ECUDA, std::string("upload: ") + cudaGetErrorString(e));
+        c->cohort.n_samples = n_samples;
+        c->cohort.n_sites = n_sites;
+        c->cohort.n_kept = -1;
+        c->loaded = true;
+        c->af_set = false;
+        return KG_OK;
+    });
+}
+
+int kg_load_genotypes_2bit(kg_ctx* c, const uint32_t* codes2, const uint32_t* observed,
+                           int64_t n_samples, int64_t n_sites) {
+    if (!c) return KG_EINVAL;
+    return guarded(c, [&]() -> int {
+        int st = use_device(c);
+        if (st) return st;
+        std::string err;
+        st = kg::unpack_2bit(c->cohort.raw, codes2, observed, n_samples, n_sites, c->stream, err);
+        if (st) return set_err(c, st, err);
+        c->cohort.n_samples = n_samples;
+        c->cohort.n_sites = n_sites;
+        c->cohort.n_kept = -1;
+        c->loaded = true;
+        c->af_set = false;
+        return KG_OK;
+    });
+}
+
+int kg_set_allele_frequencies(kg_ctx* c, const double* af) {
+    if (!c) return KG_EINVAL;
+    if (!c->loaded) return set_err(c, KG_EINVAL, "load genotypes first");
+    return guarded(c, [&]() -> int {
+        if (!af) {
+            c->af.clear();
+            c->af_set = false;
+            return KG_OK;
+        }
+        c->af.assign(af, af + 2 * c->cohort.n_sites);
+        c->af_set = true;
+        return KG_OK;
+    });
+}
+
+int kg_relatedness(kg_ctx* c, int64_t num_samples, uint64_t iterations, double maf, kg_output* out,
+                   int64_t out_cap, int64_t* n_out) {
+    if (!c) return KG_EINVAL;
+    if (!c->loaded) return set_err(c, KG_EINVAL, "no genotypes loaded");
+    if (iterations == 0) return set_err(c, KG_EINVAL, "iterations must be non-zero");
+    if (!(std::isnan(maf) || maf < 0.0) && maf > 1.0)
+        return set_err(c, KG_EINVAL, "Minimum allele frequency must be within 0 to 1");
+    int64_t ns = num_samples < 0 ? c->cohort.n_samples : num_samples;
+    if (ns > c->cohort.n_samples || ns == 0)
+        return set_err(c, KG_EINVAL, "Requested samples " + std::to_string(ns) + " exceeds total samples " +
+                                         std::to_string(c->cohort.n_samples));
+    int64_t np = ns * (ns + 1) / 2;
+    if (!out || out_cap < np) return set_err(c, KG_EINVAL, "output capacity must be at least num_samples*(num_samples+1)/2");
+    return guarded(c, [&]() -> int {
+        auto t0 = std::chrono::steady_clock::now();
+        int st = use_device(c);
+        if (st) return st;
+        std::string err;
+        cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+        cudaEventCreate(&ev0);
+        cudaEventCreate(&ev1);
+        cudaEventRecord(ev0, c->stream);
+        st = kg::prepare_cohort(c->cohort, c->cohort.raw.as<uint8_t>(), c->cohort.n_samples,
+                                c->cohort.n_sites, c->cohort.n_sites, true,
+                                c->af_set ? c->af.data() : nullptr, std::isnan(maf) ? -1.0 : maf,
+                                c->stream, err);
+        if (st) {
+            cudaEventDestroy(ev0);
+            cudaEventDestroy(ev1);
+            return set_err(c, st, err);
+        }
+        if (c->dout.reserve(sizeof(kg_output) * np) != cudaSuccess)
+            return set_err(c, KG_ENOMEM, "cannot allocate device output rows");
+        kg::PairJob jb;
+        jb.panel = &c->cohort;
+        jb.kind = 0;
+        jb.n_x = ns;
+        jb.d_out = c->dout.as<kg_output>();
+        std::vector<kg::PairJob> jobs{jb};
+        kg_run_stats stats{};
+        st = kg::run_pairs(jobs, run_config(c, iterations), c->ws, c->stream, stats, err);
+        cudaEventRecord(ev1, c->stream);
+        int st2 = copy_rows_out(c, c->dout, np, out, c->stream);
+        float dms = 0.f;
+        if (cudaEventElapsedTime(&dms, ev0, ev1) == cudaSuccess) stats.device_ms = dms;
+        cudaEventDestroy(ev0);
+        cudaEventDestroy(ev1);
+        stats.launches += 7;  // count, freq, two scans, compact, pad, pack
+        if (st2 && !st) st = st2;
+        stats.total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        c->last = stats;
+        if (n_out) *n_out = np;
+        if (st) return set_err(c, st, err.empty() ? c->err : err);
+        return KG_OK;
+    });
+}
+
+int kg_relatedness_coefficients(const uint8_t* codes, int64_t n_samples, int64_t n_sites,
+                                int64_t row_stride, const double* allele_frequencies, int64_t threads,
+                                uint64_t iterations, double maf, int64_t num_samples, kg_output* out,
+                                int64_t out_cap, int64_t* n_out) {
+    (void)threads;
+    kg_ctx* c = nullptr;
+    int st = kg_create(&c, 0, 0);
+    if (st) return st;
+    st = kg_load_genotypes(c, codes, n_samples, n_sites, row_stride);
+    if (!st && allele_frequencies) st = kg_set_allele_frequencies(c, allele_frequencies);
+    if (!st) st = kg_relatedness(c, num_samples, iterations, maf, out, out_cap, n_out);
+    kg_destroy(c);
+    return st;
+}
+
+int kg_relatedness_batch(kg_ctx* c, kg_cohort* cohorts, int n_cohorts, uint64_t iterations, double maf) {
+    if (!c) return KG_EINVAL;
+    if (!cohorts || n_cohorts <= 0) return set_err(c, KG_EINVAL, "no cohorts");
+    if (iterations == 0) return set_err(c, KG_EINVAL, "iterations must be non-zero");
+    return guarded(c, [&]() -> int {
+        auto t0 = std::chrono::steady_clock::now();
+        int st = use_device(c);
+        if (st) return st;
+        std::vector<std::unique_ptr<kg::Cohort>> prep;
+        std::vector<kg::PairJob> jobs;
+        std::vector<int> job_of(n_cohorts, -1);
+        std::vector<int64_t> offs(n_cohorts, 0);
+        int64_t total = 0;
+        std::string err;
+        for (int i = 0; i < n_cohorts; i++) {
+            kg_cohort& k = cohorts[i];
+            k.n_out = 0;
+            int64_t ns = k.num_samples < 0 ? k.n_samples : k.num_samples;
+            if (!k.codes || ns <= 0 || ns > k.n_samples || !k.out || k.out_cap < ns * (ns + 1) / 2) {
+                k.status = KG_EINVAL;
+                continue;
+            }
+            auto co = std::make_unique<kg::Cohort>();
+            std::string e1;
+            int s1 = kg::prepare_cohort(*co, k.codes, k.n_samples, k.n_sites, k.row_stride, false,
+                                        k.allele_frequencies, std::isnan(maf) ? -1.0 : maf, c->stream, e1);
+            k.status = s1;
+            if (s1) {
+                if (err.empty()) err = e1;
+                continue;
+            }
+            co->raw.release();  // packed planes are all the pair kernel needs
+            kg::PairJob jb;
+            jb.panel = co.get();
+            jb.kind = 0;
+            jb.n_x = ns;
+            offs[i] = total;
+            total += jb.n_pairs();
+            job_of[i] = (int)jobs.size();
+            jobs.push_back(jb);
+            prep.push_back(std::move(co));
+        }
+        if (jobs.empty()) return set_err(c, KG_EINVAL, err.empty() ? "no valid cohort" : err);
+        if (c->dout.reserve(sizeof(kg_output) * total) != cudaSuccess)
+            return set_err(c, KG_ENOMEM, "cannot allocate device output rows");
+        for (int i = 0; i < n_cohorts; i++)
+            if (job_of[i] >= 0) jobs[job_of[i]].d_out = c->dout.as<kg_output>() + offs[i];
+        kg_run_stats stats{};
+        st = kg::run_pairs(jobs, run_config(c, iterations), c->ws, c->stream, stats, err);
+        for (int i = 0; i < n_cohorts; i++) {
+            if (job_of[i] < 0) continue;
+            int64_t np = jobs[job_of[i]].n_pairs();
+            cudaError_t e = cudaMemcpyAsync(cohorts[i].out, c->dout.as<kg_output>() + offs[i],
+                                            sizeof(kg_output) * np, cudaMemcpyDeviceToHost, c->stream);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+            if (e != cudaSuccess) return set_err(c, KG_ECUDA, std::string("copy rows: ") + cudaGetErrorString(e));
+            cohorts[i].n_out = np;
+            if (st == KG_ENOSITES) {
+                for (int64_t r = 0; r < np; r++)
+                    if (std::isnan(cohorts[i].out[r].obj)) { cohorts[i].status = KG_ENOSITES; break; }
+            }
+        }
+        stats.total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        c->last = stats;
+        if (st) return set_err(c, st, err);
+        for (int i = 0; i < n_cohorts; i++)
+            if (cohorts[i].status) return set_err(c, cohorts[i].status, "cohort " + std::to_string(i) + " failed");
+        return KG_OK;
+    });
+}
+
+int kg_fp32_peak(int device, double* tflops) {
+    if (!tflops) return KG_EINVAL;
+    std::string err;
+    try {
+        return kg::fp32_peak(device, *tflops, err);
+    } catch (...) {
+        return KG_ECUDA;
+    }
+}
+
+int kg_last_run_stats(kg_ctx* c, kg_run_stats* s) {
+    if (!c || !s) return KG_EINVAL;
+    *s = c->last;
+    return KG_OK;
+}
+
+int kg_autotune(kg_ctx* c, int* wpb_out, int* bps_out) {
+    if (!c) return KG_EINVAL;
+    if (!c->loaded) return set_err(c, KG_EINVAL, "load genotypes first");
+    return guarded(c, [&]() -> int {
+        int st = use_device(c);
+        if (st) return st;
+        std::string err;
+        st = kg::prepare_cohort(c->cohort, c->cohort.raw.as<uint8_t>(), c->cohort.n_samples,
+                                c->cohort.n_sites, c->cohort.n_sites, true,
+                                c->af_set ? c->af.data() : nullptr, -1.0, c->stream, err);
+        if (st) return set_err(c, st, err);
+        int sm = 0;
+        cudaDeviceGetAttribute(&sm, cudaDevAttrMultiProcessorCount, c->device);
+        // a sample triangle with enough pairs to fill every candidate grid twice
+        int64_t want = (int64_t)sm * 16 * 2;
+        int64_t ns = 2;
+        while (ns < c->cohort.n_samples && ns * (ns + 1) / 2 < want) ns++;
+        int64_t np = ns * (ns + 1) / 2;
+        if (c->dout.reserve(sizeof(kg_output) * np) != cudaSuccess)
+            return set_err(c, KG_ENOMEM, "cannot allocate device output rows");
+        const int cand[][2] = {{4, 4}, {4, 3}, {2, 8}, {4, 2}, {1, 16}};
+        double best = 1e300;
+        int bw = 4, bb = 4;
+        for (auto& cd : cand) {
+            kg::PairJob jb;
+            jb.panel = &c->cohort;
+            jb.n_x = ns;
+            jb.d_out = c->dout.as<kg_output>();
+            kg::RunConfig cfg = run_config(c, 100);
+            cfg.warps_per_block = cd[0];
+            cfg.blocks_per_sm = cd[1];
+            kg_run_stats stt{};
+            st = kg::run_pairs({jb}, cfg, c->ws, c->stream, stt, err);
+            if (st && st != KG_ENOSITES) return set_err(c, st, err);
+            double cost = stt.pair_kernel_ms / std::max<double>(1.0, (double)stt.work_units);
+            if (cost < best) { best = cost; bw = cd[0]; bb = cd[1]; }
+        }
+        c->wpb = bw;
+        c->bps = bb;
+        if (wpb_out) *wpb_out = bw;
+        if (bps_out) *bps_out = bb;
+        return KG_OK;
+    });
+}
+
+// ---------------------------------------------------------------- serving
+
+int kg_panel_load(kg_ctx* c, const uint8_t* codes, int64_t n_samples, int64_t n_sites, int64_t row_stride,
+                  const double* af, double maf) {
+    if (!c) return KG_EINVAL;
+    return guarded(c, [&]() -> int {
+        int st = use_device(c);
+        if (st) return st;
+        std::unique_lock<std::mutex> lk(c->mu);
+        // wait for in-flight batches before replacing the panel
+        c->cv.wait(lk, [&] {
+            for (auto& s : c->slots) if (s.busy) return false;
+            return true;
+        });
+        std::string err;
+        c->panel_ready = false;
+        st = kg::prepare_cohort(c->panel, codes, n_samples, n_sites, row_stride, false, af,
+                                std::isnan(maf) ? -1.0 : maf, c->stream, err);
+        if (st) return set_err(c, st, err);
+        c->panel.raw.release();
+        c->panel_ready = true;
+        if (c->slots.empty()) {
+            c->slots.resize(2);
+            for (auto& s : c->slots)
+                if (cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking) != cudaSuccess)
+                    return set_err(c, KG_ECUDA, "cannot create serving streams");
+        }
+        if (!c->server.joinable()) {
+            c->stop = false;
+            c->server = std::thread(serve_loop, c);
+        }
+        return KG_OK;
+    });
+}
+
+int kg_submit(kg_ctx* c, const uint8_t* query_codes, int64_t n_query, int64_t row_stride,
+              const uint8_t* site_mask, uint64_t iterations, int64_t* request_id) {
+    if (!c) return KG_EINVAL;
+    if (!request_id) return set_err(c, KG_EINVAL, "request_id is NULL");
+    return guarded(c, [&]() -> int {
+        std::lock_guard<std::mutex> lk(c->mu);
+        if (!c->panel_ready) return set_err(c, KG_EINVAL, "no panel loaded");
+        const int64_t ns = c->panel.n_sites;
+        if (!query_codes || n_query <= 0 || row_stride < ns || iterations == 0)
+            return set_err(c, KG_EINVAL, "query rows must be positive and cover the panel's sites");
+        auto r = std::make_shared<Request>();
+        r->id = c->next_id++;
+        r->n_query = n_query;
+        r->iterations = iterations;
+        r->codes.resize((size_t)(n_query * ns));
+        for (int64_t i = 0; i < n_query; i++) {
+            const uint8_t* src = query_codes + i * row_stride;
+            for (int64_t s = 0; s < ns; s++)
+                if (src[s] > 3) return set_err(c, KG_EINVAL, "genotype codes must be 0, 1, 2 or 3 (missing)");
+            std::memcpy(r->codes.data() + i * ns, src, (size_t)ns);
+        }
+        if (site_mask) r->mask.assign(site_mask, site_mask + ns);
+        c->requests[r->id] = r;
+        c->pending.push_back(r->id);
+        *request_id = r->id;
+        c->cv.notify_all();
+        return KG_OK;
+    });
+}
+
+int kg_poll(kg_ctx* c, int64_t id, int* done) {
+    if (!c || !done) return KG_EINVAL;
+    std::lock_guard<std::mutex> lk(c->mu);
+    auto it = c->requests.find(id);
+    if (it == c->requests.end()) return set_err(c, KG_ENOTFOUND, "unknown request");
+    *done = it->second->done ? 1 : 0;
+    return KG_OK;
+}
+
+int kg_wait(kg_ctx* c, int64_t id, int64_t timeout_ms, kg_output* out, int64_t out_cap, int64_t* n_out) {
+    if (!c) return KG_EINVAL;
+    return guarded(c, [&]() -> int {
+        std::unique_lock<std::mutex> lk(c->mu);
+        auto it = c->requests.find(id);
+        if (it == c->requests.end()) return set_err(c, KG_ENOTFOUND, "unknown request");
+        auto r = it->second;
+        auto pred = [&] { return r->done; };
+        if (timeout_ms < 0) {
+            c->cv.wait(lk, pred);
+        } else if (!c->cv.wait_for(lk, std::chrono::milliseconds(timeout_ms), pred)) {
+            return set_err(c, KG_ETIMEOUT, "request still running");
+        }
+        if (r->cancelled) {
+            c->requests.erase(id);
+            return set_err(c, KG_ECANCELED, "request was cancelled");
+        }
+        if (r->status) {
+            std::string e = r->err;
+            int s = r->status;
+            c->requests.erase(id);
+            return set_err(c, s, e);
+        }
+        int64_t np = (int64_t)r->rows.size();
+        if (!out || out_cap < np) return set_err(c, KG_EINVAL, "output capacity too small");
+        std::memcpy(out, r->rows.data(), sizeof(kg_output) * np);
+        if (n_out) *n_out = np;
+        c->requests.erase(id);
+        return KG_OK;
+    });
+}
+
+int kg_cancel(kg_ctx* c, int64_t id) {
+    if (!c) return KG_EINVAL;
+    std::lock_guard<std::mutex> lk(c->mu);
+    auto it = c->requests.find(id);
+    if (it == c->requests.end()) return set_err(c, KG_ENOTFOUND, "unknown request");
+    it->second->cancelled = true;
+    auto& pq = c->pending;
+    auto pos = std::find(pq.begin(), pq.end(), id);
+    if (pos != pq.end()) {
+        pq.erase(pos);
+        it->second->done = true;
+        it->second->status = KG_ECANCELED;
+    }
+    c->cv.notify_all();
+    return KG_OK;
+}
+
+int kg_serving_stats(kg_ctx* c, int64_t* requests, int64_t* pairs, int64_t* launches) {
+    if (!c) return KG_EINVAL;
+    std::lock_guard<std::mutex> lk(c->mu);
+    if (requests) *requests = c->served_requests;
+    if (pairs) *pairs = c->served_pairs;
+    if (launches) *launches = c->served_launches;
+    return KG_OK;
+}
+
+}  // extern "C"

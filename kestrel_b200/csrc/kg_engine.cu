@@ -1,0 +1,669 @@
+// kg_engine.cu — device preparation kernels, the persistent pair kernel and
+// their host-side launch logic.
+//
+// Reference behaviour restated here:
+//   allele frequencies, count form      src/wrapper.rs:412-428
+//   maf zeroing + renormalisation        src/allele/mod.rs:120-126, default maf src/wrapper.rs:101
+//   non-segregating site drop            src/wrapper.rs:352-410
+//   per-pair driver, start points        src/coefficients.rs:77-136
+#include "kg_engine.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+#include "kg_pair.cuh"
+
+namespace kg {
+
+#define KG_CUDA_TRY(expr)                                                       \
+    do {                                                                        \
+        cudaError_t e_ = (expr);                                                \
+        if (e_ != cudaSuccess) {                                                \
+            err = std::string(#expr) + ": " + cudaGetErrorString(e_);           \
+            return e_ == cudaErrorMemoryAllocation ? KG_ENOMEM : KG_ECUDA;      \
+        }                                                                       \
+    } while (0)
+
+void DevBuf::release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+}
+
+int DevBuf::reserve(size_t n) {
+    if (n <= bytes && p) return cudaSuccess;
+    release();
+    if (n == 0) n = 16;
+    cudaError_t e = cudaMalloc(&p, n);
+    if (e != cudaSuccess) {
+        p = nullptr;
+        return e;
+    }
+    bytes = n;
+    return cudaSuccess;
+}
+
+size_t Cohort::device_bytes() const {
+    return raw.bytes + af.bytes + rc.bytes + oc.bytes + keep.bytes + kidx.bytes + bsum.bytes +
+           nkept.bytes + pfull.bytes + qfull.bytes + p32.bytes + p64.bytes + q64.bytes +
+           site_of.bytes + planes.bytes;
+}
+
+const char* engine_version() { return "kestrel-b200 0.1.0 (sm_100a)"; }
+
+// ------------------------------------------------------------ preparation
+
+constexpr int SCAN_BLOCK = 1024;
+
+// Per raw site: REF allele count and observed samples over all rows; flags any
+// code above 3.  Four sites per thread.
+__global__ void count_kernel(const uint8_t* __restrict__ codes, int64_t n_samples, int64_t n_sites,
+                             int64_t stride, int32_t* __restrict__ rc, int32_t* __restrict__ oc,
+                             int32_t* __restrict__ flags) {
+    int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= n_sites) return;
+    int r = 0, o = 0;
+    bool bad = false;
+    for (int64_t s = 0; s < n_samples; s++) {
+        unsigned c = codes[s * stride + v];
+        bad |= (c > 3u);
+        if (c < 3u) { r += 2 - (int)c; o += 1; }
+    }
+    rc[v] = r;
+    oc[v] = o;
+    if (bad) atomicOr(&flags[1], 1);
+}
+
+// Frequencies as the ML path sees them and the segregating flag.
+__global__ void freq_kernel(const int32_t* __restrict__ rc, const int32_t* __restrict__ oc,
+                            const double* __restrict__ af, int64_t n_sites, double maf,
+                            double* __restrict__ pf, double* __restrict__ qf,
+                            uint8_t* __restrict__ keep) {
+    int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= n_sites) return;
+    double x0, x1;
+    if (af) {
+        x0 = af[2 * v];
+        x1 = af[2 * v + 1];
+    } else {
+        if (oc[v] == 0) {
+            pf[v] = 0.0; qf[v] = 0.0; keep[v] = 0;
+            return;
+        }
+        double tot = 2.0 * (double)oc[v];
+        x0 = (double)rc[v] / tot;
+        x1 = (double)(2 * oc[v] - rc[v]) / tot;
+        if (x0 > 0.0 && x0 < maf) x0 = 0.0;
+        if (x1 > 0.0 && x1 < maf) x1 = 0.0;
+        double s = x0 + x1;
+        x0 = x0 / s;
+        x1 = x1 / s;
+    }
+    pf[v] = x0;
+    qf[v] = x1;
+    keep[v] = (x0 > 0.0 && x1 > 0.0) ? 1 : 0;
+}
+
+__device__ __forceinline__ int warp_incl_scan(int x, int lane) {
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        int t = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += t;
+    }
+    return x;
+}
+
+// Block-local exclusive scan of keep flags; block totals to bsum.
+__global__ void scan_block_kernel(const uint8_t* __restrict__ keep, int64_t n,
+                                  int32_t* __restrict__ kidx, int32_t* __restrict__ bsum) {
+    __shared__ int wsum[32];
+    int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    int64_t i = (int64_t)blockIdx.x * SCAN_BLOCK + threadIdx.x;
+    int v = (i < n) ? keep[i] : 0;
+    int x = warp_incl_scan(v, lane);
+    if (lane == 31) wsum[wid] = x;
+    __syncthreads();
+    if (wid == 0) {
+        int s = warp_incl_scan(wsum[lane], lane);
+        wsum[lane] = s;
+    }
+    __syncthreads();
+    int pre = (wid > 0 ? wsum[wid - 1] : 0) + x - v;
+    if (i < n) kidx[i] = pre;
+    if (threadIdx.x == SCAN_BLOCK - 1) bsum[blockIdx.x] = pre + v;
+}
+
+// Exclusive scan of the block totals in place (one block); total -> out[0].
+__global__ void scan_sums_kernel(int32_t* __restrict__ bsum, int64_t nb, int32_t* __restrict__ out) {
+    __shared__ int wsum[32];
+    __shared__ int carry;
+    int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    for (int64_t base = 0; base < nb; base += SCAN_BLOCK) {
+        int64_t i = base + threadIdx.x;
+        int v = (i < nb) ? bsum[i] : 0;
+        int x = warp_incl_scan(v, lane);
+        if (lane == 31) wsum[wid] = x;
+        __syncthreads();
+        if (wid == 0) {
+            int s = warp_incl_scan(wsum[lane], lane);
+            wsum[lane] = s;
+        }
+        __syncthreads();
+        int pre = carry + (wid > 0 ? wsum[wid - 1] : 0) + x - v;
+        if (i < nb) bsum[i] = pre;
+        __syncthreads();
+        if (threadIdx.x == SCAN_BLOCK - 1) carry = pre + v;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) out[0] = carry;
+}
+
+__global__ void compact_kernel(const uint8_t* __restrict__ keep, const int32_t* __restrict__ kidx,
+                               const int32_t* __restrict__ bsum, const double* __restrict__ pf,
+                               const double* __restrict__ qf, int64_t n, int32_t* __restrict__ site_of,
+                               float* __restrict__ p32, double* __restrict__ p64,
+                               double* __restrict__ q64) {
+    int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= n || !keep[v]) return;
+    int64_t k = (int64_t)kidx[v] + bsum[v / SCAN_BLOCK];
+    site_of[k] = (int32_t)v;
+    p64[k] = pf[v];
+    q64[k] = qf[v];
+    p32[k] = (float)pf[v];
+}
+
+__global__ void pad_kernel(const int32_t* __restrict__ nkept, int64_t cap, float* __restrict__ p32,
+                           double* __restrict__ p64, double* __restrict__ q64) {
+    int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x + nkept[0];
+    if (k >= cap) return;
+    p32[k] = 0.5f;
+    p64[k] = 0.5;
+    q64[k] = 0.5;
+}
+
+// Warp per (row, 32-site word): lanes fetch the codes of 32 kept sites and two
+// ballots build the {lo, hi} planes.  Padding and masked-out sites are 3.
+__global__ void pack_kernel(const uint8_t* __restrict__ raw, int64_t n_rows, int64_t stride,
+                            const int32_t* __restrict__ site_of, const int32_t* __restrict__ nkept,
+                            const uint8_t* __restrict__ mask, uint2* __restrict__ planes,
+                            int64_t plane_stride) {
+    int lane = threadIdx.x & 31;
+    int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    const int64_t nk = nkept[0];
+    const int64_t total = n_rows * plane_stride;
+    for (int64_t t = warp; t < total; t += nwarps) {
+        int64_t row = t / plane_stride;
+        int64_t word = t - row * plane_stride;
+        int64_t k = word * 32 + lane;
+        unsigned c = 3u;
+        if (k < nk) {
+            int32_t s = site_of[k];
+            c = raw[row * stride + s];
+            if (mask && !mask[s]) c = 3u;
+        }
+        unsigned lo = __ballot_sync(0xffffffffu, c & 1u);
+        unsigned hi = __ballot_sync(0xffffffffu, (c >> 1) & 1u);
+        if (lane == 0) planes[t] = make_uint2(lo, hi);
+    }
+}
+
+// 2-bit codes (16 per word) + observed mask (32 per word) -> byte codes.
+__global__ void unpack_2bit_kernel(const uint32_t* __restrict__ codes2,
+                                   const uint32_t* __restrict__ observed, int64_t n_rows,
+                                   int64_t n_sites, uint8_t* __restrict__ raw) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    int64_t total = n_rows * n_sites;
+    if (i >= total) return;
+    int64_t row = i / n_sites, s = i - row * n_sites;
+    int64_t w2 = (n_sites + 15) / 16, wm = (n_sites + 31) / 32;
+    unsigned c = (codes2[row * w2 + s / 16] >> (2 * (s % 16))) & 3u;
+    bool obs = (observed[row * wm + s / 32] >> (s % 32)) & 1u;
+    raw[i] = obs ? (uint8_t)c : (uint8_t)3;
+}
+
+static inline int64_t ceil_div(int64_t a, int64_t b) { return (a + b - 1) / b; }
+
+static int grid_for(int64_t n, int threads) { return (int)std::max<int64_t>(1, ceil_div(n, threads)); }
+
+int prepare_cohort(Cohort& c, const uint8_t* codes, int64_t n_samples, int64_t n_sites,
+                   int64_t row_stride, bool codes_on_device, const double* af, double maf,
+                   cudaStream_t st, std::string& err) {
+    if (n_samples <= 0 || n_sites <= 0 || row_stride < n_sites) {
+        err = "n_samples and n_sites must be positive and row_stride >= n_sites";
+        return KG_EINVAL;
+    }
+    if (n_sites > (int64_t)INT32_MAX || n_samples > (int64_t)INT32_MAX) {
+        err = "too many sites or samples";
+        return KG_EINVAL;
+    }
+    c.n_samples = n_samples;
+    c.n_sites = n_sites;
+    c.n_kept = -1;
+    c.n_seg_max = ceil_div(n_sites, SEG_SITES);
+    c.plane_stride = c.n_seg_max * SEG_WORDS;
+    const int64_t cap = c.n_seg_max * SEG_SITES;
+    const int64_t nb = ceil_div(n_sites, SCAN_BLOCK);
+    int64_t stride = row_stride;
+    if (!codes_on_device) {
+        KG_CUDA_TRY((cudaError_t)c.raw.reserve((size_t)(n_samples * n_sites)));
+        if (row_stride == n_sites) {
+            KG_CUDA_TRY(cudaMemcpyAsync(c.raw.p, codes, (size_t)(n_samples * n_sites),
+                                        cudaMemcpyHostToDevice, st));
+        } else {
+            KG_CUDA_TRY(cudaMemcpy2DAsync(c.raw.p, (size_t)n_sites, codes, (size_t)row_stride,
+                                          (size_t)n_sites, (size_t)n_samples,
+                                          cudaMemcpyHostToDevice, st));
+        }
+        stride = n_sites;
+    }
+    const uint8_t* draw = codes_on_device ? codes : c.raw.as<uint8_t>();
+    KG_CUDA_TRY((cudaError_t)c.rc.reserve(sizeof(int32_t) * n_sites));
+    KG_CUDA_TRY((cudaError_t)c.oc.reserve(sizeof(int32_t) * n_sites));
+    KG_CUDA_TRY((cudaError_t)c.keep.reserve((size_t)n_sites));
+    KG_CUDA_TRY((cudaError_t)c.kidx.reserve(sizeof(int32_t) * n_sites));
+    KG_CUDA_TRY((cudaError_t)c.bsum.reserve(sizeof(int32_t) * nb));
+    KG_CUDA_TRY((cudaError_t)c.nkept.reserve(sizeof(int32_t) * 4));
+    KG_CUDA_TRY((cudaError_t)c.pfull.reserve(sizeof(double) * n_sites));
+    KG_CUDA_TRY((cudaError_t)c.qfull.reserve(sizeof(double) * n_sites));
+    KG_CUDA_TRY((cudaError_t)c.p32.reserve(sizeof(float) * cap));
+    KG_CUDA_TRY((cudaError_t)c.p64.reserve(sizeof(double) * cap));
+    KG_CUDA_TRY((cudaError_t)c.q64.reserve(sizeof(double) * cap));
+    KG_CUDA_TRY((cudaError_t)c.site_of.reserve(sizeof(int32_t) * n_sites));
+    KG_CUDA_TRY((cudaError_t)c.planes.reserve(sizeof(uint2) * n_samples * c.plane_stride));
+    const double* daf = nullptr;
+    if (af) {
+        KG_CUDA_TRY((cudaError_t)c.af.reserve(sizeof(double) * 2 * n_sites));
+        KG_CUDA_TRY(cudaMemcpyAsync(c.af.p, af, sizeof(double) * 2 * n_sites,
+                                    cudaMemcpyHostToDevice, st));
+        daf = c.af.as<double>();
+    }
+    if (!(maf >= 0.0)) maf = 1.0 / (2.0 * (double)n_samples);
+    KG_CUDA_TRY(cudaMemsetAsync(c.nkept.p, 0, sizeof(int32_t) * 4, st));
+    count_kernel<<<grid_for(n_sites, 256), 256, 0, st>>>(draw, n_samples, n_sites, stride,
+                                                          c.rc.as<int32_t>(), c.oc.as<int32_t>(),
+                                                          c.nkept.as<int32_t>());
+    freq_kernel<<<grid_for(n_sites, 256), 256, 0, st>>>(c.rc.as<int32_t>(), c.oc.as<int32_t>(), daf,
+                                                         n_sites, maf, c.pfull.as<double>(),
+                                                         c.qfull.as<double>(), c.keep.as<uint8_t>());
+    scan_block_kernel<<<(int)nb, SCAN_BLOCK, 0, st>>>(c.keep.as<uint8_t>(), n_sites,
+                                                       c.kidx.as<int32_t>(), c.bsum.as<int32_t>());
+    scan_sums_kernel<<<1, SCAN_BLOCK, 0, st>>>(c.bsum.as<int32_t>(), nb, c.nkept.as<int32_t>());
+    compact_kernel<<<grid_for(n_sites, 256), 256, 0, st>>>(
+        c.keep.as<uint8_t>(), c.kidx.as<int32_t>(), c.bsum.as<int32_t>(), c.pfull.as<double>(),
+        c.qfull.as<double>(), n_sites, c.site_of.as<int32_t>(), c.p32.as<float>(),
+        c.p64.as<double>(), c.q64.as<double>());
+    pad_kernel<<<grid_for(cap, 256), 256, 0, st>>>(c.nkept.as<int32_t>(), cap, c.p32.as<float>(),
+                                                    c.p64.as<double>(), c.q64.as<double>());
+    {
+        int64_t work = n_samples * c.plane_stride;
+        int blocks = (int)std::min<int64_t>(ceil_div(work, 8), 148 * 32);
+        pack_kernel<<<blocks, 256, 0, st>>>(draw, n_samples, stride, c.site_of.as<int32_t>(),
+                                            c.nkept.as<int32_t>(), nullptr, c.planes.as<uint2>(),
+                                            c.plane_stride);
+    }
+    KG_CUDA_TRY(cudaGetLastError());
+    int32_t h[4];
+    KG_CUDA_TRY(cudaMemcpyAsync(h, c.nkept.p, sizeof(h), cudaMemcpyDeviceToHost, st));
+    KG_CUDA_TRY(cudaStreamSynchronize(st));
+    if (h[1]) {
+        err = "genotype codes must be 0, 1, 2 or 3 (missing)";
+        return KG_EINVAL;
+    }
+    c.n_kept = h[0];
+    if (c.n_kept == 0) {
+        err = "no segregating site left after allele-frequency filtering";
+        return KG_ENOSITES;
+    }
+    return KG_OK;
+}
+
+int unpack_2bit(DevBuf& raw, const uint32_t* codes2, const uint32_t* observed, int64_t n_samples,
+                int64_t n_sites, cudaStream_t st, std::string& err) {
+    if (!codes2 || !observed || n_samples <= 0 || n_sites <= 0) {
+        err = "invalid packed genotype arguments";
+        return KG_EINVAL;
+    }
+    int64_t w2 = ceil_div(n_sites, 16), wm = ceil_div(n_sites, 32);
+    DevBuf d2, dm;
+    KG_CUDA_TRY((cudaError_t)d2.reserve(sizeof(uint32_t) * w2 * n_samples));
+    KG_CUDA_TRY((cudaError_t)dm.reserve(sizeof(uint32_t) * wm * n_samples));
+    KG_CUDA_TRY((cudaError_t)raw.reserve((size_t)(n_samples * n_sites)));
+    KG_CUDA_TRY(cudaMemcpyAsync(d2.p, codes2, sizeof(uint32_t) * w2 * n_samples,
+                                cudaMemcpyHostToDevice, st));
+    KG_CUDA_TRY(cudaMemcpyAsync(dm.p, observed, sizeof(uint32_t) * wm * n_samples,
+                                cudaMemcpyHostToDevice, st));
+    unpack_2bit_kernel<<<grid_for(n_samples * n_sites, 256), 256, 0, st>>>(
+        d2.as<uint32_t>(), dm.as<uint32_t>(), n_samples, n_sites, raw.as<uint8_t>());
+    KG_CUDA_TRY(cudaGetLastError());
+    KG_CUDA_TRY(cudaStreamSynchronize(st));
+    return KG_OK;
+}
+
+int prepare_query(const Cohort& panel, QueryPlanes& q, const uint8_t* codes, int64_t n_rows,
+                  int64_t row_stride, const uint8_t* site_mask, cudaStream_t st, std::string& err) {
+    if (n_rows <= 0 || row_stride < panel.n_sites || !codes) {
+        err = "query rows must be positive and cover the panel's sites";
+        return KG_EINVAL;
+    }
+    const int64_t ns = panel.n_sites;
+    q.n_rows = n_rows;
+    KG_CUDA_TRY((cudaError_t)q.raw.reserve((size_t)(n_rows * ns)));
+    KG_CUDA_TRY(cudaMemcpy2DAsync(q.raw.p, (size_t)ns, codes, (size_t)row_stride, (size_t)ns,
+                                  (size_t)n_rows, cudaMemcpyHostToDevice, st));
+    const uint8_t* dmask = nullptr;
+    if (site_mask) {
+        KG_CUDA_TRY((cudaError_t)q.mask.reserve((size_t)ns));
+        KG_CUDA_TRY(cudaMemcpyAsync(q.mask.p, site_mask, (size_t)ns, cudaMemcpyHostToDevice, st));
+        dmask = q.mask.as<uint8_t>();
+    }
+    KG_CUDA_TRY((cudaError_t)q.planes.reserve(sizeof(uint2) * n_rows * panel.plane_stride));
+    int64_t work = n_rows * panel.plane_stride;
+    int blocks = (int)std::min<int64_t>(ceil_div(work, 8), 148 * 32);
+    pack_kernel<<<blocks, 256, 0, st>>>(q.raw.as<uint8_t>(), n_rows, ns, panel.site_of.as<int32_t>(),
+                                        panel.nkept.as<int32_t>(), dmask, q.planes.as<uint2>(),
+                                        panel.plane_stride);
+    KG_CUDA_TRY(cudaGetLastError());
+    return KG_OK;
+}
+
+// ----------------------------------------------------------- pair kernel
+
+__device__ __forceinline__ void decode_triangle(int64_t j, int64_t ns, int64_t& x, int64_t& y) {
+    // offset(x) = x*ns - x(x-1)/2 pairs precede row x
+    double b = 2.0 * (double)ns + 1.0;
+    double disc = b * b - 8.0 * (double)j;
+    int64_t xi = (int64_t)floor((b - sqrt(fmax(disc, 0.0))) * 0.5);
+    if (xi < 0) xi = 0;
+    if (xi > ns - 1) xi = ns - 1;
+    auto off = [ns](int64_t r) { return r * ns - r * (r - 1) / 2; };
+    while (xi > 0 && off(xi) > j) xi--;
+    while (xi + 1 < ns && off(xi + 1) <= j) xi++;
+    x = xi;
+    y = xi + (j - off(xi));
+}
+
+extern "C" __global__ void __launch_bounds__(128, 4)
+jacquard_pair_kernel(PairLaunch L) {
+    extern __shared__ __align__(16) char smem[];
+    const int lane = threadIdx.x & 31;
+    const int wib = threadIdx.x >> 5;
+    const int64_t gw = (int64_t)blockIdx.x * (blockDim.x >> 5) + wib;
+    char* wsm = smem + wib * WARP_SMEM;
+    uint16_t* buf = reinterpret_cast<uint16_t*>(wsm);
+    uint16_t* ent = L.scratch + gw * L.scratch_stride;
+    uint16_t* hdr = L.headers + gw * L.header_stride;
+    unsigned long long c_gh = 0, c_obj = 0, c_f64 = 0, c_f64p = 0, c_sites = 0, c_work = 0,
+                       c_nosite = 0, c_nonconv = 0, c_fl32 = 0, c_fl64 = 0;
+    unsigned long long c_shape[5] = {0, 0, 0, 0, 0};
+    for (;;) {
+        unsigned long long k = 0;
+        if (lane == 0) k = atomicAdd(L.queue, 1ull);
+        k = __shfl_sync(0xffffffffu, k, 0);
+        if (k >= (unsigned long long)L.total_pairs) break;
+        int c = 0;
+        while (c + 1 < L.n_cohorts && (int64_t)k >= L.cohorts[c + 1].pair_begin) c++;
+        const CohortDev& co = L.cohorts[c];
+        const int64_t j = (int64_t)k - co.pair_begin;
+        int64_t x, y;
+        if (co.kind == COHORT_TRIANGLE) {
+            decode_triangle(j, co.n_x, x, y);
+        } else {
+            x = j / co.n_y;
+            y = j - x * co.n_y;
+        }
+        int64_t shape_n[5];
+        const int64_t n = sort_pair(co, x, y, ent, hdr, buf, lane, shape_n);
+        kg_output row;
+        row.x = (uint64_t)x;
+        row.y = (uint64_t)y;
+        if (n == 0) {
+            for (int i = 0; i < 9; i++) row.jacquard[i] = CUDART_NAN;
+            row.obj = CUDART_NAN;
+            row.iters = 0;
+            row.cond = CUDART_NAN;
+            c_nosite++;
+        } else {
+            PairResult res;
+            const bool self_pair = (co.kind == COHORT_TRIANGLE) && (x == y);
+            solve_pair(co, ent, hdr, n, self_pair, L.precision, L.tune, lane, wsm, res);
+            for (int i = 0; i < 9; i++) row.jacquard[i] = res.x[i];
+            row.obj = res.f;
+            row.iters = res.iters;
+            row.cond = res.cond;
+            c_gh += res.gh_passes;
+            c_obj += res.obj_passes;
+            c_f64 += res.fp64_passes;
+            c_f64p += res.escalated ? 1 : 0;
+            c_sites += (unsigned long long)n;
+            c_work += (unsigned long long)n * (unsigned long long)res.gh_passes;
+            c_nonconv += (res.iters >= L.tune.sqp_max_iter) ? 1 : 0;
+            const int p32 = res.gh_passes - res.fp64_passes;
+#pragma unroll
+            for (int s = 0; s < 5; s++) {
+                c_shape[s] += (unsigned long long)shape_n[s];
+                c_fl32 += (unsigned long long)shape_n[s] *
+                          (unsigned long long)(p32 * flops_direct(s) + res.diff_passes * flops_diff_extra(s));
+                c_fl64 += (unsigned long long)shape_n[s] * (unsigned long long)(res.fp64_passes * flops_direct(s));
+            }
+        }
+        // 14 eight-byte words per row, one per lane
+        const uint64_t* src = reinterpret_cast<const uint64_t*>(&row);
+        uint64_t* dst = reinterpret_cast<uint64_t*>(co.out + j);
+        uint64_t wv = 0;
+#pragma unroll
+        for (int i = 0; i < 14; i++)
+            if (lane == i) wv = src[i];
+        if (lane < 14) dst[lane] = wv;
+    }
+    if (lane == 0) {
+        atomicAdd(&L.counters->gh_passes, c_gh);
+        atomicAdd(&L.counters->obj_passes, c_obj);
+        atomicAdd(&L.counters->fp64_passes, c_f64);
+        atomicAdd(&L.counters->fp64_pairs, c_f64p);
+        atomicAdd(&L.counters->pair_sites, c_sites);
+        atomicAdd(&L.counters->work_units, c_work);
+        atomicAdd(&L.counters->nosite_pairs, c_nosite);
+        atomicAdd(&L.counters->nonconverged, c_nonconv);
+        atomicAdd(&L.counters->flops_fp32, c_fl32);
+        atomicAdd(&L.counters->flops_fp64, c_fl64);
+        for (int s = 0; s < 5; s++) atomicAdd(&L.counters->shape_sites[s], c_shape[s]);
+    }
+}
+
+static_assert(sizeof(kg_output) == 14 * 8, "kg_output must be 112 bytes");
+
+void default_launch(int& warps_per_block, int& blocks_per_sm) {
+    warps_per_block = 4;
+    blocks_per_sm = 4;
+}
+
+size_t scratch_bytes_per_warp(int64_t n_segments) {
+    return (size_t)n_segments * (SEG_SITES * sizeof(uint16_t) + SEG_HDR * sizeof(uint16_t));
+}
+
+int run_pairs(const std::vector<PairJob>& jobs, const RunConfig& cfg, Workspace& ws,
+              cudaStream_t st, kg_run_stats& stats, std::string& err) {
+    std::memset(&stats, 0, sizeof(stats));
+    if (jobs.empty()) return KG_OK;
+    int dev = 0;
+    KG_CUDA_TRY(cudaGetDevice(&dev));
+    if (ws.sm_count == 0) KG_CUDA_TRY(cudaDeviceGetAttribute(&ws.sm_count, cudaDevAttrMultiProcessorCount, dev));
+    int wpb = cfg.warps_per_block, bps = cfg.blocks_per_sm;
+    {
+        int dw, db;
+        default_launch(dw, db);
+        if (wpb <= 0) wpb = dw;
+        if (bps <= 0) bps = db;
+    }
+    wpb = std::min(std::max(wpb, 1), 4);
+    const size_t smem = (size_t)wpb * WARP_SMEM;
+    {
+        static bool attr_set = false;
+        if (!attr_set) {
+            KG_CUDA_TRY(cudaFuncSetAttribute(jacquard_pair_kernel,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             4 * WARP_SMEM));
+            attr_set = true;
+        }
+        int occ = 0;
+        KG_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, jacquard_pair_kernel,
+                                                                  wpb * 32, smem));
+        if (occ <= 0) {
+            err = "pair kernel cannot be resident with this launch shape";
+            return KG_ECUDA;
+        }
+        bps = std::min(bps, occ);
+    }
+    int64_t total_pairs = 0;
+    int64_t seg_cap = 1;
+    std::vector<CohortDev> table(jobs.size());
+    for (size_t i = 0; i < jobs.size(); i++) {
+        const PairJob& jb = jobs[i];
+        const Cohort& pn = *jb.panel;
+        CohortDev& d = table[i];
+        d.planes_y = pn.planes.as<uint2>();
+        d.planes_x = (jb.kind == COHORT_RECT) ? jb.query->planes.as<uint2>() : d.planes_y;
+        d.plane_stride = pn.plane_stride;
+        d.p32 = pn.p32.as<float>();
+        d.p64 = pn.p64.as<double>();
+        d.q64 = pn.q64.as<double>();
+        d.n_sites = (int32_t)pn.n_kept;
+        d.n_segments = (int32_t)ceil_div(pn.n_kept, SEG_SITES);
+        d.kind = jb.kind;
+        d.pad = 0;
+        d.n_x = jb.n_x;
+        d.n_y = jb.n_y;
+        d.pair_begin = total_pairs;
+        d.n_pairs = jb.n_pairs();
+        d.out = jb.d_out;
+        total_pairs += d.n_pairs;
+        seg_cap = std::max<int64_t>(seg_cap, d.n_segments);
+    }
+    if (total_pairs == 0) return KG_OK;
+    int64_t blocks = (int64_t)ws.sm_count * bps;
+    int64_t warps = blocks * wpb;
+    int64_t need_warps = std::min<int64_t>(warps, total_pairs);
+    if (cfg.max_warps > 0) need_warps = std::min<int64_t>(need_warps, cfg.max_warps);
+    blocks = std::max<int64_t>(1, ceil_div(need_warps, wpb));
+    warps = blocks * wpb;
+    const int64_t ent_stride = seg_cap * SEG_SITES;
+    const int64_t hdr_stride = seg_cap * SEG_HDR;
+    if (ws.warps < warps || ws.seg_cap < seg_cap) {
+        int64_t w = std::max(ws.warps, warps), s = std::max(ws.seg_cap, seg_cap);
+        KG_CUDA_TRY((cudaError_t)ws.scratch.reserve(sizeof(uint16_t) * w * s * SEG_SITES));
+        KG_CUDA_TRY((cudaError_t)ws.headers.reserve(sizeof(uint16_t) * w * s * SEG_HDR));
+        ws.warps = w;
+        ws.seg_cap = s;
+    }
+    KG_CUDA_TRY((cudaError_t)ws.queue.reserve(sizeof(unsigned long long)));
+    KG_CUDA_TRY((cudaError_t)ws.counters.reserve(sizeof(RunCounters)));
+    KG_CUDA_TRY((cudaError_t)ws.table.reserve(sizeof(CohortDev) * table.size()));
+    KG_CUDA_TRY(cudaMemcpyAsync(ws.table.p, table.data(), sizeof(CohortDev) * table.size(),
+                                cudaMemcpyHostToDevice, st));
+    KG_CUDA_TRY(cudaMemsetAsync(ws.queue.p, 0, sizeof(unsigned long long), st));
+    KG_CUDA_TRY(cudaMemsetAsync(ws.counters.p, 0, sizeof(RunCounters), st));
+    PairLaunch L;
+    L.cohorts = ws.table.as<CohortDev>();
+    L.n_cohorts = (int)table.size();
+    L.precision = cfg.precision;
+    L.total_pairs = total_pairs;
+    L.queue = ws.queue.as<unsigned long long>();
+    L.scratch = ws.scratch.as<uint16_t>();
+    L.headers = ws.headers.as<uint16_t>();
+    // strides use the workspace's segment capacity so rows never overlap
+    L.scratch_stride = ws.seg_cap * SEG_SITES;
+    L.header_stride = ws.seg_cap * SEG_HDR;
+    (void)ent_stride;
+    (void)hdr_stride;
+    L.tune = make_tune(cfg.iterations);
+    L.counters = ws.counters.as<RunCounters>();
+    cudaEvent_t e0, e1;
+    KG_CUDA_TRY(cudaEventCreate(&e0));
+    KG_CUDA_TRY(cudaEventCreate(&e1));
+    cudaEventRecord(e0, st);
+    jacquard_pair_kernel<<<(int)blocks, wpb * 32, smem, st>>>(L);
+    cudaError_t le = cudaGetLastError();
+    cudaEventRecord(e1, st);
+    if (le != cudaSuccess) {
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        err = std::string("pair kernel launch: ") + cudaGetErrorString(le);
+        return KG_ECUDA;
+    }
+    RunCounters rc;
+    cudaError_t ce = cudaMemcpyAsync(&rc, ws.counters.p, sizeof(rc), cudaMemcpyDeviceToHost, st);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(st);
+    float ms = 0.f;
+    if (ce == cudaSuccess) cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (ce != cudaSuccess) {
+        err = std::string("pair kernel: ") + cudaGetErrorString(ce);
+        return KG_ECUDA;
+    }
+    stats.gh_passes = rc.gh_passes;
+    stats.obj_passes = rc.obj_passes;
+    stats.fp64_passes = rc.fp64_passes;
+    stats.fp64_pairs = rc.fp64_pairs;
+    stats.pair_sites = rc.pair_sites;
+    stats.work_units = rc.work_units;
+    stats.launches = 1;
+    stats.flops_fp32 = rc.flops_fp32;
+    stats.flops_fp64 = rc.flops_fp64;
+    for (int s = 0; s < 5; s++) stats.shape_sites[s] = rc.shape_sites[s];
+    stats.pair_kernel_ms = ms;
+    if (rc.nosite_pairs) {
+        err = "a pair has no jointly observed segregating site (its row is NaN)";
+        return KG_ENOSITES;
+    }
+    return KG_OK;
+}
+
+// FFMA throughput probe: 16 independent register chains per thread.
+__global__ void fma_peak_kernel(float* out, int iters, float b, float c) {
+    float a[16];
+#pragma unroll
+    for (int k = 0; k < 16; k++) a[k] = (float)(threadIdx.x + k) * 1e-3f;
+    for (int i = 0; i < iters; i++) {
+#pragma unroll
+        for (int k = 0; k < 16; k++) a[k] = fmaf(a[k], b, c);
+    }
+    float s = 0.f;
+#pragma unroll
+    for (int k = 0; k < 16; k++) s += a[k];
+    if (s == 12345.678f) out[threadIdx.x] = s;  // keeps the chains live
+}
+
+int fp32_peak(int device, double& tflops, std::string& err) {
+    KG_CUDA_TRY(cudaSetDevice(device));
+    int sm = 0;
+    KG_CUDA_TRY(cudaDeviceGetAttribute(&sm, cudaDevAttrMultiProcessorCount, device));
+    DevBuf out;
+    KG_CUDA_TRY((cudaError_t)out.reserve(1024 * sizeof(float)));
+    const int threads = 256, blocks = sm * 8, iters = 8192;
+    cudaEvent_t e0, e1;
+    KG_CUDA_TRY(cudaEventCreate(&e0));
+    KG_CUDA_TRY(cudaEventCreate(&e1));
+    fma_peak_kernel<<<blocks, threads>>>(out.as<float>(), 256, 0.999f, 1e-4f);  // warm-up
+    cudaEventRecord(e0);
+    fma_peak_kernel<<<blocks, threads>>>(out.as<float>(), iters, 0.999f, 1e-4f);
+    cudaEventRecord(e1);
+    cudaError_t e = cudaEventSynchronize(e1);
+    float ms = 0.f;
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (e != cudaSuccess) {
+        err = cudaGetErrorString(e);
+        return KG_ECUDA;
+    }
+    double flops = 2.0 * 16.0 * (double)iters * (double)threads * (double)blocks;
+    tflops = flops / ((double)ms * 1e-3) / 1e12;
+    return KG_OK;
+}
+
+}  // namespace kg

@@ -1,0 +1,122 @@
+// kg_engine.h — host-side engine of libkestrel_gpu.so (internal C++ API).
+//
+// Device-resident cohorts (bit-plane genotypes, allele frequencies of the kept
+// sites) and the launch of the persistent pair kernel.  The C ABI in kg_api.cu
+// is a thin layer over this.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "kestrel_gpu.h"
+
+namespace kg {
+
+// Owning device buffer.
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    DevBuf(DevBuf&& o) noexcept : p(o.p), bytes(o.bytes) { o.p = nullptr; o.bytes = 0; }
+    DevBuf& operator=(DevBuf&& o) noexcept {
+        if (this != &o) { release(); p = o.p; bytes = o.bytes; o.p = nullptr; o.bytes = 0; }
+        return *this;
+    }
+    ~DevBuf() { release(); }
+    void release();
+    // Grows to at least n bytes (contents not kept).  Returns a cudaError_t.
+    int reserve(size_t n);
+    template <class T> T* as() const { return static_cast<T*>(p); }
+};
+
+// A cohort prepared on the device: allele counts, frequencies, the kept
+// (segregating) sites compacted and every sample packed into {lo, hi} bit
+// planes of 32 kept sites (code = 2*hi + lo; 3 = missing or padding).
+struct Cohort {
+    int64_t n_samples = 0;
+    int64_t n_sites = 0;       // raw sites
+    int64_t plane_stride = 0;  // uint2 words per sample row
+    int64_t n_seg_max = 0;     // segments for n_sites (upper bound of the kept count)
+    int64_t n_kept = -1;       // read back after preparation (-1 = not yet)
+    DevBuf raw;                // uint8 codes, n_samples x n_sites
+    DevBuf af;                 // caller frequencies, n_sites x 2 (optional)
+    DevBuf rc, oc;             // int32 REF allele count, observed samples
+    DevBuf keep;               // uint8
+    DevBuf kidx;               // int32 exclusive prefix of keep
+    DevBuf bsum;               // int32 block sums of the scan
+    DevBuf nkept;              // int32[2]: kept count, bad-code flag
+    DevBuf pfull, qfull;       // double per raw site
+    DevBuf p32, p64, q64;      // per kept site, padded to n_seg_max * 2048
+    DevBuf site_of;            // int32 kept index -> raw site
+    DevBuf planes;             // uint2 [n_samples][plane_stride]
+    size_t device_bytes() const;
+};
+
+// Enqueues the preparation of a cohort on `st`.  codes are host memory unless
+// codes_on_device; af may be NULL.  maf < 0 selects 1/(2 n_samples).
+int prepare_cohort(Cohort& c, const uint8_t* codes, int64_t n_samples, int64_t n_sites,
+                   int64_t row_stride, bool codes_on_device, const double* af, double maf,
+                   cudaStream_t st, std::string& err);
+
+// Unpacks the VCF reader's 2-bit codes + observed mask into device byte codes.
+int unpack_2bit(DevBuf& raw, const uint32_t* codes2, const uint32_t* observed, int64_t n_samples,
+                int64_t n_sites, cudaStream_t st, std::string& err);
+
+// Packs query rows against a prepared panel (same raw site order); sites with
+// mask[s] == 0 become missing.  Host inputs.
+struct QueryPlanes {
+    int64_t n_rows = 0;
+    DevBuf raw;
+    DevBuf mask;
+    DevBuf planes;
+};
+int prepare_query(const Cohort& panel, QueryPlanes& q, const uint8_t* codes, int64_t n_rows,
+                  int64_t row_stride, const uint8_t* site_mask, cudaStream_t st, std::string& err);
+
+// One unit of pair work for the persistent kernel.
+struct PairJob {
+    const Cohort* panel = nullptr;      // frequencies, kept sites and (triangle) planes
+    const QueryPlanes* query = nullptr; // rect jobs: x rows
+    int kind = 0;                       // 0 triangle over panel rows, 1 rect query x panel
+    int64_t n_x = 0;                    // triangle: num_samples; rect: query rows
+    int64_t n_y = 0;                    // rect: panel rows
+    kg_output* d_out = nullptr;         // device rows
+    int64_t n_pairs() const { return kind == 0 ? n_x * (n_x + 1) / 2 : n_x * n_y; }
+};
+
+struct RunConfig {
+    int precision = KG_PREC_FP32C;
+    uint64_t iterations = 100;
+    int warps_per_block = 0;   // 0 = default
+    int blocks_per_sm = 0;     // 0 = default
+    int64_t max_warps = 0;     // 0 = no cap (cap the grid for small jobs)
+};
+
+// Reusable device workspace of the pair kernel (scratch lists, queue, table).
+struct Workspace {
+    DevBuf scratch, headers, queue, counters, table;
+    int64_t warps = 0;
+    int64_t seg_cap = 0;
+    int sm_count = 0;
+};
+
+int run_pairs(const std::vector<PairJob>& jobs, const RunConfig& cfg, Workspace& ws,
+              cudaStream_t st, kg_run_stats& stats, std::string& err);
+
+// Default launch shape for the device.
+void default_launch(int& warps_per_block, int& blocks_per_sm);
+
+// Bytes of scratch per warp for n segments.
+size_t scratch_bytes_per_warp(int64_t n_segments);
+
+const char* engine_version();
+
+// Measured FFMA throughput (TFLOP/s).
+int fp32_peak(int device, double& tflops, std::string& err);
+
+}  // namespace kg

@@ -1,0 +1,95 @@
+/*
+ * kestrel_oracle.h — TEST INFRASTRUCTURE ONLY.
+ *
+ * FP64 CPU restatement of the reference's all-pairs maximum-likelihood Jacquard
+ * estimator (malariagen/kestrel v0.1.2, the GL/PL path of
+ * src/coefficients.rs:40-141 driven by src/wrapper.rs:89-207), applied to hard
+ * genotype calls.  It is the checker for the CUDA product path and the timed CPU
+ * baseline; nothing in the product links or calls it.
+ *
+ * Parity status: UNPINNED by the reference itself.  The reference is Rust, no
+ * Rust toolchain exists on this machine, and the reference ships no tests, golden
+ * vectors or fixtures for this path.  The restatement is pinned instead by
+ * independent checks (a numpy evaluation of f, g and H, planted-relationship
+ * recovery, the (x,y)/(y,x) swap symmetry and hand-derived small cases).
+ *
+ * Genotype codes (sample-major, one byte per call):
+ *   0 = 0/0, 1 = 0/1, 2 = 1/1   (the reference's unphased triangular index,
+ *                               src/coefficients.rs:19-38)
+ *   3 = missing call            (the reference's NaN likelihood row,
+ *                               src/vcf.rs:397, dropped per pair by
+ *                               src/lanevector.rs:99-104)
+ */
+#ifndef KESTREL_ORACLE_H
+#define KESTREL_ORACLE_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* One row of the reference's output (src/coefficients.rs:143-151). */
+typedef struct {
+    uint64_t x, y;
+    double jacquard[9];
+    double obj;
+    uint64_t iters;
+    double cond;
+} kor_output;
+
+enum {
+    KOR_OK = 0,
+    KOR_EINVAL = 1,
+    KOR_ENOMEM = 2,
+    KOR_ENOSITES = 5
+};
+
+/* Per-site allele counts over observed samples (all n_samples rows). */
+int kor_allele_counts(const uint8_t *codes, int64_t n_samples, int64_t n_sites,
+                      int64_t stride, int32_t *ref_count, int32_t *obs_count);
+
+/* Allele frequencies as the ML path would see them: count form, maf zeroing
+ * (src/allele/mod.rs:120-126), renormalisation, and the non-segregating drop
+ * (src/wrapper.rs:366-383).  af_in (n_sites x 2, [ref, alt]) overrides the
+ * estimate when non-NULL (then only the zero drop applies).  maf < 0 selects the
+ * default 1/(2 n_samples) (src/wrapper.rs:101).  Writes p (ref) and q (alt) and
+ * keep[s] = 1 for segregating sites; returns the number kept in *n_kept. */
+int kor_site_frequencies(const uint8_t *codes, int64_t n_samples, int64_t n_sites,
+                         int64_t stride, const double *af_in, double maf,
+                         double *p, double *q, uint8_t *keep, int64_t *n_kept);
+
+/* Full all-pairs run for pairs (x, y), 0 <= x <= y < num_samples, in the
+ * reference's row order.  num_samples < 0 means all.  threads <= 0 means all
+ * OpenMP threads.  out must hold num_samples*(num_samples+1)/2 rows. */
+int kor_relatedness(const uint8_t *codes, int64_t n_samples, int64_t n_sites,
+                    int64_t stride, const double *af_in, int64_t num_samples,
+                    uint64_t iterations, double maf, int threads,
+                    kor_output *out, int64_t out_cap, int64_t *n_out);
+
+/* The same estimator for an explicit list of pairs, given frequencies already
+ * computed by kor_site_frequencies.  Used for sampled parity checks and the
+ * bounded CPU baseline. */
+int kor_relatedness_pairs(const uint8_t *codes, int64_t n_sites, int64_t stride,
+                          const double *p, const double *q, const uint8_t *keep,
+                          const int64_t *pair_x, const int64_t *pair_y,
+                          int64_t n_pairs, uint64_t iterations, int threads,
+                          kor_output *out);
+
+/* f, g, H of one pair at a fixed delta (src/jacquard/objective.rs:9-20,
+ * src/jacquard/grad_hess.rs:13-41).  H is 9x9 row-major.  *n_sites_used gets the
+ * number of jointly observed segregating sites. */
+int kor_eval_pair(const uint8_t *codes_x, const uint8_t *codes_y, int64_t n_sites,
+                  const double *p, const double *q, const uint8_t *keep,
+                  const double delta[9], double *f, double g[9], double h[81],
+                  int64_t *n_sites_used);
+
+/* Pass counters of the last kor_relatedness_pairs call on this thread group:
+ * total grad/Hessian passes and objective passes summed over pairs. */
+void kor_pass_counts(uint64_t *gh_passes, uint64_t *obj_passes);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif
