@@ -165,10 +165,12 @@ def config0(seed: int = 0) -> Cohort:
 
 
 def config1(seed: int = 1, n_samples: int = 1024, n_sites: int = 100_000) -> Cohort:
-    """N=1024 x M=100,000 with 64 each of PO, FS, HS and FC pairs planted."""
+    """N=1024 x M=100,000 with 64 each of PO, FS, HS and FC pairs planted (fewer,
+    n_samples // 16 each, for smaller test cohorts)."""
+    k = min(64, n_samples // 16)
     return make_cohort(n_samples, n_sites, seed,
-                       planted={"parent_offspring": 64, "full_sib": 64,
-                                "half_sib": 64, "first_cousin": 64},
+                       planted={"parent_offspring": k, "full_sib": k,
+                                "half_sib": k, "first_cousin": k},
                        name="cfg1")
 
 
