@@ -164,7 +164,7 @@ __global__ void scan_sums_kernel(int32_t* __restrict__ bsum, int64_t nb, int32_t
 __global__ void compact_kernel(const uint8_t* __restrict__ keep, const int32_t* __restrict__ kidx,
                                const int32_t* __restrict__ bsum, const double* __restrict__ pf,
                                const double* __restrict__ qf, int64_t n, int32_t* __restrict__ site_of,
-                               float* __restrict__ p32, double* __restrict__ p64,
+                               float2* __restrict__ pq32, double* __restrict__ p64,
                                double* __restrict__ q64) {
     int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (v >= n || !keep[v]) return;
@@ -172,14 +172,14 @@ __global__ void compact_kernel(const uint8_t* __restrict__ keep, const int32_t* 
     site_of[k] = (int32_t)v;
     p64[k] = pf[v];
     q64[k] = qf[v];
-    p32[k] = (float)pf[v];
+    pq32[k] = make_float2((float)pf[v], (float)qf[v]);
 }
 
-__global__ void pad_kernel(const int32_t* __restrict__ nkept, int64_t cap, float* __restrict__ p32,
+__global__ void pad_kernel(const int32_t* __restrict__ nkept, int64_t cap, float2* __restrict__ pq32,
                            double* __restrict__ p64, double* __restrict__ q64) {
     int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x + nkept[0];
     if (k >= cap) return;
-    p32[k] = 0.5f;
+    pq32[k] = make_float2(0.5f, 0.5f);
     p64[k] = 0.5;
     q64[k] = 0.5;
 }
@@ -269,7 +269,7 @@ int prepare_cohort(Cohort& c, const uint8_t* codes, int64_t n_samples, int64_t n
     KG_CUDA_TRY((cudaError_t)c.nkept.reserve(sizeof(int32_t) * 4));
     KG_CUDA_TRY((cudaError_t)c.pfull.reserve(sizeof(double) * n_sites));
     KG_CUDA_TRY((cudaError_t)c.qfull.reserve(sizeof(double) * n_sites));
-    KG_CUDA_TRY((cudaError_t)c.p32.reserve(sizeof(float) * cap));
+    KG_CUDA_TRY((cudaError_t)c.p32.reserve(sizeof(float2) * cap));
     KG_CUDA_TRY((cudaError_t)c.p64.reserve(sizeof(double) * cap));
     KG_CUDA_TRY((cudaError_t)c.q64.reserve(sizeof(double) * cap));
     KG_CUDA_TRY((cudaError_t)c.site_of.reserve(sizeof(int32_t) * n_sites));
@@ -294,9 +294,9 @@ int prepare_cohort(Cohort& c, const uint8_t* codes, int64_t n_samples, int64_t n
     scan_sums_kernel<<<1, SCAN_BLOCK, 0, st>>>(c.bsum.as<int32_t>(), nb, c.nkept.as<int32_t>());
     compact_kernel<<<grid_for(n_sites, 256), 256, 0, st>>>(
         c.keep.as<uint8_t>(), c.kidx.as<int32_t>(), c.bsum.as<int32_t>(), c.pfull.as<double>(),
-        c.qfull.as<double>(), n_sites, c.site_of.as<int32_t>(), c.p32.as<float>(),
+        c.qfull.as<double>(), n_sites, c.site_of.as<int32_t>(), c.p32.as<float2>(),
         c.p64.as<double>(), c.q64.as<double>());
-    pad_kernel<<<grid_for(cap, 256), 256, 0, st>>>(c.nkept.as<int32_t>(), cap, c.p32.as<float>(),
+    pad_kernel<<<grid_for(cap, 256), 256, 0, st>>>(c.nkept.as<int32_t>(), cap, c.p32.as<float2>(),
                                                     c.p64.as<double>(), c.q64.as<double>());
     {
         int64_t work = n_samples * c.plane_stride;
@@ -393,9 +393,7 @@ jacquard_pair_kernel(PairLaunch L) {
     const int wib = threadIdx.x >> 5;
     const int64_t gw = (int64_t)blockIdx.x * (blockDim.x >> 5) + wib;
     char* wsm = smem + wib * WARP_SMEM;
-    uint16_t* buf = reinterpret_cast<uint16_t*>(wsm);
-    uint16_t* ent = L.scratch + gw * L.scratch_stride;
-    uint16_t* hdr = L.headers + gw * L.header_stride;
+    void* lists = L.lists + gw * L.list_stride;
     unsigned long long c_gh = 0, c_obj = 0, c_f64 = 0, c_f64p = 0, c_sites = 0, c_work = 0,
                        c_nosite = 0, c_nonconv = 0, c_fl32 = 0, c_fl64 = 0;
     unsigned long long c_shape[5] = {0, 0, 0, 0, 0};
@@ -415,21 +413,27 @@ jacquard_pair_kernel(PairLaunch L) {
             x = j / co.n_y;
             y = j - x * co.n_y;
         }
-        int64_t shape_n[5];
-        const int64_t n = sort_pair(co, x, y, ent, hdr, buf, lane, shape_n);
+        PairLists pl;
+        count_shapes(co, x, y, lane, pl);
         kg_output row;
         row.x = (uint64_t)x;
         row.y = (uint64_t)y;
-        if (n == 0) {
+        if (pl.n == 0) {
             for (int i = 0; i < 9; i++) row.jacquard[i] = CUDART_NAN;
             row.obj = CUDART_NAN;
             row.iters = 0;
             row.cond = CUDART_NAN;
             c_nosite++;
         } else {
+            if (L.precision == 1)
+                scatter_shapes<double>(co, x, y, lane, pl, static_cast<double*>(lists),
+                                       reinterpret_cast<double*>(wsm));
+            else
+                scatter_shapes<float>(co, x, y, lane, pl, static_cast<float*>(lists),
+                                      reinterpret_cast<float*>(wsm));
             PairResult res;
             const bool self_pair = (co.kind == COHORT_TRIANGLE) && (x == y);
-            solve_pair(co, ent, hdr, n, self_pair, L.precision, L.tune, lane, wsm, res);
+            solve_pair(co, x, y, pl, lists, self_pair, L.precision, L.tune, lane, wsm, res);
             for (int i = 0; i < 9; i++) row.jacquard[i] = res.x[i];
             row.obj = res.f;
             row.iters = res.iters;
@@ -438,16 +442,16 @@ jacquard_pair_kernel(PairLaunch L) {
             c_obj += res.obj_passes;
             c_f64 += res.fp64_passes;
             c_f64p += res.escalated ? 1 : 0;
-            c_sites += (unsigned long long)n;
-            c_work += (unsigned long long)n * (unsigned long long)res.gh_passes;
+            c_sites += (unsigned long long)pl.n;
+            c_work += (unsigned long long)pl.n * (unsigned long long)res.gh_passes;
             c_nonconv += (res.iters >= L.tune.sqp_max_iter) ? 1 : 0;
             const int p32 = res.gh_passes - res.fp64_passes;
 #pragma unroll
             for (int s = 0; s < 5; s++) {
-                c_shape[s] += (unsigned long long)shape_n[s];
-                c_fl32 += (unsigned long long)shape_n[s] *
+                c_shape[s] += (unsigned long long)pl.cnt[s];
+                c_fl32 += (unsigned long long)pl.cnt[s] *
                           (unsigned long long)(p32 * flops_direct(s) + res.diff_passes * flops_diff_extra(s));
-                c_fl64 += (unsigned long long)shape_n[s] * (unsigned long long)(res.fp64_passes * flops_direct(s));
+                c_fl64 += (unsigned long long)pl.cnt[s] * (unsigned long long)(res.fp64_passes * flops_direct(s));
             }
         }
         // 14 eight-byte words per row, one per lane
@@ -481,8 +485,8 @@ void default_launch(int& warps_per_block, int& blocks_per_sm) {
     blocks_per_sm = 4;
 }
 
-size_t scratch_bytes_per_warp(int64_t n_segments) {
-    return (size_t)n_segments * (SEG_SITES * sizeof(uint16_t) + SEG_HDR * sizeof(uint16_t));
+size_t scratch_bytes_per_warp(int64_t n_kept) {
+    return sizeof(double) * (size_t)(align4(n_kept) + 32);
 }
 
 int run_pairs(const std::vector<PairJob>& jobs, const RunConfig& cfg, Workspace& ws,
@@ -528,11 +532,11 @@ int run_pairs(const std::vector<PairJob>& jobs, const RunConfig& cfg, Workspace&
         d.planes_y = pn.planes.as<uint2>();
         d.planes_x = (jb.kind == COHORT_RECT) ? jb.query->planes.as<uint2>() : d.planes_y;
         d.plane_stride = pn.plane_stride;
-        d.p32 = pn.p32.as<float>();
+        d.pq32 = pn.p32.as<float2>();
         d.p64 = pn.p64.as<double>();
         d.q64 = pn.q64.as<double>();
         d.n_sites = (int32_t)pn.n_kept;
-        d.n_segments = (int32_t)ceil_div(pn.n_kept, SEG_SITES);
+        d.n_units = (int32_t)ceil_div(pn.n_kept, UNIT_SITES);
         d.kind = jb.kind;
         d.pad = 0;
         d.n_x = jb.n_x;
@@ -541,7 +545,7 @@ int run_pairs(const std::vector<PairJob>& jobs, const RunConfig& cfg, Workspace&
         d.n_pairs = jb.n_pairs();
         d.out = jb.d_out;
         total_pairs += d.n_pairs;
-        seg_cap = std::max<int64_t>(seg_cap, d.n_segments);
+        seg_cap = std::max<int64_t>(seg_cap, align4(pn.n_kept) + 32);
     }
     if (total_pairs == 0) return KG_OK;
     int64_t blocks = (int64_t)ws.sm_count * bps;
@@ -550,12 +554,9 @@ int run_pairs(const std::vector<PairJob>& jobs, const RunConfig& cfg, Workspace&
     if (cfg.max_warps > 0) need_warps = std::min<int64_t>(need_warps, cfg.max_warps);
     blocks = std::max<int64_t>(1, ceil_div(need_warps, wpb));
     warps = blocks * wpb;
-    const int64_t ent_stride = seg_cap * SEG_SITES;
-    const int64_t hdr_stride = seg_cap * SEG_HDR;
     if (ws.warps < warps || ws.seg_cap < seg_cap) {
         int64_t w = std::max(ws.warps, warps), s = std::max(ws.seg_cap, seg_cap);
-        KG_CUDA_TRY((cudaError_t)ws.scratch.reserve(sizeof(uint16_t) * w * s * SEG_SITES));
-        KG_CUDA_TRY((cudaError_t)ws.headers.reserve(sizeof(uint16_t) * w * s * SEG_HDR));
+        KG_CUDA_TRY((cudaError_t)ws.scratch.reserve(sizeof(double) * w * s));
         ws.warps = w;
         ws.seg_cap = s;
     }
@@ -572,13 +573,9 @@ int run_pairs(const std::vector<PairJob>& jobs, const RunConfig& cfg, Workspace&
     L.precision = cfg.precision;
     L.total_pairs = total_pairs;
     L.queue = ws.queue.as<unsigned long long>();
-    L.scratch = ws.scratch.as<uint16_t>();
-    L.headers = ws.headers.as<uint16_t>();
-    // strides use the workspace's segment capacity so rows never overlap
-    L.scratch_stride = ws.seg_cap * SEG_SITES;
-    L.header_stride = ws.seg_cap * SEG_HDR;
-    (void)ent_stride;
-    (void)hdr_stride;
+    L.lists = ws.scratch.as<double>();
+    // stride from the workspace's capacity so warps never overlap
+    L.list_stride = ws.seg_cap;
     L.tune = make_tune(cfg.iterations);
     L.counters = ws.counters.as<RunCounters>();
     cudaEvent_t e0, e1;

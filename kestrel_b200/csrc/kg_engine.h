@@ -51,7 +51,8 @@ struct Cohort {
     DevBuf bsum;               // int32 block sums of the scan
     DevBuf nkept;              // int32[2]: kept count, bad-code flag
     DevBuf pfull, qfull;       // double per raw site
-    DevBuf p32, p64, q64;      // per kept site, padded to n_seg_max * 2048
+    DevBuf p32;                // float2 {REF, ALT} per kept site, padded to n_seg_max * 2048
+    DevBuf p64, q64;           // double, same length
     DevBuf site_of;            // int32 kept index -> raw site
     DevBuf planes;             // uint2 [n_samples][plane_stride]
     size_t device_bytes() const;
@@ -99,9 +100,9 @@ struct RunConfig {
 
 // Reusable device workspace of the pair kernel (scratch lists, queue, table).
 struct Workspace {
-    DevBuf scratch, headers, queue, counters, table;
+    DevBuf scratch, queue, counters, table;
     int64_t warps = 0;
-    int64_t seg_cap = 0;
+    int64_t seg_cap = 0;       // list capacity per warp, in 8-byte words
     int sm_count = 0;
 };
 
@@ -111,8 +112,8 @@ int run_pairs(const std::vector<PairJob>& jobs, const RunConfig& cfg, Workspace&
 // Default launch shape for the device.
 void default_launch(int& warps_per_block, int& blocks_per_sm);
 
-// Bytes of scratch per warp for n segments.
-size_t scratch_bytes_per_warp(int64_t n_segments);
+// Bytes of list scratch per warp for n_kept sites.
+size_t scratch_bytes_per_warp(int64_t n_kept);
 
 const char* engine_version();
 

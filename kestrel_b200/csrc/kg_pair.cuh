@@ -38,9 +38,10 @@
 
 namespace kg {
 
-constexpr int SEG_SITES = 2048;             // sites per segment
-constexpr int SEG_WORDS = SEG_SITES / 32;   // 32-site plane words per segment
-constexpr int SEG_HDR = 8;                  // u16 header entries per segment
+constexpr int SEG_SITES = 2048;             // padding unit of the bit planes
+constexpr int SEG_WORDS = SEG_SITES / 32;   // 32-site plane words per padding unit
+constexpr int UNIT_SITES = 1024;            // sites per sort unit (one plane word per lane)
+constexpr int UNIT_WORDS = UNIT_SITES / 32;
 
 enum : int { COHORT_TRIANGLE = 0, COHORT_RECT = 1 };
 
@@ -49,11 +50,11 @@ struct CohortDev {
     const uint2* planes_x;   // [rows_x][plane_stride] {lo, hi} bit planes of 32 sites
     const uint2* planes_y;   // [rows_y][plane_stride] (== planes_x for a triangle)
     int64_t plane_stride;    // words per row (multiple of SEG_WORDS)
-    const float* p32;        // REF frequency per kept site, padded
-    const double* p64;
-    const double* q64;
+    const float2* pq32;      // {REF, ALT} frequency per kept site in FP32, padded
+    const double* p64;       // REF frequency per kept site, padded
+    const double* q64;       // ALT frequency per kept site, padded
     int32_t n_sites;         // kept (segregating) sites
-    int32_t n_segments;
+    int32_t n_units;         // sort units of UNIT_SITES kept sites
     int32_t kind;            // COHORT_TRIANGLE or COHORT_RECT
     int32_t pad;
     int64_t n_x;             // triangle: num_samples; rect: query rows
@@ -83,10 +84,8 @@ struct PairLaunch {
     int precision;               // 0 FP32C, 1 FP64
     int64_t total_pairs;
     unsigned long long* queue;   // next work index
-    uint16_t* scratch;           // per warp: [n_seg_max * SEG_SITES] entries
-    uint16_t* headers;           // per warp: [n_seg_max * SEG_HDR]
-    int64_t scratch_stride;      // entries per warp
-    int64_t header_stride;       // header u16 per warp
+    double* lists;               // per warp: the pair's shape lists (FP32 or FP64 values)
+    int64_t list_stride;         // 8-byte words per warp
     Tune tune;
     RunCounters* counters;
 };
@@ -132,7 +131,7 @@ __device__ __forceinline__ HiLo split(double v) {
     return r;
 }
 
-// Moment accumulators (FP64 totals), in the order used by the rebuild:
+// Moment sums, in the order used by the rebuild:
 //  0..3  GA  sum r t^k, k=1..4          4..10 HA  sum r^2 t^k, k=2..8
 // 11..13 GB1 sum r w t^k, k=0..2        14..18 HB1 sum r^2 w^2 t^k, k=0..4
 // 19..21 GB2                            22..26 HB2
@@ -140,10 +139,6 @@ __device__ __forceinline__ HiLo split(double v) {
 // 40..41 GD  sum r w {1,w}              42..44 HD  sum r^2 w^2 {1,w,w^2}
 constexpr int NMOM = 45;
 
-struct PassOut {
-    double mom[NMOM];
-    double obj;      // sum of lg2(d) [FP32 direct], log(d) [FP64], or log(d_new/d_old) [diff]
-};
 
 // Per-pass coefficients of L.D for each shape (see the header comment).
 struct PassCoef {
@@ -217,113 +212,144 @@ __device__ inline void rebuild(const double* m, double* S, double* T) {
 
 // ------------------------------------------------------------- sorting
 
-// Builds the per-segment shape lists of pair (x, y) in this warp's scratch.
-// Entry = site-in-segment (11 bits) | sel << 15, where sel picks t = q.
-// Header per segment: {startB1, startB2, startC, startD, total}.
-// Returns the number of jointly observed segregating sites.
-__device__ inline int64_t sort_pair(const CohortDev& co, int64_t x, int64_t y, uint16_t* ent,
-                                    uint16_t* hdr, uint16_t* buf, int lane, int64_t* shape_n) {
+// Shape masks of 32 sites from the {lo, hi} planes of x and y (code = 2 hi + lo;
+// 3 = missing, which is neither hom nor het).  sel picks t = ALT frequency:
+// x's allele for A, B1 and C; y's allele for B2.
+struct ShapeMasks {
+    uint32_t m[5];
+    uint32_t sel;
+};
+
+__device__ __forceinline__ ShapeMasks shape_masks(uint2 X, uint2 Y) {
+    ShapeMasks r;
+    uint32_t xhom = ~X.x, xhet = X.x & ~X.y;
+    uint32_t yhom = ~Y.x, yhet = Y.x & ~Y.y;
+    uint32_t same = ~(X.y ^ Y.y);
+    r.m[0] = xhom & yhom & same;   // A
+    r.m[1] = xhom & yhet;          // B1
+    r.m[2] = xhet & yhom;          // B2
+    r.m[3] = xhom & yhom & ~same;  // C
+    r.m[4] = xhet & yhet;          // D
+    r.sel = (X.y & ~r.m[2]) | (Y.y & r.m[2]);
+    return r;
+}
+
+__host__ __device__ __forceinline__ int64_t align4(int64_t v) { return (v + 3) & ~(int64_t)3; }
+
+// Per-pair list layout: shape s occupies [start[s], start[s] + cnt[s]) elements
+// of the warp's list buffer; starts are multiples of 4 (16-byte float4 loads).
+struct PairLists {
+    int64_t start[5];
+    int64_t cnt[5];
+    int64_t n;
+};
+
+__device__ inline void count_shapes(const CohortDev& co, int64_t x, int64_t y, int lane, PairLists& pl) {
     const uint2* px = co.planes_x + x * co.plane_stride;
     const uint2* py = co.planes_y + y * co.plane_stride;
-    int64_t n = 0;
-    for (int s = 0; s < 5; s++) shape_n[s] = 0;
-    for (int seg = 0; seg < co.n_segments; seg++) {
-        uint32_t m[2][5], sel[2];
-        unsigned cnt[5] = {0, 0, 0, 0, 0};
+    unsigned c[5] = {0, 0, 0, 0, 0};
+    const int nw = co.n_units * UNIT_WORDS;
+    for (int w = lane; w < nw; w += 32) {
+        ShapeMasks sm = shape_masks(px[w], py[w]);
 #pragma unroll
-        for (int h = 0; h < 2; h++) {
-            uint2 X = px[seg * SEG_WORDS + h * 32 + lane];
-            uint2 Y = py[seg * SEG_WORDS + h * 32 + lane];
-            uint32_t xhom = ~X.x, xhet = X.x & ~X.y;
-            uint32_t yhom = ~Y.x, yhet = Y.x & ~Y.y;
-            uint32_t same = ~(X.y ^ Y.y);
-            m[h][0] = xhom & yhom & same;   // A
-            m[h][1] = xhom & yhet;          // B1
-            m[h][2] = xhet & yhom;          // B2
-            m[h][3] = xhom & yhom & ~same;  // C
-            m[h][4] = xhet & yhet;          // D
-            sel[h] = (X.y & ~m[h][2]) | (Y.y & m[h][2]);
+        for (int s = 0; s < 5; s++) c[s] += __popc(sm.m[s]);
+    }
+    int64_t st = 0;
+    pl.n = 0;
 #pragma unroll
-            for (int s = 0; s < 5; s++) cnt[s] += __popc(m[h][s]);
-        }
-        // warp-exclusive scan of the five counts packed in 12-bit fields
+    for (int s = 0; s < 5; s++) {
+        unsigned v = c[s];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        pl.cnt[s] = v;
+        pl.start[s] = st;
+        st = align4(st + v);
+        pl.n += v;
+    }
+}
+
+template <class T>
+__device__ __forceinline__ T site_value(const CohortDev& co, int64_t site, bool sel);
+
+template <>
+__device__ __forceinline__ float site_value<float>(const CohortDev& co, int64_t site, bool sel) {
+    float2 v = co.pq32[site];
+    return sel ? v.y : v.x;
+}
+
+template <>
+__device__ __forceinline__ double site_value<double>(const CohortDev& co, int64_t site, bool sel) {
+    return sel ? co.q64[site] : co.p64[site];
+}
+
+// Writes the frequency value t of every jointly observed site into its shape
+// list (in FP32 or FP64), one unit of 1024 sites at a time through the warp's
+// shared buffer so the global stores stay coalesced.
+template <class T>
+__device__ inline void scatter_shapes(const CohortDev& co, int64_t x, int64_t y, int lane,
+                                      const PairLists& pl, T* lists, T* buf) {
+    const uint2* px = co.planes_x + x * co.plane_stride;
+    const uint2* py = co.planes_y + y * co.plane_stride;
+    int64_t off[5];
+#pragma unroll
+    for (int s = 0; s < 5; s++) off[s] = pl.start[s];
+    for (int u = 0; u < co.n_units; u++) {
+        const int w = u * UNIT_WORDS + lane;
+        ShapeMasks sm = shape_masks(px[w], py[w]);
         unsigned long long v = 0;
 #pragma unroll
-        for (int s = 0; s < 5; s++) v |= (unsigned long long)cnt[s] << (12 * s);
+        for (int s = 0; s < 5; s++) v |= (unsigned long long)__popc(sm.m[s]) << (11 * s);
         unsigned long long inc = v;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
             unsigned long long t = __shfl_up_sync(0xffffffffu, inc, o);
             if (lane >= o) inc += t;
         }
-        unsigned long long tot = __shfl_sync(0xffffffffu, inc, 31);
-        unsigned long long exc = inc - v;
-        unsigned start[6];
-        start[0] = 0;
+        const unsigned long long tot = __shfl_sync(0xffffffffu, inc, 31);
+        const unsigned long long exc = inc - v;
+        unsigned ustart[6];
+        ustart[0] = 0;
 #pragma unroll
-        for (int s = 0; s < 5; s++) start[s + 1] = start[s] + (unsigned)((tot >> (12 * s)) & 0xFFF);
-        unsigned pos[5];
+        for (int s = 0; s < 5; s++) ustart[s + 1] = ustart[s] + (unsigned)((tot >> (11 * s)) & 0x7FF);
+        const int64_t base = (int64_t)u * UNIT_SITES + lane * 32;
 #pragma unroll
-        for (int s = 0; s < 5; s++) pos[s] = start[s] + (unsigned)((exc >> (12 * s)) & 0xFFF);
-#pragma unroll
-        for (int h = 0; h < 2; h++) {
-            unsigned base = (unsigned)((h * 32 + lane) * 32);
-#pragma unroll
-            for (int s = 0; s < 5; s++) {
-                uint32_t mm = m[h][s];
-                while (mm) {
-                    int i = __ffs(mm) - 1;
-                    mm &= mm - 1;
-                    unsigned e = (base + i) | (((sel[h] >> i) & 1u) << 15);
-                    buf[pos[s]++] = (uint16_t)e;
-                }
+        for (int s = 0; s < 5; s++) {
+            unsigned pos = ustart[s] + (unsigned)((exc >> (11 * s)) & 0x7FF);
+            uint32_t mm = sm.m[s];
+            while (mm) {
+                int i = __ffs(mm) - 1;
+                mm &= mm - 1;
+                buf[pos++] = site_value<T>(co, base + i, (sm.sel >> i) & 1u);
             }
         }
         __syncwarp();
-        // copy the segment's entries out (4 KB) with 16-byte stores
-        const uint4* src = reinterpret_cast<const uint4*>(buf);
-        uint4* dst = reinterpret_cast<uint4*>(ent + (int64_t)seg * SEG_SITES);
-        unsigned total = start[5];
-        unsigned nvec = (total + 7) / 8;
-        for (unsigned k = lane; k < nvec; k += 32) dst[k] = src[k];
-        if (lane == 0) {
-            uint4 h4;
-            h4.x = start[1] | (start[2] << 16);
-            h4.y = start[3] | (start[4] << 16);
-            h4.z = total;
-            h4.w = 0;
-            *reinterpret_cast<uint4*>(hdr + (int64_t)seg * SEG_HDR) = h4;
+#pragma unroll
+        for (int s = 0; s < 5; s++) {
+            const unsigned ns = ustart[s + 1] - ustart[s];
+            T* dst = lists + off[s];
+            const T* src = buf + ustart[s];
+            for (unsigned j = lane; j < ns; j += 32) dst[j] = src[j];
+            off[s] += ns;
         }
         __syncwarp();
-        n += total;
-#pragma unroll
-        for (int s = 0; s < 5; s++) shape_n[s] += start[s + 1] - start[s];
     }
-    return n;
 }
 
 // ----------------------------------------------------------- FP32 passes
 
 enum : int { OBJ_DIRECT = 0, OBJ_DIFF = 1 };
 
-// Warp-uniform pass coefficients, kept in shared memory and re-read at the top
-// of each shape loop so only the current shape's values occupy registers.
+// Warp-uniform pass coefficients, kept in shared memory and read at the top
+// of each shape's stream so only that shape's values occupy registers.
 struct Coef32 {
     HiLo a[4], b1[3], b2[3], c[4], d[2];
     float sa[4], sb1[3], sb2[3], sc[4], sd[2];  // step coefficients (OBJ_DIFF)
 };
 
-// Shared-memory words per warp: the FP64 accumulators (NACC per lane, lane-
-// interleaved) overlay the 2048-entry sort buffer; the coefficients follow.
-constexpr int NACC = NMOM + 1;  // moments + objective
-constexpr int WARP_SMEM_ACC = NACC * 32 * 8;
-constexpr int WARP_SMEM_COEF = 512;
-constexpr int WARP_SMEM = WARP_SMEM_ACC + WARP_SMEM_COEF;
-static_assert(WARP_SMEM_ACC >= SEG_SITES * 2, "sort buffer must fit under the accumulators");
+constexpr int WARP_SMEM_BUF = UNIT_SITES * 8;   // sort buffer (FP64 values at most)
+constexpr int WARP_SMEM_COEF = 256;
+constexpr int WARP_SMEM = WARP_SMEM_BUF + WARP_SMEM_COEF;
 static_assert(sizeof(Coef32) <= WARP_SMEM_COEF, "coefficients must fit");
-
-// acc points at this lane's first accumulator (stride 32 doubles).
-__device__ __forceinline__ void acc_add(double* acc, int i, double v) { acc[i * 32] += v; }
 
 template <class T>
 __device__ __forceinline__ T ld_volatile(const T* p) { return *reinterpret_cast<const volatile T*>(p); }
@@ -335,276 +361,230 @@ __device__ __forceinline__ HiLo ldk(const HiLo* p) {
     return r;
 }
 
-// Sums over one pair's lists at the FP32 evaluation point into this lane's
-// shared-memory accumulators.
-template <int OBJ>
-__device__ __noinline__ void pass_fp32(const CohortDev& co, const uint16_t* ent, const uint16_t* hdr,
-                                       const Coef32* K, double* acc, int lane) {
+// Per-lane FP64 sums of one pass: NMOM moments + the objective term.
+struct LaneSums {
+    double m[NMOM];
+    double obj;
+};
+
+constexpr int HESS_FLUSH = 16;   // float4 iterations between FP32 -> FP64 Hessian flushes
+
+// Streams one shape's FP32 list.  Gradient moments and the objective are
+// promoted to FP64 every 4 sites, Hessian moments every 64; each site is the
+// closed form of its shape (see the file comment).
+template <int S, int OBJ>
+__device__ __noinline__ void stream32(const float* __restrict__ L, int64_t len, const Coef32* K,
+                                      int lane, LaneSums& out) {
+    constexpr int NG = S == 0 ? 4 : S == 3 ? 4 : S == 4 ? 2 : 3;
+    constexpr int NH = S == 0 ? 7 : S == 3 ? 9 : S == 4 ? 3 : 5;
+    constexpr int GOFF = S == 0 ? 0 : S == 1 ? 11 : S == 2 ? 19 : S == 3 ? 27 : 40;
+    constexpr int HOFF = GOFF + NG;
     const float EPS = 1e-8f;
-    for (int seg = 0; seg < co.n_segments; seg++) {
-        uint4 h4 = *reinterpret_cast<const uint4*>(hdr + (int64_t)seg * SEG_HDR);
-        const int sB1 = h4.x & 0xFFFF, sB2 = h4.x >> 16, sC = h4.y & 0xFFFF, sD = h4.y >> 16;
-        const int tot = h4.z;
-        const uint16_t* E = ent + (int64_t)seg * SEG_SITES;
-        const float* P = co.p32 + (int64_t)seg * SEG_SITES;
-        // ---- shape A
-        {
-            const HiLo a0 = ldk(&K->a[0]), a1 = ldk(&K->a[1]), a2 = ldk(&K->a[2]), a3 = ldk(&K->a[3]);
-            float s0 = 0.f, s1 = 0.f, s2 = 0.f, s3 = 0.f;
-            if (OBJ == OBJ_DIFF) {
-                s0 = ld_volatile(&K->sa[0]); s1 = ld_volatile(&K->sa[1]);
-                s2 = ld_volatile(&K->sa[2]); s3 = ld_volatile(&K->sa[3]);
-            }
-            float g0 = 0, g1 = 0, g2 = 0, g3 = 0, h0 = 0, h1 = 0, h2 = 0, h3 = 0, h4_ = 0, h5 = 0, h6 = 0, ob = 0;
-#pragma unroll 2
-            for (int j = lane; j < sB1; j += 32) {
-                unsigned e = E[j];
-                float p = P[e & 0x7FF];
-                float t = (e >> 15) ? 1.0f - p : p;
-                float t2 = t * t, t3 = t2 * t, t4 = t2 * t2, t5 = t4 * t, t6 = t3 * t3;
-                float ph = fmaf(fmaf(fmaf(a3.h, t, a2.h), t, a1.h), t, a0.h);
-                float pl = fmaf(fmaf(fmaf(a3.l, t, a2.l), t, a1.l), t, a0.l);
-                float d = fmaf(t, ph + pl, EPS);
-                float r = rcp_nr(d);
-                float u = r * t;
-                g0 += u; g1 = fmaf(u, t, g1); g2 = fmaf(u, t2, g2); g3 = fmaf(u, t3, g3);
-                float u2 = u * u;
-                h0 += u2; h1 = fmaf(u2, t, h1); h2 = fmaf(u2, t2, h2); h3 = fmaf(u2, t3, h3);
-                h4_ = fmaf(u2, t4, h4_); h5 = fmaf(u2, t5, h5); h6 = fmaf(u2, t6, h6);
-                if (OBJ == OBJ_DIRECT) {
-                    ob += lg2_approx(d);
-                } else {
-                    float dl = t * fmaf(fmaf(fmaf(s3, t, s2), t, s1), t, s0);
-                    ob += neg_log1m(dl * r);
-                }
-            }
-            acc_add(acc, 0, g0); acc_add(acc, 1, g1); acc_add(acc, 2, g2); acc_add(acc, 3, g3);
-            acc_add(acc, 4, h0); acc_add(acc, 5, h1); acc_add(acc, 6, h2); acc_add(acc, 7, h3);
-            acc_add(acc, 8, h4_); acc_add(acc, 9, h5); acc_add(acc, 10, h6);
-            acc_add(acc, NMOM, ob);
-        }
-        // ---- shapes B1 and B2 (same form, different coefficients and moments)
+    HiLo k0, k1, k2, k3;
+    float s0 = 0.f, s1 = 0.f, s2 = 0.f, s3 = 0.f;
+    if (S == 0) { k0 = ldk(&K->a[0]); k1 = ldk(&K->a[1]); k2 = ldk(&K->a[2]); k3 = ldk(&K->a[3]); }
+    if (S == 1) { k0 = ldk(&K->b1[0]); k1 = ldk(&K->b1[1]); k2 = ldk(&K->b1[2]); k3 = HiLo{0.f, 0.f}; }
+    if (S == 2) { k0 = ldk(&K->b2[0]); k1 = ldk(&K->b2[1]); k2 = ldk(&K->b2[2]); k3 = HiLo{0.f, 0.f}; }
+    if (S == 3) { k0 = ldk(&K->c[0]); k1 = ldk(&K->c[1]); k2 = ldk(&K->c[2]); k3 = ldk(&K->c[3]); }
+    if (S == 4) { k0 = ldk(&K->d[0]); k1 = ldk(&K->d[1]); k2 = HiLo{0.f, 0.f}; k3 = HiLo{0.f, 0.f}; }
+    if (OBJ == OBJ_DIFF) {
+        const float* sp = S == 0 ? K->sa : S == 1 ? K->sb1 : S == 2 ? K->sb2 : S == 3 ? K->sc : K->sd;
+        s0 = ld_volatile(&sp[0]);
+        s1 = ld_volatile(&sp[1]);
+        if (S != 4) s2 = ld_volatile(&sp[2]);
+        if (S == 0 || S == 3) s3 = ld_volatile(&sp[3]);
+    }
+    double G[NG], H[NH], F = 0.0;
+    float h[NH];
 #pragma unroll
-        for (int b = 0; b < 2; b++) {
-            const HiLo* kb = b ? K->b2 : K->b1;
-            const float* sbp = b ? K->sb2 : K->sb1;
-            const HiLo k0 = ldk(&kb[0]), k1 = ldk(&kb[1]), k2 = ldk(&kb[2]);
-            float s0 = 0.f, s1 = 0.f, s2 = 0.f;
-            if (OBJ == OBJ_DIFF) { s0 = ld_volatile(&sbp[0]); s1 = ld_volatile(&sbp[1]); s2 = ld_volatile(&sbp[2]); }
-            const int lo = b ? sB2 : sB1, hi = b ? sC : sB2;
-            float g0 = 0, g1 = 0, g2 = 0, h0 = 0, h1 = 0, h2 = 0, h3 = 0, h4_ = 0, ob = 0;
-#pragma unroll 2
-            for (int j = lo + lane; j < hi; j += 32) {
-                unsigned e = E[j];
-                float p = P[e & 0x7FF];
-                float q = 1.0f - p;
-                float t = (e >> 15) ? q : p;
-                float w = p * q;
-                float t2 = t * t, t3 = t2 * t, t4 = t2 * t2;
-                float ph = fmaf(fmaf(k2.h, t, k1.h), t, k0.h);
-                float pl = fmaf(fmaf(k2.l, t, k1.l), t, k0.l);
-                float d = fmaf(w, ph + pl, EPS);
-                float r = rcp_nr(d);
-                float v = r * w;
-                g0 += v; g1 = fmaf(v, t, g1); g2 = fmaf(v, t2, g2);
-                float v2 = v * v;
-                h0 += v2; h1 = fmaf(v2, t, h1); h2 = fmaf(v2, t2, h2); h3 = fmaf(v2, t3, h3);
-                h4_ = fmaf(v2, t4, h4_);
-                if (OBJ == OBJ_DIRECT) {
-                    ob += lg2_approx(d);
-                } else {
-                    float dl = w * fmaf(fmaf(s2, t, s1), t, s0);
-                    ob += neg_log1m(dl * r);
-                }
-            }
-            const int gb = b ? 19 : 11, hb = b ? 22 : 14;
-            acc_add(acc, gb + 0, g0); acc_add(acc, gb + 1, g1); acc_add(acc, gb + 2, g2);
-            acc_add(acc, hb + 0, h0); acc_add(acc, hb + 1, h1); acc_add(acc, hb + 2, h2);
-            acc_add(acc, hb + 3, h3); acc_add(acc, hb + 4, h4_);
-            acc_add(acc, NMOM, ob);
-        }
-        // ---- shape C
-        {
-            const HiLo c0 = ldk(&K->c[0]), c1 = ldk(&K->c[1]), c2 = ldk(&K->c[2]), c3 = ldk(&K->c[3]);
-            float s0 = 0.f, s1 = 0.f, s2 = 0.f, s3 = 0.f;
-            if (OBJ == OBJ_DIFF) {
-                s0 = ld_volatile(&K->sc[0]); s1 = ld_volatile(&K->sc[1]);
-                s2 = ld_volatile(&K->sc[2]); s3 = ld_volatile(&K->sc[3]);
-            }
-            float g0 = 0, g1 = 0, g2 = 0, g3 = 0, ob = 0;
-            float h[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-            for (int j = sC + lane; j < sD; j += 32) {
-                unsigned e = E[j];
-                float p = P[e & 0x7FF];
-                float q = 1.0f - p;
-                bool s = (e >> 15) != 0;
-                float tx = s ? q : p, ty = s ? p : q;
-                float w = p * q;
-                float ph = fmaf(w, c3.h, fmaf(tx, c2.h, fmaf(ty, c1.h, c0.h)));
-                float pl = fmaf(w, c3.l, fmaf(tx, c2.l, fmaf(ty, c1.l, c0.l)));
-                float d = fmaf(w, ph + pl, EPS);
-                float r = rcp_nr(d);
-                float v = r * w;
-                g0 += v; g1 = fmaf(v, ty, g1); g2 = fmaf(v, tx, g2); g3 = fmaf(v, w, g3);
-                float v2 = v * v;
-                h[0] += v2; h[1] = fmaf(v2, ty, h[1]); h[2] = fmaf(v2, tx, h[2]); h[3] = fmaf(v2, w, h[3]);
-                h[4] = fmaf(v2, ty * ty, h[4]); h[5] = fmaf(v2, tx * tx, h[5]);
-                h[6] = fmaf(v2, w * ty, h[6]); h[7] = fmaf(v2, w * tx, h[7]); h[8] = fmaf(v2, w * w, h[8]);
-                if (OBJ == OBJ_DIRECT) {
-                    ob += lg2_approx(d);
-                } else {
-                    float dl = w * fmaf(w, s3, fmaf(tx, s2, fmaf(ty, s1, s0)));
-                    ob += neg_log1m(dl * r);
-                }
-            }
-            acc_add(acc, 27, g0); acc_add(acc, 28, g1); acc_add(acc, 29, g2); acc_add(acc, 30, g3);
+    for (int i = 0; i < NG; i++) G[i] = 0.0;
 #pragma unroll
-            for (int i = 0; i < 9; i++) acc_add(acc, 31 + i, h[i]);
-            acc_add(acc, NMOM, ob);
+    for (int i = 0; i < NH; i++) { H[i] = 0.0; h[i] = 0.f; }
+
+    // one site: adds into the FP32 gradient/objective partials g, ob and h
+    auto site = [&](float t, float* g, float& ob) {
+        float d, r, c;    // c = the per-site scale: t (A) or w (B, C, D)
+        if (S == 0) {
+            float ph = fmaf(fmaf(fmaf(k3.h, t, k2.h), t, k1.h), t, k0.h);
+            float pl = fmaf(fmaf(fmaf(k3.l, t, k2.l), t, k1.l), t, k0.l);
+            d = fmaf(t, ph + pl, EPS);
+            r = rcp_nr(d);
+            float u = r * t;
+            float t2 = t * t, t3 = t2 * t, t4 = t2 * t2, t5 = t4 * t, t6 = t3 * t3;
+            g[0] += u; g[1] = fmaf(u, t, g[1]); g[2] = fmaf(u, t2, g[2]); g[3] = fmaf(u, t3, g[3]);
+            float u2 = u * u;
+            h[0] += u2; h[1] = fmaf(u2, t, h[1]); h[2] = fmaf(u2, t2, h[2]); h[3] = fmaf(u2, t3, h[3]);
+            h[4] = fmaf(u2, t4, h[4]); h[5] = fmaf(u2, t5, h[5]); h[6] = fmaf(u2, t6, h[6]);
+            c = t;
+        } else if (S == 1 || S == 2) {
+            float w = t * (1.0f - t);
+            float ph = fmaf(fmaf(k2.h, t, k1.h), t, k0.h);
+            float pl = fmaf(fmaf(k2.l, t, k1.l), t, k0.l);
+            d = fmaf(w, ph + pl, EPS);
+            r = rcp_nr(d);
+            float v = r * w;
+            float t2 = t * t, t3 = t2 * t, t4 = t2 * t2;
+            g[0] += v; g[1] = fmaf(v, t, g[1]); g[2] = fmaf(v, t2, g[2]);
+            float v2 = v * v;
+            h[0] += v2; h[1] = fmaf(v2, t, h[1]); h[2] = fmaf(v2, t2, h[2]); h[3] = fmaf(v2, t3, h[3]);
+            h[4] = fmaf(v2, t4, h[4]);
+            c = w;
+        } else if (S == 3) {
+            float ty = 1.0f - t;   // t = tx, the frequency of x's allele
+            float w = t * ty;
+            float ph = fmaf(w, k3.h, fmaf(t, k2.h, fmaf(ty, k1.h, k0.h)));
+            float pl = fmaf(w, k3.l, fmaf(t, k2.l, fmaf(ty, k1.l, k0.l)));
+            d = fmaf(w, ph + pl, EPS);
+            r = rcp_nr(d);
+            float v = r * w;
+            g[0] += v; g[1] = fmaf(v, ty, g[1]); g[2] = fmaf(v, t, g[2]); g[3] = fmaf(v, w, g[3]);
+            float v2 = v * v;
+            h[0] += v2; h[1] = fmaf(v2, ty, h[1]); h[2] = fmaf(v2, t, h[2]); h[3] = fmaf(v2, w, h[3]);
+            h[4] = fmaf(v2, ty * ty, h[4]); h[5] = fmaf(v2, t * t, h[5]);
+            h[6] = fmaf(v2, w * ty, h[6]); h[7] = fmaf(v2, w * t, h[7]); h[8] = fmaf(v2, w * w, h[8]);
+            c = w;
+        } else {
+            float w = t * (1.0f - t);
+            float ph = fmaf(w, k1.h, k0.h);
+            float pl = fmaf(w, k1.l, k0.l);
+            d = fmaf(w, ph + pl, EPS);
+            r = rcp_nr(d);
+            float v = r * w;
+            g[0] += v; g[1] = fmaf(v, w, g[1]);
+            float v2 = v * v;
+            h[0] += v2; h[1] = fmaf(v2, w, h[1]); h[2] = fmaf(v2, w * w, h[2]);
+            c = w;
         }
-        // ---- shape D
-        {
-            const HiLo d0 = ldk(&K->d[0]), d1 = ldk(&K->d[1]);
-            float s0 = 0.f, s1 = 0.f;
-            if (OBJ == OBJ_DIFF) { s0 = ld_volatile(&K->sd[0]); s1 = ld_volatile(&K->sd[1]); }
-            float g0 = 0, g1 = 0, h0 = 0, h1 = 0, h2 = 0, ob = 0;
-            for (int j = sD + lane; j < tot; j += 32) {
-                unsigned e = E[j];
-                float p = P[e & 0x7FF];
-                float w = p * (1.0f - p);
-                float ph = fmaf(w, d1.h, d0.h);
-                float pl = fmaf(w, d1.l, d0.l);
-                float d = fmaf(w, ph + pl, EPS);
-                float r = rcp_nr(d);
-                float v = r * w;
-                g0 += v; g1 = fmaf(v, w, g1);
-                float v2 = v * v;
-                h0 += v2; h1 = fmaf(v2, w, h1); h2 = fmaf(v2, w * w, h2);
-                if (OBJ == OBJ_DIRECT) {
-                    ob += lg2_approx(d);
-                } else {
-                    float dl = w * fmaf(w, s1, s0);
-                    ob += neg_log1m(dl * r);
-                }
-            }
-            acc_add(acc, 40, g0); acc_add(acc, 41, g1);
-            acc_add(acc, 42, h0); acc_add(acc, 43, h1); acc_add(acc, 44, h2);
-            acc_add(acc, NMOM, ob);
+        if (OBJ == OBJ_DIRECT) {
+            ob += lg2_approx(d);
+        } else {
+            float dl;
+            if (S == 0) dl = t * fmaf(fmaf(fmaf(s3, t, s2), t, s1), t, s0);
+            else if (S == 1 || S == 2) dl = c * fmaf(fmaf(s2, t, s1), t, s0);
+            else if (S == 3) dl = c * fmaf(c, s3, fmaf(t, s2, fmaf(1.0f - t, s1, s0)));
+            else dl = c * fmaf(c, s1, s0);
+            ob += neg_log1m(dl * r);
+        }
+    };
+
+    const int64_t n4 = len >> 2;
+    const float4* L4 = reinterpret_cast<const float4*>(L);
+    int it = 0;
+    for (int64_t k = lane; k < n4; k += 32) {
+        const float4 tv = L4[k];
+        float g[NG], ob = 0.f;
+#pragma unroll
+        for (int i = 0; i < NG; i++) g[i] = 0.f;
+        site(tv.x, g, ob);
+        site(tv.y, g, ob);
+        site(tv.z, g, ob);
+        site(tv.w, g, ob);
+#pragma unroll
+        for (int i = 0; i < NG; i++) G[i] += (double)g[i];
+        F += (double)ob;
+        if (++it == HESS_FLUSH) {
+#pragma unroll
+            for (int i = 0; i < NH; i++) { H[i] += (double)h[i]; h[i] = 0.f; }
+            it = 0;
         }
     }
+    if (lane < (int)(len & 3)) {
+        float g[NG], ob = 0.f;
+#pragma unroll
+        for (int i = 0; i < NG; i++) g[i] = 0.f;
+        site(L[4 * n4 + lane], g, ob);
+#pragma unroll
+        for (int i = 0; i < NG; i++) G[i] += (double)g[i];
+        F += (double)ob;
+    }
+#pragma unroll
+    for (int i = 0; i < NH; i++) H[i] += (double)h[i];
+#pragma unroll
+    for (int i = 0; i < NG; i++) out.m[GOFF + i] = G[i];
+#pragma unroll
+    for (int i = 0; i < NH; i++) out.m[HOFF + i] = H[i];
+    out.obj += F;
 }
 
 // ----------------------------------------------------------- FP64 passes
 
 // The same sums in FP64 with IEEE division and the library log (the plain
-// FP64 form); per-shape partials are flushed to the shared accumulators.
-__device__ __noinline__ void pass_fp64(const CohortDev& co, const uint16_t* ent, const uint16_t* hdr,
-                                       const PassCoef* Kp, double* acc, int lane) {
+// FP64 form, and the re-evaluation of ill-conditioned or stalled pairs).
+template <int S>
+__device__ __noinline__ void stream64(const double* __restrict__ L, int64_t len, const PassCoef* K,
+                                      int lane, LaneSums& out) {
+    constexpr int NG = S == 0 ? 4 : S == 3 ? 4 : S == 4 ? 2 : 3;
+    constexpr int NH = S == 0 ? 7 : S == 3 ? 9 : S == 4 ? 3 : 5;
+    constexpr int GOFF = S == 0 ? 0 : S == 1 ? 11 : S == 2 ? 19 : S == 3 ? 27 : 40;
+    constexpr int HOFF = GOFF + NG;
     const double EPS = 1e-8;
-    for (int seg = 0; seg < co.n_segments; seg++) {
-        uint4 h4 = *reinterpret_cast<const uint4*>(hdr + (int64_t)seg * SEG_HDR);
-        const int sB1 = h4.x & 0xFFFF, sB2 = h4.x >> 16, sC = h4.y & 0xFFFF, sD = h4.y >> 16;
-        const int tot = h4.z;
-        const uint16_t* E = ent + (int64_t)seg * SEG_SITES;
-        const double* P = co.p64 + (int64_t)seg * SEG_SITES;
-        const double* Q = co.q64 + (int64_t)seg * SEG_SITES;
-        {
-            const double a0 = ld_volatile(&Kp->a[0]), a1 = ld_volatile(&Kp->a[1]);
-            const double a2 = ld_volatile(&Kp->a[2]), a3 = ld_volatile(&Kp->a[3]);
-            double m[11] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
-            double ob = 0.0;
-            for (int j = lane; j < sB1; j += 32) {
-                unsigned e = E[j];
-                double t = (e >> 15) ? Q[e & 0x7FF] : P[e & 0x7FF];
-                double t2 = t * t, t3 = t2 * t, t4 = t2 * t2, t5 = t4 * t, t6 = t3 * t3;
-                double d = fma(t, fma(fma(fma(a3, t, a2), t, a1), t, a0), EPS);
-                double r = 1.0 / d;
-                double u = r * t;
-                m[0] += u; m[1] = fma(u, t, m[1]); m[2] = fma(u, t2, m[2]); m[3] = fma(u, t3, m[3]);
-                double u2 = u * u;
-                m[4] += u2; m[5] = fma(u2, t, m[5]); m[6] = fma(u2, t2, m[6]); m[7] = fma(u2, t3, m[7]);
-                m[8] = fma(u2, t4, m[8]); m[9] = fma(u2, t5, m[9]); m[10] = fma(u2, t6, m[10]);
-                ob += log(d);
-            }
+    double k0, k1, k2 = 0.0, k3 = 0.0;
+    if (S == 0) { k0 = ld_volatile(&K->a[0]); k1 = ld_volatile(&K->a[1]); k2 = ld_volatile(&K->a[2]); k3 = ld_volatile(&K->a[3]); }
+    if (S == 1) { k0 = ld_volatile(&K->b1[0]); k1 = ld_volatile(&K->b1[1]); k2 = ld_volatile(&K->b1[2]); }
+    if (S == 2) { k0 = ld_volatile(&K->b2[0]); k1 = ld_volatile(&K->b2[1]); k2 = ld_volatile(&K->b2[2]); }
+    if (S == 3) { k0 = ld_volatile(&K->c[0]); k1 = ld_volatile(&K->c[1]); k2 = ld_volatile(&K->c[2]); k3 = ld_volatile(&K->c[3]); }
+    if (S == 4) { k0 = ld_volatile(&K->d[0]); k1 = ld_volatile(&K->d[1]); }
+    double g[NG], h[NH], F = 0.0;
 #pragma unroll
-            for (int i = 0; i < 11; i++) acc_add(acc, i, m[i]);
-            acc_add(acc, NMOM, ob);
+    for (int i = 0; i < NG; i++) g[i] = 0.0;
+#pragma unroll
+    for (int i = 0; i < NH; i++) h[i] = 0.0;
+    auto site = [&](double t) {
+        double d;
+        if (S == 0) {
+            d = fma(t, fma(fma(fma(k3, t, k2), t, k1), t, k0), EPS);
+            double r = 1.0 / d;
+            double u = r * t;
+            double t2 = t * t, t3 = t2 * t, t4 = t2 * t2, t5 = t4 * t, t6 = t3 * t3;
+            g[0] += u; g[1] = fma(u, t, g[1]); g[2] = fma(u, t2, g[2]); g[3] = fma(u, t3, g[3]);
+            double u2 = u * u;
+            h[0] += u2; h[1] = fma(u2, t, h[1]); h[2] = fma(u2, t2, h[2]); h[3] = fma(u2, t3, h[3]);
+            h[4] = fma(u2, t4, h[4]); h[5] = fma(u2, t5, h[5]); h[6] = fma(u2, t6, h[6]);
+        } else if (S == 1 || S == 2) {
+            double w = t * (1.0 - t);
+            d = fma(w, fma(fma(k2, t, k1), t, k0), EPS);
+            double r = 1.0 / d;
+            double v = r * w;
+            double t2 = t * t, t3 = t2 * t, t4 = t2 * t2;
+            g[0] += v; g[1] = fma(v, t, g[1]); g[2] = fma(v, t2, g[2]);
+            double v2 = v * v;
+            h[0] += v2; h[1] = fma(v2, t, h[1]); h[2] = fma(v2, t2, h[2]); h[3] = fma(v2, t3, h[3]);
+            h[4] = fma(v2, t4, h[4]);
+        } else if (S == 3) {
+            double ty = 1.0 - t;
+            double w = t * ty;
+            d = fma(w, fma(w, k3, fma(t, k2, fma(ty, k1, k0))), EPS);
+            double r = 1.0 / d;
+            double v = r * w;
+            g[0] += v; g[1] = fma(v, ty, g[1]); g[2] = fma(v, t, g[2]); g[3] = fma(v, w, g[3]);
+            double v2 = v * v;
+            h[0] += v2; h[1] = fma(v2, ty, h[1]); h[2] = fma(v2, t, h[2]); h[3] = fma(v2, w, h[3]);
+            h[4] = fma(v2, ty * ty, h[4]); h[5] = fma(v2, t * t, h[5]);
+            h[6] = fma(v2, w * ty, h[6]); h[7] = fma(v2, w * t, h[7]); h[8] = fma(v2, w * w, h[8]);
+        } else {
+            double w = t * (1.0 - t);
+            d = fma(w, fma(w, k1, k0), EPS);
+            double r = 1.0 / d;
+            double v = r * w;
+            g[0] += v; g[1] = fma(v, w, g[1]);
+            double v2 = v * v;
+            h[0] += v2; h[1] = fma(v2, w, h[1]); h[2] = fma(v2, w * w, h[2]);
         }
-#pragma unroll
-        for (int b = 0; b < 2; b++) {
-            const double* kb = b ? Kp->b2 : Kp->b1;
-            const double k0 = ld_volatile(&kb[0]), k1 = ld_volatile(&kb[1]), k2 = ld_volatile(&kb[2]);
-            const int lo = b ? sB2 : sB1, hi = b ? sC : sB2;
-            double m[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-            double ob = 0.0;
-            for (int j = lo + lane; j < hi; j += 32) {
-                unsigned e = E[j];
-                double p = P[e & 0x7FF], q = Q[e & 0x7FF];
-                double t = (e >> 15) ? q : p;
-                double w = p * q;
-                double t2 = t * t, t3 = t2 * t, t4 = t2 * t2;
-                double d = fma(w, fma(fma(k2, t, k1), t, k0), EPS);
-                double r = 1.0 / d;
-                double v = r * w;
-                m[0] += v; m[1] = fma(v, t, m[1]); m[2] = fma(v, t2, m[2]);
-                double v2 = v * v;
-                m[3] += v2; m[4] = fma(v2, t, m[4]); m[5] = fma(v2, t2, m[5]); m[6] = fma(v2, t3, m[6]);
-                m[7] = fma(v2, t4, m[7]);
-                ob += log(d);
-            }
-            const int gb = b ? 19 : 11, hb = b ? 22 : 14;
-#pragma unroll
-            for (int i = 0; i < 3; i++) acc_add(acc, gb + i, m[i]);
-#pragma unroll
-            for (int i = 0; i < 5; i++) acc_add(acc, hb + i, m[3 + i]);
-            acc_add(acc, NMOM, ob);
-        }
-        {
-            const double c0 = ld_volatile(&Kp->c[0]), c1 = ld_volatile(&Kp->c[1]);
-            const double c2 = ld_volatile(&Kp->c[2]), c3 = ld_volatile(&Kp->c[3]);
-            double m[13] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
-            double ob = 0.0;
-            for (int j = sC + lane; j < sD; j += 32) {
-                unsigned e = E[j];
-                double p = P[e & 0x7FF], q = Q[e & 0x7FF];
-                bool s = (e >> 15) != 0;
-                double tx = s ? q : p, ty = s ? p : q;
-                double w = p * q;
-                double d = fma(w, fma(w, c3, fma(tx, c2, fma(ty, c1, c0))), EPS);
-                double r = 1.0 / d;
-                double v = r * w;
-                m[0] += v; m[1] = fma(v, ty, m[1]); m[2] = fma(v, tx, m[2]); m[3] = fma(v, w, m[3]);
-                double v2 = v * v;
-                m[4] += v2; m[5] = fma(v2, ty, m[5]); m[6] = fma(v2, tx, m[6]); m[7] = fma(v2, w, m[7]);
-                m[8] = fma(v2, ty * ty, m[8]); m[9] = fma(v2, tx * tx, m[9]);
-                m[10] = fma(v2, w * ty, m[10]); m[11] = fma(v2, w * tx, m[11]); m[12] = fma(v2, w * w, m[12]);
-                ob += log(d);
-            }
-#pragma unroll
-            for (int i = 0; i < 13; i++) acc_add(acc, 27 + i, m[i]);
-            acc_add(acc, NMOM, ob);
-        }
-        {
-            const double d0 = ld_volatile(&Kp->d[0]), d1 = ld_volatile(&Kp->d[1]);
-            double m[5] = {0, 0, 0, 0, 0};
-            double ob = 0.0;
-            for (int j = sD + lane; j < tot; j += 32) {
-                unsigned e = E[j];
-                double p = P[e & 0x7FF], q = Q[e & 0x7FF];
-                double w = p * q;
-                double d = fma(w, fma(w, d1, d0), EPS);
-                double r = 1.0 / d;
-                double v = r * w;
-                m[0] += v; m[1] = fma(v, w, m[1]);
-                double v2 = v * v;
-                m[2] += v2; m[3] = fma(v2, w, m[3]); m[4] = fma(v2, w * w, m[4]);
-                ob += log(d);
-            }
-#pragma unroll
-            for (int i = 0; i < 5; i++) acc_add(acc, 40 + i, m[i]);
-            acc_add(acc, NMOM, ob);
-        }
+        F += log(d);
+    };
+    const int64_t n2 = len >> 1;
+    const double2* L2 = reinterpret_cast<const double2*>(L);
+    for (int64_t k = lane; k < n2; k += 32) {
+        const double2 tv = L2[k];
+        site(tv.x);
+        site(tv.y);
     }
+    if (lane == 0 && (len & 1)) site(L[len - 1]);
+#pragma unroll
+    for (int i = 0; i < NG; i++) out.m[GOFF + i] = g[i];
+#pragma unroll
+    for (int i = 0; i < NH; i++) out.m[HOFF + i] = h[i];
+    out.obj += F;
 }
 
 // ----------------------------------------------------------- reductions
@@ -613,16 +593,6 @@ __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
     return v;
-}
-
-// Sums the lane accumulators across the warp into o (all lanes get the totals).
-__device__ inline void reduce_pass(const double* acc, PassOut& o) {
-    for (int i = 0; i < NMOM; i++) o.mom[i] = warp_sum(acc[i * 32]);
-    o.obj = warp_sum(acc[NMOM * 32]);
-}
-
-__device__ inline void zero_acc(double* acc) {
-    for (int i = 0; i < NACC; i++) acc[i * 32] = 0.0;
 }
 
 // ------------------------------------------------------------- pair SQP
@@ -635,13 +605,13 @@ struct PairEval {
     double H[81];
 };
 
-// Evaluates f, g, H at x.  For PASS_FP32_DIFF, f = f_base - (sum log(d/d_base))/n
-// with x_base the accepted point.  wsm is the warp's shared-memory block.
-__device__ inline void evaluate(const CohortDev& co, const uint16_t* ent, const uint16_t* hdr,
-                                int64_t n, int kind, const double* x, const double* x_base,
-                                double f_base, int lane, char* wsm, PairEval& ev, PassOut& po) {
-    double* acc = reinterpret_cast<double*>(wsm) + lane;
-    void* kbuf = wsm + WARP_SMEM_ACC;
+// Evaluates f, g, H at x from the pair's lists (FP32 lists for the FP32
+// kinds, FP64 lists for PASS_FP64).  For PASS_FP32_DIFF,
+// f = f_base - (sum log(d/d_base))/n with x_base the accepted point.
+__device__ inline void evaluate(const PairLists& pl, const void* lists, int kind, const double* x,
+                                const double* x_base, double f_base, int lane, char* wsm,
+                                PairEval& ev) {
+    void* kbuf = wsm + WARP_SMEM_BUF;
     PassCoef k;
     make_coef(x, k);
     __syncwarp();
@@ -661,28 +631,48 @@ __device__ inline void evaluate(const CohortDev& co, const uint16_t* ent, const 
         for (int i = 0; i < 2; i++) c.sd[i] = (float)ks.d[i];
         *reinterpret_cast<Coef32*>(kbuf) = c;
     }
-    zero_acc(acc);
     __syncwarp();
+    LaneSums ls;
+    ls.obj = 0.0;
     if (kind == PASS_FP64) {
-        pass_fp64(co, ent, hdr, reinterpret_cast<const PassCoef*>(kbuf), acc, lane);
-    } else if (kind == PASS_FP32_DIFF) {
-        pass_fp32<OBJ_DIFF>(co, ent, hdr, reinterpret_cast<const Coef32*>(kbuf), acc, lane);
+        const double* L = static_cast<const double*>(lists);
+        const PassCoef* K = reinterpret_cast<const PassCoef*>(kbuf);
+        stream64<0>(L + pl.start[0], pl.cnt[0], K, lane, ls);
+        stream64<1>(L + pl.start[1], pl.cnt[1], K, lane, ls);
+        stream64<2>(L + pl.start[2], pl.cnt[2], K, lane, ls);
+        stream64<3>(L + pl.start[3], pl.cnt[3], K, lane, ls);
+        stream64<4>(L + pl.start[4], pl.cnt[4], K, lane, ls);
     } else {
-        pass_fp32<OBJ_DIRECT>(co, ent, hdr, reinterpret_cast<const Coef32*>(kbuf), acc, lane);
+        const float* L = static_cast<const float*>(lists);
+        const Coef32* K = reinterpret_cast<const Coef32*>(kbuf);
+        if (kind == PASS_FP32_DIFF) {
+            stream32<0, OBJ_DIFF>(L + pl.start[0], pl.cnt[0], K, lane, ls);
+            stream32<1, OBJ_DIFF>(L + pl.start[1], pl.cnt[1], K, lane, ls);
+            stream32<2, OBJ_DIFF>(L + pl.start[2], pl.cnt[2], K, lane, ls);
+            stream32<3, OBJ_DIFF>(L + pl.start[3], pl.cnt[3], K, lane, ls);
+            stream32<4, OBJ_DIFF>(L + pl.start[4], pl.cnt[4], K, lane, ls);
+        } else {
+            stream32<0, OBJ_DIRECT>(L + pl.start[0], pl.cnt[0], K, lane, ls);
+            stream32<1, OBJ_DIRECT>(L + pl.start[1], pl.cnt[1], K, lane, ls);
+            stream32<2, OBJ_DIRECT>(L + pl.start[2], pl.cnt[2], K, lane, ls);
+            stream32<3, OBJ_DIRECT>(L + pl.start[3], pl.cnt[3], K, lane, ls);
+            stream32<4, OBJ_DIRECT>(L + pl.start[4], pl.cnt[4], K, lane, ls);
+        }
     }
-    __syncwarp();
-    reduce_pass(acc, po);
-    const double inv_n = 1.0 / (double)n;
+    double mom[NMOM];
+    for (int i = 0; i < NMOM; i++) mom[i] = warp_sum(ls.m[i]);
+    const double obj = warp_sum(ls.obj);
+    const double n = (double)pl.n;
     double S[9];
-    rebuild(po.mom, S, ev.H);
-    for (int i = 0; i < 9; i++) ev.g[i] = -S[i] / (double)n;
-    for (int i = 0; i < 81; i++) ev.H[i] = ev.H[i] / (double)n;
+    rebuild(mom, S, ev.H);
+    for (int i = 0; i < 9; i++) ev.g[i] = -S[i] / n;
+    for (int i = 0; i < 81; i++) ev.H[i] = ev.H[i] / n;
     if (kind == PASS_FP64) {
-        ev.f = -po.obj / (double)n;
+        ev.f = -obj / n;
     } else if (kind == PASS_FP32_DIRECT) {
-        ev.f = -(po.obj * 0.69314718055994530942) * inv_n;
+        ev.f = -(obj * 0.69314718055994530942) / n;
     } else {
-        ev.f = f_base - po.obj * inv_n;
+        ev.f = f_base - obj / n;
     }
 }
 
@@ -711,9 +701,11 @@ __host__ __device__ constexpr int flops_diff_extra(int s) {
     return s == 0 ? 18 : s == 1 ? 16 : s == 2 ? 16 : s == 3 ? 18 : 14;
 }
 
-__device__ inline void solve_pair(const CohortDev& co, const uint16_t* ent, const uint16_t* hdr,
-                                  int64_t n, bool self_pair, int precision, const Tune& tu, int lane,
-                                  char* wsm, PairResult& res) {
+// SQP of one pair (src/sqp.rs:49-93) over its sorted lists.  The FP32 lists
+// are replaced by FP64 lists when the pair escalates.
+__device__ inline void solve_pair(const CohortDev& co, int64_t px, int64_t py, const PairLists& pl,
+                                  void* lists, bool self_pair, int precision, const Tune& tu,
+                                  int lane, char* wsm, PairResult& res) {
     double x[9];
     for (int i = 0; i < 9; i++) x[i] = self_pair ? 0.0 : 1.0 / 9.0;
     if (self_pair) { x[0] = 0.5; x[6] = 0.5; }
@@ -725,8 +717,7 @@ __device__ inline void solve_pair(const CohortDev& co, const uint16_t* ent, cons
     res.diff_passes = 0;
     res.escalated = false;
     PairEval ev;
-    PassOut po;
-    evaluate(co, ent, hdr, n, fp64 ? PASS_FP64 : PASS_FP32_DIRECT, x, x, 0.0, lane, wsm, ev, po);
+    evaluate(pl, lists, fp64 ? PASS_FP64 : PASS_FP32_DIRECT, x, x, 0.0, lane, wsm, ev);
     res.obj_passes++;
     res.gh_passes++;
     if (fp64) res.fp64_passes++;
@@ -744,7 +735,9 @@ __device__ inline void solve_pair(const CohortDev& co, const uint16_t* ent, cons
             bool recheck = conv ? !(cond <= COND_RECHECK) : (near_count >= 3);
             if (recheck) {
                 // FP64 re-evaluation at the same point; the pair stays FP64 from here.
-                evaluate(co, ent, hdr, n, PASS_FP64, x, x, f, lane, wsm, ev, po);
+                scatter_shapes<double>(co, px, py, lane, pl, static_cast<double*>(lists),
+                                       reinterpret_cast<double*>(wsm));
+                evaluate(pl, lists, PASS_FP64, x, x, f, lane, wsm, ev);
                 res.fp64_passes++;
                 res.gh_passes++;
                 res.obj_passes++;
@@ -783,7 +776,7 @@ __device__ inline void solve_pair(const CohortDev& co, const uint16_t* ent, cons
             normalise9(xn);
             int kind = fp64 ? PASS_FP64
                             : (fabs(alpha * gp) < DIFF_BELOW ? PASS_FP32_DIFF : PASS_FP32_DIRECT);
-            evaluate(co, ent, hdr, n, kind, xn, x, f, lane, wsm, ev, po);
+            evaluate(pl, lists, kind, xn, x, f, lane, wsm, ev);
             res.obj_passes++;
             res.gh_passes++;
             if (kind == PASS_FP64) res.fp64_passes++;
