@@ -274,7 +274,7 @@ def main():
             "e2e": e2e, "roofline": roof, "clocks": clk,
             "gpu_launches": int(stats["launches"]) * args.steps,
             "stats": {k: stats[k] for k in ("gh_passes", "fp64_passes", "fp64_pairs", "pair_sites",
-                                            "work_units", "shape_sites")}}
+                                            "work_units", "shape_sites", "phase_cycles")}}
     if rank == 0 and not args.no_cpu and world == 1:
         line["cpu_baseline"] = cpu_baseline(codes, cohort.planted, args.cpu_seconds)
     if rank == 0:

@@ -159,6 +159,7 @@ class Estimator:
         _check(self._L.kg_last_run_stats(self._h, ctypes.byref(s)), self._h)
         d = {f: getattr(s, f) for f, _ in KgRunStats._fields_}
         d["shape_sites"] = list(s.shape_sites)
+        d["phase_cycles"] = list(s.phase_cycles)
         return d
 
     def relatedness_batch(self, cohorts, iterations: int = 100, maf=None):

@@ -164,7 +164,7 @@ __global__ void scan_sums_kernel(int32_t* __restrict__ bsum, int64_t nb, int32_t
 __global__ void compact_kernel(const uint8_t* __restrict__ keep, const int32_t* __restrict__ kidx,
                                const int32_t* __restrict__ bsum, const double* __restrict__ pf,
                                const double* __restrict__ qf, int64_t n, int32_t* __restrict__ site_of,
-                               float2* __restrict__ pq32, double* __restrict__ p64,
+                               float* __restrict__ p32, double* __restrict__ p64,
                                double* __restrict__ q64) {
     int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (v >= n || !keep[v]) return;
@@ -172,14 +172,14 @@ __global__ void compact_kernel(const uint8_t* __restrict__ keep, const int32_t* 
     site_of[k] = (int32_t)v;
     p64[k] = pf[v];
     q64[k] = qf[v];
-    pq32[k] = make_float2((float)pf[v], (float)qf[v]);
+    p32[k] = (float)pf[v];
 }
 
-__global__ void pad_kernel(const int32_t* __restrict__ nkept, int64_t cap, float2* __restrict__ pq32,
+__global__ void pad_kernel(const int32_t* __restrict__ nkept, int64_t cap, float* __restrict__ p32,
                            double* __restrict__ p64, double* __restrict__ q64) {
     int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x + nkept[0];
     if (k >= cap) return;
-    pq32[k] = make_float2(0.5f, 0.5f);
+    p32[k] = 0.5f;
     p64[k] = 0.5;
     q64[k] = 0.5;
 }
@@ -269,7 +269,7 @@ int prepare_cohort(Cohort& c, const uint8_t* codes, int64_t n_samples, int64_t n
     KG_CUDA_TRY((cudaError_t)c.nkept.reserve(sizeof(int32_t) * 4));
     KG_CUDA_TRY((cudaError_t)c.pfull.reserve(sizeof(double) * n_sites));
     KG_CUDA_TRY((cudaError_t)c.qfull.reserve(sizeof(double) * n_sites));
-    KG_CUDA_TRY((cudaError_t)c.p32.reserve(sizeof(float2) * cap));
+    KG_CUDA_TRY((cudaError_t)c.p32.reserve(sizeof(float) * cap));
     KG_CUDA_TRY((cudaError_t)c.p64.reserve(sizeof(double) * cap));
     KG_CUDA_TRY((cudaError_t)c.q64.reserve(sizeof(double) * cap));
     KG_CUDA_TRY((cudaError_t)c.site_of.reserve(sizeof(int32_t) * n_sites));
@@ -294,9 +294,9 @@ int prepare_cohort(Cohort& c, const uint8_t* codes, int64_t n_samples, int64_t n
     scan_sums_kernel<<<1, SCAN_BLOCK, 0, st>>>(c.bsum.as<int32_t>(), nb, c.nkept.as<int32_t>());
     compact_kernel<<<grid_for(n_sites, 256), 256, 0, st>>>(
         c.keep.as<uint8_t>(), c.kidx.as<int32_t>(), c.bsum.as<int32_t>(), c.pfull.as<double>(),
-        c.qfull.as<double>(), n_sites, c.site_of.as<int32_t>(), c.p32.as<float2>(),
+        c.qfull.as<double>(), n_sites, c.site_of.as<int32_t>(), c.p32.as<float>(),
         c.p64.as<double>(), c.q64.as<double>());
-    pad_kernel<<<grid_for(cap, 256), 256, 0, st>>>(c.nkept.as<int32_t>(), cap, c.p32.as<float2>(),
+    pad_kernel<<<grid_for(cap, 256), 256, 0, st>>>(c.nkept.as<int32_t>(), cap, c.p32.as<float>(),
                                                     c.p64.as<double>(), c.q64.as<double>());
     {
         int64_t work = n_samples * c.plane_stride;
@@ -397,6 +397,7 @@ jacquard_pair_kernel(PairLaunch L) {
     unsigned long long c_gh = 0, c_obj = 0, c_f64 = 0, c_f64p = 0, c_sites = 0, c_work = 0,
                        c_nosite = 0, c_nonconv = 0, c_fl32 = 0, c_fl64 = 0;
     unsigned long long c_shape[5] = {0, 0, 0, 0, 0};
+    unsigned long long c_cyc[4] = {0, 0, 0, 0};
     for (;;) {
         unsigned long long k = 0;
         if (lane == 0) k = atomicAdd(L.queue, 1ull);
@@ -414,7 +415,9 @@ jacquard_pair_kernel(PairLaunch L) {
             y = j - x * co.n_y;
         }
         PairLists pl;
+        long long tc0 = clock64();
         count_shapes(co, x, y, lane, pl);
+        c_cyc[0] += clock64() - tc0;
         kg_output row;
         row.x = (uint64_t)x;
         row.y = (uint64_t)y;
@@ -425,12 +428,12 @@ jacquard_pair_kernel(PairLaunch L) {
             row.cond = CUDART_NAN;
             c_nosite++;
         } else {
+            long long ts0 = clock64();
             if (L.precision == 1)
-                scatter_shapes<double>(co, x, y, lane, pl, static_cast<double*>(lists),
-                                       reinterpret_cast<double*>(wsm));
+                scatter_shapes<double>(co, x, y, lane, pl, static_cast<double*>(lists), wsm);
             else
-                scatter_shapes<float>(co, x, y, lane, pl, static_cast<float*>(lists),
-                                      reinterpret_cast<float*>(wsm));
+                scatter_shapes<float>(co, x, y, lane, pl, static_cast<float*>(lists), wsm);
+            c_cyc[1] += clock64() - ts0;
             PairResult res;
             const bool self_pair = (co.kind == COHORT_TRIANGLE) && (x == y);
             solve_pair(co, x, y, pl, lists, self_pair, L.precision, L.tune, lane, wsm, res);
@@ -438,6 +441,8 @@ jacquard_pair_kernel(PairLaunch L) {
             row.obj = res.f;
             row.iters = res.iters;
             row.cond = res.cond;
+            c_cyc[2] += res.cyc_pass;
+            c_cyc[3] += res.cyc_solve;
             c_gh += res.gh_passes;
             c_obj += res.obj_passes;
             c_f64 += res.fp64_passes;
@@ -475,6 +480,7 @@ jacquard_pair_kernel(PairLaunch L) {
         atomicAdd(&L.counters->flops_fp32, c_fl32);
         atomicAdd(&L.counters->flops_fp64, c_fl64);
         for (int s = 0; s < 5; s++) atomicAdd(&L.counters->shape_sites[s], c_shape[s]);
+        for (int s = 0; s < 4; s++) atomicAdd(&L.counters->cycles[s], c_cyc[s]);
     }
 }
 
@@ -532,7 +538,7 @@ int run_pairs(const std::vector<PairJob>& jobs, const RunConfig& cfg, Workspace&
         d.planes_y = pn.planes.as<uint2>();
         d.planes_x = (jb.kind == COHORT_RECT) ? jb.query->planes.as<uint2>() : d.planes_y;
         d.plane_stride = pn.plane_stride;
-        d.pq32 = pn.p32.as<float2>();
+        d.p32 = pn.p32.as<float>();
         d.p64 = pn.p64.as<double>();
         d.q64 = pn.q64.as<double>();
         d.n_sites = (int32_t)pn.n_kept;
@@ -612,6 +618,7 @@ int run_pairs(const std::vector<PairJob>& jobs, const RunConfig& cfg, Workspace&
     stats.flops_fp32 = rc.flops_fp32;
     stats.flops_fp64 = rc.flops_fp64;
     for (int s = 0; s < 5; s++) stats.shape_sites[s] = rc.shape_sites[s];
+    for (int s = 0; s < 4; s++) stats.phase_cycles[s] = rc.cycles[s];
     stats.pair_kernel_ms = ms;
     if (rc.nosite_pairs) {
         err = "a pair has no jointly observed segregating site (its row is NaN)";

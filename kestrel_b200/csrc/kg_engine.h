@@ -51,7 +51,7 @@ struct Cohort {
     DevBuf bsum;               // int32 block sums of the scan
     DevBuf nkept;              // int32[2]: kept count, bad-code flag
     DevBuf pfull, qfull;       // double per raw site
-    DevBuf p32;                // float2 {REF, ALT} per kept site, padded to n_seg_max * 2048
+    DevBuf p32;                // float REF frequency per kept site, padded to n_seg_max * 2048
     DevBuf p64, q64;           // double, same length
     DevBuf site_of;            // int32 kept index -> raw site
     DevBuf planes;             // uint2 [n_samples][plane_stride]

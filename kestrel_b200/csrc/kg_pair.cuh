@@ -34,6 +34,7 @@
 #include <math_constants.h>
 
 #include "kestrel_gpu.h"
+#include "kg_rowsolve.cuh"
 #include "kg_solver.cuh"
 
 namespace kg {
@@ -50,7 +51,7 @@ struct CohortDev {
     const uint2* planes_x;   // [rows_x][plane_stride] {lo, hi} bit planes of 32 sites
     const uint2* planes_y;   // [rows_y][plane_stride] (== planes_x for a triangle)
     int64_t plane_stride;    // words per row (multiple of SEG_WORDS)
-    const float2* pq32;      // {REF, ALT} frequency per kept site in FP32, padded
+    const float* p32;        // REF frequency per kept site in FP32, padded
     const double* p64;       // REF frequency per kept site, padded
     const double* q64;       // ALT frequency per kept site, padded
     int32_t n_sites;         // kept (segregating) sites
@@ -76,6 +77,7 @@ struct RunCounters {
     unsigned long long flops_fp32;
     unsigned long long flops_fp64;
     unsigned long long shape_sites[5];
+    unsigned long long cycles[4];   // SM clocks per phase: count, scatter, site passes, solver
 };
 
 struct PairLaunch {
@@ -268,34 +270,45 @@ __device__ inline void count_shapes(const CohortDev& co, int64_t x, int64_t y, i
     }
 }
 
-template <class T>
-__device__ __forceinline__ T site_value(const CohortDev& co, int64_t site, bool sel);
-
-template <>
-__device__ __forceinline__ float site_value<float>(const CohortDev& co, int64_t site, bool sel) {
-    float2 v = co.pq32[site];
-    return sel ? v.y : v.x;
-}
-
-template <>
-__device__ __forceinline__ double site_value<double>(const CohortDev& co, int64_t site, bool sel) {
-    return sel ? co.q64[site] : co.p64[site];
-}
-
 // Writes the frequency value t of every jointly observed site into its shape
-// list (in FP32 or FP64), one unit of 1024 sites at a time through the warp's
-// shared buffer so the global stores stay coalesced.
+// list (in FP32 or FP64), one unit of 1024 sites at a time.  The unit's REF
+// frequencies are first staged in shared memory with coalesced loads (lane l
+// holds sites 32 l .. 32 l + 31, stored transposed so the per-site reads are
+// conflict-free); t is p or 1 - p by the site's sel bit.  FP32 values go through
+// a shared output buffer so the global stores stay coalesced; FP64 values (the
+// FP64 form and re-evaluated pairs) are stored directly.
 template <class T>
 __device__ inline void scatter_shapes(const CohortDev& co, int64_t x, int64_t y, int lane,
-                                      const PairLists& pl, T* lists, T* buf) {
+                                      const PairLists& pl, T* lists, char* wsm) {
     const uint2* px = co.planes_x + x * co.plane_stride;
     const uint2* py = co.planes_y + y * co.plane_stride;
+    T* stage = reinterpret_cast<T*>(wsm);                       // UNIT_SITES values
+    float* obuf = reinterpret_cast<float*>(wsm + UNIT_SITES * sizeof(float));  // FP32 only
     int64_t off[5];
 #pragma unroll
     for (int s = 0; s < 5; s++) off[s] = pl.start[s];
     for (int u = 0; u < co.n_units; u++) {
         const int w = u * UNIT_WORDS + lane;
-        ShapeMasks sm = shape_masks(px[w], py[w]);
+        const uint2 X = px[w], Y = py[w];
+        // stage this lane's 32 REF frequencies: site 32 lane + i at [i * 32 + lane]
+        if (sizeof(T) == 4) {
+            const float4* src = reinterpret_cast<const float4*>(co.p32 + (int64_t)u * UNIT_SITES + lane * 32);
+#pragma unroll
+            for (int v4 = 0; v4 < 8; v4++) {
+                const float4 f = src[v4];
+                float* st = reinterpret_cast<float*>(stage) + (v4 * 4) * 32 + lane;
+                st[0] = f.x; st[32] = f.y; st[64] = f.z; st[96] = f.w;
+            }
+        } else {
+            const double2* src = reinterpret_cast<const double2*>(co.p64 + (int64_t)u * UNIT_SITES + lane * 32);
+#pragma unroll
+            for (int v2 = 0; v2 < 16; v2++) {
+                const double2 f = src[v2];
+                double* st = reinterpret_cast<double*>(stage) + (v2 * 2) * 32 + lane;
+                st[0] = f.x; st[32] = f.y;
+            }
+        }
+        ShapeMasks sm = shape_masks(X, Y);
         unsigned long long v = 0;
 #pragma unroll
         for (int s = 0; s < 5; s++) v |= (unsigned long long)__popc(sm.m[s]) << (11 * s);
@@ -311,27 +324,34 @@ __device__ inline void scatter_shapes(const CohortDev& co, int64_t x, int64_t y,
         ustart[0] = 0;
 #pragma unroll
         for (int s = 0; s < 5; s++) ustart[s + 1] = ustart[s] + (unsigned)((tot >> (11 * s)) & 0x7FF);
-        const int64_t base = (int64_t)u * UNIT_SITES + lane * 32;
+        __syncwarp();
 #pragma unroll
         for (int s = 0; s < 5; s++) {
-            unsigned pos = ustart[s] + (unsigned)((exc >> (11 * s)) & 0x7FF);
+            unsigned rank = (unsigned)((exc >> (11 * s)) & 0x7FF);
             uint32_t mm = sm.m[s];
             while (mm) {
-                int i = __ffs(mm) - 1;
+                const int i = __ffs(mm) - 1;
                 mm &= mm - 1;
-                buf[pos++] = site_value<T>(co, base + i, (sm.sel >> i) & 1u);
+                const T p = stage[i * 32 + lane];
+                const T t = ((sm.sel >> i) & 1u) ? (T)1 - p : p;
+                if (sizeof(T) == 4) obuf[ustart[s] + rank] = (float)t;
+                else lists[off[s] + rank] = t;
+                rank++;
             }
         }
         __syncwarp();
+        if (sizeof(T) == 4) {
 #pragma unroll
-        for (int s = 0; s < 5; s++) {
-            const unsigned ns = ustart[s + 1] - ustart[s];
-            T* dst = lists + off[s];
-            const T* src = buf + ustart[s];
-            for (unsigned j = lane; j < ns; j += 32) dst[j] = src[j];
-            off[s] += ns;
+            for (int s = 0; s < 5; s++) {
+                const unsigned ns = ustart[s + 1] - ustart[s];
+                float* dst = reinterpret_cast<float*>(lists) + off[s];
+                const float* srcb = obuf + ustart[s];
+                for (unsigned j = lane; j < ns; j += 32) dst[j] = srcb[j];
+            }
+            __syncwarp();
         }
-        __syncwarp();
+#pragma unroll
+        for (int s = 0; s < 5; s++) off[s] += ustart[s + 1] - ustart[s];
     }
 }
 
@@ -346,7 +366,7 @@ struct Coef32 {
     float sa[4], sb1[3], sb2[3], sc[4], sd[2];  // step coefficients (OBJ_DIFF)
 };
 
-constexpr int WARP_SMEM_BUF = UNIT_SITES * 8;   // sort buffer (FP64 values at most)
+constexpr int WARP_SMEM_BUF = UNIT_SITES * 8;   // frequency stage + FP32 output buffer
 constexpr int WARP_SMEM_COEF = 256;
 constexpr int WARP_SMEM = WARP_SMEM_BUF + WARP_SMEM_COEF;
 static_assert(sizeof(Coef32) <= WARP_SMEM_COEF, "coefficients must fit");
@@ -470,8 +490,18 @@ __device__ __noinline__ void stream32(const float* __restrict__ L, int64_t len, 
     const int64_t n4 = len >> 2;
     const float4* L4 = reinterpret_cast<const float4*>(L);
     int it = 0;
+    // four float4 loads in flight per lane: the lists stream from HBM
+    const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
+    float4 q0 = (lane < n4) ? L4[lane] : z4;
+    float4 q1 = (lane + 32 < n4) ? L4[lane + 32] : z4;
+    float4 q2 = (lane + 64 < n4) ? L4[lane + 64] : z4;
+    float4 q3 = (lane + 96 < n4) ? L4[lane + 96] : z4;
     for (int64_t k = lane; k < n4; k += 32) {
-        const float4 tv = L4[k];
+        const float4 tv = q0;
+        q0 = q1;
+        q1 = q2;
+        q2 = q3;
+        q3 = (k + 128 < n4) ? L4[k + 128] : z4;
         float g[NG], ob = 0.f;
 #pragma unroll
         for (int i = 0; i < NG; i++) g[i] = 0.f;
@@ -574,8 +604,17 @@ __device__ __noinline__ void stream64(const double* __restrict__ L, int64_t len,
     };
     const int64_t n2 = len >> 1;
     const double2* L2 = reinterpret_cast<const double2*>(L);
+    const double2 z2 = make_double2(0.0, 0.0);
+    double2 q0 = (lane < n2) ? L2[lane] : z2;
+    double2 q1 = (lane + 32 < n2) ? L2[lane + 32] : z2;
+    double2 q2 = (lane + 64 < n2) ? L2[lane + 64] : z2;
+    double2 q3 = (lane + 96 < n2) ? L2[lane + 96] : z2;
     for (int64_t k = lane; k < n2; k += 32) {
-        const double2 tv = L2[k];
+        const double2 tv = q0;
+        q0 = q1;
+        q1 = q2;
+        q2 = q3;
+        q3 = (k + 128 < n2) ? L2[k + 128] : z2;
         site(tv.x);
         site(tv.y);
     }
@@ -601,9 +640,56 @@ enum : int { PASS_FP32_DIRECT = 0, PASS_FP32_DIFF = 1, PASS_FP64 = 2 };
 
 struct PairEval {
     double f;       // objective at the evaluated point
-    double g[9];
-    double H[81];
+    double g[9];    // gradient (warp-uniform)
+    double Hr[9];   // this lane's row of the Hessian (lanes 0..8)
 };
+
+__constant__ int kEA[9] = {1, 2, 2, 3, 2, 3, 2, 3, 4};      // t-power of each entry in shape A
+__constant__ int kPosB1[9] = {-1, -1, 0, 1, -1, -1, -1, 2, 3};
+__constant__ int kPosB2[9] = {-1, -1, -1, -1, 0, 1, -1, 2, 3};
+__constant__ int kPosC[9] = {-1, 0, -1, 1, -1, 2, -1, -1, 3};
+__constant__ int kPosD[9] = {-1, -1, -1, -1, -1, -1, 0, 1, 2};
+__constant__ int kHC[4][4] = {{0, 1, 2, 3}, {1, 4, 3, 6}, {2, 3, 5, 7}, {3, 6, 7, 8}};
+
+// Row r of S = sum L r and T = sum L L' r^2 from the 45 moment totals (shared
+// memory), adding the shapes' contributions in the order A, B1, B2, C, D.
+__device__ inline void rebuild_row(const double* mom, int r, double& S, double* T) {
+    const int cb[4] = {1, 2, 1, 2};
+    const int pb[4] = {0, 1, 1, 2};
+    const int i1[4] = {2, 3, 7, 8};
+    const int i2[4] = {4, 5, 7, 8};
+    const int ic[4] = {1, 3, 5, 8};
+    const int id[3] = {6, 7, 8};
+    const double cd[3] = {2.0, 1.0, 4.0};
+    const int pd[3] = {0, 0, 1};
+    const int er = kEA[r];
+    S = mom[er - 1];
+#pragma unroll
+    for (int j = 0; j < 9; j++) {
+        const int ej = (j == 0) ? 1 : (j == 8) ? 4 : (j == 3 || j == 5 || j == 7) ? 3 : 2;
+        T[j] = mom[4 + er + ej - 2];
+    }
+    const int a1 = kPosB1[r], a2 = kPosB2[r], ac = kPosC[r], ad = kPosD[r];
+    if (a1 >= 0) S += (double)cb[a1] * mom[11 + pb[a1]];
+    if (a2 >= 0) S += (double)cb[a2] * mom[19 + pb[a2]];
+    if (ac >= 0) S += mom[27 + ac];
+    if (ad >= 0) S += (ad == 0 ? 2.0 : ad == 1 ? 1.0 : 4.0) * mom[40 + (ad == 2 ? 1 : 0)];
+#pragma unroll
+    for (int b = 0; b < 4; b++) {
+        if (a1 >= 0) T[i1[b]] += (double)(cb[a1] * cb[b]) * mom[14 + pb[a1] + pb[b]];
+        if (a2 >= 0) T[i2[b]] += (double)(cb[a2] * cb[b]) * mom[22 + pb[a2] + pb[b]];
+    }
+    if (ac >= 0) {
+#pragma unroll
+        for (int b = 0; b < 4; b++) T[ic[b]] += mom[31 + kHC[ac][b]];
+    }
+    if (ad >= 0) {
+        const double ca = (ad == 0 ? 2.0 : ad == 1 ? 1.0 : 4.0);
+        const int pa = (ad == 2 ? 1 : 0);
+#pragma unroll
+        for (int b = 0; b < 3; b++) T[id[b]] += ca * cd[b] * mom[42 + pa + pd[b]];
+    }
+}
 
 // Evaluates f, g, H at x from the pair's lists (FP32 lists for the FP32
 // kinds, FP64 lists for PASS_FP64).  For PASS_FP32_DIFF,
@@ -612,6 +698,7 @@ __device__ inline void evaluate(const PairLists& pl, const void* lists, int kind
                                 const double* x_base, double f_base, int lane, char* wsm,
                                 PairEval& ev) {
     void* kbuf = wsm + WARP_SMEM_BUF;
+    double* mom_s = reinterpret_cast<double*>(wsm);   // NMOM + 1 totals (sort buffer is free)
     PassCoef k;
     make_coef(x, k);
     __syncwarp();
@@ -659,14 +746,23 @@ __device__ inline void evaluate(const PairLists& pl, const void* lists, int kind
             stream32<4, OBJ_DIRECT>(L + pl.start[4], pl.cnt[4], K, lane, ls);
         }
     }
-    double mom[NMOM];
-    for (int i = 0; i < NMOM; i++) mom[i] = warp_sum(ls.m[i]);
+    for (int i = 0; i < NMOM; i++) {
+        const double v = warp_sum(ls.m[i]);
+        if (lane == 0) mom_s[i] = v;
+    }
     const double obj = warp_sum(ls.obj);
+    __syncwarp();
     const double n = (double)pl.n;
-    double S[9];
-    rebuild(mom, S, ev.H);
-    for (int i = 0; i < 9; i++) ev.g[i] = -S[i] / n;
-    for (int i = 0; i < 81; i++) ev.H[i] = ev.H[i] / n;
+    double S = 0.0;
+#pragma unroll
+    for (int j = 0; j < 9; j++) ev.Hr[j] = 0.0;
+    if (lane < 9) {
+        rebuild_row(mom_s, lane, S, ev.Hr);
+#pragma unroll
+        for (int j = 0; j < 9; j++) ev.Hr[j] = ev.Hr[j] / n;
+    }
+    gather9(-S / n, ev.g);
+    __syncwarp();
     if (kind == PASS_FP64) {
         ev.f = -obj / n;
     } else if (kind == PASS_FP32_DIRECT) {
@@ -680,6 +776,8 @@ constexpr double COND_RECHECK = 1e4;   // FP32 condition estimates above this ar
 constexpr double DIFF_BELOW = 1e-4;    // |alpha g.p| under which the objective change is summed directly
 
 struct PairResult {
+    unsigned long long cyc_pass;    // clocks spent in site passes
+    unsigned long long cyc_solve;   // clocks spent in the 9x9 solver steps
     double x[9];
     double f;
     uint64_t iters;
@@ -701,12 +799,23 @@ __host__ __device__ constexpr int flops_diff_extra(int s) {
     return s == 0 ? 18 : s == 1 ? 16 : s == 2 ? 16 : s == 3 ? 18 : 14;
 }
 
+// Condition estimate from the row-distributed Hessian (once per pair).
+__device__ inline double condition_rows(const double* x, const double* g, const double* Hr, double tol) {
+    double H[81];
+#pragma unroll
+    for (int i = 0; i < 9; i++)
+#pragma unroll
+        for (int j = 0; j < 9; j++) H[i * 9 + j] = bcast(Hr[j], i);
+    return condition_estimate(x, g, H, tol);
+}
+
 // SQP of one pair (src/sqp.rs:49-93) over its sorted lists.  The FP32 lists
 // are replaced by FP64 lists when the pair escalates.
 __device__ inline void solve_pair(const CohortDev& co, int64_t px, int64_t py, const PairLists& pl,
                                   void* lists, bool self_pair, int precision, const Tune& tu,
                                   int lane, char* wsm, PairResult& res) {
     double x[9];
+#pragma unroll
     for (int i = 0; i < 9; i++) x[i] = self_pair ? 0.0 : 1.0 / 9.0;
     if (self_pair) { x[0] = 0.5; x[6] = 0.5; }
     normalise9(x);
@@ -716,85 +825,101 @@ __device__ inline void solve_pair(const CohortDev& co, int64_t px, int64_t py, c
     res.obj_passes = 0;
     res.diff_passes = 0;
     res.escalated = false;
+    res.cyc_pass = 0;
+    res.cyc_solve = 0;
     PairEval ev;
+    const long long t_0 = clock64();
     evaluate(pl, lists, fp64 ? PASS_FP64 : PASS_FP32_DIRECT, x, x, 0.0, lane, wsm, ev);
+    res.cyc_pass += clock64() - t_0;
     res.obj_passes++;
     res.gh_passes++;
     if (fp64) res.fp64_passes++;
     double f = ev.f;
-    double g[9], H[81];
-    for (int i = 0; i < 9; i++) g[i] = ev.g[i];
-    for (int i = 0; i < 81; i++) H[i] = ev.H[i];
+    double g[9], Hr[9];
+#pragma unroll
+    for (int i = 0; i < 9; i++) { g[i] = ev.g[i]; Hr[i] = ev.Hr[i]; }
     int near_count = 0;
     for (uint64_t it = 0; it < tu.sqp_max_iter; it++) {
         double resid;
         bool conv = kkt_ok(x, g, tu.sqp_conv_tol, &resid);
         if (!fp64 && (conv || resid < 1e-6)) {
             if (!conv) near_count++;
-            double cond = conv ? condition_estimate(x, g, H, tu.sqp_conv_tol) : 0.0;
+            double cond = conv ? condition_rows(x, g, Hr, tu.sqp_conv_tol) : 0.0;
             bool recheck = conv ? !(cond <= COND_RECHECK) : (near_count >= 3);
             if (recheck) {
                 // FP64 re-evaluation at the same point; the pair stays FP64 from here.
-                scatter_shapes<double>(co, px, py, lane, pl, static_cast<double*>(lists),
-                                       reinterpret_cast<double*>(wsm));
+                scatter_shapes<double>(co, px, py, lane, pl, static_cast<double*>(lists), wsm);
+                const long long ta = clock64();
                 evaluate(pl, lists, PASS_FP64, x, x, f, lane, wsm, ev);
+                res.cyc_pass += clock64() - ta;
                 res.fp64_passes++;
                 res.gh_passes++;
                 res.obj_passes++;
                 fp64 = true;
                 res.escalated = true;
                 f = ev.f;
-                for (int i = 0; i < 9; i++) g[i] = ev.g[i];
-                for (int i = 0; i < 81; i++) H[i] = ev.H[i];
+#pragma unroll
+                for (int i = 0; i < 9; i++) { g[i] = ev.g[i]; Hr[i] = ev.Hr[i]; }
                 conv = kkt_ok(x, g, tu.sqp_conv_tol, &resid);
             } else if (conv) {
+#pragma unroll
                 for (int i = 0; i < 9; i++) res.x[i] = x[i];
                 res.f = f;
                 res.iters = it;
                 res.cond = cond;
+                res.cyc_solve = (clock64() - t_0) - res.cyc_pass;
                 return;
             }
         }
         if (conv) {
+#pragma unroll
             for (int i = 0; i < 9; i++) res.x[i] = x[i];
             res.f = f;
             res.iters = it;
-            res.cond = condition_estimate(x, g, H, tu.sqp_conv_tol);
+            res.cond = condition_rows(x, g, Hr, tu.sqp_conv_tol);
+            res.cyc_solve = (clock64() - t_0) - res.cyc_pass;
             return;
         }
         // QP step: c = g - H x
+        double cr = 0.0;
+        if (lane < 9) cr = pick9(g, lane) - dot_fma(9, Hr, x);
         double c[9], y[9], p[9];
-        for (int i = 0; i < 9; i++) c[i] = g[i] - dot_fma(9, H + i * 9, x);
-        qp_simplex(H, c, x, tu, y);
+        gather9(cr, c);
+        qp_simplex_rows(Hr, c, x, tu, lane, y);
+#pragma unroll
         for (int i = 0; i < 9; i++) p[i] = y[i] - x[i];
-        double gp = dot_fma(9, g, p);
-        double tt = tu.bls_sufficient_decrease * gp;
+        const double gp = dot_fma(9, g, p);
+        const double tt = tu.bls_sufficient_decrease * gp;
         double alpha = 1.0;
         double xn[9];
         for (int bls = 0;;) {
+#pragma unroll
             for (int i = 0; i < 9; i++) xn[i] = x[i] + alpha * p[i];
             normalise9(xn);
-            int kind = fp64 ? PASS_FP64
-                            : (fabs(alpha * gp) < DIFF_BELOW ? PASS_FP32_DIFF : PASS_FP32_DIRECT);
+            const int kind = fp64 ? PASS_FP64
+                                  : (fabs(alpha * gp) < DIFF_BELOW ? PASS_FP32_DIFF : PASS_FP32_DIRECT);
+            const long long ta = clock64();
             evaluate(pl, lists, kind, xn, x, f, lane, wsm, ev);
+            res.cyc_pass += clock64() - ta;
             res.obj_passes++;
             res.gh_passes++;
             if (kind == PASS_FP64) res.fp64_passes++;
             if (kind == PASS_FP32_DIFF) res.diff_passes++;
-            bool accept = ev.f <= f + alpha * tt;
+            const bool accept = ev.f <= f + alpha * tt;
             bls++;
             if (accept || bls == tu.bls_max_iter) break;
             alpha *= tu.bls_step_size_reduce;
         }
-        for (int i = 0; i < 9; i++) x[i] = xn[i];
+#pragma unroll
+        for (int i = 0; i < 9; i++) { x[i] = xn[i]; g[i] = ev.g[i]; Hr[i] = ev.Hr[i]; }
         f = ev.f;
-        for (int i = 0; i < 9; i++) g[i] = ev.g[i];
-        for (int i = 0; i < 81; i++) H[i] = ev.H[i];
     }
+#pragma unroll
     for (int i = 0; i < 9; i++) res.x[i] = x[i];
     res.f = f;
     res.iters = tu.sqp_max_iter;
     res.cond = CUDART_NAN;
+    res.cyc_solve = (clock64() - t_0) - res.cyc_pass;
 }
 
 }  // namespace kg
