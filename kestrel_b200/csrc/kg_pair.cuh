@@ -357,8 +357,6 @@ __device__ inline void scatter_shapes(const CohortDev& co, int64_t x, int64_t y,
 
 // ----------------------------------------------------------- FP32 passes
 
-enum : int { OBJ_DIRECT = 0, OBJ_DIFF = 1 };
-
 // Warp-uniform pass coefficients, kept in shared memory and read at the top
 // of each shape's stream so only that shape's values occupy registers.
 struct Coef32 {
@@ -387,14 +385,17 @@ struct LaneSums {
     double obj;
 };
 
-constexpr int HESS_FLUSH = 16;   // float4 iterations between FP32 -> FP64 Hessian flushes
+constexpr int HESS_FLUSH = 8;   // loop iterations (8 sites each) between FP32 -> FP64 Hessian flushes
 
-// Streams one shape's FP32 list.  Gradient moments and the objective are
-// promoted to FP64 every 4 sites, Hessian moments every 64; each site is the
-// closed form of its shape (see the file comment).
-template <int S, int OBJ>
+// Streams one shape's FP32 list.  Each loop iteration handles two float4
+// (8 sites per lane) held in two registers that are refilled right after use,
+// so every load has a full iteration to arrive.  Gradient moments and the
+// objective are promoted to FP64 every 8 sites, Hessian moments every 64; each
+// site is the closed form of its shape (see the file comment).  diff selects
+// the log(d_new/d_old) objective.
+template <int S>
 __device__ __noinline__ void stream32(const float* __restrict__ L, int64_t len, const Coef32* K,
-                                      int lane, LaneSums& out) {
+                                      bool diff, int lane, LaneSums& out) {
     constexpr int NG = S == 0 ? 4 : S == 3 ? 4 : S == 4 ? 2 : 3;
     constexpr int NH = S == 0 ? 7 : S == 3 ? 9 : S == 4 ? 3 : 5;
     constexpr int GOFF = S == 0 ? 0 : S == 1 ? 11 : S == 2 ? 19 : S == 3 ? 27 : 40;
@@ -407,7 +408,7 @@ __device__ __noinline__ void stream32(const float* __restrict__ L, int64_t len, 
     if (S == 2) { k0 = ldk(&K->b2[0]); k1 = ldk(&K->b2[1]); k2 = ldk(&K->b2[2]); k3 = HiLo{0.f, 0.f}; }
     if (S == 3) { k0 = ldk(&K->c[0]); k1 = ldk(&K->c[1]); k2 = ldk(&K->c[2]); k3 = ldk(&K->c[3]); }
     if (S == 4) { k0 = ldk(&K->d[0]); k1 = ldk(&K->d[1]); k2 = HiLo{0.f, 0.f}; k3 = HiLo{0.f, 0.f}; }
-    if (OBJ == OBJ_DIFF) {
+    if (diff) {
         const float* sp = S == 0 ? K->sa : S == 1 ? K->sb1 : S == 2 ? K->sb2 : S == 3 ? K->sc : K->sd;
         s0 = ld_volatile(&sp[0]);
         s1 = ld_volatile(&sp[1]);
@@ -421,7 +422,7 @@ __device__ __noinline__ void stream32(const float* __restrict__ L, int64_t len, 
 #pragma unroll
     for (int i = 0; i < NH; i++) { H[i] = 0.0; h[i] = 0.f; }
 
-    // one site: adds into the FP32 gradient/objective partials g, ob and h
+    // one site: adds into the FP32 partials g, ob (per iteration) and h
     auto site = [&](float t, float* g, float& ob) {
         float d, r, c;    // c = the per-site scale: t (A) or w (B, C, D)
         if (S == 0) {
@@ -475,7 +476,7 @@ __device__ __noinline__ void stream32(const float* __restrict__ L, int64_t len, 
             h[0] += v2; h[1] = fmaf(v2, w, h[1]); h[2] = fmaf(v2, w * w, h[2]);
             c = w;
         }
-        if (OBJ == OBJ_DIRECT) {
+        if (!diff) {
             ob += lg2_approx(d);
         } else {
             float dl;
@@ -489,26 +490,27 @@ __device__ __noinline__ void stream32(const float* __restrict__ L, int64_t len, 
 
     const int64_t n4 = len >> 2;
     const float4* L4 = reinterpret_cast<const float4*>(L);
-    int it = 0;
-    // four float4 loads in flight per lane: the lists stream from HBM
     const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
-    float4 q0 = (lane < n4) ? L4[lane] : z4;
-    float4 q1 = (lane + 32 < n4) ? L4[lane + 32] : z4;
-    float4 q2 = (lane + 64 < n4) ? L4[lane + 64] : z4;
-    float4 q3 = (lane + 96 < n4) ? L4[lane + 96] : z4;
-    for (int64_t k = lane; k < n4; k += 32) {
-        const float4 tv = q0;
-        q0 = q1;
-        q1 = q2;
-        q2 = q3;
-        q3 = (k + 128 < n4) ? L4[k + 128] : z4;
+    int64_t k = lane;
+    float4 va = (k < n4) ? L4[k] : z4;
+    float4 vb = (k + 32 < n4) ? L4[k + 32] : z4;
+    int it = 0;
+    while (k < n4) {
         float g[NG], ob = 0.f;
 #pragma unroll
         for (int i = 0; i < NG; i++) g[i] = 0.f;
-        site(tv.x, g, ob);
-        site(tv.y, g, ob);
-        site(tv.z, g, ob);
-        site(tv.w, g, ob);
+        site(va.x, g, ob);
+        site(va.y, g, ob);
+        site(va.z, g, ob);
+        site(va.w, g, ob);
+        va = (k + 64 < n4) ? L4[k + 64] : z4;
+        if (k + 32 < n4) {
+            site(vb.x, g, ob);
+            site(vb.y, g, ob);
+            site(vb.z, g, ob);
+            site(vb.w, g, ob);
+        }
+        vb = (k + 96 < n4) ? L4[k + 96] : z4;
 #pragma unroll
         for (int i = 0; i < NG; i++) G[i] += (double)g[i];
         F += (double)ob;
@@ -517,6 +519,7 @@ __device__ __noinline__ void stream32(const float* __restrict__ L, int64_t len, 
             for (int i = 0; i < NH; i++) { H[i] += (double)h[i]; h[i] = 0.f; }
             it = 0;
         }
+        k += 64;
     }
     if (lane < (int)(len & 3)) {
         float g[NG], ob = 0.f;
@@ -605,18 +608,19 @@ __device__ __noinline__ void stream64(const double* __restrict__ L, int64_t len,
     const int64_t n2 = len >> 1;
     const double2* L2 = reinterpret_cast<const double2*>(L);
     const double2 z2 = make_double2(0.0, 0.0);
-    double2 q0 = (lane < n2) ? L2[lane] : z2;
-    double2 q1 = (lane + 32 < n2) ? L2[lane + 32] : z2;
-    double2 q2 = (lane + 64 < n2) ? L2[lane + 64] : z2;
-    double2 q3 = (lane + 96 < n2) ? L2[lane + 96] : z2;
-    for (int64_t k = lane; k < n2; k += 32) {
-        const double2 tv = q0;
-        q0 = q1;
-        q1 = q2;
-        q2 = q3;
-        q3 = (k + 128 < n2) ? L2[k + 128] : z2;
-        site(tv.x);
-        site(tv.y);
+    int64_t k = lane;
+    double2 va = (k < n2) ? L2[k] : z2;
+    double2 vb = (k + 32 < n2) ? L2[k + 32] : z2;
+    while (k < n2) {
+        site(va.x);
+        site(va.y);
+        va = (k + 64 < n2) ? L2[k + 64] : z2;
+        if (k + 32 < n2) {
+            site(vb.x);
+            site(vb.y);
+        }
+        vb = (k + 96 < n2) ? L2[k + 96] : z2;
+        k += 64;
     }
     if (lane == 0 && (len & 1)) site(L[len - 1]);
 #pragma unroll
@@ -732,19 +736,12 @@ __device__ inline void evaluate(const PairLists& pl, const void* lists, int kind
     } else {
         const float* L = static_cast<const float*>(lists);
         const Coef32* K = reinterpret_cast<const Coef32*>(kbuf);
-        if (kind == PASS_FP32_DIFF) {
-            stream32<0, OBJ_DIFF>(L + pl.start[0], pl.cnt[0], K, lane, ls);
-            stream32<1, OBJ_DIFF>(L + pl.start[1], pl.cnt[1], K, lane, ls);
-            stream32<2, OBJ_DIFF>(L + pl.start[2], pl.cnt[2], K, lane, ls);
-            stream32<3, OBJ_DIFF>(L + pl.start[3], pl.cnt[3], K, lane, ls);
-            stream32<4, OBJ_DIFF>(L + pl.start[4], pl.cnt[4], K, lane, ls);
-        } else {
-            stream32<0, OBJ_DIRECT>(L + pl.start[0], pl.cnt[0], K, lane, ls);
-            stream32<1, OBJ_DIRECT>(L + pl.start[1], pl.cnt[1], K, lane, ls);
-            stream32<2, OBJ_DIRECT>(L + pl.start[2], pl.cnt[2], K, lane, ls);
-            stream32<3, OBJ_DIRECT>(L + pl.start[3], pl.cnt[3], K, lane, ls);
-            stream32<4, OBJ_DIRECT>(L + pl.start[4], pl.cnt[4], K, lane, ls);
-        }
+        const bool diff = (kind == PASS_FP32_DIFF);
+        stream32<0>(L + pl.start[0], pl.cnt[0], K, diff, lane, ls);
+        stream32<1>(L + pl.start[1], pl.cnt[1], K, diff, lane, ls);
+        stream32<2>(L + pl.start[2], pl.cnt[2], K, diff, lane, ls);
+        stream32<3>(L + pl.start[3], pl.cnt[3], K, diff, lane, ls);
+        stream32<4>(L + pl.start[4], pl.cnt[4], K, diff, lane, ls);
     }
     for (int i = 0; i < NMOM; i++) {
         const double v = warp_sum(ls.m[i]);
