@@ -193,8 +193,9 @@ typedef struct {
     uint64_t flops_fp32;       /* executed FP32 site arithmetic (FMA = 2) */
     uint64_t flops_fp64;       /* executed FP64 site arithmetic */
     uint64_t shape_sites[5];   /* pair-sites per genotype-pair shape A,B1,B2,C,D */
-    uint64_t phase_cycles[4];  /* SM clocks summed over warps: shape count, list
-                                  build, site passes, 9x9 solver */
+    uint64_t phase_cycles[5];  /* SM clocks summed over warps: shape count, list
+                                  build, site passes, 9x9 solver, and the part of
+                                  the site passes inside the shape streams */
     double pair_kernel_ms;     /* CUDA-event time of the pair kernel */
     double device_ms;          /* CUDA-event time of preparation + pair kernel */
     double total_ms;           /* host time of the call */

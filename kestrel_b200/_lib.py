@@ -42,7 +42,7 @@ class KgRunStats(ctypes.Structure):
                 ("pair_sites", ctypes.c_uint64), ("work_units", ctypes.c_uint64),
                 ("launches", ctypes.c_uint64), ("flops_fp32", ctypes.c_uint64),
                 ("flops_fp64", ctypes.c_uint64), ("shape_sites", ctypes.c_uint64 * 5),
-                ("phase_cycles", ctypes.c_uint64 * 4),
+                ("phase_cycles", ctypes.c_uint64 * 5),
                 ("pair_kernel_ms", ctypes.c_double), ("device_ms", ctypes.c_double),
                 ("total_ms", ctypes.c_double)]
 

@@ -397,7 +397,7 @@ jacquard_pair_kernel(PairLaunch L) {
     unsigned long long c_gh = 0, c_obj = 0, c_f64 = 0, c_f64p = 0, c_sites = 0, c_work = 0,
                        c_nosite = 0, c_nonconv = 0, c_fl32 = 0, c_fl64 = 0;
     unsigned long long c_shape[5] = {0, 0, 0, 0, 0};
-    unsigned long long c_cyc[4] = {0, 0, 0, 0};
+    unsigned long long c_cyc[5] = {0, 0, 0, 0, 0};
     for (;;) {
         unsigned long long k = 0;
         if (lane == 0) k = atomicAdd(L.queue, 1ull);
@@ -443,6 +443,7 @@ jacquard_pair_kernel(PairLaunch L) {
             row.cond = res.cond;
             c_cyc[2] += res.cyc_pass;
             c_cyc[3] += res.cyc_solve;
+            c_cyc[4] += res.cyc_stream;
             c_gh += res.gh_passes;
             c_obj += res.obj_passes;
             c_f64 += res.fp64_passes;
@@ -480,7 +481,7 @@ jacquard_pair_kernel(PairLaunch L) {
         atomicAdd(&L.counters->flops_fp32, c_fl32);
         atomicAdd(&L.counters->flops_fp64, c_fl64);
         for (int s = 0; s < 5; s++) atomicAdd(&L.counters->shape_sites[s], c_shape[s]);
-        for (int s = 0; s < 4; s++) atomicAdd(&L.counters->cycles[s], c_cyc[s]);
+        for (int s = 0; s < 5; s++) atomicAdd(&L.counters->cycles[s], c_cyc[s]);
     }
 }
 
@@ -618,7 +619,7 @@ int run_pairs(const std::vector<PairJob>& jobs, const RunConfig& cfg, Workspace&
     stats.flops_fp32 = rc.flops_fp32;
     stats.flops_fp64 = rc.flops_fp64;
     for (int s = 0; s < 5; s++) stats.shape_sites[s] = rc.shape_sites[s];
-    for (int s = 0; s < 4; s++) stats.phase_cycles[s] = rc.cycles[s];
+    for (int s = 0; s < 5; s++) stats.phase_cycles[s] = rc.cycles[s];
     stats.pair_kernel_ms = ms;
     if (rc.nosite_pairs) {
         err = "a pair has no jointly observed segregating site (its row is NaN)";

@@ -77,7 +77,7 @@ struct RunCounters {
     unsigned long long flops_fp32;
     unsigned long long flops_fp64;
     unsigned long long shape_sites[5];
-    unsigned long long cycles[4];   // SM clocks per phase: count, scatter, site passes, solver
+    unsigned long long cycles[5];   // SM clocks per phase: count, scatter, site passes, solver, streams
 };
 
 struct PairLaunch {
@@ -700,7 +700,7 @@ __device__ inline void rebuild_row(const double* mom, int r, double& S, double* 
 // f = f_base - (sum log(d/d_base))/n with x_base the accepted point.
 __device__ inline void evaluate(const PairLists& pl, const void* lists, int kind, const double* x,
                                 const double* x_base, double f_base, int lane, char* wsm,
-                                PairEval& ev) {
+                                PairEval& ev, unsigned long long& cyc_stream) {
     void* kbuf = wsm + WARP_SMEM_BUF;
     double* mom_s = reinterpret_cast<double*>(wsm);   // NMOM + 1 totals (sort buffer is free)
     PassCoef k;
@@ -725,6 +725,7 @@ __device__ inline void evaluate(const PairLists& pl, const void* lists, int kind
     __syncwarp();
     LaneSums ls;
     ls.obj = 0.0;
+    const long long ts0 = clock64();
     if (kind == PASS_FP64) {
         const double* L = static_cast<const double*>(lists);
         const PassCoef* K = reinterpret_cast<const PassCoef*>(kbuf);
@@ -743,6 +744,7 @@ __device__ inline void evaluate(const PairLists& pl, const void* lists, int kind
         stream32<3>(L + pl.start[3], pl.cnt[3], K, diff, lane, ls);
         stream32<4>(L + pl.start[4], pl.cnt[4], K, diff, lane, ls);
     }
+    cyc_stream += clock64() - ts0;
     for (int i = 0; i < NMOM; i++) {
         const double v = warp_sum(ls.m[i]);
         if (lane == 0) mom_s[i] = v;
@@ -774,6 +776,7 @@ constexpr double DIFF_BELOW = 1e-4;    // |alpha g.p| under which the objective 
 
 struct PairResult {
     unsigned long long cyc_pass;    // clocks spent in site passes
+    unsigned long long cyc_stream;  // of which inside the shape streams
     unsigned long long cyc_solve;   // clocks spent in the 9x9 solver steps
     double x[9];
     double f;
@@ -824,9 +827,10 @@ __device__ inline void solve_pair(const CohortDev& co, int64_t px, int64_t py, c
     res.escalated = false;
     res.cyc_pass = 0;
     res.cyc_solve = 0;
+    res.cyc_stream = 0;
     PairEval ev;
     const long long t_0 = clock64();
-    evaluate(pl, lists, fp64 ? PASS_FP64 : PASS_FP32_DIRECT, x, x, 0.0, lane, wsm, ev);
+    evaluate(pl, lists, fp64 ? PASS_FP64 : PASS_FP32_DIRECT, x, x, 0.0, lane, wsm, ev, res.cyc_stream);
     res.cyc_pass += clock64() - t_0;
     res.obj_passes++;
     res.gh_passes++;
@@ -847,7 +851,7 @@ __device__ inline void solve_pair(const CohortDev& co, int64_t px, int64_t py, c
                 // FP64 re-evaluation at the same point; the pair stays FP64 from here.
                 scatter_shapes<double>(co, px, py, lane, pl, static_cast<double*>(lists), wsm);
                 const long long ta = clock64();
-                evaluate(pl, lists, PASS_FP64, x, x, f, lane, wsm, ev);
+                evaluate(pl, lists, PASS_FP64, x, x, f, lane, wsm, ev, res.cyc_stream);
                 res.cyc_pass += clock64() - ta;
                 res.fp64_passes++;
                 res.gh_passes++;
@@ -896,7 +900,7 @@ __device__ inline void solve_pair(const CohortDev& co, int64_t px, int64_t py, c
             const int kind = fp64 ? PASS_FP64
                                   : (fabs(alpha * gp) < DIFF_BELOW ? PASS_FP32_DIFF : PASS_FP32_DIRECT);
             const long long ta = clock64();
-            evaluate(pl, lists, kind, xn, x, f, lane, wsm, ev);
+            evaluate(pl, lists, kind, xn, x, f, lane, wsm, ev, res.cyc_stream);
             res.cyc_pass += clock64() - ta;
             res.obj_passes++;
             res.gh_passes++;
