@@ -177,6 +177,32 @@ int kg_cancel(kg_ctx *ctx, int64_t request_id);
 int kg_serving_stats(kg_ctx *ctx, int64_t *requests, int64_t *pairs,
                      int64_t *launches);
 
+/* ------------------------------------------------------ no allocation */
+
+/* This entry point has no counterpart in the reference.  It serves callers that
+ * cannot allocate device memory (an application that owns every byte through
+ * its own pool or reservation, or that must not call the CUDA allocator from
+ * this thread): it computes all pairs (x, y), 0 <= x <= y < n_samples, exactly
+ * as kg_relatedness does with default settings (FP32C, allele frequencies
+ * estimated, maf < 0 or NaN = 1/(2 n_samples)), but calls no cudaMalloc,
+ * cudaFree or allocating library routine.
+ *   d_codes: device pointer to the genotype codes (sample-major, row_stride
+ *            bytes per sample, 0/1/2, 3 = missing);
+ *   d_out:   device pointer to out_cap >= n_samples*(n_samples+1)/2 rows;
+ *   stream:  a cudaStream_t (NULL = the default stream); the call returns once
+ *            the rows are written.
+ * Limits: n_samples <= 512 and n_sites <= 32768; larger inputs return
+ * KG_ENOMEM.  Every intermediate lives in one 48 MiB file-scope __device__
+ * array that each GPU loading the library holds until the process exits.  Its
+ * device address is looked up on the first call on each device, so make that
+ * first call before any stream capture.  All calls share the array: calls that
+ * overlap on the GPU (other host threads, other streams) race and must be
+ * serialised by the caller. */
+int kg_relatedness_noalloc(const uint8_t *d_codes, int64_t n_samples,
+                           int64_t n_sites, int64_t row_stride,
+                           uint64_t iterations, double maf, kg_output *d_out,
+                           int64_t out_cap, void *stream);
+
 /* --------------------------------------------------------- diagnostics */
 
 /* Per-run counters of the last kg_relatedness / batch call: grad-Hessian and

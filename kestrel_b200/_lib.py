@@ -56,7 +56,8 @@ EXPORTS = ("kg_create", "kg_destroy", "kg_last_error", "kg_version", "kg_set_pre
            "kg_set_launch", "kg_autotune", "kg_load_genotypes", "kg_load_genotypes_2bit",
            "kg_set_allele_frequencies", "kg_relatedness", "kg_relatedness_coefficients",
            "kg_relatedness_batch", "kg_panel_load", "kg_submit", "kg_poll", "kg_wait",
-           "kg_cancel", "kg_serving_stats", "kg_last_run_stats", "kg_fp32_peak", "kg_run_cli")
+           "kg_cancel", "kg_serving_stats", "kg_relatedness_noalloc", "kg_last_run_stats",
+           "kg_fp32_peak", "kg_run_cli")
 
 
 class KestrelError(RuntimeError):
@@ -99,6 +100,7 @@ def lib():
         "kg_cancel": ([P, i64], i32),
         "kg_serving_stats": ([P, ctypes.POINTER(i64), ctypes.POINTER(i64), ctypes.POINTER(i64)], i32),
         "kg_last_run_stats": ([P, ctypes.POINTER(KgRunStats)], i32),
+        "kg_relatedness_noalloc": ([P, i64, i64, i64, u64, dbl, P, i64, P], i32),
         "kg_fp32_peak": ([i32, ctypes.POINTER(dbl)], i32),
         "kg_run_cli": ([i32, ctypes.POINTER(ctypes.c_char_p)], i32),
     }
