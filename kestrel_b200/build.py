@@ -19,9 +19,9 @@ LIB = os.path.join(HERE, "libkestrel_gpu.so")
 CLI = os.path.join(HERE, "bin", "kestrel")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-CUDA_SOURCES = ["kg_engine.cu", "kg_api.cu", "kg_noalloc.cu"]
+CUDA_SOURCES = ["kg_engine.cu", "kg_wave.cu", "kg_api.cu", "kg_noalloc.cu"]
 HOST_SOURCES = ["kg_cli.cpp"]
-HEADERS = ["kg_engine.h", "kg_pair.cuh", "kg_solver.cuh"]
+HEADERS = ["kg_engine.h", "kg_pair.cuh", "kg_solver.cuh", "kg_rowsolve.cuh", "kg_wave.cuh"]
 
 
 def nvcc() -> str:

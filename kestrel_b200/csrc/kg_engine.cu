@@ -555,77 +555,9 @@ int run_pairs(const std::vector<PairJob>& jobs, const RunConfig& cfg, Workspace&
         seg_cap = std::max<int64_t>(seg_cap, align4(pn.n_kept) + 32);
     }
     if (total_pairs == 0) return KG_OK;
-    int64_t blocks = (int64_t)ws.sm_count * bps;
-    int64_t warps = blocks * wpb;
-    int64_t need_warps = std::min<int64_t>(warps, total_pairs);
-    if (cfg.max_warps > 0) need_warps = std::min<int64_t>(need_warps, cfg.max_warps);
-    blocks = std::max<int64_t>(1, ceil_div(need_warps, wpb));
-    warps = blocks * wpb;
-    if (ws.warps < warps || ws.seg_cap < seg_cap) {
-        int64_t w = std::max(ws.warps, warps), s = std::max(ws.seg_cap, seg_cap);
-        KG_CUDA_TRY((cudaError_t)ws.scratch.reserve(sizeof(double) * w * s));
-        ws.warps = w;
-        ws.seg_cap = s;
-    }
-    KG_CUDA_TRY((cudaError_t)ws.queue.reserve(sizeof(unsigned long long)));
-    KG_CUDA_TRY((cudaError_t)ws.counters.reserve(sizeof(RunCounters)));
-    KG_CUDA_TRY((cudaError_t)ws.table.reserve(sizeof(CohortDev) * table.size()));
-    KG_CUDA_TRY(cudaMemcpyAsync(ws.table.p, table.data(), sizeof(CohortDev) * table.size(),
-                                cudaMemcpyHostToDevice, st));
-    KG_CUDA_TRY(cudaMemsetAsync(ws.queue.p, 0, sizeof(unsigned long long), st));
-    KG_CUDA_TRY(cudaMemsetAsync(ws.counters.p, 0, sizeof(RunCounters), st));
-    PairLaunch L;
-    L.cohorts = ws.table.as<CohortDev>();
-    L.n_cohorts = (int)table.size();
-    L.precision = cfg.precision;
-    L.total_pairs = total_pairs;
-    L.queue = ws.queue.as<unsigned long long>();
-    L.lists = ws.scratch.as<double>();
-    // stride from the workspace's capacity so warps never overlap
-    L.list_stride = ws.seg_cap;
-    L.tune = make_tune(cfg.iterations);
-    L.counters = ws.counters.as<RunCounters>();
-    cudaEvent_t e0, e1;
-    KG_CUDA_TRY(cudaEventCreate(&e0));
-    KG_CUDA_TRY(cudaEventCreate(&e1));
-    cudaEventRecord(e0, st);
-    jacquard_pair_kernel<<<(int)blocks, wpb * 32, smem, st>>>(L);
-    cudaError_t le = cudaGetLastError();
-    cudaEventRecord(e1, st);
-    if (le != cudaSuccess) {
-        cudaEventDestroy(e0);
-        cudaEventDestroy(e1);
-        err = std::string("pair kernel launch: ") + cudaGetErrorString(le);
-        return KG_ECUDA;
-    }
-    RunCounters rc;
-    cudaError_t ce = cudaMemcpyAsync(&rc, ws.counters.p, sizeof(rc), cudaMemcpyDeviceToHost, st);
-    if (ce == cudaSuccess) ce = cudaStreamSynchronize(st);
-    float ms = 0.f;
-    if (ce == cudaSuccess) cudaEventElapsedTime(&ms, e0, e1);
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
-    if (ce != cudaSuccess) {
-        err = std::string("pair kernel: ") + cudaGetErrorString(ce);
-        return KG_ECUDA;
-    }
-    stats.gh_passes = rc.gh_passes;
-    stats.obj_passes = rc.obj_passes;
-    stats.fp64_passes = rc.fp64_passes;
-    stats.fp64_pairs = rc.fp64_pairs;
-    stats.pair_sites = rc.pair_sites;
-    stats.work_units = rc.work_units;
-    stats.launches = 1;
-    stats.flops_fp32 = rc.flops_fp32;
-    stats.flops_fp64 = rc.flops_fp64;
-    for (int s = 0; s < 5; s++) stats.shape_sites[s] = rc.shape_sites[s];
-    for (int s = 0; s < 5; s++) stats.phase_cycles[s] = rc.cycles[s];
-    stats.pair_kernel_ms = ms;
-    if (rc.nosite_pairs) {
-        err = "a pair has no jointly observed segregating site (its row is NaN)";
-        return KG_ENOSITES;
-    }
-    return KG_OK;
+    (void)bps;
+    (void)smem;
+    return run_waves(jobs, cfg, ws, st, stats, err, table, total_pairs, seg_cap);
 }
 
 // FFMA throughput probe: 16 independent register chains per thread.
@@ -672,3 +604,4 @@ int fp32_peak(int device, double& tflops, std::string& err) {
 }
 
 }  // namespace kg
+

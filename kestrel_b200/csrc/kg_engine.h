@@ -96,11 +96,13 @@ struct RunConfig {
     int warps_per_block = 0;   // 0 = default
     int blocks_per_sm = 0;     // 0 = default
     int64_t max_warps = 0;     // 0 = no cap (cap the grid for small jobs)
+    int64_t max_slots = 0;     // pair slots per wave batch (0 = default 8192)
 };
 
 // Reusable device workspace of the pair kernel (scratch lists, queue, table).
 struct Workspace {
     DevBuf scratch, queue, counters, table;
+    DevBuf partial, slots, lists_a, lists_b, counts;   // wave state
     int64_t warps = 0;
     int64_t seg_cap = 0;       // list capacity per warp, in 8-byte words
     int sm_count = 0;
@@ -108,6 +110,12 @@ struct Workspace {
 
 int run_pairs(const std::vector<PairJob>& jobs, const RunConfig& cfg, Workspace& ws,
               cudaStream_t st, kg_run_stats& stats, std::string& err);
+
+struct CohortDev;
+// The wave loop (kg_wave.cu) over a prepared cohort table.
+int run_waves(const std::vector<PairJob>& jobs, const RunConfig& cfg, Workspace& ws, cudaStream_t st,
+              kg_run_stats& stats, std::string& err, const std::vector<CohortDev>& table,
+              int64_t total_pairs, int64_t list_cap);
 
 // Default launch shape for the device.
 void default_launch(int& warps_per_block, int& blocks_per_sm);

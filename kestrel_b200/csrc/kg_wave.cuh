@@ -1,0 +1,150 @@
+// kg_wave.cuh — the all-pairs estimator as waves over a batch of pair slots.
+//
+// A slot holds one pair's SQP state (src/sqp.rs:49-93) in HBM.  Each wave runs
+// three small kernels, so each has the SM to itself with compact code:
+//   admit : free slots take the next pairs from the device work queue (an atomic
+//           counter over all cohorts' pairs) and build their shape lists;
+//   pass  : a persistent kernel over work units (slot, shape, chunk of
+//           UNIT_ELEMS list entries) streams the lists at each slot's pending
+//           point and writes per-unit partial moments;
+//   solve : one warp per slot sums its units' partials in a fixed order, rebuilds
+//           f, g, H and advances the slot's SQP: KKT test, condition estimate,
+//           simplex QP, Armijo line search.  Converged slots write their output
+//           row and free the slot for the next admit.
+// A pair's result depends only on its own lists and the fixed reduction order,
+// never on which other pairs share its waves.
+#pragma once
+
+#include "kg_pair.cuh"
+
+namespace kg {
+
+constexpr int UNIT_ELEMS = 8192;   // list entries per pass work unit
+constexpr int UNIT_VALS = 14;      // partial values per unit: <= 13 moments + objective
+
+enum : int { SLOT_FREE = 0, SLOT_PASS = 1, SLOT_RESORT = 2 };
+enum : int { EV_INIT = 0, EV_TRIAL = 1, EV_REEVAL = 2 };
+
+struct SlotState {
+    int64_t k;            // global work index of the pair
+    int64_t x, y;
+    int64_t start[5], cnt[5], n;
+    int32_t ustart[6];    // prefix of work units over the five shapes
+    int32_t cohort;
+    int32_t status;       // SLOT_*
+    int32_t lists64;      // the lists hold FP64 values
+    int32_t fp64;         // passes run in FP64
+    int32_t kind;         // PASS_* of the pending pass
+    int32_t ev;           // EV_*: what the pending pass evaluates
+    int32_t near_count;
+    int32_t bls;
+    int32_t escalated;
+    int32_t gh, f64p, diffp;
+    uint64_t it;
+    double xc[9];         // accepted point
+    double f;             // objective at xc
+    double g[9];          // gradient at xc
+    double H[81];         // Hessian at xc
+    double p[9];          // search direction
+    double gp;            // g . p
+    double alpha;
+    double xt[9];         // point of the pending pass
+    Coef32 c32;           // its FP32 pass coefficients
+    PassCoef c64;         // its FP64 pass coefficients
+};
+
+struct WaveArgs {
+    const CohortDev* cohorts;
+    int n_cohorts;
+    int precision;
+    int64_t total_pairs;
+    unsigned long long* queue;
+    SlotState* slots;
+    int n_slots;
+    double* lists;                 // per slot: list_stride 8-byte words
+    int64_t list_stride;
+    double* partial;               // per slot: max_units * UNIT_VALS
+    int max_units;
+    const int* pass_list;          // slots with a pending pass (this wave)
+    const int* n_pass;
+    int* next_list;                // slots whose next pass the solve step scheduled
+    int* n_next;
+    int* n_resort;
+    unsigned long long* task;      // pass work-unit counter
+    Tune tune;
+    RunCounters* counters;
+};
+
+__device__ __forceinline__ int shape_ng(int s) { return s == 0 ? 4 : s == 3 ? 4 : s == 4 ? 2 : 3; }
+__device__ __forceinline__ int shape_nh(int s) { return s == 0 ? 7 : s == 3 ? 9 : s == 4 ? 3 : 5; }
+__device__ __forceinline__ int shape_goff(int s) { return s == 0 ? 0 : s == 1 ? 11 : s == 2 ? 19 : s == 3 ? 27 : 40; }
+
+// Coefficients of the pending pass at xt (relative to the accepted xc for the
+// log(d_new/d_old) objective).  Called by lane 0.
+__device__ inline void set_coefficients(SlotState& S, int kind) {
+    PassCoef k;
+    make_coef(S.xt, k);
+    S.c64 = k;
+    Coef32 c;
+    for (int i = 0; i < 4; i++) { c.a[i] = split(k.a[i]); c.c[i] = split(k.c[i]); }
+    for (int i = 0; i < 3; i++) { c.b1[i] = split(k.b1[i]); c.b2[i] = split(k.b2[i]); }
+    for (int i = 0; i < 2; i++) c.d[i] = split(k.d[i]);
+    double s[9];
+    for (int i = 0; i < 9; i++) s[i] = S.xt[i] - S.xc[i];
+    PassCoef ks;
+    make_coef(s, ks);
+    for (int i = 0; i < 4; i++) { c.sa[i] = (float)ks.a[i]; c.sc[i] = (float)ks.c[i]; }
+    for (int i = 0; i < 3; i++) { c.sb1[i] = (float)ks.b1[i]; c.sb2[i] = (float)ks.b2[i]; }
+    for (int i = 0; i < 2; i++) c.sd[i] = (float)ks.d[i];
+    S.c32 = c;
+    S.kind = kind;
+}
+
+__device__ inline void units_from_counts(SlotState& S) {
+    S.ustart[0] = 0;
+    for (int s = 0; s < 5; s++)
+        S.ustart[s + 1] = S.ustart[s] + (int)((S.cnt[s] + UNIT_ELEMS - 1) / UNIT_ELEMS);
+}
+
+__device__ __forceinline__ void decode_pair(const WaveArgs& A, int64_t k, int& c, int64_t& j,
+                                            int64_t& x, int64_t& y) {
+    c = 0;
+    while (c + 1 < A.n_cohorts && k >= A.cohorts[c + 1].pair_begin) c++;
+    const CohortDev& co = A.cohorts[c];
+    j = k - co.pair_begin;
+    if (co.kind == COHORT_TRIANGLE) {
+        double b = 2.0 * (double)co.n_x + 1.0;
+        double disc = b * b - 8.0 * (double)j;
+        int64_t xi = (int64_t)floor((b - sqrt(fmax(disc, 0.0))) * 0.5);
+        const int64_t ns = co.n_x;
+        if (xi < 0) xi = 0;
+        if (xi > ns - 1) xi = ns - 1;
+        auto off = [ns](int64_t r) { return r * ns - r * (r - 1) / 2; };
+        while (xi > 0 && off(xi) > j) xi--;
+        while (xi + 1 < ns && off(xi + 1) <= j) xi++;
+        x = xi;
+        y = xi + (j - off(xi));
+    } else {
+        x = j / co.n_y;
+        y = j - x * co.n_y;
+    }
+}
+
+__device__ inline void write_row(kg_output* out, int64_t x, int64_t y, const double* d, double obj,
+                                 uint64_t iters, double cond, int lane) {
+    kg_output row;
+    row.x = (uint64_t)x;
+    row.y = (uint64_t)y;
+    for (int i = 0; i < 9; i++) row.jacquard[i] = d[i];
+    row.obj = obj;
+    row.iters = iters;
+    row.cond = cond;
+    const uint64_t* src = reinterpret_cast<const uint64_t*>(&row);
+    uint64_t wv = 0;
+#pragma unroll
+    for (int i = 0; i < 14; i++)
+        if (lane == i) wv = src[i];
+    if (lane < 14) reinterpret_cast<uint64_t*>(out)[lane] = wv;
+}
+
+}  // namespace kg
