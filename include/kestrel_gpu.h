@@ -76,13 +76,15 @@ const char *kg_version(void);
 /* Arithmetic of the per-site sums (kg_precision). */
 int kg_set_precision(kg_ctx *ctx, int precision);
 
-/* Launch shape: warps per block and blocks per SM of the persistent pair
- * kernel (0 = autotuned choice).  Exposed for the autotuner and tests. */
-int kg_set_launch(kg_ctx *ctx, int warps_per_block, int blocks_per_sm);
+/* Launch shape of the pair engine: pairs in flight per wave (slots, 0 = up to
+ * 8192 as memory allows) and blocks per SM of the site-pass kernel (0 = the
+ * occupancy limit).  Exposed for the autotuner and tests; results do not
+ * depend on it. */
+int kg_set_launch(kg_ctx *ctx, int slots, int blocks_per_sm);
 
 /* Runs the autotuner on a sample of the loaded cohort and keeps the fastest
- * launch shape; writes it to *warps_per_block / *blocks_per_sm if non-NULL. */
-int kg_autotune(kg_ctx *ctx, int *warps_per_block, int *blocks_per_sm);
+ * launch shape; writes it to *slots / *blocks_per_sm if non-NULL. */
+int kg_autotune(kg_ctx *ctx, int *slots, int *blocks_per_sm);
 
 /* ---------------------------------------------------------------- cohort */
 
@@ -219,10 +221,12 @@ typedef struct {
     uint64_t flops_fp32;       /* executed FP32 site arithmetic (FMA = 2) */
     uint64_t flops_fp64;       /* executed FP64 site arithmetic */
     uint64_t shape_sites[5];   /* pair-sites per genotype-pair shape A,B1,B2,C,D */
-    uint64_t phase_cycles[5];  /* SM clocks summed over warps: shape count, list
-                                  build, site passes, 9x9 solver, and the part of
-                                  the site passes inside the shape streams */
-    double pair_kernel_ms;     /* CUDA-event time of the pair kernel */
+    uint64_t waves;            /* admit / pass / solve waves of the pair engine */
+    uint64_t slots;            /* pairs in flight per wave */
+    double admit_ms;           /* CUDA-event time of the admit kernels (list build) */
+    double pass_ms;            /* CUDA-event time of the site-pass kernels */
+    double solve_ms;           /* CUDA-event time of the solve kernels (SQP steps) */
+    double pair_kernel_ms;     /* CUDA-event time of all pair-engine waves */
     double device_ms;          /* CUDA-event time of preparation + pair kernel */
     double total_ms;           /* host time of the call */
 } kg_run_stats;

@@ -116,8 +116,9 @@ class Estimator:
         p = {"fp32c": KG_PREC_FP32C, "fp64": KG_PREC_FP64}[precision]
         _check(self._L.kg_set_precision(self._h, p), self._h)
 
-    def set_launch(self, warps_per_block: int = 0, blocks_per_sm: int = 0):
-        _check(self._L.kg_set_launch(self._h, warps_per_block, blocks_per_sm), self._h)
+    def set_launch(self, slots: int = 0, blocks_per_sm: int = 0):
+        """Pairs in flight per wave and site-pass blocks per SM (0 = automatic)."""
+        _check(self._L.kg_set_launch(self._h, slots, blocks_per_sm), self._h)
 
     def autotune(self):
         w, b = ctypes.c_int(), ctypes.c_int()
@@ -159,7 +160,6 @@ class Estimator:
         _check(self._L.kg_last_run_stats(self._h, ctypes.byref(s)), self._h)
         d = {f: getattr(s, f) for f, _ in KgRunStats._fields_}
         d["shape_sites"] = list(s.shape_sites)
-        d["phase_cycles"] = list(s.phase_cycles)
         return d
 
     def relatedness_batch(self, cohorts, iterations: int = 100, maf=None):

@@ -51,7 +51,8 @@ struct kg_ctx {
     int device = 0;
     size_t budget = 0;
     int precision = KG_PREC_FP32C;
-    int wpb = 0, bps = 0;
+    int64_t wave_slots = 0;
+    int pass_bps = 0;
     std::string err;
     cudaStream_t stream = nullptr;
     // single cohort
@@ -117,8 +118,8 @@ kg::RunConfig run_config(const kg_ctx* c, uint64_t iterations) {
     kg::RunConfig cfg;
     cfg.precision = c->precision;
     cfg.iterations = iterations;
-    cfg.warps_per_block = c->wpb;
-    cfg.blocks_per_sm = c->bps;
+    cfg.slots = c->wave_slots;
+    cfg.pass_blocks_per_sm = c->pass_bps;
     return cfg;
 }
 
@@ -164,7 +165,6 @@ void serve_batch(kg_ctx* c, Slot& slot, std::vector<std::shared_ptr<Request>>& b
         uint64_t it = 1;
         for (auto& r : batch) it = std::max<uint64_t>(it, r->iterations);
         cfg.iterations = it;
-        cfg.max_warps = total;
         st = kg::run_pairs(jobs, cfg, slot.ws, slot.stream, stats, err);
         if (st == KG_ENOSITES) st = KG_OK;  // per-pair NaN rows; reported on the rows
     }
@@ -323,11 +323,11 @@ int kg_set_precision(kg_ctx* c, int precision) {
     return KG_OK;
 }
 
-int kg_set_launch(kg_ctx* c, int warps_per_block, int blocks_per_sm) {
-    if (!c || warps_per_block < 0 || warps_per_block > 4 || blocks_per_sm < 0 || blocks_per_sm > 32)
-        return set_err(c, KG_EINVAL, "warps_per_block must be 0..4 and blocks_per_sm 0..32");
-    c->wpb = warps_per_block;
-    c->bps = blocks_per_sm;
+int kg_set_launch(kg_ctx* c, int slots, int blocks_per_sm) {
+    if (!c || slots < 0 || slots > (1 << 20) || blocks_per_sm < 0 || blocks_per_sm > 32)
+        return set_err(c, KG_EINVAL, "slots must be 0..2^20 and blocks_per_sm 0..32");
+    c->wave_slots = slots;
+    c->pass_bps = blocks_per_sm;
     return KG_OK;
 }
 
@@ -547,7 +547,7 @@ int kg_last_run_stats(kg_ctx* c, kg_run_stats* s) {
     return KG_OK;
 }
 
-int kg_autotune(kg_ctx* c, int* wpb_out, int* bps_out) {
+int kg_autotune(kg_ctx* c, int* slots_out, int* bps_out) {
     if (!c) return KG_EINVAL;
     if (!c->loaded) return set_err(c, KG_EINVAL, "load genotypes first");
     return guarded(c, [&]() -> int {
@@ -558,35 +558,34 @@ int kg_autotune(kg_ctx* c, int* wpb_out, int* bps_out) {
                                 c->cohort.n_sites, c->cohort.n_sites, true,
                                 c->af_set ? c->af.data() : nullptr, -1.0, c->stream, err);
         if (st) return set_err(c, st, err);
-        int sm = 0;
-        cudaDeviceGetAttribute(&sm, cudaDevAttrMultiProcessorCount, c->device);
-        // a sample triangle with enough pairs to fill every candidate grid twice
-        int64_t want = (int64_t)sm * 16 * 2;
+        // a sample triangle of about 4096 pairs
         int64_t ns = 2;
-        while (ns < c->cohort.n_samples && ns * (ns + 1) / 2 < want) ns++;
+        while (ns < c->cohort.n_samples && ns * (ns + 1) / 2 < 4096) ns++;
         int64_t np = ns * (ns + 1) / 2;
         if (c->dout.reserve(sizeof(kg_output) * np) != cudaSuccess)
             return set_err(c, KG_ENOMEM, "cannot allocate device output rows");
-        const int cand[][2] = {{4, 4}, {4, 3}, {2, 8}, {4, 2}, {1, 16}};
+        // the site-pass kernel's blocks per SM decide its latency hiding; the
+        // slot count only needs to cover the work (the default)
+        const int cand[] = {4, 3, 2};
         double best = 1e300;
-        int bw = 4, bb = 4;
-        for (auto& cd : cand) {
+        int bb = 0;
+        for (int cd : cand) {
             kg::PairJob jb;
             jb.panel = &c->cohort;
             jb.n_x = ns;
             jb.d_out = c->dout.as<kg_output>();
             kg::RunConfig cfg = run_config(c, 100);
-            cfg.warps_per_block = cd[0];
-            cfg.blocks_per_sm = cd[1];
+            cfg.slots = 0;
+            cfg.pass_blocks_per_sm = cd;
             kg_run_stats stt{};
             st = kg::run_pairs({jb}, cfg, c->ws, c->stream, stt, err);
             if (st && st != KG_ENOSITES) return set_err(c, st, err);
-            double cost = stt.pair_kernel_ms / std::max<double>(1.0, (double)stt.work_units);
-            if (cost < best) { best = cost; bw = cd[0]; bb = cd[1]; }
+            double cost = stt.pass_ms / std::max<double>(1.0, (double)stt.work_units);
+            if (cost < best) { best = cost; bb = cd; }
         }
-        c->wpb = bw;
-        c->bps = bb;
-        if (wpb_out) *wpb_out = bw;
+        c->wave_slots = 0;
+        c->pass_bps = bb;
+        if (slots_out) *slots_out = 0;
         if (bps_out) *bps_out = bb;
         return KG_OK;
     });

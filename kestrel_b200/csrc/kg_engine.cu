@@ -487,15 +487,6 @@ jacquard_pair_kernel(PairLaunch L) {
 
 static_assert(sizeof(kg_output) == 14 * 8, "kg_output must be 112 bytes");
 
-void default_launch(int& warps_per_block, int& blocks_per_sm) {
-    warps_per_block = 4;
-    blocks_per_sm = 4;
-}
-
-size_t scratch_bytes_per_warp(int64_t n_kept) {
-    return sizeof(double) * (size_t)(align4(n_kept) + 32);
-}
-
 int run_pairs(const std::vector<PairJob>& jobs, const RunConfig& cfg, Workspace& ws,
               cudaStream_t st, kg_run_stats& stats, std::string& err) {
     std::memset(&stats, 0, sizeof(stats));
@@ -503,32 +494,6 @@ int run_pairs(const std::vector<PairJob>& jobs, const RunConfig& cfg, Workspace&
     int dev = 0;
     KG_CUDA_TRY(cudaGetDevice(&dev));
     if (ws.sm_count == 0) KG_CUDA_TRY(cudaDeviceGetAttribute(&ws.sm_count, cudaDevAttrMultiProcessorCount, dev));
-    int wpb = cfg.warps_per_block, bps = cfg.blocks_per_sm;
-    {
-        int dw, db;
-        default_launch(dw, db);
-        if (wpb <= 0) wpb = dw;
-        if (bps <= 0) bps = db;
-    }
-    wpb = std::min(std::max(wpb, 1), 4);
-    const size_t smem = (size_t)wpb * WARP_SMEM;
-    {
-        static bool attr_set = false;
-        if (!attr_set) {
-            KG_CUDA_TRY(cudaFuncSetAttribute(jacquard_pair_kernel,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             4 * WARP_SMEM));
-            attr_set = true;
-        }
-        int occ = 0;
-        KG_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, jacquard_pair_kernel,
-                                                                  wpb * 32, smem));
-        if (occ <= 0) {
-            err = "pair kernel cannot be resident with this launch shape";
-            return KG_ECUDA;
-        }
-        bps = std::min(bps, occ);
-    }
     int64_t total_pairs = 0;
     int64_t seg_cap = 1;
     std::vector<CohortDev> table(jobs.size());
@@ -555,8 +520,6 @@ int run_pairs(const std::vector<PairJob>& jobs, const RunConfig& cfg, Workspace&
         seg_cap = std::max<int64_t>(seg_cap, align4(pn.n_kept) + 32);
     }
     if (total_pairs == 0) return KG_OK;
-    (void)bps;
-    (void)smem;
     return run_waves(jobs, cfg, ws, st, stats, err, table, total_pairs, seg_cap);
 }
 

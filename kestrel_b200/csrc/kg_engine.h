@@ -93,18 +93,15 @@ struct PairJob {
 struct RunConfig {
     int precision = KG_PREC_FP32C;
     uint64_t iterations = 100;
-    int warps_per_block = 0;   // 0 = default
-    int blocks_per_sm = 0;     // 0 = default
-    int64_t max_warps = 0;     // 0 = no cap (cap the grid for small jobs)
-    int64_t max_slots = 0;     // pair slots per wave batch (0 = default 8192)
+    int64_t slots = 0;         // pairs in flight per wave (0 = up to 8192 as memory allows)
+    int pass_blocks_per_sm = 0;   // site-pass kernel blocks per SM (0 = occupancy limit)
 };
 
-// Reusable device workspace of the pair kernel (scratch lists, queue, table).
+// Reusable device workspace of the pair engine (per-slot lists and partial
+// sums, slot states, pass lists, queue, counters, cohort table).
 struct Workspace {
     DevBuf scratch, queue, counters, table;
-    DevBuf partial, slots, lists_a, lists_b, counts;   // wave state
-    int64_t warps = 0;
-    int64_t seg_cap = 0;       // list capacity per warp, in 8-byte words
+    DevBuf partial, slots, lists_a, lists_b, counts;
     int sm_count = 0;
 };
 
@@ -117,11 +114,6 @@ int run_waves(const std::vector<PairJob>& jobs, const RunConfig& cfg, Workspace&
               kg_run_stats& stats, std::string& err, const std::vector<CohortDev>& table,
               int64_t total_pairs, int64_t list_cap);
 
-// Default launch shape for the device.
-void default_launch(int& warps_per_block, int& blocks_per_sm);
-
-// Bytes of list scratch per warp for n_kept sites.
-size_t scratch_bytes_per_warp(int64_t n_kept);
 
 const char* engine_version();
 

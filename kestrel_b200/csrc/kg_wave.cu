@@ -374,7 +374,7 @@ int run_waves(const std::vector<PairJob>& jobs, const RunConfig& cfg, Workspace&
                             sizeof(SlotState) + 2 * sizeof(int);
     size_t fr = 0, tot = 0;
     KG_WAVE_TRY(cudaMemGetInfo(&fr, &tot));
-    int64_t want = cfg.max_slots > 0 ? cfg.max_slots : 8192;
+    int64_t want = cfg.slots > 0 ? cfg.slots : 8192;
     int64_t by_mem = (int64_t)((fr / 2) / per_slot);
     int64_t n_slots = std::max<int64_t>(1, std::min<int64_t>({want, by_mem, total_pairs}));
     // device buffers (grown and reused through the workspace)
@@ -400,7 +400,12 @@ int run_waves(const std::vector<PairJob>& jobs, const RunConfig& cfg, Workspace&
     }
     int occ = 0;
     KG_WAVE_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, wave_pass_kernel, 128, 4 * WARP_SMEM));
-    const int pass_blocks = ws.sm_count * std::max(1, occ);
+    if (occ <= 0) {
+        err = "site-pass kernel cannot be resident";
+        return KG_ECUDA;
+    }
+    if (cfg.pass_blocks_per_sm > 0) occ = std::min(occ, cfg.pass_blocks_per_sm);
+    const int pass_blocks = ws.sm_count * occ;
     int* counts = ws.counts.as<int>();   // [0] n_a, [1] n_b, [2] n_resort
     unsigned long long* q = ws.queue.as<unsigned long long>();   // [0] pairs, [1] pass units
     WaveArgs A;
@@ -423,23 +428,28 @@ int run_waves(const std::vector<PairJob>& jobs, const RunConfig& cfg, Workspace&
     int cur = 0;
     const int slot_blocks = (int)((n_slots + WAVE_WPB - 1) / WAVE_WPB);
     const size_t wsm = WAVE_WPB * WARP_SMEM;
-    cudaEvent_t e0, e1;
-    KG_WAVE_TRY(cudaEventCreate(&e0));
-    KG_WAVE_TRY(cudaEventCreate(&e1));
-    cudaEventRecord(e0, st);
+    // events: [0] start, then per wave admit / pass / solve ends
+    cudaEvent_t ev[4];
+    for (auto& e : ev) KG_WAVE_TRY(cudaEventCreate(&e));
+    struct EvGuard { cudaEvent_t* e; ~EvGuard() { for (int i = 0; i < 4; i++) cudaEventDestroy(e[i]); } } eg{ev};
     uint64_t waves = 0, launches = 0;
+    double phase[3] = {0.0, 0.0, 0.0}, total = 0.0;
     for (;;) {
         A.pass_list = lst[cur];
         A.n_pass = counts + cur;
         A.next_list = lst[cur ^ 1];
         A.n_next = counts + (cur ^ 1);
+        KG_WAVE_TRY(cudaEventRecord(ev[0], st));
         wave_admit_kernel<<<slot_blocks, 128, wsm, st>>>(A, lst[cur], counts + cur);
         KG_WAVE_TRY(cudaMemsetAsync(q + 1, 0, sizeof(unsigned long long), st));
+        KG_WAVE_TRY(cudaEventRecord(ev[1], st));
         wave_pass_kernel<<<pass_blocks, 128, wsm, st>>>(A);
+        KG_WAVE_TRY(cudaEventRecord(ev[2], st));
         KG_WAVE_TRY(cudaMemsetAsync(counts + (cur ^ 1), 0, sizeof(int), st));
         KG_WAVE_TRY(cudaMemsetAsync(counts + 2, 0, sizeof(int), st));
         wave_solve_kernel<<<slot_blocks, 128, wsm, st>>>(A);
         KG_WAVE_TRY(cudaGetLastError());
+        KG_WAVE_TRY(cudaEventRecord(ev[3], st));
         launches += 3;
         waves++;
         int h[3];
@@ -447,17 +457,18 @@ int run_waves(const std::vector<PairJob>& jobs, const RunConfig& cfg, Workspace&
         KG_WAVE_TRY(cudaMemcpyAsync(h, counts, sizeof(h), cudaMemcpyDeviceToHost, st));
         KG_WAVE_TRY(cudaMemcpyAsync(&hq, q, sizeof(hq), cudaMemcpyDeviceToHost, st));
         KG_WAVE_TRY(cudaStreamSynchronize(st));
+        for (int i = 0; i < 3; i++) {
+            float ms = 0.f;
+            KG_WAVE_TRY(cudaEventElapsedTime(&ms, ev[i], ev[i + 1]));
+            phase[i] += ms;
+            total += ms;
+        }
         cur ^= 1;
         if (h[cur] == 0 && h[2] == 0 && hq >= (unsigned long long)total_pairs) break;
     }
-    cudaEventRecord(e1, st);
     RunCounters rc;
     KG_WAVE_TRY(cudaMemcpyAsync(&rc, ws.counters.p, sizeof(rc), cudaMemcpyDeviceToHost, st));
     KG_WAVE_TRY(cudaStreamSynchronize(st));
-    float ms = 0.f;
-    cudaEventElapsedTime(&ms, e0, e1);
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
     stats.gh_passes = rc.gh_passes;
     stats.obj_passes = rc.obj_passes;
     stats.fp64_passes = rc.fp64_passes;
@@ -468,9 +479,12 @@ int run_waves(const std::vector<PairJob>& jobs, const RunConfig& cfg, Workspace&
     stats.flops_fp32 = rc.flops_fp32;
     stats.flops_fp64 = rc.flops_fp64;
     for (int k = 0; k < 5; k++) stats.shape_sites[k] = rc.shape_sites[k];
-    stats.phase_cycles[0] = waves;
-    stats.phase_cycles[1] = (uint64_t)n_slots;
-    stats.pair_kernel_ms = ms;
+    stats.waves = waves;
+    stats.slots = (uint64_t)n_slots;
+    stats.admit_ms = phase[0];
+    stats.pass_ms = phase[1];
+    stats.solve_ms = phase[2];
+    stats.pair_kernel_ms = total;
     if (rc.nosite_pairs) {
         err = "a pair has no jointly observed segregating site (its row is NaN)";
         return KG_ENOSITES;
