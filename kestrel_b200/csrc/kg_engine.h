@@ -101,7 +101,7 @@ struct RunConfig {
 // sums, slot states, pass lists, queue, counters, cohort table).
 struct Workspace {
     DevBuf scratch, queue, counters, table;
-    DevBuf partial, slots, lists_a, lists_b, counts;
+    DevBuf partial, slots, lists_a, lists_b, tasks, counts;
     int sm_count = 0;
 };
 

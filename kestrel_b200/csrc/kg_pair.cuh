@@ -277,17 +277,19 @@ __device__ inline void count_shapes(const CohortDev& co, int64_t x, int64_t y, i
 // conflict-free); t is p or 1 - p by the site's sel bit.  FP32 values go through
 // a shared output buffer so the global stores stay coalesced; FP64 values (the
 // FP64 form and re-evaluated pairs) are stored directly.
+// scatter_units covers units [u0, u1) with the shapes' write positions starting
+// at off[]; scatter_shapes is the whole pair.
 template <class T>
-__device__ inline void scatter_shapes(const CohortDev& co, int64_t x, int64_t y, int lane,
-                                      const PairLists& pl, T* lists, char* wsm) {
+__device__ inline void scatter_units(const CohortDev& co, int64_t x, int64_t y, int lane, int u0,
+                                     int u1, const int64_t* off0, T* lists, char* wsm) {
     const uint2* px = co.planes_x + x * co.plane_stride;
     const uint2* py = co.planes_y + y * co.plane_stride;
     T* stage = reinterpret_cast<T*>(wsm);                       // UNIT_SITES values
     float* obuf = reinterpret_cast<float*>(wsm + UNIT_SITES * sizeof(float));  // FP32 only
     int64_t off[5];
 #pragma unroll
-    for (int s = 0; s < 5; s++) off[s] = pl.start[s];
-    for (int u = 0; u < co.n_units; u++) {
+    for (int s = 0; s < 5; s++) off[s] = off0[s];
+    for (int u = u0; u < u1; u++) {
         const int w = u * UNIT_WORDS + lane;
         const uint2 X = px[w], Y = py[w];
         // stage this lane's 32 REF frequencies: site 32 lane + i at [i * 32 + lane]
@@ -353,6 +355,12 @@ __device__ inline void scatter_shapes(const CohortDev& co, int64_t x, int64_t y,
 #pragma unroll
         for (int s = 0; s < 5; s++) off[s] += ustart[s + 1] - ustart[s];
     }
+}
+
+template <class T>
+__device__ inline void scatter_shapes(const CohortDev& co, int64_t x, int64_t y, int lane,
+                                      const PairLists& pl, T* lists, char* wsm) {
+    scatter_units<T>(co, x, y, lane, 0, co.n_units, pl.start, lists, wsm);
 }
 
 // ----------------------------------------------------------- FP32 passes

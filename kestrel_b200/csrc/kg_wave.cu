@@ -21,82 +21,139 @@ constexpr int WAVE_WPB = 4;   // warps per block of the three wave kernels
 
 // ------------------------------------------------------------------ admit
 
-extern "C" __global__ void __launch_bounds__(128) wave_admit_kernel(WaveArgs A, int* pass_list,
-                                                                     int* n_pass) {
-    extern __shared__ __align__(16) char smem[];
-    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-    const int s = blockIdx.x * WAVE_WPB + wib;
-    if (s >= A.n_slots) return;
-    char* wsm = smem + wib * WARP_SMEM;
-    SlotState& S = A.slots[s];
-    void* lists = A.lists + (int64_t)s * A.list_stride;
-    const int status = S.status;
-    if (status == SLOT_RESORT) {
-        PairLists pl;
-        for (int i = 0; i < 5; i++) { pl.start[i] = S.start[i]; pl.cnt[i] = S.cnt[i]; }
-        pl.n = S.n;
-        scatter_shapes<double>(A.cohorts[S.cohort], S.x, S.y, lane, pl, static_cast<double*>(lists), wsm);
-        __syncwarp();
-        if (lane == 0) {
-            S.lists64 = 1;
-            S.status = SLOT_PASS;
-            pass_list[atomicAdd(n_pass, 1)] = s;
+constexpr int ADMIT_WARPS = 8;   // warps that build one pair's lists together
+
+// Each warp of the block takes a contiguous eighth of the pair's 1024-site
+// units: it counts its sites per shape, the block turns the counts into write
+// offsets (so the lists stay in site order), and each warp scatters its units.
+template <class T>
+__device__ inline int64_t build_lists(const CohortDev& co, int64_t x, int64_t y, T* lists, char* wsm,
+                                      unsigned (*cnt)[5], int64_t* start, int64_t* count) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int u0 = (int)((int64_t)co.n_units * w / ADMIT_WARPS);
+    const int u1 = (int)((int64_t)co.n_units * (w + 1) / ADMIT_WARPS);
+    {
+        const uint2* px = co.planes_x + x * co.plane_stride;
+        const uint2* py = co.planes_y + y * co.plane_stride;
+        unsigned c[5] = {0, 0, 0, 0, 0};
+        for (int wd = u0 * UNIT_WORDS + lane; wd < u1 * UNIT_WORDS; wd += 32) {
+            ShapeMasks sm = shape_masks(px[wd], py[wd]);
+#pragma unroll
+            for (int k = 0; k < 5; k++) c[k] += __popc(sm.m[k]);
         }
-        return;
+#pragma unroll
+        for (int k = 0; k < 5; k++) {
+            unsigned v = c[k];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+            if (lane == 0) cnt[w][k] = v;
+        }
     }
-    if (status != SLOT_FREE) return;
+    __syncthreads();
+    int64_t off[5], st = 0, n = 0;
+#pragma unroll
+    for (int k = 0; k < 5; k++) {
+        int64_t tot = 0, before = 0;
+        for (int v = 0; v < ADMIT_WARPS; v++) {
+            if (v < w) before += cnt[v][k];
+            tot += cnt[v][k];
+        }
+        start[k] = st;
+        count[k] = tot;
+        off[k] = st + before;
+        st = align4(st + tot);
+        n += tot;
+    }
+    if (n > 0) scatter_units<T>(co, x, y, lane, u0, u1, off, lists, wsm);
+    __syncthreads();   // cnt is reused by the block's next pair
+    return n;
+}
+
+extern "C" __global__ void __launch_bounds__(ADMIT_WARPS * 32) wave_admit_kernel(WaveArgs A) {
+    extern __shared__ __align__(16) char smem[];
+    __shared__ int sh_e;
+    __shared__ unsigned long long sh_k;
+    __shared__ unsigned cnt[ADMIT_WARPS][5];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    char* wsm = smem + w * WARP_SMEM;
+    const int nfree = A.wc_cur->n_free;
     for (;;) {
-        unsigned long long k = 0;
-        if (lane == 0) k = atomicAdd(A.queue, 1ull);
-        k = __shfl_sync(0xffffffffu, k, 0);
-        if (k >= (unsigned long long)A.total_pairs) return;
-        int c;
-        int64_t j, x, y;
-        decode_pair(A, (int64_t)k, c, j, x, y);
-        const CohortDev& co = A.cohorts[c];
-        PairLists pl;
-        count_shapes(co, x, y, lane, pl);
-        if (pl.n == 0) {
-            double nan9[9];
-            for (int i = 0; i < 9; i++) nan9[i] = CUDART_NAN;
-            write_row(co.out + j, x, y, nan9, CUDART_NAN, 0, CUDART_NAN, lane);
-            if (lane == 0) atomicAdd(&A.counters->nosite_pairs, 1ull);
+        if (threadIdx.x == 0) sh_e = atomicAdd(A.admit_task, 1);
+        __syncthreads();
+        const int e = sh_e;
+        __syncthreads();
+        if (e >= nfree) return;
+        const int s = A.free_cur[e];
+        SlotState& S = A.slots[s];
+        void* lists = A.lists + (int64_t)s * A.list_stride;
+        int64_t start[5], count[5];
+        if (S.status == SLOT_RESORT) {
+            // an escalated pair: the same lists again, in FP64
+            build_lists<double>(A.cohorts[S.cohort], S.x, S.y, static_cast<double*>(lists), wsm, cnt, start,
+                                count);
+            if (threadIdx.x == 0) {
+                S.lists64 = 1;
+                S.status = SLOT_PASS;
+            }
+            __syncthreads();
+            if (w == 0) enqueue_pass(A.pass_cur, A.tasks_cur, A.task_cap, A.wc_cur, s, S, lane);
             continue;
         }
-        const bool f64 = (A.precision == 1);
-        if (f64) scatter_shapes<double>(co, x, y, lane, pl, static_cast<double*>(lists), wsm);
-        else scatter_shapes<float>(co, x, y, lane, pl, static_cast<float*>(lists), wsm);
-        __syncwarp();
-        if (lane == 0) {
-            S.k = (int64_t)k;
-            S.x = x;
-            S.y = y;
-            S.cohort = c;
-            for (int i = 0; i < 5; i++) { S.start[i] = pl.start[i]; S.cnt[i] = pl.cnt[i]; }
-            S.n = pl.n;
-            units_from_counts(S);
-            S.lists64 = f64 ? 1 : 0;
-            S.fp64 = f64 ? 1 : 0;
-            S.near_count = 0;
-            S.bls = 0;
-            S.escalated = 0;
-            S.gh = 0;
-            S.f64p = 0;
-            S.diffp = 0;
-            S.it = 0;
-            const bool self_pair = (co.kind == COHORT_TRIANGLE) && (x == y);
-            double x0[9];
-            for (int i = 0; i < 9; i++) x0[i] = self_pair ? 0.0 : 1.0 / 9.0;
-            if (self_pair) { x0[0] = 0.5; x0[6] = 0.5; }
-            normalise9(x0);
-            for (int i = 0; i < 9; i++) { S.xc[i] = x0[i]; S.xt[i] = x0[i]; }
-            S.f = 0.0;
-            S.ev = EV_INIT;
-            set_coefficients(S, f64 ? PASS_FP64 : PASS_FP32_DIRECT);
-            S.status = SLOT_PASS;
-            pass_list[atomicAdd(n_pass, 1)] = s;
+        // a free slot takes pairs until one has jointly observed sites
+        for (;;) {
+            if (threadIdx.x == 0) sh_k = atomicAdd(A.queue, 1ull);
+            __syncthreads();
+            const unsigned long long k = sh_k;
+            __syncthreads();
+            if (k >= (unsigned long long)A.total_pairs) break;
+            int c;
+            int64_t j, x, y;
+            decode_pair(A, (int64_t)k, c, j, x, y);
+            const CohortDev& co = A.cohorts[c];
+            const bool f64 = (A.precision == 1);
+            const int64_t n = f64 ? build_lists<double>(co, x, y, static_cast<double*>(lists), wsm, cnt, start, count)
+                                  : build_lists<float>(co, x, y, static_cast<float*>(lists), wsm, cnt, start, count);
+            if (n == 0) {
+                if (w == 0) {
+                    double nan9[9];
+                    for (int i = 0; i < 9; i++) nan9[i] = CUDART_NAN;
+                    write_row(co.out + j, x, y, nan9, CUDART_NAN, 0, CUDART_NAN, lane);
+                    if (lane == 0) atomicAdd(&A.counters->nosite_pairs, 1ull);
+                }
+                continue;
+            }
+            if (threadIdx.x == 0) {
+                S.k = (int64_t)k;
+                S.x = x;
+                S.y = y;
+                S.cohort = c;
+                for (int i = 0; i < 5; i++) { S.start[i] = start[i]; S.cnt[i] = count[i]; }
+                S.n = n;
+                units_from_counts(S);
+                S.lists64 = f64 ? 1 : 0;
+                S.fp64 = f64 ? 1 : 0;
+                S.near_count = 0;
+                S.bls = 0;
+                S.escalated = 0;
+                S.gh = 0;
+                S.f64p = 0;
+                S.diffp = 0;
+                S.it = 0;
+                const bool self_pair = (co.kind == COHORT_TRIANGLE) && (x == y);
+                double x0[9];
+                for (int i = 0; i < 9; i++) x0[i] = self_pair ? 0.0 : 1.0 / 9.0;
+                if (self_pair) { x0[0] = 0.5; x0[6] = 0.5; }
+                normalise9(x0);
+                for (int i = 0; i < 9; i++) { S.xc[i] = x0[i]; S.xt[i] = x0[i]; }
+                S.f = 0.0;
+                S.ev = EV_INIT;
+                set_coefficients(S, f64 ? PASS_FP64 : PASS_FP32_DIRECT);
+                S.status = SLOT_PASS;
+            }
+            __syncthreads();
+            if (w == 0) enqueue_pass(A.pass_cur, A.tasks_cur, A.task_cap, A.wc_cur, s, S, lane);
+            break;
         }
-        return;
     }
 }
 
@@ -118,19 +175,22 @@ extern "C" __global__ void __launch_bounds__(128, 4) wave_pass_kernel(WaveArgs A
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     char* wsm = smem + wib * WARP_SMEM;
     char* kbuf = wsm + WARP_SMEM_BUF;
-    const int np = *A.n_pass;
-    const int64_t ntask = (int64_t)np * A.max_units;
+    int pre[6];
+    pre[0] = 0;
+#pragma unroll
+    for (int k = 0; k < 5; k++) pre[k + 1] = pre[k] + A.wc_cur->units[k];
+    const int64_t ntask = pre[5];
     for (;;) {
         unsigned long long t = 0;
-        if (lane == 0) t = atomicAdd(A.task, 1ull);
+        if (lane == 0) t = atomicAdd(A.pass_task, 1ull);
         t = __shfl_sync(0xffffffffu, t, 0);
         if ((int64_t)t >= ntask) break;
-        const int s = A.pass_list[t / A.max_units];
-        const int u = (int)(t % A.max_units);
-        const SlotState& S = A.slots[s];
-        if (u >= S.ustart[5]) continue;
         int sh = 0;
-        while (u >= S.ustart[sh + 1]) sh++;
+        while ((int)t >= pre[sh + 1]) sh++;
+        const int2 tk = A.tasks_cur[sh * A.task_cap + ((int)t - pre[sh])];
+        const int s = tk.x;
+        const int u = tk.y;
+        const SlotState& S = A.slots[s];
         const int64_t c0 = (int64_t)(u - S.ustart[sh]) * UNIT_ELEMS;
         const int64_t off = S.start[sh] + c0;
         const int64_t len = min((int64_t)UNIT_ELEMS, S.cnt[sh] - c0);
@@ -167,7 +227,7 @@ extern "C" __global__ void __launch_bounds__(128, 4) wave_pass_kernel(WaveArgs A
 
 // ------------------------------------------------------------------ solve
 
-__device__ inline void finish_slot(const WaveArgs& A, SlotState& S, const double* x, double f,
+__device__ inline void finish_slot(const WaveArgs& A, SlotState& S, int s, const double* x, double f,
                                    uint64_t iters, double cond, int lane) {
     const CohortDev& co = A.cohorts[S.cohort];
     const int64_t j = S.k - co.pair_begin;
@@ -183,38 +243,44 @@ __device__ inline void finish_slot(const WaveArgs& A, SlotState& S, const double
         if (iters >= A.tune.sqp_max_iter) atomicAdd(&C->nonconverged, 1ull);
         const int p32 = S.gh - S.f64p;
         unsigned long long f32 = 0, f64 = 0;
-        for (int s = 0; s < 5; s++) {
-            atomicAdd(&C->shape_sites[s], (unsigned long long)S.cnt[s]);
-            f32 += (unsigned long long)S.cnt[s] * (unsigned long long)(p32 * flops_direct(s) + S.diffp * flops_diff_extra(s));
-            f64 += (unsigned long long)S.cnt[s] * (unsigned long long)(S.f64p * flops_direct(s));
+        for (int sh = 0; sh < 5; sh++) {
+            atomicAdd(&C->shape_sites[sh], (unsigned long long)S.cnt[sh]);
+            f32 += (unsigned long long)S.cnt[sh] * (unsigned long long)(p32 * flops_direct(sh) + S.diffp * flops_diff_extra(sh));
+            f64 += (unsigned long long)S.cnt[sh] * (unsigned long long)(S.f64p * flops_direct(sh));
         }
         atomicAdd(&C->flops_fp32, f32);
         atomicAdd(&C->flops_fp64, f64);
         S.status = SLOT_FREE;
+        A.free_next[atomicAdd(&A.wc_next->n_free, 1)] = s;
     }
 }
 
-// Schedules the slot's next pass at S.xt (lane 0 has written xt).
+// Schedules the slot's next pass at S.xt (lane 0 has written xt).  A pass in
+// FP64 on FP32 lists first goes back through the admit step for FP64 lists.
 __device__ inline void schedule_pass(const WaveArgs& A, SlotState& S, int s, int kind, int ev, int lane) {
     if (lane == 0) {
         S.ev = ev;
         set_coefficients(S, kind);
-        if (kind == PASS_FP64 && !S.lists64) {
-            S.status = SLOT_RESORT;
-            atomicAdd(A.n_resort, 1);
-        } else {
-            S.status = SLOT_PASS;
-            A.next_list[atomicAdd(A.n_next, 1)] = s;
-        }
     }
+    if (kind == PASS_FP64 && !S.lists64) {
+        if (lane == 0) {
+            S.status = SLOT_RESORT;
+            A.free_next[atomicAdd(&A.wc_next->n_free, 1)] = s;
+            atomicAdd(&A.wc_next->n_resort, 1);
+        }
+        return;
+    }
+    if (lane == 0) S.status = SLOT_PASS;
+    __syncwarp();
+    enqueue_pass(A.pass_next, A.tasks_next, A.task_cap, A.wc_next, s, S, lane);
 }
 
 extern "C" __global__ void __launch_bounds__(128) wave_solve_kernel(WaveArgs A) {
     extern __shared__ __align__(16) char smem[];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const int i = blockIdx.x * WAVE_WPB + wib;
-    if (i >= *A.n_pass) return;
-    const int s = A.pass_list[i];
+    if (i >= A.wc_cur->n_pass) return;
+    const int s = A.pass_cur[i];
     SlotState& S = A.slots[s];
     char* wsm = smem + wib * WARP_SMEM;
     double* mom_s = reinterpret_cast<double*>(wsm);
@@ -310,7 +376,7 @@ extern "C" __global__ void __launch_bounds__(128) wave_solve_kernel(WaveArgs A) 
         for (int k = 0; k < 9; k++) S.H[lane * 9 + k] = Hr[k];
     }
     if (it >= tu.sqp_max_iter) {
-        finish_slot(A, S, x, f, tu.sqp_max_iter, CUDART_NAN, lane);
+        finish_slot(A, S, s, x, f, tu.sqp_max_iter, CUDART_NAN, lane);
         return;
     }
     // ---- KKT test (src/sqp.rs:95-109) and the FP32 -> FP64 recheck
@@ -329,12 +395,12 @@ extern "C" __global__ void __launch_bounds__(128) wave_solve_kernel(WaveArgs A) 
             return;
         }
         if (conv) {
-            finish_slot(A, S, x, f, it, cond, lane);
+            finish_slot(A, S, s, x, f, it, cond, lane);
             return;
         }
     }
     if (conv) {
-        finish_slot(A, S, x, f, it, condition_rows(x, g, Hr, tu.sqp_conv_tol), lane);
+        finish_slot(A, S, s, x, f, it, condition_rows(x, g, Hr, tu.sqp_conv_tol), lane);
         return;
     }
     // ---- QP step (src/sqp.rs:78-83): c = g - H x, y = QP(H, c, x), p = y - x
@@ -362,40 +428,66 @@ extern "C" __global__ void __launch_bounds__(128) wave_solve_kernel(WaveArgs A) 
 
 // ------------------------------------------------------------------- host
 
+__global__ void wave_iota_kernel(int* v, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) v[i] = i;
+}
+
 int run_waves(const std::vector<PairJob>& jobs, const RunConfig& cfg, Workspace& ws,
               cudaStream_t st, kg_run_stats& stats, std::string& err,
               const std::vector<CohortDev>& table, int64_t total_pairs, int64_t list_cap) {
+    (void)jobs;
     int dev = 0;
     KG_WAVE_TRY(cudaGetDevice(&dev));
     if (ws.sm_count == 0) KG_WAVE_TRY(cudaDeviceGetAttribute(&ws.sm_count, cudaDevAttrMultiProcessorCount, dev));
+    // work units: per shape at most ceil(list_cap / UNIT_ELEMS), over the five
+    // shapes at most that + 5
+    const int64_t shape_units = (list_cap + UNIT_ELEMS - 1) / UNIT_ELEMS;
+    const int max_units = (int)shape_units + 5;
     // slots: as many as the work and the memory allow
-    const int max_units = (int)((list_cap + UNIT_ELEMS - 1) / UNIT_ELEMS) + 5;
     const size_t per_slot = sizeof(double) * (size_t)list_cap + sizeof(double) * max_units * UNIT_VALS +
-                            sizeof(SlotState) + 2 * sizeof(int);
+                            sizeof(SlotState) + 4 * sizeof(int) + 2 * 5 * shape_units * sizeof(int2);
     size_t fr = 0, tot = 0;
     KG_WAVE_TRY(cudaMemGetInfo(&fr, &tot));
     int64_t want = cfg.slots > 0 ? cfg.slots : 8192;
     int64_t by_mem = (int64_t)((fr / 2) / per_slot);
     int64_t n_slots = std::max<int64_t>(1, std::min<int64_t>({want, by_mem, total_pairs}));
+    const int64_t task_cap = n_slots * shape_units;
     // device buffers (grown and reused through the workspace)
     KG_WAVE_TRY((cudaError_t)ws.scratch.reserve(sizeof(double) * (size_t)list_cap * n_slots));
     KG_WAVE_TRY((cudaError_t)ws.partial.reserve(sizeof(double) * (size_t)max_units * UNIT_VALS * n_slots));
     KG_WAVE_TRY((cudaError_t)ws.slots.reserve(sizeof(SlotState) * n_slots));
-    KG_WAVE_TRY((cudaError_t)ws.lists_a.reserve(sizeof(int) * n_slots));
-    KG_WAVE_TRY((cudaError_t)ws.lists_b.reserve(sizeof(int) * n_slots));
-    KG_WAVE_TRY((cudaError_t)ws.counts.reserve(sizeof(int) * 8));
+    KG_WAVE_TRY((cudaError_t)ws.lists_a.reserve(sizeof(int) * 2 * n_slots));   // pass lists
+    KG_WAVE_TRY((cudaError_t)ws.lists_b.reserve(sizeof(int) * 2 * n_slots));   // free lists
+    KG_WAVE_TRY((cudaError_t)ws.tasks.reserve(sizeof(int2) * 2 * 5 * task_cap));
+    KG_WAVE_TRY((cudaError_t)ws.counts.reserve(sizeof(WaveCounts) * 2 + 64));
     KG_WAVE_TRY((cudaError_t)ws.queue.reserve(sizeof(unsigned long long) * 2));
     KG_WAVE_TRY((cudaError_t)ws.counters.reserve(sizeof(RunCounters)));
     KG_WAVE_TRY((cudaError_t)ws.table.reserve(sizeof(CohortDev) * table.size()));
     KG_WAVE_TRY(cudaMemcpyAsync(ws.table.p, table.data(), sizeof(CohortDev) * table.size(),
                                 cudaMemcpyHostToDevice, st));
+    WaveCounts* wc = reinterpret_cast<WaveCounts*>(ws.counts.p);
+    int* admit_task = reinterpret_cast<int*>(wc + 2);
+    unsigned long long* q = ws.queue.as<unsigned long long>();   // [0] pairs, [1] pass units
+    int* pass_l[2] = {ws.lists_a.as<int>(), ws.lists_a.as<int>() + n_slots};
+    int* free_l[2] = {ws.lists_b.as<int>(), ws.lists_b.as<int>() + n_slots};
+    int2* tasks_l[2] = {ws.tasks.as<int2>(), ws.tasks.as<int2>() + 5 * task_cap};
     KG_WAVE_TRY(cudaMemsetAsync(ws.slots.p, 0, sizeof(SlotState) * n_slots, st));   // all SLOT_FREE
     KG_WAVE_TRY(cudaMemsetAsync(ws.queue.p, 0, sizeof(unsigned long long) * 2, st));
-    KG_WAVE_TRY(cudaMemsetAsync(ws.counts.p, 0, sizeof(int) * 8, st));
+    KG_WAVE_TRY(cudaMemsetAsync(ws.counts.p, 0, sizeof(WaveCounts) * 2 + 64, st));
     KG_WAVE_TRY(cudaMemsetAsync(ws.counters.p, 0, sizeof(RunCounters), st));
+    // the first wave admits every slot
+    wave_iota_kernel<<<(int)((n_slots + 255) / 256), 256, 0, st>>>(free_l[0], (int)n_slots);
+    {
+        const int nf = (int)n_slots;
+        KG_WAVE_TRY(cudaMemcpyAsync(&wc[0].n_free, &nf, sizeof(int), cudaMemcpyHostToDevice, st));
+        KG_WAVE_TRY(cudaStreamSynchronize(st));   // nf lives on this stack frame
+    }
     static bool attr = false;
     if (!attr) {
         KG_WAVE_TRY(cudaFuncSetAttribute(wave_pass_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 4 * WARP_SMEM));
+        KG_WAVE_TRY(cudaFuncSetAttribute(wave_admit_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         ADMIT_WARPS * WARP_SMEM));
         attr = true;
     }
     int occ = 0;
@@ -406,8 +498,14 @@ int run_waves(const std::vector<PairJob>& jobs, const RunConfig& cfg, Workspace&
     }
     if (cfg.pass_blocks_per_sm > 0) occ = std::min(occ, cfg.pass_blocks_per_sm);
     const int pass_blocks = ws.sm_count * occ;
-    int* counts = ws.counts.as<int>();   // [0] n_a, [1] n_b, [2] n_resort
-    unsigned long long* q = ws.queue.as<unsigned long long>();   // [0] pairs, [1] pass units
+    int aocc = 0;
+    KG_WAVE_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&aocc, wave_admit_kernel, ADMIT_WARPS * 32,
+                                                              ADMIT_WARPS * WARP_SMEM));
+    if (aocc <= 0) {
+        err = "admit kernel cannot be resident";
+        return KG_ECUDA;
+    }
+    const int admit_blocks = ws.sm_count * aocc;
     WaveArgs A;
     A.cohorts = ws.table.as<CohortDev>();
     A.n_cohorts = (int)table.size();
@@ -420,41 +518,46 @@ int run_waves(const std::vector<PairJob>& jobs, const RunConfig& cfg, Workspace&
     A.list_stride = list_cap;
     A.partial = ws.partial.as<double>();
     A.max_units = max_units;
-    A.n_resort = counts + 2;
-    A.task = q + 1;
+    A.task_cap = task_cap;
+    A.pass_task = q + 1;
+    A.admit_task = admit_task;
     A.tune = make_tune(cfg.iterations);
     A.counters = ws.counters.as<RunCounters>();
-    int* lst[2] = {ws.lists_a.as<int>(), ws.lists_b.as<int>()};
     int cur = 0;
     const int slot_blocks = (int)((n_slots + WAVE_WPB - 1) / WAVE_WPB);
     const size_t wsm = WAVE_WPB * WARP_SMEM;
-    // events: [0] start, then per wave admit / pass / solve ends
+    // events: per wave, before admit and after admit / pass / solve
     cudaEvent_t ev[4];
     for (auto& e : ev) KG_WAVE_TRY(cudaEventCreate(&e));
     struct EvGuard { cudaEvent_t* e; ~EvGuard() { for (int i = 0; i < 4; i++) cudaEventDestroy(e[i]); } } eg{ev};
-    uint64_t waves = 0, launches = 0;
+    uint64_t waves = 0, launches = 1;
     double phase[3] = {0.0, 0.0, 0.0}, total = 0.0;
     for (;;) {
-        A.pass_list = lst[cur];
-        A.n_pass = counts + cur;
-        A.next_list = lst[cur ^ 1];
-        A.n_next = counts + (cur ^ 1);
+        const int nxt = cur ^ 1;
+        A.pass_cur = pass_l[cur];
+        A.pass_next = pass_l[nxt];
+        A.free_cur = free_l[cur];
+        A.free_next = free_l[nxt];
+        A.tasks_cur = tasks_l[cur];
+        A.tasks_next = tasks_l[nxt];
+        A.wc_cur = wc + cur;
+        A.wc_next = wc + nxt;
         KG_WAVE_TRY(cudaEventRecord(ev[0], st));
-        wave_admit_kernel<<<slot_blocks, 128, wsm, st>>>(A, lst[cur], counts + cur);
+        KG_WAVE_TRY(cudaMemsetAsync(admit_task, 0, sizeof(int), st));
         KG_WAVE_TRY(cudaMemsetAsync(q + 1, 0, sizeof(unsigned long long), st));
+        KG_WAVE_TRY(cudaMemsetAsync(wc + nxt, 0, sizeof(WaveCounts), st));
+        wave_admit_kernel<<<admit_blocks, ADMIT_WARPS * 32, ADMIT_WARPS * WARP_SMEM, st>>>(A);
         KG_WAVE_TRY(cudaEventRecord(ev[1], st));
         wave_pass_kernel<<<pass_blocks, 128, wsm, st>>>(A);
         KG_WAVE_TRY(cudaEventRecord(ev[2], st));
-        KG_WAVE_TRY(cudaMemsetAsync(counts + (cur ^ 1), 0, sizeof(int), st));
-        KG_WAVE_TRY(cudaMemsetAsync(counts + 2, 0, sizeof(int), st));
         wave_solve_kernel<<<slot_blocks, 128, wsm, st>>>(A);
         KG_WAVE_TRY(cudaGetLastError());
         KG_WAVE_TRY(cudaEventRecord(ev[3], st));
         launches += 3;
         waves++;
-        int h[3];
+        WaveCounts h;
         unsigned long long hq = 0;
-        KG_WAVE_TRY(cudaMemcpyAsync(h, counts, sizeof(h), cudaMemcpyDeviceToHost, st));
+        KG_WAVE_TRY(cudaMemcpyAsync(&h, wc + nxt, sizeof(h), cudaMemcpyDeviceToHost, st));
         KG_WAVE_TRY(cudaMemcpyAsync(&hq, q, sizeof(hq), cudaMemcpyDeviceToHost, st));
         KG_WAVE_TRY(cudaStreamSynchronize(st));
         for (int i = 0; i < 3; i++) {
@@ -463,8 +566,8 @@ int run_waves(const std::vector<PairJob>& jobs, const RunConfig& cfg, Workspace&
             phase[i] += ms;
             total += ms;
         }
-        cur ^= 1;
-        if (h[cur] == 0 && h[2] == 0 && hq >= (unsigned long long)total_pairs) break;
+        cur = nxt;
+        if (h.n_pass == 0 && h.n_resort == 0 && hq >= (unsigned long long)total_pairs) break;
     }
     RunCounters rc;
     KG_WAVE_TRY(cudaMemcpyAsync(&rc, ws.counters.p, sizeof(rc), cudaMemcpyDeviceToHost, st));

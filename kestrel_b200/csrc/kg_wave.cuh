@@ -53,24 +53,39 @@ struct SlotState {
     PassCoef c64;         // its FP64 pass coefficients
 };
 
+// Per-wave counters (one set for the current wave, one for the next).
+struct WaveCounts {
+    int n_pass;      // slots with a pending pass
+    int n_free;      // slots for the admit step: free ones and those waiting for FP64 lists
+    int n_resort;    // of those, slots waiting for FP64 lists
+    int units[5];    // pass work units per shape
+};
+
 struct WaveArgs {
     const CohortDev* cohorts;
     int n_cohorts;
     int precision;
     int64_t total_pairs;
-    unsigned long long* queue;
+    unsigned long long* queue;     // next pair (global work index)
     SlotState* slots;
     int n_slots;
     double* lists;                 // per slot: list_stride 8-byte words
     int64_t list_stride;
     double* partial;               // per slot: max_units * UNIT_VALS
     int max_units;
-    const int* pass_list;          // slots with a pending pass (this wave)
-    const int* n_pass;
-    int* next_list;                // slots whose next pass the solve step scheduled
-    int* n_next;
-    int* n_resort;
-    unsigned long long* task;      // pass work-unit counter
+    // the current wave's lists (filled by the previous solve step and this
+    // wave's admit step) and the next wave's (filled by this solve step)
+    int* pass_cur;
+    int* pass_next;
+    int* free_cur;
+    int* free_next;
+    int2* tasks_cur;               // per shape: task_cap entries {slot, unit}
+    int2* tasks_next;
+    int64_t task_cap;
+    WaveCounts* wc_cur;
+    WaveCounts* wc_next;
+    unsigned long long* pass_task; // pass work-unit counter
+    int* admit_task;               // admit entry counter
     Tune tune;
     RunCounters* counters;
 };
@@ -128,6 +143,24 @@ __device__ __forceinline__ void decode_pair(const WaveArgs& A, int64_t k, int& c
         x = j / co.n_y;
         y = j - x * co.n_y;
     }
+}
+
+// Queues slot s for a pass in the wave whose lists are (pass, tasks, wc): its
+// work units go to the shape-major task lists, so that the warps of the pass
+// kernel run one shape's code at a time.  Called by a whole warp after S.ustart
+// is set.
+__device__ inline void enqueue_pass(int* pass, int2* tasks, int64_t task_cap, WaveCounts* wc, int s,
+                                    const SlotState& S, int lane) {
+#pragma unroll 1
+    for (int sh = 0; sh < 5; sh++) {
+        const int u0 = S.ustart[sh], nu = S.ustart[sh + 1] - u0;
+        if (nu == 0) continue;
+        int base = 0;
+        if (lane == 0) base = atomicAdd(&wc->units[sh], nu);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        for (int i = lane; i < nu; i += 32) tasks[sh * task_cap + base + i] = make_int2(s, u0 + i);
+    }
+    if (lane == 0) pass[atomicAdd(&wc->n_pass, 1)] = s;
 }
 
 __device__ inline void write_row(kg_output* out, int64_t x, int64_t y, const double* d, double obj,
