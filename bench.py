@@ -46,6 +46,8 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--slots", type=int, default=0, help="pairs in flight per wave (0 = automatic)")
+    ap.add_argument("--pass-bps", type=int, default=0, help="site-pass blocks per SM (0 = automatic)")
     return ap.parse_args()
 
 
@@ -195,6 +197,7 @@ def main():
     n, m = codes.shape
     pairs = n * (n - 1) // 2
     est = kb.Estimator(device=local, precision=args.precision)
+    est.set_launch(args.slots, args.pass_bps)
     est.load(codes)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")
 

@@ -21,7 +21,7 @@ CLI = os.path.join(HERE, "bin", "kestrel")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CUDA_SOURCES = ["kg_engine.cu", "kg_wave.cu", "kg_api.cu", "kg_noalloc.cu"]
 HOST_SOURCES = ["kg_cli.cpp"]
-HEADERS = ["kg_engine.h", "kg_pair.cuh", "kg_solver.cuh", "kg_rowsolve.cuh", "kg_wave.cuh"]
+HEADERS = ["kg_engine.h", "kg_pair.cuh", "kg_solver.cuh", "kg_rowsolve.cuh", "kg_wave.cuh", "kg_bulk.cuh"]
 
 
 def nvcc() -> str:

@@ -78,6 +78,7 @@ struct RunCounters {
     unsigned long long flops_fp64;
     unsigned long long shape_sites[5];
     unsigned long long cycles[5];   // SM clocks per phase: count, scatter, site passes, solver, streams
+    unsigned long long stalled_waits;   // device waits that ran out of their limit
 };
 
 struct PairLaunch {
@@ -395,43 +396,38 @@ struct LaneSums {
 
 constexpr int HESS_FLUSH = 8;   // loop iterations (8 sites each) between FP32 -> FP64 Hessian flushes
 
-// Streams one shape's FP32 list.  Each loop iteration handles two float4
-// (8 sites per lane) held in two registers that are refilled right after use,
-// so every load has a full iteration to arrive.  Gradient moments and the
-// objective are promoted to FP64 every 8 sites, Hessian moments every 64; each
-// site is the closed form of its shape (see the file comment).  diff selects
-// the log(d_new/d_old) objective.
+// The FP32 closed form of one shape: coefficients of the pending pass (from
+// shared memory) and the per-site update of the FP32 partial sums.
 template <int S>
-__device__ __noinline__ void stream32(const float* __restrict__ L, int64_t len, const Coef32* K,
-                                      bool diff, int lane, LaneSums& out) {
-    constexpr int NG = S == 0 ? 4 : S == 3 ? 4 : S == 4 ? 2 : 3;
-    constexpr int NH = S == 0 ? 7 : S == 3 ? 9 : S == 4 ? 3 : 5;
-    constexpr int GOFF = S == 0 ? 0 : S == 1 ? 11 : S == 2 ? 19 : S == 3 ? 27 : 40;
-    constexpr int HOFF = GOFF + NG;
-    const float EPS = 1e-8f;
+struct Shape32 {
+    static constexpr int NG = S == 0 ? 4 : S == 3 ? 4 : S == 4 ? 2 : 3;
+    static constexpr int NH = S == 0 ? 7 : S == 3 ? 9 : S == 4 ? 3 : 5;
+    static constexpr int GOFF = S == 0 ? 0 : S == 1 ? 11 : S == 2 ? 19 : S == 3 ? 27 : 40;
+    static constexpr int HOFF = GOFF + NG;
     HiLo k0, k1, k2, k3;
-    float s0 = 0.f, s1 = 0.f, s2 = 0.f, s3 = 0.f;
-    if (S == 0) { k0 = ldk(&K->a[0]); k1 = ldk(&K->a[1]); k2 = ldk(&K->a[2]); k3 = ldk(&K->a[3]); }
-    if (S == 1) { k0 = ldk(&K->b1[0]); k1 = ldk(&K->b1[1]); k2 = ldk(&K->b1[2]); k3 = HiLo{0.f, 0.f}; }
-    if (S == 2) { k0 = ldk(&K->b2[0]); k1 = ldk(&K->b2[1]); k2 = ldk(&K->b2[2]); k3 = HiLo{0.f, 0.f}; }
-    if (S == 3) { k0 = ldk(&K->c[0]); k1 = ldk(&K->c[1]); k2 = ldk(&K->c[2]); k3 = ldk(&K->c[3]); }
-    if (S == 4) { k0 = ldk(&K->d[0]); k1 = ldk(&K->d[1]); k2 = HiLo{0.f, 0.f}; k3 = HiLo{0.f, 0.f}; }
-    if (diff) {
-        const float* sp = S == 0 ? K->sa : S == 1 ? K->sb1 : S == 2 ? K->sb2 : S == 3 ? K->sc : K->sd;
-        s0 = ld_volatile(&sp[0]);
-        s1 = ld_volatile(&sp[1]);
-        if (S != 4) s2 = ld_volatile(&sp[2]);
-        if (S == 0 || S == 3) s3 = ld_volatile(&sp[3]);
+    float s0, s1, s2, s3;
+    bool diff;
+
+    __device__ __forceinline__ void load(const Coef32* K, bool diff_) {
+        diff = diff_;
+        s0 = s1 = s2 = s3 = 0.f;
+        if (S == 0) { k0 = ldk(&K->a[0]); k1 = ldk(&K->a[1]); k2 = ldk(&K->a[2]); k3 = ldk(&K->a[3]); }
+        if (S == 1) { k0 = ldk(&K->b1[0]); k1 = ldk(&K->b1[1]); k2 = ldk(&K->b1[2]); k3 = HiLo{0.f, 0.f}; }
+        if (S == 2) { k0 = ldk(&K->b2[0]); k1 = ldk(&K->b2[1]); k2 = ldk(&K->b2[2]); k3 = HiLo{0.f, 0.f}; }
+        if (S == 3) { k0 = ldk(&K->c[0]); k1 = ldk(&K->c[1]); k2 = ldk(&K->c[2]); k3 = ldk(&K->c[3]); }
+        if (S == 4) { k0 = ldk(&K->d[0]); k1 = ldk(&K->d[1]); k2 = HiLo{0.f, 0.f}; k3 = HiLo{0.f, 0.f}; }
+        if (diff) {
+            const float* sp = S == 0 ? K->sa : S == 1 ? K->sb1 : S == 2 ? K->sb2 : S == 3 ? K->sc : K->sd;
+            s0 = ld_volatile(&sp[0]);
+            s1 = ld_volatile(&sp[1]);
+            if (S != 4) s2 = ld_volatile(&sp[2]);
+            if (S == 0 || S == 3) s3 = ld_volatile(&sp[3]);
+        }
     }
-    double G[NG], H[NH], F = 0.0;
-    float h[NH];
-#pragma unroll
-    for (int i = 0; i < NG; i++) G[i] = 0.0;
-#pragma unroll
-    for (int i = 0; i < NH; i++) { H[i] = 0.0; h[i] = 0.f; }
 
     // one site: adds into the FP32 partials g, ob (per iteration) and h
-    auto site = [&](float t, float* g, float& ob) {
+    __device__ __forceinline__ void site(float t, float* g, float& ob, float* h) const {
+        const float EPS = 1e-8f;
         float d, r, c;    // c = the per-site scale: t (A) or w (B, C, D)
         if (S == 0) {
             float ph = fmaf(fmaf(fmaf(k3.h, t, k2.h), t, k1.h), t, k0.h);
@@ -494,7 +490,29 @@ __device__ __noinline__ void stream32(const float* __restrict__ L, int64_t len, 
             else dl = c * fmaf(c, s1, s0);
             ob += neg_log1m(dl * r);
         }
-    };
+    }
+};
+
+// Streams one shape's FP32 list.  Each loop iteration handles two float4
+// (8 sites per lane) held in two registers that are refilled right after use,
+// so every load has a full iteration to arrive.  Gradient moments and the
+// objective are promoted to FP64 every 8 sites, Hessian moments every 64; each
+// site is the closed form of its shape (see the file comment).  diff selects
+// the log(d_new/d_old) objective.
+template <int S>
+__device__ __noinline__ void stream32(const float* __restrict__ L, int64_t len, const Coef32* K,
+                                      bool diff, int lane, LaneSums& out) {
+    using E = Shape32<S>;
+    constexpr int NG = E::NG, NH = E::NH, GOFF = E::GOFF, HOFF = E::HOFF;
+    E ev;
+    ev.load(K, diff);
+    double G[NG], H[NH], F = 0.0;
+    float h[NH];
+#pragma unroll
+    for (int i = 0; i < NG; i++) G[i] = 0.0;
+#pragma unroll
+    for (int i = 0; i < NH; i++) { H[i] = 0.0; h[i] = 0.f; }
+    auto site = [&](float t, float* g, float& ob) { ev.site(t, g, ob, h); };
 
     const int64_t n4 = len >> 2;
     const float4* L4 = reinterpret_cast<const float4*>(L);

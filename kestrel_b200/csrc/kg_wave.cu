@@ -4,6 +4,7 @@
 #include <cstring>
 
 #include "kg_engine.h"
+#include "kg_bulk.cuh"
 #include "kg_wave.cuh"
 
 namespace kg {
@@ -159,15 +160,139 @@ extern "C" __global__ void __launch_bounds__(ADMIT_WARPS * 32) wave_admit_kernel
 
 // ------------------------------------------------------------------- pass
 
+// Each pass warp streams its FP32 lists through a ring of RING_STAGES stages
+// in its shared memory: lane 0 keeps up to RING_STAGES bulk copies in flight,
+// so the site arithmetic reads shared memory while HBM fills the stages ahead.
+constexpr int RING_STAGES = 8;
+constexpr int STAGE_F4 = 64;                  // float4 per stage: two per lane
+constexpr int STAGE_ELEMS = STAGE_F4 * 4;     // list entries per stage
+static_assert(RING_STAGES * STAGE_F4 * 16 <= WARP_SMEM_BUF, "ring must fit the warp's buffer");
+static_assert(sizeof(Coef32) + RING_STAGES * 8 <= WARP_SMEM_COEF, "coefficients and barriers must fit");
+
+struct Ring {
+    float4* buf;      // RING_STAGES * STAGE_F4
+    uint64_t* bar;    // RING_STAGES barriers
+    uint32_t seq;     // stages this warp has consumed so far
+};
+
+__device__ __forceinline__ void ring_issue(const Ring& R, const float* L, int64_t len, int i, uint32_t slot) {
+    const int64_t e0 = (int64_t)i * STAGE_ELEMS;
+    const int64_t ne = min((int64_t)STAGE_ELEMS, len - e0);
+    const uint32_t bytes = (uint32_t)((ne * 4 + 15) & ~int64_t(15));
+    bulk_load(R.buf + slot * STAGE_F4, L + e0, bytes, &R.bar[slot]);
+}
+
+// The FP32 stream of stream32 fed from the ring: the same lane-to-site
+// assignment (stage i holds float4 64 i .. 64 i + 63; lane l takes 64 i + l
+// and 64 i + 32 + l) and the same summation order, so the sums are identical.
+// L and every stage start are 16-byte aligned (list starts are multiples of
+// four entries); a stage's copy rounds its size up to 16 bytes, which stays
+// inside the slot's list buffer.  Returns false if a wait ran out.
+template <int S>
+__device__ __noinline__ bool stream32_ring(const float* __restrict__ L, int64_t len, const Coef32* K,
+                                           bool diff, int lane, Ring& R, LaneSums& out) {
+    using E = Shape32<S>;
+    constexpr int NG = E::NG, NH = E::NH, GOFF = E::GOFF, HOFF = E::HOFF;
+    E ev;
+    ev.load(K, diff);
+    double G[NG], H[NH], F = 0.0;
+    float h[NH];
+#pragma unroll
+    for (int i = 0; i < NG; i++) G[i] = 0.0;
+#pragma unroll
+    for (int i = 0; i < NH; i++) { H[i] = 0.0; h[i] = 0.f; }
+    const int64_t n4 = len >> 2;
+    const int nst = (int)((len + STAGE_ELEMS - 1) / STAGE_ELEMS);
+    if (lane == 0) {
+        const int pro = min(nst, RING_STAGES);
+        fence_proxy_async_smem();
+        for (int i = 0; i < pro; i++) ring_issue(R, L, len, i, (R.seq + i) % RING_STAGES);
+    }
+    bool ok = true;
+    int it = 0, done = 0;
+    for (int i = 0; i < nst; i++) {
+        const uint32_t q = R.seq + i;
+        const uint32_t slot = q % RING_STAGES;
+        if (!mbar_wait(&R.bar[slot], (q / RING_STAGES) & 1u)) { ok = false; break; }
+        done = i + 1;
+        const float4* B = R.buf + slot * STAGE_F4;
+        const int64_t k = (int64_t)i * STAGE_F4 + lane;
+        float g[NG], ob = 0.f;
+#pragma unroll
+        for (int j = 0; j < NG; j++) g[j] = 0.f;
+        if (k < n4) {
+            const float4 v = B[lane];
+            ev.site(v.x, g, ob, h);
+            ev.site(v.y, g, ob, h);
+            ev.site(v.z, g, ob, h);
+            ev.site(v.w, g, ob, h);
+        }
+        if (k + 32 < n4) {
+            const float4 v = B[lane + 32];
+            ev.site(v.x, g, ob, h);
+            ev.site(v.y, g, ob, h);
+            ev.site(v.z, g, ob, h);
+            ev.site(v.w, g, ob, h);
+        }
+        if (k < n4) {
+#pragma unroll
+            for (int j = 0; j < NG; j++) G[j] += (double)g[j];
+            F += (double)ob;
+            if (++it == HESS_FLUSH) {
+#pragma unroll
+                for (int j = 0; j < NH; j++) { H[j] += (double)h[j]; h[j] = 0.f; }
+                it = 0;
+            }
+        }
+        if (i + RING_STAGES < nst) {
+            __syncwarp();
+            if (lane == 0) {
+                fence_proxy_async_smem();
+                ring_issue(R, L, len, i + RING_STAGES, slot);
+            }
+        }
+    }
+    if (!ok) {
+        // let this warp's copies in flight land before it leaves
+        const int issued = min(nst, done + RING_STAGES);
+        for (int i = done; i < issued; i++) {
+            const uint32_t q = R.seq + i;
+            if (!mbar_wait(&R.bar[q % RING_STAGES], (q / RING_STAGES) & 1u)) break;
+        }
+        return false;
+    }
+    if (lane < (int)(len & 3)) {
+        const float* B = reinterpret_cast<const float*>(R.buf + ((R.seq + nst - 1) % RING_STAGES) * STAGE_F4);
+        float g[NG], ob = 0.f;
+#pragma unroll
+        for (int j = 0; j < NG; j++) g[j] = 0.f;
+        ev.site(B[4 * n4 - (int64_t)(nst - 1) * STAGE_ELEMS + lane], g, ob, h);
+#pragma unroll
+        for (int j = 0; j < NG; j++) G[j] += (double)g[j];
+        F += (double)ob;
+    }
+    __syncwarp();   // every lane has read the ring before the next copies
+    R.seq += nst;
+#pragma unroll
+    for (int j = 0; j < NH; j++) H[j] += (double)h[j];
+#pragma unroll
+    for (int j = 0; j < NG; j++) out.m[GOFF + j] = G[j];
+#pragma unroll
+    for (int j = 0; j < NH; j++) out.m[HOFF + j] = H[j];
+    out.obj += F;
+    return true;
+}
+
 template <int SH>
-__device__ __forceinline__ void run_unit(const void* lists, bool l64, int64_t off, int64_t len,
-                                         const void* kbuf, bool diff, int lane, LaneSums& ls) {
-    if (l64)
+__device__ __forceinline__ bool run_unit(const void* lists, bool l64, int64_t off, int64_t len,
+                                         const void* kbuf, bool diff, int lane, Ring& R, LaneSums& ls) {
+    if (l64) {
         stream64<SH>(static_cast<const double*>(lists) + off, len, reinterpret_cast<const PassCoef*>(kbuf),
                      lane, ls);
-    else
-        stream32<SH>(static_cast<const float*>(lists) + off, len, reinterpret_cast<const Coef32*>(kbuf),
-                     diff, lane, ls);
+        return true;
+    }
+    return stream32_ring<SH>(static_cast<const float*>(lists) + off, len, reinterpret_cast<const Coef32*>(kbuf),
+                             diff, lane, R, ls);
 }
 
 extern "C" __global__ void __launch_bounds__(128, 4) wave_pass_kernel(WaveArgs A) {
@@ -175,6 +300,15 @@ extern "C" __global__ void __launch_bounds__(128, 4) wave_pass_kernel(WaveArgs A
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     char* wsm = smem + wib * WARP_SMEM;
     char* kbuf = wsm + WARP_SMEM_BUF;
+    Ring R;
+    R.buf = reinterpret_cast<float4*>(wsm);
+    R.bar = reinterpret_cast<uint64_t*>(kbuf + sizeof(Coef32));
+    R.seq = 0;
+    if (lane == 0) {
+        for (int i = 0; i < RING_STAGES; i++) mbar_init(&R.bar[i], 1);
+        fence_mbar_init();
+    }
+    __syncwarp();
     int pre[6];
     pre[0] = 0;
 #pragma unroll
@@ -186,7 +320,8 @@ extern "C" __global__ void __launch_bounds__(128, 4) wave_pass_kernel(WaveArgs A
         t = __shfl_sync(0xffffffffu, t, 0);
         if ((int64_t)t >= ntask) break;
         int sh = 0;
-        while ((int)t >= pre[sh + 1]) sh++;
+#pragma unroll
+        for (int k = 1; k < 5; k++) sh += ((int)t >= pre[k]) ? 1 : 0;
         const int2 tk = A.tasks_cur[sh * A.task_cap + ((int)t - pre[sh])];
         const int s = tk.x;
         const int u = tk.y;
@@ -206,12 +341,17 @@ extern "C" __global__ void __launch_bounds__(128, 4) wave_pass_kernel(WaveArgs A
         const bool diff = (kind == PASS_FP32_DIFF);
         LaneSums ls;
         ls.obj = 0.0;
+        bool ok;
         switch (sh) {
-        case 0: run_unit<0>(lists, l64, off, len, kbuf, diff, lane, ls); break;
-        case 1: run_unit<1>(lists, l64, off, len, kbuf, diff, lane, ls); break;
-        case 2: run_unit<2>(lists, l64, off, len, kbuf, diff, lane, ls); break;
-        case 3: run_unit<3>(lists, l64, off, len, kbuf, diff, lane, ls); break;
-        default: run_unit<4>(lists, l64, off, len, kbuf, diff, lane, ls); break;
+        case 0: ok = run_unit<0>(lists, l64, off, len, kbuf, diff, lane, R, ls); break;
+        case 1: ok = run_unit<1>(lists, l64, off, len, kbuf, diff, lane, R, ls); break;
+        case 2: ok = run_unit<2>(lists, l64, off, len, kbuf, diff, lane, R, ls); break;
+        case 3: ok = run_unit<3>(lists, l64, off, len, kbuf, diff, lane, R, ls); break;
+        default: ok = run_unit<4>(lists, l64, off, len, kbuf, diff, lane, R, ls); break;
+        }
+        if (!__all_sync(0xffffffffu, ok)) {
+            if (lane == 0) atomicAdd(&A.counters->stalled_waits, 1ull);
+            return;
         }
         const int go = shape_goff(sh), nv = shape_ng(sh) + shape_nh(sh);
         double* P = A.partial + ((int64_t)s * A.max_units + u) * UNIT_VALS;
@@ -588,6 +728,10 @@ int run_waves(const std::vector<PairJob>& jobs, const RunConfig& cfg, Workspace&
     stats.pass_ms = phase[1];
     stats.solve_ms = phase[2];
     stats.pair_kernel_ms = total;
+    if (rc.stalled_waits) {
+        err = "a device wait for a list copy ran out of its limit";
+        return KG_ETIMEOUT;
+    }
     if (rc.nosite_pairs) {
         err = "a pair has no jointly observed segregating site (its row is NaN)";
         return KG_ENOSITES;
