@@ -456,8 +456,8 @@ jacquard_pair_kernel(PairLaunch L) {
             for (int s = 0; s < 5; s++) {
                 c_shape[s] += (unsigned long long)pl.cnt[s];
                 c_fl32 += (unsigned long long)pl.cnt[s] *
-                          (unsigned long long)(p32 * flops_direct(s) + res.diff_passes * flops_diff_extra(s));
-                c_fl64 += (unsigned long long)pl.cnt[s] * (unsigned long long)(res.fp64_passes * flops_direct(s));
+                          (unsigned long long)(p32 * flops_fp32_lo(s) + res.diff_passes * flops_diff_extra(s));
+                c_fl64 += (unsigned long long)pl.cnt[s] * (unsigned long long)(res.fp64_passes * flops_fp64(s));
             }
         }
         // 14 eight-byte words per row, one per lane

@@ -397,8 +397,16 @@ struct LaneSums {
 constexpr int HESS_FLUSH = 8;   // loop iterations (8 sites each) between FP32 -> FP64 Hessian flushes
 
 // The FP32 closed form of one shape: coefficients of the pending pass (from
-// shared memory) and the per-site update of the FP32 partial sums.
-template <int S>
+// shared memory) and the per-site update of the FP32 partial sums.  The
+// moments share their products: with u = r c (c = t for A, w otherwise) the
+// gradient terms are u times powers of the shape's monomials and every Hessian
+// term is a product of two gradient terms.
+//
+// LO = true evaluates L.Delta with the hi + lo split coefficients (the FP64
+// iterate to ~1e-14); LO = false uses the hi parts only, and the solve step
+// restores the lo part to first order in FP64 from the moments themselves
+// (lo_correction), which leaves an error of (lo / hi)^2 ~ 1e-15 relative.
+template <int S, bool LO = true>
 struct Shape32 {
     static constexpr int NG = S == 0 ? 4 : S == 3 ? 4 : S == 4 ? 2 : 3;
     static constexpr int NH = S == 0 ? 7 : S == 3 ? 9 : S == 4 ? 3 : 5;
@@ -431,53 +439,48 @@ struct Shape32 {
         float d, r, c;    // c = the per-site scale: t (A) or w (B, C, D)
         if (S == 0) {
             float ph = fmaf(fmaf(fmaf(k3.h, t, k2.h), t, k1.h), t, k0.h);
-            float pl = fmaf(fmaf(fmaf(k3.l, t, k2.l), t, k1.l), t, k0.l);
-            d = fmaf(t, ph + pl, EPS);
+            if (LO) ph = ph + fmaf(fmaf(fmaf(k3.l, t, k2.l), t, k1.l), t, k0.l);
+            d = fmaf(t, ph, EPS);
             r = rcp_nr(d);
-            float u = r * t;
-            float t2 = t * t, t3 = t2 * t, t4 = t2 * t2, t5 = t4 * t, t6 = t3 * t3;
-            g[0] += u; g[1] = fmaf(u, t, g[1]); g[2] = fmaf(u, t2, g[2]); g[3] = fmaf(u, t3, g[3]);
-            float u2 = u * u;
-            h[0] += u2; h[1] = fmaf(u2, t, h[1]); h[2] = fmaf(u2, t2, h[2]); h[3] = fmaf(u2, t3, h[3]);
-            h[4] = fmaf(u2, t4, h[4]); h[5] = fmaf(u2, t5, h[5]); h[6] = fmaf(u2, t6, h[6]);
+            const float u = r * t, v1 = u * t, v2 = v1 * t, v3 = v2 * t;   // r t^1..4
+            g[0] += u; g[1] += v1; g[2] += v2; g[3] += v3;
+            h[0] = fmaf(u, u, h[0]); h[1] = fmaf(u, v1, h[1]); h[2] = fmaf(v1, v1, h[2]);
+            h[3] = fmaf(v1, v2, h[3]); h[4] = fmaf(v2, v2, h[4]); h[5] = fmaf(v2, v3, h[5]);
+            h[6] = fmaf(v3, v3, h[6]);
             c = t;
         } else if (S == 1 || S == 2) {
-            float w = t * (1.0f - t);
+            const float w = fmaf(-t, t, t);
             float ph = fmaf(fmaf(k2.h, t, k1.h), t, k0.h);
-            float pl = fmaf(fmaf(k2.l, t, k1.l), t, k0.l);
-            d = fmaf(w, ph + pl, EPS);
+            if (LO) ph = ph + fmaf(fmaf(k2.l, t, k1.l), t, k0.l);
+            d = fmaf(w, ph, EPS);
             r = rcp_nr(d);
-            float v = r * w;
-            float t2 = t * t, t3 = t2 * t, t4 = t2 * t2;
-            g[0] += v; g[1] = fmaf(v, t, g[1]); g[2] = fmaf(v, t2, g[2]);
-            float v2 = v * v;
-            h[0] += v2; h[1] = fmaf(v2, t, h[1]); h[2] = fmaf(v2, t2, h[2]); h[3] = fmaf(v2, t3, h[3]);
-            h[4] = fmaf(v2, t4, h[4]);
+            const float v = r * w, v1 = v * t, v2 = v1 * t;                 // r w t^0..2
+            g[0] += v; g[1] += v1; g[2] += v2;
+            h[0] = fmaf(v, v, h[0]); h[1] = fmaf(v, v1, h[1]); h[2] = fmaf(v1, v1, h[2]);
+            h[3] = fmaf(v1, v2, h[3]); h[4] = fmaf(v2, v2, h[4]);
             c = w;
         } else if (S == 3) {
-            float ty = 1.0f - t;   // t = tx, the frequency of x's allele
-            float w = t * ty;
+            const float ty = 1.0f - t;   // t = tx, the frequency of x's allele
+            const float w = t * ty;
             float ph = fmaf(w, k3.h, fmaf(t, k2.h, fmaf(ty, k1.h, k0.h)));
-            float pl = fmaf(w, k3.l, fmaf(t, k2.l, fmaf(ty, k1.l, k0.l)));
-            d = fmaf(w, ph + pl, EPS);
+            if (LO) ph = ph + fmaf(w, k3.l, fmaf(t, k2.l, fmaf(ty, k1.l, k0.l)));
+            d = fmaf(w, ph, EPS);
             r = rcp_nr(d);
-            float v = r * w;
-            g[0] += v; g[1] = fmaf(v, ty, g[1]); g[2] = fmaf(v, t, g[2]); g[3] = fmaf(v, w, g[3]);
-            float v2 = v * v;
-            h[0] += v2; h[1] = fmaf(v2, ty, h[1]); h[2] = fmaf(v2, t, h[2]); h[3] = fmaf(v2, w, h[3]);
-            h[4] = fmaf(v2, ty * ty, h[4]); h[5] = fmaf(v2, t * t, h[5]);
-            h[6] = fmaf(v2, w * ty, h[6]); h[7] = fmaf(v2, w * t, h[7]); h[8] = fmaf(v2, w * w, h[8]);
+            const float v = r * w, a = v * ty, b = v * t, e = v * w;          // r w {1, ty, t, w}
+            g[0] += v; g[1] += a; g[2] += b; g[3] += e;
+            h[0] = fmaf(v, v, h[0]); h[1] = fmaf(v, a, h[1]); h[2] = fmaf(v, b, h[2]);
+            h[3] = fmaf(v, e, h[3]); h[4] = fmaf(a, a, h[4]); h[5] = fmaf(b, b, h[5]);
+            h[6] = fmaf(e, a, h[6]); h[7] = fmaf(e, b, h[7]); h[8] = fmaf(e, e, h[8]);
             c = w;
         } else {
-            float w = t * (1.0f - t);
+            const float w = fmaf(-t, t, t);
             float ph = fmaf(w, k1.h, k0.h);
-            float pl = fmaf(w, k1.l, k0.l);
-            d = fmaf(w, ph + pl, EPS);
+            if (LO) ph = ph + fmaf(w, k1.l, k0.l);
+            d = fmaf(w, ph, EPS);
             r = rcp_nr(d);
-            float v = r * w;
-            g[0] += v; g[1] = fmaf(v, w, g[1]);
-            float v2 = v * v;
-            h[0] += v2; h[1] = fmaf(v2, w, h[1]); h[2] = fmaf(v2, w * w, h[2]);
+            const float v = r * w, a = v * w;                                // r w {1, w}
+            g[0] += v; g[1] += a;
+            h[0] = fmaf(v, v, h[0]); h[1] = fmaf(v, a, h[1]); h[2] = fmaf(a, a, h[2]);
             c = w;
         }
         if (!diff) {
@@ -492,6 +495,69 @@ struct Shape32 {
         }
     }
 };
+
+// First-order restoration of the lo coefficients for sums taken with the hi
+// parts only (Shape32<S, false>).  With d = d_hi + delta, delta = c(t) times
+// the lo polynomial, every gradient moment sum_s r c m(s) changes by
+// -sum_s r^2 c^2 m(s) lo(s), a combination of the shape's Hessian moments, and
+// the natural-log objective by +sum_s delta / d = sum_j lo_j G_j.  mom holds
+// the 45 FP64 moments (corrected in place); returns the objective correction.
+__device__ inline double lo_correction(double* mom, const Coef32& K) {
+    double corr = 0.0;
+    // A: G_k = m[k] (r t^{k+1}, k = 0..3), H_m = m[4 + m] (r^2 t^{m+2}); lo = t sum_j l_j t^j
+    {
+        double l[4], gd[4];
+        for (int j = 0; j < 4; j++) l[j] = (double)K.a[j].l;
+        for (int k = 0; k < 4; k++) {
+            double s = 0.0;
+            for (int j = 0; j < 4; j++) s = fma(l[j], mom[4 + k + j], s);
+            gd[k] = s;
+        }
+        for (int j = 0; j < 4; j++) corr = fma(l[j], mom[j], corr);
+        for (int k = 0; k < 4; k++) mom[k] -= gd[k];
+    }
+    // B1, B2: G_k = m[go + k] (r w t^k, k = 0..2), H_m = m[go + 3 + m] (r^2 w^2 t^m)
+    for (int b = 0; b < 2; b++) {
+        const int go = b == 0 ? 11 : 19;
+        const HiLo* kk = b == 0 ? K.b1 : K.b2;
+        double l[3], gd[3];
+        for (int j = 0; j < 3; j++) l[j] = (double)kk[j].l;
+        for (int k = 0; k < 3; k++) {
+            double s = 0.0;
+            for (int j = 0; j < 3; j++) s = fma(l[j], mom[go + 3 + k + j], s);
+            gd[k] = s;
+        }
+        for (int j = 0; j < 3; j++) corr = fma(l[j], mom[go + j], corr);
+        for (int k = 0; k < 3; k++) mom[go + k] -= gd[k];
+    }
+    // C: G = m[27..30] (r w {1, ty, t, w}), H = m[31..39] (r^2 w^2 {1, ty, t, w, ty^2, t^2, w ty, w t, w^2})
+    {
+        // products of {1, ty, t, w} x {1, ty, t, w} as Hessian moment indices (ty t = w)
+        const int P[4][4] = {{0, 1, 2, 3}, {1, 4, 3, 6}, {2, 3, 5, 7}, {3, 6, 7, 8}};
+        double l[4], gd[4];
+        for (int j = 0; j < 4; j++) l[j] = (double)K.c[j].l;
+        for (int k = 0; k < 4; k++) {
+            double s = 0.0;
+            for (int j = 0; j < 4; j++) s = fma(l[j], mom[31 + P[k][j]], s);
+            gd[k] = s;
+        }
+        for (int j = 0; j < 4; j++) corr = fma(l[j], mom[27 + j], corr);
+        for (int k = 0; k < 4; k++) mom[27 + k] -= gd[k];
+    }
+    // D: G = m[40..41] (r w {1, w}), H = m[42..44] (r^2 w^2 {1, w, w^2})
+    {
+        double l[2], gd[2];
+        for (int j = 0; j < 2; j++) l[j] = (double)K.d[j].l;
+        for (int k = 0; k < 2; k++) {
+            double s = 0.0;
+            for (int j = 0; j < 2; j++) s = fma(l[j], mom[42 + k + j], s);
+            gd[k] = s;
+        }
+        for (int j = 0; j < 2; j++) corr = fma(l[j], mom[40 + j], corr);
+        for (int k = 0; k < 2; k++) mom[40 + k] -= gd[k];
+    }
+    return corr;
+}
 
 // Streams one shape's FP32 list.  Each loop iteration handles two float4
 // (8 sites per lane) held in two registers that are refilled right after use,
@@ -816,9 +882,17 @@ struct PairResult {
 };
 
 // Executed site arithmetic per pass and shape (A, B1, B2, C, D), counting an
-// FMA as 2 and a MUFU op as 1: the direct pass, and the extra of the
-// log(d_new/d_old) objective.  Read off the loops of pass_fp32.
-__host__ __device__ constexpr int flops_direct(int s) {
+// FMA as 2 and a MUFU op as 1, read off Shape32::site and stream64: FP32 passes
+// on the hi coefficients (the wave engine), FP32 passes with the hi + lo
+// polynomial (the single-kernel engine), FP64 passes, and the extra of the
+// log(d_new/d_old) objective.
+__host__ __device__ constexpr int flops_fp32_hi(int s) {
+    return s == 0 ? 37 : s == 1 ? 31 : s == 2 ? 31 : s == 3 ? 43 : 23;
+}
+__host__ __device__ constexpr int flops_fp32_lo(int s) {
+    return s == 0 ? 44 : s == 1 ? 36 : s == 2 ? 36 : s == 3 ? 50 : 26;
+}
+__host__ __device__ constexpr int flops_fp64(int s) {
     return s == 0 ? 50 : s == 1 ? 39 : s == 2 ? 39 : s == 3 ? 55 : 27;
 }
 __host__ __device__ constexpr int flops_diff_extra(int s) {

@@ -163,8 +163,8 @@ extern "C" __global__ void __launch_bounds__(ADMIT_WARPS * 32) wave_admit_kernel
 // Each pass warp streams its FP32 lists through a ring of RING_STAGES stages
 // in its shared memory: lane 0 keeps up to RING_STAGES bulk copies in flight,
 // so the site arithmetic reads shared memory while HBM fills the stages ahead.
-constexpr int RING_STAGES = 8;
-constexpr int STAGE_F4 = 64;                  // float4 per stage: two per lane
+constexpr int RING_STAGES = 4;
+constexpr int STAGE_F4 = 128;                 // float4 per stage: four per lane
 constexpr int STAGE_ELEMS = STAGE_F4 * 4;     // list entries per stage
 static_assert(RING_STAGES * STAGE_F4 * 16 <= WARP_SMEM_BUF, "ring must fit the warp's buffer");
 static_assert(sizeof(Coef32) + RING_STAGES * 8 <= WARP_SMEM_COEF, "coefficients and barriers must fit");
@@ -182,16 +182,18 @@ __device__ __forceinline__ void ring_issue(const Ring& R, const float* L, int64_
     bulk_load(R.buf + slot * STAGE_F4, L + e0, bytes, &R.bar[slot]);
 }
 
-// The FP32 stream of stream32 fed from the ring: the same lane-to-site
-// assignment (stage i holds float4 64 i .. 64 i + 63; lane l takes 64 i + l
-// and 64 i + 32 + l) and the same summation order, so the sums are identical.
-// L and every stage start are 16-byte aligned (list starts are multiples of
-// four entries); a stage's copy rounds its size up to 16 bytes, which stays
-// inside the slot's list buffer.  Returns false if a wait ran out.
+// One shape's FP32 list from the ring.  Stage i holds float4 128 i .. 128 i +
+// 127; lane l takes 128 i + 32 j + l (j = 0..3), in two steps of 8 sites
+// after each of which the FP32 gradient and objective partials go to FP64
+// (the Hessian partials every HESS_FLUSH steps).  L and every stage start are
+// 16-byte aligned (list starts are multiples of four entries); a stage's copy
+// rounds its size up to 16 bytes, which stays inside the slot's list buffer.
+// The sums use the hi coefficients only (lo_correction restores the rest).
+// Returns false if a wait ran out.
 template <int S>
 __device__ __noinline__ bool stream32_ring(const float* __restrict__ L, int64_t len, const Coef32* K,
                                            bool diff, int lane, Ring& R, LaneSums& out) {
-    using E = Shape32<S>;
+    using E = Shape32<S, false>;
     constexpr int NG = E::NG, NH = E::NH, GOFF = E::GOFF, HOFF = E::HOFF;
     E ev;
     ev.load(K, diff);
@@ -203,45 +205,48 @@ __device__ __noinline__ bool stream32_ring(const float* __restrict__ L, int64_t 
     for (int i = 0; i < NH; i++) { H[i] = 0.0; h[i] = 0.f; }
     const int64_t n4 = len >> 2;
     const int nst = (int)((len + STAGE_ELEMS - 1) / STAGE_ELEMS);
+    const uint32_t seq0 = R.seq;
     if (lane == 0) {
         const int pro = min(nst, RING_STAGES);
         fence_proxy_async_smem();
-        for (int i = 0; i < pro; i++) ring_issue(R, L, len, i, (R.seq + i) % RING_STAGES);
+        for (int i = 0; i < pro; i++) ring_issue(R, L, len, i, (seq0 + i) % RING_STAGES);
     }
     bool ok = true;
     int it = 0, done = 0;
     for (int i = 0; i < nst; i++) {
-        const uint32_t q = R.seq + i;
+        const uint32_t q = seq0 + i;
         const uint32_t slot = q % RING_STAGES;
         if (!mbar_wait(&R.bar[slot], (q / RING_STAGES) & 1u)) { ok = false; break; }
         done = i + 1;
         const float4* B = R.buf + slot * STAGE_F4;
         const int64_t k = (int64_t)i * STAGE_F4 + lane;
-        float g[NG], ob = 0.f;
 #pragma unroll
-        for (int j = 0; j < NG; j++) g[j] = 0.f;
-        if (k < n4) {
-            const float4 v = B[lane];
-            ev.site(v.x, g, ob, h);
-            ev.site(v.y, g, ob, h);
-            ev.site(v.z, g, ob, h);
-            ev.site(v.w, g, ob, h);
-        }
-        if (k + 32 < n4) {
-            const float4 v = B[lane + 32];
-            ev.site(v.x, g, ob, h);
-            ev.site(v.y, g, ob, h);
-            ev.site(v.z, g, ob, h);
-            ev.site(v.w, g, ob, h);
-        }
-        if (k < n4) {
+        for (int half = 0; half < 2; half++) {
+            const int64_t kh = k + 64 * half;
+            if (kh < n4) {
+                float g[NG], ob = 0.f;
 #pragma unroll
-            for (int j = 0; j < NG; j++) G[j] += (double)g[j];
-            F += (double)ob;
-            if (++it == HESS_FLUSH) {
+                for (int j = 0; j < NG; j++) g[j] = 0.f;
+                const float4 va = B[lane + 64 * half];
+                ev.site(va.x, g, ob, h);
+                ev.site(va.y, g, ob, h);
+                ev.site(va.z, g, ob, h);
+                ev.site(va.w, g, ob, h);
+                if (kh + 32 < n4) {
+                    const float4 vb = B[lane + 64 * half + 32];
+                    ev.site(vb.x, g, ob, h);
+                    ev.site(vb.y, g, ob, h);
+                    ev.site(vb.z, g, ob, h);
+                    ev.site(vb.w, g, ob, h);
+                }
 #pragma unroll
-                for (int j = 0; j < NH; j++) { H[j] += (double)h[j]; h[j] = 0.f; }
-                it = 0;
+                for (int j = 0; j < NG; j++) G[j] += (double)g[j];
+                F += (double)ob;
+                if (++it == HESS_FLUSH) {
+#pragma unroll
+                    for (int j = 0; j < NH; j++) { H[j] += (double)h[j]; h[j] = 0.f; }
+                    it = 0;
+                }
             }
         }
         if (i + RING_STAGES < nst) {
@@ -256,13 +261,13 @@ __device__ __noinline__ bool stream32_ring(const float* __restrict__ L, int64_t 
         // let this warp's copies in flight land before it leaves
         const int issued = min(nst, done + RING_STAGES);
         for (int i = done; i < issued; i++) {
-            const uint32_t q = R.seq + i;
+            const uint32_t q = seq0 + i;
             if (!mbar_wait(&R.bar[q % RING_STAGES], (q / RING_STAGES) & 1u)) break;
         }
         return false;
     }
     if (lane < (int)(len & 3)) {
-        const float* B = reinterpret_cast<const float*>(R.buf + ((R.seq + nst - 1) % RING_STAGES) * STAGE_F4);
+        const float* B = reinterpret_cast<const float*>(R.buf + ((seq0 + nst - 1) % RING_STAGES) * STAGE_F4);
         float g[NG], ob = 0.f;
 #pragma unroll
         for (int j = 0; j < NG; j++) g[j] = 0.f;
@@ -272,7 +277,7 @@ __device__ __noinline__ bool stream32_ring(const float* __restrict__ L, int64_t 
         F += (double)ob;
     }
     __syncwarp();   // every lane has read the ring before the next copies
-    R.seq += nst;
+    R.seq = seq0 + nst;
 #pragma unroll
     for (int j = 0; j < NH; j++) H[j] += (double)h[j];
 #pragma unroll
@@ -295,7 +300,10 @@ __device__ __forceinline__ bool run_unit(const void* lists, bool l64, int64_t of
                              diff, lane, R, ls);
 }
 
-extern "C" __global__ void __launch_bounds__(128, 4) wave_pass_kernel(WaveArgs A) {
+// Five blocks of four warps per SM (at most 102 registers a thread): the site
+// arithmetic hides its latencies with warps rather than with registers.
+constexpr int PASS_MIN_BLOCKS = 5;
+extern "C" __global__ void __launch_bounds__(128, PASS_MIN_BLOCKS) wave_pass_kernel(WaveArgs A) {
     extern __shared__ __align__(16) char smem[];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     char* wsm = smem + wib * WARP_SMEM;
@@ -385,8 +393,8 @@ __device__ inline void finish_slot(const WaveArgs& A, SlotState& S, int s, const
         unsigned long long f32 = 0, f64 = 0;
         for (int sh = 0; sh < 5; sh++) {
             atomicAdd(&C->shape_sites[sh], (unsigned long long)S.cnt[sh]);
-            f32 += (unsigned long long)S.cnt[sh] * (unsigned long long)(p32 * flops_direct(sh) + S.diffp * flops_diff_extra(sh));
-            f64 += (unsigned long long)S.cnt[sh] * (unsigned long long)(S.f64p * flops_direct(sh));
+            f32 += (unsigned long long)S.cnt[sh] * (unsigned long long)(p32 * flops_fp32_hi(sh) + S.diffp * flops_diff_extra(sh));
+            f64 += (unsigned long long)S.cnt[sh] * (unsigned long long)(S.f64p * flops_fp64(sh));
         }
         atomicAdd(&C->flops_fp32, f32);
         atomicAdd(&C->flops_fp64, f64);
@@ -446,10 +454,17 @@ extern "C" __global__ void __launch_bounds__(128) wave_solve_kernel(WaveArgs A) 
     __syncwarp();
     const int kind = S.kind;
     const double n = (double)S.n;
+    double corr = 0.0;
+    if (kind != PASS_FP64) {
+        // FP32 passes ran on the hi coefficients
+        if (lane == 0) mom_s[NMOM + 1] = lo_correction(mom_s, S.c32);
+        __syncwarp();
+        corr = mom_s[NMOM + 1];
+    }
     const double obj = mom_s[NMOM];
     double ft;
     if (kind == PASS_FP64) ft = -obj / n;
-    else if (kind == PASS_FP32_DIRECT) ft = -(obj * 0.69314718055994530942) / n;
+    else if (kind == PASS_FP32_DIRECT) ft = -(obj * 0.69314718055994530942 + corr) / n;
     else ft = S.f - obj / n;
     double gt[9], Ht[9];
     {
@@ -589,7 +604,7 @@ int run_waves(const std::vector<PairJob>& jobs, const RunConfig& cfg, Workspace&
                             sizeof(SlotState) + 4 * sizeof(int) + 2 * 5 * shape_units * sizeof(int2);
     size_t fr = 0, tot = 0;
     KG_WAVE_TRY(cudaMemGetInfo(&fr, &tot));
-    int64_t want = cfg.slots > 0 ? cfg.slots : 8192;
+    int64_t want = cfg.slots > 0 ? cfg.slots : 16384;
     int64_t by_mem = (int64_t)((fr / 2) / per_slot);
     int64_t n_slots = std::max<int64_t>(1, std::min<int64_t>({want, by_mem, total_pairs}));
     const int64_t task_cap = n_slots * shape_units;
