@@ -282,7 +282,7 @@ def main():
             "phases_ms": dict(zip(("admit", "pass", "solve", "waves_total"),
                                   [float(v) for v in np.mean(np.array(phases), axis=0)])),
             "stats": {k: stats[k] for k in ("gh_passes", "fp64_passes", "fp64_pairs", "pair_sites",
-                                            "work_units", "shape_sites", "waves", "slots",
+                                            "work_units", "shape_sites", "waves", "slots", "nonconverged",
                                             "flops_fp64")}}
     if rank == 0 and not args.no_cpu and world == 1:
         line["cpu_baseline"] = cpu_baseline(codes, cohort.planted, args.cpu_seconds)

@@ -221,6 +221,7 @@ typedef struct {
     uint64_t flops_fp32;       /* executed FP32 site arithmetic (FMA = 2) */
     uint64_t flops_fp64;       /* executed FP64 site arithmetic */
     uint64_t shape_sites[5];   /* pair-sites per genotype-pair shape A,B1,B2,C,D */
+    uint64_t nonconverged;     /* pairs that stopped at the iteration limit */
     uint64_t waves;            /* admit / pass / solve waves of the pair engine */
     uint64_t slots;            /* pairs in flight per wave */
     double admit_ms;           /* CUDA-event time of the admit kernels (list build) */

@@ -42,6 +42,7 @@ class KgRunStats(ctypes.Structure):
                 ("pair_sites", ctypes.c_uint64), ("work_units", ctypes.c_uint64),
                 ("launches", ctypes.c_uint64), ("flops_fp32", ctypes.c_uint64),
                 ("flops_fp64", ctypes.c_uint64), ("shape_sites", ctypes.c_uint64 * 5),
+                ("nonconverged", ctypes.c_uint64),
                 ("waves", ctypes.c_uint64), ("slots", ctypes.c_uint64),
                 ("admit_ms", ctypes.c_double), ("pass_ms", ctypes.c_double),
                 ("solve_ms", ctypes.c_double), ("pair_kernel_ms", ctypes.c_double), ("device_ms", ctypes.c_double),

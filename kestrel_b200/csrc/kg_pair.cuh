@@ -399,8 +399,8 @@ constexpr int HESS_FLUSH = 8;   // loop iterations (8 sites each) between FP32 -
 // The FP32 closed form of one shape: coefficients of the pending pass (from
 // shared memory) and the per-site update of the FP32 partial sums.  The
 // moments share their products: with u = r c (c = t for A, w otherwise) the
-// gradient terms are u times powers of the shape's monomials and every Hessian
-// term is a product of two gradient terms.
+// gradient terms are u times the shape's monomials (each summed by one FMA,
+// a single rounding) and every Hessian term is a product of two of them.
 //
 // LO = true evaluates L.Delta with the hi + lo split coefficients (the FP64
 // iterate to ~1e-14); LO = false uses the hi parts only, and the solve step
@@ -443,7 +443,7 @@ struct Shape32 {
             d = fmaf(t, ph, EPS);
             r = rcp_nr(d);
             const float u = r * t, v1 = u * t, v2 = v1 * t, v3 = v2 * t;   // r t^1..4
-            g[0] += u; g[1] += v1; g[2] += v2; g[3] += v3;
+            g[0] += u; g[1] = fmaf(u, t, g[1]); g[2] = fmaf(v1, t, g[2]); g[3] = fmaf(v2, t, g[3]);
             h[0] = fmaf(u, u, h[0]); h[1] = fmaf(u, v1, h[1]); h[2] = fmaf(v1, v1, h[2]);
             h[3] = fmaf(v1, v2, h[3]); h[4] = fmaf(v2, v2, h[4]); h[5] = fmaf(v2, v3, h[5]);
             h[6] = fmaf(v3, v3, h[6]);
@@ -455,7 +455,7 @@ struct Shape32 {
             d = fmaf(w, ph, EPS);
             r = rcp_nr(d);
             const float v = r * w, v1 = v * t, v2 = v1 * t;                 // r w t^0..2
-            g[0] += v; g[1] += v1; g[2] += v2;
+            g[0] += v; g[1] = fmaf(v, t, g[1]); g[2] = fmaf(v1, t, g[2]);
             h[0] = fmaf(v, v, h[0]); h[1] = fmaf(v, v1, h[1]); h[2] = fmaf(v1, v1, h[2]);
             h[3] = fmaf(v1, v2, h[3]); h[4] = fmaf(v2, v2, h[4]);
             c = w;
@@ -467,7 +467,7 @@ struct Shape32 {
             d = fmaf(w, ph, EPS);
             r = rcp_nr(d);
             const float v = r * w, a = v * ty, b = v * t, e = v * w;          // r w {1, ty, t, w}
-            g[0] += v; g[1] += a; g[2] += b; g[3] += e;
+            g[0] += v; g[1] = fmaf(v, ty, g[1]); g[2] = fmaf(v, t, g[2]); g[3] = fmaf(v, w, g[3]);
             h[0] = fmaf(v, v, h[0]); h[1] = fmaf(v, a, h[1]); h[2] = fmaf(v, b, h[2]);
             h[3] = fmaf(v, e, h[3]); h[4] = fmaf(a, a, h[4]); h[5] = fmaf(b, b, h[5]);
             h[6] = fmaf(e, a, h[6]); h[7] = fmaf(e, b, h[7]); h[8] = fmaf(e, e, h[8]);
@@ -479,7 +479,7 @@ struct Shape32 {
             d = fmaf(w, ph, EPS);
             r = rcp_nr(d);
             const float v = r * w, a = v * w;                                // r w {1, w}
-            g[0] += v; g[1] += a;
+            g[0] += v; g[1] = fmaf(v, w, g[1]);
             h[0] = fmaf(v, v, h[0]); h[1] = fmaf(v, a, h[1]); h[2] = fmaf(a, a, h[2]);
             c = w;
         }

@@ -737,6 +737,7 @@ int run_waves(const std::vector<PairJob>& jobs, const RunConfig& cfg, Workspace&
     stats.flops_fp32 = rc.flops_fp32;
     stats.flops_fp64 = rc.flops_fp64;
     for (int k = 0; k < 5; k++) stats.shape_sites[k] = rc.shape_sites[k];
+    stats.nonconverged = rc.nonconverged;
     stats.waves = waves;
     stats.slots = (uint64_t)n_slots;
     stats.admit_ms = phase[0];
