@@ -23,6 +23,111 @@ constexpr int WAVE_WPB = 4;   // warps per block of the three wave kernels
 // ------------------------------------------------------------------ admit
 
 constexpr int ADMIT_WARPS = 8;   // warps that build one pair's lists together
+constexpr int ADMIT_WARP_SMEM = UNIT_SITES * 8;   // frequency stage + FP32 output buffer (FP64: stage)
+
+// Writes the frequency value t (p or 1 - p by the site's sel bit) of every
+// jointly observed site of units [u0, u1) into its shape list, in site order,
+// starting at off[] in each list.  Lane l owns word l of a unit (sites 32 l ..
+// 32 l + 31): it forms the word's code planes (code = shape + 1 in three bit
+// planes) and the exclusive prefix of the shape counts over the lanes, then
+// steps through its 32 bits in lockstep with the other lanes (no divergence),
+// keeping its five write positions packed 11 bits apiece in one 64-bit word.
+// The unit's frequencies are staged in shared memory transposed (site 32 l + i
+// at [32 i + l], conflict-free); FP32 values go through a shared output buffer
+// so the global stores are coalesced, FP64 values are stored directly.
+template <class T>
+__device__ inline void scatter_lockstep(const CohortDev& co, int64_t x, int64_t y, int lane, int u0, int u1,
+                                        const int64_t* off0, T* lists, char* wsm) {
+    const uint2* px = co.planes_x + x * co.plane_stride;
+    const uint2* py = co.planes_y + y * co.plane_stride;
+    T* stage = reinterpret_cast<T*>(wsm);                                        // UNIT_SITES values
+    float* obuf = reinterpret_cast<float*>(wsm + UNIT_SITES * sizeof(float));   // FP32 only
+    int64_t off[5];
+#pragma unroll
+    for (int k = 0; k < 5; k++) off[k] = off0[k];
+    for (int u = u0; u < u1; u++) {
+        const uint2 X = px[u * UNIT_WORDS + lane], Y = py[u * UNIT_WORDS + lane];
+        if (sizeof(T) == 4) {
+            const float4* src = reinterpret_cast<const float4*>(co.p32 + (int64_t)u * UNIT_SITES + lane * 32);
+#pragma unroll
+            for (int v4 = 0; v4 < 8; v4++) {
+                const float4 f = src[v4];
+                float* st = reinterpret_cast<float*>(stage) + (v4 * 4) * 32 + lane;
+                st[0] = f.x; st[32] = f.y; st[64] = f.z; st[96] = f.w;
+            }
+        } else {
+            const double2* src = reinterpret_cast<const double2*>(co.p64 + (int64_t)u * UNIT_SITES + lane * 32);
+#pragma unroll
+            for (int v2 = 0; v2 < 16; v2++) {
+                const double2 f = src[v2];
+                double* st = reinterpret_cast<double*>(stage) + (v2 * 2) * 32 + lane;
+                st[0] = f.x; st[32] = f.y;
+            }
+        }
+        const ShapeMasks sm = shape_masks(X, Y);
+        unsigned c0 = sm.m[0] | sm.m[2] | sm.m[4];   // A 1, B1 2, B2 3, C 4, D 5
+        unsigned c1 = sm.m[1] | sm.m[2];
+        unsigned c2 = sm.m[3] | sm.m[4];
+        unsigned sl = sm.sel;
+        unsigned long long v = 0;
+#pragma unroll
+        for (int k = 0; k < 5; k++) v |= (unsigned long long)__popc(sm.m[k]) << (11 * k);
+        unsigned long long inc = v;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned long long t = __shfl_up_sync(0xffffffffu, inc, o);
+            if (lane >= o) inc += t;
+        }
+        const unsigned long long tot = __shfl_sync(0xffffffffu, inc, 31);
+        // unit-local write positions: shape starts in the unit plus this lane's prefix
+        unsigned long long ust = 0;
+        {
+            unsigned acc = 0;
+#pragma unroll
+            for (int k = 0; k < 5; k++) {
+                ust |= (unsigned long long)acc << (11 * k);
+                acc += (unsigned)((tot >> (11 * k)) & 0x7FFull);
+            }
+        }
+        unsigned long long Q = (sizeof(T) == 4 ? ust : 0ull) + (inc - v);
+        __syncwarp();
+#pragma unroll 8
+        for (int i = 0; i < 32; i++) {
+            const int code = (int)((c0 & 1u) | ((c1 & 1u) << 1) | ((c2 & 1u) << 2));
+            const bool flip = (sl & 1u) != 0;
+            c0 >>= 1; c1 >>= 1; c2 >>= 1; sl >>= 1;
+            if (code) {
+                const int sh = 11 * (code - 1);
+                const int pos = (int)((Q >> sh) & 0x7FFull);
+                Q += 1ull << sh;
+                const T p = stage[i * 32 + lane];
+                const T t = flip ? (T)1 - p : p;
+                if (sizeof(T) == 4) {
+                    obuf[pos] = (float)t;
+                } else {
+                    const int k = code - 1;
+                    const int64_t o = k == 0 ? off[0] : k == 1 ? off[1] : k == 2 ? off[2] : k == 3 ? off[3] : off[4];
+                    lists[o + pos] = t;
+                }
+            }
+        }
+        __syncwarp();
+        if (sizeof(T) == 4) {
+            unsigned a = 0;
+#pragma unroll
+            for (int k = 0; k < 5; k++) {
+                const unsigned nk = (unsigned)((tot >> (11 * k)) & 0x7FFull);
+                float* dst = reinterpret_cast<float*>(lists) + off[k];
+                const float* srcb = obuf + a;
+                for (unsigned j = lane; j < nk; j += 32) dst[j] = srcb[j];
+                a += nk;
+            }
+            __syncwarp();
+        }
+#pragma unroll
+        for (int k = 0; k < 5; k++) off[k] += (int64_t)((tot >> (11 * k)) & 0x7FFull);
+    }
+}
 
 // Each warp of the block takes a contiguous eighth of the pair's 1024-site
 // units: it counts its sites per shape, the block turns the counts into write
@@ -65,18 +170,18 @@ __device__ inline int64_t build_lists(const CohortDev& co, int64_t x, int64_t y,
         st = align4(st + tot);
         n += tot;
     }
-    if (n > 0) scatter_units<T>(co, x, y, lane, u0, u1, off, lists, wsm);
+    if (n > 0) scatter_lockstep<T>(co, x, y, lane, u0, u1, off, lists, wsm);
     __syncthreads();   // cnt is reused by the block's next pair
     return n;
 }
 
-extern "C" __global__ void __launch_bounds__(ADMIT_WARPS * 32) wave_admit_kernel(WaveArgs A) {
-    extern __shared__ __align__(16) char smem[];
+extern "C" __global__ void __launch_bounds__(ADMIT_WARPS * 32, 4) wave_admit_kernel(WaveArgs A) {
     __shared__ int sh_e;
     __shared__ unsigned long long sh_k;
     __shared__ unsigned cnt[ADMIT_WARPS][5];
+    extern __shared__ __align__(16) char smem[];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    char* wsm = smem + w * WARP_SMEM;
+    char* wsm = smem + w * ADMIT_WARP_SMEM;
     const int nfree = A.wc_cur->n_free;
     for (;;) {
         if (threadIdx.x == 0) sh_e = atomicAdd(A.admit_task, 1);
@@ -642,7 +747,7 @@ int run_waves(const std::vector<PairJob>& jobs, const RunConfig& cfg, Workspace&
     if (!attr) {
         KG_WAVE_TRY(cudaFuncSetAttribute(wave_pass_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 4 * WARP_SMEM));
         KG_WAVE_TRY(cudaFuncSetAttribute(wave_admit_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         ADMIT_WARPS * WARP_SMEM));
+                                         ADMIT_WARPS * ADMIT_WARP_SMEM));
         attr = true;
     }
     int occ = 0;
@@ -655,7 +760,7 @@ int run_waves(const std::vector<PairJob>& jobs, const RunConfig& cfg, Workspace&
     const int pass_blocks = ws.sm_count * occ;
     int aocc = 0;
     KG_WAVE_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&aocc, wave_admit_kernel, ADMIT_WARPS * 32,
-                                                              ADMIT_WARPS * WARP_SMEM));
+                                                              ADMIT_WARPS * ADMIT_WARP_SMEM));
     if (aocc <= 0) {
         err = "admit kernel cannot be resident";
         return KG_ECUDA;
@@ -701,7 +806,7 @@ int run_waves(const std::vector<PairJob>& jobs, const RunConfig& cfg, Workspace&
         KG_WAVE_TRY(cudaMemsetAsync(admit_task, 0, sizeof(int), st));
         KG_WAVE_TRY(cudaMemsetAsync(q + 1, 0, sizeof(unsigned long long), st));
         KG_WAVE_TRY(cudaMemsetAsync(wc + nxt, 0, sizeof(WaveCounts), st));
-        wave_admit_kernel<<<admit_blocks, ADMIT_WARPS * 32, ADMIT_WARPS * WARP_SMEM, st>>>(A);
+        wave_admit_kernel<<<admit_blocks, ADMIT_WARPS * 32, ADMIT_WARPS * ADMIT_WARP_SMEM, st>>>(A);
         KG_WAVE_TRY(cudaEventRecord(ev[1], st));
         wave_pass_kernel<<<pass_blocks, 128, wsm, st>>>(A);
         KG_WAVE_TRY(cudaEventRecord(ev[2], st));
