@@ -20,9 +20,9 @@
 // FP64.  f = -(1/n) sum log(eps + L.D), g = -(1/n) sum L r, H = (1/n) sum L L' r^2
 // with r = 1/(eps + L.D) (src/jacquard/objective.rs:9-20, grad_hess.rs:13-41).
 //
-// Precision (KG_PREC_FP32C): per-site terms in FP32 with MUFU rcp/lg2 plus a
-// Newton step, the pair's coefficients split hi+lo so the evaluation point is
-// the exact FP64 iterate, FP32 partial sums promoted to FP64 per segment, and
+// Precision (KG_PREC_FP32C): per-site terms in FP32 with MUFU rcp/lg2 (one lg2
+// per four sites), the pair's coefficients split hi+lo so the evaluation point
+// is the exact FP64 iterate, FP32 partial sums promoted to FP64 per segment, and
 // near convergence the objective change is summed directly as
 // log(d_new/d_old) = -log1p(-delta/d_new) so the Armijo test (src/sqp.rs:294)
 // keeps its resolution.  The 9x9 QP, LDL^T, KKT and condition estimate are
@@ -95,11 +95,11 @@ struct PairLaunch {
 
 // ------------------------------------------------------------ FP32 helpers
 
-__device__ __forceinline__ float rcp_nr(float d) {
+// MUFU reciprocal: at most 1 ulp from 1 / d over the whole FP32 range.
+__device__ __forceinline__ float rcp_approx(float d) {
     float r;
     asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(d));
-    float e = fmaf(-d, r, 1.0f);
-    return fmaf(r, e, r);
+    return r;
 }
 
 __device__ __forceinline__ float lg2_approx(float a) {
@@ -433,15 +433,16 @@ struct Shape32 {
         }
     }
 
-    // one site: adds into the FP32 partials g, ob (per iteration) and h
-    __device__ __forceinline__ void site(float t, float* g, float& ob, float* h) const {
+    // one site's gradient and Hessian terms into the FP32 partials g and h;
+    // returns d = L.Delta + eps, r = 1 / d and the site's scale c (t for A,
+    // w for B, C, D)
+    __device__ __forceinline__ void core(float t, float* g, float* h, float& d, float& r, float& c) const {
         const float EPS = 1e-8f;
-        float d, r, c;    // c = the per-site scale: t (A) or w (B, C, D)
         if (S == 0) {
             float ph = fmaf(fmaf(fmaf(k3.h, t, k2.h), t, k1.h), t, k0.h);
             if (LO) ph = ph + fmaf(fmaf(fmaf(k3.l, t, k2.l), t, k1.l), t, k0.l);
             d = fmaf(t, ph, EPS);
-            r = rcp_nr(d);
+            r = rcp_approx(d);
             const float u = r * t, v1 = u * t, v2 = v1 * t, v3 = v2 * t;   // r t^1..4
             g[0] += u; g[1] = fmaf(u, t, g[1]); g[2] = fmaf(v1, t, g[2]); g[3] = fmaf(v2, t, g[3]);
             h[0] = fmaf(u, u, h[0]); h[1] = fmaf(u, v1, h[1]); h[2] = fmaf(v1, v1, h[2]);
@@ -453,7 +454,7 @@ struct Shape32 {
             float ph = fmaf(fmaf(k2.h, t, k1.h), t, k0.h);
             if (LO) ph = ph + fmaf(fmaf(k2.l, t, k1.l), t, k0.l);
             d = fmaf(w, ph, EPS);
-            r = rcp_nr(d);
+            r = rcp_approx(d);
             const float v = r * w, v1 = v * t, v2 = v1 * t;                 // r w t^0..2
             g[0] += v; g[1] = fmaf(v, t, g[1]); g[2] = fmaf(v1, t, g[2]);
             h[0] = fmaf(v, v, h[0]); h[1] = fmaf(v, v1, h[1]); h[2] = fmaf(v1, v1, h[2]);
@@ -465,7 +466,7 @@ struct Shape32 {
             float ph = fmaf(w, k3.h, fmaf(t, k2.h, fmaf(ty, k1.h, k0.h)));
             if (LO) ph = ph + fmaf(w, k3.l, fmaf(t, k2.l, fmaf(ty, k1.l, k0.l)));
             d = fmaf(w, ph, EPS);
-            r = rcp_nr(d);
+            r = rcp_approx(d);
             const float v = r * w, a = v * ty, b = v * t, e = v * w;          // r w {1, ty, t, w}
             g[0] += v; g[1] = fmaf(v, ty, g[1]); g[2] = fmaf(v, t, g[2]); g[3] = fmaf(v, w, g[3]);
             h[0] = fmaf(v, v, h[0]); h[1] = fmaf(v, a, h[1]); h[2] = fmaf(v, b, h[2]);
@@ -477,21 +478,48 @@ struct Shape32 {
             float ph = fmaf(w, k1.h, k0.h);
             if (LO) ph = ph + fmaf(w, k1.l, k0.l);
             d = fmaf(w, ph, EPS);
-            r = rcp_nr(d);
+            r = rcp_approx(d);
             const float v = r * w, a = v * w;                                // r w {1, w}
             g[0] += v; g[1] = fmaf(v, w, g[1]);
             h[0] = fmaf(v, v, h[0]); h[1] = fmaf(v, a, h[1]); h[2] = fmaf(a, a, h[2]);
             c = w;
         }
+    }
+
+    // the site's objective term in diff mode: -log(1 - delta / d_new)
+    __device__ __forceinline__ float diff_term(float t, float r, float c) const {
+        float dl;
+        if (S == 0) dl = t * fmaf(fmaf(fmaf(s3, t, s2), t, s1), t, s0);
+        else if (S == 1 || S == 2) dl = c * fmaf(fmaf(s2, t, s1), t, s0);
+        else if (S == 3) dl = c * fmaf(c, s3, fmaf(t, s2, fmaf(1.0f - t, s1, s0)));
+        else dl = c * fmaf(c, s1, s0);
+        return neg_log1m(dl * r);
+    }
+
+    // one site: adds into the FP32 partials g, ob (per iteration) and h
+    __device__ __forceinline__ void site(float t, float* g, float& ob, float* h) const {
+        float d, r, c;
+        core(t, g, h, d, r, c);
+        if (!diff) ob += lg2_approx(d);
+        else ob += diff_term(t, r, c);
+    }
+
+    // four sites (one float4): in direct mode one lg2 of the product of the
+    // four d (each d lies in [1e-8, 1 + 1e-8], so the product stays a normal
+    // FP32 number)
+    __device__ __forceinline__ void site4(float4 v, float* g, float& ob, float* h) const {
+        float d0, d1, d2, d3, r0, r1, r2, r3, c0, c1, c2, c3;
+        core(v.x, g, h, d0, r0, c0);
+        core(v.y, g, h, d1, r1, c1);
+        core(v.z, g, h, d2, r2, c2);
+        core(v.w, g, h, d3, r3, c3);
         if (!diff) {
-            ob += lg2_approx(d);
+            ob += lg2_approx((d0 * d1) * (d2 * d3));
         } else {
-            float dl;
-            if (S == 0) dl = t * fmaf(fmaf(fmaf(s3, t, s2), t, s1), t, s0);
-            else if (S == 1 || S == 2) dl = c * fmaf(fmaf(s2, t, s1), t, s0);
-            else if (S == 3) dl = c * fmaf(c, s3, fmaf(t, s2, fmaf(1.0f - t, s1, s0)));
-            else dl = c * fmaf(c, s1, s0);
-            ob += neg_log1m(dl * r);
+            ob += diff_term(v.x, r0, c0);
+            ob += diff_term(v.y, r1, c1);
+            ob += diff_term(v.z, r2, c2);
+            ob += diff_term(v.w, r3, c3);
         }
     }
 };
@@ -882,21 +910,24 @@ struct PairResult {
 };
 
 // Executed site arithmetic per pass and shape (A, B1, B2, C, D), counting an
-// FMA as 2 and a MUFU op as 1, read off Shape32::site and stream64: FP32 passes
-// on the hi coefficients (the wave engine), FP32 passes with the hi + lo
-// polynomial (the single-kernel engine), FP64 passes, and the extra of the
-// log(d_new/d_old) objective.
-__host__ __device__ constexpr int flops_fp32_hi(int s) {
-    return s == 0 ? 37 : s == 1 ? 31 : s == 2 ? 31 : s == 3 ? 43 : 23;
+// FMA as 2 and a MUFU op as 1, read off Shape32 and stream64.  The wave engine
+// (hi coefficients, one lg2 per four sites) is counted per four sites, with the
+// extra of the log(d_new/d_old) objective beside it; the single-kernel engine
+// (hi + lo polynomial, one lg2 per site) and FP64 passes per site.
+__host__ __device__ constexpr int flops4_fp32_hi(int s) {
+    return s == 0 ? 141 : s == 1 ? 113 : s == 2 ? 113 : s == 3 ? 165 : 77;
+}
+__host__ __device__ constexpr int flops4_diff_extra(int s) {
+    return s == 0 ? 75 : s == 1 ? 67 : s == 2 ? 67 : s == 3 ? 79 : 59;
 }
 __host__ __device__ constexpr int flops_fp32_lo(int s) {
-    return s == 0 ? 44 : s == 1 ? 36 : s == 2 ? 36 : s == 3 ? 50 : 26;
+    return s == 0 ? 43 : s == 1 ? 34 : s == 2 ? 34 : s == 3 ? 49 : 23;
 }
 __host__ __device__ constexpr int flops_fp64(int s) {
     return s == 0 ? 50 : s == 1 ? 39 : s == 2 ? 39 : s == 3 ? 55 : 27;
 }
 __host__ __device__ constexpr int flops_diff_extra(int s) {
-    return s == 0 ? 18 : s == 1 ? 16 : s == 2 ? 16 : s == 3 ? 18 : 14;
+    return s == 0 ? 18 : s == 1 ? 16 : s == 2 ? 16 : s == 3 ? 19 : 14;
 }
 
 // Condition estimate from the row-distributed Hessian (once per pair).

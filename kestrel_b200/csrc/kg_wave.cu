@@ -332,18 +332,8 @@ __device__ __noinline__ bool stream32_ring(const float* __restrict__ L, int64_t 
                 float g[NG], ob = 0.f;
 #pragma unroll
                 for (int j = 0; j < NG; j++) g[j] = 0.f;
-                const float4 va = B[lane + 64 * half];
-                ev.site(va.x, g, ob, h);
-                ev.site(va.y, g, ob, h);
-                ev.site(va.z, g, ob, h);
-                ev.site(va.w, g, ob, h);
-                if (kh + 32 < n4) {
-                    const float4 vb = B[lane + 64 * half + 32];
-                    ev.site(vb.x, g, ob, h);
-                    ev.site(vb.y, g, ob, h);
-                    ev.site(vb.z, g, ob, h);
-                    ev.site(vb.w, g, ob, h);
-                }
+                ev.site4(B[lane + 64 * half], g, ob, h);
+                if (kh + 32 < n4) ev.site4(B[lane + 64 * half + 32], g, ob, h);
 #pragma unroll
                 for (int j = 0; j < NG; j++) G[j] += (double)g[j];
                 F += (double)ob;
@@ -498,10 +488,10 @@ __device__ inline void finish_slot(const WaveArgs& A, SlotState& S, int s, const
         unsigned long long f32 = 0, f64 = 0;
         for (int sh = 0; sh < 5; sh++) {
             atomicAdd(&C->shape_sites[sh], (unsigned long long)S.cnt[sh]);
-            f32 += (unsigned long long)S.cnt[sh] * (unsigned long long)(p32 * flops_fp32_hi(sh) + S.diffp * flops_diff_extra(sh));
+            f32 += (unsigned long long)S.cnt[sh] * (unsigned long long)(p32 * flops4_fp32_hi(sh) + S.diffp * flops4_diff_extra(sh));
             f64 += (unsigned long long)S.cnt[sh] * (unsigned long long)(S.f64p * flops_fp64(sh));
         }
-        atomicAdd(&C->flops_fp32, f32);
+        atomicAdd(&C->flops_fp32, f32 / 4);
         atomicAdd(&C->flops_fp64, f64);
         S.status = SLOT_FREE;
         A.free_next[atomicAdd(&A.wc_next->n_free, 1)] = s;
