@@ -48,6 +48,11 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--slots", type=int, default=0, help="pairs in flight per wave (0 = automatic)")
     ap.add_argument("--pass-bps", type=int, default=0, help="site-pass blocks per SM (0 = automatic)")
+    ap.add_argument("--workload", default="allpairs", choices=["allpairs", "batch", "inbred", "serving"],
+                    help="allpairs: N x M all pairs (the headline); batch: 8 uneven cohorts in one "
+                         "launch; inbred: N=512 x M=50k inbred stress; serving: panel + Poisson "
+                         "query stream (p50/p99 latency)")
+    ap.add_argument("--requests", type=int, default=64, help="serving: number of requests")
     return ap.parse_args()
 
 
@@ -114,6 +119,24 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def max_over_ranks(value: float, pg, device: str) -> float:
+    """The largest of every rank's value (one all-reduce; every rank calls it in
+    the same order).  pg is torch.distributed or None for one process; device is
+    where the reduction tensor lives (a CUDA device for NCCL, "cpu" for gloo)."""
+    if pg is None:
+        return float(value)
+    import torch
+    t = torch.tensor([float(value)], device=device, dtype=torch.float64)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(pairs_per_rank: int, world: int, ms_per_step: float) -> float:
+    """Pairs per second of the whole job: every rank runs its own replica of the
+    workload, timed by the slowest rank."""
+    return world * pairs_per_rank / (ms_per_step * 1e-3)
+
+
 def measured_hbm_peak():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
@@ -175,9 +198,128 @@ def run_reference(args, codes, planted):
     print(json.dumps(line), flush=True)
 
 
+def run_batch(args, local):
+    """Eight cohorts of uneven N, M and missingness in one launch."""
+    import kestrel_b200 as kb
+    from kestrel_b200 import synth
+    cohorts = synth.config2()
+    pairs = sum(c.codes.shape[0] * (c.codes.shape[0] - 1) // 2 for c in cohorts)
+    est = kb.Estimator(device=local, precision=args.precision)
+    est.set_launch(args.slots, args.pass_bps)
+    inputs = [(c.codes,) for c in cohorts]
+    for _ in range(max(1, args.warmup)):
+        est.relatedness_batch(inputs)
+    wall, waves_ms, st = [], [], None
+    for _ in range(max(1, args.steps)):
+        t0 = time.perf_counter()
+        est.relatedness_batch(inputs)
+        wall.append(time.perf_counter() - t0)
+        st = est.run_stats()
+        waves_ms.append(st["pair_kernel_ms"])
+    est.close()
+    tw = float(np.mean(wall))
+    return {"metric": "all-pairs/s, 8 uneven cohorts in one launch", "value": pairs / tw, "unit": "pairs/s",
+            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": tw * 1e3,
+            "higher_is_better": True, "dtype": "f32" if args.precision == "fp32c" else "f64",
+            "data": "synthetic",
+            "config": {"workload": "cohorts N=" + "/".join(str(c.codes.shape[0]) for c in cohorts) +
+                                   " x M=" + "/".join(str(c.codes.shape[1]) for c in cohorts) +
+                                   ", per-sample missingness U(0, 0.2)", "pairs": pairs},
+            "timing": "host wall clock around kg_relatedness_batch (uploads, preparation, waves, rows back)",
+            "waves_ms": float(np.mean(waves_ms)), "waves_pairs_per_s": pairs / (np.mean(waves_ms) * 1e-3),
+            "stats": {k: st[k] for k in ("gh_passes", "fp64_pairs", "waves", "slots", "nonconverged")}}
+
+
+def run_inbred(args, local):
+    """N=512 x M=50k with 128 inbred samples, 32 identical-inbred pairs and a
+    low-information block (ill-conditioned Hessians)."""
+    import kestrel_b200 as kb
+    from kestrel_b200 import synth
+    co = synth.config3()
+    n = co.codes.shape[0]
+    pairs = n * (n - 1) // 2
+    est = kb.Estimator(device=local, precision=args.precision)
+    est.load(co.codes)
+    for _ in range(max(1, args.warmup)):
+        est.relatedness()
+    dev = []
+    for _ in range(max(1, args.steps)):
+        rows = est.relatedness()
+        st = est.run_stats()
+        dev.append(st["device_ms"])
+    est.close()
+    t = float(np.mean(dev))
+    cond = rows["cond"]
+    return {"metric": "all-pairs/s, inbred / ill-conditioned stress", "value": pairs / (t * 1e-3),
+            "unit": "pairs/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": t,
+            "higher_is_better": True, "dtype": "f32" if args.precision == "fp32c" else "f64",
+            "data": "synthetic",
+            "config": {"workload": f"N={n} x M={co.codes.shape[1]}, 128 inbred, 32 identical-inbred pairs, "
+                                   "5,000-site low-information block", "pairs": pairs},
+            "flagged_cond_gt_1e15": int(np.sum(~(np.log10(np.where(cond > 0, cond, np.nan)) <= 15))),
+            "stats": {k: st[k] for k in ("gh_passes", "fp64_pairs", "fp64_passes", "waves", "nonconverged")}}
+
+
+def run_serving(args, local):
+    """A resident 4,096 x 100,000 panel; query batches of 1-64 samples, each with
+    its own site mask, arrive as a Poisson stream at 200 requests/s and are
+    submitted at their arrival times; latency = completion - arrival."""
+    import concurrent.futures as cf
+    import kestrel_b200 as kb
+    from kestrel_b200 import synth
+    panel = synth.config4_panel()
+    reqs = synth.config4_requests(panel, args.requests)
+    warm = synth.config4_requests(panel, 4, seed=7)
+    est = kb.Estimator(device=local, precision=args.precision)
+    est.panel_load(panel.codes)
+    for r in warm:
+        est.wait(est.submit(r["codes"], r["site_mask"]))
+    n_panel = panel.codes.shape[0]
+    done_t = {}
+    pool = cf.ThreadPoolExecutor(max_workers=len(reqs))
+
+    def waiter(rid, i):
+        est.wait(rid)
+        done_t[i] = time.perf_counter()
+
+    futs = []
+    t0 = time.perf_counter()
+    for i, r in enumerate(reqs):
+        delay = t0 + r["arrival_s"] - time.perf_counter()
+        if delay > 0:
+            time.sleep(delay)
+        rid = est.submit(r["codes"], r["site_mask"])
+        futs.append(pool.submit(waiter, rid, i))
+    for f in futs:
+        f.result()
+    pool.shutdown()
+    lat = np.array([(done_t[i] - (t0 + r["arrival_s"])) * 1e3 for i, r in enumerate(reqs)])
+    span = max(done_t.values()) - t0
+    pairs = sum(r["codes"].shape[0] * n_panel for r in reqs)
+    sv = est.serving_stats()
+    est.close()
+    return {"metric": "serving pairs/s; query p50/p99 ms", "value": pairs / span, "unit": "pairs/s",
+            "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+            "n_gpus": 1, "requests": len(reqs), "higher_is_better": True,
+            "dtype": "f32" if args.precision == "fp32c" else "f64", "data": "synthetic",
+            "config": {"workload": f"panel {n_panel} x {panel.codes.shape[1]}, Poisson 200 req/s, 1-64 query "
+                                   "samples, per-request site mask keeping U(0.6, 1.0) of sites",
+                       "pairs": pairs},
+            "timing": "host wall clock from the first arrival to the last completion; latency per request "
+                      "from its arrival time to the return of its kg_wait",
+            "launches": sv["launches"]}
+
+
 def main():
     args = parse()
     rank, world, local = dist_env()
+    if args.workload != "allpairs":
+        import torch
+        torch.cuda.set_device(local)
+        fn = {"batch": run_batch, "inbred": run_inbred, "serving": run_serving}[args.workload]
+        if rank == 0:
+            print(json.dumps(fn(args, local)), flush=True)
+        return
     from kestrel_b200 import synth
     cohort = synth.config1(n_samples=args.samples, n_sites=args.sites)
     codes = cohort.codes
@@ -226,11 +368,8 @@ def main():
     clk = clocks.stop()
     t_step = max(dev_ms) if dev_ms else float("nan")
     t_mean = float(np.mean(dev_ms))
-    if pg:
-        tt = torch.tensor([t_mean], device=f"cuda:{local}", dtype=torch.float64)
-        pg.all_reduce(tt, op=pg.ReduceOp.MAX)
-        t_mean = float(tt.item())
-    value = world * pairs / (t_mean / 1e3)
+    t_mean = max_over_ranks(t_mean, pg, f"cuda:{local}")
+    value = whole_job_rate(pairs, world, t_mean)
     # ---- end to end through the C ABI from host buffers
     e2e = None
     if not args.no_e2e:
@@ -245,29 +384,42 @@ def main():
                 e2.load(codes)
                 e2.relatedness(out=out)
             e2e_ms.append((time.perf_counter() - t0) * 1e3)
-        tm = float(np.mean(e2e_ms))
-        if pg:
-            tt = torch.tensor([tm], device=f"cuda:{local}", dtype=torch.float64)
-            pg.all_reduce(tt, op=pg.ReduceOp.MAX)
-            tm = float(tt.item())
-        e2e = {"value": world * pairs / (tm / 1e3), "unit": "pairs/s",
+        tm = max_over_ranks(float(np.mean(e2e_ms)), pg, f"cuda:{local}")
+        e2e = {"value": whole_job_rate(pairs, world, tm), "unit": "pairs/s",
                "h2d_bytes_per_step": int(codes.nbytes), "d2h_bytes_per_step": int(out.nbytes),
                "ms_per_step": tm, "timing": "host wall clock around the synchronous C-ABI calls "
                                             "(context create, upload, estimate, rows to host)"}
-    # ---- roofline of the site-pass kernel (FP32 CUDA-core bound)
-    peak = ctypes_peak(local)
+    # ---- roofline of the site-pass kernel (FP32 CUDA-core bound; FP64 for the FP64 form)
+    peak32 = ctypes_peak(local)
     kms = float(np.mean(kern_ms))
-    achieved = float(np.mean(fl32)) / (kms * 1e-3) / 1e12
-    ref_equiv = stats["work_units"] * 156.0 / (kms * 1e-3) / 1e12
-    roof = {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-            "frac": achieved / peak if peak else None, "traffic": None,
-            "kernel": "wave_pass_kernel", "kernel_ms": kms,
+    launches = max(1, int(stats["waves"]))           # one pass launch per wave
+    pass_sites = float(stats["work_units"])          # pair-site evaluations of the step
+    fp64_form = args.precision == "fp64"
+    flops = float(stats["flops_fp64"]) if fp64_form else float(np.mean(fl32))
+    peak = (peak32 / 2.0 if peak32 else None) if fp64_form else peak32
+    achieved = flops / (kms * 1e-3) / 1e12
+    ref_equiv = pass_sites * 156.0 / (kms * 1e-3) / 1e12
+    list_bytes = 8.0 if fp64_form else 4.0
+    roof = {"bound": "fp64" if fp64_form else "fp32", "achieved": achieved, "peak": peak,
+            "unit": "TFLOP/s", "frac": achieved / peak if peak else None,
+            # DRAM bytes per pair-site-pass from the ncu capture in
+            # profiles/wave_pass_kernel_N96_M100k.md, times the pair-sites of an
+            # average pass launch of this step
+            "traffic": (PASS_DRAM_BYTES_PER_SITE * pass_sites / launches) if not fp64_form else None,
+            "traffic_unit": "bytes per launch",
+            "algorithmic_bytes": list_bytes * pass_sites / launches,
+            "hbm_achieved_gbs": list_bytes * pass_sites / (kms * 1e-3) / 1e9,
+            "hbm_peak_gbs": measured_hbm_peak(),
+            "kernel": "wave_pass_kernel", "kernel_ms": kms, "launches": launches,
             "kernel_timing": "CUDA events around every wave's site-pass launch, summed per step",
-            "peak_source": "kg_fp32_peak (FFMA loop over all SMs, measured in this run)",
-            "flops_counted": "executed FP32 site arithmetic of the shape-moment passes (FMA = 2); "
-                             "FP64 re-evaluation passes excluded",
+            "peak_source": ("half of kg_fp32_peak (B200 FP64 CUDA-core rate)" if fp64_form else
+                            "kg_fp32_peak (FFMA loop over all SMs, measured in this run)"),
+            "flops_counted": ("executed site arithmetic of the shape-moment passes (FMA = 2, MUFU = 1) "
+                              "per shape and pass kind; FP64 re-evaluation passes excluded" if not fp64_form
+                              else "executed FP64 site arithmetic of the shape-moment passes (FMA = 2)"),
             "ref_formulation_tflops": ref_equiv,
-            "hbm_peak_gbs": measured_hbm_peak()}
+            "ref_formulation_note": "the same pair-site-passes counted at the reference formulation's "
+                                    "136 + 20 FLOP (dense 9 + 45 sums); the shape moments need 19-41"}
     line = {"metric": METRIC, "value": value, "unit": "pairs/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_mean,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -291,6 +443,11 @@ def main():
     est.close()
     if pg:
         pg.destroy_process_group()
+
+
+# DRAM bytes (read + write) per pair-site-pass of wave_pass_kernel, measured by
+# ncu (profiles/wave_pass_kernel_N96_M100k.md): 1.985 GB over 447,339,158.
+PASS_DRAM_BYTES_PER_SITE = 4.44
 
 
 def ctypes_peak(device):

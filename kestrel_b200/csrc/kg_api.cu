@@ -155,6 +155,7 @@ void serve_batch(kg_ctx* c, Slot& slot, std::vector<std::shared_ptr<Request>>& b
         jb.n_x = batch[i]->n_query;
         jb.n_y = c->panel.n_samples;
         jb.d_out = slot.out.as<kg_output>() + off;
+        jb.iterations = batch[i]->iterations;   // each request keeps its own limit
         off += jb.n_pairs();
         jobs.push_back(jb);
         slot.queries.push_back(std::move(q));

@@ -516,6 +516,7 @@ int run_pairs(const std::vector<PairJob>& jobs, const RunConfig& cfg, Workspace&
         d.pair_begin = total_pairs;
         d.n_pairs = jb.n_pairs();
         d.out = jb.d_out;
+        d.max_iter = jb.iterations ? jb.iterations : cfg.iterations;
         total_pairs += d.n_pairs;
         seg_cap = std::max<int64_t>(seg_cap, align4(pn.n_kept) + 32);
     }

@@ -87,6 +87,7 @@ struct PairJob {
     int64_t n_x = 0;                    // triangle: num_samples; rect: query rows
     int64_t n_y = 0;                    // rect: panel rows
     kg_output* d_out = nullptr;         // device rows
+    uint64_t iterations = 0;            // SQP iteration limit (0 = the run's)
     int64_t n_pairs() const { return kind == 0 ? n_x * (n_x + 1) / 2 : n_x * n_y; }
 };
 

@@ -101,6 +101,7 @@ __global__ void noalloc_table_kernel(kg::CohortDev* table, const uint2* planes, 
     d.pair_begin = 0;
     d.n_pairs = n_x * (n_x + 1) / 2;
     d.out = out;
+    d.max_iter = 0;   // the single-kernel engine takes the limit from its launch
     *table = d;
 }
 

@@ -63,6 +63,7 @@ struct CohortDev {
     int64_t pair_begin;      // first global work index
     int64_t n_pairs;
     kg_output* out;          // rows in the reference's order
+    uint64_t max_iter;       // SQP iteration limit of this cohort's pairs
 };
 
 struct RunCounters {

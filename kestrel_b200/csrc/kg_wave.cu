@@ -483,7 +483,7 @@ __device__ inline void finish_slot(const WaveArgs& A, SlotState& S, int s, const
         atomicAdd(&C->fp64_pairs, (unsigned long long)S.escalated);
         atomicAdd(&C->pair_sites, (unsigned long long)S.n);
         atomicAdd(&C->work_units, (unsigned long long)S.n * (unsigned long long)S.gh);
-        if (iters >= A.tune.sqp_max_iter) atomicAdd(&C->nonconverged, 1ull);
+        if (iters >= co.max_iter) atomicAdd(&C->nonconverged, 1ull);
         const int p32 = S.gh - S.f64p;
         unsigned long long f32 = 0, f64 = 0;
         for (int sh = 0; sh < 5; sh++) {
@@ -625,8 +625,9 @@ extern "C" __global__ void __launch_bounds__(128) wave_solve_kernel(WaveArgs A) 
 #pragma unroll
         for (int k = 0; k < 9; k++) S.H[lane * 9 + k] = Hr[k];
     }
-    if (it >= tu.sqp_max_iter) {
-        finish_slot(A, S, s, x, f, tu.sqp_max_iter, CUDART_NAN, lane);
+    const uint64_t max_iter = A.cohorts[S.cohort].max_iter;
+    if (it >= max_iter) {
+        finish_slot(A, S, s, x, f, max_iter, CUDART_NAN, lane);
         return;
     }
     // ---- KKT test (src/sqp.rs:95-109) and the FP32 -> FP64 recheck

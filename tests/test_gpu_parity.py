@@ -12,29 +12,9 @@ import pytest
 import kestrel_b200 as kb
 from kestrel_b200 import synth
 
+from .parity import compare
+
 pytestmark = pytest.mark.gpu
-
-KIN = kb.KINSHIP_VECTOR
-
-
-def compare(gpu, ref, strict_cond=4.0):
-    assert np.array_equal(gpu["x"], ref["x"]) and np.array_equal(gpu["y"], ref["y"])
-    lc_ref = np.log10(ref["cond"])
-    lc_gpu = np.log10(gpu["cond"])
-    ident = np.isfinite(lc_ref) & (lc_ref <= strict_cond)
-    dd = np.abs(gpu["jacquard"] - ref["jacquard"]).max(1)
-    dk = np.abs(gpu["jacquard"] @ KIN - ref["jacquard"] @ KIN)
-    do = np.abs(gpu["obj"] - ref["obj"]) / np.abs(ref["obj"])
-    assert np.all(np.isfinite(gpu["obj"]))
-    assert dd[ident].max(initial=0) <= 1e-5, f"max Delta err {dd[ident].max()}"
-    assert dk[ident].max(initial=0) <= 1e-5
-    assert do.max() <= 1e-6, f"max objective rel err {do.max()}"
-    below = np.isfinite(lc_ref) & (lc_ref < 15)
-    assert np.all((lc_gpu[below] > 15) == (lc_ref[below] > 15))
-    return {"max_delta_err": float(dd[ident].max(initial=0)),
-            "max_kin_err": float(dk.max(initial=0)),
-            "max_obj_rel_err": float(do.max()),
-            "identifiable": int(ident.sum()), "pairs": len(ref)}
 
 
 @pytest.fixture(scope="module")

@@ -1,0 +1,130 @@
+"""GPU tests of the serving path, the inbred stress cohort and the CLI, through
+the C ABI, against the FP64 oracle (the same bar as test_gpu_parity.py)."""
+import os
+import subprocess
+import tempfile
+
+import numpy as np
+import pytest
+
+import kestrel_b200 as kb
+from kestrel_b200 import synth
+
+from .parity import compare
+
+pytestmark = pytest.mark.gpu
+
+
+def _bitwise_equal(a, b):
+    return a.shape == b.shape and np.array_equal(a.view(np.uint8), b.view(np.uint8))
+
+
+@pytest.fixture(scope="module")
+def panel():
+    return synth.make_cohort(80, 3000, seed=21, name="panel")
+
+
+def test_serving_alone_equals_mix_and_oracle(panel, oracle):
+    reqs = synth.config4_requests(panel, 6, seed=5, max_query=5)
+    with kb.Estimator() as est:
+        est.panel_load(panel.codes)
+        alone = [est.wait(est.submit(r["codes"], r["site_mask"])) for r in reqs]
+        ids = [est.submit(r["codes"], r["site_mask"]) for r in reqs]    # all in flight together
+        mixed = [est.wait(i) for i in ids]
+        stats = est.serving_stats()
+    for a, b, r in zip(alone, mixed, reqs):
+        assert len(a) == r["codes"].shape[0] * panel.codes.shape[0]
+        assert _bitwise_equal(a, b)
+    assert stats["requests"] == 2 * len(reqs)
+    # oracle: panel frequencies; the query's masked-out sites are missing
+    p, q, keep = oracle.site_frequencies(panel.codes)
+    for r, rows in list(zip(reqs, alone))[:2]:
+        qc = r["codes"].copy()
+        qc[:, ~r["site_mask"]] = 3
+        nq, npn = qc.shape[0], panel.codes.shape[0]
+        combined = np.vstack([qc, panel.codes])
+        pairs = np.array([(i, nq + j) for i in range(nq) for j in range(npn)])
+        ref = oracle.relatedness_pairs(combined, p, q, keep, pairs)
+        assert np.array_equal(rows["x"], pairs[:, 0]) and np.array_equal(rows["y"], pairs[:, 1] - nq)
+        print(compare(rows, ref, check_xy=False))
+
+
+def test_serving_request_keeps_its_iteration_limit(panel):
+    reqs = synth.config4_requests(panel, 3, seed=9, max_query=3)
+    with kb.Estimator() as est:
+        est.panel_load(panel.codes)
+        alone = est.wait(est.submit(reqs[0]["codes"], reqs[0]["site_mask"], iterations=2))
+        ids = [est.submit(reqs[0]["codes"], reqs[0]["site_mask"], iterations=2)] + \
+              [est.submit(r["codes"], r["site_mask"], iterations=100) for r in reqs[1:]]
+        mixed = [est.wait(i) for i in ids]
+    assert np.all(alone["iters"] <= 2)
+    assert _bitwise_equal(alone, mixed[0])
+
+
+def test_serving_cancel(panel):
+    reqs = synth.config4_requests(panel, 2, seed=13, max_query=2)
+    with kb.Estimator() as est:
+        est.panel_load(panel.codes)
+        rid = est.submit(reqs[0]["codes"], reqs[0]["site_mask"])
+        est.cancel(rid)
+        keep = est.submit(reqs[1]["codes"], reqs[1]["site_mask"])
+        rows = est.wait(keep)
+        assert len(rows) == reqs[1]["codes"].shape[0] * panel.codes.shape[0]
+        with pytest.raises(kb.KestrelError):
+            est.wait(rid)
+
+
+def test_inbred_stress_vs_oracle(oracle):
+    co = synth.make_cohort(64, 5000, seed=31, planted={"identical_inbred": 4}, inbred=16,
+                           low_info_sites=500, name="inbred")
+    ref = oracle.relatedness(co.codes)
+    with kb.Estimator() as est:
+        est.load(co.codes)
+        gpu = est.relatedness()
+        st = est.run_stats()
+    out = compare(gpu, ref)
+    print(out, st["fp64_pairs"])
+    lc = np.log10(ref["cond"])
+    assert np.any(~(lc <= 15)), "the stress cohort should hold flagged pairs"
+    # identical inbred pairs: Delta1 dominant
+    for x, y, rel, delta in co.planted:
+        i = int(np.nonzero((gpu["x"] == x) & (gpu["y"] == y))[0][0])
+        assert gpu["jacquard"][i][0] > 0.5
+
+
+def _read_tsv(path):
+    with open(path) as fh:
+        head = fh.readline().rstrip("\n").split("\t")
+        rows = [ln.rstrip("\n").split("\t") for ln in fh]
+    return head, rows
+
+
+def test_cli_gt_and_pl_match_oracle(oracle):
+    co = synth.make_cohort(24, 2500, seed=41, planted={"parent_offspring": 2})
+    cli = os.path.join(os.path.dirname(kb.__file__), "bin", "kestrel")
+    ref = oracle.relatedness(co.codes, num_samples=20)
+    outs = {}
+    with tempfile.TemporaryDirectory() as td:
+        for field in ("GT", "PL"):
+            vcf = os.path.join(td, f"in_{field}.vcf")
+            tsv = os.path.join(td, f"out_{field}.tsv")
+            synth.write_vcf(vcf, co.codes, field=field)
+            r = subprocess.run([cli, vcf, tsv, "-f", field, "-s", "20"], capture_output=True, text=True,
+                               timeout=300)
+            assert r.returncode == 0, r.stderr
+            with open(tsv) as fh:
+                outs[field] = fh.read()
+            head, rows = _read_tsv(tsv)
+    assert outs["GT"] == outs["PL"]
+    assert head[:3] == ["sample1", "sample2", "kinship"] and head[-3:] == ["iterations", "objective",
+                                                                          "condition"]
+    assert len(rows) == len(ref)
+    jac = np.array([[float(v) for v in r[3:12]] for r in rows])
+    kin = np.array([float(r[2]) for r in rows])
+    obj = np.array([float(r[13]) for r in rows])
+    lc_ref = np.log10(ref["cond"])
+    ident = np.isfinite(lc_ref) & (lc_ref <= 4)
+    assert np.abs(jac - ref["jacquard"]).max(1)[ident].max() <= 1e-5
+    assert np.abs(kin - ref["jacquard"] @ kb.KINSHIP_VECTOR)[ident].max() <= 1e-5
+    assert (np.abs(obj - ref["obj"]) / np.abs(ref["obj"])).max() <= 1e-6
+    assert [r[0] for r in rows[:2]] == ["S0", "S0"] and [r[1] for r in rows[:2]] == ["S0", "S1"]
