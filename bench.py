@@ -53,6 +53,7 @@ def parse():
                          "launch; inbred: N=512 x M=50k inbred stress; serving: panel + Poisson "
                          "query stream (p50/p99 latency)")
     ap.add_argument("--requests", type=int, default=64, help="serving: number of requests")
+    ap.add_argument("--rate", type=float, default=200.0, help="serving: Poisson arrival rate (requests/s)")
     return ap.parse_args()
 
 
@@ -268,7 +269,7 @@ def run_serving(args, local):
     import kestrel_b200 as kb
     from kestrel_b200 import synth
     panel = synth.config4_panel()
-    reqs = synth.config4_requests(panel, args.requests)
+    reqs = synth.config4_requests(panel, args.requests, rate_hz=args.rate)
     warm = synth.config4_requests(panel, 4, seed=7)
     est = kb.Estimator(device=local, precision=args.precision)
     est.panel_load(panel.codes)
@@ -302,7 +303,7 @@ def run_serving(args, local):
             "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
             "n_gpus": 1, "requests": len(reqs), "higher_is_better": True,
             "dtype": "f32" if args.precision == "fp32c" else "f64", "data": "synthetic",
-            "config": {"workload": f"panel {n_panel} x {panel.codes.shape[1]}, Poisson 200 req/s, 1-64 query "
+            "config": {"workload": f"panel {n_panel} x {panel.codes.shape[1]}, Poisson {args.rate:g} req/s, 1-64 query "
                                    "samples, per-request site mask keeping U(0.6, 1.0) of sites",
                        "pairs": pairs},
             "timing": "host wall clock from the first arrival to the last completion; latency per request "

@@ -160,36 +160,43 @@ void serve_batch(kg_ctx* c, Slot& slot, std::vector<std::shared_ptr<Request>>& b
         jobs.push_back(jb);
         slot.queries.push_back(std::move(q));
     }
+    // a request is answered as soon as its own pairs are done, between waves
+    std::vector<int64_t> offs(batch.size(), 0);
+    for (size_t i = 1; i < batch.size(); i++) offs[i] = offs[i - 1] + batch[i - 1]->n_query * c->panel.n_samples;
+    std::vector<char> answered(batch.size(), 0);
+    auto answer = [&](size_t i, int status, const std::string& why) {
+        auto& r = batch[i];
+        const int64_t np = r->n_query * c->panel.n_samples;
+        if (status == KG_OK) {
+            r->rows.resize(np);
+            cudaError_t ce = cudaMemcpyAsync(r->rows.data(), slot.out.as<kg_output>() + offs[i],
+                                             sizeof(kg_output) * np, cudaMemcpyDeviceToHost, slot.stream);
+            if (ce == cudaSuccess) ce = cudaStreamSynchronize(slot.stream);
+            if (ce != cudaSuccess) { r->status = KG_ECUDA; r->err = cudaGetErrorString(ce); }
+        } else {
+            r->status = status;
+            r->err = why;
+        }
+        answered[i] = 1;
+        std::lock_guard<std::mutex> lk(c->mu);
+        r->done = true;
+        c->served_requests++;
+        c->served_pairs += np;
+        c->cv.notify_all();
+    };
     kg_run_stats stats{};
     if (st == KG_OK) {
         kg::RunConfig cfg = run_config(c, batch.empty() ? 100 : batch[0]->iterations);
         uint64_t it = 1;
         for (auto& r : batch) it = std::max<uint64_t>(it, r->iterations);
         cfg.iterations = it;
+        cfg.job_done = [&](int j) { answer((size_t)j, KG_OK, std::string()); };
         st = kg::run_pairs(jobs, cfg, slot.ws, slot.stream, stats, err);
         if (st == KG_ENOSITES) st = KG_OK;  // per-pair NaN rows; reported on the rows
     }
-    off = 0;
-    for (auto& r : batch) {
-        int64_t np = r->n_query * c->panel.n_samples;
-        if (st == KG_OK) {
-            r->rows.resize(np);
-            cudaError_t ce = cudaMemcpyAsync(r->rows.data(), slot.out.as<kg_output>() + off,
-                                             sizeof(kg_output) * np, cudaMemcpyDeviceToHost, slot.stream);
-            if (ce == cudaSuccess) ce = cudaStreamSynchronize(slot.stream);
-            if (ce != cudaSuccess) { r->status = KG_ECUDA; r->err = cudaGetErrorString(ce); }
-        } else {
-            r->status = st;
-            r->err = err;
-        }
-        off += np;
-    }
+    for (size_t i = 0; i < batch.size(); i++)
+        if (!answered[i]) answer(i, st, err);
     std::lock_guard<std::mutex> lk(c->mu);
-    for (auto& r : batch) {
-        r->done = true;
-        c->served_requests++;
-        c->served_pairs += r->n_query * c->panel.n_samples;
-    }
     c->served_launches++;
     c->cv.notify_all();
 }

@@ -8,6 +8,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <functional>
 #include <string>
 #include <vector>
 
@@ -96,13 +97,16 @@ struct RunConfig {
     uint64_t iterations = 100;
     int64_t slots = 0;         // pairs in flight per wave (0 = up to 16384 as memory allows)
     int pass_blocks_per_sm = 0;   // site-pass kernel blocks per SM (0 = occupancy limit)
+    // Called between waves, on the calling thread, once per job whose pairs
+    // have all finished (their rows are final in device memory).
+    std::function<void(int job)> job_done;
 };
 
 // Reusable device workspace of the pair engine (per-slot lists and partial
 // sums, slot states, pass lists, queue, counters, cohort table).
 struct Workspace {
     DevBuf scratch, queue, counters, table;
-    DevBuf partial, slots, lists_a, lists_b, tasks, counts;
+    DevBuf partial, slots, lists_a, lists_b, tasks, counts, done;
     int sm_count = 0;
 };
 

@@ -224,7 +224,10 @@ extern "C" __global__ void __launch_bounds__(ADMIT_WARPS * 32, 4) wave_admit_ker
                     double nan9[9];
                     for (int i = 0; i < 9; i++) nan9[i] = CUDART_NAN;
                     write_row(co.out + j, x, y, nan9, CUDART_NAN, 0, CUDART_NAN, lane);
-                    if (lane == 0) atomicAdd(&A.counters->nosite_pairs, 1ull);
+                    if (lane == 0) {
+                        atomicAdd(&A.counters->nosite_pairs, 1ull);
+                        atomicAdd(&A.cohort_done[c], 1ull);
+                    }
                 }
                 continue;
             }
@@ -495,6 +498,7 @@ __device__ inline void finish_slot(const WaveArgs& A, SlotState& S, int s, const
         atomicAdd(&C->flops_fp64, f64);
         S.status = SLOT_FREE;
         A.free_next[atomicAdd(&A.wc_next->n_free, 1)] = s;
+        atomicAdd(&A.cohort_done[S.cohort], 1ull);
     }
 }
 
@@ -715,6 +719,8 @@ int run_waves(const std::vector<PairJob>& jobs, const RunConfig& cfg, Workspace&
     KG_WAVE_TRY((cudaError_t)ws.queue.reserve(sizeof(unsigned long long) * 2));
     KG_WAVE_TRY((cudaError_t)ws.counters.reserve(sizeof(RunCounters)));
     KG_WAVE_TRY((cudaError_t)ws.table.reserve(sizeof(CohortDev) * table.size()));
+    KG_WAVE_TRY((cudaError_t)ws.done.reserve(sizeof(unsigned long long) * table.size()));
+    KG_WAVE_TRY(cudaMemsetAsync(ws.done.p, 0, sizeof(unsigned long long) * table.size(), st));
     KG_WAVE_TRY(cudaMemcpyAsync(ws.table.p, table.data(), sizeof(CohortDev) * table.size(),
                                 cudaMemcpyHostToDevice, st));
     WaveCounts* wc = reinterpret_cast<WaveCounts*>(ws.counts.p);
@@ -774,6 +780,9 @@ int run_waves(const std::vector<PairJob>& jobs, const RunConfig& cfg, Workspace&
     A.admit_task = admit_task;
     A.tune = make_tune(cfg.iterations);
     A.counters = ws.counters.as<RunCounters>();
+    A.cohort_done = ws.done.as<unsigned long long>();
+    std::vector<unsigned long long> h_done(table.size(), 0);
+    std::vector<char> reported(table.size(), 0);
     int cur = 0;
     const int slot_blocks = (int)((n_slots + WAVE_WPB - 1) / WAVE_WPB);
     const size_t wsm = WAVE_WPB * WARP_SMEM;
@@ -810,7 +819,16 @@ int run_waves(const std::vector<PairJob>& jobs, const RunConfig& cfg, Workspace&
         unsigned long long hq = 0;
         KG_WAVE_TRY(cudaMemcpyAsync(&h, wc + nxt, sizeof(h), cudaMemcpyDeviceToHost, st));
         KG_WAVE_TRY(cudaMemcpyAsync(&hq, q, sizeof(hq), cudaMemcpyDeviceToHost, st));
+        if (cfg.job_done)
+            KG_WAVE_TRY(cudaMemcpyAsync(h_done.data(), A.cohort_done, sizeof(unsigned long long) * table.size(),
+                                        cudaMemcpyDeviceToHost, st));
         KG_WAVE_TRY(cudaStreamSynchronize(st));
+        if (cfg.job_done)
+            for (size_t j = 0; j < table.size(); j++)
+                if (!reported[j] && h_done[j] >= (unsigned long long)table[j].n_pairs) {
+                    reported[j] = 1;
+                    cfg.job_done((int)j);
+                }
         for (int i = 0; i < 3; i++) {
             float ms = 0.f;
             KG_WAVE_TRY(cudaEventElapsedTime(&ms, ev[i], ev[i + 1]));

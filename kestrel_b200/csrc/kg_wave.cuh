@@ -88,6 +88,7 @@ struct WaveArgs {
     int* admit_task;               // admit entry counter
     Tune tune;
     RunCounters* counters;
+    unsigned long long* cohort_done;   // finished pairs per cohort
 };
 
 __device__ __forceinline__ int shape_ng(int s) { return s == 0 ? 4 : s == 3 ? 4 : s == 4 ? 2 : 3; }
