@@ -52,6 +52,18 @@ __device__ __forceinline__ double warp_max_plain(double v) {
     return v;
 }
 
+// Maximum over lanes of non-negative values (NaN counts as 0, as fmax drops
+// it): for doubles >= 0 the bit patterns order as the values, so two 32-bit
+// warp reductions (high words, then the low words of the lanes holding the
+// largest high word) give the maximum without a shuffle tree.
+__device__ __forceinline__ double warp_max_nonneg(double v) {
+    if (!(v >= 0.0)) v = 0.0;
+    const unsigned hi = (unsigned)__double2hiint(v), lo = (unsigned)__double2loint(v);
+    const unsigned mh = __reduce_max_sync(FULL_MASK, hi);
+    const unsigned ml = __reduce_max_sync(FULL_MASK, hi == mh ? lo : 0u);
+    return __hiloint2double((int)mh, (int)ml);
+}
+
 // GMW81-modified LDL^T of the masked matrix: q = this lane's row of Q with
 // free mask F (nf free variables).  Returns this lane's row of L and the
 // uniform diagonal d.
@@ -65,8 +77,8 @@ __device__ __forceinline__ void ldl_gmw_rows(const double* q, unsigned F, int nf
         if (rf && j == r) diag = fabs(q[j]);
         if (rf && jf && j > r) off = fmax(off, fabs(q[j]));
     }
-    const double gamma = warp_max_plain(diag);
-    const double xi = warp_max_plain(off);
+    const double gamma = warp_max_nonneg(diag);
+    const double xi = warp_max_nonneg(off);
     const double eps = 2.220446049250313e-16;
     const double delta = eps * fmax(1.0, gamma + xi);
     const double t = sqrt((double)nf * (double)nf - 1.0);
@@ -95,7 +107,7 @@ __device__ __forceinline__ void ldl_gmw_rows(const double* q, unsigned F, int nf
         for (int s = 0; s < j; s++) sij = fma(p[s], Lr[s], sij);
         const double cij = q[j] - sij;
         const bool act = rf && (r > j);
-        const double theta = warp_max_plain(act ? fabs(cij) : 0.0);
+        const double theta = warp_max_nonneg(act ? fabs(cij) : 0.0);
         const double dj = fmax(fmax(fabs(cjj), theta * theta / beta2), delta);
         if (act) Lr[j] = cij / dj;
         if (r == j) Lr[j] = 1.0;

@@ -522,7 +522,9 @@ __device__ inline void schedule_pass(const WaveArgs& A, SlotState& S, int s, int
     enqueue_pass(A.pass_next, A.tasks_next, A.task_cap, A.wc_next, s, S, lane);
 }
 
-extern "C" __global__ void __launch_bounds__(128) wave_solve_kernel(WaveArgs A) {
+// Four blocks of four warps per SM (at most 128 registers a thread): the solver
+// is latency-bound, so warps count for more than the few spilled values.
+extern "C" __global__ void __launch_bounds__(128, 4) wave_solve_kernel(WaveArgs A) {
     extern __shared__ __align__(16) char smem[];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const int i = blockIdx.x * WAVE_WPB + wib;
@@ -532,20 +534,30 @@ extern "C" __global__ void __launch_bounds__(128) wave_solve_kernel(WaveArgs A) 
     char* wsm = smem + wib * WARP_SMEM;
     double* mom_s = reinterpret_cast<double*>(wsm);
     const Tune& tu = A.tune;
-    // ---- sum the units' partials in unit order: lane owns moments lane and lane + 32
+    // ---- sum the units' partials in unit order: lane owns moments lane and
+    // lane + 32 (45 = the objective); a moment's units are those of its shape
     {
-        double m0 = 0.0, m1 = 0.0;
-        const int nu = S.ustart[5];
+        int us[6];
+#pragma unroll
+        for (int k = 0; k < 6; k++) us[k] = S.ustart[k];
         const double* P0 = A.partial + (int64_t)s * A.max_units * UNIT_VALS;
-        int sh = 0;
-        for (int u = 0; u < nu; u++) {
-            while (u >= S.ustart[sh + 1]) sh++;
-            const double* P = P0 + (int64_t)u * UNIT_VALS;
-            const int go = shape_goff(sh), nv = shape_ng(sh) + shape_nh(sh);
-            if (lane >= go && lane < go + nv) m0 += P[lane - go];
-            const int l1 = lane + 32;
-            if (l1 == NMOM) m1 += P[UNIT_VALS - 1];
-            else if (l1 < NMOM && l1 >= go && l1 < go + nv) m1 += P[l1 - go];
+        // moment m belongs to shape A (0..10), B1 (11..18), B2 (19..26), C (27..39) or D (40..44)
+        auto shape_of = [](int m) { return m < 11 ? 0 : m < 19 ? 1 : m < 27 ? 2 : m < 40 ? 3 : 4; };
+        auto sum_range = [&](int u0, int u1, int col) {
+            double acc = 0.0;
+#pragma unroll 4
+            for (int u = u0; u < u1; u++) acc += P0[(int64_t)u * UNIT_VALS + col];
+            return acc;
+        };
+        const int sh0 = shape_of(lane);
+        const double m0 = sum_range(us[sh0], us[sh0 + 1], lane - shape_goff(sh0));
+        double m1 = 0.0;
+        const int l1 = lane + 32;
+        if (l1 == NMOM) {
+            m1 = sum_range(0, us[5], UNIT_VALS - 1);
+        } else if (l1 < NMOM) {
+            const int sh1 = shape_of(l1);
+            m1 = sum_range(us[sh1], us[sh1 + 1], l1 - shape_goff(sh1));
         }
         mom_s[lane] = m0;
         if (lane + 32 <= NMOM) mom_s[lane + 32] = m1;
