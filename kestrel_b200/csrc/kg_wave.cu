@@ -290,6 +290,16 @@ __device__ __forceinline__ void ring_issue(const Ring& R, const float* L, int64_
     bulk_load(R.buf + slot * STAGE_F4, L + e0, bytes, &R.bar[slot]);
 }
 
+// Lane 0 starts the first RING_STAGES stage copies of a list of len entries.
+__device__ __forceinline__ void ring_prologue(const Ring& R, const float* L, int64_t len, int lane) {
+    if (lane == 0) {
+        const int nst = (int)((len + STAGE_ELEMS - 1) / STAGE_ELEMS);
+        const int pro = min(nst, RING_STAGES);
+        fence_proxy_async_smem();
+        for (int i = 0; i < pro; i++) ring_issue(R, L, len, i, (R.seq + i) % RING_STAGES);
+    }
+}
+
 // One shape's FP32 list from the ring.  Stage i holds float4 128 i .. 128 i +
 // 127; lane l takes 128 i + 32 j + l (j = 0..3), in two steps of 8 sites
 // after each of which the FP32 gradient and objective partials go to FP64
@@ -313,12 +323,7 @@ __device__ __noinline__ bool stream32_ring(const float* __restrict__ L, int64_t 
     for (int i = 0; i < NH; i++) { H[i] = 0.0; h[i] = 0.f; }
     const int64_t n4 = len >> 2;
     const int nst = (int)((len + STAGE_ELEMS - 1) / STAGE_ELEMS);
-    const uint32_t seq0 = R.seq;
-    if (lane == 0) {
-        const int pro = min(nst, RING_STAGES);
-        fence_proxy_async_smem();
-        for (int i = 0; i < pro; i++) ring_issue(R, L, len, i, (seq0 + i) % RING_STAGES);
-    }
+    const uint32_t seq0 = R.seq;   // ring_prologue has issued the first stages
     bool ok = true;
     int it = 0, done = 0;
     for (int i = 0; i < nst; i++) {
@@ -420,24 +425,28 @@ extern "C" __global__ void __launch_bounds__(128, PASS_MIN_BLOCKS) wave_pass_ker
 #pragma unroll
     for (int k = 0; k < 5; k++) pre[k + 1] = pre[k] + A.wc_cur->units[k];
     const int64_t ntask = pre[5];
+    // the next task is claimed as the current one starts, so the claim's
+    // latency hides behind the current task's sites
+    unsigned long long t = 0;
+    if (lane == 0) t = atomicAdd(A.pass_task, 1ull);
+    t = __shfl_sync(0xffffffffu, t, 0);
     for (;;) {
-        unsigned long long t = 0;
-        if (lane == 0) t = atomicAdd(A.pass_task, 1ull);
-        t = __shfl_sync(0xffffffffu, t, 0);
         if ((int64_t)t >= ntask) break;
         int sh = 0;
 #pragma unroll
         for (int k = 1; k < 5; k++) sh += ((int)t >= pre[k]) ? 1 : 0;
-        const int2 tk = A.tasks_cur[sh * A.task_cap + ((int)t - pre[sh])];
+        const int4 tk = A.tasks_cur[sh * A.task_cap + ((int)t - pre[sh])];
+        unsigned long long t_next = 0;
+        if (lane == 0) t_next = atomicAdd(A.pass_task, 1ull);
         const int s = tk.x;
         const int u = tk.y;
-        const SlotState& S = A.slots[s];
-        const int64_t c0 = (int64_t)(u - S.ustart[sh]) * UNIT_ELEMS;
-        const int64_t off = S.start[sh] + c0;
-        const int64_t len = min((int64_t)UNIT_ELEMS, S.cnt[sh] - c0);
-        const int kind = S.kind;
+        const int64_t off = tk.z;
+        const int64_t len = tk.w & 0xFFFFFF;
+        const int kind = tk.w >> 24;
         const bool l64 = (kind == PASS_FP64);
-        // the pending pass's coefficients into this warp's shared memory
+        const SlotState& S = A.slots[s];
+        // first list stages in flight, then the pass's coefficients into shared memory
+        if (!l64) ring_prologue(R, reinterpret_cast<const float*>(A.lists + (int64_t)s * A.list_stride) + off, len, lane);
         const int nwords = l64 ? (int)(sizeof(PassCoef) / 4) : (int)(sizeof(Coef32) / 4);
         const uint32_t* src = l64 ? reinterpret_cast<const uint32_t*>(&S.c64)
                                   : reinterpret_cast<const uint32_t*>(&S.c32);
@@ -468,6 +477,7 @@ extern "C" __global__ void __launch_bounds__(128, PASS_MIN_BLOCKS) wave_pass_ker
         const double ob = warp_sum(ls.obj);
         if (lane == 0) P[UNIT_VALS - 1] = ob;
         __syncwarp();
+        t = __shfl_sync(0xffffffffu, t_next, 0);
     }
 }
 
@@ -713,7 +723,7 @@ int run_waves(const std::vector<PairJob>& jobs, const RunConfig& cfg, Workspace&
     const int max_units = (int)shape_units + 5;
     // slots: as many as the work and the memory allow
     const size_t per_slot = sizeof(double) * (size_t)list_cap + sizeof(double) * max_units * UNIT_VALS +
-                            sizeof(SlotState) + 4 * sizeof(int) + 2 * 5 * shape_units * sizeof(int2);
+                            sizeof(SlotState) + 4 * sizeof(int) + 2 * 5 * shape_units * sizeof(int4);
     size_t fr = 0, tot = 0;
     KG_WAVE_TRY(cudaMemGetInfo(&fr, &tot));
     int64_t want = cfg.slots > 0 ? cfg.slots : 16384;
@@ -726,7 +736,7 @@ int run_waves(const std::vector<PairJob>& jobs, const RunConfig& cfg, Workspace&
     KG_WAVE_TRY((cudaError_t)ws.slots.reserve(sizeof(SlotState) * n_slots));
     KG_WAVE_TRY((cudaError_t)ws.lists_a.reserve(sizeof(int) * 2 * n_slots));   // pass lists
     KG_WAVE_TRY((cudaError_t)ws.lists_b.reserve(sizeof(int) * 2 * n_slots));   // free lists
-    KG_WAVE_TRY((cudaError_t)ws.tasks.reserve(sizeof(int2) * 2 * 5 * task_cap));
+    KG_WAVE_TRY((cudaError_t)ws.tasks.reserve(sizeof(int4) * 2 * 5 * task_cap));
     KG_WAVE_TRY((cudaError_t)ws.counts.reserve(sizeof(WaveCounts) * 2 + 64));
     KG_WAVE_TRY((cudaError_t)ws.queue.reserve(sizeof(unsigned long long) * 2));
     KG_WAVE_TRY((cudaError_t)ws.counters.reserve(sizeof(RunCounters)));
@@ -740,7 +750,7 @@ int run_waves(const std::vector<PairJob>& jobs, const RunConfig& cfg, Workspace&
     unsigned long long* q = ws.queue.as<unsigned long long>();   // [0] pairs, [1] pass units
     int* pass_l[2] = {ws.lists_a.as<int>(), ws.lists_a.as<int>() + n_slots};
     int* free_l[2] = {ws.lists_b.as<int>(), ws.lists_b.as<int>() + n_slots};
-    int2* tasks_l[2] = {ws.tasks.as<int2>(), ws.tasks.as<int2>() + 5 * task_cap};
+    int4* tasks_l[2] = {ws.tasks.as<int4>(), ws.tasks.as<int4>() + 5 * task_cap};
     KG_WAVE_TRY(cudaMemsetAsync(ws.slots.p, 0, sizeof(SlotState) * n_slots, st));   // all SLOT_FREE
     KG_WAVE_TRY(cudaMemsetAsync(ws.queue.p, 0, sizeof(unsigned long long) * 2, st));
     KG_WAVE_TRY(cudaMemsetAsync(ws.counts.p, 0, sizeof(WaveCounts) * 2 + 64, st));

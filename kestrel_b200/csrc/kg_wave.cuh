@@ -19,7 +19,7 @@
 
 namespace kg {
 
-constexpr int UNIT_ELEMS = 8192;   // list entries per pass work unit
+constexpr int UNIT_ELEMS = 16384;  // list entries per pass work unit
 constexpr int UNIT_VALS = 14;      // partial values per unit: <= 13 moments + objective
 
 enum : int { SLOT_FREE = 0, SLOT_PASS = 1, SLOT_RESORT = 2 };
@@ -79,8 +79,8 @@ struct WaveArgs {
     int* pass_next;
     int* free_cur;
     int* free_next;
-    int2* tasks_cur;               // per shape: task_cap entries {slot, unit}
-    int2* tasks_next;
+    int4* tasks_cur;               // per shape: task_cap entries (PassTask)
+    int4* tasks_next;
     int64_t task_cap;
     WaveCounts* wc_cur;
     WaveCounts* wc_next;
@@ -146,11 +146,17 @@ __device__ __forceinline__ void decode_pair(const WaveArgs& A, int64_t k, int& c
     }
 }
 
+// A pass work unit as stored in the task lists: everything the pass kernel
+// needs before its first list copy, {slot, unit, list offset, length | kind << 24}.
+__device__ __forceinline__ int4 make_task(int s, int u, int64_t off, int64_t len, int kind) {
+    return make_int4(s, u, (int)off, (int)len | (kind << 24));
+}
+
 // Queues slot s for a pass in the wave whose lists are (pass, tasks, wc): its
 // work units go to the shape-major task lists, so that the warps of the pass
 // kernel run one shape's code at a time.  Called by a whole warp after S.ustart
 // is set.
-__device__ inline void enqueue_pass(int* pass, int2* tasks, int64_t task_cap, WaveCounts* wc, int s,
+__device__ inline void enqueue_pass(int* pass, int4* tasks, int64_t task_cap, WaveCounts* wc, int s,
                                     const SlotState& S, int lane) {
 #pragma unroll 1
     for (int sh = 0; sh < 5; sh++) {
@@ -159,7 +165,12 @@ __device__ inline void enqueue_pass(int* pass, int2* tasks, int64_t task_cap, Wa
         int base = 0;
         if (lane == 0) base = atomicAdd(&wc->units[sh], nu);
         base = __shfl_sync(0xffffffffu, base, 0);
-        for (int i = lane; i < nu; i += 32) tasks[sh * task_cap + base + i] = make_int2(s, u0 + i);
+        const int64_t st = S.start[sh], cnt = S.cnt[sh];
+        const int kind = S.kind;
+        for (int i = lane; i < nu; i += 32) {
+            const int64_t c0 = (int64_t)i * UNIT_ELEMS;
+            tasks[sh * task_cap + base + i] = make_task(s, u0 + i, st + c0, min((int64_t)UNIT_ELEMS, cnt - c0), kind);
+        }
     }
     if (lane == 0) pass[atomicAdd(&wc->n_pass, 1)] = s;
 }
