@@ -932,13 +932,18 @@ __host__ __device__ constexpr int flops_diff_extra(int s) {
 }
 
 // Condition estimate from the row-distributed Hessian (once per pair).
-__device__ inline double condition_rows(const double* x, const double* g, const double* Hr, double tol) {
+template <class G>
+__device__ inline double condition_rows(const G& grp, const double* x, const double* g, const double* Hr,
+                                        double tol) {
     double H[81];
 #pragma unroll
     for (int i = 0; i < 9; i++)
 #pragma unroll
-        for (int j = 0; j < 9; j++) H[i * 9 + j] = bcast(Hr[j], i);
+        for (int j = 0; j < 9; j++) H[i * 9 + j] = grp.bcast(Hr[j], i);
     return condition_estimate(x, g, H, tol);
+}
+__device__ inline double condition_rows(const double* x, const double* g, const double* Hr, double tol) {
+    return condition_rows(WarpGrp{FULL_MASK}, x, g, Hr, tol);
 }
 
 // SQP of one pair (src/sqp.rs:49-93) over its sorted lists.  The FP32 lists
@@ -1018,7 +1023,7 @@ __device__ inline void solve_pair(const CohortDev& co, int64_t px, int64_t py, c
         if (lane < 9) cr = pick9(g, lane) - dot_fma(9, Hr, x);
         double c[9], y[9], p[9];
         gather9(cr, c);
-        qp_simplex_rows(Hr, c, x, tu, lane, y);
+        qp_simplex_rows(WarpGrp{FULL_MASK}, Hr, c, x, tu, lane, y);
 #pragma unroll
         for (int i = 0; i < 9; i++) p[i] = y[i] - x[i];
         const double gp = dot_fma(9, g, p);

@@ -19,13 +19,27 @@ namespace kg {
 
 constexpr unsigned FULL_MASK = 0xffffffffu;
 
+// The lanes that run one pair's solver: a whole warp (W = 32) or a half-warp
+// (W = 16, two pairs per warp).  Row r of the 9x9 matrices lives in the
+// group's lane r; 9-vectors are uniform across the group.
+template <int W>
+struct Grp {
+    unsigned mask;
+    __device__ __forceinline__ double bcast(double v, int src) const { return __shfl_sync(mask, v, src, W); }
+    __device__ __forceinline__ void sync() const { __syncwarp(mask); }
+};
+using WarpGrp = Grp<32>;
+using HalfGrp = Grp<16>;
+
 __device__ __forceinline__ double bcast(double v, int src) { return __shfl_sync(FULL_MASK, v, src); }
 
-// Warp-uniform copy of the values held by lanes 0..8.
-__device__ __forceinline__ void gather9(double v, double* out) {
+// Group-uniform copy of the values held by lanes 0..8.
+template <class G>
+__device__ __forceinline__ void gather9(const G& g, double v, double* out) {
 #pragma unroll
-    for (int i = 0; i < 9; i++) out[i] = bcast(v, i);
+    for (int i = 0; i < 9; i++) out[i] = g.bcast(v, i);
 }
+__device__ __forceinline__ void gather9(double v, double* out) { gather9(WarpGrp{FULL_MASK}, v, out); }
 
 // Element `r` (a lane index) of a uniform register vector.
 __device__ __forceinline__ double pick9(const double* v, int r) {
@@ -46,28 +60,24 @@ __device__ __forceinline__ double warp_max_nan(double v) {
     return v;
 }
 
-__device__ __forceinline__ double warp_max_plain(double v) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(FULL_MASK, v, o));
-    return v;
-}
-
-// Maximum over lanes of non-negative values (NaN counts as 0, as fmax drops
-// it): for doubles >= 0 the bit patterns order as the values, so two 32-bit
-// warp reductions (high words, then the low words of the lanes holding the
-// largest high word) give the maximum without a shuffle tree.
-__device__ __forceinline__ double warp_max_nonneg(double v) {
+// Maximum over the group's lanes of non-negative values (NaN counts as 0, as
+// fmax drops it): for doubles >= 0 the bit patterns order as the values, so
+// two 32-bit reductions (high words, then the low words of the lanes holding
+// the largest high word) give the maximum without a shuffle tree.
+template <class G>
+__device__ __forceinline__ double group_max_nonneg(const G& g, double v) {
     if (!(v >= 0.0)) v = 0.0;
     const unsigned hi = (unsigned)__double2hiint(v), lo = (unsigned)__double2loint(v);
-    const unsigned mh = __reduce_max_sync(FULL_MASK, hi);
-    const unsigned ml = __reduce_max_sync(FULL_MASK, hi == mh ? lo : 0u);
+    const unsigned mh = __reduce_max_sync(g.mask, hi);
+    const unsigned ml = __reduce_max_sync(g.mask, hi == mh ? lo : 0u);
     return __hiloint2double((int)mh, (int)ml);
 }
 
 // GMW81-modified LDL^T of the masked matrix: q = this lane's row of Q with
 // free mask F (nf free variables).  Returns this lane's row of L and the
 // uniform diagonal d.
-__device__ __forceinline__ void ldl_gmw_rows(const double* q, unsigned F, int nf, int r,
+template <class G>
+__device__ __forceinline__ void ldl_gmw_rows(const G& g, const double* q, unsigned F, int nf, int r,
                                              double* Lr, double* d) {
     const bool rf = (r < 9) && ((F >> r) & 1u);
     double diag = 0.0, off = 0.0;
@@ -77,8 +87,8 @@ __device__ __forceinline__ void ldl_gmw_rows(const double* q, unsigned F, int nf
         if (rf && j == r) diag = fabs(q[j]);
         if (rf && jf && j > r) off = fmax(off, fabs(q[j]));
     }
-    const double gamma = warp_max_nonneg(diag);
-    const double xi = warp_max_nonneg(off);
+    const double gamma = group_max_nonneg(g, diag);
+    const double xi = group_max_nonneg(g, off);
     const double eps = 2.220446049250313e-16;
     const double delta = eps * fmax(1.0, gamma + xi);
     const double t = sqrt((double)nf * (double)nf - 1.0);
@@ -97,17 +107,17 @@ __device__ __forceinline__ void ldl_gmw_rows(const double* q, unsigned F, int nf
         double sjj = 0.0;
 #pragma unroll
         for (int s = 0; s < j; s++) {
-            const double ljs = bcast(Lr[s], j);
+            const double ljs = g.bcast(Lr[s], j);
             p[s] = d[s] * ljs;
             sjj = fma(p[s], ljs, sjj);
         }
-        const double cjj = bcast(q[j], j) - sjj;
+        const double cjj = g.bcast(q[j], j) - sjj;
         double sij = 0.0;
 #pragma unroll
         for (int s = 0; s < j; s++) sij = fma(p[s], Lr[s], sij);
         const double cij = q[j] - sij;
         const bool act = rf && (r > j);
-        const double theta = warp_max_nonneg(act ? fabs(cij) : 0.0);
+        const double theta = group_max_nonneg(g, act ? fabs(cij) : 0.0);
         const double dj = fmax(fmax(fabs(cjj), theta * theta / beta2), delta);
         if (act) Lr[j] = cij / dj;
         if (r == j) Lr[j] = 1.0;
@@ -117,14 +127,15 @@ __device__ __forceinline__ void ldl_gmw_rows(const double* q, unsigned F, int nf
 
 // Solves L D L^T z = b for two right-hand sides held one element per lane
 // (b0, b1 for this lane's row), in the reference's summation order.
-__device__ __forceinline__ void ldl_solve2_rows(const double* Lr, const double* d, int r, double& b0,
+template <class G>
+__device__ __forceinline__ void ldl_solve2_rows(const G& g, const double* Lr, const double* d, int r, double& b0,
                                                 double& b1) {
     // forward: b_i -= sum_{j<i} b_j L[i][j]
     double s0 = 0.0, s1 = 0.0;
 #pragma unroll
     for (int j = 0; j < 9; j++) {
-        const double f0 = bcast(b0 - s0, j);
-        const double f1 = bcast(b1 - s1, j);
+        const double f0 = g.bcast(b0 - s0, j);
+        const double f1 = g.bcast(b1 - s1, j);
         if (r > j) {
             s0 = fma(f0, Lr[j], s0);
             s1 = fma(f1, Lr[j], s1);
@@ -142,19 +153,21 @@ __device__ __forceinline__ void ldl_solve2_rows(const double* Lr, const double* 
         double t0 = 0.0, t1 = 0.0;
 #pragma unroll
         for (int j = i + 1; j < 9; j++) {
-            const double lji = bcast(Lr[i], j);
+            const double lji = g.bcast(Lr[i], j);
             t0 = fma(fin0[j], lji, t0);
             t1 = fma(fin1[j], lji, t1);
         }
-        fin0[i] = bcast(b0, i) - t0;
-        fin1[i] = bcast(b1, i) - t1;
+        fin0[i] = g.bcast(b0, i) - t0;
+        fin1[i] = g.bcast(b1, i) - t1;
     }
     b0 = pick9(fin0, r);
     b1 = pick9(fin1, r);
 }
 
-// min 1/2 y'Qy + c'y s.t. y >= 0, sum y = 1, from y0.  Hr: this lane's row of Q.
-__device__ inline void qp_simplex_rows(const double* Hr, const double* c, const double* y0,
+// min 1/2 y'Qy + c'y s.t. y >= 0, sum y = 1, from y0.  Hr: this lane's row of Q;
+// lane: the lane's index within the group.
+template <class G>
+__device__ inline void qp_simplex_rows(const G& grp, const double* Hr, const double* c, const double* y0,
                                        const Tune& tu, int lane, double* y) {
     unsigned work = 0;
 #pragma unroll
@@ -182,12 +195,12 @@ __device__ inline void qp_simplex_rows(const double* Hr, const double* c, const 
             gf = pick9(c, r) + s;
         }
         double Lr[9], d[9];
-        ldl_gmw_rows(q, F, nf, r, Lr, d);
+        ldl_gmw_rows(grp, q, F, nf, r, Lr, d);
         double ones = rf ? 1.0 : 0.0;
-        ldl_solve2_rows(Lr, d, r, gf, ones);
+        ldl_solve2_rows(grp, Lr, d, r, gf, ones);
         double gfu[9], onu[9];
-        gather9(gf, gfu);
-        gather9(ones, onu);
+        gather9(grp, gf, gfu);
+        gather9(grp, ones, onu);
         double sg = 0.0, so = 0.0;
 #pragma unroll
         for (int i = 0; i < 9; i++)
@@ -209,7 +222,7 @@ __device__ inline void qp_simplex_rows(const double* Hr, const double* c, const 
             double gq = 0.0;
             if (r < 9) gq = pick9(c, r) + dot_fma(9, Hr, y);
             double gqu[9];
-            gather9(gq, gqu);
+            gather9(grp, gq, gqu);
             int best = -1;
 #pragma unroll
             for (int i = 0; i < 9; i++)

@@ -202,7 +202,7 @@ extern "C" __global__ void __launch_bounds__(ADMIT_WARPS * 32, 4) wave_admit_ker
                 S.status = SLOT_PASS;
             }
             __syncthreads();
-            if (w == 0) enqueue_pass(A.pass_cur, A.tasks_cur, A.task_cap, A.wc_cur, s, S, lane);
+            if (w == 0) enqueue_pass<32>(A.pass_cur, A.tasks_cur, A.task_cap, A.wc_cur, s, S, lane, 0xffffffffu);
             continue;
         }
         // a free slot takes pairs until one has jointly observed sites
@@ -260,7 +260,7 @@ extern "C" __global__ void __launch_bounds__(ADMIT_WARPS * 32, 4) wave_admit_ker
                 S.status = SLOT_PASS;
             }
             __syncthreads();
-            if (w == 0) enqueue_pass(A.pass_cur, A.tasks_cur, A.task_cap, A.wc_cur, s, S, lane);
+            if (w == 0) enqueue_pass<32>(A.pass_cur, A.tasks_cur, A.task_cap, A.wc_cur, s, S, lane, 0xffffffffu);
             break;
         }
     }
@@ -310,7 +310,7 @@ __device__ __forceinline__ void ring_prologue(const Ring& R, const float* L, int
 // Returns false if a wait ran out.
 template <int S>
 __device__ __noinline__ bool stream32_ring(const float* __restrict__ L, int64_t len, const Coef32* K,
-                                           bool diff, int lane, Ring& R, LaneSums& out) {
+                                           bool diff, int lane, const Ring R, LaneSums& out) {
     using E = Shape32<S, false>;
     constexpr int NG = E::NG, NH = E::NH, GOFF = E::GOFF, HOFF = E::HOFF;
     E ev;
@@ -380,7 +380,6 @@ __device__ __noinline__ bool stream32_ring(const float* __restrict__ L, int64_t 
         F += (double)ob;
     }
     __syncwarp();   // every lane has read the ring before the next copies
-    R.seq = seq0 + nst;
 #pragma unroll
     for (int j = 0; j < NH; j++) H[j] += (double)h[j];
 #pragma unroll
@@ -393,7 +392,7 @@ __device__ __noinline__ bool stream32_ring(const float* __restrict__ L, int64_t 
 
 template <int SH>
 __device__ __forceinline__ bool run_unit(const void* lists, bool l64, int64_t off, int64_t len,
-                                         const void* kbuf, bool diff, int lane, Ring& R, LaneSums& ls) {
+                                         const void* kbuf, bool diff, int lane, const Ring R, LaneSums& ls) {
     if (l64) {
         stream64<SH>(static_cast<const double*>(lists) + off, len, reinterpret_cast<const PassCoef*>(kbuf),
                      lane, ls);
@@ -468,6 +467,7 @@ extern "C" __global__ void __launch_bounds__(128, PASS_MIN_BLOCKS) wave_pass_ker
             if (lane == 0) atomicAdd(&A.counters->stalled_waits, 1ull);
             return;
         }
+        if (!l64) R.seq += (uint32_t)((len + STAGE_ELEMS - 1) / STAGE_ELEMS);
         const int go = shape_goff(sh), nv = shape_ng(sh) + shape_nh(sh);
         double* P = A.partial + ((int64_t)s * A.max_units + u) * UNIT_VALS;
         for (int i = 0; i < nv; i++) {
@@ -483,6 +483,7 @@ extern "C" __global__ void __launch_bounds__(128, PASS_MIN_BLOCKS) wave_pass_ker
 
 // ------------------------------------------------------------------ solve
 
+// (lane: the lane's index in its half-warp group)
 __device__ inline void finish_slot(const WaveArgs& A, SlotState& S, int s, const double* x, double f,
                                    uint64_t iters, double cond, int lane) {
     const CohortDev& co = A.cohorts[S.cohort];
@@ -514,7 +515,8 @@ __device__ inline void finish_slot(const WaveArgs& A, SlotState& S, int s, const
 
 // Schedules the slot's next pass at S.xt (lane 0 has written xt).  A pass in
 // FP64 on FP32 lists first goes back through the admit step for FP64 lists.
-__device__ inline void schedule_pass(const WaveArgs& A, SlotState& S, int s, int kind, int ev, int lane) {
+__device__ inline void schedule_pass(const WaveArgs& A, SlotState& S, int s, int kind, int ev, int lane,
+                                     const HalfGrp& grp) {
     if (lane == 0) {
         S.ev = ev;
         set_coefficients(S, kind);
@@ -528,24 +530,29 @@ __device__ inline void schedule_pass(const WaveArgs& A, SlotState& S, int s, int
         return;
     }
     if (lane == 0) S.status = SLOT_PASS;
-    __syncwarp();
-    enqueue_pass(A.pass_next, A.tasks_next, A.task_cap, A.wc_next, s, S, lane);
+    grp.sync();
+    enqueue_pass<16>(A.pass_next, A.tasks_next, A.task_cap, A.wc_next, s, S, lane, grp.mask);
 }
 
-// Four blocks of four warps per SM (at most 128 registers a thread): the solver
-// is latency-bound, so warps count for more than the few spilled values.
+// Two slots per warp, one per half-warp (the row-parallel solver needs nine
+// lanes), four blocks of four warps per SM (at most 128 registers a thread):
+// the solver is latency-bound, so warps count for more than the few spilled
+// values.  `lane` below is the lane's index in its half.
 extern "C" __global__ void __launch_bounds__(128, 4) wave_solve_kernel(WaveArgs A) {
     extern __shared__ __align__(16) char smem[];
-    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-    const int i = blockIdx.x * WAVE_WPB + wib;
+    const int wib = threadIdx.x >> 5, half = (threadIdx.x >> 4) & 1;
+    const int lane = threadIdx.x & 15;
+    const HalfGrp grp{half ? 0xFFFF0000u : 0x0000FFFFu};
+    const int i = (blockIdx.x * WAVE_WPB + wib) * 2 + half;
     if (i >= A.wc_cur->n_pass) return;
     const int s = A.pass_cur[i];
     SlotState& S = A.slots[s];
     char* wsm = smem + wib * WARP_SMEM;
-    double* mom_s = reinterpret_cast<double*>(wsm);
+    double* mom_s = reinterpret_cast<double*>(wsm) + half * 64;
     const Tune& tu = A.tune;
-    // ---- sum the units' partials in unit order: lane owns moments lane and
-    // lane + 32 (45 = the objective); a moment's units are those of its shape
+    // ---- sum the units' partials in unit order: lane owns moments lane,
+    // lane + 16 and lane + 32 (45 = the objective); a moment's units are those
+    // of its shape
     {
         int us[6];
 #pragma unroll
@@ -559,27 +566,25 @@ extern "C" __global__ void __launch_bounds__(128, 4) wave_solve_kernel(WaveArgs 
             for (int u = u0; u < u1; u++) acc += P0[(int64_t)u * UNIT_VALS + col];
             return acc;
         };
-        const int sh0 = shape_of(lane);
-        const double m0 = sum_range(us[sh0], us[sh0 + 1], lane - shape_goff(sh0));
-        double m1 = 0.0;
-        const int l1 = lane + 32;
-        if (l1 == NMOM) {
-            m1 = sum_range(0, us[5], UNIT_VALS - 1);
-        } else if (l1 < NMOM) {
-            const int sh1 = shape_of(l1);
-            m1 = sum_range(us[sh1], us[sh1 + 1], l1 - shape_goff(sh1));
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+            const int m = lane + 16 * k;
+            if (m < NMOM) {
+                const int sh = shape_of(m);
+                mom_s[m] = sum_range(us[sh], us[sh + 1], m - shape_goff(sh));
+            } else if (m == NMOM) {
+                mom_s[m] = sum_range(0, us[5], UNIT_VALS - 1);
+            }
         }
-        mom_s[lane] = m0;
-        if (lane + 32 <= NMOM) mom_s[lane + 32] = m1;
     }
-    __syncwarp();
+    grp.sync();
     const int kind = S.kind;
     const double n = (double)S.n;
     double corr = 0.0;
     if (kind != PASS_FP64) {
         // FP32 passes ran on the hi coefficients
         if (lane == 0) mom_s[NMOM + 1] = lo_correction(mom_s, S.c32);
-        __syncwarp();
+        grp.sync();
         corr = mom_s[NMOM + 1];
     }
     const double obj = mom_s[NMOM];
@@ -597,9 +602,9 @@ extern "C" __global__ void __launch_bounds__(128, 4) wave_solve_kernel(WaveArgs 
 #pragma unroll
             for (int j = 0; j < 9; j++) Ht[j] = Ht[j] / n;
         }
-        gather9(-Sg / n, gt);
+        gather9(grp, -Sg / n, gt);
     }
-    __syncwarp();
+    grp.sync();
     if (lane == 0) {
         S.gh++;
         if (kind == PASS_FP64) S.f64p++;
@@ -628,7 +633,7 @@ extern "C" __global__ void __launch_bounds__(128, 4) wave_solve_kernel(WaveArgs 
                 S.alpha = alpha;
                 for (int k = 0; k < 9; k++) S.xt[k] = xn[k];
             }
-            schedule_pass(A, S, s, nkind, EV_TRIAL, lane);
+            schedule_pass(A, S, s, nkind, EV_TRIAL, lane, grp);
             return;
         }
         it = it + 1;
@@ -662,13 +667,13 @@ extern "C" __global__ void __launch_bounds__(128, 4) wave_solve_kernel(WaveArgs 
     if (!fp64 && !after_reeval && (conv || resid < 1e-6)) {
         const int near = S.near_count + (conv ? 0 : 1);
         if (lane == 0) S.near_count = near;
-        const double cond = conv ? condition_rows(x, g, Hr, tu.sqp_conv_tol) : 0.0;
+        const double cond = conv ? condition_rows(grp, x, g, Hr, tu.sqp_conv_tol) : 0.0;
         const bool recheck = conv ? !(cond <= COND_RECHECK) : (near >= 3);
         if (recheck) {
             // FP64 re-evaluation at the same point; the pair stays FP64 from here.
             if (lane == 0)
                 for (int k = 0; k < 9; k++) S.xt[k] = x[k];
-            schedule_pass(A, S, s, PASS_FP64, EV_REEVAL, lane);
+            schedule_pass(A, S, s, PASS_FP64, EV_REEVAL, lane, grp);
             return;
         }
         if (conv) {
@@ -677,15 +682,15 @@ extern "C" __global__ void __launch_bounds__(128, 4) wave_solve_kernel(WaveArgs 
         }
     }
     if (conv) {
-        finish_slot(A, S, s, x, f, it, condition_rows(x, g, Hr, tu.sqp_conv_tol), lane);
+        finish_slot(A, S, s, x, f, it, condition_rows(grp, x, g, Hr, tu.sqp_conv_tol), lane);
         return;
     }
     // ---- QP step (src/sqp.rs:78-83): c = g - H x, y = QP(H, c, x), p = y - x
     double cr = 0.0;
     if (lane < 9) cr = pick9(g, lane) - dot_fma(9, Hr, x);
     double c[9], y[9], p[9];
-    gather9(cr, c);
-    qp_simplex_rows(Hr, c, x, tu, lane, y);
+    gather9(grp, cr, c);
+    qp_simplex_rows(grp, Hr, c, x, tu, lane, y);
 #pragma unroll
     for (int k = 0; k < 9; k++) p[k] = y[k] - x[k];
     const double gp = dot_fma(9, g, p);
@@ -700,7 +705,7 @@ extern "C" __global__ void __launch_bounds__(128, 4) wave_solve_kernel(WaveArgs 
         S.alpha = 1.0;
         S.bls = 0;
     }
-    schedule_pass(A, S, s, nkind, EV_TRIAL, lane);
+    schedule_pass(A, S, s, nkind, EV_TRIAL, lane, grp);
 }
 
 // ------------------------------------------------------------------- host
@@ -806,7 +811,7 @@ int run_waves(const std::vector<PairJob>& jobs, const RunConfig& cfg, Workspace&
     std::vector<unsigned long long> h_done(table.size(), 0);
     std::vector<char> reported(table.size(), 0);
     int cur = 0;
-    const int slot_blocks = (int)((n_slots + WAVE_WPB - 1) / WAVE_WPB);
+    const int solve_blocks = (int)((n_slots + 2 * WAVE_WPB - 1) / (2 * WAVE_WPB));   // two slots per warp
     const size_t wsm = WAVE_WPB * WARP_SMEM;
     // events: per wave, before admit and after admit / pass / solve
     cudaEvent_t ev[4];
@@ -832,7 +837,7 @@ int run_waves(const std::vector<PairJob>& jobs, const RunConfig& cfg, Workspace&
         KG_WAVE_TRY(cudaEventRecord(ev[1], st));
         wave_pass_kernel<<<pass_blocks, 128, wsm, st>>>(A);
         KG_WAVE_TRY(cudaEventRecord(ev[2], st));
-        wave_solve_kernel<<<slot_blocks, 128, wsm, st>>>(A);
+        wave_solve_kernel<<<solve_blocks, 128, wsm, st>>>(A);
         KG_WAVE_TRY(cudaGetLastError());
         KG_WAVE_TRY(cudaEventRecord(ev[3], st));
         launches += 3;

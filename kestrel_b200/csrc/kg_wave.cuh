@@ -154,20 +154,21 @@ __device__ __forceinline__ int4 make_task(int s, int u, int64_t off, int64_t len
 
 // Queues slot s for a pass in the wave whose lists are (pass, tasks, wc): its
 // work units go to the shape-major task lists, so that the warps of the pass
-// kernel run one shape's code at a time.  Called by a whole warp after S.ustart
-// is set.
+// kernel run one shape's code at a time.  Called after S.ustart is set by W
+// lanes (a warp or a half-warp, given by mask); lane is the index among them.
+template <int W>
 __device__ inline void enqueue_pass(int* pass, int4* tasks, int64_t task_cap, WaveCounts* wc, int s,
-                                    const SlotState& S, int lane) {
+                                    const SlotState& S, int lane, unsigned mask) {
 #pragma unroll 1
     for (int sh = 0; sh < 5; sh++) {
         const int u0 = S.ustart[sh], nu = S.ustart[sh + 1] - u0;
         if (nu == 0) continue;
         int base = 0;
         if (lane == 0) base = atomicAdd(&wc->units[sh], nu);
-        base = __shfl_sync(0xffffffffu, base, 0);
+        base = __shfl_sync(mask, base, 0, W);
         const int64_t st = S.start[sh], cnt = S.cnt[sh];
         const int kind = S.kind;
-        for (int i = lane; i < nu; i += 32) {
+        for (int i = lane; i < nu; i += W) {
             const int64_t c0 = (int64_t)i * UNIT_ELEMS;
             tasks[sh * task_cap + base + i] = make_task(s, u0 + i, st + c0, min((int64_t)UNIT_ELEMS, cnt - c0), kind);
         }
