@@ -25,6 +25,24 @@ namespace kg {
         }                                                                       \
     } while (0)
 
+void PinBuf::release() {
+    if (p) cudaFreeHost(p);
+    p = nullptr;
+    bytes = 0;
+}
+
+int PinBuf::reserve(size_t n) {
+    if (n <= bytes && p) return cudaSuccess;
+    release();
+    cudaError_t e = cudaHostAlloc(&p, n, cudaHostAllocDefault);
+    if (e != cudaSuccess) {
+        p = nullptr;
+        return e;
+    }
+    bytes = n;
+    return cudaSuccess;
+}
+
 void DevBuf::release() {
     if (p) cudaFree(p);
     p = nullptr;

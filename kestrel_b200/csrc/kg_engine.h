@@ -17,6 +17,24 @@
 namespace kg {
 
 // Owning device buffer.
+// Page-locked host memory (cudaHostAlloc), grown and reused.
+struct PinBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    PinBuf() = default;
+    PinBuf(const PinBuf&) = delete;
+    PinBuf& operator=(const PinBuf&) = delete;
+    PinBuf(PinBuf&& o) noexcept : p(o.p), bytes(o.bytes) { o.p = nullptr; o.bytes = 0; }
+    PinBuf& operator=(PinBuf&& o) noexcept {
+        if (this != &o) { release(); p = o.p; bytes = o.bytes; o.p = nullptr; o.bytes = 0; }
+        return *this;
+    }
+    ~PinBuf() { release(); }
+    void release();
+    int reserve(size_t n);   // returns a cudaError_t
+    template <class T> T* as() const { return static_cast<T*>(p); }
+};
+
 struct DevBuf {
     void* p = nullptr;
     size_t bytes = 0;
@@ -107,6 +125,7 @@ struct RunConfig {
 struct Workspace {
     DevBuf scratch, queue, counters, table;
     DevBuf partial, slots, lists_a, lists_b, tasks, counts, done;
+    PinBuf host;   // per-wave counters read back by the host loop
     int sm_count = 0;
 };
 

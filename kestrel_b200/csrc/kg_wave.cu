@@ -808,48 +808,80 @@ int run_waves(const std::vector<PairJob>& jobs, const RunConfig& cfg, Workspace&
     A.tune = make_tune(cfg.iterations);
     A.counters = ws.counters.as<RunCounters>();
     A.cohort_done = ws.done.as<unsigned long long>();
-    std::vector<unsigned long long> h_done(table.size(), 0);
-    std::vector<char> reported(table.size(), 0);
-    int cur = 0;
     const int solve_blocks = (int)((n_slots + 2 * WAVE_WPB - 1) / (2 * WAVE_WPB));   // two slots per warp
     const size_t wsm = WAVE_WPB * WARP_SMEM;
-    // events: per wave, before admit and after admit / pass / solve
-    cudaEvent_t ev[4];
-    for (auto& e : ev) KG_WAVE_TRY(cudaEventCreate(&e));
-    struct EvGuard { cudaEvent_t* e; ~EvGuard() { for (int i = 0; i < 4; i++) cudaEventDestroy(e[i]); } } eg{ev};
+    // What the host reads after each wave, in page-locked memory so the graph
+    // can copy it: the next wave's counters, the pair queue, finished pairs per job.
+    const size_t hbytes = sizeof(WaveCounts) + sizeof(unsigned long long) * (1 + table.size());
+    KG_WAVE_TRY((cudaError_t)ws.host.reserve(hbytes));
+    WaveCounts* h_wc = ws.host.as<WaveCounts>();
+    unsigned long long* h_q = reinterpret_cast<unsigned long long*>(h_wc + 1);
+    unsigned long long* h_done = h_q + 1;
+    std::vector<char> reported(table.size(), 0);
+    // One wave (counter resets, admit, pass, solve, read-back) captured as a
+    // CUDA graph per parity of the current/next lists, then replayed: one
+    // launch per wave instead of a dozen API calls.  External event nodes time
+    // its phases.
+    struct WaveGraphs {
+        cudaGraph_t g[2] = {nullptr, nullptr};
+        cudaGraphExec_t x[2] = {nullptr, nullptr};
+        cudaEvent_t ev[2][4] = {};
+        ~WaveGraphs() {
+            for (int p = 0; p < 2; p++) {
+                if (x[p]) cudaGraphExecDestroy(x[p]);
+                if (g[p]) cudaGraphDestroy(g[p]);
+                for (auto& e : ev[p])
+                    if (e) cudaEventDestroy(e);
+            }
+        }
+    } wg;
+    for (int par = 0; par < 2; par++) {
+        for (auto& e : wg.ev[par]) KG_WAVE_TRY(cudaEventCreate(&e));
+        const int cur = par, nxt = par ^ 1;
+        WaveArgs Aw = A;
+        Aw.pass_cur = pass_l[cur];
+        Aw.pass_next = pass_l[nxt];
+        Aw.free_cur = free_l[cur];
+        Aw.free_next = free_l[nxt];
+        Aw.tasks_cur = tasks_l[cur];
+        Aw.tasks_next = tasks_l[nxt];
+        Aw.wc_cur = wc + cur;
+        Aw.wc_next = wc + nxt;
+        KG_WAVE_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+        cudaError_t ce = cudaEventRecordWithFlags(wg.ev[par][0], st, cudaEventRecordExternal);
+        if (ce == cudaSuccess) ce = cudaMemsetAsync(admit_task, 0, sizeof(int), st);
+        if (ce == cudaSuccess) ce = cudaMemsetAsync(q + 1, 0, sizeof(unsigned long long), st);
+        if (ce == cudaSuccess) ce = cudaMemsetAsync(wc + nxt, 0, sizeof(WaveCounts), st);
+        if (ce == cudaSuccess) {
+            wave_admit_kernel<<<admit_blocks, ADMIT_WARPS * 32, ADMIT_WARPS * ADMIT_WARP_SMEM, st>>>(Aw);
+            ce = cudaEventRecordWithFlags(wg.ev[par][1], st, cudaEventRecordExternal);
+        }
+        if (ce == cudaSuccess) {
+            wave_pass_kernel<<<pass_blocks, 128, wsm, st>>>(Aw);
+            ce = cudaEventRecordWithFlags(wg.ev[par][2], st, cudaEventRecordExternal);
+        }
+        if (ce == cudaSuccess) {
+            wave_solve_kernel<<<solve_blocks, 128, wsm, st>>>(Aw);
+            ce = cudaEventRecordWithFlags(wg.ev[par][3], st, cudaEventRecordExternal);
+        }
+        if (ce == cudaSuccess) ce = cudaMemcpyAsync(h_wc, wc + nxt, sizeof(WaveCounts), cudaMemcpyDeviceToHost, st);
+        if (ce == cudaSuccess) ce = cudaMemcpyAsync(h_q, q, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st);
+        if (ce == cudaSuccess && cfg.job_done)
+            ce = cudaMemcpyAsync(h_done, A.cohort_done, sizeof(unsigned long long) * table.size(),
+                                 cudaMemcpyDeviceToHost, st);
+        const cudaError_t ee = cudaStreamEndCapture(st, &wg.g[par]);
+        KG_WAVE_TRY(ce);
+        KG_WAVE_TRY(ee);
+        KG_WAVE_TRY(cudaGraphInstantiate(&wg.x[par], wg.g[par], 0));
+    }
     uint64_t waves = 0, launches = 1;
     double phase[3] = {0.0, 0.0, 0.0}, total = 0.0;
+    int cur = 0;
     for (;;) {
-        const int nxt = cur ^ 1;
-        A.pass_cur = pass_l[cur];
-        A.pass_next = pass_l[nxt];
-        A.free_cur = free_l[cur];
-        A.free_next = free_l[nxt];
-        A.tasks_cur = tasks_l[cur];
-        A.tasks_next = tasks_l[nxt];
-        A.wc_cur = wc + cur;
-        A.wc_next = wc + nxt;
-        KG_WAVE_TRY(cudaEventRecord(ev[0], st));
-        KG_WAVE_TRY(cudaMemsetAsync(admit_task, 0, sizeof(int), st));
-        KG_WAVE_TRY(cudaMemsetAsync(q + 1, 0, sizeof(unsigned long long), st));
-        KG_WAVE_TRY(cudaMemsetAsync(wc + nxt, 0, sizeof(WaveCounts), st));
-        wave_admit_kernel<<<admit_blocks, ADMIT_WARPS * 32, ADMIT_WARPS * ADMIT_WARP_SMEM, st>>>(A);
-        KG_WAVE_TRY(cudaEventRecord(ev[1], st));
-        wave_pass_kernel<<<pass_blocks, 128, wsm, st>>>(A);
-        KG_WAVE_TRY(cudaEventRecord(ev[2], st));
-        wave_solve_kernel<<<solve_blocks, 128, wsm, st>>>(A);
-        KG_WAVE_TRY(cudaGetLastError());
-        KG_WAVE_TRY(cudaEventRecord(ev[3], st));
+        KG_WAVE_TRY(cudaGraphLaunch(wg.x[cur], st));
+        KG_WAVE_TRY(cudaStreamSynchronize(st));
         launches += 3;
         waves++;
-        WaveCounts h;
-        unsigned long long hq = 0;
-        KG_WAVE_TRY(cudaMemcpyAsync(&h, wc + nxt, sizeof(h), cudaMemcpyDeviceToHost, st));
-        KG_WAVE_TRY(cudaMemcpyAsync(&hq, q, sizeof(hq), cudaMemcpyDeviceToHost, st));
-        if (cfg.job_done)
-            KG_WAVE_TRY(cudaMemcpyAsync(h_done.data(), A.cohort_done, sizeof(unsigned long long) * table.size(),
-                                        cudaMemcpyDeviceToHost, st));
-        KG_WAVE_TRY(cudaStreamSynchronize(st));
         if (cfg.job_done)
             for (size_t j = 0; j < table.size(); j++)
                 if (!reported[j] && h_done[j] >= (unsigned long long)table[j].n_pairs) {
@@ -858,11 +890,13 @@ int run_waves(const std::vector<PairJob>& jobs, const RunConfig& cfg, Workspace&
                 }
         for (int i = 0; i < 3; i++) {
             float ms = 0.f;
-            KG_WAVE_TRY(cudaEventElapsedTime(&ms, ev[i], ev[i + 1]));
+            KG_WAVE_TRY(cudaEventElapsedTime(&ms, wg.ev[cur][i], wg.ev[cur][i + 1]));
             phase[i] += ms;
             total += ms;
         }
-        cur = nxt;
+        const WaveCounts h = *h_wc;
+        const unsigned long long hq = *h_q;
+        cur ^= 1;
         if (h.n_pass == 0 && h.n_resort == 0 && hq >= (unsigned long long)total_pairs) break;
     }
     RunCounters rc;
