@@ -454,8 +454,8 @@ def main():
 
 
 # DRAM bytes (read + write) per pair-site-pass of wave_pass_kernel, measured by
-# ncu (profiles/wave_pass_kernel_N96_M100k.md): 1.985 GB over 447,339,158.
-PASS_DRAM_BYTES_PER_SITE = 4.44
+# ncu (profiles/wave_pass_kernel_N96_M100k.md): 1.959 GB over 447,339,158.
+PASS_DRAM_BYTES_PER_SITE = 4.38
 
 
 def ctypes_peak(device):

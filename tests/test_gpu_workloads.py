@@ -128,3 +128,17 @@ def test_cli_gt_and_pl_match_oracle(oracle):
     assert np.abs(kin - ref["jacquard"] @ kb.KINSHIP_VECTOR)[ident].max() <= 1e-5
     assert (np.abs(obj - ref["obj"]) / np.abs(ref["obj"])).max() <= 1e-6
     assert [r[0] for r in rows[:2]] == ["S0", "S0"] and [r[1] for r in rows[:2]] == ["S0", "S1"]
+
+
+def test_autotune_and_launch_shape_leave_results_unchanged():
+    co = synth.make_cohort(48, 4000, seed=51)
+    with kb.Estimator() as est:
+        est.load(co.codes)
+        base = est.relatedness()
+        slots, bps = est.autotune()
+        assert slots == 0 and bps in (3, 4, 5)
+        tuned = est.relatedness()
+        est.set_launch(64, 2)      # few slots in flight: many more waves
+        small = est.relatedness()
+        assert est.run_stats()["slots"] == 64
+    assert _bitwise_equal(base, tuned) and _bitwise_equal(base, small)
