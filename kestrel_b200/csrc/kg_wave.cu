@@ -91,7 +91,7 @@ __device__ inline void scatter_lockstep(const CohortDev& co, int64_t x, int64_t 
         }
         unsigned long long Q = (sizeof(T) == 4 ? ust : 0ull) + (inc - v);
         __syncwarp();
-#pragma unroll 8
+#pragma unroll
         for (int i = 0; i < 32; i++) {
             const int code = (int)((c0 & 1u) | ((c1 & 1u) << 1) | ((c2 & 1u) << 2));
             const bool flip = (sl & 1u) != 0;
