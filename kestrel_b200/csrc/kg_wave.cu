@@ -334,7 +334,7 @@ __device__ __noinline__ bool stream32_ring(const float* __restrict__ L, int64_t 
         const float4* B = R.buf + slot * STAGE_F4;
         const int64_t k = (int64_t)i * STAGE_F4 + lane;
 #pragma unroll
-        for (int half = 0; half < 2; half++) {
+        for (int half = 0; half < STAGE_F4 / 64; half++) {
             const int64_t kh = k + 64 * half;
             if (kh < n4) {
                 float g[NG], ob = 0.f;
