@@ -10,7 +10,7 @@
  *   src/coefficients.rs:143-151 struct Output
  * Every entry point takes plain pointers and sizes, returns a kg_status, and
  * never lets a C++ exception or a CUDA error escape; kg_last_error() gives the
- * message.  Buffers are caller-owned.  One context per host thread, except the
+ * message of the calling thread's last failing call.  Buffers are caller-owned.  One context per host thread, except the
  * serving calls (kg_panel_*, kg_submit/kg_poll/kg_wait/kg_cancel), which are
  * thread-safe.
  *

@@ -53,7 +53,6 @@ struct kg_ctx {
     int precision = KG_PREC_FP32C;
     int64_t wave_slots = 0;
     int pass_bps = 0;
-    std::string err;
     cudaStream_t stream = nullptr;
     // single cohort
     kg::Cohort cohort;
@@ -79,8 +78,13 @@ struct kg_ctx {
 
 namespace {
 
+// The message of the calling thread's last failing call: serving calls run on
+// several threads at once, so each thread keeps its own.
+thread_local std::string t_last_err;
+
 int set_err(kg_ctx* c, int st, const std::string& msg) {
-    if (c) c->err = msg;
+    (void)c;
+    t_last_err = msg;
     return st;
 }
 
@@ -323,7 +327,7 @@ int kg_destroy(kg_ctx* c) {
     return KG_OK;
 }
 
-const char* kg_last_error(const kg_ctx* c) { return c ? c->err.c_str() : "null context"; }
+const char* kg_last_error(const kg_ctx* c) { return c ? t_last_err.c_str() : "null context"; }
 
 int kg_set_precision(kg_ctx* c, int precision) {
     if (!c || (precision != KG_PREC_FP32C && precision != KG_PREC_FP64)) return set_err(c, KG_EINVAL, "precision must be KG_PREC_FP32C or KG_PREC_FP64");
@@ -448,7 +452,7 @@ int kg_relatedness(kg_ctx* c, int64_t num_samples, uint64_t iterations, double m
         stats.total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
         c->last = stats;
         if (n_out) *n_out = np;
-        if (st) return set_err(c, st, err.empty() ? c->err : err);
+        if (st) return set_err(c, st, err.empty() ? t_last_err : err);
         return KG_OK;
     });
 }
