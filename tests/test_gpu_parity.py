@@ -125,3 +125,31 @@ def test_python_api_build_arrays(oracle, cfg0):
     assert np.abs(co.inbreeding - inb).max() < 1e-5
     perm = [0, 1, 4, 5, 2, 3, 6, 7, 8]
     np.testing.assert_allclose(co.jacquard[3, 9], co.jacquard[9, 3][perm])
+
+
+def test_config1_full_size_sampled_pairs(est, oracle):
+    """The benchmark's own workload, N=1024 x M=100,000 (523,776 pairs + 1,024
+    self): 200 random pairs and every planted pair against the oracle, and the
+    size-independent properties of all rows (Delta on the simplex, finite
+    objective, kinship in [0, 1], planted relationships recovered)."""
+    c = synth.config1()
+    est.load(c.codes)
+    gpu = est.relatedness()
+    n = c.codes.shape[0]
+    assert len(gpu) == n * (n + 1) // 2
+    jac = gpu["jacquard"]
+    assert np.all(jac >= 0.0) and np.abs(jac.sum(1) - 1.0).max() < 1e-12
+    assert np.all(np.isfinite(gpu["obj"]))
+    kin = jac @ kb.KINSHIP_VECTOR
+    assert kin.min() >= 0.0 and kin.max() <= 1.0 + 1e-12
+    xs, ys = gpu["x"].astype(int), gpu["y"].astype(int)
+    pos = {(a, b): i for i, (a, b) in enumerate(zip(xs, ys))}
+    for a, b, rel, delta in c.planted:
+        i = pos[(a, b)]
+        assert np.abs(kin[i] - delta @ kb.KINSHIP_VECTOR) < 0.05, (rel, kin[i])
+    rng = np.random.default_rng(11)
+    idx = rng.choice(len(gpu), 200, replace=False)
+    idx = np.unique(np.concatenate([idx, [pos[(a, b)] for a, b, _, _ in c.planted]]))
+    p, q, keep = oracle.site_frequencies(c.codes)
+    ref = oracle.relatedness_pairs(c.codes, p, q, keep, np.stack([xs[idx], ys[idx]], 1))
+    print(compare(gpu[idx], ref), est.run_stats()["nonconverged"])
