@@ -206,11 +206,17 @@ void serve_batch(kg_ctx* c, Slot& slot, std::vector<std::shared_ptr<Request>>& b
 }
 
 // The scheduler: admits every queued request whose inputs fit the memory
-// budget into one batched launch (continuous batching); one batch per slot,
-// slots run concurrently on their own streams.
+// budget into one batch (continuous batching); one batch per serving slot,
+// kServeSlots of them running concurrently on their own streams, so a request
+// that arrives while others run starts as soon as a slot frees.
+constexpr int kServeSlots = 4;
 void serve_loop(kg_ctx* c) {
     cudaSetDevice(c->device);
-    std::vector<std::thread> workers;
+    struct Worker {
+        std::thread t;
+        std::shared_ptr<std::atomic<bool>> done;
+    };
+    std::vector<Worker> workers;
     const size_t kMaxPairs = (size_t)1 << 22;
     for (;;) {
         std::vector<std::shared_ptr<Request>> batch;
@@ -261,21 +267,28 @@ void serve_loop(kg_ctx* c) {
             if (batch.empty()) continue;
             c->slots[slot_idx].busy = true;
         }
-        workers.emplace_back([c, slot_idx, batch]() mutable {
-            cudaSetDevice(c->device);
-            serve_batch(c, c->slots[slot_idx], batch);
-            std::lock_guard<std::mutex> lk(c->mu);
-            c->slots[slot_idx].busy = false;
-            c->cv.notify_all();
-        });
-        // reap finished workers
-        if (workers.size() > 8) {
-            for (auto& w : workers) if (w.joinable()) w.join();
-            workers.clear();
+        auto done = std::make_shared<std::atomic<bool>>(false);
+        workers.push_back({std::thread([c, slot_idx, batch, done]() mutable {
+                               cudaSetDevice(c->device);
+                               serve_batch(c, c->slots[slot_idx], batch);
+                               std::lock_guard<std::mutex> lk(c->mu);
+                               c->slots[slot_idx].busy = false;
+                               done->store(true);
+                               c->cv.notify_all();
+                           }),
+                           done});
+        // reap the workers that have finished (never wait on a running one)
+        for (auto it = workers.begin(); it != workers.end();) {
+            if (it->done->load()) {
+                it->t.join();
+                it = workers.erase(it);
+            } else {
+                ++it;
+            }
         }
     }
     for (auto& w : workers)
-        if (w.joinable()) w.join();
+        if (w.t.joinable()) w.t.join();
 }
 
 }  // namespace
@@ -625,7 +638,7 @@ int kg_panel_load(kg_ctx* c, const uint8_t* codes, int64_t n_samples, int64_t n_
         c->panel.raw.release();
         c->panel_ready = true;
         if (c->slots.empty()) {
-            c->slots.resize(2);
+            c->slots.resize(kServeSlots);
             for (auto& s : c->slots)
                 if (cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking) != cudaSuccess)
                     return set_err(c, KG_ECUDA, "cannot create serving streams");
