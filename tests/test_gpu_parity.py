@@ -153,3 +153,15 @@ def test_config1_full_size_sampled_pairs(est, oracle):
     p, q, keep = oracle.site_frequencies(c.codes)
     ref = oracle.relatedness_pairs(c.codes, p, q, keep, np.stack([xs[idx], ys[idx]], 1))
     print(compare(gpu[idx], ref), est.run_stats()["nonconverged"])
+
+
+def test_config0_against_committed_golden_rows(est):
+    """The CUDA path on the committed config-0 genotypes against the committed
+    oracle rows (no live oracle run)."""
+    import os
+    g = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "config0_oracle.npz"))
+    ref = np.zeros(len(g["x"]), kb.OUTPUT_DTYPE)
+    for k in ("x", "y", "jacquard", "obj", "iters", "cond"):
+        ref[k] = g[k]
+    est.load(g["codes"])
+    print(compare(est.relatedness(), ref))

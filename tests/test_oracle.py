@@ -95,3 +95,20 @@ def test_no_jointly_observed_site_is_an_error(oracle):
     codes = np.array([[0, 1, 2, 3, 3], [3, 3, 3, 0, 1], [1, 1, 0, 2, 0]], np.uint8)
     with pytest.raises(RuntimeError):
         oracle.relatedness(codes)
+
+
+def _golden():
+    import os
+    g = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "config0_oracle.npz"))
+    return {k: g[k] for k in g.files}
+
+
+def test_oracle_reproduces_committed_golden_rows(oracle):
+    """The oracle on the committed config-0 genotypes gives the committed rows
+    (tests/golden/make_golden.py), to the last few ulps across hosts."""
+    g = _golden()
+    rows = oracle.relatedness(g["codes"])
+    assert np.array_equal(rows["x"], g["x"]) and np.array_equal(rows["y"], g["y"])
+    assert np.array_equal(rows["iters"], g["iters"])
+    assert np.abs(rows["jacquard"] - g["jacquard"]).max() <= 1e-12
+    assert (np.abs(rows["obj"] - g["obj"]) / np.abs(g["obj"])).max() <= 1e-12
