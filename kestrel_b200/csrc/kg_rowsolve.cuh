@@ -50,15 +50,6 @@ __device__ __forceinline__ double pick9(const double* v, int r) {
     return o;
 }
 
-// Maximum over lanes; NaN wins (total order of the reference's max_by).
-__device__ __forceinline__ double warp_max_nan(double v) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        double w = __shfl_xor_sync(FULL_MASK, v, o);
-        v = (isnan(v) || isnan(w)) ? CUDART_NAN : fmax(v, w);
-    }
-    return v;
-}
 
 // Maximum over the group's lanes of non-negative values (NaN counts as 0, as
 // fmax drops it): for doubles >= 0 the bit patterns order as the values, so

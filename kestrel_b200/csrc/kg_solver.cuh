@@ -4,11 +4,10 @@
 // the results are warp-uniform without broadcasts; the arrays live in each
 // lane's local memory (L1-cached).  The algorithm is the reference's, restated:
 //   check_convergence        src/sqp.rs:95-109
-//   solve_qp_active_set      src/sqp.rs:112-250   (modify = true, <= 10 its)
-//   feasible_step_size       src/sqp.rs:252-268
 //   estimate_condition_number src/sqp.rs:313-391
-//   modify_gmw_n / unmodified_n / solve_ldl_mut_n src/cholesky.rs:6-140
+//   unmodified_n / forward and back substitution  src/cholesky.rs:66-140
 //   dot (fma chain), sum_to_one  src/algebra.rs:4-84
+// The QP and its GMW81-modified LDL^T run row-parallel (kg_rowsolve.cuh).
 #pragma once
 
 #include <cstdint>
@@ -81,39 +80,6 @@ __device__ inline bool kkt_ok(const double* x, const double* g, double tol, doub
     return ok;
 }
 
-// GMW81-style modified LDL^T on the leading n x n block of a (row stride 9).
-__device__ inline void ldl_gmw(int n, const double* a, double* l, double* d) {
-    double gamma = 0.0, xi = 0.0;
-    for (int i = 0; i < n; i++) gamma = fmax(gamma, fabs(a[i * 9 + i]));
-    for (int i = 0; i < n; i++)
-        for (int j = i + 1; j < n; j++) xi = fmax(xi, fabs(a[i * 9 + j]));
-    const double eps = 2.220446049250313e-16;
-    double delta = eps * fmax(1.0, gamma + xi);
-    double t = sqrt((double)n * (double)n - 1.0);
-    double ratio = (n <= 1) ? 0.0 : xi / t;
-    double beta2 = fmax(fmax(gamma, ratio), eps);
-    double pv[9];
-    for (int j = 0; j < n; j++) {
-        double sjj = 0.0;
-        for (int s = 0; s < j; s++) {
-            pv[s] = d[s] * l[j * 9 + s];
-            sjj = fma(pv[s], l[j * 9 + s], sjj);
-        }
-        double cjj = a[j * 9 + j] - sjj;
-        l[j * 9 + j] = 1.0;
-        double theta = 0.0;
-        for (int i = j + 1; i < n; i++) {
-            double sij = 0.0;
-            for (int s = 0; s < j; s++) sij = fma(pv[s], l[i * 9 + s], sij);
-            double cij = a[i * 9 + j] - sij;
-            theta = fmax(theta, fabs(cij));
-            l[i * 9 + j] = cij;
-        }
-        double dj = fmax(fmax(fabs(cjj), theta * theta / beta2), delta);
-        for (int i = j + 1; i < n; i++) l[i * 9 + j] /= dj;
-        d[j] = dj;
-    }
-}
 
 // Plain LDL^T (no pivoting, no modification).
 __device__ inline void ldl_plain(int n, const double* a, double* l, double* d) {
@@ -151,77 +117,7 @@ __device__ __forceinline__ void unit_upper_solve_t(int n, const double* l, doubl
     }
 }
 
-__device__ __forceinline__ void ldl_solve(int n, const double* l, const double* d, double* b) {
-    unit_lower_solve(n, l, b);
-    for (int i = 0; i < n; i++) b[i] /= d[i];
-    unit_upper_solve_t(n, l, b);
-}
 
-// min 1/2 y'Qy + c'y  s.t. y >= 0, sum(y) = 1, started from y0.
-__device__ inline void qp_simplex(const double* Q, const double* c, const double* y0,
-                                  const Tune& tu, double* y) {
-    bool work[9];
-    for (int i = 0; i < 9; i++) {
-        y[i] = y0[i];
-        work[i] = (y[i] == 0.0);
-    }
-    for (int it = 0; it < tu.qp_max_iter; it++) {
-        normalise9(y);
-        int fi[9];
-        int nf = 0;
-        for (int i = 0; i < 9; i++)
-            if (!work[i]) fi[nf++] = i;
-        if (nf == 0) return;  // the reference asserts; unreachable for a simplex start
-        double yf[9], cf[9], Qf[81], L[81], D[9], gf[9], ones[9];
-        for (int i = 0; i < 9; i++) {
-            yf[i] = 0.0; cf[i] = 0.0; D[i] = 0.0; gf[i] = 0.0; ones[i] = 0.0;
-        }
-        for (int i = 0; i < 81; i++) { Qf[i] = 0.0; L[i] = 0.0; }
-        for (int i = 0; i < nf; i++) {
-            yf[i] = y[fi[i]];
-            cf[i] = c[fi[i]];
-            for (int j = 0; j < nf; j++) Qf[i * 9 + j] = Q[fi[i] * 9 + fi[j]];
-        }
-        for (int i = 0; i < nf; i++) gf[i] = cf[i] + dot_fma(nf, Qf + i * 9, yf);
-        ldl_gmw(nf, Qf, L, D);
-        ldl_solve(nf, L, D, gf);
-        for (int i = 0; i < nf; i++) ones[i] = 1.0;
-        ldl_solve(nf, L, D, ones);
-        double lambda = sum_seq(nf, gf) / sum_seq(nf, ones);
-        double m = 0.0;
-        bool m_nan = false;
-        for (int i = 0; i < 9; i++) {
-            gf[i] = lambda * ones[i] - gf[i];
-            double a = fabs(gf[i]);
-            if (isnan(a)) m_nan = true;
-            else m = fmax(m, a);
-        }
-        if (!m_nan && m <= tu.qp_zero_search_tol) {
-            if (nf == 9) return;
-            double gq[9];
-            for (int i = 0; i < 9; i++) gq[i] = c[i] + dot_fma(9, Q + i * 9, y);
-            int best = -1;
-            for (int i = 0; i < 9; i++)
-                if (work[i] && (best < 0 || gq[i] < gq[best])) best = i;
-            if (gq[best] - lambda >= -tu.qp_conv_tol) return;
-            work[best] = false;
-        } else {
-            double p[9];
-            int k = 0;
-            for (int i = 0; i < 9; i++) p[i] = work[i] ? 0.0 : gf[k++];
-            double alpha = 1.0;
-            int block = -1;
-            for (int i = 0; i < 9; i++) {
-                if (p[i] < 0.0) {
-                    double a = -y[i] / p[i];
-                    if (a < alpha) { alpha = a; block = i; }
-                }
-            }
-            for (int i = 0; i < 9; i++) y[i] = fmax(y[i] + alpha * p[i], 0.0);
-            if (block >= 0) { work[block] = true; y[block] = 0.0; }
-        }
-    }
-}
 
 // Condition estimate of the reduced Hessian at a KKT point.
 __device__ inline double condition_estimate(const double* x, const double* g, const double* H,
