@@ -893,7 +893,12 @@ __device__ inline void evaluate(const PairLists& pl, const void* lists, int kind
 }
 
 constexpr double COND_RECHECK = 1e4;   // FP32 condition estimates above this are redone in FP64
-constexpr double DIFF_BELOW = 1e-4;    // |alpha g.p| under which the objective change is summed directly
+// |alpha g.p| under which the objective change is summed directly.  The
+// direct FP32 objective (one lg2 per four sites, rounding ~3e-7 in log2 units
+// per call, independent across calls) is off by ~3e-10 at n = 1e5 sites, and
+// the Armijo test's margin is about |alpha g.p| / 2: at 1e-7 that margin is
+// ~70 times the error of the difference f_new - f_old.
+constexpr double DIFF_BELOW = 1e-7;
 
 struct PairResult {
     unsigned long long cyc_pass;    // clocks spent in site passes
