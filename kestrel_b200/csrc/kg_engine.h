@@ -133,7 +133,39 @@ int run_pairs(const std::vector<PairJob>& jobs, const RunConfig& cfg, Workspace&
               cudaStream_t st, kg_run_stats& stats, std::string& err);
 
 struct CohortDev;
-// The wave loop (kg_wave.cu) over a prepared cohort table.
+
+// The wave engine (kg_wave.cu): up to n_slots pairs in flight over a job
+// table that can grow between waves (the serving loop appends requests while
+// others run).  open() sizes it for lists of up to list_cap entries and at most
+// max_jobs jobs; add() appends jobs (their pair_begin is assigned); wave() runs
+// one admit / pass / solve wave and appends the jobs whose pairs are all done
+// to `finished`; idle() is true when nothing is in flight and every pair has
+// been taken.
+class WaveEngine {
+  public:
+    WaveEngine();
+    ~WaveEngine();
+    WaveEngine(const WaveEngine&) = delete;
+    WaveEngine& operator=(const WaveEngine&) = delete;
+    int open(Workspace& ws, cudaStream_t st, const RunConfig& cfg, int64_t list_cap, int64_t expected_pairs,
+             int max_jobs, std::string& err);
+    int add(const std::vector<CohortDev>& jobs, std::string& err);
+    int wave(std::vector<int>& finished, std::string& err);
+    bool idle() const;
+    int64_t n_slots() const;
+    int64_t list_cap() const;
+    // Empties the job table (only when idle), so a long-running loop reuses it.
+    int reset_jobs(std::string& err);
+    // Counters and phase times since open().
+    int stats(kg_run_stats& stats, std::string& err);
+
+  private:
+    struct Impl;
+    Impl* d_;
+};
+
+// All jobs of one call through one engine (kg_wave.cu), over a prepared
+// cohort table.
 int run_waves(const std::vector<PairJob>& jobs, const RunConfig& cfg, Workspace& ws, cudaStream_t st,
               kg_run_stats& stats, std::string& err, const std::vector<CohortDev>& table,
               int64_t total_pairs, int64_t list_cap);

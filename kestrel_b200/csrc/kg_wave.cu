@@ -211,7 +211,11 @@ extern "C" __global__ void __launch_bounds__(ADMIT_WARPS * 32, 4) wave_admit_ker
             __syncthreads();
             const unsigned long long k = sh_k;
             __syncthreads();
-            if (k >= (unsigned long long)A.total_pairs) break;
+            if (k >= (unsigned long long)A.live->total_pairs) {
+                // no pair left for now: the slot waits in the next free list
+                if (threadIdx.x == 0) A.free_next[atomicAdd(&A.wc_next->n_free, 1)] = s;
+                break;
+            }
             int c;
             int64_t j, x, y;
             decode_pair(A, (int64_t)k, c, j, x, y);
@@ -715,56 +719,112 @@ __global__ void wave_iota_kernel(int* v, int n) {
     if (i < n) v[i] = i;
 }
 
-int run_waves(const std::vector<PairJob>& jobs, const RunConfig& cfg, Workspace& ws,
-              cudaStream_t st, kg_run_stats& stats, std::string& err,
-              const std::vector<CohortDev>& table, int64_t total_pairs, int64_t list_cap) {
-    (void)jobs;
+// ------------------------------------------------------------ the engine
+
+struct WaveEngine::Impl {
+    Workspace* ws = nullptr;
+    cudaStream_t st = nullptr;
+    RunConfig cfg;
+    int64_t n_slots = 0, list_cap = 0, task_cap = 0;
+    int max_units = 0, max_jobs = 0;
+    int pass_blocks = 0, admit_blocks = 0, solve_blocks = 0;
+    WaveArgs A{};
+    WaveCounts* wc = nullptr;
+    int* admit_task = nullptr;
+    unsigned long long* q = nullptr;
+    LiveQueue* live_d = nullptr;
+    // host side
+    std::vector<CohortDev> table;
+    std::vector<char> reported;
+    LiveQueue* live_h = nullptr;          // page-locked staging of the live extent
+    WaveCounts* h_wc = nullptr;
+    unsigned long long* h_q = nullptr;
+    unsigned long long* h_done = nullptr;
+    unsigned long long last_q = 0;
+    int cur = 0;
+    bool idle = true;
+    uint64_t waves = 0, launches = 0;
+    double phase[3] = {0.0, 0.0, 0.0}, total = 0.0;
+    // one wave captured per parity of the current/next lists
+    cudaGraph_t g[2] = {nullptr, nullptr};
+    cudaGraphExec_t x[2] = {nullptr, nullptr};
+    cudaEvent_t ev[2][4] = {};
+    ~Impl() {
+        for (int p = 0; p < 2; p++) {
+            if (x[p]) cudaGraphExecDestroy(x[p]);
+            if (g[p]) cudaGraphDestroy(g[p]);
+            for (auto& e : ev[p])
+                if (e) cudaEventDestroy(e);
+        }
+    }
+};
+
+WaveEngine::WaveEngine() : d_(new Impl) {}
+WaveEngine::~WaveEngine() { delete d_; }
+
+int WaveEngine::open(Workspace& ws, cudaStream_t st, const RunConfig& cfg, int64_t list_cap,
+                     int64_t expected_pairs, int max_jobs, std::string& err) {
+    Impl& E = *d_;
+    E.ws = &ws;
+    E.st = st;
+    E.cfg = cfg;
+    E.list_cap = list_cap;
+    E.max_jobs = std::max(1, max_jobs);
     int dev = 0;
     KG_WAVE_TRY(cudaGetDevice(&dev));
     if (ws.sm_count == 0) KG_WAVE_TRY(cudaDeviceGetAttribute(&ws.sm_count, cudaDevAttrMultiProcessorCount, dev));
     // work units: per shape at most ceil(list_cap / UNIT_ELEMS), over the five
     // shapes at most that + 5
     const int64_t shape_units = (list_cap + UNIT_ELEMS - 1) / UNIT_ELEMS;
-    const int max_units = (int)shape_units + 5;
+    E.max_units = (int)shape_units + 5;
     // slots: as many as the work and the memory allow
-    const size_t per_slot = sizeof(double) * (size_t)list_cap + sizeof(double) * max_units * UNIT_VALS +
+    const size_t per_slot = sizeof(double) * (size_t)list_cap + sizeof(double) * E.max_units * UNIT_VALS +
                             sizeof(SlotState) + 4 * sizeof(int) + 2 * 5 * shape_units * sizeof(int4);
     size_t fr = 0, tot = 0;
     KG_WAVE_TRY(cudaMemGetInfo(&fr, &tot));
-    int64_t want = cfg.slots > 0 ? cfg.slots : 16384;
-    int64_t by_mem = (int64_t)((fr / 2) / per_slot);
-    int64_t n_slots = std::max<int64_t>(1, std::min<int64_t>({want, by_mem, total_pairs}));
-    const int64_t task_cap = n_slots * shape_units;
+    const int64_t want = cfg.slots > 0 ? cfg.slots : 16384;
+    const int64_t by_mem = (int64_t)((fr / 2) / per_slot);
+    E.n_slots = std::max<int64_t>(1, std::min<int64_t>({want, by_mem, std::max<int64_t>(1, expected_pairs)}));
+    const int64_t n_slots = E.n_slots;
+    E.task_cap = n_slots * shape_units;
     // device buffers (grown and reused through the workspace)
     KG_WAVE_TRY((cudaError_t)ws.scratch.reserve(sizeof(double) * (size_t)list_cap * n_slots));
-    KG_WAVE_TRY((cudaError_t)ws.partial.reserve(sizeof(double) * (size_t)max_units * UNIT_VALS * n_slots));
+    KG_WAVE_TRY((cudaError_t)ws.partial.reserve(sizeof(double) * (size_t)E.max_units * UNIT_VALS * n_slots));
     KG_WAVE_TRY((cudaError_t)ws.slots.reserve(sizeof(SlotState) * n_slots));
     KG_WAVE_TRY((cudaError_t)ws.lists_a.reserve(sizeof(int) * 2 * n_slots));   // pass lists
     KG_WAVE_TRY((cudaError_t)ws.lists_b.reserve(sizeof(int) * 2 * n_slots));   // free lists
-    KG_WAVE_TRY((cudaError_t)ws.tasks.reserve(sizeof(int4) * 2 * 5 * task_cap));
-    KG_WAVE_TRY((cudaError_t)ws.counts.reserve(sizeof(WaveCounts) * 2 + 64));
+    KG_WAVE_TRY((cudaError_t)ws.tasks.reserve(sizeof(int4) * 2 * 5 * E.task_cap));
+    KG_WAVE_TRY((cudaError_t)ws.counts.reserve(sizeof(WaveCounts) * 2 + 64 + sizeof(LiveQueue)));
     KG_WAVE_TRY((cudaError_t)ws.queue.reserve(sizeof(unsigned long long) * 2));
     KG_WAVE_TRY((cudaError_t)ws.counters.reserve(sizeof(RunCounters)));
-    KG_WAVE_TRY((cudaError_t)ws.table.reserve(sizeof(CohortDev) * table.size()));
-    KG_WAVE_TRY((cudaError_t)ws.done.reserve(sizeof(unsigned long long) * table.size()));
-    KG_WAVE_TRY(cudaMemsetAsync(ws.done.p, 0, sizeof(unsigned long long) * table.size(), st));
-    KG_WAVE_TRY(cudaMemcpyAsync(ws.table.p, table.data(), sizeof(CohortDev) * table.size(),
-                                cudaMemcpyHostToDevice, st));
-    WaveCounts* wc = reinterpret_cast<WaveCounts*>(ws.counts.p);
-    int* admit_task = reinterpret_cast<int*>(wc + 2);
-    unsigned long long* q = ws.queue.as<unsigned long long>();   // [0] pairs, [1] pass units
+    KG_WAVE_TRY((cudaError_t)ws.table.reserve(sizeof(CohortDev) * E.max_jobs));
+    KG_WAVE_TRY((cudaError_t)ws.done.reserve(sizeof(unsigned long long) * E.max_jobs));
+    E.wc = reinterpret_cast<WaveCounts*>(ws.counts.p);
+    E.admit_task = reinterpret_cast<int*>(E.wc + 2);
+    E.live_d = reinterpret_cast<LiveQueue*>(reinterpret_cast<char*>(ws.counts.p) + sizeof(WaveCounts) * 2 + 64);
+    E.q = ws.queue.as<unsigned long long>();   // [0] pairs, [1] pass units
     int* pass_l[2] = {ws.lists_a.as<int>(), ws.lists_a.as<int>() + n_slots};
     int* free_l[2] = {ws.lists_b.as<int>(), ws.lists_b.as<int>() + n_slots};
-    int4* tasks_l[2] = {ws.tasks.as<int4>(), ws.tasks.as<int4>() + 5 * task_cap};
+    int4* tasks_l[2] = {ws.tasks.as<int4>(), ws.tasks.as<int4>() + 5 * E.task_cap};
+    // host read-back (page-locked so the graph can copy into it)
+    const size_t hbytes = sizeof(LiveQueue) + sizeof(WaveCounts) + sizeof(unsigned long long) * (1 + E.max_jobs);
+    KG_WAVE_TRY((cudaError_t)ws.host.reserve(hbytes));
+    E.live_h = ws.host.as<LiveQueue>();
+    E.h_wc = reinterpret_cast<WaveCounts*>(E.live_h + 1);
+    E.h_q = reinterpret_cast<unsigned long long*>(E.h_wc + 1);
+    E.h_done = E.h_q + 1;
+    E.live_h->total_pairs = 0;
+    E.live_h->n_cohorts = 0;
     KG_WAVE_TRY(cudaMemsetAsync(ws.slots.p, 0, sizeof(SlotState) * n_slots, st));   // all SLOT_FREE
     KG_WAVE_TRY(cudaMemsetAsync(ws.queue.p, 0, sizeof(unsigned long long) * 2, st));
-    KG_WAVE_TRY(cudaMemsetAsync(ws.counts.p, 0, sizeof(WaveCounts) * 2 + 64, st));
+    KG_WAVE_TRY(cudaMemsetAsync(ws.counts.p, 0, sizeof(WaveCounts) * 2 + 64 + sizeof(LiveQueue), st));
     KG_WAVE_TRY(cudaMemsetAsync(ws.counters.p, 0, sizeof(RunCounters), st));
-    // the first wave admits every slot
+    KG_WAVE_TRY(cudaMemsetAsync(ws.done.p, 0, sizeof(unsigned long long) * E.max_jobs, st));
+    // the first wave's free list holds every slot
     wave_iota_kernel<<<(int)((n_slots + 255) / 256), 256, 0, st>>>(free_l[0], (int)n_slots);
     {
         const int nf = (int)n_slots;
-        KG_WAVE_TRY(cudaMemcpyAsync(&wc[0].n_free, &nf, sizeof(int), cudaMemcpyHostToDevice, st));
+        KG_WAVE_TRY(cudaMemcpyAsync(&E.wc[0].n_free, &nf, sizeof(int), cudaMemcpyHostToDevice, st));
         KG_WAVE_TRY(cudaStreamSynchronize(st));   // nf lives on this stack frame
     }
     static bool attr = false;
@@ -781,7 +841,7 @@ int run_waves(const std::vector<PairJob>& jobs, const RunConfig& cfg, Workspace&
         return KG_ECUDA;
     }
     if (cfg.pass_blocks_per_sm > 0) occ = std::min(occ, cfg.pass_blocks_per_sm);
-    const int pass_blocks = ws.sm_count * occ;
+    E.pass_blocks = ws.sm_count * occ;
     int aocc = 0;
     KG_WAVE_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&aocc, wave_admit_kernel, ADMIT_WARPS * 32,
                                                               ADMIT_WARPS * ADMIT_WARP_SMEM));
@@ -789,54 +849,33 @@ int run_waves(const std::vector<PairJob>& jobs, const RunConfig& cfg, Workspace&
         err = "admit kernel cannot be resident";
         return KG_ECUDA;
     }
-    const int admit_blocks = ws.sm_count * aocc;
-    WaveArgs A;
+    E.admit_blocks = ws.sm_count * aocc;
+    E.solve_blocks = (int)((n_slots + 2 * WAVE_WPB - 1) / (2 * WAVE_WPB));   // two slots per warp
+    WaveArgs& A = E.A;
     A.cohorts = ws.table.as<CohortDev>();
-    A.n_cohorts = (int)table.size();
+    A.live = E.live_d;
     A.precision = cfg.precision;
-    A.total_pairs = total_pairs;
-    A.queue = q;
+    A.queue = E.q;
     A.slots = ws.slots.as<SlotState>();
     A.n_slots = (int)n_slots;
     A.lists = ws.scratch.as<double>();
     A.list_stride = list_cap;
     A.partial = ws.partial.as<double>();
-    A.max_units = max_units;
-    A.task_cap = task_cap;
-    A.pass_task = q + 1;
-    A.admit_task = admit_task;
+    A.max_units = E.max_units;
+    A.task_cap = E.task_cap;
+    A.pass_task = E.q + 1;
+    A.admit_task = E.admit_task;
     A.tune = make_tune(cfg.iterations);
     A.counters = ws.counters.as<RunCounters>();
     A.cohort_done = ws.done.as<unsigned long long>();
-    const int solve_blocks = (int)((n_slots + 2 * WAVE_WPB - 1) / (2 * WAVE_WPB));   // two slots per warp
-    const size_t wsm = WAVE_WPB * WARP_SMEM;
-    // What the host reads after each wave, in page-locked memory so the graph
-    // can copy it: the next wave's counters, the pair queue, finished pairs per job.
-    const size_t hbytes = sizeof(WaveCounts) + sizeof(unsigned long long) * (1 + table.size());
-    KG_WAVE_TRY((cudaError_t)ws.host.reserve(hbytes));
-    WaveCounts* h_wc = ws.host.as<WaveCounts>();
-    unsigned long long* h_q = reinterpret_cast<unsigned long long*>(h_wc + 1);
-    unsigned long long* h_done = h_q + 1;
-    std::vector<char> reported(table.size(), 0);
     // One wave (counter resets, admit, pass, solve, read-back) captured as a
     // CUDA graph per parity of the current/next lists, then replayed: one
     // launch per wave instead of a dozen API calls.  External event nodes time
     // its phases.
-    struct WaveGraphs {
-        cudaGraph_t g[2] = {nullptr, nullptr};
-        cudaGraphExec_t x[2] = {nullptr, nullptr};
-        cudaEvent_t ev[2][4] = {};
-        ~WaveGraphs() {
-            for (int p = 0; p < 2; p++) {
-                if (x[p]) cudaGraphExecDestroy(x[p]);
-                if (g[p]) cudaGraphDestroy(g[p]);
-                for (auto& e : ev[p])
-                    if (e) cudaEventDestroy(e);
-            }
-        }
-    } wg;
+    const size_t wsm = WAVE_WPB * WARP_SMEM;
+    WaveCounts* wc = E.wc;
     for (int par = 0; par < 2; par++) {
-        for (auto& e : wg.ev[par]) KG_WAVE_TRY(cudaEventCreate(&e));
+        for (auto& e : E.ev[par]) KG_WAVE_TRY(cudaEventCreate(&e));
         const int cur = par, nxt = par ^ 1;
         WaveArgs Aw = A;
         Aw.pass_cur = pass_l[cur];
@@ -848,77 +887,140 @@ int run_waves(const std::vector<PairJob>& jobs, const RunConfig& cfg, Workspace&
         Aw.wc_cur = wc + cur;
         Aw.wc_next = wc + nxt;
         KG_WAVE_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-        cudaError_t ce = cudaEventRecordWithFlags(wg.ev[par][0], st, cudaEventRecordExternal);
-        if (ce == cudaSuccess) ce = cudaMemsetAsync(admit_task, 0, sizeof(int), st);
-        if (ce == cudaSuccess) ce = cudaMemsetAsync(q + 1, 0, sizeof(unsigned long long), st);
+        cudaError_t ce = cudaEventRecordWithFlags(E.ev[par][0], st, cudaEventRecordExternal);
+        if (ce == cudaSuccess) ce = cudaMemsetAsync(E.admit_task, 0, sizeof(int), st);
+        if (ce == cudaSuccess) ce = cudaMemsetAsync(E.q + 1, 0, sizeof(unsigned long long), st);
         if (ce == cudaSuccess) ce = cudaMemsetAsync(wc + nxt, 0, sizeof(WaveCounts), st);
         if (ce == cudaSuccess) {
-            wave_admit_kernel<<<admit_blocks, ADMIT_WARPS * 32, ADMIT_WARPS * ADMIT_WARP_SMEM, st>>>(Aw);
-            ce = cudaEventRecordWithFlags(wg.ev[par][1], st, cudaEventRecordExternal);
+            wave_admit_kernel<<<E.admit_blocks, ADMIT_WARPS * 32, ADMIT_WARPS * ADMIT_WARP_SMEM, st>>>(Aw);
+            ce = cudaEventRecordWithFlags(E.ev[par][1], st, cudaEventRecordExternal);
         }
         if (ce == cudaSuccess) {
-            wave_pass_kernel<<<pass_blocks, 128, wsm, st>>>(Aw);
-            ce = cudaEventRecordWithFlags(wg.ev[par][2], st, cudaEventRecordExternal);
+            wave_pass_kernel<<<E.pass_blocks, 128, wsm, st>>>(Aw);
+            ce = cudaEventRecordWithFlags(E.ev[par][2], st, cudaEventRecordExternal);
         }
         if (ce == cudaSuccess) {
-            wave_solve_kernel<<<solve_blocks, 128, wsm, st>>>(Aw);
-            ce = cudaEventRecordWithFlags(wg.ev[par][3], st, cudaEventRecordExternal);
+            wave_solve_kernel<<<E.solve_blocks, 128, wsm, st>>>(Aw);
+            ce = cudaEventRecordWithFlags(E.ev[par][3], st, cudaEventRecordExternal);
         }
-        if (ce == cudaSuccess) ce = cudaMemcpyAsync(h_wc, wc + nxt, sizeof(WaveCounts), cudaMemcpyDeviceToHost, st);
-        if (ce == cudaSuccess) ce = cudaMemcpyAsync(h_q, q, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st);
-        if (ce == cudaSuccess && cfg.job_done)
-            ce = cudaMemcpyAsync(h_done, A.cohort_done, sizeof(unsigned long long) * table.size(),
+        if (ce == cudaSuccess) ce = cudaMemcpyAsync(E.h_wc, wc + nxt, sizeof(WaveCounts), cudaMemcpyDeviceToHost, st);
+        if (ce == cudaSuccess) ce = cudaMemcpyAsync(E.h_q, E.q, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st);
+        if (ce == cudaSuccess)
+            ce = cudaMemcpyAsync(E.h_done, A.cohort_done, sizeof(unsigned long long) * E.max_jobs,
                                  cudaMemcpyDeviceToHost, st);
-        const cudaError_t ee = cudaStreamEndCapture(st, &wg.g[par]);
+        const cudaError_t ee = cudaStreamEndCapture(st, &E.g[par]);
         KG_WAVE_TRY(ce);
         KG_WAVE_TRY(ee);
-        KG_WAVE_TRY(cudaGraphInstantiate(&wg.x[par], wg.g[par], 0));
+        KG_WAVE_TRY(cudaGraphInstantiate(&E.x[par], E.g[par], 0));
     }
-    uint64_t waves = 0, launches = 1;
-    double phase[3] = {0.0, 0.0, 0.0}, total = 0.0;
-    int cur = 0;
-    for (;;) {
-        KG_WAVE_TRY(cudaGraphLaunch(wg.x[cur], st));
-        KG_WAVE_TRY(cudaStreamSynchronize(st));
-        launches += 3;
-        waves++;
-        if (cfg.job_done)
-            for (size_t j = 0; j < table.size(); j++)
-                if (!reported[j] && h_done[j] >= (unsigned long long)table[j].n_pairs) {
-                    reported[j] = 1;
-                    cfg.job_done((int)j);
-                }
-        for (int i = 0; i < 3; i++) {
-            float ms = 0.f;
-            KG_WAVE_TRY(cudaEventElapsedTime(&ms, wg.ev[cur][i], wg.ev[cur][i + 1]));
-            phase[i] += ms;
-            total += ms;
-        }
-        const WaveCounts h = *h_wc;
-        const unsigned long long hq = *h_q;
-        cur ^= 1;
-        if (h.n_pass == 0 && h.n_resort == 0 && hq >= (unsigned long long)total_pairs) break;
+    E.launches = 1;
+    return KG_OK;
+}
+
+int WaveEngine::add(const std::vector<CohortDev>& jobs, std::string& err) {
+    Impl& E = *d_;
+    const cudaStream_t st = E.st;
+    if ((int64_t)E.table.size() + (int64_t)jobs.size() > E.max_jobs) {
+        err = "job table full";
+        return KG_ENOMEM;
     }
-    RunCounters rc;
-    KG_WAVE_TRY(cudaMemcpyAsync(&rc, ws.counters.p, sizeof(rc), cudaMemcpyDeviceToHost, st));
+    int64_t total = E.live_h->total_pairs;
+    // claims past the old end (slots that found no pair) handed out no pair:
+    // the queue restarts at the old end
+    if (E.last_q > (unsigned long long)total) {
+        const unsigned long long t = (unsigned long long)total;
+        KG_WAVE_TRY(cudaMemcpyAsync(E.q, &t, sizeof(t), cudaMemcpyHostToDevice, st));
+        KG_WAVE_TRY(cudaStreamSynchronize(st));   // t lives on this stack frame
+        E.last_q = t;
+    }
+    const size_t first = E.table.size();
+    for (CohortDev d : jobs) {
+        d.pair_begin = total;
+        if (d.max_iter == 0) d.max_iter = E.cfg.iterations;
+        total += d.n_pairs;
+        E.table.push_back(d);
+        E.reported.push_back(0);
+    }
+    if (jobs.empty()) return KG_OK;
+    KG_WAVE_TRY(cudaMemcpyAsync(const_cast<CohortDev*>(E.A.cohorts) + first, E.table.data() + first, sizeof(CohortDev) * jobs.size(),
+                                cudaMemcpyHostToDevice, st));
+    E.live_h->total_pairs = total;
+    E.live_h->n_cohorts = (int32_t)E.table.size();
+    KG_WAVE_TRY(cudaMemcpyAsync(E.live_d, E.live_h, sizeof(LiveQueue), cudaMemcpyHostToDevice, st));
+    KG_WAVE_TRY(cudaStreamSynchronize(st));   // the staging is reused by the next add
+    E.idle = false;
+    return KG_OK;
+}
+
+int WaveEngine::wave(std::vector<int>& finished, std::string& err) {
+    Impl& E = *d_;
+    const cudaStream_t st = E.st;
+    KG_WAVE_TRY(cudaGraphLaunch(E.x[E.cur], st));
     KG_WAVE_TRY(cudaStreamSynchronize(st));
+    E.launches += 3;
+    E.waves++;
+    for (size_t k = 0; k < E.table.size(); k++)
+        if (!E.reported[k] && E.h_done[k] >= (unsigned long long)E.table[k].n_pairs) {
+            E.reported[k] = 1;
+            finished.push_back((int)k);
+        }
+    for (int i = 0; i < 3; i++) {
+        float ms = 0.f;
+        KG_WAVE_TRY(cudaEventElapsedTime(&ms, E.ev[E.cur][i], E.ev[E.cur][i + 1]));
+        E.phase[i] += ms;
+        E.total += ms;
+    }
+    const WaveCounts h = *E.h_wc;
+    E.last_q = *E.h_q;
+    E.cur ^= 1;
+    E.idle = (h.n_pass == 0 && h.n_resort == 0 && E.last_q >= (unsigned long long)E.live_h->total_pairs);
+    return KG_OK;
+}
+
+bool WaveEngine::idle() const { return d_->idle; }
+int64_t WaveEngine::n_slots() const { return d_->n_slots; }
+int64_t WaveEngine::list_cap() const { return d_->list_cap; }
+
+int WaveEngine::reset_jobs(std::string& err) {
+    Impl& E = *d_;
+    if (!E.idle) {
+        err = "jobs still in flight";
+        return KG_EINVAL;
+    }
+    E.table.clear();
+    E.reported.clear();
+    E.live_h->total_pairs = 0;
+    E.live_h->n_cohorts = 0;
+    E.last_q = 0;
+    KG_WAVE_TRY(cudaMemcpyAsync(E.live_d, E.live_h, sizeof(LiveQueue), cudaMemcpyHostToDevice, E.st));
+    KG_WAVE_TRY(cudaMemsetAsync(E.q, 0, sizeof(unsigned long long), E.st));
+    KG_WAVE_TRY(cudaMemsetAsync(E.A.cohort_done, 0, sizeof(unsigned long long) * E.max_jobs, E.st));
+    KG_WAVE_TRY(cudaStreamSynchronize(E.st));
+    return KG_OK;
+}
+
+int WaveEngine::stats(kg_run_stats& stats, std::string& err) {
+    Impl& E = *d_;
+    RunCounters rc;
+    KG_WAVE_TRY(cudaMemcpyAsync(&rc, E.ws->counters.p, sizeof(rc), cudaMemcpyDeviceToHost, E.st));
+    KG_WAVE_TRY(cudaStreamSynchronize(E.st));
     stats.gh_passes = rc.gh_passes;
     stats.obj_passes = rc.obj_passes;
     stats.fp64_passes = rc.fp64_passes;
     stats.fp64_pairs = rc.fp64_pairs;
     stats.pair_sites = rc.pair_sites;
     stats.work_units = rc.work_units;
-    stats.launches = launches;
+    stats.launches = E.launches;
     stats.flops_fp32 = rc.flops_fp32;
     stats.flops_fp64 = rc.flops_fp64;
     for (int k = 0; k < 5; k++) stats.shape_sites[k] = rc.shape_sites[k];
     stats.nonconverged = rc.nonconverged;
-    stats.waves = waves;
-    stats.slots = (uint64_t)n_slots;
-    stats.admit_ms = phase[0];
-    stats.pass_ms = phase[1];
-    stats.solve_ms = phase[2];
-    stats.pair_kernel_ms = total;
+    stats.waves = E.waves;
+    stats.slots = (uint64_t)E.n_slots;
+    stats.admit_ms = E.phase[0];
+    stats.pass_ms = E.phase[1];
+    stats.solve_ms = E.phase[2];
+    stats.pair_kernel_ms = E.total;
     if (rc.stalled_waits) {
         err = "a device wait for a list copy ran out of its limit";
         return KG_ETIMEOUT;
@@ -928,6 +1030,27 @@ int run_waves(const std::vector<PairJob>& jobs, const RunConfig& cfg, Workspace&
         return KG_ENOSITES;
     }
     return KG_OK;
+}
+
+// All jobs of one call through one engine, waves until every pair is done.
+int run_waves(const std::vector<PairJob>& jobs, const RunConfig& cfg, Workspace& ws,
+              cudaStream_t st, kg_run_stats& stats, std::string& err,
+              const std::vector<CohortDev>& table, int64_t total_pairs, int64_t list_cap) {
+    (void)jobs;
+    WaveEngine eng;
+    int r = eng.open(ws, st, cfg, list_cap, total_pairs, (int)table.size(), err);
+    if (r) return r;
+    r = eng.add(table, err);
+    if (r) return r;
+    std::vector<int> fin;
+    while (!eng.idle()) {
+        fin.clear();
+        r = eng.wave(fin, err);
+        if (r) return r;
+        if (cfg.job_done)
+            for (int k : fin) cfg.job_done(k);
+    }
+    return eng.stats(stats, err);
 }
 
 }  // namespace kg

@@ -61,11 +61,18 @@ struct WaveCounts {
     int units[5];    // pass work units per shape
 };
 
+// The job table's extent, in device memory so that jobs can be appended
+// between waves without touching the captured launches.
+struct LiveQueue {
+    int64_t total_pairs;   // pairs of all jobs so far (global work indices 0 .. total - 1)
+    int32_t n_cohorts;     // jobs in the table
+    int32_t pad;
+};
+
 struct WaveArgs {
     const CohortDev* cohorts;
-    int n_cohorts;
+    const LiveQueue* live;
     int precision;
-    int64_t total_pairs;
     unsigned long long* queue;     // next pair (global work index)
     SlotState* slots;
     int n_slots;
@@ -124,8 +131,14 @@ __device__ inline void units_from_counts(SlotState& S) {
 
 __device__ __forceinline__ void decode_pair(const WaveArgs& A, int64_t k, int& c, int64_t& j,
                                             int64_t& x, int64_t& y) {
-    c = 0;
-    while (c + 1 < A.n_cohorts && k >= A.cohorts[c + 1].pair_begin) c++;
+    // the last job whose range starts at or before k
+    int lo = 0, hi = A.live->n_cohorts - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (A.cohorts[mid].pair_begin <= k) lo = mid;
+        else hi = mid - 1;
+    }
+    c = lo;
     const CohortDev& co = A.cohorts[c];
     j = k - co.pair_begin;
     if (co.kind == COHORT_TRIANGLE) {
