@@ -21,6 +21,7 @@
 
 #include "kestrel_gpu.h"
 #include "kg_engine.h"
+#include "kg_pair.cuh"
 
 namespace {
 
@@ -35,14 +36,6 @@ struct Request {
     std::string err;
     bool done = false;
     bool cancelled = false;
-};
-
-struct Slot {
-    cudaStream_t stream = nullptr;
-    kg::Workspace ws;
-    kg::DevBuf out;
-    std::vector<std::unique_ptr<kg::QueryPlanes>> queries;
-    bool busy = false;
 };
 
 }  // namespace
@@ -65,7 +58,7 @@ struct kg_ctx {
     // serving
     std::mutex mu;
     std::condition_variable cv;
-    std::thread server;
+    std::vector<std::thread> servers;
     bool stop = false;
     bool panel_ready = false;
     kg::Cohort panel;
@@ -73,7 +66,13 @@ struct kg_ctx {
     std::deque<int64_t> pending;
     int64_t next_id = 1;
     int64_t served_requests = 0, served_pairs = 0, served_launches = 0;
-    std::vector<Slot> slots;
+    int64_t in_flight = 0;               // requests admitted into a serving engine
+    int64_t panel_gen = 0;               // bumped by every kg_panel_load
+    struct ServeWorker {
+        cudaStream_t stream = nullptr;
+        kg::Workspace ws;
+    };
+    std::vector<ServeWorker> workers;
 };
 
 namespace {
@@ -136,103 +135,61 @@ int copy_rows_out(kg_ctx* c, const kg::DevBuf& d, int64_t n, kg_output* out, cud
 
 // ------------------------------------------------------------- serving loop
 
-void serve_batch(kg_ctx* c, Slot& slot, std::vector<std::shared_ptr<Request>>& batch) {
+// Requests in the engine's job table between idle moments; when it fills, new
+// requests wait until the in-flight ones drain.
+constexpr int kMaxServeJobs = 1 << 16;
+
+// One request in the serving engine: its query planes and device rows live
+// until its last pair is done.
+struct LiveRequest {
+    std::shared_ptr<Request> r;
+    std::unique_ptr<kg::QueryPlanes> q;
+    kg_output* d_out = nullptr;
+};
+
+// Serving workers, each with its own stream and wave engine; their kernels
+// overlap on the device.
+constexpr int kServeWorkers = 2;
+// Pairs in flight per worker (as memory allows).
+constexpr int64_t kServeSlots = 32768;
+// A worker takes more requests only while fewer than this many of its pairs
+// wait for a slot (its slots stay busy; a burst spreads over the workers).
+constexpr int64_t kWorkerBacklog = 1 << 16;
+
+// One serving worker.  Its wave engine runs while it has requests in flight.
+// Between waves, queued requests whose inputs and rows fit the memory budget
+// join the engine's job table, so their pairs take slots as slots free
+// (continuous batching); a request is answered as soon as its own pairs are
+// done.  A pair's result does not depend on which requests share its waves.
+void serve_loop(kg_ctx* c, int wid) {
+    cudaSetDevice(c->device);
+    const cudaStream_t st = c->workers[wid].stream;
+    kg::Workspace& wws = c->workers[wid].ws;
+    int64_t my_backlog = 0;   // pairs of this worker's requests not yet in a slot
+    std::unique_ptr<kg::WaveEngine> eng;   // (re)opened for each panel
+    int64_t eng_gen = -1;
+    std::map<int, LiveRequest> live;     // by job index
+    int next_job = 0;
     std::string err;
-    int st = KG_OK;
-    std::vector<kg::PairJob> jobs;
-    int64_t total = 0;
-    for (auto& r : batch) total += r->n_query * c->panel.n_samples;
-    slot.queries.clear();
-    int e = slot.out.reserve(sizeof(kg_output) * std::max<int64_t>(total, 1));
-    if (e != cudaSuccess) { st = KG_ENOMEM; err = "request outputs do not fit"; }
-    int64_t off = 0;
-    for (size_t i = 0; st == KG_OK && i < batch.size(); i++) {
-        auto q = std::make_unique<kg::QueryPlanes>();
-        st = kg::prepare_query(c->panel, *q, batch[i]->codes.data(), batch[i]->n_query,
-                               c->panel.n_sites, batch[i]->mask.empty() ? nullptr : batch[i]->mask.data(),
-                               slot.stream, err);
-        if (st != KG_OK) break;
-        kg::PairJob jb;
-        jb.panel = &c->panel;
-        jb.query = q.get();
-        jb.kind = 1;
-        jb.n_x = batch[i]->n_query;
-        jb.n_y = c->panel.n_samples;
-        jb.d_out = slot.out.as<kg_output>() + off;
-        jb.iterations = batch[i]->iterations;   // each request keeps its own limit
-        off += jb.n_pairs();
-        jobs.push_back(jb);
-        slot.queries.push_back(std::move(q));
-    }
-    // a request is answered as soon as its own pairs are done, between waves
-    std::vector<int64_t> offs(batch.size(), 0);
-    for (size_t i = 1; i < batch.size(); i++) offs[i] = offs[i - 1] + batch[i - 1]->n_query * c->panel.n_samples;
-    std::vector<char> answered(batch.size(), 0);
-    auto answer = [&](size_t i, int status, const std::string& why) {
-        auto& r = batch[i];
-        const int64_t np = r->n_query * c->panel.n_samples;
-        if (status == KG_OK) {
-            r->rows.resize(np);
-            cudaError_t ce = cudaMemcpyAsync(r->rows.data(), slot.out.as<kg_output>() + offs[i],
-                                             sizeof(kg_output) * np, cudaMemcpyDeviceToHost, slot.stream);
-            if (ce == cudaSuccess) ce = cudaStreamSynchronize(slot.stream);
-            if (ce != cudaSuccess) { r->status = KG_ECUDA; r->err = cudaGetErrorString(ce); }
-        } else {
-            r->status = status;
-            r->err = why;
-        }
-        answered[i] = 1;
+    auto fail_all = [&](int status, const std::string& why) {
         std::lock_guard<std::mutex> lk(c->mu);
-        r->done = true;
-        c->served_requests++;
-        c->served_pairs += np;
+        for (auto& kv : live) {
+            kv.second.r->status = status;
+            kv.second.r->err = why;
+            kv.second.r->done = true;
+            if (kv.second.d_out) cudaFreeAsync(kv.second.d_out, st);
+        }
+        c->in_flight -= (int64_t)live.size();
+        live.clear();
+        my_backlog = 0;
         c->cv.notify_all();
     };
-    kg_run_stats stats{};
-    if (st == KG_OK) {
-        kg::RunConfig cfg = run_config(c, batch.empty() ? 100 : batch[0]->iterations);
-        uint64_t it = 1;
-        for (auto& r : batch) it = std::max<uint64_t>(it, r->iterations);
-        cfg.iterations = it;
-        cfg.job_done = [&](int j) { answer((size_t)j, KG_OK, std::string()); };
-        st = kg::run_pairs(jobs, cfg, slot.ws, slot.stream, stats, err);
-        if (st == KG_ENOSITES) st = KG_OK;  // per-pair NaN rows; reported on the rows
-    }
-    for (size_t i = 0; i < batch.size(); i++)
-        if (!answered[i]) answer(i, st, err);
-    std::lock_guard<std::mutex> lk(c->mu);
-    c->served_launches++;
-    c->cv.notify_all();
-}
-
-// The scheduler: admits every queued request whose inputs fit the memory
-// budget into one batch (continuous batching); one batch per serving slot,
-// kServeSlots of them running concurrently on their own streams, so a request
-// that arrives while others run starts as soon as a slot frees.
-constexpr int kServeSlots = 4;
-void serve_loop(kg_ctx* c) {
-    cudaSetDevice(c->device);
-    struct Worker {
-        std::thread t;
-        std::shared_ptr<std::atomic<bool>> done;
-    };
-    std::vector<Worker> workers;
-    const size_t kMaxPairs = (size_t)1 << 22;
     for (;;) {
-        std::vector<std::shared_ptr<Request>> batch;
-        int slot_idx = -1;
+        std::vector<std::shared_ptr<Request>> admit;
         {
             std::unique_lock<std::mutex> lk(c->mu);
-            c->cv.wait(lk, [&] {
-                if (c->stop) return true;
-                if (c->pending.empty()) return false;
-                for (auto& s : c->slots)
-                    if (!s.busy) return true;
-                return false;
-            });
-            if (c->stop && c->pending.empty()) break;
+            c->cv.wait(lk, [&] { return c->stop || !live.empty() || !c->pending.empty(); });
             if (c->stop) {
-                // drop what is still queued
                 for (int64_t id : c->pending) {
                     auto it = c->requests.find(id);
                     if (it != c->requests.end()) {
@@ -242,53 +199,128 @@ void serve_loop(kg_ctx* c) {
                 }
                 c->pending.clear();
                 c->cv.notify_all();
+                lk.unlock();
+                fail_all(KG_ECANCELED, "context destroyed");
                 break;
             }
-            for (size_t i = 0; i < c->slots.size(); i++)
-                if (!c->slots[i].busy) { slot_idx = (int)i; break; }
-            size_t pairs = 0, bytes = 0;
-            while (!c->pending.empty()) {
-                int64_t id = c->pending.front();
+            // the queued requests that fit, in arrival order
+            size_t bytes = 0;
+            int64_t take = my_backlog;
+            while (!c->pending.empty() && next_job + (int)admit.size() < kMaxServeJobs &&
+                   (admit.empty() && live.empty() ? true : take < kWorkerBacklog)) {
+                const int64_t id = c->pending.front();
                 auto it = c->requests.find(id);
                 if (it == c->requests.end() || it->second->cancelled) {
                     c->pending.pop_front();
                     continue;
                 }
                 auto& r = it->second;
-                size_t np = (size_t)(r->n_query * c->panel.n_samples);
-                size_t nb = np * sizeof(kg_output) +
-                            (size_t)r->n_query * (size_t)(c->panel.n_sites + c->panel.plane_stride * 8);
-                if (!batch.empty() && (pairs + np > kMaxPairs || !budget_ok(c, bytes + nb))) break;
-                batch.push_back(r);
-                pairs += np;
+                const size_t nb = (size_t)(r->n_query * c->panel.n_samples) * sizeof(kg_output) +
+                                  (size_t)r->n_query * (size_t)(c->panel.n_sites + c->panel.plane_stride * 8);
+                if ((!admit.empty() || !live.empty()) && !budget_ok(c, bytes + nb)) break;
+                admit.push_back(r);
                 bytes += nb;
+                take += r->n_query * c->panel.n_samples;
                 c->pending.pop_front();
             }
-            if (batch.empty()) continue;
-            c->slots[slot_idx].busy = true;
+            c->in_flight += (int64_t)admit.size();
         }
-        auto done = std::make_shared<std::atomic<bool>>(false);
-        workers.push_back({std::thread([c, slot_idx, batch, done]() mutable {
-                               cudaSetDevice(c->device);
-                               serve_batch(c, c->slots[slot_idx], batch);
-                               std::lock_guard<std::mutex> lk(c->mu);
-                               c->slots[slot_idx].busy = false;
-                               done->store(true);
-                               c->cv.notify_all();
-                           }),
-                           done});
-        // reap the workers that have finished (never wait on a running one)
-        for (auto it = workers.begin(); it != workers.end();) {
-            if (it->done->load()) {
-                it->t.join();
-                it = workers.erase(it);
-            } else {
-                ++it;
+        if (!eng || (eng_gen != c->panel_gen && live.empty())) {
+            // a new panel (kg_panel_load waits for in-flight requests first)
+            eng = std::make_unique<kg::WaveEngine>();
+            next_job = 0;
+            kg::RunConfig cfg = run_config(c, 100);
+            if (cfg.slots == 0) cfg.slots = kServeSlots;
+            const int r = eng->open(wws, st, cfg, kg::list_capacity(c->panel), (int64_t)1 << 40,
+                                    kMaxServeJobs, err);
+            if (r) {
+                eng.reset();
+                std::lock_guard<std::mutex> lk(c->mu);
+                for (auto& rq : admit) { rq->status = r; rq->err = err; rq->done = true; }
+                c->in_flight -= (int64_t)admit.size();
+                c->cv.notify_all();
+                continue;
             }
+            eng_gen = c->panel_gen;
+        }
+        // the admitted requests join the engine
+        std::vector<kg::CohortDev> add;
+        for (auto& rq : admit) {
+            LiveRequest lr;
+            lr.r = rq;
+            lr.q = std::make_unique<kg::QueryPlanes>();
+            const int64_t np = rq->n_query * c->panel.n_samples;
+            int r = kg::prepare_query(c->panel, *lr.q, rq->codes.data(), rq->n_query, c->panel.n_sites,
+                                      rq->mask.empty() ? nullptr : rq->mask.data(), st, err);
+            if (r == KG_OK && cudaMallocAsync(reinterpret_cast<void**>(&lr.d_out), sizeof(kg_output) * np, st) !=
+                                  cudaSuccess) {
+                r = KG_ENOMEM;
+                err = "request rows do not fit";
+                lr.d_out = nullptr;
+            }
+            if (r != KG_OK) {
+                std::lock_guard<std::mutex> lk(c->mu);
+                rq->status = r;
+                rq->err = err;
+                rq->done = true;
+                c->in_flight--;
+                c->cv.notify_all();
+                continue;
+            }
+            kg::PairJob jb;
+            jb.panel = &c->panel;
+            jb.query = lr.q.get();
+            jb.kind = 1;
+            jb.n_x = rq->n_query;
+            jb.n_y = c->panel.n_samples;
+            jb.d_out = lr.d_out;
+            jb.iterations = rq->iterations;   // each request keeps its own limit
+            add.push_back(kg::make_cohort_dev(jb, rq->iterations));
+            live[next_job++] = std::move(lr);
+        }
+        int r = add.empty() ? KG_OK : eng->add(add, err);
+        std::vector<int> fin;
+        if (r == KG_OK && !eng->idle()) {
+            r = eng->wave(fin, err);
+            std::lock_guard<std::mutex> lk(c->mu);
+            c->served_launches++;
+        }
+        if (r != KG_OK) {
+            // the engine's state is unknown after a failure: start a new one
+            fail_all(r, err);
+            eng.reset();
+            continue;
+        }
+        // answer the requests whose pairs are all done
+        for (int j : fin) {
+            auto it = live.find(j);
+            if (it == live.end()) continue;
+            LiveRequest& lr = it->second;
+            const int64_t np = lr.r->n_query * c->panel.n_samples;
+            lr.r->rows.resize(np);
+            cudaError_t ce = cudaMemcpyAsync(lr.r->rows.data(), lr.d_out, sizeof(kg_output) * np,
+                                             cudaMemcpyDeviceToHost, st);
+            if (ce == cudaSuccess) ce = cudaFreeAsync(lr.d_out, st);
+            if (ce == cudaSuccess) ce = cudaStreamSynchronize(st);
+            std::lock_guard<std::mutex> lk(c->mu);
+            if (ce != cudaSuccess) {
+                lr.r->status = KG_ECUDA;
+                lr.r->err = cudaGetErrorString(ce);
+            }
+            lr.r->done = true;
+            c->served_requests++;
+            c->served_pairs += np;
+            c->in_flight--;
+            c->cv.notify_all();
+            live.erase(it);
+        }
+        my_backlog = eng ? eng->backlog() : 0;
+        if (eng->idle() && live.empty() && next_job > 0) {
+            std::string e2;
+            if (eng->reset_jobs(e2) == KG_OK) next_job = 0;
+            else eng.reset();
         }
     }
-    for (auto& w : workers)
-        if (w.t.joinable()) w.t.join();
 }
 
 }  // namespace
@@ -325,13 +357,13 @@ int kg_destroy(kg_ctx* c) {
         c->stop = true;
         c->cv.notify_all();
     }
-    if (c->server.joinable()) c->server.join();
-    for (auto& s : c->slots)
-        if (s.stream) {
-            cudaStreamSynchronize(s.stream);
-            cudaStreamDestroy(s.stream);
+    for (auto& t : c->servers)
+        if (t.joinable()) t.join();
+    for (auto& w : c->workers)
+        if (w.stream) {
+            cudaStreamSynchronize(w.stream);
+            cudaStreamDestroy(w.stream);
         }
-    c->slots.clear();
     if (c->stream) {
         cudaStreamSynchronize(c->stream);
         cudaStreamDestroy(c->stream);
@@ -625,11 +657,8 @@ int kg_panel_load(kg_ctx* c, const uint8_t* codes, int64_t n_samples, int64_t n_
         int st = use_device(c);
         if (st) return st;
         std::unique_lock<std::mutex> lk(c->mu);
-        // wait for in-flight batches before replacing the panel
-        c->cv.wait(lk, [&] {
-            for (auto& s : c->slots) if (s.busy) return false;
-            return true;
-        });
+        // wait for in-flight requests before replacing the panel
+        c->cv.wait(lk, [&] { return c->in_flight == 0 && c->pending.empty(); });
         std::string err;
         c->panel_ready = false;
         st = kg::prepare_cohort(c->panel, codes, n_samples, n_sites, row_stride, false, af,
@@ -637,15 +666,16 @@ int kg_panel_load(kg_ctx* c, const uint8_t* codes, int64_t n_samples, int64_t n_
         if (st) return set_err(c, st, err);
         c->panel.raw.release();
         c->panel_ready = true;
-        if (c->slots.empty()) {
-            c->slots.resize(kServeSlots);
-            for (auto& s : c->slots)
-                if (cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking) != cudaSuccess)
-                    return set_err(c, KG_ECUDA, "cannot create serving streams");
+        c->panel_gen++;
+        if (c->workers.empty()) {
+            c->workers.resize(kServeWorkers);
+            for (auto& w : c->workers)
+                if (cudaStreamCreateWithFlags(&w.stream, cudaStreamNonBlocking) != cudaSuccess)
+                    return set_err(c, KG_ECUDA, "cannot create the serving streams");
         }
-        if (!c->server.joinable()) {
+        if (c->servers.empty()) {
             c->stop = false;
-            c->server = std::thread(serve_loop, c);
+            for (int w = 0; w < kServeWorkers; w++) c->servers.emplace_back(serve_loop, c, w);
         }
         return KG_OK;
     });

@@ -505,6 +505,30 @@ jacquard_pair_kernel(PairLaunch L) {
 
 static_assert(sizeof(kg_output) == 14 * 8, "kg_output must be 112 bytes");
 
+CohortDev make_cohort_dev(const PairJob& jb, uint64_t iterations) {
+    const Cohort& pn = *jb.panel;
+    CohortDev d;
+    d.planes_y = pn.planes.as<uint2>();
+    d.planes_x = (jb.kind == COHORT_RECT) ? jb.query->planes.as<uint2>() : d.planes_y;
+    d.plane_stride = pn.plane_stride;
+    d.p32 = pn.p32.as<float>();
+    d.p64 = pn.p64.as<double>();
+    d.q64 = pn.q64.as<double>();
+    d.n_sites = (int32_t)pn.n_kept;
+    d.n_units = (int32_t)ceil_div(pn.n_kept, UNIT_SITES);
+    d.kind = jb.kind;
+    d.pad = 0;
+    d.n_x = jb.n_x;
+    d.n_y = jb.n_y;
+    d.pair_begin = 0;
+    d.n_pairs = jb.n_pairs();
+    d.out = jb.d_out;
+    d.max_iter = jb.iterations ? jb.iterations : iterations;
+    return d;
+}
+
+int64_t list_capacity(const Cohort& panel) { return align4(panel.n_kept) + 32; }
+
 int run_pairs(const std::vector<PairJob>& jobs, const RunConfig& cfg, Workspace& ws,
               cudaStream_t st, kg_run_stats& stats, std::string& err) {
     std::memset(&stats, 0, sizeof(stats));
@@ -517,26 +541,11 @@ int run_pairs(const std::vector<PairJob>& jobs, const RunConfig& cfg, Workspace&
     std::vector<CohortDev> table(jobs.size());
     for (size_t i = 0; i < jobs.size(); i++) {
         const PairJob& jb = jobs[i];
-        const Cohort& pn = *jb.panel;
         CohortDev& d = table[i];
-        d.planes_y = pn.planes.as<uint2>();
-        d.planes_x = (jb.kind == COHORT_RECT) ? jb.query->planes.as<uint2>() : d.planes_y;
-        d.plane_stride = pn.plane_stride;
-        d.p32 = pn.p32.as<float>();
-        d.p64 = pn.p64.as<double>();
-        d.q64 = pn.q64.as<double>();
-        d.n_sites = (int32_t)pn.n_kept;
-        d.n_units = (int32_t)ceil_div(pn.n_kept, UNIT_SITES);
-        d.kind = jb.kind;
-        d.pad = 0;
-        d.n_x = jb.n_x;
-        d.n_y = jb.n_y;
+        d = make_cohort_dev(jb, cfg.iterations);
         d.pair_begin = total_pairs;
-        d.n_pairs = jb.n_pairs();
-        d.out = jb.d_out;
-        d.max_iter = jb.iterations ? jb.iterations : cfg.iterations;
         total_pairs += d.n_pairs;
-        seg_cap = std::max<int64_t>(seg_cap, align4(pn.n_kept) + 32);
+        seg_cap = std::max<int64_t>(seg_cap, list_capacity(*jb.panel));
     }
     if (total_pairs == 0) return KG_OK;
     return run_waves(jobs, cfg, ws, st, stats, err, table, total_pairs, seg_cap);

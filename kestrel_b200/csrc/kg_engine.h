@@ -154,6 +154,8 @@ class WaveEngine {
     bool idle() const;
     int64_t n_slots() const;
     int64_t list_cap() const;
+    // Pairs of the table that no slot has taken yet.
+    int64_t backlog() const;
     // Empties the job table (only when idle), so a long-running loop reuses it.
     int reset_jobs(std::string& err);
     // Counters and phase times since open().
@@ -163,6 +165,11 @@ class WaveEngine {
     struct Impl;
     Impl* d_;
 };
+
+// The device table entry of a job (pair_begin left 0 for the engine to set),
+// and the list capacity (entries per slot) a cohort's pairs need.
+CohortDev make_cohort_dev(const PairJob& jb, uint64_t iterations);
+int64_t list_capacity(const Cohort& panel);
 
 // All jobs of one call through one engine (kg_wave.cu), over a prepared
 // cohort table.

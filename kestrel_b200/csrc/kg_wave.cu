@@ -980,6 +980,10 @@ int WaveEngine::wave(std::vector<int>& finished, std::string& err) {
 bool WaveEngine::idle() const { return d_->idle; }
 int64_t WaveEngine::n_slots() const { return d_->n_slots; }
 int64_t WaveEngine::list_cap() const { return d_->list_cap; }
+int64_t WaveEngine::backlog() const {
+    const int64_t total = d_->live_h ? d_->live_h->total_pairs : 0;
+    return total - std::min<int64_t>(total, (int64_t)d_->last_q);
+}
 
 int WaveEngine::reset_jobs(std::string& err) {
     Impl& E = *d_;
