@@ -148,6 +148,10 @@ int kg_relatedness_batch(kg_ctx *ctx, kg_cohort *cohorts, int n_cohorts,
 
 /* ------------------------------------------------------------- serving */
 
+/* Serving is continuous batching: worker threads each run a wave engine, and
+ * queued requests join a running engine between its waves as memory allows;
+ * a request is answered as soon as its own pairs are done. */
+
 /* Makes `codes` the resident reference panel (packed in HBM with its allele
  * frequencies, estimated unless af is given).  Query requests are scored
  * against it until the next kg_panel_load or kg_destroy. */
@@ -175,7 +179,7 @@ int kg_wait(kg_ctx *ctx, int64_t request_id, int64_t timeout_ms,
 /* Drops a queued request (a running one finishes but its rows are discarded). */
 int kg_cancel(kg_ctx *ctx, int64_t request_id);
 
-/* Serving counters: requests completed, pairs completed, device launches. */
+/* Serving counters: requests completed, pairs completed, waves run. */
 int kg_serving_stats(kg_ctx *ctx, int64_t *requests, int64_t *pairs,
                      int64_t *launches);
 
