@@ -827,13 +827,11 @@ int WaveEngine::open(Workspace& ws, cudaStream_t st, const RunConfig& cfg, int64
         KG_WAVE_TRY(cudaMemcpyAsync(&E.wc[0].n_free, &nf, sizeof(int), cudaMemcpyHostToDevice, st));
         KG_WAVE_TRY(cudaStreamSynchronize(st));   // nf lives on this stack frame
     }
-    static bool attr = false;
-    if (!attr) {
-        KG_WAVE_TRY(cudaFuncSetAttribute(wave_pass_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 4 * WARP_SMEM));
-        KG_WAVE_TRY(cudaFuncSetAttribute(wave_admit_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         ADMIT_WARPS * ADMIT_WARP_SMEM));
-        attr = true;
-    }
+    // per device, and cheap: set on every open (serving workers open engines
+    // on several threads)
+    KG_WAVE_TRY(cudaFuncSetAttribute(wave_pass_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 4 * WARP_SMEM));
+    KG_WAVE_TRY(cudaFuncSetAttribute(wave_admit_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     ADMIT_WARPS * ADMIT_WARP_SMEM));
     int occ = 0;
     KG_WAVE_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, wave_pass_kernel, 128, 4 * WARP_SMEM));
     if (occ <= 0) {
