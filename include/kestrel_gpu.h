@@ -77,7 +77,7 @@ const char *kg_version(void);
 int kg_set_precision(kg_ctx *ctx, int precision);
 
 /* Launch shape of the pair engine: pairs in flight per wave (slots, 0 = up to
- * 16384 as memory allows) and blocks per SM of the site-pass kernel (0 = the
+ * 32768 as memory allows) and blocks per SM of the site-pass kernel (0 = the
  * occupancy limit).  Exposed for the autotuner and tests; results do not
  * depend on it. */
 int kg_set_launch(kg_ctx *ctx, int slots, int blocks_per_sm);
