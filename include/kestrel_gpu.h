@@ -76,10 +76,10 @@ const char *kg_version(void);
 /* Arithmetic of the per-site sums (kg_precision). */
 int kg_set_precision(kg_ctx *ctx, int precision);
 
-/* Launch shape of the pair engine: pairs in flight per wave (slots, 0 = up to
- * 32768 as memory allows) and blocks per SM of the site-pass kernel (0 = the
- * occupancy limit).  Exposed for the autotuner and tests; results do not
- * depend on it. */
+/* Launch shape of the pair engine: pairs in flight per wave (slots; 0 = an
+ * eighth of the pairs, from 4096 to 32768, as memory allows) and blocks per SM
+ * of the site-pass kernel (0 = the occupancy limit).  Exposed for the
+ * autotuner and tests; results do not depend on it. */
 int kg_set_launch(kg_ctx *ctx, int slots, int blocks_per_sm);
 
 /* Runs the autotuner on a sample of the loaded cohort and keeps the fastest

@@ -113,7 +113,7 @@ struct PairJob {
 struct RunConfig {
     int precision = KG_PREC_FP32C;
     uint64_t iterations = 100;
-    int64_t slots = 0;         // pairs in flight per wave (0 = up to 32768 as memory allows)
+    int64_t slots = 0;         // pairs in flight per wave (0 = pairs / 8 within 4096..32768, as memory allows)
     int pass_blocks_per_sm = 0;   // site-pass kernel blocks per SM (0 = occupancy limit)
     // Called between waves, on the calling thread, once per job whose pairs
     // have all finished (their rows are final in device memory).

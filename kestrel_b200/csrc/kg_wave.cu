@@ -782,7 +782,10 @@ int WaveEngine::open(Workspace& ws, cudaStream_t st, const RunConfig& cfg, int64
                             sizeof(SlotState) + 4 * sizeof(int) + 2 * 5 * shape_units * sizeof(int4);
     size_t fr = 0, tot = 0;
     KG_WAVE_TRY(cudaMemGetInfo(&fr, &tot));
-    const int64_t want = cfg.slots > 0 ? cfg.slots : 32768;
+    // by default an eighth of the job's pairs, between 4,096 and 32,768: enough
+    // to fill the waves, few enough that the last waves drain quickly
+    const int64_t want = cfg.slots > 0 ? cfg.slots
+                                       : std::min<int64_t>(32768, std::max<int64_t>(4096, expected_pairs / 8));
     const int64_t by_mem = (int64_t)((fr / 2) / per_slot);
     E.n_slots = std::max<int64_t>(1, std::min<int64_t>({want, by_mem, std::max<int64_t>(1, expected_pairs)}));
     const int64_t n_slots = E.n_slots;
