@@ -505,16 +505,17 @@ struct Shape32 {
         else ob += diff_term(t, r, c);
     }
 
-    // four sites (one float4): in direct mode one lg2 of the product of the
-    // four d (each d lies in [1e-8, 1 + 1e-8], so the product stays a normal
-    // FP32 number)
+    // four sites (one float4), the objective kind fixed at compile time: in
+    // direct mode one lg2 of the product of the four d (each d lies in
+    // [1e-8, 1 + 1e-8], so the product stays a normal FP32 number)
+    template <bool DIFF>
     __device__ __forceinline__ void site4(float4 v, float* g, float& ob, float* h) const {
         float d0, d1, d2, d3, r0, r1, r2, r3, c0, c1, c2, c3;
         core(v.x, g, h, d0, r0, c0);
         core(v.y, g, h, d1, r1, c1);
         core(v.z, g, h, d2, r2, c2);
         core(v.w, g, h, d3, r3, c3);
-        if (!diff) {
+        if (!DIFF) {
             ob += lg2_approx((d0 * d1) * (d2 * d3));
         } else {
             ob += diff_term(v.x, r0, c0);

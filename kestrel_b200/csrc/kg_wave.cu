@@ -304,21 +304,47 @@ __device__ __forceinline__ void ring_prologue(const Ring& R, const float* L, int
     }
 }
 
+// One 16-byte read of a ring stage (a shared-memory address).
+__device__ __forceinline__ float4 lds4(uint32_t a) {
+    float4 v;
+    asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];" : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w) : "r"(a));
+    return v;
+}
+
+// Eight sites of one lane (two float4): FP32 gradient and objective partials,
+// promoted to FP64 at the end.
+template <int S, bool DIFF>
+__device__ __forceinline__ void step8(const Shape32<S, false>& ev, float4 a, float4 b, bool second, double* G,
+                                      double& F, float* h) {
+    constexpr int NG = Shape32<S, false>::NG;
+    float g[NG], ob = 0.f;
+#pragma unroll
+    for (int j = 0; j < NG; j++) g[j] = 0.f;
+    ev.template site4<DIFF>(a, g, ob, h);
+    if (second) ev.template site4<DIFF>(b, g, ob, h);
+#pragma unroll
+    for (int j = 0; j < NG; j++) G[j] += (double)g[j];
+    F += (double)ob;
+}
+
 // One shape's FP32 list from the ring.  Stage i holds float4 128 i .. 128 i +
 // 127; lane l takes 128 i + 32 j + l (j = 0..3), in two steps of 8 sites
-// after each of which the FP32 gradient and objective partials go to FP64
-// (the Hessian partials every HESS_FLUSH steps).  L and every stage start are
-// 16-byte aligned (list starts are multiples of four entries); a stage's copy
-// rounds its size up to 16 bytes, which stays inside the slot's list buffer.
-// The sums use the hi coefficients only (lo_correction restores the rest).
-// Returns false if a wait ran out.
-template <int S>
-__device__ __noinline__ bool stream32_ring(const float* __restrict__ L, int64_t len, const Coef32* K,
-                                           bool diff, int lane, const Ring R, LaneSums& out) {
+// after each of which the FP32 gradient and objective partials go to FP64;
+// the Hessian partials go every HESS_STAGES stages (64 sites a lane).  Only
+// the list's last stage can be partly filled; the others run without bounds
+// tests.  L and every stage start are 16-byte aligned (list starts are
+// multiples of four entries); a stage's copy rounds its size up to 16 bytes,
+// which stays inside the slot's list buffer.  The sums use the hi
+// coefficients only (lo_correction restores the rest).  Returns false if a
+// wait ran out.
+constexpr int HESS_STAGES = 4;
+template <int S, bool DIFF>
+__device__ __forceinline__ bool stream32_ring(const float* __restrict__ L, int64_t len, const Coef32* K, int lane,
+                                           const Ring R, LaneSums& out) {
     using E = Shape32<S, false>;
     constexpr int NG = E::NG, NH = E::NH, GOFF = E::GOFF, HOFF = E::HOFF;
     E ev;
-    ev.load(K, diff);
+    ev.load(K, DIFF);
     double G[NG], H[NH], F = 0.0;
     float h[NH];
 #pragma unroll
@@ -327,33 +353,31 @@ __device__ __noinline__ bool stream32_ring(const float* __restrict__ L, int64_t 
     for (int i = 0; i < NH; i++) { H[i] = 0.0; h[i] = 0.f; }
     const int64_t n4 = len >> 2;
     const int nst = (int)((len + STAGE_ELEMS - 1) / STAGE_ELEMS);
+    const int nfull = (int)(n4 / STAGE_F4);   // stages with all 128 float4 inside the list
+    const uint32_t base = smem_u32(R.buf) + 16u * (uint32_t)lane;
     const uint32_t seq0 = R.seq;   // ring_prologue has issued the first stages
     bool ok = true;
-    int it = 0, done = 0;
+    int done = 0;
     for (int i = 0; i < nst; i++) {
         const uint32_t q = seq0 + i;
         const uint32_t slot = q % RING_STAGES;
         if (!mbar_wait(&R.bar[slot], (q / RING_STAGES) & 1u)) { ok = false; break; }
         done = i + 1;
-        const float4* B = R.buf + slot * STAGE_F4;
-        const int64_t k = (int64_t)i * STAGE_F4 + lane;
+        const uint32_t b = base + slot * (STAGE_F4 * 16);
+        if (i < nfull) {
+            step8<S, DIFF>(ev, lds4(b), lds4(b + 512), true, G, F, h);
+            step8<S, DIFF>(ev, lds4(b + 1024), lds4(b + 1536), true, G, F, h);
+            if (i % HESS_STAGES == HESS_STAGES - 1) {
 #pragma unroll
-        for (int half = 0; half < STAGE_F4 / 64; half++) {
-            const int64_t kh = k + 64 * half;
-            if (kh < n4) {
-                float g[NG], ob = 0.f;
+                for (int j = 0; j < NH; j++) { H[j] += (double)h[j]; h[j] = 0.f; }
+            }
+        } else {
+            const int rem = (int)(n4 - (int64_t)i * STAGE_F4);   // float4 in this stage, 0..127
 #pragma unroll
-                for (int j = 0; j < NG; j++) g[j] = 0.f;
-                ev.site4(B[lane + 64 * half], g, ob, h);
-                if (kh + 32 < n4) ev.site4(B[lane + 64 * half + 32], g, ob, h);
-#pragma unroll
-                for (int j = 0; j < NG; j++) G[j] += (double)g[j];
-                F += (double)ob;
-                if (++it == HESS_FLUSH) {
-#pragma unroll
-                    for (int j = 0; j < NH; j++) { H[j] += (double)h[j]; h[j] = 0.f; }
-                    it = 0;
-                }
+            for (int half = 0; half < 2; half++) {
+                const int kh = lane + 64 * half;   // this lane's float4 within the stage
+                if (kh < rem)
+                    step8<S, DIFF>(ev, lds4(b + 1024 * half), lds4(b + 1024 * half + 512), kh + 32 < rem, G, F, h);
             }
         }
         if (i + RING_STAGES < nst) {
@@ -402,8 +426,9 @@ __device__ __forceinline__ bool run_unit(const void* lists, bool l64, int64_t of
                      lane, ls);
         return true;
     }
-    return stream32_ring<SH>(static_cast<const float*>(lists) + off, len, reinterpret_cast<const Coef32*>(kbuf),
-                             diff, lane, R, ls);
+    const float* L = static_cast<const float*>(lists) + off;
+    const Coef32* K = reinterpret_cast<const Coef32*>(kbuf);
+    return diff ? stream32_ring<SH, true>(L, len, K, lane, R, ls) : stream32_ring<SH, false>(L, len, K, lane, R, ls);
 }
 
 // Five blocks of four warps per SM (at most 102 registers a thread): the site
