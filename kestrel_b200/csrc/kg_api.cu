@@ -623,7 +623,7 @@ int kg_autotune(kg_ctx* c, int* slots_out, int* bps_out) {
             return set_err(c, KG_ENOMEM, "cannot allocate device output rows");
         // the site-pass kernel's blocks per SM decide its latency hiding; the
         // slot count only needs to cover the work (the default)
-        const int cand[] = {5, 4, 3};
+        const int cand[] = {4, 3, 2};
         double best = 1e300;
         int bb = 0;
         for (int cd : cand) {

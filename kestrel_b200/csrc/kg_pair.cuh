@@ -526,6 +526,120 @@ struct Shape32 {
     }
 };
 
+// ---------------------------------------------------------------- packed pairs
+// Shape32's hi-coefficient site arithmetic on two sites at once with the
+// sm_100 packed FP32 instructions (fma/mul/add .f32x2): one instruction per
+// operation for both sites, each half rounded exactly as the scalar operation
+// (the reciprocal and the logarithm stay scalar MUFU operations).  Gradient,
+// Hessian and objective partials are pairs, one half per site parity.
+
+__device__ __forceinline__ float2 dup2(float a) { return make_float2(a, a); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 neg2(float2 a) { return make_float2(-a.x, -a.y); }
+__device__ __forceinline__ float2 rcp2(float2 d) { return make_float2(rcp_approx(d.x), rcp_approx(d.y)); }
+
+template <int S>
+struct Shape32x2 {
+    using One = Shape32<S, false>;
+    static constexpr int NG = One::NG, NH = One::NH, GOFF = One::GOFF, HOFF = One::HOFF;
+    float2 k0, k1, k2, k3, s0, s1, s2, s3;
+
+    __device__ __forceinline__ void load(const Coef32* K, bool diff) {
+        const HiLo* kk = S == 0 ? K->a : S == 1 ? K->b1 : S == 2 ? K->b2 : S == 3 ? K->c : K->d;
+        k0 = dup2(ld_volatile(&kk[0].h));
+        k1 = dup2(ld_volatile(&kk[1].h));
+        k2 = S == 4 ? dup2(0.f) : dup2(ld_volatile(&kk[2].h));
+        k3 = (S == 0 || S == 3) ? dup2(ld_volatile(&kk[3].h)) : dup2(0.f);
+        s0 = s1 = s2 = s3 = dup2(0.f);
+        if (diff) {
+            const float* sp = S == 0 ? K->sa : S == 1 ? K->sb1 : S == 2 ? K->sb2 : S == 3 ? K->sc : K->sd;
+            s0 = dup2(ld_volatile(&sp[0]));
+            s1 = dup2(ld_volatile(&sp[1]));
+            if (S != 4) s2 = dup2(ld_volatile(&sp[2]));
+            if (S == 0 || S == 3) s3 = dup2(ld_volatile(&sp[3]));
+        }
+    }
+
+    // Shape32::core on a pair of sites
+    __device__ __forceinline__ void core(float2 t, float2* g, float2* h, float2& d, float2& r, float2& c) const {
+        const float2 EPS = dup2(1e-8f);
+        if (S == 0) {
+            const float2 ph = fma2(fma2(fma2(k3, t, k2), t, k1), t, k0);
+            d = fma2(t, ph, EPS);
+            r = rcp2(d);
+            const float2 u = mul2(r, t), v1 = mul2(u, t), v2 = mul2(v1, t), v3 = mul2(v2, t);
+            g[0] = add2(g[0], u); g[1] = fma2(u, t, g[1]); g[2] = fma2(v1, t, g[2]); g[3] = fma2(v2, t, g[3]);
+            h[0] = fma2(u, u, h[0]); h[1] = fma2(u, v1, h[1]); h[2] = fma2(v1, v1, h[2]);
+            h[3] = fma2(v1, v2, h[3]); h[4] = fma2(v2, v2, h[4]); h[5] = fma2(v2, v3, h[5]);
+            h[6] = fma2(v3, v3, h[6]);
+            c = t;
+        } else if (S == 1 || S == 2) {
+            const float2 w = fma2(neg2(t), t, t);
+            const float2 ph = fma2(fma2(k2, t, k1), t, k0);
+            d = fma2(w, ph, EPS);
+            r = rcp2(d);
+            const float2 v = mul2(r, w), v1 = mul2(v, t), v2 = mul2(v1, t);
+            g[0] = add2(g[0], v); g[1] = fma2(v, t, g[1]); g[2] = fma2(v1, t, g[2]);
+            h[0] = fma2(v, v, h[0]); h[1] = fma2(v, v1, h[1]); h[2] = fma2(v1, v1, h[2]);
+            h[3] = fma2(v1, v2, h[3]); h[4] = fma2(v2, v2, h[4]);
+            c = w;
+        } else if (S == 3) {
+            const float2 ty = add2(dup2(1.0f), neg2(t));
+            const float2 w = mul2(t, ty);
+            const float2 ph = fma2(w, k3, fma2(t, k2, fma2(ty, k1, k0)));
+            d = fma2(w, ph, EPS);
+            r = rcp2(d);
+            const float2 v = mul2(r, w), a = mul2(v, ty), b = mul2(v, t), e = mul2(v, w);
+            g[0] = add2(g[0], v); g[1] = fma2(v, ty, g[1]); g[2] = fma2(v, t, g[2]); g[3] = fma2(v, w, g[3]);
+            h[0] = fma2(v, v, h[0]); h[1] = fma2(v, a, h[1]); h[2] = fma2(v, b, h[2]);
+            h[3] = fma2(v, e, h[3]); h[4] = fma2(a, a, h[4]); h[5] = fma2(b, b, h[5]);
+            h[6] = fma2(e, a, h[6]); h[7] = fma2(e, b, h[7]); h[8] = fma2(e, e, h[8]);
+            c = w;
+        } else {
+            const float2 w = fma2(neg2(t), t, t);
+            const float2 ph = fma2(w, k1, k0);
+            d = fma2(w, ph, EPS);
+            r = rcp2(d);
+            const float2 v = mul2(r, w), a = mul2(v, w);
+            g[0] = add2(g[0], v); g[1] = fma2(v, w, g[1]);
+            h[0] = fma2(v, v, h[0]); h[1] = fma2(v, a, h[1]); h[2] = fma2(a, a, h[2]);
+            c = w;
+        }
+    }
+
+    // Shape32::diff_term on a pair of sites
+    __device__ __forceinline__ float2 diff_term(float2 t, float2 r, float2 c) const {
+        float2 dl;
+        if (S == 0) dl = mul2(t, fma2(fma2(fma2(s3, t, s2), t, s1), t, s0));
+        else if (S == 1 || S == 2) dl = mul2(c, fma2(fma2(s2, t, s1), t, s0));
+        else if (S == 3) dl = mul2(c, fma2(c, s3, fma2(t, s2, fma2(add2(dup2(1.0f), neg2(t)), s1, s0))));
+        else dl = mul2(c, fma2(c, s1, s0));
+        const float2 z = mul2(dl, r);
+        return make_float2(neg_log1m(z.x), neg_log1m(z.y));
+    }
+
+    // four sites (one float4) as two pairs; o collects the objective terms
+    // (direct mode: one lg2 of the product of the four d, in o.y for odd
+    // float4 and o.x for even ones, so each half takes every other one)
+    template <bool DIFF>
+    __device__ __forceinline__ void site4(float4 v, float2* g, float2& o, float2* h, bool odd) const {
+        const float2 ta = make_float2(v.x, v.y), tb = make_float2(v.z, v.w);
+        float2 da, db, ra, rb, ca, cb;
+        core(ta, g, h, da, ra, ca);
+        core(tb, g, h, db, rb, cb);
+        if (!DIFF) {
+            const float2 p = mul2(da, db);
+            const float l = lg2_approx(p.x * p.y);
+            if (odd) o.y += l;
+            else o.x += l;
+        } else {
+            o = add2(o, add2(diff_term(ta, ra, ca), diff_term(tb, rb, cb)));
+        }
+    }
+};
+
 // First-order restoration of the lo coefficients for sums taken with the hi
 // parts only (Shape32<S, false>).  With d = d_hi + delta, delta = c(t) times
 // the lo polynomial, every gradient moment sum_s r c m(s) changes by

@@ -311,46 +311,30 @@ __device__ __forceinline__ float4 lds4(uint32_t a) {
     return v;
 }
 
-// Eight sites of one lane (two float4): FP32 gradient and objective partials,
-// promoted to FP64 at the end.
-template <int S, bool DIFF>
-__device__ __forceinline__ void step8(const Shape32<S, false>& ev, float4 a, float4 b, bool second, double* G,
-                                      double& F, float* h) {
-    constexpr int NG = Shape32<S, false>::NG;
-    float g[NG], ob = 0.f;
-#pragma unroll
-    for (int j = 0; j < NG; j++) g[j] = 0.f;
-    ev.template site4<DIFF>(a, g, ob, h);
-    if (second) ev.template site4<DIFF>(b, g, ob, h);
-#pragma unroll
-    for (int j = 0; j < NG; j++) G[j] += (double)g[j];
-    F += (double)ob;
-}
-
 // One shape's FP32 list from the ring.  Stage i holds float4 128 i .. 128 i +
-// 127; lane l takes 128 i + 32 j + l (j = 0..3), in two steps of 8 sites
-// after each of which the FP32 gradient and objective partials go to FP64;
-// the Hessian partials go every HESS_STAGES stages (64 sites a lane).  Only
-// the list's last stage can be partly filled; the others run without bounds
-// tests.  L and every stage start are 16-byte aligned (list starts are
-// multiples of four entries); a stage's copy rounds its size up to 16 bytes,
-// which stays inside the slot's list buffer.  The sums use the hi
-// coefficients only (lo_correction restores the rest).  Returns false if a
-// wait ran out.
-constexpr int HESS_STAGES = 4;
+// 127; lane l takes 128 i + 32 j + l (j = 0..3): 16 sites, in packed pairs
+// (Shape32x2), whose FP32 gradient and objective partials go to FP64 after
+// every stage (8 sites per partial) and whose Hessian partials go every
+// HESS_STAGES stages (64 sites per partial).  Only the list's last stage can
+// be partly filled; the others run without bounds tests.  L and every stage
+// start are 16-byte aligned (list starts are multiples of four entries); a
+// stage's copy rounds its size up to 16 bytes, which stays inside the slot's
+// list buffer.  The sums use the hi coefficients only (lo_correction restores
+// the rest).  Returns false if a wait ran out.
+constexpr int HESS_STAGES = 8;
 template <int S, bool DIFF>
 __device__ __forceinline__ bool stream32_ring(const float* __restrict__ L, int64_t len, const Coef32* K, int lane,
-                                           const Ring R, LaneSums& out) {
-    using E = Shape32<S, false>;
+                                              const Ring R, LaneSums& out) {
+    using E = Shape32x2<S>;
     constexpr int NG = E::NG, NH = E::NH, GOFF = E::GOFF, HOFF = E::HOFF;
     E ev;
     ev.load(K, DIFF);
     double G[NG], H[NH], F = 0.0;
-    float h[NH];
+    float2 h[NH];
 #pragma unroll
     for (int i = 0; i < NG; i++) G[i] = 0.0;
 #pragma unroll
-    for (int i = 0; i < NH; i++) { H[i] = 0.0; h[i] = 0.f; }
+    for (int i = 0; i < NH; i++) { H[i] = 0.0; h[i] = dup2(0.f); }
     const int64_t n4 = len >> 2;
     const int nst = (int)((len + STAGE_ELEMS - 1) / STAGE_ELEMS);
     const int nfull = (int)(n4 / STAGE_F4);   // stages with all 128 float4 inside the list
@@ -364,21 +348,25 @@ __device__ __forceinline__ bool stream32_ring(const float* __restrict__ L, int64
         if (!mbar_wait(&R.bar[slot], (q / RING_STAGES) & 1u)) { ok = false; break; }
         done = i + 1;
         const uint32_t b = base + slot * (STAGE_F4 * 16);
-        if (i < nfull) {
-            step8<S, DIFF>(ev, lds4(b), lds4(b + 512), true, G, F, h);
-            step8<S, DIFF>(ev, lds4(b + 1024), lds4(b + 1536), true, G, F, h);
-            if (i % HESS_STAGES == HESS_STAGES - 1) {
+        float2 g[NG], o = dup2(0.f);
 #pragma unroll
-                for (int j = 0; j < NH; j++) { H[j] += (double)h[j]; h[j] = 0.f; }
-            }
+        for (int j = 0; j < NG; j++) g[j] = dup2(0.f);
+        if (i < nfull) {
+#pragma unroll
+            for (int j = 0; j < 4; j++) ev.template site4<DIFF>(lds4(b + 512 * j), g, o, h, j & 1);
         } else {
             const int rem = (int)(n4 - (int64_t)i * STAGE_F4);   // float4 in this stage, 0..127
 #pragma unroll
-            for (int half = 0; half < 2; half++) {
-                const int kh = lane + 64 * half;   // this lane's float4 within the stage
-                if (kh < rem)
-                    step8<S, DIFF>(ev, lds4(b + 1024 * half), lds4(b + 1024 * half + 512), kh + 32 < rem, G, F, h);
-            }
+            for (int j = 0; j < 4; j++)
+                if (lane + 32 * j < rem) ev.template site4<DIFF>(lds4(b + 512 * j), g, o, h, j & 1);
+        }
+#pragma unroll
+        for (int j = 0; j < NG; j++) { G[j] += (double)g[j].x; G[j] += (double)g[j].y; }
+        F += (double)o.x;
+        F += (double)o.y;
+        if (i % HESS_STAGES == HESS_STAGES - 1) {
+#pragma unroll
+            for (int j = 0; j < NH; j++) { H[j] += (double)(h[j].x + h[j].y); h[j] = dup2(0.f); }
         }
         if (i + RING_STAGES < nst) {
             __syncwarp();
@@ -397,19 +385,26 @@ __device__ __forceinline__ bool stream32_ring(const float* __restrict__ L, int64
         }
         return false;
     }
+#pragma unroll
+    for (int j = 0; j < NH; j++) H[j] += (double)(h[j].x + h[j].y);
     if (lane < (int)(len & 3)) {
+        // the last len % 4 entries, one site per lane
+        Shape32<S, false> es;
+        es.load(K, DIFF);
         const float* B = reinterpret_cast<const float*>(R.buf + ((seq0 + nst - 1) % RING_STAGES) * STAGE_F4);
-        float g[NG], ob = 0.f;
+        float g[NG], hs[NH], ob = 0.f;
 #pragma unroll
         for (int j = 0; j < NG; j++) g[j] = 0.f;
-        ev.site(B[4 * n4 - (int64_t)(nst - 1) * STAGE_ELEMS + lane], g, ob, h);
+#pragma unroll
+        for (int j = 0; j < NH; j++) hs[j] = 0.f;
+        es.site(B[4 * n4 - (int64_t)(nst - 1) * STAGE_ELEMS + lane], g, ob, hs);
 #pragma unroll
         for (int j = 0; j < NG; j++) G[j] += (double)g[j];
+#pragma unroll
+        for (int j = 0; j < NH; j++) H[j] += (double)hs[j];
         F += (double)ob;
     }
     __syncwarp();   // every lane has read the ring before the next copies
-#pragma unroll
-    for (int j = 0; j < NH; j++) H[j] += (double)h[j];
 #pragma unroll
     for (int j = 0; j < NG; j++) out.m[GOFF + j] = G[j];
 #pragma unroll
@@ -431,9 +426,9 @@ __device__ __forceinline__ bool run_unit(const void* lists, bool l64, int64_t of
     return diff ? stream32_ring<SH, true>(L, len, K, lane, R, ls) : stream32_ring<SH, false>(L, len, K, lane, R, ls);
 }
 
-// Five blocks of four warps per SM (at most 102 registers a thread): the site
-// arithmetic hides its latencies with warps rather than with registers.
-constexpr int PASS_MIN_BLOCKS = 5;
+// Four blocks of four warps per SM (at most 128 registers a thread): the
+// packed site arithmetic needs about 120 registers to run without spills.
+constexpr int PASS_MIN_BLOCKS = 4;
 extern "C" __global__ void __launch_bounds__(128, PASS_MIN_BLOCKS) wave_pass_kernel(WaveArgs A) {
     extern __shared__ __align__(16) char smem[];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
