@@ -151,6 +151,9 @@ class WaveEngine {
              int max_jobs, std::string& err);
     int add(const std::vector<CohortDev>& jobs, std::string& err);
     int wave(std::vector<int>& finished, std::string& err);
+    // Runs waves until the engine is idle inside one graph launch (a device
+    // loop: no host round trip per wave), at most max_waves of them.
+    int run_until_idle(unsigned long long max_waves, std::string& err);
     bool idle() const;
     int64_t n_slots() const;
     int64_t list_cap() const;

@@ -35,6 +35,18 @@ constexpr int ADMIT_WARP_SMEM = UNIT_SITES * 8;   // frequency stage + FP32 outp
 // The unit's frequencies are staged in shared memory transposed (site 32 l + i
 // at [32 i + l], conflict-free); FP32 values go through a shared output buffer
 // so the global stores are coalesced, FP64 values are stored directly.
+// 64-bit shifts as PTX defines them: an amount of 64 or more gives 0.
+__device__ __forceinline__ unsigned long long shr64(unsigned long long v, unsigned s) {
+    unsigned long long r;
+    asm("shr.b64 %0, %1, %2;" : "=l"(r) : "l"(v), "r"(s));
+    return r;
+}
+__device__ __forceinline__ unsigned long long shl64(unsigned long long v, unsigned s) {
+    unsigned long long r;
+    asm("shl.b64 %0, %1, %2;" : "=l"(r) : "l"(v), "r"(s));
+    return r;
+}
+
 template <class T>
 __device__ inline void scatter_lockstep(const CohortDev& co, int64_t x, int64_t y, int lane, int u0, int u1,
                                         const int64_t* off0, T* lists, char* wsm) {
@@ -89,10 +101,37 @@ __device__ inline void scatter_lockstep(const CohortDev& co, int64_t x, int64_t 
                 acc += (unsigned)((tot >> (11 * k)) & 0x7FFull);
             }
         }
-        unsigned long long Q = (sizeof(T) == 4 ? ust : 0ull) + (inc - v);
         __syncwarp();
+        if (sizeof(T) == 4) {
+            // Branch-free: each site has a field index f (A 0, B1 1, B2 2, C 3,
+            // D 4, not jointly observed 5) and the lane's position counters sit
+            // 13 bits apart in R, counting down from 1023: a site of shape f
+            // goes to 1023 - field f and decrements it.  For f = 5 the shift
+            // of 65 reads 0 and decrements nothing, so such a site writes to
+            // position 1023, which no list value of the unit uses (the unit
+            // has fewer than 1024 of them).  A counter that passes 0 only
+            // borrows from counters this lane no longer writes.
+            const unsigned obs = sm.m[0] | sm.m[1] | sm.m[2] | sm.m[3] | sm.m[4];
+            const unsigned f0 = sm.m[1] | sm.m[3] | ~obs, f1 = sm.m[2] | sm.m[3], f2 = sm.m[4] | ~obs;
+            const unsigned long long pre = ust + (inc - v);
+            unsigned long long R = 0;
 #pragma unroll
-        for (int i = 0; i < 32; i++) {
+            for (int k = 0; k < 5; k++)
+                R += (unsigned long long)((long long)(1023 - (int)((pre >> (11 * k)) & 0x7FFull)) << (13 * k));
+            const float* st = reinterpret_cast<const float*>(stage);
+#pragma unroll 8
+            for (int i = 0; i < 32; i++) {
+                const unsigned f = ((f0 >> i) & 1u) | (((f1 >> i) & 1u) << 1) | (((f2 >> i) & 1u) << 2);
+                const unsigned sh = 13u * f;
+                const int pos = 1023 - (int)(shr64(R, sh) & 0x3FFull);
+                R -= shl64(1ull, sh);
+                const float p = st[i * 32 + lane];
+                obuf[pos] = ((sl >> i) & 1u) ? 1.0f - p : p;
+            }
+        }
+        unsigned long long Q = inc - v;
+#pragma unroll
+        for (int i = 0; i < (sizeof(T) == 4 ? 0 : 32); i++) {
             const int code = (int)((c0 & 1u) | ((c1 & 1u) << 1) | ((c2 & 1u) << 2));
             const bool flip = (sl & 1u) != 0;
             c0 >>= 1; c1 >>= 1; c2 >>= 1; sl >>= 1;
@@ -175,13 +214,16 @@ __device__ inline int64_t build_lists(const CohortDev& co, int64_t x, int64_t y,
     return n;
 }
 
-extern "C" __global__ void __launch_bounds__(ADMIT_WARPS * 32, 4) wave_admit_kernel(WaveArgs A) {
+extern "C" __global__ void __launch_bounds__(ADMIT_WARPS * 32, 3) wave_admit_kernel(WaveArgs A) {
     __shared__ int sh_e;
     __shared__ unsigned long long sh_k;
     __shared__ unsigned cnt[ADMIT_WARPS][5];
     extern __shared__ __align__(16) char smem[];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     char* wsm = smem + w * ADMIT_WARP_SMEM;
+    if (A.clk->stop) return;   // a device loop past its last wave
+    if (threadIdx.x == 0) atomicMin(&A.clk->start[0], global_ns());
+    const PhaseEnd pe{&A.clk->end[0], threadIdx.x == 0};
     const int nfree = A.wc_cur->n_free;
     for (;;) {
         if (threadIdx.x == 0) sh_e = atomicAdd(A.admit_task, 1);
@@ -319,22 +361,25 @@ __device__ __forceinline__ float4 lds4(uint32_t a) {
 // be partly filled; the others run without bounds tests.  L and every stage
 // start are 16-byte aligned (list starts are multiples of four entries); a
 // stage's copy rounds its size up to 16 bytes, which stays inside the slot's
-// list buffer.  The sums use the hi coefficients only (lo_correction restores
-// the rest).  Returns false if a wait ran out.
+// list buffer.  The FP64 Hessian sums live in the warp's shared memory (Hs,
+// moment j of lane l at Hs[32 j + l]), which leaves registers for a fifth
+// block per SM.  The sums use the hi coefficients only (lo_correction
+// restores the rest).  Returns false if a wait ran out.
 constexpr int HESS_STAGES = 8;
 template <int S, bool DIFF>
 __device__ __forceinline__ bool stream32_ring(const float* __restrict__ L, int64_t len, const Coef32* K, int lane,
-                                              const Ring R, LaneSums& out) {
+                                              const Ring R, double* Hs, LaneSums& out) {
     using E = Shape32x2<S>;
     constexpr int NG = E::NG, NH = E::NH, GOFF = E::GOFF, HOFF = E::HOFF;
     E ev;
     ev.load(K, DIFF);
-    double G[NG], H[NH], F = 0.0;
+    double G[NG], F = 0.0;
+    double* H = Hs + lane;
     float2 h[NH];
 #pragma unroll
     for (int i = 0; i < NG; i++) G[i] = 0.0;
 #pragma unroll
-    for (int i = 0; i < NH; i++) { H[i] = 0.0; h[i] = dup2(0.f); }
+    for (int i = 0; i < NH; i++) { H[32 * i] = 0.0; h[i] = dup2(0.f); }
     const int64_t n4 = len >> 2;
     const int nst = (int)((len + STAGE_ELEMS - 1) / STAGE_ELEMS);
     const int nfull = (int)(n4 / STAGE_F4);   // stages with all 128 float4 inside the list
@@ -366,7 +411,7 @@ __device__ __forceinline__ bool stream32_ring(const float* __restrict__ L, int64
         F += (double)o.y;
         if (i % HESS_STAGES == HESS_STAGES - 1) {
 #pragma unroll
-            for (int j = 0; j < NH; j++) { H[j] += (double)(h[j].x + h[j].y); h[j] = dup2(0.f); }
+            for (int j = 0; j < NH; j++) { H[32 * j] += (double)(h[j].x + h[j].y); h[j] = dup2(0.f); }
         }
         if (i + RING_STAGES < nst) {
             __syncwarp();
@@ -385,8 +430,9 @@ __device__ __forceinline__ bool stream32_ring(const float* __restrict__ L, int64
         }
         return false;
     }
+    double Hf[NH];
 #pragma unroll
-    for (int j = 0; j < NH; j++) H[j] += (double)(h[j].x + h[j].y);
+    for (int j = 0; j < NH; j++) Hf[j] = H[32 * j] + (double)(h[j].x + h[j].y);
     if (lane < (int)(len & 3)) {
         // the last len % 4 entries, one site per lane
         Shape32<S, false> es;
@@ -401,21 +447,22 @@ __device__ __forceinline__ bool stream32_ring(const float* __restrict__ L, int64
 #pragma unroll
         for (int j = 0; j < NG; j++) G[j] += (double)g[j];
 #pragma unroll
-        for (int j = 0; j < NH; j++) H[j] += (double)hs[j];
+        for (int j = 0; j < NH; j++) Hf[j] += (double)hs[j];
         F += (double)ob;
     }
     __syncwarp();   // every lane has read the ring before the next copies
 #pragma unroll
     for (int j = 0; j < NG; j++) out.m[GOFF + j] = G[j];
 #pragma unroll
-    for (int j = 0; j < NH; j++) out.m[HOFF + j] = H[j];
+    for (int j = 0; j < NH; j++) out.m[HOFF + j] = Hf[j];
     out.obj += F;
     return true;
 }
 
 template <int SH>
 __device__ __forceinline__ bool run_unit(const void* lists, bool l64, int64_t off, int64_t len,
-                                         const void* kbuf, bool diff, int lane, const Ring R, LaneSums& ls) {
+                                         const void* kbuf, bool diff, int lane, const Ring R, double* Hs,
+                                         LaneSums& ls) {
     if (l64) {
         stream64<SH>(static_cast<const double*>(lists) + off, len, reinterpret_cast<const PassCoef*>(kbuf),
                      lane, ls);
@@ -423,17 +470,25 @@ __device__ __forceinline__ bool run_unit(const void* lists, bool l64, int64_t of
     }
     const float* L = static_cast<const float*>(lists) + off;
     const Coef32* K = reinterpret_cast<const Coef32*>(kbuf);
-    return diff ? stream32_ring<SH, true>(L, len, K, lane, R, ls) : stream32_ring<SH, false>(L, len, K, lane, R, ls);
+    return diff ? stream32_ring<SH, true>(L, len, K, lane, R, Hs, ls)
+                : stream32_ring<SH, false>(L, len, K, lane, R, Hs, ls);
 }
 
-// Four blocks of four warps per SM (at most 128 registers a thread): the
-// packed site arithmetic needs about 120 registers to run without spills.
-constexpr int PASS_MIN_BLOCKS = 4;
+// Five blocks of four warps per SM (at most 102 registers a thread).  Each
+// warp's shared memory: the list ring, the pass coefficients with the ring's
+// barriers, and the FP64 Hessian sums of its lanes.
+constexpr int PASS_MIN_BLOCKS = 5;
+constexpr int PASS_HESS_BYTES = 9 * 32 * 8;
+constexpr int PASS_WARP_SMEM = WARP_SMEM + PASS_HESS_BYTES;
 extern "C" __global__ void __launch_bounds__(128, PASS_MIN_BLOCKS) wave_pass_kernel(WaveArgs A) {
     extern __shared__ __align__(16) char smem[];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-    char* wsm = smem + wib * WARP_SMEM;
+    char* wsm = smem + wib * PASS_WARP_SMEM;
     char* kbuf = wsm + WARP_SMEM_BUF;
+    double* hsm = reinterpret_cast<double*>(wsm + WARP_SMEM);
+    if (A.clk->stop) return;   // a device loop past its last wave
+    if (threadIdx.x == 0) atomicMin(&A.clk->start[1], global_ns());
+    const PhaseEnd pe{&A.clk->end[1], lane == 0};
     Ring R;
     R.buf = reinterpret_cast<float4*>(wsm);
     R.bar = reinterpret_cast<uint64_t*>(kbuf + sizeof(Coef32));
@@ -481,11 +536,11 @@ extern "C" __global__ void __launch_bounds__(128, PASS_MIN_BLOCKS) wave_pass_ker
         ls.obj = 0.0;
         bool ok;
         switch (sh) {
-        case 0: ok = run_unit<0>(lists, l64, off, len, kbuf, diff, lane, R, ls); break;
-        case 1: ok = run_unit<1>(lists, l64, off, len, kbuf, diff, lane, R, ls); break;
-        case 2: ok = run_unit<2>(lists, l64, off, len, kbuf, diff, lane, R, ls); break;
-        case 3: ok = run_unit<3>(lists, l64, off, len, kbuf, diff, lane, R, ls); break;
-        default: ok = run_unit<4>(lists, l64, off, len, kbuf, diff, lane, R, ls); break;
+        case 0: ok = run_unit<0>(lists, l64, off, len, kbuf, diff, lane, R, hsm, ls); break;
+        case 1: ok = run_unit<1>(lists, l64, off, len, kbuf, diff, lane, R, hsm, ls); break;
+        case 2: ok = run_unit<2>(lists, l64, off, len, kbuf, diff, lane, R, hsm, ls); break;
+        case 3: ok = run_unit<3>(lists, l64, off, len, kbuf, diff, lane, R, hsm, ls); break;
+        default: ok = run_unit<4>(lists, l64, off, len, kbuf, diff, lane, R, hsm, ls); break;
         }
         if (!__all_sync(0xffffffffu, ok)) {
             if (lane == 0) atomicAdd(&A.counters->stalled_waits, 1ull);
@@ -568,6 +623,9 @@ extern "C" __global__ void __launch_bounds__(128, 4) wave_solve_kernel(WaveArgs 
     const int lane = threadIdx.x & 15;
     const HalfGrp grp{half ? 0xFFFF0000u : 0x0000FFFFu};
     const int i = (blockIdx.x * WAVE_WPB + wib) * 2 + half;
+    if (A.clk->stop) return;   // a device loop past its last wave
+    if (threadIdx.x == 0) atomicMin(&A.clk->start[2], global_ns());
+    const PhaseEnd pe{&A.clk->end[2], (threadIdx.x & 31) == 0};
     if (i >= A.wc_cur->n_pass) return;
     const int s = A.pass_cur[i];
     SlotState& S = A.slots[s];
@@ -739,6 +797,42 @@ __global__ void wave_iota_kernel(int* v, int n) {
     if (i < n) v[i] = i;
 }
 
+// The device loop's step after each wave: adds the wave's phase times and
+// readies the next wave's counters (the next wave reads this wave's next
+// counts as its current ones and accumulates into this wave's current ones).
+// The loop stops once nothing is left (no pass and no resort scheduled, the
+// queue exhausted) or after max_waves waves; the body's last step hands that
+// to the loop condition.  A wave slot past the stop ran nothing and changes
+// nothing.
+__global__ void wave_end_kernel(WaveArgs A, int last, cudaGraphConditionalHandle loop,
+                                unsigned long long max_waves) {
+    if (threadIdx.x != 0) return;
+    WaveClock* c = A.clk;
+    if (!c->stop) {
+        for (int i = 0; i < 3; i++)
+            if (c->end[i] > c->start[i]) c->acc[i] += c->end[i] - c->start[i];
+        c->waves++;
+        const WaveCounts& n = *A.wc_next;
+        if (n.n_pass == 0 && n.n_resort == 0 && *A.queue >= (unsigned long long)A.live->total_pairs) {
+            c->stop = 1;
+        } else if (c->waves >= max_waves) {
+            c->stop = 1;
+            c->limit_hit = 1;
+        }
+        *A.admit_task = 0;
+        *A.pass_task = 0;
+        *A.wc_cur = WaveCounts{};
+    }
+    for (int i = 0; i < 3; i++) {
+        c->start[i] = ~0ull;
+        c->end[i] = 0ull;
+    }
+    if (last) {
+        c->iters++;
+        cudaGraphSetConditional(loop, c->stop ? 0u : 1u);
+    }
+}
+
 // ------------------------------------------------------------ the engine
 
 struct WaveEngine::Impl {
@@ -769,7 +863,23 @@ struct WaveEngine::Impl {
     cudaGraph_t g[2] = {nullptr, nullptr};
     cudaGraphExec_t x[2] = {nullptr, nullptr};
     cudaEvent_t ev[2][4] = {};
+    WaveArgs args[2]{};
+    // the device loop: a WHILE node over two waves (first parity loop_first)
+    WaveClock* clk = nullptr;
+    WaveClock* clk_h = nullptr;
+    cudaGraph_t lg = nullptr;
+    cudaGraphExec_t lx = nullptr;
+    int loop_first = -1;
+    unsigned long long loop_cap = 0;
+    void drop_loop() {
+        if (lx) cudaGraphExecDestroy(lx);
+        if (lg) cudaGraphDestroy(lg);
+        lx = nullptr;
+        lg = nullptr;
+        loop_first = -1;
+    }
     ~Impl() {
+        drop_loop();
         for (int p = 0; p < 2; p++) {
             if (x[p]) cudaGraphExecDestroy(x[p]);
             if (g[p]) cudaGraphDestroy(g[p]);
@@ -817,7 +927,8 @@ int WaveEngine::open(Workspace& ws, cudaStream_t st, const RunConfig& cfg, int64
     KG_WAVE_TRY((cudaError_t)ws.lists_a.reserve(sizeof(int) * 2 * n_slots));   // pass lists
     KG_WAVE_TRY((cudaError_t)ws.lists_b.reserve(sizeof(int) * 2 * n_slots));   // free lists
     KG_WAVE_TRY((cudaError_t)ws.tasks.reserve(sizeof(int4) * 2 * 5 * E.task_cap));
-    KG_WAVE_TRY((cudaError_t)ws.counts.reserve(sizeof(WaveCounts) * 2 + 64 + sizeof(LiveQueue)));
+    const size_t clk_off = (sizeof(WaveCounts) * 2 + 64 + sizeof(LiveQueue) + 15) & ~(size_t)15;
+    KG_WAVE_TRY((cudaError_t)ws.counts.reserve(clk_off + sizeof(WaveClock)));
     KG_WAVE_TRY((cudaError_t)ws.queue.reserve(sizeof(unsigned long long) * 2));
     KG_WAVE_TRY((cudaError_t)ws.counters.reserve(sizeof(RunCounters)));
     KG_WAVE_TRY((cudaError_t)ws.table.reserve(sizeof(CohortDev) * E.max_jobs));
@@ -825,14 +936,17 @@ int WaveEngine::open(Workspace& ws, cudaStream_t st, const RunConfig& cfg, int64
     E.wc = reinterpret_cast<WaveCounts*>(ws.counts.p);
     E.admit_task = reinterpret_cast<int*>(E.wc + 2);
     E.live_d = reinterpret_cast<LiveQueue*>(reinterpret_cast<char*>(ws.counts.p) + sizeof(WaveCounts) * 2 + 64);
+    E.clk = reinterpret_cast<WaveClock*>(reinterpret_cast<char*>(ws.counts.p) + clk_off);
     E.q = ws.queue.as<unsigned long long>();   // [0] pairs, [1] pass units
     int* pass_l[2] = {ws.lists_a.as<int>(), ws.lists_a.as<int>() + n_slots};
     int* free_l[2] = {ws.lists_b.as<int>(), ws.lists_b.as<int>() + n_slots};
     int4* tasks_l[2] = {ws.tasks.as<int4>(), ws.tasks.as<int4>() + 5 * E.task_cap};
     // host read-back (page-locked so the graph can copy into it)
-    const size_t hbytes = sizeof(LiveQueue) + sizeof(WaveCounts) + sizeof(unsigned long long) * (1 + E.max_jobs);
+    const size_t hbytes = sizeof(WaveClock) + sizeof(LiveQueue) + sizeof(WaveCounts) +
+                          sizeof(unsigned long long) * (1 + E.max_jobs);
     KG_WAVE_TRY((cudaError_t)ws.host.reserve(hbytes));
-    E.live_h = ws.host.as<LiveQueue>();
+    E.clk_h = ws.host.as<WaveClock>();
+    E.live_h = reinterpret_cast<LiveQueue*>(E.clk_h + 1);
     E.h_wc = reinterpret_cast<WaveCounts*>(E.live_h + 1);
     E.h_q = reinterpret_cast<unsigned long long*>(E.h_wc + 1);
     E.h_done = E.h_q + 1;
@@ -840,7 +954,7 @@ int WaveEngine::open(Workspace& ws, cudaStream_t st, const RunConfig& cfg, int64
     E.live_h->n_cohorts = 0;
     KG_WAVE_TRY(cudaMemsetAsync(ws.slots.p, 0, sizeof(SlotState) * n_slots, st));   // all SLOT_FREE
     KG_WAVE_TRY(cudaMemsetAsync(ws.queue.p, 0, sizeof(unsigned long long) * 2, st));
-    KG_WAVE_TRY(cudaMemsetAsync(ws.counts.p, 0, sizeof(WaveCounts) * 2 + 64 + sizeof(LiveQueue), st));
+    KG_WAVE_TRY(cudaMemsetAsync(ws.counts.p, 0, clk_off + sizeof(WaveClock), st));
     KG_WAVE_TRY(cudaMemsetAsync(ws.counters.p, 0, sizeof(RunCounters), st));
     KG_WAVE_TRY(cudaMemsetAsync(ws.done.p, 0, sizeof(unsigned long long) * E.max_jobs, st));
     // the first wave's free list holds every slot
@@ -852,11 +966,12 @@ int WaveEngine::open(Workspace& ws, cudaStream_t st, const RunConfig& cfg, int64
     }
     // per device, and cheap: set on every open (serving workers open engines
     // on several threads)
-    KG_WAVE_TRY(cudaFuncSetAttribute(wave_pass_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 4 * WARP_SMEM));
+    KG_WAVE_TRY(
+        cudaFuncSetAttribute(wave_pass_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 4 * PASS_WARP_SMEM));
     KG_WAVE_TRY(cudaFuncSetAttribute(wave_admit_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      ADMIT_WARPS * ADMIT_WARP_SMEM));
     int occ = 0;
-    KG_WAVE_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, wave_pass_kernel, 128, 4 * WARP_SMEM));
+    KG_WAVE_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, wave_pass_kernel, 128, 4 * PASS_WARP_SMEM));
     if (occ <= 0) {
         err = "site-pass kernel cannot be resident";
         return KG_ECUDA;
@@ -889,6 +1004,8 @@ int WaveEngine::open(Workspace& ws, cudaStream_t st, const RunConfig& cfg, int64
     A.tune = make_tune(cfg.iterations);
     A.counters = ws.counters.as<RunCounters>();
     A.cohort_done = ws.done.as<unsigned long long>();
+    A.clk = E.clk;
+    E.drop_loop();
     // One wave (counter resets, admit, pass, solve, read-back) captured as a
     // CUDA graph per parity of the current/next lists, then replayed: one
     // launch per wave instead of a dozen API calls.  External event nodes time
@@ -907,6 +1024,7 @@ int WaveEngine::open(Workspace& ws, cudaStream_t st, const RunConfig& cfg, int64
         Aw.tasks_next = tasks_l[nxt];
         Aw.wc_cur = wc + cur;
         Aw.wc_next = wc + nxt;
+        E.args[par] = Aw;
         KG_WAVE_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
         cudaError_t ce = cudaEventRecordWithFlags(E.ev[par][0], st, cudaEventRecordExternal);
         if (ce == cudaSuccess) ce = cudaMemsetAsync(E.admit_task, 0, sizeof(int), st);
@@ -917,7 +1035,7 @@ int WaveEngine::open(Workspace& ws, cudaStream_t st, const RunConfig& cfg, int64
             ce = cudaEventRecordWithFlags(E.ev[par][1], st, cudaEventRecordExternal);
         }
         if (ce == cudaSuccess) {
-            wave_pass_kernel<<<E.pass_blocks, 128, wsm, st>>>(Aw);
+            wave_pass_kernel<<<E.pass_blocks, 128, WAVE_WPB * PASS_WARP_SMEM, st>>>(Aw);
             ce = cudaEventRecordWithFlags(E.ev[par][2], st, cudaEventRecordExternal);
         }
         if (ce == cudaSuccess) {
@@ -998,6 +1116,77 @@ int WaveEngine::wave(std::vector<int>& finished, std::string& err) {
     return KG_OK;
 }
 
+int WaveEngine::run_until_idle(unsigned long long max_waves, std::string& err) {
+    Impl& E = *d_;
+    const cudaStream_t st = E.st;
+    if (E.idle) return KG_OK;
+    if (!E.lx || E.loop_first != E.cur || E.loop_cap != max_waves) {
+        E.drop_loop();
+        KG_WAVE_TRY(cudaGraphCreate(&E.lg, 0));
+        cudaGraphConditionalHandle h;
+        KG_WAVE_TRY(cudaGraphConditionalHandleCreate(&h, E.lg, 1, cudaGraphCondAssignDefault));
+        cudaGraphNodeParams np{};
+        np.type = cudaGraphNodeTypeConditional;
+        np.conditional.handle = h;
+        np.conditional.type = cudaGraphCondTypeWhile;
+        np.conditional.size = 1;
+        cudaGraphNode_t node;
+        KG_WAVE_TRY(cudaGraphAddNode(&node, E.lg, nullptr, 0, &np));
+        cudaGraph_t body = np.conditional.phGraph_out[0];
+        KG_WAVE_TRY(cudaStreamBeginCaptureToGraph(st, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+        for (int k = 0; k < 2; k++) {
+            const WaveArgs& Aw = E.args[E.cur ^ k];
+            wave_admit_kernel<<<E.admit_blocks, ADMIT_WARPS * 32, ADMIT_WARPS * ADMIT_WARP_SMEM, st>>>(Aw);
+            wave_pass_kernel<<<E.pass_blocks, 128, WAVE_WPB * PASS_WARP_SMEM, st>>>(Aw);
+            wave_solve_kernel<<<E.solve_blocks, 128, WAVE_WPB * WARP_SMEM, st>>>(Aw);
+            wave_end_kernel<<<1, 32, 0, st>>>(Aw, k, h, max_waves);
+        }
+        cudaGraph_t captured = nullptr;
+        const cudaError_t ce = cudaGetLastError();
+        const cudaError_t ee = cudaStreamEndCapture(st, &captured);
+        KG_WAVE_TRY(ce);
+        KG_WAVE_TRY(ee);
+        KG_WAVE_TRY(cudaGraphInstantiate(&E.lx, E.lg, 0));
+        E.loop_first = E.cur;
+        E.loop_cap = max_waves;
+    }
+    // the first wave's counters (later waves: wave_end_kernel) and the clock
+    KG_WAVE_TRY(cudaMemsetAsync(E.admit_task, 0, sizeof(int), st));
+    KG_WAVE_TRY(cudaMemsetAsync(E.q + 1, 0, sizeof(unsigned long long), st));
+    KG_WAVE_TRY(cudaMemsetAsync(E.wc + (E.cur ^ 1), 0, sizeof(WaveCounts), st));
+    KG_WAVE_TRY(cudaMemsetAsync(E.clk, 0, sizeof(WaveClock), st));
+    KG_WAVE_TRY(cudaMemsetAsync(E.clk->start, 0xFF, sizeof(E.clk->start), st));
+    KG_WAVE_TRY(cudaGraphLaunch(E.lx, st));
+    KG_WAVE_TRY(cudaMemcpyAsync(E.clk_h, E.clk, sizeof(WaveClock), cudaMemcpyDeviceToHost, st));
+    KG_WAVE_TRY(cudaMemcpyAsync(E.h_q, E.q, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+    KG_WAVE_TRY(cudaStreamSynchronize(st));
+    const WaveClock c = *E.clk_h;
+    for (int i = 0; i < 3; i++) {
+        E.phase[i] += (double)c.acc[i] * 1e-6;
+        E.total += (double)c.acc[i] * 1e-6;
+    }
+    E.waves += c.waves;
+    E.launches += 8 * c.iters;
+    E.cur ^= (int)(c.waves & 1);
+    E.last_q = *E.h_q;
+    // the next wave's counts, as a host wave would have read them; the clock
+    // no longer stops the kernels
+    KG_WAVE_TRY(cudaMemcpyAsync(E.h_wc, E.wc + E.cur, sizeof(WaveCounts), cudaMemcpyDeviceToHost, st));
+    KG_WAVE_TRY(cudaMemcpyAsync(E.h_done, E.A.cohort_done, sizeof(unsigned long long) * E.max_jobs,
+                                cudaMemcpyDeviceToHost, st));
+    KG_WAVE_TRY(cudaMemsetAsync(&E.clk->stop, 0, sizeof(unsigned int), st));
+    KG_WAVE_TRY(cudaStreamSynchronize(st));
+    const WaveCounts h = *E.h_wc;
+    E.idle = (h.n_pass == 0 && h.n_resort == 0 && E.last_q >= (unsigned long long)E.live_h->total_pairs);
+    for (size_t k = 0; k < E.table.size(); k++)
+        if (E.h_done[k] >= (unsigned long long)E.table[k].n_pairs) E.reported[k] = 1;
+    if (c.limit_hit) {
+        err = "the device wave loop reached its wave limit";
+        return KG_ETIMEOUT;
+    }
+    return KG_OK;
+}
+
 bool WaveEngine::idle() const { return d_->idle; }
 int64_t WaveEngine::n_slots() const { return d_->n_slots; }
 int64_t WaveEngine::list_cap() const { return d_->list_cap; }
@@ -1067,13 +1256,25 @@ int run_waves(const std::vector<PairJob>& jobs, const RunConfig& cfg, Workspace&
     if (r) return r;
     r = eng.add(table, err);
     if (r) return r;
+    if (!cfg.job_done) {
+        // the whole job in one graph launch: no host round trip per wave.
+        // The wave limit only bounds a loop that would not end: a pair takes
+        // at most (1 + backtracks) passes per iteration, twice over if it is
+        // re-run in FP64, and a wave gives every slot one pass.
+        const unsigned long long gens = (unsigned long long)(total_pairs / std::max<int64_t>(1, eng.n_slots())) + 2;
+        uint64_t max_iter = cfg.iterations;
+        for (const CohortDev& d : table) max_iter = std::max<uint64_t>(max_iter, (uint64_t)d.max_iter);
+        const unsigned long long per_pair = 2ull * (max_iter + 2) * 16ull + 64ull;
+        r = eng.run_until_idle(gens * per_pair, err);
+        if (r) return r;
+        return eng.stats(stats, err);
+    }
     std::vector<int> fin;
     while (!eng.idle()) {
         fin.clear();
         r = eng.wave(fin, err);
         if (r) return r;
-        if (cfg.job_done)
-            for (int k : fin) cfg.job_done(k);
+        for (int k : fin) cfg.job_done(k);
     }
     return eng.stats(stats, err);
 }

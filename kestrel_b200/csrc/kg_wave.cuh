@@ -69,6 +69,36 @@ struct LiveQueue {
     int32_t pad;
 };
 
+// Device-side phase clock of the waves (%globaltimer, ns): each wave kernel
+// lowers start[] as its blocks begin and raises end[] as its warps finish;
+// wave_end_kernel adds end - start to acc[] and decides whether the device
+// loop goes on.
+struct WaveClock {
+    unsigned long long start[3];   // admit, pass, solve of the current wave
+    unsigned long long end[3];
+    unsigned long long acc[3];     // summed over the waves of the device loop
+    unsigned long long waves;      // waves the device loop ran
+    unsigned long long iters;      // loop bodies (two wave slots each)
+    unsigned int stop;             // set once the job is done or the limit is hit
+    unsigned int limit_hit;
+};
+
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Raises the phase's end time as the scope closes (one thread per warp or
+// block, as the kernel chooses).
+struct PhaseEnd {
+    unsigned long long* end;
+    bool on;
+    __device__ ~PhaseEnd() {
+        if (on) atomicMax(end, global_ns());
+    }
+};
+
 struct WaveArgs {
     const CohortDev* cohorts;
     const LiveQueue* live;
@@ -96,6 +126,7 @@ struct WaveArgs {
     Tune tune;
     RunCounters* counters;
     unsigned long long* cohort_done;   // finished pairs per cohort
+    WaveClock* clk;
 };
 
 __device__ __forceinline__ int shape_ng(int s) { return s == 0 ? 4 : s == 3 ? 4 : s == 4 ? 2 : 3; }
