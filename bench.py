@@ -419,7 +419,8 @@ def main():
             "hbm_achieved_gbs": list_bytes * pass_sites / (kms * 1e-3) / 1e9,
             "hbm_peak_gbs": measured_hbm_peak(),
             "kernel": "wave_pass_kernel", "kernel_ms": kms, "launches": launches,
-            "kernel_timing": "CUDA events around every wave's site-pass launch, summed per step",
+            "kernel_timing": "device clock (%globaltimer) from the first block's start to the last warp's end "
+                             "of every wave's site-pass launch, summed per step",
             "peak_source": ("half of kg_fp32_peak (B200 FP64 CUDA-core rate)" if fp64_form else
                             "kg_fp32_peak (FFMA loop over all SMs, measured in this run)"),
             "flops_counted": ("executed site arithmetic of the shape-moment passes (FMA = 2, MUFU = 1) "

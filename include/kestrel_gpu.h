@@ -19,6 +19,11 @@
  * a missing call, which the reference turns into a NaN likelihood row
  * (src/vcf.rs:397) and drops for that pair only (src/lanevector.rs:99-104).
  * Codes are sample-major: codes[sample * row_stride + site].
+ *
+ * A call that estimates whole cohorts runs all its waves inside one CUDA graph
+ * launch (a device-side loop).  Kernel profilers cannot see kernels inside such
+ * graphs; with the environment variable KESTREL_HOST_WAVES=1 the host drives
+ * every wave instead (same results, one graph launch per wave).
  */
 #ifndef KESTREL_GPU_H
 #define KESTREL_GPU_H

@@ -188,17 +188,17 @@ __global__ void compact_kernel(const uint8_t* __restrict__ keep, const int32_t* 
     if (v >= n || !keep[v]) return;
     int64_t k = (int64_t)kidx[v] + bsum[v / SCAN_BLOCK];
     site_of[k] = (int32_t)v;
-    p64[k] = pf[v];
+    p64[freq_index(k)] = pf[v];
     q64[k] = qf[v];
-    p32[k] = (float)pf[v];
+    p32[freq_index(k)] = (float)pf[v];
 }
 
 __global__ void pad_kernel(const int32_t* __restrict__ nkept, int64_t cap, float* __restrict__ p32,
                            double* __restrict__ p64, double* __restrict__ q64) {
     int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x + nkept[0];
     if (k >= cap) return;
-    p32[k] = 0.5f;
-    p64[k] = 0.5;
+    p32[freq_index(k)] = 0.5f;
+    p64[freq_index(k)] = 0.5;
     q64[k] = 0.5;
 }
 

@@ -44,6 +44,14 @@ constexpr int SEG_WORDS = SEG_SITES / 32;   // 32-site plane words per padding u
 constexpr int UNIT_SITES = 1024;            // sites per sort unit (one plane word per lane)
 constexpr int UNIT_WORDS = UNIT_SITES / 32;
 
+// Position of kept site k in the unit-transposed frequency arrays: site
+// 1024 u + 32 l + i (lane l's word, bit i) sits at 1024 u + 32 i + l, so the
+// lanes of a warp stepping through bit i of their words read 32 consecutive
+// values.
+__host__ __device__ __forceinline__ int64_t freq_index(int64_t k) {
+    return (k & ~(int64_t)(UNIT_SITES - 1)) | ((k & 31) << 5) | ((k >> 5) & 31);
+}
+
 enum : int { COHORT_TRIANGLE = 0, COHORT_RECT = 1 };
 
 // Device-side description of one cohort (or one serving request).
@@ -51,8 +59,8 @@ struct CohortDev {
     const uint2* planes_x;   // [rows_x][plane_stride] {lo, hi} bit planes of 32 sites
     const uint2* planes_y;   // [rows_y][plane_stride] (== planes_x for a triangle)
     int64_t plane_stride;    // words per row (multiple of SEG_WORDS)
-    const float* p32;        // REF frequency per kept site in FP32, padded
-    const double* p64;       // REF frequency per kept site, padded
+    const float* p32;        // REF frequency per kept site in FP32, padded, unit-transposed (freq_index)
+    const double* p64;       // REF frequency per kept site, padded, unit-transposed (freq_index)
     const double* q64;       // ALT frequency per kept site, padded
     int32_t n_sites;         // kept (segregating) sites
     int32_t n_units;         // sort units of UNIT_SITES kept sites
@@ -294,23 +302,16 @@ __device__ inline void scatter_units(const CohortDev& co, int64_t x, int64_t y, 
     for (int u = u0; u < u1; u++) {
         const int w = u * UNIT_WORDS + lane;
         const uint2 X = px[w], Y = py[w];
-        // stage this lane's 32 REF frequencies: site 32 lane + i at [i * 32 + lane]
+        // stage the unit's REF frequencies (already unit-transposed: site
+        // 32 lane + i at [i * 32 + lane])
         if (sizeof(T) == 4) {
-            const float4* src = reinterpret_cast<const float4*>(co.p32 + (int64_t)u * UNIT_SITES + lane * 32);
+            const float4* src = reinterpret_cast<const float4*>(co.p32 + (int64_t)u * UNIT_SITES);
 #pragma unroll
-            for (int v4 = 0; v4 < 8; v4++) {
-                const float4 f = src[v4];
-                float* st = reinterpret_cast<float*>(stage) + (v4 * 4) * 32 + lane;
-                st[0] = f.x; st[32] = f.y; st[64] = f.z; st[96] = f.w;
-            }
+            for (int v4 = 0; v4 < 8; v4++) reinterpret_cast<float4*>(stage)[v4 * 32 + lane] = src[v4 * 32 + lane];
         } else {
-            const double2* src = reinterpret_cast<const double2*>(co.p64 + (int64_t)u * UNIT_SITES + lane * 32);
+            const double2* src = reinterpret_cast<const double2*>(co.p64 + (int64_t)u * UNIT_SITES);
 #pragma unroll
-            for (int v2 = 0; v2 < 16; v2++) {
-                const double2 f = src[v2];
-                double* st = reinterpret_cast<double*>(stage) + (v2 * 2) * 32 + lane;
-                st[0] = f.x; st[32] = f.y;
-            }
+            for (int v2 = 0; v2 < 16; v2++) reinterpret_cast<double2*>(stage)[v2 * 32 + lane] = src[v2 * 32 + lane];
         }
         ShapeMasks sm = shape_masks(X, Y);
         unsigned long long v = 0;

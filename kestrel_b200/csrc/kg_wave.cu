@@ -1,6 +1,7 @@
 // kg_wave.cu — wave kernels (admit / pass / solve) and their host loop.
 // See kg_wave.cuh for the scheme; the SQP logic restates src/sqp.rs:49-310.
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
 
 #include "kg_engine.h"
@@ -23,18 +24,8 @@ constexpr int WAVE_WPB = 4;   // warps per block of the three wave kernels
 // ------------------------------------------------------------------ admit
 
 constexpr int ADMIT_WARPS = 8;   // warps that build one pair's lists together
-constexpr int ADMIT_WARP_SMEM = UNIT_SITES * 8;   // frequency stage + FP32 output buffer (FP64: stage)
+constexpr int ADMIT_WARP_SMEM = UNIT_SITES * 4;   // FP32 output buffer
 
-// Writes the frequency value t (p or 1 - p by the site's sel bit) of every
-// jointly observed site of units [u0, u1) into its shape list, in site order,
-// starting at off[] in each list.  Lane l owns word l of a unit (sites 32 l ..
-// 32 l + 31): it forms the word's code planes (code = shape + 1 in three bit
-// planes) and the exclusive prefix of the shape counts over the lanes, then
-// steps through its 32 bits in lockstep with the other lanes (no divergence),
-// keeping its five write positions packed 11 bits apiece in one 64-bit word.
-// The unit's frequencies are staged in shared memory transposed (site 32 l + i
-// at [32 i + l], conflict-free); FP32 values go through a shared output buffer
-// so the global stores are coalesced, FP64 values are stored directly.
 // 64-bit shifts as PTX defines them: an amount of 64 or more gives 0.
 __device__ __forceinline__ unsigned long long shr64(unsigned long long v, unsigned s) {
     unsigned long long r;
@@ -47,35 +38,30 @@ __device__ __forceinline__ unsigned long long shl64(unsigned long long v, unsign
     return r;
 }
 
+// Writes the frequency value t (p or 1 - p by the site's sel bit) of every
+// jointly observed site of units [u0, u1) into its shape list, in site order,
+// starting at off[] in each list.  Lane l owns word l of a unit (sites 32 l ..
+// 32 l + 31): it forms the exclusive prefix of the shape counts over the lanes,
+// then steps through its 32 bits in lockstep with the other lanes (no
+// divergence).  The frequencies are read from the unit-transposed arrays, so
+// each step's 32 lanes read 32 consecutive values (L1/L2 hits: every pair
+// reads the same ones); FP32 values go through a shared output buffer so the
+// global stores are coalesced, FP64 values are stored directly.
 template <class T>
 __device__ inline void scatter_lockstep(const CohortDev& co, int64_t x, int64_t y, int lane, int u0, int u1,
                                         const int64_t* off0, T* lists, char* wsm) {
     const uint2* px = co.planes_x + x * co.plane_stride;
     const uint2* py = co.planes_y + y * co.plane_stride;
-    T* stage = reinterpret_cast<T*>(wsm);                                        // UNIT_SITES values
-    float* obuf = reinterpret_cast<float*>(wsm + UNIT_SITES * sizeof(float));   // FP32 only
+    float* obuf = reinterpret_cast<float*>(wsm);   // FP32 only
     int64_t off[5];
 #pragma unroll
     for (int k = 0; k < 5; k++) off[k] = off0[k];
     for (int u = u0; u < u1; u++) {
         const uint2 X = px[u * UNIT_WORDS + lane], Y = py[u * UNIT_WORDS + lane];
-        if (sizeof(T) == 4) {
-            const float4* src = reinterpret_cast<const float4*>(co.p32 + (int64_t)u * UNIT_SITES + lane * 32);
-#pragma unroll
-            for (int v4 = 0; v4 < 8; v4++) {
-                const float4 f = src[v4];
-                float* st = reinterpret_cast<float*>(stage) + (v4 * 4) * 32 + lane;
-                st[0] = f.x; st[32] = f.y; st[64] = f.z; st[96] = f.w;
-            }
-        } else {
-            const double2* src = reinterpret_cast<const double2*>(co.p64 + (int64_t)u * UNIT_SITES + lane * 32);
-#pragma unroll
-            for (int v2 = 0; v2 < 16; v2++) {
-                const double2 f = src[v2];
-                double* st = reinterpret_cast<double*>(stage) + (v2 * 2) * 32 + lane;
-                st[0] = f.x; st[32] = f.y;
-            }
-        }
+        // the unit's REF frequencies, unit-transposed: site 32 lane + i at
+        // [32 i + lane], so step i of the lanes reads 32 consecutive values
+        const T* freq = (sizeof(T) == 4 ? reinterpret_cast<const T*>(co.p32) : reinterpret_cast<const T*>(co.p64)) +
+                        (int64_t)u * UNIT_SITES;
         const ShapeMasks sm = shape_masks(X, Y);
         unsigned c0 = sm.m[0] | sm.m[2] | sm.m[4];   // A 1, B1 2, B2 3, C 4, D 5
         unsigned c1 = sm.m[1] | sm.m[2];
@@ -118,14 +104,14 @@ __device__ inline void scatter_lockstep(const CohortDev& co, int64_t x, int64_t 
 #pragma unroll
             for (int k = 0; k < 5; k++)
                 R += (unsigned long long)((long long)(1023 - (int)((pre >> (11 * k)) & 0x7FFull)) << (13 * k));
-            const float* st = reinterpret_cast<const float*>(stage);
+            const float* st = reinterpret_cast<const float*>(freq);
 #pragma unroll 8
             for (int i = 0; i < 32; i++) {
                 const unsigned f = ((f0 >> i) & 1u) | (((f1 >> i) & 1u) << 1) | (((f2 >> i) & 1u) << 2);
                 const unsigned sh = 13u * f;
                 const int pos = 1023 - (int)(shr64(R, sh) & 0x3FFull);
                 R -= shl64(1ull, sh);
-                const float p = st[i * 32 + lane];
+                const float p = __ldg(st + i * 32 + lane);
                 obuf[pos] = ((sl >> i) & 1u) ? 1.0f - p : p;
             }
         }
@@ -139,7 +125,7 @@ __device__ inline void scatter_lockstep(const CohortDev& co, int64_t x, int64_t 
                 const int sh = 11 * (code - 1);
                 const int pos = (int)((Q >> sh) & 0x7FFull);
                 Q += 1ull << sh;
-                const T p = stage[i * 32 + lane];
+                const T p = __ldg(freq + i * 32 + lane);
                 const T t = flip ? (T)1 - p : p;
                 if (sizeof(T) == 4) {
                     obuf[pos] = (float)t;
@@ -214,7 +200,7 @@ __device__ inline int64_t build_lists(const CohortDev& co, int64_t x, int64_t y,
     return n;
 }
 
-extern "C" __global__ void __launch_bounds__(ADMIT_WARPS * 32, 3) wave_admit_kernel(WaveArgs A) {
+extern "C" __global__ void __launch_bounds__(ADMIT_WARPS * 32, 4) wave_admit_kernel(WaveArgs A) {
     __shared__ int sh_e;
     __shared__ unsigned long long sh_k;
     __shared__ unsigned cnt[ADMIT_WARPS][5];
@@ -1256,7 +1242,11 @@ int run_waves(const std::vector<PairJob>& jobs, const RunConfig& cfg, Workspace&
     if (r) return r;
     r = eng.add(table, err);
     if (r) return r;
-    if (!cfg.job_done) {
+    // KESTREL_HOST_WAVES=1 drives every wave from the host instead (kernel
+    // profilers do not see kernels inside graphs with conditional nodes)
+    const char* hw = std::getenv("KESTREL_HOST_WAVES");
+    const bool host_waves = hw && hw[0] == '1';
+    if (!cfg.job_done && !host_waves) {
         // the whole job in one graph launch: no host round trip per wave.
         // The wave limit only bounds a loop that would not end: a pair takes
         // at most (1 + backtracks) passes per iteration, twice over if it is
@@ -1274,7 +1264,8 @@ int run_waves(const std::vector<PairJob>& jobs, const RunConfig& cfg, Workspace&
         fin.clear();
         r = eng.wave(fin, err);
         if (r) return r;
-        for (int k : fin) cfg.job_done(k);
+        if (cfg.job_done)
+            for (int k : fin) cfg.job_done(k);
     }
     return eng.stats(stats, err);
 }
