@@ -9,6 +9,7 @@
 
 #include <cstdint>
 #include <functional>
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -122,11 +123,17 @@ struct RunConfig {
 
 // Reusable device workspace of the pair engine (per-slot lists and partial
 // sums, slot states, pass lists, queue, counters, cohort table).
+class WaveEngine;
+
 struct Workspace {
     DevBuf scratch, queue, counters, table;
     DevBuf partial, slots, lists_a, lists_b, tasks, counts, done;
     PinBuf host;   // per-wave counters read back by the host loop
     int sm_count = 0;
+    // run_pairs' engine, kept between calls: a call of the same shape only
+    // resets its state and reuses its instantiated graphs (declared last, so
+    // it goes before the buffers its graphs point into)
+    std::shared_ptr<WaveEngine> engine;
 };
 
 int run_pairs(const std::vector<PairJob>& jobs, const RunConfig& cfg, Workspace& ws,

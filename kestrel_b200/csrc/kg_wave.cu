@@ -778,9 +778,11 @@ extern "C" __global__ void __launch_bounds__(128, 4) wave_solve_kernel(WaveArgs 
 
 // ------------------------------------------------------------------- host
 
-__global__ void wave_iota_kernel(int* v, int n) {
+// The first wave's free list: every slot, and its count.
+__global__ void wave_iota_kernel(int* v, int n, int* n_free) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) v[i] = i;
+    if (i == 0) *n_free = n;
 }
 
 // The device loop's step after each wave: adds the wave's phase times and
@@ -857,6 +859,13 @@ struct WaveEngine::Impl {
     cudaGraphExec_t lx = nullptr;
     int loop_first = -1;
     unsigned long long loop_cap = 0;
+    // what open() was last called with, and the buffers its graphs point into
+    bool opened = false;
+    int64_t key_list_cap = 0, key_want = 0, key_expected = 0;
+    int key_max_jobs = 0, key_precision = 0, key_bps = 0, key_dev = -1;
+    uint64_t key_iterations = 0;
+    cudaStream_t key_st = nullptr;
+    std::vector<void*> key_bufs;
     void drop_loop() {
         if (lx) cudaGraphExecDestroy(lx);
         if (lg) cudaGraphDestroy(lg);
@@ -889,6 +898,10 @@ int WaveEngine::open(Workspace& ws, cudaStream_t st, const RunConfig& cfg, int64
     int dev = 0;
     KG_WAVE_TRY(cudaGetDevice(&dev));
     if (ws.sm_count == 0) KG_WAVE_TRY(cudaDeviceGetAttribute(&ws.sm_count, cudaDevAttrMultiProcessorCount, dev));
+    const bool same_call = E.opened && E.key_list_cap == list_cap && E.key_want == cfg.slots &&
+                           E.key_expected == expected_pairs && E.key_max_jobs == E.max_jobs &&
+                           E.key_precision == cfg.precision && E.key_bps == cfg.pass_blocks_per_sm &&
+                           E.key_iterations == cfg.iterations && E.key_dev == dev && E.key_st == st;
     // work units: per shape at most ceil(list_cap / UNIT_ELEMS), over the five
     // shapes at most that + 5
     const int64_t shape_units = (list_cap + UNIT_ELEMS - 1) / UNIT_ELEMS;
@@ -897,13 +910,15 @@ int WaveEngine::open(Workspace& ws, cudaStream_t st, const RunConfig& cfg, int64
     const size_t per_slot = sizeof(double) * (size_t)list_cap + sizeof(double) * E.max_units * UNIT_VALS +
                             sizeof(SlotState) + 4 * sizeof(int) + 2 * 5 * shape_units * sizeof(int4);
     size_t fr = 0, tot = 0;
-    KG_WAVE_TRY(cudaMemGetInfo(&fr, &tot));
     // by default an eighth of the job's pairs, between 4,096 and 32,768: enough
     // to fill the waves, few enough that the last waves drain quickly
     const int64_t want = cfg.slots > 0 ? cfg.slots
                                        : std::min<int64_t>(32768, std::max<int64_t>(4096, expected_pairs / 8));
-    const int64_t by_mem = (int64_t)((fr / 2) / per_slot);
-    E.n_slots = std::max<int64_t>(1, std::min<int64_t>({want, by_mem, std::max<int64_t>(1, expected_pairs)}));
+    if (!same_call) {
+        KG_WAVE_TRY(cudaMemGetInfo(&fr, &tot));
+        const int64_t by_mem = (int64_t)((fr / 2) / per_slot);
+        E.n_slots = std::max<int64_t>(1, std::min<int64_t>({want, by_mem, std::max<int64_t>(1, expected_pairs)}));
+    }
     const int64_t n_slots = E.n_slots;
     E.task_cap = n_slots * shape_units;
     // device buffers (grown and reused through the workspace)
@@ -938,17 +953,29 @@ int WaveEngine::open(Workspace& ws, cudaStream_t st, const RunConfig& cfg, int64
     E.h_done = E.h_q + 1;
     E.live_h->total_pairs = 0;
     E.live_h->n_cohorts = 0;
+    const std::vector<void*> bufs{ws.scratch.p, ws.partial.p, ws.slots.p, ws.lists_a.p, ws.lists_b.p, ws.tasks.p,
+                                  ws.counts.p,  ws.queue.p,   ws.counters.p, ws.table.p, ws.done.p, ws.host.p};
+    const bool reuse = same_call && bufs == E.key_bufs;
+    // the job state of a fresh engine
+    E.table.clear();
+    E.reported.clear();
+    E.last_q = 0;
+    E.cur = 0;
+    E.idle = true;
+    E.waves = 0;
+    for (double& ph : E.phase) ph = 0.0;
+    E.total = 0.0;
     KG_WAVE_TRY(cudaMemsetAsync(ws.slots.p, 0, sizeof(SlotState) * n_slots, st));   // all SLOT_FREE
     KG_WAVE_TRY(cudaMemsetAsync(ws.queue.p, 0, sizeof(unsigned long long) * 2, st));
     KG_WAVE_TRY(cudaMemsetAsync(ws.counts.p, 0, clk_off + sizeof(WaveClock), st));
     KG_WAVE_TRY(cudaMemsetAsync(ws.counters.p, 0, sizeof(RunCounters), st));
     KG_WAVE_TRY(cudaMemsetAsync(ws.done.p, 0, sizeof(unsigned long long) * E.max_jobs, st));
     // the first wave's free list holds every slot
-    wave_iota_kernel<<<(int)((n_slots + 255) / 256), 256, 0, st>>>(free_l[0], (int)n_slots);
-    {
-        const int nf = (int)n_slots;
-        KG_WAVE_TRY(cudaMemcpyAsync(&E.wc[0].n_free, &nf, sizeof(int), cudaMemcpyHostToDevice, st));
-        KG_WAVE_TRY(cudaStreamSynchronize(st));   // nf lives on this stack frame
+    wave_iota_kernel<<<(int)((n_slots + 255) / 256), 256, 0, st>>>(free_l[0], (int)n_slots, &E.wc[0].n_free);
+    KG_WAVE_TRY(cudaGetLastError());
+    if (reuse) {
+        E.launches = 1;
+        return KG_OK;
     }
     // per device, and cheap: set on every open (serving workers open engines
     // on several threads)
@@ -998,6 +1025,18 @@ int WaveEngine::open(Workspace& ws, cudaStream_t st, const RunConfig& cfg, int64
     // its phases.
     const size_t wsm = WAVE_WPB * WARP_SMEM;
     WaveCounts* wc = E.wc;
+    E.opened = false;
+    for (int par = 0; par < 2; par++) {
+        // graphs and events of an earlier open() with other sizes
+        if (E.x[par]) cudaGraphExecDestroy(E.x[par]);
+        if (E.g[par]) cudaGraphDestroy(E.g[par]);
+        E.x[par] = nullptr;
+        E.g[par] = nullptr;
+        for (auto& e : E.ev[par]) {
+            if (e) cudaEventDestroy(e);
+            e = nullptr;
+        }
+    }
     for (int par = 0; par < 2; par++) {
         for (auto& e : E.ev[par]) KG_WAVE_TRY(cudaEventCreate(&e));
         const int cur = par, nxt = par ^ 1;
@@ -1039,6 +1078,17 @@ int WaveEngine::open(Workspace& ws, cudaStream_t st, const RunConfig& cfg, int64
         KG_WAVE_TRY(cudaGraphInstantiate(&E.x[par], E.g[par], 0));
     }
     E.launches = 1;
+    E.opened = true;
+    E.key_list_cap = list_cap;
+    E.key_want = cfg.slots;
+    E.key_expected = expected_pairs;
+    E.key_max_jobs = E.max_jobs;
+    E.key_precision = cfg.precision;
+    E.key_bps = cfg.pass_blocks_per_sm;
+    E.key_iterations = cfg.iterations;
+    E.key_dev = dev;
+    E.key_st = st;
+    E.key_bufs = bufs;
     return KG_OK;
 }
 
@@ -1237,7 +1287,8 @@ int run_waves(const std::vector<PairJob>& jobs, const RunConfig& cfg, Workspace&
               cudaStream_t st, kg_run_stats& stats, std::string& err,
               const std::vector<CohortDev>& table, int64_t total_pairs, int64_t list_cap) {
     (void)jobs;
-    WaveEngine eng;
+    if (!ws.engine) ws.engine = std::make_shared<WaveEngine>();
+    WaveEngine& eng = *ws.engine;
     int r = eng.open(ws, st, cfg, list_cap, total_pairs, (int)table.size(), err);
     if (r) return r;
     r = eng.add(table, err);
