@@ -117,6 +117,19 @@ int kg_set_allele_frequencies(kg_ctx *ctx, const double *af);
 int kg_relatedness(kg_ctx *ctx, int64_t num_samples, uint64_t iterations,
                    double maf, kg_output *out, int64_t out_cap, int64_t *n_out);
 
+/* The reference's default hard-call estimator (-f GT): conditional least
+ * squares with the Brier objective, replacing
+ * calculate_relatedness_coefficients_gt (src/wrapper.rs:22-29, the estimator of
+ * src/coefficients.rs:166-278).  Only sites that every loaded sample calls are
+ * used (the GT reader drops a record with a missing call, src/vcf.rs:217-221);
+ * frequencies are the allele counts over all samples (src/wrapper.rs:412-428)
+ * or those of kg_set_allele_frequencies, with no maf filter.  Rows as
+ * kg_relatedness: obj is the Brier score, iters the QP iterations (at most
+ * `iterations`, src/coefficients.rs:207), cond the reduced-Hessian estimate of
+ * Q at the solution.  Returns KG_ENOSITES when no site is complete. */
+int kg_relatedness_gt(kg_ctx *ctx, int64_t num_samples, uint64_t iterations,
+                      kg_output *out, int64_t out_cap, int64_t *n_out);
+
 /* One-shot form of the reference's
  * calculate_relatedness_coefficients_gl(genotype_likelihoods,
  * allele_frequencies, threads, iterations, minimum_allele_frequency,

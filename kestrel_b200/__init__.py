@@ -155,6 +155,21 @@ class Estimator:
         _check(st, self._h)
         return out
 
+    def relatedness_gt(self, num_samples=None, iterations: int = 100,
+                       out: np.ndarray | None = None) -> np.ndarray:
+        """The reference's default hard-call estimator (-f GT): conditional least
+        squares with the Brier objective (calculate_relatedness_coefficients_gt).
+        Rows as `relatedness`; obj is the Brier score and iters the QP
+        iterations.  Only sites every loaded sample calls are used."""
+        ns = self.n_samples if num_samples is None else int(num_samples)
+        np_ = ns * (ns + 1) // 2
+        if out is None:
+            out = np.empty(np_, OUTPUT_DTYPE)
+        nout = ctypes.c_int64()
+        st = self._L.kg_relatedness_gt(self._h, ns, iterations, ptr(out), out.size, ctypes.byref(nout))
+        _check(st, self._h)
+        return out
+
     def run_stats(self) -> dict:
         s = KgRunStats()
         _check(self._L.kg_last_run_stats(self._h, ctypes.byref(s)), self._h)

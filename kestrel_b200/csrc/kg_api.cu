@@ -502,6 +502,66 @@ int kg_relatedness(kg_ctx* c, int64_t num_samples, uint64_t iterations, double m
     });
 }
 
+// The reference's default hard-call estimator, conditional least squares with
+// the Brier objective (calculate_relatedness_coefficients_gt,
+// src/wrapper.rs:22-29 -> src/coefficients.rs:166-278): the cohort is prepared
+// with the GT reader's site rule and count frequencies, then every pair takes
+// one CLS moment pass and the simplex QP in the wave engine.
+int kg_relatedness_gt(kg_ctx* c, int64_t num_samples, uint64_t iterations, kg_output* out, int64_t out_cap,
+                      int64_t* n_out) {
+    if (!c) return KG_EINVAL;
+    if (!c->loaded) return set_err(c, KG_EINVAL, "no genotypes loaded");
+    if (iterations == 0) return set_err(c, KG_EINVAL, "iterations must be non-zero");
+    int64_t ns = num_samples < 0 ? c->cohort.n_samples : num_samples;
+    if (ns > c->cohort.n_samples || ns == 0)
+        return set_err(c, KG_EINVAL, "Requested samples " + std::to_string(ns) + " exceeds total samples " +
+                                         std::to_string(c->cohort.n_samples));
+    int64_t np = ns * (ns + 1) / 2;
+    if (!out || out_cap < np) return set_err(c, KG_EINVAL, "output capacity must be at least num_samples*(num_samples+1)/2");
+    return guarded(c, [&]() -> int {
+        auto t0 = std::chrono::steady_clock::now();
+        int st = use_device(c);
+        if (st) return st;
+        std::string err;
+        cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+        cudaEventCreate(&ev0);
+        cudaEventCreate(&ev1);
+        cudaEventRecord(ev0, c->stream);
+        st = kg::prepare_cohort(c->cohort, c->cohort.raw.as<uint8_t>(), c->cohort.n_samples,
+                                c->cohort.n_sites, c->cohort.n_sites, true,
+                                c->af_set ? c->af.data() : nullptr, -1.0, c->stream, err, true);
+        if (st) {
+            cudaEventDestroy(ev0);
+            cudaEventDestroy(ev1);
+            return set_err(c, st, err);
+        }
+        if (c->dout.reserve(sizeof(kg_output) * np) != cudaSuccess)
+            return set_err(c, KG_ENOMEM, "cannot allocate device output rows");
+        kg::PairJob jb;
+        jb.panel = &c->cohort;
+        jb.kind = 0;
+        jb.n_x = ns;
+        jb.d_out = c->dout.as<kg_output>();
+        jb.method = kg::ESTIMATOR_CLS;
+        std::vector<kg::PairJob> jobs{jb};
+        kg_run_stats stats{};
+        st = kg::run_pairs(jobs, run_config(c, iterations), c->ws, c->stream, stats, err);
+        cudaEventRecord(ev1, c->stream);
+        int st2 = copy_rows_out(c, c->dout, np, out, c->stream);
+        float dms = 0.f;
+        if (cudaEventElapsedTime(&dms, ev0, ev1) == cudaSuccess) stats.device_ms = dms;
+        cudaEventDestroy(ev0);
+        cudaEventDestroy(ev1);
+        stats.launches += 9;  // count, freq, two scans, compact, pad, pack, Gram, Gram total
+        if (st2 && !st) st = st2;
+        stats.total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        c->last = stats;
+        if (n_out) *n_out = np;
+        if (st) return set_err(c, st, err.empty() ? t_last_err : err);
+        return KG_OK;
+    });
+}
+
 int kg_relatedness_coefficients(const uint8_t* codes, int64_t n_samples, int64_t n_sites,
                                 int64_t row_stride, const double* allele_frequencies, int64_t threads,
                                 uint64_t iterations, double maf, int64_t num_samples, kg_output* out,

@@ -97,10 +97,27 @@ __global__ void count_kernel(const uint8_t* __restrict__ codes, int64_t n_sample
 __global__ void freq_kernel(const int32_t* __restrict__ rc, const int32_t* __restrict__ oc,
                             const double* __restrict__ af, int64_t n_sites, double maf,
                             double* __restrict__ pf, double* __restrict__ qf,
-                            uint8_t* __restrict__ keep) {
+                            uint8_t* __restrict__ keep, int cls, int64_t n_samples) {
     int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (v >= n_sites) return;
     double x0, x1;
+    if (cls) {
+        // the CLS estimator's sites: every sample called (the reference's GT
+        // reader drops a record with any missing call, src/vcf.rs:217-221);
+        // counts over all samples (src/wrapper.rs:412-428), no maf, no drop
+        if (af) {
+            x0 = af[2 * v];
+            x1 = af[2 * v + 1];
+        } else {
+            const double tot = 2.0 * (double)n_samples;
+            x0 = (double)rc[v] / tot;
+            x1 = (double)(2 * n_samples - rc[v]) / tot;
+        }
+        pf[v] = x0;
+        qf[v] = x1;
+        keep[v] = oc[v] == n_samples ? 1 : 0;
+        return;
+    }
     if (af) {
         x0 = af[2 * v];
         x1 = af[2 * v + 1];
@@ -202,6 +219,58 @@ __global__ void pad_kernel(const int32_t* __restrict__ nkept, int64_t cap, float
     q64[k] = 0.5;
 }
 
+// CLS quadratic matrix Q = (1/M) sum over kept sites and all nine (gx, gy) of
+// m m^T (src/quadratic.rs:13-37): per-block partial sums of the 45 upper
+// entries in a fixed order (deterministic), then one block adds the partials
+// in block order.
+constexpr int GRAM_BLOCKS = 148;
+constexpr int GRAM_THREADS = 128;
+__global__ void __launch_bounds__(GRAM_THREADS) cls_gram_kernel(const double* __restrict__ p64,
+                                                                const double* __restrict__ q64,
+                                                                const int32_t* __restrict__ nkept,
+                                                                double* __restrict__ part) {
+    __shared__ double sh[45][GRAM_THREADS];
+    const int64_t n = nkept[0];
+    double h[45];
+#pragma unroll
+    for (int a = 0; a < 45; a++) h[a] = 0.0;
+    for (int64_t k = (int64_t)blockIdx.x * GRAM_THREADS + threadIdx.x; k < n; k += (int64_t)GRAM_BLOCKS * GRAM_THREADS) {
+        const double p = p64[freq_index(k)], q = q64[k];
+        for (int gx = 0; gx < 3; gx++)
+            for (int gy = 0; gy < 3; gy++) {
+                double row[9];
+                cls_row(gx, gy, p, q, row);
+                int a = 0;
+#pragma unroll
+                for (int i = 0; i < 9; i++)
+#pragma unroll
+                    for (int j = i; j < 9; j++) h[a++] += row[i] * row[j];
+            }
+    }
+#pragma unroll
+    for (int a = 0; a < 45; a++) sh[a][threadIdx.x] = h[a];
+    __syncthreads();
+    if (threadIdx.x < 45) {
+        double s = 0.0;
+        for (int t = 0; t < GRAM_THREADS; t++) s += sh[threadIdx.x][t];
+        part[(int64_t)blockIdx.x * 45 + threadIdx.x] = s;
+    }
+}
+
+__global__ void cls_gram_final_kernel(const double* __restrict__ part, const int32_t* __restrict__ nkept,
+                                      double* __restrict__ Q) {
+    const int a = threadIdx.x;
+    if (a >= 45) return;
+    double s = 0.0;
+    for (int b = 0; b < GRAM_BLOCKS; b++) s += part[b * 45 + a];
+    int i = 0, rem = a;
+    while (rem >= 9 - i) { rem -= 9 - i; i++; }
+    const int j = i + rem;
+    const double v = s / (double)nkept[0];
+    Q[i * 9 + j] = v;
+    Q[j * 9 + i] = v;
+}
+
 // Warp per (row, 32-site word): lanes fetch the codes of 32 kept sites and two
 // ballots build the {lo, hi} planes.  Padding and masked-out sites are 3.
 __global__ void pack_kernel(const uint8_t* __restrict__ raw, int64_t n_rows, int64_t stride,
@@ -249,7 +318,7 @@ static int grid_for(int64_t n, int threads) { return (int)std::max<int64_t>(1, c
 
 int prepare_cohort(Cohort& c, const uint8_t* codes, int64_t n_samples, int64_t n_sites,
                    int64_t row_stride, bool codes_on_device, const double* af, double maf,
-                   cudaStream_t st, std::string& err) {
+                   cudaStream_t st, std::string& err, bool cls) {
     if (n_samples <= 0 || n_sites <= 0 || row_stride < n_sites) {
         err = "n_samples and n_sites must be positive and row_stride >= n_sites";
         return KG_EINVAL;
@@ -261,6 +330,7 @@ int prepare_cohort(Cohort& c, const uint8_t* codes, int64_t n_samples, int64_t n
     c.n_samples = n_samples;
     c.n_sites = n_sites;
     c.n_kept = -1;
+    c.cls = cls;
     c.n_seg_max = ceil_div(n_sites, SEG_SITES);
     c.plane_stride = c.n_seg_max * SEG_WORDS;
     const int64_t cap = c.n_seg_max * SEG_SITES;
@@ -306,7 +376,8 @@ int prepare_cohort(Cohort& c, const uint8_t* codes, int64_t n_samples, int64_t n
                                                           c.nkept.as<int32_t>());
     freq_kernel<<<grid_for(n_sites, 256), 256, 0, st>>>(c.rc.as<int32_t>(), c.oc.as<int32_t>(), daf,
                                                          n_sites, maf, c.pfull.as<double>(),
-                                                         c.qfull.as<double>(), c.keep.as<uint8_t>());
+                                                         c.qfull.as<double>(), c.keep.as<uint8_t>(),
+                                                         cls ? 1 : 0, n_samples);
     scan_block_kernel<<<(int)nb, SCAN_BLOCK, 0, st>>>(c.keep.as<uint8_t>(), n_sites,
                                                        c.kidx.as<int32_t>(), c.bsum.as<int32_t>());
     scan_sums_kernel<<<1, SCAN_BLOCK, 0, st>>>(c.bsum.as<int32_t>(), nb, c.nkept.as<int32_t>());
@@ -323,6 +394,14 @@ int prepare_cohort(Cohort& c, const uint8_t* codes, int64_t n_samples, int64_t n
                                             c.nkept.as<int32_t>(), nullptr, c.planes.as<uint2>(),
                                             c.plane_stride);
     }
+    if (cls) {
+        KG_CUDA_TRY((cudaError_t)c.cls_part.reserve(sizeof(double) * GRAM_BLOCKS * 45));
+        KG_CUDA_TRY((cudaError_t)c.cls_q.reserve(sizeof(double) * 81));
+        cls_gram_kernel<<<GRAM_BLOCKS, GRAM_THREADS, 0, st>>>(c.p64.as<double>(), c.q64.as<double>(),
+                                                              c.nkept.as<int32_t>(), c.cls_part.as<double>());
+        cls_gram_final_kernel<<<1, 64, 0, st>>>(c.cls_part.as<double>(), c.nkept.as<int32_t>(),
+                                                c.cls_q.as<double>());
+    }
     KG_CUDA_TRY(cudaGetLastError());
     int32_t h[4];
     KG_CUDA_TRY(cudaMemcpyAsync(h, c.nkept.p, sizeof(h), cudaMemcpyDeviceToHost, st));
@@ -333,7 +412,7 @@ int prepare_cohort(Cohort& c, const uint8_t* codes, int64_t n_samples, int64_t n
     }
     c.n_kept = h[0];
     if (c.n_kept == 0) {
-        err = "no segregating site left after allele-frequency filtering";
+        err = cls ? "no site with a call for every sample" : "no segregating site left after allele-frequency filtering";
         return KG_ENOSITES;
     }
     return KG_OK;
@@ -517,13 +596,14 @@ CohortDev make_cohort_dev(const PairJob& jb, uint64_t iterations) {
     d.n_sites = (int32_t)pn.n_kept;
     d.n_units = (int32_t)ceil_div(pn.n_kept, UNIT_SITES);
     d.kind = jb.kind;
-    d.pad = 0;
+    d.method = jb.method;
     d.n_x = jb.n_x;
     d.n_y = jb.n_y;
     d.pair_begin = 0;
     d.n_pairs = jb.n_pairs();
     d.out = jb.d_out;
     d.max_iter = jb.iterations ? jb.iterations : iterations;
+    d.cls_q = jb.method == ESTIMATOR_CLS ? pn.cls_q.as<double>() : nullptr;
     return d;
 }
 

@@ -75,14 +75,19 @@ struct Cohort {
     DevBuf p64, q64;           // double, same length
     DevBuf site_of;            // int32 kept index -> raw site
     DevBuf planes;             // uint2 [n_samples][plane_stride]
+    bool cls = false;          // prepared for the CLS estimator (complete sites, counts over all samples)
+    DevBuf cls_q;              // CLS: the 9 x 9 quadratic matrix Q, row-major double
+    DevBuf cls_part;           // CLS: per-block partial sums of Q's upper triangle
     size_t device_bytes() const;
 };
 
 // Enqueues the preparation of a cohort on `st`.  codes are host memory unless
-// codes_on_device; af may be NULL.  maf < 0 selects 1/(2 n_samples).
+// codes_on_device; af may be NULL.  maf < 0 selects 1/(2 n_samples).  With cls
+// the sites are those every sample calls, frequencies are counts over all
+// samples (or af), nothing is filtered by frequency, and Q is computed.
 int prepare_cohort(Cohort& c, const uint8_t* codes, int64_t n_samples, int64_t n_sites,
                    int64_t row_stride, bool codes_on_device, const double* af, double maf,
-                   cudaStream_t st, std::string& err);
+                   cudaStream_t st, std::string& err, bool cls = false);
 
 // Unpacks the VCF reader's 2-bit codes + observed mask into device byte codes.
 int unpack_2bit(DevBuf& raw, const uint32_t* codes2, const uint32_t* observed, int64_t n_samples,
@@ -107,7 +112,8 @@ struct PairJob {
     int64_t n_x = 0;                    // triangle: num_samples; rect: query rows
     int64_t n_y = 0;                    // rect: panel rows
     kg_output* d_out = nullptr;         // device rows
-    uint64_t iterations = 0;            // SQP iteration limit (0 = the run's)
+    uint64_t iterations = 0;            // SQP iteration limit (0 = the run's); CLS: QP iterations
+    int method = 0;                     // ESTIMATOR_ML or ESTIMATOR_CLS (panel prepared with cls)
     int64_t n_pairs() const { return kind == 0 ? n_x * (n_x + 1) / 2 : n_x * n_y; }
 };
 

@@ -28,7 +28,7 @@ namespace kg {
 // Kernels defined in kg_engine.cu.
 __global__ void count_kernel(const uint8_t*, int64_t, int64_t, int64_t, int32_t*, int32_t*, int32_t*);
 __global__ void freq_kernel(const int32_t*, const int32_t*, const double*, int64_t, double, double*,
-                            double*, uint8_t*);
+                            double*, uint8_t*, int, int64_t);
 __global__ void scan_block_kernel(const uint8_t*, int64_t, int32_t*, int32_t*);
 __global__ void scan_sums_kernel(int32_t*, int64_t, int32_t*);
 __global__ void compact_kernel(const uint8_t*, const int32_t*, const int32_t*, const double*,
@@ -95,13 +95,14 @@ __global__ void noalloc_table_kernel(kg::CohortDev* table, const uint2* planes, 
     d.n_sites = nkept[0];
     d.n_units = (nkept[0] + kg::UNIT_SITES - 1) / kg::UNIT_SITES;
     d.kind = kg::COHORT_TRIANGLE;
-    d.pad = 0;
+    d.method = kg::ESTIMATOR_ML;
     d.n_x = n_x;
     d.n_y = 0;
     d.pair_begin = 0;
     d.n_pairs = n_x * (n_x + 1) / 2;
     d.out = out;
     d.max_iter = 0;   // the single-kernel engine takes the limit from its launch
+    d.cls_q = nullptr;
     *table = d;
 }
 
@@ -156,7 +157,7 @@ extern "C" int kg_relatedness_noalloc(const uint8_t* d_codes, int64_t n_samples,
     if (e != cudaSuccess) return KG_ECUDA;
     const int g256 = (int)((n_sites + 255) / 256);
     kg::count_kernel<<<g256, 256, 0, s>>>(d_codes, n_samples, n_sites, row_stride, rc, oc, nkept);
-    kg::freq_kernel<<<g256, 256, 0, s>>>(rc, oc, nullptr, n_sites, maf, pfull, qfull, keep);
+    kg::freq_kernel<<<g256, 256, 0, s>>>(rc, oc, nullptr, n_sites, maf, pfull, qfull, keep, 0, n_samples);
     kg::scan_block_kernel<<<(int)nb, 1024, 0, s>>>(keep, n_sites, kidx, bsum);
     kg::scan_sums_kernel<<<1, 1024, 0, s>>>(bsum, nb, nkept);
     kg::compact_kernel<<<g256, 256, 0, s>>>(keep, kidx, bsum, pfull, qfull, n_sites, site_of, p32, p64, q64);

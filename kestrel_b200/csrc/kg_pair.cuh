@@ -65,14 +65,60 @@ struct CohortDev {
     int32_t n_sites;         // kept (segregating) sites
     int32_t n_units;         // sort units of UNIT_SITES kept sites
     int32_t kind;            // COHORT_TRIANGLE or COHORT_RECT
-    int32_t pad;
+    int32_t method;          // ESTIMATOR_ML or ESTIMATOR_CLS
     int64_t n_x;             // triangle: num_samples; rect: query rows
     int64_t n_y;             // rect: panel rows
     int64_t pair_begin;      // first global work index
     int64_t n_pairs;
     kg_output* out;          // rows in the reference's order
-    uint64_t max_iter;       // SQP iteration limit of this cohort's pairs
+    uint64_t max_iter;       // SQP iteration limit of this cohort's pairs (CLS: QP iterations)
+    const double* cls_q;     // CLS: the 9 x 9 quadratic matrix Q (row-major)
 };
+
+// The estimators: maximum likelihood (the GL/PL path, src/coefficients.rs:40-141)
+// and the hard-call conditional least squares with the Brier objective (the
+// reference's default -f GT, src/coefficients.rs:166-278).
+enum : int { ESTIMATOR_ML = 0, ESTIMATOR_CLS = 1 };
+
+// m[gx][gy] of one biallelic site for the CLS estimator: src/iis.rs:279-462
+// with the biallelic joint-genotype modes of src/conditional.rs:6-55 (allele 0
+// = REF with frequency p, allele 1 = ALT with q), products in the reference's
+// order.
+__host__ __device__ inline void cls_row(int gx, int gy, double p, double q, double* row) {
+    for (int k = 0; k < 9; k++) row[k] = 0.0;
+    switch (gx * 3 + gy) {
+    case 0: case 8: {   // ii-ii
+        const double pi = gx == 0 ? p : q, pi2 = pi * pi, pi3 = pi2 * pi;
+        row[0] = pi; row[1] = pi2; row[2] = pi2; row[3] = pi3; row[4] = pi2;
+        row[5] = pi3; row[6] = pi2; row[7] = pi3; row[8] = pi2 * pi2;
+        break;
+    }
+    case 2: case 6: {   // ii-kk
+        const double pi = gx == 0 ? p : q, pk = gx == 0 ? q : p, pi2 = pi * pi, pk2 = pk * pk;
+        row[1] = pi * pk; row[3] = pi * pk2; row[5] = pi2 * pk; row[8] = pi2 * pk2;
+        break;
+    }
+    case 1: case 7: {   // ii-il (0/0, 0/1) and ii-ki (1/1, 0/1)
+        const double pi = gx == 0 ? p : q, po = gx == 0 ? q : p, pi2 = pi * pi, pi3 = pi2 * pi;
+        row[2] = pi * po; row[3] = (2.0 * pi2) * po; row[7] = pi2 * po; row[8] = (2.0 * pi3) * po;
+        break;
+    }
+    case 3: {           // ij-ii
+        const double pi2 = p * p, pi3 = pi2 * p;
+        row[4] = p * q; row[5] = (2.0 * pi2) * q; row[7] = pi2 * q; row[8] = (2.0 * pi3) * q;
+        break;
+    }
+    case 5: {           // ij-jj
+        const double pj2 = q * q;
+        row[4] = p * q; row[5] = (2.0 * pj2) * p; row[7] = pj2 * p; row[8] = (2.0 * (pj2 * q)) * p;
+        break;
+    }
+    case 4: {           // ij-ij
+        row[6] = (2.0 * p) * q; row[7] = (p * q) * (p + q); row[8] = (4.0 * (p * p)) * (q * q);
+        break;
+    }
+    }
+}
 
 struct RunCounters {
     unsigned long long gh_passes;
@@ -877,7 +923,9 @@ __device__ __forceinline__ double warp_sum(double v) {
 
 // ------------------------------------------------------------- pair SQP
 
-enum : int { PASS_FP32_DIRECT = 0, PASS_FP32_DIFF = 1, PASS_FP64 = 2 };
+// Pass kinds: the ML passes (FP32 lists with the direct or the difference
+// objective; FP64) and the single CLS moment pass (FP32 or FP64 lists).
+enum : int { PASS_FP32_DIRECT = 0, PASS_FP32_DIFF = 1, PASS_FP64 = 2, PASS_CLS = 3, PASS_CLS64 = 4 };
 
 struct PairEval {
     double f;       // objective at the evaluated point

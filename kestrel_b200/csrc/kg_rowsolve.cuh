@@ -156,10 +156,11 @@ __device__ __forceinline__ void ldl_solve2_rows(const G& g, const double* Lr, co
 }
 
 // min 1/2 y'Qy + c'y s.t. y >= 0, sum y = 1, from y0.  Hr: this lane's row of Q;
-// lane: the lane's index within the group.
+// lane: the lane's index within the group.  Returns the iteration count the
+// reference returns beside y (src/sqp.rs:112-250).
 template <class G>
-__device__ inline void qp_simplex_rows(const G& grp, const double* Hr, const double* c, const double* y0,
-                                       const Tune& tu, int lane, double* y) {
+__device__ inline int qp_simplex_rows(const G& grp, const double* Hr, const double* c, const double* y0,
+                                      const Tune& tu, int lane, double* y) {
     unsigned work = 0;
 #pragma unroll
     for (int i = 0; i < 9; i++) {
@@ -171,7 +172,7 @@ __device__ inline void qp_simplex_rows(const G& grp, const double* Hr, const dou
         normalise9(y);
         const unsigned F = (~work) & 0x1FFu;
         const int nf = __popc(F);
-        if (nf == 0) return;
+        if (nf == 0) return it;
         const bool rf = (r < 9) && ((F >> r) & 1u);
         double q[9];
 #pragma unroll
@@ -208,7 +209,7 @@ __device__ inline void qp_simplex_rows(const G& grp, const double* Hr, const dou
             else m = fmax(m, a);
         }
         if (!m_nan && m <= tu.qp_zero_search_tol) {
-            if (nf == 9) return;
+            if (nf == 9) return it;
             // full gradient c + Q y
             double gq = 0.0;
             if (r < 9) gq = pick9(c, r) + dot_fma(9, Hr, y);
@@ -218,7 +219,7 @@ __device__ inline void qp_simplex_rows(const G& grp, const double* Hr, const dou
 #pragma unroll
             for (int i = 0; i < 9; i++)
                 if (((work >> i) & 1u) && (best < 0 || gqu[i] < pick9(gqu, best))) best = i;
-            if (pick9(gqu, best) - lambda >= -tu.qp_conv_tol) return;
+            if (pick9(gqu, best) - lambda >= -tu.qp_conv_tol) return it;
             work &= ~(1u << best);
         } else {
             double pv[9];
@@ -243,6 +244,7 @@ __device__ inline void qp_simplex_rows(const G& grp, const double* Hr, const dou
             }
         }
     }
+    return tu.qp_max_iter;
 }
 
 }  // namespace kg

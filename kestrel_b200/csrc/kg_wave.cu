@@ -1,6 +1,7 @@
 // kg_wave.cu — wave kernels (admit / pass / solve) and their host loop.
 // See kg_wave.cuh for the scheme; the SQP logic restates src/sqp.rs:49-310.
 #include <algorithm>
+#include <climits>
 #include <cstdlib>
 #include <cstring>
 
@@ -288,7 +289,8 @@ extern "C" __global__ void __launch_bounds__(ADMIT_WARPS * 32, 4) wave_admit_ker
                 for (int i = 0; i < 9; i++) { S.xc[i] = x0[i]; S.xt[i] = x0[i]; }
                 S.f = 0.0;
                 S.ev = EV_INIT;
-                set_coefficients(S, f64 ? PASS_FP64 : PASS_FP32_DIRECT);
+                if (co.method == ESTIMATOR_CLS) set_coefficients(S, f64 ? PASS_CLS64 : PASS_CLS);
+                else set_coefficients(S, f64 ? PASS_FP64 : PASS_FP32_DIRECT);
                 S.status = SLOT_PASS;
             }
             __syncthreads();
@@ -445,10 +447,155 @@ __device__ __forceinline__ bool stream32_ring(const float* __restrict__ L, int64
     return true;
 }
 
+// ------------------------------------------------------------- CLS moments
+// The CLS estimator's c needs the sums over a pair's sites of its likelihood
+// rows, which are the ML gradient moments with r = 1: per shape sum t^k (A),
+// sum w t^k (B1, B2), sum w {1, ty, t, w} (C) and sum w {1, w} (D).  One pass,
+// no reciprocal and no logarithm; the same FP32 partials of 8 sites per half,
+// promoted to FP64 (the Hessian and objective slots of the partials stay 0).
+template <int S>
+__device__ __forceinline__ void cls_pair(float2 t, float2* g) {
+    if (S == 0) {
+        const float2 t2 = mul2(t, t), t3 = mul2(t2, t);
+        g[0] = add2(g[0], t); g[1] = fma2(t, t, g[1]); g[2] = fma2(t2, t, g[2]); g[3] = fma2(t3, t, g[3]);
+    } else if (S == 1 || S == 2) {
+        const float2 w = fma2(neg2(t), t, t), w1 = mul2(w, t);
+        g[0] = add2(g[0], w); g[1] = fma2(w, t, g[1]); g[2] = fma2(w1, t, g[2]);
+    } else if (S == 3) {
+        const float2 ty = add2(dup2(1.0f), neg2(t)), w = mul2(t, ty);
+        g[0] = add2(g[0], w); g[1] = fma2(w, ty, g[1]); g[2] = fma2(w, t, g[2]); g[3] = fma2(w, w, g[3]);
+    } else {
+        const float2 w = fma2(neg2(t), t, t);
+        g[0] = add2(g[0], w); g[1] = fma2(w, w, g[1]);
+    }
+}
+
+template <int S>
+__device__ __forceinline__ void cls_site(float t, float* g) {
+    if (S == 0) {
+        const float t2 = t * t, t3 = t2 * t;
+        g[0] += t; g[1] = fmaf(t, t, g[1]); g[2] = fmaf(t2, t, g[2]); g[3] = fmaf(t3, t, g[3]);
+    } else if (S == 1 || S == 2) {
+        const float w = fmaf(-t, t, t), w1 = w * t;
+        g[0] += w; g[1] = fmaf(w, t, g[1]); g[2] = fmaf(w1, t, g[2]);
+    } else if (S == 3) {
+        const float ty = 1.0f - t, w = t * ty;
+        g[0] += w; g[1] = fmaf(w, ty, g[1]); g[2] = fmaf(w, t, g[2]); g[3] = fmaf(w, w, g[3]);
+    } else {
+        const float w = fmaf(-t, t, t);
+        g[0] += w; g[1] = fmaf(w, w, g[1]);
+    }
+}
+
+// FP32 lists through the ring (the protocol of stream32_ring).
+template <int S>
+__device__ __forceinline__ bool cls_stream32_ring(const float* __restrict__ L, int64_t len, int lane, const Ring R,
+                                                  LaneSums& out) {
+    constexpr int NG = Shape32x2<S>::NG, NH = Shape32x2<S>::NH, GOFF = Shape32x2<S>::GOFF,
+                  HOFF = Shape32x2<S>::HOFF;
+    double G[NG];
+#pragma unroll
+    for (int i = 0; i < NG; i++) G[i] = 0.0;
+    const int64_t n4 = len >> 2;
+    const int nst = (int)((len + STAGE_ELEMS - 1) / STAGE_ELEMS);
+    const int nfull = (int)(n4 / STAGE_F4);
+    const uint32_t base = smem_u32(R.buf) + 16u * (uint32_t)lane;
+    const uint32_t seq0 = R.seq;
+    bool ok = true;
+    int done = 0;
+    for (int i = 0; i < nst; i++) {
+        const uint32_t q = seq0 + i;
+        const uint32_t slot = q % RING_STAGES;
+        if (!mbar_wait(&R.bar[slot], (q / RING_STAGES) & 1u)) { ok = false; break; }
+        done = i + 1;
+        const uint32_t b = base + slot * (STAGE_F4 * 16);
+        float2 g[NG];
+#pragma unroll
+        for (int j = 0; j < NG; j++) g[j] = dup2(0.f);
+        const int rem = i < nfull ? STAGE_F4 : (int)(n4 - (int64_t)i * STAGE_F4);
+#pragma unroll
+        for (int j = 0; j < 4; j++)
+            if (lane + 32 * j < rem) {
+                const float4 v = lds4(b + 512 * j);
+                cls_pair<S>(make_float2(v.x, v.y), g);
+                cls_pair<S>(make_float2(v.z, v.w), g);
+            }
+#pragma unroll
+        for (int j = 0; j < NG; j++) { G[j] += (double)g[j].x; G[j] += (double)g[j].y; }
+        if (i + RING_STAGES < nst) {
+            __syncwarp();
+            if (lane == 0) {
+                fence_proxy_async_smem();
+                ring_issue(R, L, len, i + RING_STAGES, slot);
+            }
+        }
+    }
+    if (!ok) {
+        const int issued = min(nst, done + RING_STAGES);
+        for (int i = done; i < issued; i++) {
+            const uint32_t q = seq0 + i;
+            if (!mbar_wait(&R.bar[q % RING_STAGES], (q / RING_STAGES) & 1u)) break;
+        }
+        return false;
+    }
+    if (lane < (int)(len & 3)) {
+        const float* B = reinterpret_cast<const float*>(R.buf + ((seq0 + nst - 1) % RING_STAGES) * STAGE_F4);
+        float g[NG];
+#pragma unroll
+        for (int j = 0; j < NG; j++) g[j] = 0.f;
+        cls_site<S>(B[4 * n4 - (int64_t)(nst - 1) * STAGE_ELEMS + lane], g);
+#pragma unroll
+        for (int j = 0; j < NG; j++) G[j] += (double)g[j];
+    }
+    __syncwarp();
+#pragma unroll
+    for (int j = 0; j < NG; j++) out.m[GOFF + j] = G[j];
+#pragma unroll
+    for (int j = 0; j < NH; j++) out.m[HOFF + j] = 0.0;
+    return true;
+}
+
+// FP64 lists (the FP64 form): the same moments in FP64, read directly.
+template <int S>
+__device__ __noinline__ void cls_stream64(const double* __restrict__ L, int64_t len, int lane, LaneSums& out) {
+    constexpr int NG = Shape32x2<S>::NG, NH = Shape32x2<S>::NH, GOFF = Shape32x2<S>::GOFF,
+                  HOFF = Shape32x2<S>::HOFF;
+    double g[NG];
+#pragma unroll
+    for (int i = 0; i < NG; i++) g[i] = 0.0;
+    for (int64_t i = lane; i < len; i += 32) {
+        const double t = L[i];
+        if (S == 0) {
+            const double t2 = t * t, t3 = t2 * t;
+            g[0] += t; g[1] = fma(t, t, g[1]); g[2] = fma(t2, t, g[2]); g[3] = fma(t3, t, g[3]);
+        } else if (S == 1 || S == 2) {
+            const double w = t * (1.0 - t), w1 = w * t;
+            g[0] += w; g[1] = fma(w, t, g[1]); g[2] = fma(w1, t, g[2]);
+        } else if (S == 3) {
+            const double ty = 1.0 - t, w = t * ty;
+            g[0] += w; g[1] = fma(w, ty, g[1]); g[2] = fma(w, t, g[2]); g[3] = fma(w, w, g[3]);
+        } else {
+            const double w = t * (1.0 - t);
+            g[0] += w; g[1] = fma(w, w, g[1]);
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < NG; j++) out.m[GOFF + j] = g[j];
+#pragma unroll
+    for (int j = 0; j < NH; j++) out.m[HOFF + j] = 0.0;
+}
+
 template <int SH>
 __device__ __forceinline__ bool run_unit(const void* lists, bool l64, int64_t off, int64_t len,
                                          const void* kbuf, bool diff, int lane, const Ring R, double* Hs,
-                                         LaneSums& ls) {
+                                         LaneSums& ls, bool cls) {
+    if (cls) {
+        if (l64) {
+            cls_stream64<SH>(static_cast<const double*>(lists) + off, len, lane, ls);
+            return true;
+        }
+        return cls_stream32_ring<SH>(static_cast<const float*>(lists) + off, len, lane, R, ls);
+    }
     if (l64) {
         stream64<SH>(static_cast<const double*>(lists) + off, len, reinterpret_cast<const PassCoef*>(kbuf),
                      lane, ls);
@@ -507,7 +654,8 @@ extern "C" __global__ void __launch_bounds__(128, PASS_MIN_BLOCKS) wave_pass_ker
         const int64_t off = tk.z;
         const int64_t len = tk.w & 0xFFFFFF;
         const int kind = tk.w >> 24;
-        const bool l64 = (kind == PASS_FP64);
+        const bool cls = (kind == PASS_CLS || kind == PASS_CLS64);
+        const bool l64 = (kind == PASS_FP64 || kind == PASS_CLS64);
         const SlotState& S = A.slots[s];
         // first list stages in flight, then the pass's coefficients into shared memory
         if (!l64) ring_prologue(R, reinterpret_cast<const float*>(A.lists + (int64_t)s * A.list_stride) + off, len, lane);
@@ -522,11 +670,11 @@ extern "C" __global__ void __launch_bounds__(128, PASS_MIN_BLOCKS) wave_pass_ker
         ls.obj = 0.0;
         bool ok;
         switch (sh) {
-        case 0: ok = run_unit<0>(lists, l64, off, len, kbuf, diff, lane, R, hsm, ls); break;
-        case 1: ok = run_unit<1>(lists, l64, off, len, kbuf, diff, lane, R, hsm, ls); break;
-        case 2: ok = run_unit<2>(lists, l64, off, len, kbuf, diff, lane, R, hsm, ls); break;
-        case 3: ok = run_unit<3>(lists, l64, off, len, kbuf, diff, lane, R, hsm, ls); break;
-        default: ok = run_unit<4>(lists, l64, off, len, kbuf, diff, lane, R, hsm, ls); break;
+        case 0: ok = run_unit<0>(lists, l64, off, len, kbuf, diff, lane, R, hsm, ls, cls); break;
+        case 1: ok = run_unit<1>(lists, l64, off, len, kbuf, diff, lane, R, hsm, ls, cls); break;
+        case 2: ok = run_unit<2>(lists, l64, off, len, kbuf, diff, lane, R, hsm, ls, cls); break;
+        case 3: ok = run_unit<3>(lists, l64, off, len, kbuf, diff, lane, R, hsm, ls, cls); break;
+        default: ok = run_unit<4>(lists, l64, off, len, kbuf, diff, lane, R, hsm, ls, cls); break;
         }
         if (!__all_sync(0xffffffffu, ok)) {
             if (lane == 0) atomicAdd(&A.counters->stalled_waits, 1ull);
@@ -563,7 +711,7 @@ __device__ inline void finish_slot(const WaveArgs& A, SlotState& S, int s, const
         atomicAdd(&C->pair_sites, (unsigned long long)S.n);
         atomicAdd(&C->work_units, (unsigned long long)S.n * (unsigned long long)S.gh);
         if (iters >= co.max_iter) atomicAdd(&C->nonconverged, 1ull);
-        const int p32 = S.gh - S.f64p;
+        const int p32 = co.method == ESTIMATOR_CLS ? 0 : S.gh - S.f64p;   // the ML site arithmetic only
         unsigned long long f32 = 0, f64 = 0;
         for (int sh = 0; sh < 5; sh++) {
             atomicAdd(&C->shape_sites[sh], (unsigned long long)S.cnt[sh]);
@@ -576,6 +724,148 @@ __device__ inline void finish_slot(const WaveArgs& A, SlotState& S, int s, const
         A.free_next[atomicAdd(&A.wc_next->n_free, 1)] = s;
         atomicAdd(&A.cohort_done[S.cohort], 1ull);
     }
+}
+
+// A self pair's CLS problem: the two-variable QP on (Delta1, Delta7) from
+// (1/2, 1/2) (src/coefficients.rs:231-240), the active-set method of
+// src/sqp.rs:112-250 with N = 2 written out on scalars (GMW81 LDL^T of
+// src/cholesky.rs:6-65 for one or two free variables).  One thread.
+__device__ __forceinline__ int cls_self_qp(double q00, double q01, double q10, double q11, double c0, double c1,
+                                           const Tune& tq, double& y0, double& y1) {
+    const double eps = 2.220446049250313e-16;
+    y0 = 0.5;
+    y1 = 0.5;
+    bool w0 = y0 == 0.0, w1 = y1 == 0.0;
+    int it = 0;
+    while (it < tq.qp_max_iter) {
+        const double sy = (0.0 + y0) + y1;
+        y0 = y0 / sy;
+        y1 = y1 / sy;
+        const int nf = (w0 ? 0 : 1) + (w1 ? 0 : 1);
+        if (nf == 0) return it;
+        double lambda, p0 = 0.0, p1 = 0.0, m;
+        bool m_nan;
+        if (nf == 2) {
+            const double g0 = c0 + fma(q01, y1, fma(q00, y0, 0.0));
+            const double g1 = c1 + fma(q11, y1, fma(q10, y0, 0.0));
+            const double gamma = fmax(fmax(0.0, fabs(q00)), fabs(q11));
+            const double xi = fmax(0.0, fabs(q01));
+            const double delta = eps * fmax(1.0, gamma + xi);
+            const double beta2 = fmax(fmax(gamma, xi / sqrt(3.0)), eps);
+            const double theta = fmax(0.0, fabs(q10));
+            const double d0 = fmax(fmax(fabs(q00), theta * theta / beta2), delta);
+            const double l10 = q10 / d0;
+            const double pv0 = d0 * l10;
+            const double d1 = fmax(fmax(fabs(q11 - fma(pv0, l10, 0.0)), 0.0 / beta2), delta);
+            double b0 = g0, b1 = g1 - fma(b0, l10, 0.0);
+            b0 = b0 / d0;
+            b1 = b1 / d1;
+            b0 = b0 - fma(b1, l10, 0.0);
+            double o0 = 1.0, o1 = 1.0 - fma(o0, l10, 0.0);
+            o0 = o0 / d0;
+            o1 = o1 / d1;
+            o0 = o0 - fma(o1, l10, 0.0);
+            lambda = ((0.0 + b0) + b1) / ((0.0 + o0) + o1);
+            const double f0 = lambda * o0 - b0, f1 = lambda * o1 - b1;
+            m_nan = isnan(f0) || isnan(f1);
+            m = fmax(fabs(f0), fabs(f1));
+            p0 = f0;
+            p1 = f1;
+        } else {
+            // one free variable k: the 1 x 1 factor
+            const bool k0 = !w0;
+            const double a = k0 ? q00 : q11, ck = k0 ? c0 : c1, yk = k0 ? y0 : y1;
+            const double g = ck + fma(a, yk, 0.0);
+            const double gamma = fmax(0.0, fabs(a));
+            const double delta = eps * fmax(1.0, gamma + 0.0);
+            const double d0 = fmax(fmax(fabs(a), 0.0), delta);
+            const double b = g / d0, o = 1.0 / d0;
+            lambda = (0.0 + b) / (0.0 + o);
+            const double f = lambda * o - b, f_pad = lambda * 0.0 - 0.0;
+            m_nan = isnan(f) || isnan(f_pad);
+            m = fmax(fabs(f), fabs(f_pad));
+            if (k0) p0 = f;
+            else p1 = f;
+        }
+        if (!m_nan && m <= tq.qp_zero_search_tol) {
+            if (nf == 2) return it;
+            const double gq0 = c0 + fma(q01, y1, fma(q00, y0, 0.0));
+            const double gq1 = c1 + fma(q11, y1, fma(q10, y0, 0.0));
+            const int best = w0 ? ((w1 && gq1 < gq0) ? 1 : 0) : 1;
+            const double gb = best == 0 ? gq0 : gq1;
+            if (gb - lambda >= -tq.qp_conv_tol) return it;
+            if (best == 0) w0 = false;
+            else w1 = false;
+        } else {
+            double alpha = 1.0;
+            int block = -1;
+            if (p0 < 0.0) {
+                const double a = -y0 / p0;
+                if (a < alpha) { alpha = a; block = 0; }
+            }
+            if (p1 < 0.0) {
+                const double a = -y1 / p1;
+                if (a < alpha) { alpha = a; block = 1; }
+            }
+            y0 = fmax(y0 + alpha * p0, 0.0);
+            y1 = fmax(y1 + alpha * p1, 0.0);
+            if (block == 0) { w0 = true; y0 = 0.0; }
+            if (block == 1) { w1 = true; y1 = 0.0; }
+        }
+        it++;
+    }
+    return it;
+}
+
+// The CLS estimator's step after its one moment pass (src/coefficients.rs:
+// 218-268): c = (the pair's summed likelihood rows) / (-M), every pair using
+// all M kept sites; the simplex QP on the cohort's Q from 1/9, or the
+// two-variable QP on (Delta1, Delta7) from (1/2, 1/2) for a self pair, with the
+// cohort's iteration limit; then the Brier score, the condition estimate at
+// g = Q delta + c, and the row (iters = the QP's iteration count).
+__device__ __forceinline__ void cls_finish(const WaveArgs& A, SlotState& S, int s, const double* mom_s, int lane,
+                                  const HalfGrp& grp) {
+    const CohortDev& co = A.cohorts[S.cohort];
+    const double m = (double)co.n_sites;
+    double Sg = 0.0, Ht[9];
+    if (lane < 9) rebuild_row(mom_s, lane, Sg, Ht);
+    double c[9];
+    gather9(grp, Sg / -m, c);
+    double Qr[9];
+#pragma unroll
+    for (int j = 0; j < 9; j++) Qr[j] = lane < 9 ? co.cls_q[lane * 9 + j] : 0.0;
+    Tune tq = A.tune;
+    tq.qp_max_iter = co.max_iter > (uint64_t)INT_MAX ? INT_MAX : (int)co.max_iter;
+    double delta[9];
+    int iters;
+    if (co.kind == COHORT_TRIANGLE && S.x == S.y) {
+        double e0 = 0.0, e6 = 0.0;
+        int it2 = 0;
+        if (lane == 0)
+            it2 = cls_self_qp(co.cls_q[0], co.cls_q[6], co.cls_q[6 * 9], co.cls_q[6 * 9 + 6], c[0], c[6], tq, e0, e6);
+        e0 = __shfl_sync(grp.mask, e0, 0, 16);
+        e6 = __shfl_sync(grp.mask, e6, 0, 16);
+        iters = __shfl_sync(grp.mask, it2, 0, 16);
+#pragma unroll
+        for (int j = 0; j < 9; j++) delta[j] = 0.0;
+        delta[0] = e0;
+        delta[6] = e6;
+    } else {
+        double y0[9];
+#pragma unroll
+        for (int j = 0; j < 9; j++) y0[j] = 1.0 / 9.0;
+        iters = qp_simplex_rows(grp, Qr, c, y0, tq, lane, delta);
+    }
+    double qd[9];
+    gather9(grp, lane < 9 ? dot_fma(9, Qr, delta) : 0.0, qd);
+    const double quad = dot_fma(9, delta, qd);
+    const double lin = 2.0 * dot_fma(9, c, delta);
+    const double brier = (quad + lin) + 1.0;
+    double g[9];
+#pragma unroll
+    for (int j = 0; j < 9; j++) g[j] = qd[j] + c[j];
+    const double cond = condition_rows(grp, delta, g, Qr, tq.sqp_conv_tol);
+    finish_slot(A, S, s, delta, brier, (uint64_t)iters, cond, lane);
 }
 
 // Schedules the slot's next pass at S.xt (lane 0 has written xt).  A pass in
@@ -647,6 +937,11 @@ extern "C" __global__ void __launch_bounds__(128, 4) wave_solve_kernel(WaveArgs 
     }
     grp.sync();
     const int kind = S.kind;
+    if (kind == PASS_CLS || kind == PASS_CLS64) {
+        if (lane == 0) S.gh++;
+        cls_finish(A, S, s, mom_s, lane, grp);
+        return;
+    }
     const double n = (double)S.n;
     double corr = 0.0;
     if (kind != PASS_FP64) {

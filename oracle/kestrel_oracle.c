@@ -281,10 +281,11 @@ static double sumn(int n, const double *a) {
     for (int i = 0; i < n; i++) s += a[i];
     return s;
 }
-static void sum_to_one(const double *x, double *out) {
-    double s = sumn(9, x);
-    for (int i = 0; i < 9; i++) out[i] = x[i] / s;
+static void sum_to_one_n(int n, const double *x, double *out) {
+    double s = sumn(n, x);
+    for (int i = 0; i < n; i++) out[i] = x[i] / s;
 }
+static void sum_to_one(const double *x, double *out) { sum_to_one_n(9, x, out); }
 static void matvec(int n, const double M[9][9], const double *v, double *out) {
     for (int i = 0; i < n; i++) out[i] = dotn(n, M[i], v);
 }
@@ -379,10 +380,10 @@ static int kkt_converged(const double x[9], const double g[9], double tol) {
 }
 
 /* src/sqp.rs:252-268 */
-static double feasible_step(const double y[9], const double p[9], int *block) {
+static double feasible_step_n(int n, const double y[9], const double p[9], int *block) {
     double alpha = 1.0;
     *block = -1;
-    for (int i = 0; i < 9; i++) {
+    for (int i = 0; i < n; i++) {
         if (p[i] < 0.0) {
             double a = -y[i] / p[i];
             if (a < alpha) { alpha = a; *block = i; }
@@ -391,20 +392,22 @@ static double feasible_step(const double y[9], const double p[9], int *block) {
     return alpha;
 }
 
-/* Active-set QP on the simplex, src/sqp.rs:112-250 (modify = true). */
-static void qp_active_set(const double Q[9][9], const double c[9], const double y0[9],
-                          const tune_t *tu, double y_out[9]) {
-    double y[9];
-    int work[9];
-    memcpy(y, y0, sizeof y);
-    for (int i = 0; i < 9; i++) work[i] = (y[i] == 0.0);
+/* Active-set QP on the simplex of dimension n <= 9, src/sqp.rs:112-250
+ * (modify = true; the reference's const generic N is n here).  Returns the
+ * iteration count the reference returns beside y. */
+static uint64_t qp_active_set_n(int n, const double Q[9][9], const double c[9], const double y0[9],
+                                const tune_t *tu, double y_out[9]) {
+    double y[9] = {0};
+    int work[9] = {0};
+    memcpy(y, y0, sizeof(double) * n);
+    for (int i = 0; i < n; i++) work[i] = (y[i] == 0.0);
     uint64_t it = 0;
     while (it < tu->qp_max_iter) {
         double ys[9];
-        sum_to_one(y, ys);
-        memcpy(y, ys, sizeof y);
+        sum_to_one_n(n, y, ys);
+        memcpy(y, ys, sizeof(double) * n);
         int fi[9], nf = 0;
-        for (int i = 0; i < 9; i++) if (!work[i]) fi[nf++] = i;
+        for (int i = 0; i < n; i++) if (!work[i]) fi[nf++] = i;
         if (nf == 0) abort(); /* the reference asserts here */
         double yf[9] = {0}, cf[9] = {0}, Qf[9][9] = {{0}};
         for (int i = 0; i < nf; i++) {
@@ -422,10 +425,10 @@ static void qp_active_set(const double Q[9][9], const double c[9], const double 
         for (int i = 0; i < nf; i++) ones[i] = 1.0;
         ldl_solve(nf, L, D, ones);
         double lambda = sumn(nf, gf) / sumn(nf, ones);
-        /* The reference forms lambda*ones - g over all 9 slots; the slots past
+        /* The reference forms lambda*ones - g over all N slots; the slots past
          * nf are zero on both sides. */
         double m = 0.0;
-        for (int i = 0; i < 9; i++) {
+        for (int i = 0; i < n; i++) {
             gf[i] = lambda * ones[i] - gf[i];
             double a = fabs(gf[i]);
             /* a total order that ranks NaN above everything, as total_cmp does */
@@ -433,28 +436,34 @@ static void qp_active_set(const double Q[9][9], const double c[9], const double 
             else if (a > m) m = a;
         }
         if (m <= tu->qp_zero_search_tol) {
-            if (nf == 9) { memcpy(y_out, y, sizeof y); return; }
+            if (nf == n) { memcpy(y_out, y, sizeof(double) * n); return it; }
             double qy9[9], gq[9];
-            matvec(9, Q, y, qy9);
-            for (int i = 0; i < 9; i++) gq[i] = c[i] + qy9[i];
+            matvec(n, Q, y, qy9);
+            for (int i = 0; i < n; i++) gq[i] = c[i] + qy9[i];
             int best = -1;
-            for (int i = 0; i < 9; i++)
+            for (int i = 0; i < n; i++)
                 if (work[i] && (best < 0 || gq[i] < gq[best])) best = i;
             double mult = gq[best] - lambda;
-            if (mult >= -tu->qp_conv_tol) { memcpy(y_out, y, sizeof y); return; }
+            if (mult >= -tu->qp_conv_tol) { memcpy(y_out, y, sizeof(double) * n); return it; }
             work[best] = 0;
         } else {
             double p[9] = {0};
             int k = 0;
-            for (int i = 0; i < 9; i++) if (!work[i]) p[i] = gf[k++];
+            for (int i = 0; i < n; i++) if (!work[i]) p[i] = gf[k++];
             int block;
-            double alpha = feasible_step(y, p, &block);
-            for (int i = 0; i < 9; i++) y[i] = fmax(y[i] + alpha * p[i], 0.0);
+            double alpha = feasible_step_n(n, y, p, &block);
+            for (int i = 0; i < n; i++) y[i] = fmax(y[i] + alpha * p[i], 0.0);
             if (block >= 0) { work[block] = 1; y[block] = 0.0; }
         }
         it++;
     }
-    memcpy(y_out, y, sizeof y);
+    memcpy(y_out, y, sizeof(double) * n);
+    return it;
+}
+
+static void qp_active_set(const double Q[9][9], const double c[9], const double y0[9],
+                          const tune_t *tu, double y_out[9]) {
+    (void)qp_active_set_n(9, Q, c, y0, tu, y_out);
 }
 
 /* Reduced-Hessian condition estimate, src/sqp.rs:313-391. */
@@ -736,5 +745,174 @@ int kor_eval_pair(const uint8_t *codes_x, const uint8_t *codes_y, int64_t n_site
     pair_grad_hess(&rb, delta, 1e-8, g, H);
     memcpy(h, H, sizeof H);
     free(rb.blocks);
+    return KOR_OK;
+}
+
+/* ------------------------------------------- GT conditional least squares */
+/* m[gx][gy] of one biallelic site, src/iis.rs:279-462 with the biallelic IIS
+ * modes of src/conditional.rs:6-55 (allele 0 = REF with frequency p, 1 = ALT
+ * with q), products in the reference's order. */
+static void cls_row(int gx, int gy, double p, double q, double row[9]) {
+    for (int k = 0; k < 9; k++) row[k] = 0.0;
+    switch (gx * 3 + gy) {
+    case 0: case 8: { /* M1 ii-ii, pi = p or q */
+        const double pi = gx == 0 ? p : q, pi2 = pi * pi, pi3 = pi2 * pi;
+        row[0] = pi; row[1] = pi2; row[2] = pi2; row[3] = pi3; row[4] = pi2;
+        row[5] = pi3; row[6] = pi2; row[7] = pi3; row[8] = pi2 * pi2; break;
+    }
+    case 2: case 6: { /* M2 ii-kk */
+        const double pi = gx == 0 ? p : q, pk = gx == 0 ? q : p;
+        const double pi2 = pi * pi, pk2 = pk * pk;
+        row[1] = pi * pk; row[3] = pi * pk2; row[5] = pi2 * pk; row[8] = pi2 * pk2; break;
+    }
+    case 1: case 7: { /* M3 ii-il (0/0, 0/1: pl = q) and M4 ii-ki (1/1, 0/1: pk = p) */
+        const double pi = gx == 0 ? p : q, po = gx == 0 ? q : p;
+        const double pi2 = pi * pi, pi3 = pi2 * pi;
+        row[2] = pi * po; row[3] = (2.0 * pi2) * po; row[7] = pi2 * po; row[8] = (2.0 * pi3) * po; break;
+    }
+    case 3: { /* M6 ij-ii: pi = p, pj = q */
+        const double pi = p, pj = q, pi2 = pi * pi, pi3 = pi2 * pi;
+        row[4] = pi * pj; row[5] = (2.0 * pi2) * pj; row[7] = pi2 * pj; row[8] = (2.0 * pi3) * pj; break;
+    }
+    case 5: { /* M7 ij-jj: pi = p, pj = q */
+        const double pi = p, pj = q, pj2 = pj * pj;
+        row[4] = pi * pj; row[5] = (2.0 * pj2) * pi; row[7] = pj2 * pi; row[8] = (2.0 * (pj2 * pj)) * pi; break;
+    }
+    case 4: { /* M9 ij-ij */
+        const double pi = p, pj = q, pi2 = pi * pi, pj2 = pj * pj;
+        row[6] = (2.0 * pi) * pj; row[7] = (pi * pj) * (pi + pj); row[8] = (4.0 * pi2) * pj2; break;
+    }
+    }
+}
+
+/* The reference's default hard-call estimator (src/coefficients.rs:166-278 with
+ * src/cls.rs:6-49 and the Gram matrix of src/quadratic.rs), for biallelic
+ * sites:
+ *  - a site is used only if every sample has a call (src/vcf.rs:217-221 drops
+ *    the whole record otherwise); monomorphic sites stay, and there is no maf
+ *    filter (src/wrapper.rs:22-40);
+ *  - allele frequencies are counts / (2 n_samples) over all samples
+ *    (src/wrapper.rs:412-428) unless af_in gives them;
+ *  - the per-site rows m[gx][gy] are src/iis.rs:279-462 through
+ *    src/cls.rs:6-25 (cls_row);
+ *  - Q = (1/M) sum over sites and all nine (gx, gy) of m m^T (src/quadratic.rs:13-37);
+ *  - per pair c = (sum over sites of m[gx][gy]) / (-M) (src/cls.rs:27-49,
+ *    scale_div of src/algebra.rs:61-63);
+ *  - the simplex QP from 1/9 (x != y), or the two-variable QP on (Delta1,
+ *    Delta7) from (1/2, 1/2) for x == y, with qp_max_iter = iterations
+ *    (src/coefficients.rs:207, :231-244);
+ *  - obj = delta.Q delta + 2 c.delta + 1 (Brier), iters = the QP's iteration
+ *    count, cond = the reduced-Hessian estimate at g = Q delta + c
+ *    (src/coefficients.rs:253-268). */
+int kor_cls_relatedness(const uint8_t *codes, int64_t n_samples, int64_t n_sites, int64_t stride,
+                        const double *af_in, int64_t num_samples, uint64_t iterations, int threads,
+                        kor_output *out, int64_t out_cap, int64_t *n_out) {
+    if (!codes || n_samples <= 0 || n_sites <= 0 || stride < n_sites || !out || !n_out || iterations == 0)
+        return KOR_EINVAL;
+    if (num_samples < 0) num_samples = n_samples;
+    if (num_samples == 0 || num_samples > n_samples) return KOR_EINVAL;
+    int64_t npairs = num_samples * (num_samples + 1) / 2;
+    if (out_cap < npairs) return KOR_EINVAL;
+    int64_t *site = (int64_t *)malloc(sizeof(int64_t) * (size_t)n_sites);
+    double *p = (double *)malloc(sizeof(double) * (size_t)n_sites);
+    double *q = (double *)malloc(sizeof(double) * (size_t)n_sites);
+    if (!site || !p || !q) { free(site); free(p); free(q); return KOR_ENOMEM; }
+    int64_t m = 0;
+    for (int64_t v = 0; v < n_sites; v++) {
+        int64_t refc = 0, altc = 0;
+        int complete = 1;
+        for (int64_t s = 0; s < n_samples; s++) {
+            const uint8_t g = codes[s * stride + v];
+            if (g > 2) { complete = 0; break; }
+            refc += 2 - g;
+            altc += g;
+        }
+        if (!complete) continue;
+        site[m] = v;
+        if (af_in) {
+            p[m] = af_in[2 * v];
+            q[m] = af_in[2 * v + 1];
+        } else {
+            const double tot = (double)(2 * n_samples);
+            p[m] = (double)refc / tot;
+            q[m] = (double)altc / tot;
+        }
+        m++;
+    }
+    if (m == 0) { free(site); free(p); free(q); return KOR_ENOSITES; }
+    /* the Gram matrix, upper triangle in the reference's row-major order */
+    double h[45] = {0};
+    for (int64_t k = 0; k < m; k++) {
+        for (int gx = 0; gx < 3; gx++)
+            for (int gy = 0; gy < 3; gy++) {
+                double row[9];
+                cls_row(gx, gy, p[k], q[k], row);
+                int a = 0;
+                for (int i = 0; i < 9; i++)
+                    for (int j = i; j < 9; j++) h[a++] += row[i] * row[j];
+            }
+    }
+    double Q[9][9];
+    {
+        int a = 0;
+        for (int i = 0; i < 9; i++)
+            for (int j = i; j < 9; j++) {
+                const double v = h[a++] / (double)m;
+                Q[i][j] = v;
+                Q[j][i] = v;
+            }
+    }
+    tune_t tu = make_tune(iterations);
+    tu.qp_max_iter = iterations;
+    double Q2[9][9] = {{0}};
+    Q2[0][0] = Q[0][0]; Q2[0][1] = Q[0][6];
+    Q2[1][0] = Q[6][0]; Q2[1][1] = Q[6][6];
+#ifdef _OPENMP
+    if (threads > 0) omp_set_num_threads(threads);
+#pragma omp parallel for schedule(dynamic, 1)
+#endif
+    for (int64_t x = 0; x < num_samples; x++) {
+        int64_t row0 = x * num_samples - x * (x - 1) / 2;
+        for (int64_t y = x; y < num_samples; y++) {
+            double c[9] = {0};
+            for (int64_t k = 0; k < m; k++) {
+                double row[9];
+                const int64_t v = site[k];
+                cls_row(codes[x * stride + v], codes[y * stride + v], p[k], q[k], row);
+                for (int i = 0; i < 9; i++) c[i] = c[i] + row[i];
+            }
+            for (int i = 0; i < 9; i++) c[i] = c[i] / (-(double)m);
+            double delta[9] = {0};
+            uint64_t its;
+            if (x == y) {
+                const double x0[9] = {0.5, 0.5};
+                const double c2[9] = {c[0], c[6]};
+                double d2[9] = {0};
+                its = qp_active_set_n(2, Q2, c2, x0, &tu, d2);
+                delta[0] = d2[0];
+                delta[6] = d2[1];
+            } else {
+                double x0[9];
+                for (int i = 0; i < 9; i++) x0[i] = 1.0 / 9.0;
+                its = qp_active_set_n(9, Q, c, x0, &tu, delta);
+            }
+            double qd[9];
+            matvec(9, Q, delta, qd);
+            const double quad = dotn(9, delta, qd);
+            const double lin = 2.0 * dotn(9, c, delta);
+            const double brier = (quad + lin) + 1.0;
+            double g[9];
+            for (int i = 0; i < 9; i++) g[i] = qd[i] + c[i];
+            kor_output *o = &out[row0 + (y - x)];
+            o->x = (uint64_t)x;
+            o->y = (uint64_t)y;
+            memcpy(o->jacquard, delta, sizeof delta);
+            o->obj = brier;
+            o->iters = its;
+            o->cond = condition_estimate(delta, g, Q, tu.sqp_conv_tol);
+        }
+    }
+    *n_out = npairs;
+    free(site); free(p); free(q);
     return KOR_OK;
 }

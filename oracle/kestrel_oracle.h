@@ -84,6 +84,14 @@ int kor_eval_pair(const uint8_t *codes_x, const uint8_t *codes_y, int64_t n_site
                   const double delta[9], double *f, double g[9], double h[81],
                   int64_t *n_sites_used);
 
+/* The reference's default hard-call estimator (-f GT): conditional least
+ * squares with the Brier objective (src/coefficients.rs:166-278).  Sites with a
+ * missing call in any sample are dropped; frequencies are counts over all
+ * samples (or af_in, n_sites x 2); rows as kor_relatedness, with obj = Brier
+ * score, iters = QP iterations.  The QP runs at most `iterations` iterations. */
+int kor_cls_relatedness(const uint8_t *codes, int64_t n_samples, int64_t n_sites, int64_t stride,
+                        const double *af_in, int64_t num_samples, uint64_t iterations, int threads,
+                        kor_output *out, int64_t out_cap, int64_t *n_out);
 /* Pass counters of the last kor_relatedness_pairs call on this thread group:
  * total grad/Hessian passes and objective passes summed over pairs. */
 void kor_pass_counts(uint64_t *gh_passes, uint64_t *obj_passes);

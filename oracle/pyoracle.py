@@ -50,8 +50,10 @@ def lib():
         L.kor_eval_pair.argtypes = [P, P, i64, P, P, P, P, P, P, P, ctypes.POINTER(i64)]
         L.kor_allele_counts.argtypes = [P, i64, i64, i64, P, P]
         L.kor_pass_counts.argtypes = [ctypes.POINTER(u64), ctypes.POINTER(u64)]
+        L.kor_cls_relatedness.argtypes = [P, i64, i64, i64, P, i64, u64, ctypes.c_int, P, i64,
+                                          ctypes.POINTER(i64)]
         for f in ("kor_site_frequencies", "kor_relatedness", "kor_relatedness_pairs",
-                  "kor_eval_pair", "kor_allele_counts"):
+                  "kor_eval_pair", "kor_allele_counts", "kor_cls_relatedness"):
             getattr(L, f).restype = ctypes.c_int
         L.kor_pass_counts.restype = None
         _lib = L
@@ -107,6 +109,23 @@ def relatedness(codes, af=None, num_samples=None, iterations=100, maf=None, thre
                                _ptr(out), out.size, ctypes.byref(nout))
     if st:
         raise RuntimeError(f"kor_relatedness failed: {st}")
+    return out
+
+
+def cls_relatedness(codes, af=None, num_samples=None, iterations=100, threads=0):
+    """The reference's default hard-call estimator (conditional least squares,
+    Brier objective): rows as `relatedness`, obj = Brier score, iters = QP
+    iterations."""
+    codes = _codes(codes)
+    n, m = codes.shape
+    ns = n if num_samples is None else num_samples
+    out = np.zeros(ns * (ns + 1) // 2, OUTPUT_DTYPE)
+    nout = ctypes.c_int64()
+    afa = None if af is None else np.ascontiguousarray(af, dtype=np.float64)
+    st = lib().kor_cls_relatedness(_ptr(codes), n, m, m, _ptr(afa), ns, iterations, threads,
+                                   _ptr(out), out.size, ctypes.byref(nout))
+    if st:
+        raise RuntimeError(f"kor_cls_relatedness failed: {st}")
     return out
 
 

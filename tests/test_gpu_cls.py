@@ -1,0 +1,85 @@
+"""GPU parity of the CLS/Brier hard-call estimator (kg_relatedness_gt, the
+reference's default -f GT path, src/coefficients.rs:166-278) against the FP64
+oracle.  Same bar as the ML path: Delta and kinship within 1e-5 absolute for
+identifiable pairs (oracle log10 cond <= 4), the Brier objective within 1e-6
+relative, the condition flag equal below log10 cond 15."""
+import numpy as np
+import pytest
+
+import kestrel_b200 as kb
+from kestrel_b200 import synth
+
+from .parity import compare
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def est():
+    e = kb.Estimator()
+    yield e
+    e.close()
+
+
+@pytest.fixture(scope="module")
+def complete():
+    return synth.make_cohort(64, 10_000, 21, missing=0.0,
+                             planted={"parent_offspring": 4, "full_sib": 4, "half_sib": 4,
+                                      "first_cousin": 4}, name="cls")
+
+
+@pytest.mark.parametrize("precision", ["fp32c", "fp64"])
+def test_cls_parity(est, oracle, complete, precision):
+    ref = oracle.cls_relatedness(complete.codes)
+    est.set_precision(precision)
+    est.load(complete.codes)
+    gpu = est.relatedness_gt()
+    est.set_precision("fp32c")
+    stats = compare(gpu, ref)
+    same_iters = float(np.mean(gpu["iters"] == ref["iters"]))
+    print(precision, stats, "same QP iterations", same_iters)
+    assert same_iters > 0.95
+    s = gpu[gpu["x"] == gpu["y"]]["jacquard"]
+    assert np.allclose(s[:, 0] + s[:, 6], 1.0, atol=1e-9)
+    assert np.all(s[:, [1, 2, 3, 4, 5, 7, 8]] == 0.0)
+
+
+def test_cls_drops_incomplete_sites(est, oracle):
+    c = synth.make_cohort(48, 20_000, 22, missing=0.0005, name="cls-miss")
+    complete_sites = int(np.all(c.codes < 3, 0).sum())
+    assert 0 < complete_sites < c.codes.shape[1]
+    ref = oracle.cls_relatedness(c.codes)
+    est.load(c.codes)
+    gpu = est.relatedness_gt()
+    compare(gpu, ref)
+
+
+def test_cls_supplied_frequencies_and_subset(est, oracle, complete):
+    codes = complete.codes
+    n = codes.shape[0]
+    rng = np.random.default_rng(4)
+    p = np.clip(rng.uniform(0.05, 0.95, codes.shape[1]), 0.05, 0.95)
+    af = np.stack([p, 1.0 - p], 1)
+    ref = oracle.cls_relatedness(codes, af=af, num_samples=40)
+    est.load(codes, allele_frequencies=af)
+    gpu = est.relatedness_gt(num_samples=40)
+    compare(gpu, ref)
+    est.load(codes)
+
+
+def test_cls_iteration_cap(est, oracle, complete):
+    ref = oracle.cls_relatedness(complete.codes, iterations=3)
+    est.load(complete.codes)
+    gpu = est.relatedness_gt(iterations=3)
+    assert gpu["iters"].max() <= 3
+    assert np.mean(gpu["iters"] == ref["iters"]) > 0.95
+
+
+def test_cls_no_complete_site(est):
+    codes = np.ones((8, 64), np.uint8)
+    codes[np.arange(8), np.arange(8)] = synth.MISSING
+    codes[:, 8:] = synth.MISSING
+    est.load(codes)
+    with pytest.raises(kb.KestrelError) as e:
+        est.relatedness_gt()
+    assert e.value.status == kb.KG_ENOSITES
