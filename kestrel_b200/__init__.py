@@ -248,16 +248,25 @@ class Estimator:
         return {"requests": r.value, "pairs": p.value, "launches": l_.value}
 
 
-def relatedness_coefficients_gt(genotypes, allele_frequencies=None, threads=None, iterations=100):
+def relatedness_coefficients_gt(genotypes, allele_frequencies=None, threads=None, iterations=100,
+                                estimator="ml"):
     """Jacquard, kinship and inbreeding for every pair of samples from hard
     calls (the reference's signature, src/lib.rs:46-70).  genotypes: u8/int
     [variants, samples, 2] allele indices; allele_frequencies: f64 [variants, 2]
-    ([REF, ALT]) or None to estimate.  `threads` is accepted and unused."""
+    ([REF, ALT]) or None to estimate.  `threads` is accepted and unused.
+    estimator "ml" runs the maximum-likelihood estimator on the calls; "cls"
+    runs the reference's own hard-call estimator (conditional least squares
+    with the Brier objective, src/coefficients.rs:166-278)."""
     del threads
+    if estimator not in ("ml", "cls"):
+        raise ValueError("estimator must be 'ml' or 'cls'")
     codes = genotype_codes(genotypes)
     with Estimator() as est:
         est.load(codes, allele_frequencies)
-        rows = est.relatedness(iterations=iterations)
+        if estimator == "cls":
+            rows = est.relatedness_gt(iterations=iterations)
+        else:
+            rows = est.relatedness(iterations=iterations)
     return Coefficients(*build_arrays(rows, codes.shape[0]))
 
 

@@ -31,6 +31,7 @@ struct Options {
     uint64_t iterations = 100;
     double maf = NAN;
     int64_t samples = -1;
+    bool cls = false;  // --estimator cls: the reference's default GT estimator (CLS/Brier)
 };
 
 void log_info(const char* fmt, const std::string& a = "") {
@@ -49,7 +50,9 @@ int usage(const char* why) {
                  "  -t, --threads <THREADS>             accepted, unused on the GPU\n"
                  "  -i, --iterations <ITERATIONS>       [default: 100]\n"
                  "  -m, --minimum-allele-frequency <F>\n"
-                 "  -s, --samples <N>\n",
+                 "  -s, --samples <N>\n"
+                 "  -e, --estimator <ml|cls>            [default: ml; cls = conditional least squares\n"
+                 "                                       with the Brier objective, GT only]\n",
                  why);
     return 2;
 }
@@ -93,6 +96,11 @@ bool parse_args(int argc, const char* const* argv, Options& o, std::string& why)
         } else if (is("-m", "--minimum-allele-frequency")) {
             if (!val(v)) { why = "missing value for -m"; return false; }
             o.maf = std::atof(v.c_str());
+        } else if (is("-e", "--estimator")) {
+            if (!val(v)) { why = "missing value for -e"; return false; }
+            if (v == "ml") o.cls = false;
+            else if (v == "cls") o.cls = true;
+            else { why = "invalid value '" + v + "' for --estimator"; return false; }
         } else if (is("-s", "--samples")) {
             if (!val(v)) { why = "missing value for -s"; return false; }
             o.samples = std::atoll(v.c_str());
@@ -112,6 +120,10 @@ bool parse_args(int argc, const char* const* argv, Options& o, std::string& why)
     }
     o.input = pos[0];
     o.output = pos[1];
+    if (o.cls && o.field != 'T') {
+        why = "--estimator cls needs hard calls (-f GT)";
+        return false;
+    }
     return true;
 }
 
@@ -358,7 +370,10 @@ extern "C" int kg_run_cli(int argc, const char* const* argv) {
     st = kg_load_genotypes(ctx, codes.data(), ns, nv, nv);
     if (!st && o.af_info) st = kg_set_allele_frequencies(ctx, af.data());
     int64_t nout = 0;
-    if (!st) st = kg_relatedness(ctx, nsel, o.iterations, o.maf, out.data(), np, &nout);
+    if (!st) {
+        if (o.cls) st = kg_relatedness_gt(ctx, nsel, o.iterations, out.data(), np, &nout);
+        else st = kg_relatedness(ctx, nsel, o.iterations, o.maf, out.data(), np, &nout);
+    }
     if (st) {
         std::fprintf(stderr, "Error: %s\n", kg_last_error(ctx));
         kg_destroy(ctx);

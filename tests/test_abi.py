@@ -53,3 +53,8 @@ def test_null_context_is_einval(L):
 def test_cli_usage_error_without_gpu(L):
     argv = (ctypes.c_char_p * 2)(b"kestrel", b"--bogus")
     assert L.kg_run_cli(2, argv) == 2
+
+
+def test_cli_cls_needs_hard_calls(L):
+    argv = (ctypes.c_char_p * 7)(b"kestrel", b"in.vcf", b"out.tsv", b"-f", b"PL", b"-e", b"cls")
+    assert L.kg_run_cli(7, argv) == 2

@@ -130,6 +130,27 @@ def test_cli_gt_and_pl_match_oracle(oracle):
     assert [r[0] for r in rows[:2]] == ["S0", "S0"] and [r[1] for r in rows[:2]] == ["S0", "S1"]
 
 
+def test_cli_cls_estimator_matches_oracle(oracle):
+    co = synth.make_cohort(24, 2500, seed=43, missing=0.0, planted={"parent_offspring": 2})
+    cli = os.path.join(os.path.dirname(kb.__file__), "bin", "kestrel")
+    ref = oracle.cls_relatedness(co.codes, num_samples=20)
+    with tempfile.TemporaryDirectory() as td:
+        vcf = os.path.join(td, "in.vcf")
+        tsv = os.path.join(td, "out.tsv")
+        synth.write_vcf(vcf, co.codes, field="GT")
+        r = subprocess.run([cli, vcf, tsv, "-f", "GT", "-e", "cls", "-s", "20"], capture_output=True,
+                           text=True, timeout=300)
+        assert r.returncode == 0, r.stderr
+        head, rows = _read_tsv(tsv)
+    assert len(rows) == len(ref)
+    jac = np.array([[float(v) for v in r[3:12]] for r in rows])
+    obj = np.array([float(r[13]) for r in rows])
+    lc_ref = np.log10(ref["cond"])
+    ident = np.isfinite(lc_ref) & (lc_ref <= 4)
+    assert np.abs(jac - ref["jacquard"]).max(1)[ident].max() <= 1e-5
+    assert (np.abs(obj - ref["obj"]) / np.abs(ref["obj"])).max() <= 1e-6
+
+
 def test_autotune_and_launch_shape_leave_results_unchanged():
     co = synth.make_cohort(48, 4000, seed=51)
     with kb.Estimator() as est:
