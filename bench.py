@@ -542,8 +542,8 @@ def main():
 
 
 # DRAM bytes (read + write) per pair-site-pass of wave_pass_kernel, measured by
-# ncu (profiles/wave_pass_kernel_N96_M100k.md): 1.959 GB over 447,339,158.
-PASS_DRAM_BYTES_PER_SITE = 4.38
+# ncu (profiles/wave_pass_kernel_N96_M100k.md): 1.911 GB over 447,339,158.
+PASS_DRAM_BYTES_PER_SITE = 4.27
 
 
 def ctypes_peak(device):
