@@ -265,6 +265,32 @@ int kg_fp32_peak(int device, double *tflops);
  * src/cli.rs:12-127) in-process; argv[0] is the program name. */
 int kg_run_cli(int argc, const char *const *argv);
 
+/* ------------------------------------------------------------ VCF reader */
+
+/* The VCF reader the CLI uses, replacing the reference's parse_vcf with the GT
+ * and GL/PL sample parsers (src/vcf.rs:96-236, :384-421): biallelic SNP
+ * records of a plain, gzip or bgzip VCF become genotype codes (0/1/2, 3 =
+ * missing).  Records whose REF or ALT is not a single base, or with more than
+ * one ALT, are skipped and counted; GL/PL rows reduce to the most likely
+ * genotype.  BGZF blocks are inflated and the records parsed on `threads` host
+ * threads (<= 0: all).  field is "GT", "GL" or "PL"; af_info != 0 also reads
+ * INFO/AF (the reference's -a info).  *out is always set when memory allows;
+ * on failure kg_vcf_error() gives the message (the first bad record in file
+ * order).  Free with kg_vcf_free. */
+typedef struct kg_vcf kg_vcf;
+int kg_vcf_read(const char *path, const char *field, int af_info, int threads, kg_vcf **out);
+const char *kg_vcf_error(const kg_vcf *vcf);
+/* counts (optional, 4 entries): records, non-SNP records skipped,
+ * multi-allelic records skipped, GL/PL rows that were not one-hot. */
+int kg_vcf_info(const kg_vcf *vcf, int64_t *n_samples, int64_t *n_sites, uint64_t *counts);
+/* codes: n_samples x n_sites, sample-major (the layout kg_load_genotypes takes);
+ * af: n_sites x 2 [REF, ALT] from INFO/AF (KG_EINVAL if it was not read).
+ * Either may be NULL. */
+int kg_vcf_codes(const kg_vcf *vcf, uint8_t *codes, double *af);
+/* Sample name i (NULL when out of range). */
+const char *kg_vcf_sample(const kg_vcf *vcf, int64_t i);
+void kg_vcf_free(kg_vcf *vcf);
+
 #ifdef __cplusplus
 }
 #endif

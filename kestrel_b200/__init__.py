@@ -9,6 +9,7 @@ panel) of include/kestrel_gpu.h.
 from __future__ import annotations
 
 import ctypes
+import os
 import sys
 import warnings
 
@@ -17,7 +18,7 @@ import numpy as np
 from ._lib import (KG_ENOSITES, KG_ETIMEOUT, KG_OK, KG_PREC_FP32C, KG_PREC_FP64, MISSING,
                    OUTPUT_DTYPE, KestrelError, KgCohort, KgRunStats, lib, ptr)
 
-__all__ = ["Coefficients", "relatedness_coefficients_gt", "relatedness_coefficients_gl",
+__all__ = ["Coefficients", "relatedness_coefficients_gt", "relatedness_coefficients_gl", "read_vcf",
            "run_cli", "Estimator", "genotype_codes", "build_arrays", "KestrelError",
            "OUTPUT_DTYPE", "MISSING", "KINSHIP_VECTOR"]
 
@@ -268,6 +269,40 @@ def relatedness_coefficients_gt(genotypes, allele_frequencies=None, threads=None
         else:
             rows = est.relatedness(iterations=iterations)
     return Coefficients(*build_arrays(rows, codes.shape[0]))
+
+
+def read_vcf(path, field: str = "GT", allele_freqs: str = "estimate", threads: int = 0):
+    """Reads a plain, gzip or bgzip VCF with the library's multithreaded reader
+    (the CLI's): biallelic SNP records become genotype codes.  Returns
+    (codes u8 [samples, sites], allele_frequencies f64 [sites, 2] or None,
+    sample names, counts dict).  allele_freqs "info" reads INFO/AF."""
+    if allele_freqs not in ("estimate", "info"):
+        raise ValueError("allele_freqs must be 'estimate' or 'info'")
+    L = lib()
+    h = ctypes.c_void_p()
+    st = L.kg_vcf_read(os.fsencode(path), field.encode(), 1 if allele_freqs == "info" else 0, int(threads),
+                       ctypes.byref(h))
+    try:
+        if st != KG_OK:
+            msg = L.kg_vcf_error(h) if h.value else b"out of memory"
+            raise KestrelError(st, msg.decode())
+        ns, nv = ctypes.c_int64(), ctypes.c_int64()
+        counts = (ctypes.c_uint64 * 4)()
+        _check_vcf(L.kg_vcf_info(h, ctypes.byref(ns), ctypes.byref(nv), counts), L, h)
+        codes = np.empty((ns.value, nv.value), np.uint8)
+        af = np.empty((nv.value, 2)) if allele_freqs == "info" else None
+        _check_vcf(L.kg_vcf_codes(h, ptr(codes), ptr(af)), L, h)
+        names = [L.kg_vcf_sample(h, i).decode() for i in range(ns.value)]
+        return codes, af, names, {"records": counts[0], "not_snp": counts[1], "multiallelic": counts[2],
+                                  "soft_likelihoods": counts[3]}
+    finally:
+        if h.value:
+            L.kg_vcf_free(h)
+
+
+def _check_vcf(st, L, h):
+    if st != KG_OK:
+        raise KestrelError(st, L.kg_vcf_error(h).decode())
 
 
 def relatedness_coefficients_gl(genotype_likelihoods, allele_frequencies=None, threads=None,

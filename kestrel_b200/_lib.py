@@ -59,7 +59,8 @@ EXPORTS = ("kg_create", "kg_destroy", "kg_last_error", "kg_version", "kg_set_pre
            "kg_set_allele_frequencies", "kg_relatedness", "kg_relatedness_gt", "kg_relatedness_coefficients",
            "kg_relatedness_batch", "kg_panel_load", "kg_submit", "kg_poll", "kg_wait",
            "kg_cancel", "kg_serving_stats", "kg_relatedness_noalloc", "kg_last_run_stats",
-           "kg_fp32_peak", "kg_run_cli")
+           "kg_fp32_peak", "kg_run_cli", "kg_vcf_read", "kg_vcf_error", "kg_vcf_info", "kg_vcf_codes",
+           "kg_vcf_sample", "kg_vcf_free")
 
 
 class KestrelError(RuntimeError):
@@ -106,6 +107,12 @@ def lib():
         "kg_relatedness_noalloc": ([P, i64, i64, i64, u64, dbl, P, i64, P], i32),
         "kg_fp32_peak": ([i32, ctypes.POINTER(dbl)], i32),
         "kg_run_cli": ([i32, ctypes.POINTER(ctypes.c_char_p)], i32),
+        "kg_vcf_read": ([ctypes.c_char_p, ctypes.c_char_p, i32, i32, ctypes.POINTER(P)], i32),
+        "kg_vcf_error": ([P], ctypes.c_char_p),
+        "kg_vcf_info": ([P, ctypes.POINTER(i64), ctypes.POINTER(i64), P], i32),
+        "kg_vcf_codes": ([P, P, P], i32),
+        "kg_vcf_sample": ([P, i64], ctypes.c_char_p),
+        "kg_vcf_free": ([P], None),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)

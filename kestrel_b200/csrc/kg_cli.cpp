@@ -10,7 +10,7 @@
 // dropped per pair, as the reference's NaN likelihood rows are
 // (src/vcf.rs:355,397; src/lanevector.rs:99-104).  Only biallelic SNPs are
 // estimated; tri- and tetra-allelic SNPs are counted and skipped.
-#include <zlib.h>
+#include "kg_vcf.h"
 
 #include <charconv>
 #include <chrono>
@@ -32,6 +32,7 @@ struct Options {
     double maf = NAN;
     int64_t samples = -1;
     bool cls = false;  // --estimator cls: the reference's default GT estimator (CLS/Brier)
+    int threads = 0;   // VCF reader threads (0 = all)
 };
 
 void log_info(const char* fmt, const std::string& a = "") {
@@ -47,7 +48,7 @@ int usage(const char* why) {
                  "  <OUTPUT>  Tab-separated file to write the coefficients to\n\n"
                  "Options:\n  -a, --allele-freqs <estimate|info>  [default: estimate]\n"
                  "  -f, --field <GT|GL|PL>              [default: GT]\n"
-                 "  -t, --threads <THREADS>             accepted, unused on the GPU\n"
+                 "  -t, --threads <THREADS>             VCF reader threads [default: all]\n"
                  "  -i, --iterations <ITERATIONS>       [default: 100]\n"
                  "  -m, --minimum-allele-frequency <F>\n"
                  "  -s, --samples <N>\n"
@@ -88,6 +89,7 @@ bool parse_args(int argc, const char* const* argv, Options& o, std::string& why)
             else { why = "invalid value '" + v + "' for --field"; return false; }
         } else if (is("-t", "--threads")) {
             if (!val(v) || std::atol(v.c_str()) <= 0) { why = "threads must be a positive integer"; return false; }
+            o.threads = (int)std::atol(v.c_str());
         } else if (is("-i", "--iterations")) {
             if (!val(v)) { why = "missing value for -i"; return false; }
             long long n = std::atoll(v.c_str());
@@ -124,108 +126,6 @@ bool parse_args(int argc, const char* const* argv, Options& o, std::string& why)
         why = "--estimator cls needs hard calls (-f GT)";
         return false;
     }
-    return true;
-}
-
-// Line reader over plain or gzip-compressed text.
-struct LineReader {
-    gzFile f = nullptr;
-    std::vector<char> buf;
-    explicit LineReader(const std::string& path) { f = gzopen(path.c_str(), "rb"); buf.resize(1 << 20); }
-    ~LineReader() { if (f) gzclose(f); }
-    bool ok() const { return f != nullptr; }
-    bool next(std::string& line) {
-        line.clear();
-        for (;;) {
-            if (!gzgets(f, buf.data(), (int)buf.size())) return !line.empty();
-            size_t n = std::strlen(buf.data());
-            line.append(buf.data(), n);
-            if (n && buf[n - 1] == '\n') {
-                line.pop_back();
-                if (!line.empty() && line.back() == '\r') line.pop_back();
-                return true;
-            }
-        }
-    }
-};
-
-void split(const std::string& s, char sep, std::vector<std::string_view>& out) {
-    out.clear();
-    size_t b = 0;
-    for (size_t i = 0; i <= s.size(); i++) {
-        if (i == s.size() || s[i] == sep) {
-            out.emplace_back(s.data() + b, i - b);
-            b = i + 1;
-        }
-    }
-}
-
-void split_sv(std::string_view s, char sep, std::vector<std::string_view>& out) {
-    out.clear();
-    size_t b = 0;
-    for (size_t i = 0; i <= s.size(); i++) {
-        if (i == s.size() || s[i] == sep) {
-            out.emplace_back(s.data() + b, i - b);
-            b = i + 1;
-        }
-    }
-}
-
-bool is_base(std::string_view b) {
-    return b.size() == 1 && std::strchr("ACGTacgt", b[0]) != nullptr;
-}
-
-// Genotype code of one sample's FORMAT value; false on a malformed entry.
-bool parse_call(std::string_view v, char field, uint8_t& code, uint64_t& soft) {
-    std::vector<std::string_view> parts;
-    if (field == 'T') {
-        // alleles separated by / or |
-        int a[2];
-        int k = 0;
-        size_t b = 0;
-        bool missing = false;
-        for (size_t i = 0; i <= v.size(); i++) {
-            if (i == v.size() || v[i] == '/' || v[i] == '|') {
-                std::string_view t = v.substr(b, i - b);
-                if (k >= 2) return false;
-                if (t == ".") {
-                    missing = true;
-                    a[k++] = 0;
-                } else {
-                    int x = 0;
-                    auto r = std::from_chars(t.data(), t.data() + t.size(), x);
-                    if (r.ec != std::errc() || x < 0 || x > 1) return false;
-                    a[k++] = x;
-                }
-                b = i + 1;
-            }
-        }
-        if (missing) { code = 3; return true; }
-        if (k != 2) return false;
-        code = (uint8_t)(a[0] + a[1]);
-        return true;
-    }
-    split_sv(v, ',', parts);
-    if (parts.size() == 1 && parts[0] == ".") { code = 3; return true; }
-    if (parts.size() != 3) return false;
-    double val[3];
-    bool any_missing = false;
-    for (int i = 0; i < 3; i++) {
-        if (parts[i] == ".") { any_missing = true; val[i] = 0; continue; }
-        std::string t(parts[i]);
-        char* end = nullptr;
-        val[i] = std::strtod(t.c_str(), &end);
-        if (end == t.c_str()) return false;
-    }
-    if (any_missing) { code = 3; return true; }
-    // likelihood scale: PL = -10 log10 L, GL = log10 L
-    double ll[3];
-    for (int i = 0; i < 3; i++) ll[i] = (field == 'P') ? -val[i] / 10.0 : val[i];
-    int best = 0;
-    for (int i = 1; i < 3; i++) if (ll[i] > ll[best]) best = i;
-    for (int i = 0; i < 3; i++)
-        if (i != best && ll[best] - ll[i] < 25.5 - 1e-9) { soft++; break; }
-    code = (uint8_t)best;
     return true;
 }
 
@@ -274,85 +174,27 @@ extern "C" int kg_run_cli(int argc, const char* const* argv) {
     if (!parse_args(argc, argv, o, why)) return usage(why.c_str());
     log_info("Kestrel %s", kg_version());
     log_info("Parsing VCF \"%s\"", o.input);
-    LineReader rd(o.input);
-    if (!rd.ok()) {
-        std::fprintf(stderr, "Error: cannot open %s\n", o.input.c_str());
+    kg::VcfData vcf;
+    std::string err;
+    if (kg::read_vcf(o.input, o.field, o.af_info, o.threads, vcf, err)) {
+        std::fprintf(stderr, "Error: %s\n", err.c_str());
         return 1;
     }
-    std::string line;
-    std::vector<std::string> samples;
-    std::vector<std::string_view> cols, fmt;
-    std::vector<std::vector<uint8_t>> sites;  // per site, codes per sample
-    std::vector<double> af;
-    uint64_t total = 0, not_snp = 0, multi = 0, soft = 0;
-    const char* key = o.field == 'T' ? "GT" : (o.field == 'P' ? "PL" : "GL");
-    while (rd.next(line)) {
-        if (line.rfind("##", 0) == 0) continue;
-        if (line.rfind("#CHROM", 0) == 0) {
-            split(line, '\t', cols);
-            for (size_t i = 9; i < cols.size(); i++) samples.emplace_back(cols[i]);
-            continue;
-        }
-        if (line.empty()) continue;
-        total++;
-        split(line, '\t', cols);
-        if (cols.size() < 9 + samples.size() || samples.empty()) {
-            std::fprintf(stderr, "Error: malformed record %llu\n", (unsigned long long)total);
-            return 1;
-        }
-        std::vector<std::string_view> alts;
-        split_sv(cols[4], ',', alts);
-        bool snp = is_base(cols[3]);
-        for (auto& a : alts) snp = snp && is_base(a);
-        if (!snp) { not_snp++; continue; }
-        if (alts.size() != 1) { multi++; continue; }
-        split_sv(cols[8], ':', fmt);
-        int fi = -1;
-        for (size_t i = 0; i < fmt.size(); i++) if (fmt[i] == key) fi = (int)i;
-        if (fi < 0) {
-            std::fprintf(stderr, "Error: No %s data found\n", key);
-            return 1;
-        }
-        std::vector<uint8_t> row(samples.size());
-        std::vector<std::string_view> sub;
-        for (size_t s = 0; s < samples.size(); s++) {
-            split_sv(cols[9 + s], ':', sub);
-            std::string_view v = (fi < (int)sub.size()) ? sub[fi] : std::string_view(".");
-            if (!parse_call(v, o.field, row[s], soft)) {
-                std::fprintf(stderr, "Error: Value %.*s is not a valid %s\n", (int)v.size(), v.data(), key);
-                return 1;
-            }
-        }
-        if (o.af_info) {
-            std::vector<std::string_view> info;
-            split_sv(cols[7], ';', info);
-            double a = NAN;
-            for (auto& kv : info)
-                if (kv.rfind("AF=", 0) == 0) a = std::strtod(std::string(kv.substr(3)).c_str(), nullptr);
-            if (std::isnan(a)) {
-                std::fprintf(stderr, "Error: No AF info found\n");
-                return 1;
-            }
-            double alt = std::min(std::max(a, 0.0), 1.0);
-            af.push_back(1.0 - alt);
-            af.push_back(a);
-        }
-        sites.push_back(std::move(row));
-    }
-    log_info("Parsed %s total sites", std::to_string(total));
-    log_info("Skipped %s sites that were not SNPs", std::to_string(not_snp));
-    log_info("Skipped %s tri- or tetra-allelic sites (biallelic sites only)", std::to_string(multi));
-    log_info("Found %s di-allelic sites", std::to_string(sites.size()));
-    if (soft) log_info("%s likelihood entries were not one-hot; their most likely genotype was used", std::to_string(soft));
-    const int64_t ns = (int64_t)samples.size(), nv = (int64_t)sites.size();
+    log_info("Parsed %s total sites", std::to_string(vcf.total));
+    log_info("Skipped %s sites that were not SNPs", std::to_string(vcf.not_snp));
+    log_info("Skipped %s tri- or tetra-allelic sites (biallelic sites only)", std::to_string(vcf.multi));
+    log_info("Found %s di-allelic sites", std::to_string(vcf.n_sites));
+    if (vcf.soft)
+        log_info("%s likelihood entries were not one-hot; their most likely genotype was used",
+                 std::to_string(vcf.soft));
+    const std::vector<std::string>& samples = vcf.samples;
+    const std::vector<double>& af = vcf.af;
+    const int64_t ns = (int64_t)samples.size(), nv = vcf.n_sites;
     if (nv == 0 || ns == 0) {
         std::fprintf(stderr, "Error: Must have at least one site and one sample\n");
         return 1;
     }
-    std::vector<uint8_t> codes((size_t)(ns * nv));
-    for (int64_t v = 0; v < nv; v++)
-        for (int64_t s = 0; s < ns; s++) codes[(size_t)(s * nv + v)] = sites[v][s];
-    sites.clear();
+    const std::vector<uint8_t>& codes = vcf.codes;
     int64_t nsel = o.samples < 0 ? ns : o.samples;
     if (nsel > ns) {
         std::fprintf(stderr, "Error: Requested samples %lld exceeds total samples %lld\n", (long long)nsel, (long long)ns);

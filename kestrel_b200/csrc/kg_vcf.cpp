@@ -1,0 +1,538 @@
+// kg_vcf.cpp — multithreaded VCF reader (see kg_vcf.h).
+#include "kg_vcf.h"
+
+#include <zlib.h>
+
+#include <new>
+#include <stdexcept>
+
+#include "kestrel_gpu.h"
+
+#include <algorithm>
+#include <charconv>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string_view>
+#include <thread>
+
+namespace kg {
+namespace {
+
+template <class F>
+void parallel_for(int n_threads, int64_t n, F&& f) {
+    if (n <= 0) return;
+    const int t = (int)std::max<int64_t>(1, std::min<int64_t>(n_threads, n));
+    if (t == 1) {
+        f(0, (int64_t)0, n);
+        return;
+    }
+    std::vector<std::thread> pool;
+    for (int i = 0; i < t; i++) {
+        const int64_t b = n * i / t, e = n * (i + 1) / t;
+        pool.emplace_back([&f, i, b, e] { f(i, b, e); });
+    }
+    for (auto& th : pool) th.join();
+}
+
+bool read_file(const std::string& path, std::vector<char>& buf, std::string& err) {
+    FILE* f = std::fopen(path.c_str(), "rb");
+    if (!f) {
+        err = "cannot open " + path;
+        return false;
+    }
+    std::fseek(f, 0, SEEK_END);
+    const long long n = ftello(f);
+    std::fseek(f, 0, SEEK_SET);
+    if (n < 0) {
+        std::fclose(f);
+        err = "cannot read " + path;
+        return false;
+    }
+    buf.resize((size_t)n);
+    const size_t got = n ? std::fread(buf.data(), 1, (size_t)n, f) : 0;
+    std::fclose(f);
+    if (got != (size_t)n) {
+        err = "cannot read " + path;
+        return false;
+    }
+    return true;
+}
+
+// BGZF (RFC 1952 members with a 'BC' extra subfield holding the block size
+// minus one): the members' starts and uncompressed sizes, or false if any
+// member is not BGZF.
+bool bgzf_blocks(const std::vector<char>& b, std::vector<size_t>& start, std::vector<size_t>& clen,
+                 std::vector<uint32_t>& isize, std::vector<size_t>& hlen) {
+    size_t p = 0;
+    while (p < b.size()) {
+        if (p + 18 > b.size()) return false;
+        const uint8_t* h = reinterpret_cast<const uint8_t*>(b.data() + p);
+        if (h[0] != 0x1f || h[1] != 0x8b || h[2] != 8 || !(h[3] & 4)) return false;
+        const size_t xlen = (size_t)h[10] | ((size_t)h[11] << 8);
+        size_t q = p + 12;
+        const size_t qe = q + xlen;
+        if (qe > b.size()) return false;
+        long bsize = -1;
+        while (q + 4 <= qe) {
+            const uint8_t* s = reinterpret_cast<const uint8_t*>(b.data() + q);
+            const size_t slen = (size_t)s[2] | ((size_t)s[3] << 8);
+            if (s[0] == 'B' && s[1] == 'C' && slen == 2 && q + 6 <= qe) bsize = (long)s[4] | ((long)s[5] << 8);
+            q += 4 + slen;
+        }
+        if (bsize < 0) return false;
+        const size_t total = (size_t)bsize + 1;
+        if (p + total > b.size() || total < 12 + xlen + 8) return false;
+        const uint8_t* t = reinterpret_cast<const uint8_t*>(b.data() + p + total - 4);
+        start.push_back(p);
+        hlen.push_back(12 + xlen);
+        clen.push_back(total - 12 - xlen - 8);
+        isize.push_back((uint32_t)t[0] | ((uint32_t)t[1] << 8) | ((uint32_t)t[2] << 16) | ((uint32_t)t[3] << 24));
+        p += total;
+    }
+    return true;
+}
+
+bool inflate_raw(const char* src, size_t n, char* dst, size_t dn) {
+    char dummy[1];
+    z_stream zs{};
+    if (inflateInit2(&zs, -15) != Z_OK) return false;
+    zs.next_in = reinterpret_cast<Bytef*>(const_cast<char*>(src));
+    zs.avail_in = (uInt)n;
+    zs.next_out = reinterpret_cast<Bytef*>(dn ? dst : dummy);
+    zs.avail_out = (uInt)(dn ? dn : 1);
+    const int r = inflate(&zs, Z_FINISH);
+    const bool ok = r == Z_STREAM_END && zs.total_out == dn;
+    inflateEnd(&zs);
+    return ok;
+}
+
+bool gunzip_stream(const std::string& path, std::vector<char>& text, std::string& err) {
+    gzFile f = gzopen(path.c_str(), "rb");
+    if (!f) {
+        err = "cannot open " + path;
+        return false;
+    }
+    gzbuffer(f, 1 << 20);
+    const size_t step = (size_t)16 << 20;
+    size_t used = 0;
+    for (;;) {
+        text.resize(used + step);
+        const int r = gzread(f, text.data() + used, (unsigned)step);
+        if (r < 0) {
+            gzclose(f);
+            err = "cannot decompress " + path;
+            return false;
+        }
+        used += (size_t)r;
+        if ((size_t)r < step) break;
+    }
+    text.resize(used);
+    gzclose(f);
+    return true;
+}
+
+// The file's text: plain, BGZF (blocks inflated in parallel) or plain gzip.
+bool load_text(const std::string& path, int threads, std::vector<char>& text, std::string& err) {
+    std::vector<char> raw;
+    if (!read_file(path, raw, err)) return false;
+    if (raw.size() < 2 || (uint8_t)raw[0] != 0x1f || (uint8_t)raw[1] != 0x8b) {
+        text.swap(raw);
+        return true;
+    }
+    std::vector<size_t> st, cl, hl;
+    std::vector<uint32_t> is;
+    if (!bgzf_blocks(raw, st, cl, is, hl)) return gunzip_stream(path, text, err);
+    std::vector<size_t> off(st.size() + 1, 0);
+    for (size_t i = 0; i < st.size(); i++) off[i + 1] = off[i] + is[i];
+    text.resize(off.back());
+    std::vector<char> bad((size_t)std::max(1, threads), 0);
+    parallel_for(threads, (int64_t)st.size(), [&](int t, int64_t b, int64_t e) {
+        for (int64_t i = b; i < e; i++)
+            if (!inflate_raw(raw.data() + st[i] + hl[i], cl[i], text.data() + off[i], is[i])) bad[t] = 1;
+    });
+    if (std::find(bad.begin(), bad.end(), 1) != bad.end()) {
+        err = "cannot decompress " + path;
+        return false;
+    }
+    return true;
+}
+
+bool is_base(std::string_view b) { return b.size() == 1 && std::strchr("ACGTacgt", b[0]) != nullptr; }
+
+// Genotype code of one sample's value of the FORMAT key; false if malformed.
+bool parse_call(std::string_view v, char field, uint8_t& code, uint64_t& soft) {
+    if (field == 'T') {
+        int a[2] = {0, 0};
+        int k = 0;
+        size_t b = 0;
+        bool missing = false;
+        for (size_t i = 0; i <= v.size(); i++) {
+            if (i == v.size() || v[i] == '/' || v[i] == '|') {
+                const std::string_view t = v.substr(b, i - b);
+                if (k >= 2) return false;
+                if (t == ".") {
+                    missing = true;
+                    a[k++] = 0;
+                } else {
+                    int x = 0;
+                    const auto r = std::from_chars(t.data(), t.data() + t.size(), x);
+                    if (r.ec != std::errc() || r.ptr != t.data() + t.size() || x < 0 || x > 1) return false;
+                    a[k++] = x;
+                }
+                b = i + 1;
+            }
+        }
+        if (missing) {
+            code = 3;
+            return true;
+        }
+        if (k != 2) return false;
+        code = (uint8_t)(a[0] + a[1]);
+        return true;
+    }
+    if (v == ".") {
+        code = 3;
+        return true;
+    }
+    double val[3];
+    int k = 0;
+    bool any_missing = false;
+    size_t b = 0;
+    for (size_t i = 0; i <= v.size(); i++) {
+        if (i == v.size() || v[i] == ',') {
+            if (k >= 3) return false;
+            const std::string_view t = v.substr(b, i - b);
+            if (t == ".") {
+                any_missing = true;
+                val[k++] = 0.0;
+            } else {
+                const auto r = std::from_chars(t.data(), t.data() + t.size(), val[k]);
+                if (r.ec != std::errc() || r.ptr == t.data()) return false;
+                k++;
+            }
+            b = i + 1;
+        }
+    }
+    if (k != 3) return false;
+    if (any_missing) {
+        code = 3;
+        return true;
+    }
+    // likelihood scale: PL = -10 log10 L, GL = log10 L
+    double ll[3];
+    for (int i = 0; i < 3; i++) ll[i] = (field == 'P') ? -val[i] / 10.0 : val[i];
+    int best = 0;
+    for (int i = 1; i < 3; i++)
+        if (ll[i] > ll[best]) best = i;
+    for (int i = 0; i < 3; i++)
+        if (i != best && ll[best] - ll[i] < 25.5 - 1e-9) {
+            soft++;
+            break;
+        }
+    code = (uint8_t)best;
+    return true;
+}
+
+struct Chunk {
+    const char* b = nullptr;
+    const char* e = nullptr;
+    std::vector<uint8_t> rows;   // kept records x samples
+    std::vector<double> af;
+    uint64_t total = 0, not_snp = 0, multi = 0, soft = 0;
+    int64_t kept = 0;
+    bool failed = false;
+    uint64_t fail_rec = 0;       // 1-based record index within the chunk
+    std::string fail_kind;       // message with %R for the global record number
+};
+
+void parse_chunk(Chunk& c, char field, bool af_info, size_t n_samples) {
+    const std::string_view key = field == 'T' ? "GT" : (field == 'P' ? "PL" : "GL");
+    std::string_view last_fmt;
+    int last_fi = -1;
+    const char* p = c.b;
+    auto fail = [&](const std::string& what) {
+        c.failed = true;
+        c.fail_rec = c.total;
+        c.fail_kind = what;
+    };
+    while (p < c.e) {
+        const char* nl = static_cast<const char*>(std::memchr(p, '\n', (size_t)(c.e - p)));
+        const char* le = nl ? nl : c.e;
+        const char* next = nl ? nl + 1 : c.e;
+        if (le > p && le[-1] == '\r') le--;
+        if (le == p || *p == '#') {
+            p = next;
+            continue;
+        }
+        c.total++;
+        // the record must have 9 + n_samples columns (extra ones are ignored)
+        const size_t tabs = (size_t)std::count(p, le, '\t');
+        if (n_samples == 0 || tabs + 1 < 9 + n_samples) {
+            fail("malformed record %R");
+            return;
+        }
+        const char* col[10];
+        col[0] = p;
+        const char* q = p;
+        for (int k = 1; k < 10; k++) {
+            const char* t = static_cast<const char*>(std::memchr(q, '\t', (size_t)(le - q)));
+            q = t + 1;
+            col[k] = q;
+        }
+        auto field_of = [&](int k) { return std::string_view(col[k], (size_t)(col[k + 1] - 1 - col[k])); };
+        const std::string_view ref = field_of(3), alt = field_of(4);
+        bool snp = is_base(ref);
+        size_t n_alts = 0, ab = 0;
+        for (size_t i = 0; i <= alt.size(); i++) {
+            if (i == alt.size() || alt[i] == ',') {
+                snp = snp && is_base(alt.substr(ab, i - ab));
+                n_alts++;
+                ab = i + 1;
+            }
+        }
+        if (!snp) {
+            c.not_snp++;
+            p = next;
+            continue;
+        }
+        if (n_alts != 1) {
+            c.multi++;
+            p = next;
+            continue;
+        }
+        const std::string_view fmt = field_of(8);
+        int fi = -1;
+        if (fmt == last_fmt) {
+            fi = last_fi;
+        } else {
+            size_t fb = 0;
+            int idx = 0;
+            for (size_t i = 0; i <= fmt.size(); i++) {
+                if (i == fmt.size() || fmt[i] == ':') {
+                    if (fmt.substr(fb, i - fb) == key) fi = idx;
+                    idx++;
+                    fb = i + 1;
+                }
+            }
+            last_fmt = fmt;
+            last_fi = fi;
+        }
+        if (fi < 0) {
+            fail("No " + std::string(key) + " data found");
+            return;
+        }
+        const size_t base = c.rows.size();
+        c.rows.resize(base + n_samples);
+        const char* s = col[9];
+        for (size_t k = 0; k < n_samples; k++) {
+            const char* t = static_cast<const char*>(std::memchr(s, '\t', (size_t)(le - s)));
+            const char* se = t ? t : le;
+            // the fi-th ':' subfield ("." when the value has fewer)
+            const char* a = s;
+            int idx = 0;
+            while (idx < fi) {
+                const char* cpos = static_cast<const char*>(std::memchr(a, ':', (size_t)(se - a)));
+                if (!cpos) break;
+                a = cpos + 1;
+                idx++;
+            }
+            std::string_view v(".");
+            if (idx == fi) {
+                const char* cpos = static_cast<const char*>(std::memchr(a, ':', (size_t)(se - a)));
+                v = std::string_view(a, (size_t)((cpos ? cpos : se) - a));
+            }
+            if (!parse_call(v, field, c.rows[base + k], c.soft)) {
+                fail("Value " + std::string(v) + " is not a valid " + std::string(key));
+                return;
+            }
+            s = t ? t + 1 : le;
+        }
+        if (af_info) {
+            const std::string_view info = field_of(7);
+            double a = NAN;
+            size_t ib = 0;
+            for (size_t i = 0; i <= info.size(); i++) {
+                if (i == info.size() || info[i] == ';') {
+                    const std::string_view kv = info.substr(ib, i - ib);
+                    if (kv.size() >= 3 && kv.substr(0, 3) == "AF=") {
+                        const std::string num(kv.substr(3));
+                        a = std::strtod(num.c_str(), nullptr);
+                    }
+                    ib = i + 1;
+                }
+            }
+            if (std::isnan(a)) {
+                fail("No AF info found");
+                return;
+            }
+            const double altf = std::min(std::max(a, 0.0), 1.0);
+            c.af.push_back(1.0 - altf);
+            c.af.push_back(a);
+        }
+        c.kept++;
+        p = next;
+    }
+}
+
+}  // namespace
+
+int read_vcf(const std::string& path, char field, bool af_info, int threads, VcfData& out, std::string& err) {
+    if (threads <= 0) threads = (int)std::max(1u, std::thread::hardware_concurrency());
+    std::vector<char> text;
+    if (!load_text(path, threads, text, err)) return 1;
+    const char* b = text.data();
+    const char* e = b + text.size();
+    // header: ## lines, then #CHROM with the sample names
+    const char* p = b;
+    out = VcfData{};
+    while (p < e && *p == '#') {
+        const char* nl = static_cast<const char*>(std::memchr(p, '\n', (size_t)(e - p)));
+        const char* le = nl ? nl : e;
+        const char* lt = (le > p && le[-1] == '\r') ? le - 1 : le;
+        if ((size_t)(lt - p) >= 6 && std::memcmp(p, "#CHROM", 6) == 0) {
+            int k = 0;
+            const char* f = p;
+            for (;;) {
+                const char* t = static_cast<const char*>(std::memchr(f, '\t', (size_t)(lt - f)));
+                const char* fe = t ? t : lt;
+                if (k >= 9) out.samples.emplace_back(f, (size_t)(fe - f));
+                k++;
+                if (!t) break;
+                f = t + 1;
+            }
+        }
+        p = nl ? nl + 1 : e;
+    }
+    // the body, cut at line boundaries into about 4 chunks per thread
+    const int64_t body = (int64_t)(e - p);
+    const int n_chunks = body > (1 << 20) ? std::max(1, threads * 4) : 1;
+    std::vector<Chunk> chunks((size_t)n_chunks);
+    const char* cur = p;
+    for (int i = 0; i < n_chunks; i++) {
+        const char* target = (i == n_chunks - 1) ? e : p + body * (i + 1) / n_chunks;
+        if (target < cur) target = cur;
+        if (target < e) {
+            const char* nl = static_cast<const char*>(std::memchr(target, '\n', (size_t)(e - target)));
+            target = nl ? nl + 1 : e;
+        }
+        chunks[i].b = cur;
+        chunks[i].e = target;
+        cur = target;
+    }
+    const size_t ns = out.samples.size();
+    parallel_for(threads, n_chunks, [&](int, int64_t cb, int64_t ce) {
+        for (int64_t i = cb; i < ce; i++) parse_chunk(chunks[i], field, af_info, ns);
+    });
+    // counts and the first failure in file order
+    uint64_t before = 0;
+    for (auto& c : chunks) {
+        if (c.failed) {
+            std::string m = c.fail_kind;
+            const size_t at = m.find("%R");
+            if (at != std::string::npos) m.replace(at, 2, std::to_string(before + c.fail_rec));
+            err = m;
+            out.total = before + c.fail_rec;
+            return 1;
+        }
+        before += c.total;
+        out.total += c.total;
+        out.not_snp += c.not_snp;
+        out.multi += c.multi;
+        out.soft += c.soft;
+        out.n_sites += c.kept;
+    }
+    // sample-major codes: each thread a range of samples, sites in blocks
+    const int64_t nv = out.n_sites;
+    out.codes.resize((size_t)(nv * (int64_t)ns));
+    std::vector<int64_t> first((size_t)n_chunks + 1, 0);
+    for (int i = 0; i < n_chunks; i++) first[i + 1] = first[i] + chunks[i].kept;
+    parallel_for(threads, (int64_t)ns, [&](int, int64_t s0, int64_t s1) {
+        for (int i = 0; i < n_chunks; i++) {
+            const Chunk& c = chunks[i];
+            for (int64_t v0 = 0; v0 < c.kept; v0 += 64) {
+                const int64_t v1 = std::min<int64_t>(c.kept, v0 + 64);
+                for (int64_t s = s0; s < s1; s++) {
+                    uint8_t* dst = out.codes.data() + s * nv + first[i];
+                    for (int64_t v = v0; v < v1; v++) dst[v] = c.rows[(size_t)(v * (int64_t)ns + s)];
+                }
+            }
+        }
+    });
+    if (af_info) {
+        out.af.reserve((size_t)(2 * nv));
+        for (auto& c : chunks) out.af.insert(out.af.end(), c.af.begin(), c.af.end());
+    }
+    return 0;
+}
+
+}  // namespace kg
+
+// ------------------------------------------------------------------- C ABI
+struct kg_vcf {
+    kg::VcfData d;
+    std::string err;
+};
+
+extern "C" int kg_vcf_read(const char* path, const char* field, int af_info, int threads, kg_vcf** out) {
+    if (!out) return KG_EINVAL;
+    *out = nullptr;
+    kg_vcf* v = new (std::nothrow) kg_vcf;
+    if (!v) return KG_ENOMEM;
+    *out = v;
+    try {
+        if (!path || !field) {
+            v->err = "path and field are required";
+            return KG_EINVAL;
+        }
+        const std::string f(field);
+        char fc;
+        if (f == "GT") fc = 'T';
+        else if (f == "GL") fc = 'L';
+        else if (f == "PL") fc = 'P';
+        else {
+            v->err = "field must be GT, GL or PL";
+            return KG_EINVAL;
+        }
+        if (kg::read_vcf(path, fc, af_info != 0, threads, v->d, v->err)) return KG_EINVAL;
+        return KG_OK;
+    } catch (const std::bad_alloc&) {
+        v->err = "out of host memory";
+        return KG_ENOMEM;
+    } catch (const std::exception& e) {
+        v->err = e.what();
+        return KG_EINVAL;
+    }
+}
+
+extern "C" const char* kg_vcf_error(const kg_vcf* v) { return v ? v->err.c_str() : "null handle"; }
+
+extern "C" int kg_vcf_info(const kg_vcf* v, int64_t* n_samples, int64_t* n_sites, uint64_t* counts) {
+    if (!v) return KG_EINVAL;
+    if (n_samples) *n_samples = (int64_t)v->d.samples.size();
+    if (n_sites) *n_sites = v->d.n_sites;
+    if (counts) {
+        counts[0] = v->d.total;
+        counts[1] = v->d.not_snp;
+        counts[2] = v->d.multi;
+        counts[3] = v->d.soft;
+    }
+    return KG_OK;
+}
+
+extern "C" int kg_vcf_codes(const kg_vcf* v, uint8_t* codes, double* af) {
+    if (!v) return KG_EINVAL;
+    if (codes && !v->d.codes.empty()) std::memcpy(codes, v->d.codes.data(), v->d.codes.size());
+    if (af) {
+        if (v->d.af.empty()) return KG_EINVAL;
+        std::memcpy(af, v->d.af.data(), sizeof(double) * v->d.af.size());
+    }
+    return KG_OK;
+}
+
+extern "C" const char* kg_vcf_sample(const kg_vcf* v, int64_t i) {
+    if (!v || i < 0 || i >= (int64_t)v->d.samples.size()) return nullptr;
+    return v->d.samples[(size_t)i].c_str();
+}
+
+extern "C" void kg_vcf_free(kg_vcf* v) { delete v; }

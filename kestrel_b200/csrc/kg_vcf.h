@@ -1,0 +1,33 @@
+// kg_vcf.h — multithreaded VCF reader for the CLI and the C ABI.
+//
+// Reads biallelic SNP records of a VCF 4.x file (plain, gzip or bgzip) into
+// per-sample genotype codes (0 = 0/0, 1 = 0/1, 2 = 1/1, 3 = missing), with the
+// reference's record rules (src/vcf.rs:96-236): records whose REF or ALT is not
+// a single base are skipped, as are records with more than one ALT; GT calls
+// are diploid allele indices separated by '/' or '|' ('.' = missing); GL/PL
+// calls are three likelihoods reduced to the most likely genotype (a row that
+// is not one-hot to 25.5 log10 units is counted as soft).  BGZF blocks are
+// inflated in parallel; the text is cut at line boundaries and the chunks are
+// parsed in parallel, then merged in file order.
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+namespace kg {
+
+struct VcfData {
+    std::vector<std::string> samples;
+    int64_t n_sites = 0;            // kept (biallelic SNP) records
+    std::vector<uint8_t> codes;     // sample-major: codes[s * n_sites + v]
+    std::vector<double> af;         // with allele frequencies from INFO/AF: [REF, ALT] per kept site
+    uint64_t total = 0, not_snp = 0, multi = 0, soft = 0;
+};
+
+// field: 'T' GT, 'L' GL, 'P' PL.  af_info: read INFO/AF (an error when absent).
+// threads <= 0: all hardware threads.  Returns 0, or 1 with err set (the
+// message of the first bad record in file order).
+int read_vcf(const std::string& path, char field, bool af_info, int threads, VcfData& out, std::string& err);
+
+}  // namespace kg

@@ -1,0 +1,218 @@
+"""The multithreaded VCF reader (kg_vcf_read; the CLI's reader) against a plain
+Python parser written from the same record rules: plain, gzip and bgzip input,
+GT/PL/GL fields, skipped records, INFO/AF, thread-count invariance, and the
+first error in file order.  CPU only."""
+import gzip
+import os
+import struct
+import tempfile
+import zlib
+
+import numpy as np
+import pytest
+
+import kestrel_b200 as kb
+from kestrel_b200 import synth
+
+BASES = set("ACGTacgt")
+
+
+def py_parse(text, field="GT", af_info=False):
+    """Reference parse: returns (codes [S, V], af or None, samples, counts)."""
+    key = field
+    samples, rows, afs = [], [], []
+    total = not_snp = multi = soft = 0
+    for line in text.split("\n"):
+        line = line.rstrip("\r")
+        if line.startswith("#CHROM"):
+            samples = line.split("\t")[9:]
+            continue
+        if not line or line.startswith("#"):
+            continue
+        total += 1
+        cols = line.split("\t")
+        if len(cols) < 9 + len(samples) or not samples:
+            raise ValueError(f"malformed record {total}")
+        alts = cols[4].split(",")
+        snp = len(cols[3]) == 1 and cols[3] in BASES and all(len(a) == 1 and a in BASES for a in alts)
+        if not snp:
+            not_snp += 1
+            continue
+        if len(alts) != 1:
+            multi += 1
+            continue
+        fmt = cols[8].split(":")
+        fi = max([i for i, f in enumerate(fmt) if f == key], default=-1)
+        if fi < 0:
+            raise ValueError(f"No {key} data found")
+        row = []
+        for s in range(len(samples)):
+            sub = cols[9 + s].split(":")
+            v = sub[fi] if fi < len(sub) else "."
+            if field == "GT":
+                parts = v.replace("|", "/").split("/")
+                if "." in parts:
+                    if len(parts) > 2:
+                        raise ValueError(f"Value {v} is not a valid GT")
+                    row.append(3)
+                    continue
+                if len(parts) != 2 or not all(p in ("0", "1") for p in parts):
+                    raise ValueError(f"Value {v} is not a valid GT")
+                row.append(int(parts[0]) + int(parts[1]))
+            else:
+                if v == ".":
+                    row.append(3)
+                    continue
+                parts = v.split(",")
+                if len(parts) != 3:
+                    raise ValueError(f"Value {v} is not a valid {key}")
+                if "." in parts:
+                    row.append(3)
+                    continue
+                val = [float(p) for p in parts]
+                ll = [-x / 10.0 for x in val] if field == "PL" else val
+                best = int(np.argmax(ll))
+                if any(i != best and ll[best] - ll[i] < 25.5 - 1e-9 for i in range(3)):
+                    soft += 1
+                row.append(best)
+        if af_info:
+            a = float("nan")
+            for kv in cols[7].split(";"):
+                if kv.startswith("AF="):
+                    a = float(kv[3:].split(",")[0])
+            if np.isnan(a):
+                raise ValueError("No AF info found")
+            afs.append([1.0 - min(max(a, 0.0), 1.0), a])
+        rows.append(row)
+    codes = np.array(rows, np.uint8).T.reshape(len(samples), len(rows)) if rows else np.zeros((len(samples), 0), np.uint8)
+    return codes, (np.array(afs) if af_info else None), samples, \
+        {"records": total, "not_snp": not_snp, "multiallelic": multi, "soft_likelihoods": soft}
+
+
+def write_bgzip(path, data: bytes, block=65280):
+    """BGZF: gzip members of at most 64 KB with the 'BC' extra subfield, then the
+    empty end-of-file member."""
+    with open(path, "wb") as fh:
+        for i in range(0, len(data) + 1, block):
+            chunk = data[i:i + block]
+            if not chunk and i:
+                break
+            co = zlib.compressobj(6, zlib.DEFLATED, -15)
+            comp = co.compress(chunk) + co.flush()
+            bsize = 18 + len(comp) + 8 - 1
+            fh.write(b"\x1f\x8b\x08\x04\x00\x00\x00\x00\x00\xff\x06\x00BC\x02\x00" + struct.pack("<H", bsize))
+            fh.write(comp)
+            fh.write(struct.pack("<II", zlib.crc32(chunk) & 0xffffffff, len(chunk)))
+        fh.write(bytes.fromhex("1f8b08040000000000ff0600424302001b0003000000000000000000"))
+
+
+def edge_records(n):
+    def calls(txt):
+        return "\t".join([txt] * n)
+    return [f"2\t1\t.\tA\tC,G\t.\tPASS\tAF=0.2\tGT\t{calls('0/1')}",      # multi-allelic
+            f"2\t2\t.\tAT\tC\t.\tPASS\tAF=0.2\tGT\t{calls('0/1')}",       # not a SNP
+            f"2\t3\t.\tG\t<DEL>\t.\tPASS\tAF=0.2\tGT\t{calls('1/1')}",    # symbolic ALT
+            f"2\t4\t.\tT\tG\t.\tPASS\tAF=0.4;DP=9\tGT:DP\t{calls('0|1:7')}",
+            f"2\t5\t.\tc\tg\t.\tPASS\tDP=3;AF=0.7\tDP:GT\t{calls('5:1/1')}",
+            f"2\t6\t.\tA\tT\t.\tPASS\tAF=0.5\tGT\t{calls('./.')}"]
+
+
+@pytest.fixture(scope="module")
+def cohort():
+    return synth.make_cohort(37, 3000, 61, missing=0.03, name="vcf")
+
+
+def make_text(codes, field, extra=True, crlf=False):
+    with tempfile.TemporaryDirectory() as td:
+        p = os.path.join(td, "x.vcf")
+        synth.write_vcf(p, codes, field=field)
+        text = open(p).read()
+    text = text.replace("\tPASS\t.\t", "\tPASS\tAF=0.25\t")
+    if extra and field == "GT":
+        text += "\n".join(edge_records(codes.shape[0])) + "\n"
+    if crlf:
+        text = text.replace("\n", "\r\n")
+    return text
+
+
+@pytest.mark.parametrize("compression", ["plain", "gzip", "bgzip"])
+@pytest.mark.parametrize("field", ["GT", "PL"])
+def test_reader_matches_python(cohort, field, compression):
+    text = make_text(cohort.codes, field)
+    ref = py_parse(text, field, af_info=True)
+    with tempfile.TemporaryDirectory() as td:
+        p = os.path.join(td, "x.vcf" + ("" if compression == "plain" else ".gz"))
+        data = text.encode()
+        if compression == "plain":
+            open(p, "wb").write(data)
+        elif compression == "gzip":
+            with gzip.open(p, "wb") as fh:
+                fh.write(data)
+        else:
+            write_bgzip(p, data)
+        for threads in (1, 3, 8):
+            codes, af, names, counts = kb.read_vcf(p, field, allele_freqs="info", threads=threads)
+            assert np.array_equal(codes, ref[0])
+            assert np.array_equal(af, ref[1])
+            assert names == ref[2]
+            assert counts == ref[3]
+    if field == "GT":
+        assert counts["multiallelic"] == 1 and counts["not_snp"] == 2
+
+
+def test_crlf_and_gl_field(cohort):
+    gl = np.array(["0,-25.5,-30", "-26,0,-40", "-50,-30,0", "."])
+    lines = ["##fileformat=VCFv4.2", "#CHROM\tPOS\tID\tREF\tALT\tQUAL\tFILTER\tINFO\tFORMAT\tA\tB\tC"]
+    rng = np.random.default_rng(2)
+    for s in range(200):
+        c = rng.integers(0, 4, 3)
+        lines.append(f"1\t{s + 1}\t.\tA\tG\t.\tPASS\t.\tGL\t" + "\t".join(gl[c]))
+    text = "\r\n".join(lines) + "\r\n"
+    ref = py_parse(text, "GL")
+    with tempfile.TemporaryDirectory() as td:
+        p = os.path.join(td, "gl.vcf")
+        open(p, "w", newline="").write(text)
+        codes, _, names, counts = kb.read_vcf(p, "GL", threads=4)
+    assert names == ["A", "B", "C"]
+    assert np.array_equal(codes, ref[0]) and counts == ref[3]
+
+
+def test_multichunk_first_error_in_file_order():
+    # a body above 1 MB is cut into chunks; the first bad record (file order)
+    # is reported with its global record number
+    co = synth.make_cohort(64, 12000, 62, missing=0.01, name="big")
+    text = make_text(co.codes, "GT", extra=False)
+    lines = text.split("\n")
+    body = [i for i, ln in enumerate(lines) if ln and not ln.startswith("#")]
+    bad1, bad2 = body[7000], body[9000]
+    lines[bad2] = lines[bad2].replace("0/0", "0/7", 1).replace("0/1", "0/7", 1).replace("1/1", "0/7", 1)
+    lines[bad1] = "\t".join(lines[bad1].split("\t")[:20])   # too few columns
+    bad_text = "\n".join(lines)
+    with tempfile.TemporaryDirectory() as td:
+        p = os.path.join(td, "bad.vcf")
+        open(p, "w").write(bad_text)
+        assert len(bad_text) > (1 << 20)
+        for threads in (1, 8):
+            with pytest.raises(kb.KestrelError, match="malformed record 7001"):
+                kb.read_vcf(p, "GT", threads=threads)
+        good = os.path.join(td, "good.vcf")
+        open(good, "w").write(text)
+        codes, _, _, counts = kb.read_vcf(good, "GT", threads=8)
+        assert np.array_equal(codes, co.codes) and counts["records"] == 12000
+
+
+def test_reader_errors(cohort):
+    with tempfile.TemporaryDirectory() as td:
+        p = os.path.join(td, "x.vcf")
+        open(p, "w").write("##fileformat=VCFv4.2\n#CHROM\tPOS\tID\tREF\tALT\tQUAL\tFILTER\tINFO\tFORMAT\tA\n"
+                           "1\t1\t.\tA\tC\t.\tPASS\t.\tDP\t3\n")
+        with pytest.raises(kb.KestrelError, match="No GT data found"):
+            kb.read_vcf(p, "GT")
+        with pytest.raises(kb.KestrelError, match="No AF info found"):
+            open(p, "w").write("#CHROM\tPOS\tID\tREF\tALT\tQUAL\tFILTER\tINFO\tFORMAT\tA\n"
+                               "1\t1\t.\tA\tC\t.\tPASS\t.\tGT\t0/1\n")
+            kb.read_vcf(p, "GT", allele_freqs="info")
+        with pytest.raises(kb.KestrelError, match="cannot open"):
+            kb.read_vcf(os.path.join(td, "missing.vcf"))
+        with pytest.raises(kb.KestrelError, match="field must be"):
+            kb.read_vcf(p, "XX")
