@@ -194,7 +194,7 @@ extern "C" int kg_run_cli(int argc, const char* const* argv) {
         std::fprintf(stderr, "Error: Must have at least one site and one sample\n");
         return 1;
     }
-    const std::vector<uint8_t>& codes = vcf.codes;
+    const kg::Bytes& codes = vcf.codes;
     int64_t nsel = o.samples < 0 ? ns : o.samples;
     if (nsel > ns) {
         std::fprintf(stderr, "Error: Requested samples %lld exceeds total samples %lld\n", (long long)nsel, (long long)ns);

@@ -1,6 +1,10 @@
 // kg_vcf.cpp — multithreaded VCF reader (see kg_vcf.h).
 #include "kg_vcf.h"
 
+#include <fcntl.h>
+#include <sys/mman.h>
+#include <sys/stat.h>
+#include <unistd.h>
 #include <zlib.h>
 
 #include <new>
@@ -13,6 +17,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <memory>
 #include <string_view>
 #include <thread>
 
@@ -35,55 +40,96 @@ void parallel_for(int n_threads, int64_t n, F&& f) {
     for (auto& th : pool) th.join();
 }
 
-bool read_file(const std::string& path, std::vector<char>& buf, std::string& err) {
-    FILE* f = std::fopen(path.c_str(), "rb");
-    if (!f) {
-        err = "cannot open " + path;
-        return false;
+// A file's bytes: a read-only mapping of a regular file (the parse threads
+// fault its pages in parallel), else a copy read with stdio.
+class FileBytes {
+public:
+    FileBytes() = default;
+    FileBytes(const FileBytes&) = delete;
+    FileBytes& operator=(const FileBytes&) = delete;
+    ~FileBytes() {
+        if (map_) munmap(map_, n_);
     }
-    std::fseek(f, 0, SEEK_END);
-    const long long n = ftello(f);
-    std::fseek(f, 0, SEEK_SET);
-    if (n < 0) {
+    bool open(const std::string& path, std::string& err) {
+        const int fd = ::open(path.c_str(), O_RDONLY);
+        if (fd < 0) {
+            err = "cannot open " + path;
+            return false;
+        }
+        struct stat st {};
+        if (fstat(fd, &st) == 0 && S_ISREG(st.st_mode) && st.st_size > 0) {
+            void* m = mmap(nullptr, (size_t)st.st_size, PROT_READ, MAP_PRIVATE, fd, 0);
+            if (m != MAP_FAILED) {
+                ::close(fd);
+                map_ = m;
+                n_ = (size_t)st.st_size;
+                p_ = static_cast<const char*>(m);
+                return true;
+            }
+        }
+        ::close(fd);
+        FILE* f = std::fopen(path.c_str(), "rb");
+        if (!f) {
+            err = "cannot open " + path;
+            return false;
+        }
+        char buf[1 << 16];
+        size_t got;
+        while ((got = std::fread(buf, 1, sizeof buf, f)) > 0) copy_.insert(copy_.end(), buf, buf + got);
+        const bool bad = std::ferror(f) != 0;
         std::fclose(f);
-        err = "cannot read " + path;
-        return false;
+        if (bad) {
+            err = "cannot read " + path;
+            return false;
+        }
+        p_ = copy_.data();
+        n_ = copy_.size();
+        return true;
     }
-    buf.resize((size_t)n);
-    const size_t got = n ? std::fread(buf.data(), 1, (size_t)n, f) : 0;
-    std::fclose(f);
-    if (got != (size_t)n) {
-        err = "cannot read " + path;
-        return false;
-    }
-    return true;
-}
+    const char* data() const { return p_; }
+    size_t size() const { return n_; }
+
+private:
+    void* map_ = nullptr;
+    const char* p_ = nullptr;
+    size_t n_ = 0;
+    std::vector<char> copy_;
+};
+
+// The decompressed (or mapped) text of a VCF file.
+struct Text {
+    FileBytes file;                  // plain text: the file itself
+    std::unique_ptr<char[]> bgzf;    // BGZF: blocks inflated in parallel
+    std::vector<char> gz;            // plain gzip: one serial stream
+    const char* data = nullptr;
+    size_t size = 0;
+};
 
 // BGZF (RFC 1952 members with a 'BC' extra subfield holding the block size
 // minus one): the members' starts and uncompressed sizes, or false if any
 // member is not BGZF.
-bool bgzf_blocks(const std::vector<char>& b, std::vector<size_t>& start, std::vector<size_t>& clen,
+bool bgzf_blocks(const char* b, size_t nb, std::vector<size_t>& start, std::vector<size_t>& clen,
                  std::vector<uint32_t>& isize, std::vector<size_t>& hlen) {
     size_t p = 0;
-    while (p < b.size()) {
-        if (p + 18 > b.size()) return false;
-        const uint8_t* h = reinterpret_cast<const uint8_t*>(b.data() + p);
+    while (p < nb) {
+        if (p + 18 > nb) return false;
+        const uint8_t* h = reinterpret_cast<const uint8_t*>(b + p);
         if (h[0] != 0x1f || h[1] != 0x8b || h[2] != 8 || !(h[3] & 4)) return false;
         const size_t xlen = (size_t)h[10] | ((size_t)h[11] << 8);
         size_t q = p + 12;
         const size_t qe = q + xlen;
-        if (qe > b.size()) return false;
+        if (qe > nb) return false;
         long bsize = -1;
         while (q + 4 <= qe) {
-            const uint8_t* s = reinterpret_cast<const uint8_t*>(b.data() + q);
+            const uint8_t* s = reinterpret_cast<const uint8_t*>(b + q);
             const size_t slen = (size_t)s[2] | ((size_t)s[3] << 8);
             if (s[0] == 'B' && s[1] == 'C' && slen == 2 && q + 6 <= qe) bsize = (long)s[4] | ((long)s[5] << 8);
             q += 4 + slen;
         }
         if (bsize < 0) return false;
         const size_t total = (size_t)bsize + 1;
-        if (p + total > b.size() || total < 12 + xlen + 8) return false;
-        const uint8_t* t = reinterpret_cast<const uint8_t*>(b.data() + p + total - 4);
+        if (p + total > nb || total < 12 + xlen + 8) return false;
+        const uint8_t* t = reinterpret_cast<const uint8_t*>(b + p + total - 4);
         start.push_back(p);
         hlen.push_back(12 + xlen);
         clen.push_back(total - 12 - xlen - 8);
@@ -132,29 +178,40 @@ bool gunzip_stream(const std::string& path, std::vector<char>& text, std::string
     return true;
 }
 
-// The file's text: plain, BGZF (blocks inflated in parallel) or plain gzip.
-bool load_text(const std::string& path, int threads, std::vector<char>& text, std::string& err) {
-    std::vector<char> raw;
-    if (!read_file(path, raw, err)) return false;
-    if (raw.size() < 2 || (uint8_t)raw[0] != 0x1f || (uint8_t)raw[1] != 0x8b) {
-        text.swap(raw);
+// The file's text: plain (mapped), BGZF (blocks inflated in parallel) or
+// plain gzip.
+bool load_text(const std::string& path, int threads, Text& text, std::string& err) {
+    if (!text.file.open(path, err)) return false;
+    const char* raw = text.file.data();
+    const size_t nraw = text.file.size();
+    if (nraw < 2 || (uint8_t)raw[0] != 0x1f || (uint8_t)raw[1] != 0x8b) {
+        text.data = raw;
+        text.size = nraw;
         return true;
     }
     std::vector<size_t> st, cl, hl;
     std::vector<uint32_t> is;
-    if (!bgzf_blocks(raw, st, cl, is, hl)) return gunzip_stream(path, text, err);
+    if (!bgzf_blocks(raw, nraw, st, cl, is, hl)) {
+        if (!gunzip_stream(path, text.gz, err)) return false;
+        text.data = text.gz.data();
+        text.size = text.gz.size();
+        return true;
+    }
     std::vector<size_t> off(st.size() + 1, 0);
     for (size_t i = 0; i < st.size(); i++) off[i + 1] = off[i] + is[i];
-    text.resize(off.back());
+    text.bgzf.reset(new char[std::max<size_t>(1, off.back())]);
+    char* out = text.bgzf.get();
     std::vector<char> bad((size_t)std::max(1, threads), 0);
     parallel_for(threads, (int64_t)st.size(), [&](int t, int64_t b, int64_t e) {
         for (int64_t i = b; i < e; i++)
-            if (!inflate_raw(raw.data() + st[i] + hl[i], cl[i], text.data() + off[i], is[i])) bad[t] = 1;
+            if (!inflate_raw(raw + st[i] + hl[i], cl[i], out + off[i], is[i])) bad[t] = 1;
     });
     if (std::find(bad.begin(), bad.end(), 1) != bad.end()) {
         err = "cannot decompress " + path;
         return false;
     }
+    text.data = out;
+    text.size = off.back();
     return true;
 }
 
@@ -232,6 +289,46 @@ bool parse_call(std::string_view v, char field, uint8_t& code, uint64_t& soft) {
         }
     code = (uint8_t)best;
     return true;
+}
+
+// Allele digit of a three-character GT value: 0, 1, 2 for '.', -1 otherwise.
+struct AlleleTable {
+    int8_t a[256];
+    constexpr AlleleTable() : a{} {
+        for (int i = 0; i < 256; i++) a[i] = -1;
+        a[(unsigned char)'0'] = 0;
+        a[(unsigned char)'1'] = 1;
+        a[(unsigned char)'.'] = 2;
+    }
+};
+constexpr AlleleTable kAllele{};
+
+// Code of "a/b" or "a|b" with a, b in {0, 1, .}; -1 when the value has another
+// form (parse_call then decides).  Same results as parse_call on these values.
+inline int gt3_code(const char* s) {
+    const int a = kAllele.a[(unsigned char)s[0]], b = kAllele.a[(unsigned char)s[2]];
+    if ((a | b) < 0 || (s[1] != '/' && s[1] != '|')) return -1;
+    return (a == 2 || b == 2) ? 3 : a + b;
+}
+
+// 8 x 8 byte transpose: byte j of r[i] moves to byte i of r[j] (three rounds
+// of block swaps: 4 x 4, 2 x 2, 1 x 1).
+inline void transpose8x8(uint64_t r[8]) {
+    for (int i = 0; i < 4; i++) {
+        const uint64_t t = ((r[i] >> 32) ^ r[i + 4]) & 0x00000000FFFFFFFFull;
+        r[i] ^= t << 32;
+        r[i + 4] ^= t;
+    }
+    for (int i : {0, 1, 4, 5}) {
+        const uint64_t t = ((r[i] >> 16) ^ r[i + 2]) & 0x0000FFFF0000FFFFull;
+        r[i] ^= t << 16;
+        r[i + 2] ^= t;
+    }
+    for (int i : {0, 2, 4, 6}) {
+        const uint64_t t = ((r[i] >> 8) ^ r[i + 1]) & 0x00FF00FF00FF00FFull;
+        r[i] ^= t << 8;
+        r[i + 1] ^= t;
+    }
 }
 
 struct Chunk {
@@ -323,9 +420,32 @@ void parse_chunk(Chunk& c, char field, bool af_info, size_t n_samples) {
             return;
         }
         const size_t base = c.rows.size();
+        if (base == 0) {
+            // room for the chunk's records at this record's length
+            const size_t per = (size_t)(next - p);
+            c.rows.reserve(((size_t)(c.e - p) / per + 1) * n_samples);
+        }
         c.rows.resize(base + n_samples);
         const char* s = col[9];
+        const bool gt_first = field == 'T' && fi == 0;
         for (size_t k = 0; k < n_samples; k++) {
+            if (gt_first && le - s >= 3) {
+                // the common "a/b" call, alone or first of its subfields
+                const int code = gt3_code(s);
+                const char* after = s + 3;
+                if (code >= 0 && (after == le || *after == '\t' || *after == ':')) {
+                    c.rows[base + k] = (uint8_t)code;
+                    if (after == le) {
+                        s = le;
+                    } else if (*after == '\t') {
+                        s = after + 1;
+                    } else {
+                        const char* t = static_cast<const char*>(std::memchr(after, '\t', (size_t)(le - after)));
+                        s = t ? t + 1 : le;
+                    }
+                    continue;
+                }
+            }
             const char* t = static_cast<const char*>(std::memchr(s, '\t', (size_t)(le - s)));
             const char* se = t ? t : le;
             // the fi-th ':' subfield ("." when the value has fewer)
@@ -379,10 +499,10 @@ void parse_chunk(Chunk& c, char field, bool af_info, size_t n_samples) {
 
 int read_vcf(const std::string& path, char field, bool af_info, int threads, VcfData& out, std::string& err) {
     if (threads <= 0) threads = (int)std::max(1u, std::thread::hardware_concurrency());
-    std::vector<char> text;
+    Text text;
     if (!load_text(path, threads, text, err)) return 1;
-    const char* b = text.data();
-    const char* e = b + text.size();
+    const char* b = text.data;
+    const char* e = b + text.size;
     // header: ## lines, then #CHROM with the sample names
     const char* p = b;
     out = VcfData{};
@@ -442,19 +562,33 @@ int read_vcf(const std::string& path, char field, bool af_info, int threads, Vcf
         out.soft += c.soft;
         out.n_sites += c.kept;
     }
-    // sample-major codes: each thread a range of samples, sites in blocks
+    // sample-major codes: each thread a range of samples (a multiple of 8),
+    // 8 x 8 tiles of sites x samples transposed in 64-bit words
     const int64_t nv = out.n_sites;
-    out.codes.resize((size_t)(nv * (int64_t)ns));
+    out.codes.allocate((size_t)(nv * (int64_t)ns));
     std::vector<int64_t> first((size_t)n_chunks + 1, 0);
     for (int i = 0; i < n_chunks; i++) first[i + 1] = first[i] + chunks[i].kept;
-    parallel_for(threads, (int64_t)ns, [&](int, int64_t s0, int64_t s1) {
+    const int64_t n_groups = ((int64_t)ns + 7) / 8;
+    parallel_for(threads, n_groups, [&](int, int64_t g0, int64_t g1) {
+        const int64_t s0 = g0 * 8, s1 = std::min<int64_t>((int64_t)ns, g1 * 8);
+        uint8_t* codes = out.codes.data();
         for (int i = 0; i < n_chunks; i++) {
             const Chunk& c = chunks[i];
-            for (int64_t v0 = 0; v0 < c.kept; v0 += 64) {
-                const int64_t v1 = std::min<int64_t>(c.kept, v0 + 64);
-                for (int64_t s = s0; s < s1; s++) {
-                    uint8_t* dst = out.codes.data() + s * nv + first[i];
-                    for (int64_t v = v0; v < v1; v++) dst[v] = c.rows[(size_t)(v * (int64_t)ns + s)];
+            const uint8_t* rows = c.rows.data();
+            for (int64_t b0 = 0; b0 < c.kept; b0 += 64) {
+                const int64_t b1 = std::min<int64_t>(c.kept, b0 + 64);
+                for (int64_t s = s0; s < s1; s += 8) {
+                    int64_t v = b0;
+                    if (s + 8 <= s1) {
+                        for (; v + 8 <= b1; v += 8) {
+                            uint64_t r[8];
+                            for (int k = 0; k < 8; k++) std::memcpy(&r[k], rows + (v + k) * (int64_t)ns + s, 8);
+                            transpose8x8(r);
+                            for (int k = 0; k < 8; k++) std::memcpy(codes + (s + k) * nv + first[i] + v, &r[k], 8);
+                        }
+                    }
+                    for (int64_t t = s; t < std::min<int64_t>(s1, s + 8); t++)
+                        for (int64_t w = v; w < b1; w++) codes[t * nv + first[i] + w] = rows[w * (int64_t)ns + t];
                 }
             }
         }

@@ -12,15 +12,34 @@
 #pragma once
 
 #include <cstdint>
+#include <memory>
 #include <string>
 #include <vector>
 
 namespace kg {
 
+// A byte array that is not zero-filled on allocation (its writers touch every
+// byte, from several threads).
+class Bytes {
+public:
+    void allocate(size_t n) {
+        p_.reset(new uint8_t[n ? n : 1]);
+        n_ = n;
+    }
+    uint8_t* data() { return p_.get(); }
+    const uint8_t* data() const { return p_.get(); }
+    size_t size() const { return n_; }
+    bool empty() const { return n_ == 0; }
+
+private:
+    std::unique_ptr<uint8_t[]> p_;
+    size_t n_ = 0;
+};
+
 struct VcfData {
     std::vector<std::string> samples;
     int64_t n_sites = 0;            // kept (biallelic SNP) records
-    std::vector<uint8_t> codes;     // sample-major: codes[s * n_sites + v]
+    Bytes codes;                    // sample-major: codes[s * n_sites + v]
     std::vector<double> af;         // with allele frequencies from INFO/AF: [REF, ALT] per kept site
     uint64_t total = 0, not_snp = 0, multi = 0, soft = 0;
 };

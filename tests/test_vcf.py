@@ -216,3 +216,22 @@ def test_reader_errors(cohort):
             kb.read_vcf(os.path.join(td, "missing.vcf"))
         with pytest.raises(kb.KestrelError, match="field must be"):
             kb.read_vcf(p, "XX")
+
+
+def test_fifo_input_is_read_without_mapping(cohort):
+    # a pipe cannot be mapped: the reader falls back to reading it
+    import threading
+    text = make_text(cohort.codes, "GT")
+    ref = py_parse(text, "GT")
+    with tempfile.TemporaryDirectory() as td:
+        p = os.path.join(td, "pipe.vcf")
+        os.mkfifo(p)
+
+        def feed():
+            with open(p, "w") as fh:
+                fh.write(text)
+        th = threading.Thread(target=feed)
+        th.start()
+        codes, _, names, counts = kb.read_vcf(p, "GT", threads=4)
+        th.join()
+    assert np.array_equal(codes, ref[0]) and names == ref[2] and counts == ref[3]
