@@ -1,5 +1,7 @@
 // kg_cli.cpp — the reference-compatible command line (src/cli.rs:12-181) on
-// top of the C ABI, plus its VCF reader (src/vcf.rs:96-482) for biallelic SNPs.
+// top of the C ABI; its VCF reader (src/vcf.rs:96-482, biallelic SNPs) is
+// kg_vcf.cpp.  The CUDA context is created while the VCF is read, and the
+// output rows are formatted on the host threads in blocks, written in order.
 //
 //   kestrel input.vcf[.gz] kinship.tsv [-a estimate|info] [-f GT|GL|PL]
 //           [-t threads] [-i iterations] [-m maf] [-s samples]
@@ -10,6 +12,7 @@
 // dropped per pair, as the reference's NaN likelihood rows are
 // (src/vcf.rs:355,397; src/lanevector.rs:99-104).  Only biallelic SNPs are
 // estimated; tri- and tetra-allelic SNPs are counted and skipped.
+#include "kg_threads.h"
 #include "kg_vcf.h"
 
 #include <charconv>
@@ -18,6 +21,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "kestrel_gpu.h"
@@ -32,7 +36,7 @@ struct Options {
     double maf = NAN;
     int64_t samples = -1;
     bool cls = false;  // --estimator cls: the reference's default GT estimator (CLS/Brier)
-    int threads = 0;   // VCF reader threads (0 = all)
+    int threads = 0;   // host threads for VCF reading and output writing (0 = all)
 };
 
 void log_info(const char* fmt, const std::string& a = "") {
@@ -48,7 +52,7 @@ int usage(const char* why) {
                  "  <OUTPUT>  Tab-separated file to write the coefficients to\n\n"
                  "Options:\n  -a, --allele-freqs <estimate|info>  [default: estimate]\n"
                  "  -f, --field <GT|GL|PL>              [default: GT]\n"
-                 "  -t, --threads <THREADS>             VCF reader threads [default: all]\n"
+                 "  -t, --threads <THREADS>             Host threads (VCF reading, output) [default: all]\n"
                  "  -i, --iterations <ITERATIONS>       [default: 100]\n"
                  "  -m, --minimum-allele-frequency <F>\n"
                  "  -s, --samples <N>\n"
@@ -131,39 +135,125 @@ bool parse_args(int argc, const char* const* argv, Options& o, std::string& why)
 
 // Shortest round-trip decimal in the layout the reference's TSV writer uses
 // (decimal notation for 1e-5 <= |v| < 1e16, else d.ddde[-]x; "NaN", "inf").
-std::string fmt_f64(double v) {
-    if (std::isnan(v)) return "NaN";
-    if (std::isinf(v)) return v > 0 ? "inf" : "-inf";
-    char buf[64];
-    auto r = std::to_chars(buf, buf + sizeof buf, v, std::chars_format::scientific);
-    std::string s(buf, r.ptr);
-    bool neg = false;
-    if (s[0] == '-') { neg = true; s.erase(0, 1); }
-    size_t e = s.find('e');
-    std::string mant = s.substr(0, e);
-    int exp10 = std::atoi(s.c_str() + e + 1);
-    std::string digits;
-    for (char ch : mant) if (ch != '.') digits.push_back(ch);
-    while (digits.size() > 1 && digits.back() == '0') digits.pop_back();
-    if (v == 0.0) digits = "0";
-    int k = (int)digits.size();
-    int kk = exp10 + 1;  // value = 0.digits x 10^kk
-    std::string out;
-    if (v == 0.0) {
-        out = "0.0";
-    } else if (k <= kk && kk <= 16) {
-        out = digits + std::string(kk - k, '0') + ".0";
-    } else if (0 < kk && kk <= 16) {
-        out = digits.substr(0, kk) + "." + digits.substr(kk);
-    } else if (-5 < kk && kk <= 0) {
-        out = "0." + std::string(-kk, '0') + digits;
-    } else if (k == 1) {
-        out = digits + "e" + std::to_string(kk - 1);
-    } else {
-        out = digits.substr(0, 1) + "." + digits.substr(1) + "e" + std::to_string(kk - 1);
+// Writes at most 32 characters at out and returns their count.
+int fmt_f64(double v, char* out) {
+    if (std::isnan(v)) {
+        std::memcpy(out, "NaN", 3);
+        return 3;
     }
-    return neg ? "-" + out : out;
+    if (std::isinf(v)) {
+        if (v > 0) {
+            std::memcpy(out, "inf", 3);
+            return 3;
+        }
+        std::memcpy(out, "-inf", 4);
+        return 4;
+    }
+    char buf[40];
+    const auto r = std::to_chars(buf, buf + sizeof buf, v, std::chars_format::scientific);
+    const char* p = buf;
+    char* o = out;
+    if (*p == '-') {
+        *o++ = '-';
+        p++;
+    }
+    // the significant digits (no point, no trailing zeros) and the exponent
+    char digits[24];
+    int k = 0;
+    for (; p < r.ptr && *p != 'e'; p++)
+        if (*p != '.') digits[k++] = *p;
+    int exp10 = 0;
+    bool neg_exp = false;
+    for (p++; p < r.ptr; p++) {
+        if (*p == '-') neg_exp = true;
+        else if (*p != '+') exp10 = exp10 * 10 + (*p - '0');
+    }
+    if (neg_exp) exp10 = -exp10;
+    while (k > 1 && digits[k - 1] == '0') k--;
+    auto put = [&](const char* x, int n) {
+        std::memcpy(o, x, (size_t)n);
+        o += n;
+    };
+    auto zeros = [&](int n) {
+        for (int i = 0; i < n; i++) *o++ = '0';
+    };
+    auto exponent = [&](int x) {
+        *o++ = 'e';
+        const auto e = std::to_chars(o, o + 8, x);
+        o = e.ptr;
+    };
+    const int kk = exp10 + 1;  // value = 0.digits x 10^kk
+    if (v == 0.0) {
+        put("0.0", 3);
+    } else if (k <= kk && kk <= 16) {
+        put(digits, k);
+        zeros(kk - k);
+        put(".0", 2);
+    } else if (0 < kk && kk <= 16) {
+        put(digits, kk);
+        *o++ = '.';
+        put(digits + kk, k - kk);
+    } else if (-5 < kk && kk <= 0) {
+        put("0.", 2);
+        zeros(-kk);
+        put(digits, k);
+    } else if (k == 1) {
+        put(digits, 1);
+        exponent(kk - 1);
+    } else {
+        put(digits, 1);
+        *o++ = '.';
+        put(digits + 1, k - 1);
+        exponent(kk - 1);
+    }
+    return (int)(o - out);
 }
+
+// One TSV row of a pair's result.
+void append_row(std::string& dst, const kg_output& r, const std::vector<std::string>& samples) {
+    static const double kv[9] = {1.0, 0.0, 0.5, 0.0, 0.5, 0.0, 0.5, 0.25, 0.0};
+    double kin = 0.0;
+    for (int i = 0; i < 9; i++) kin = std::fma(r.jacquard[i], kv[i], kin);
+    char b[32 * 13 + 64];
+    char* o = b;
+    auto num = [&](double x) {
+        *o++ = '\t';
+        o += fmt_f64(x, o);
+    };
+    num(kin);
+    for (int i = 0; i < 9; i++) num(r.jacquard[i]);
+    *o++ = '\t';
+    o = std::to_chars(o, o + 24, r.iters).ptr;
+    num(r.obj);
+    num(std::log10(r.cond));
+    *o++ = '\n';
+    dst += samples[r.x];
+    dst += '\t';
+    dst += samples[r.y];
+    dst.append(b, (size_t)(o - b));
+}
+
+// The CUDA context (about a second to create) is made on another thread while
+// the VCF is read.
+struct DeviceInit {
+    kg_ctx* ctx = nullptr;
+    int st = 0;
+    std::thread th;
+    DeviceInit() : th([this] { st = kg_create(&ctx, 0, 0); }) {}
+    DeviceInit(const DeviceInit&) = delete;
+    DeviceInit& operator=(const DeviceInit&) = delete;
+    ~DeviceInit() {
+        join();
+        release();
+    }
+    void join() {
+        if (th.joinable()) th.join();
+    }
+    void release() {
+        if (ctx) kg_destroy(ctx);
+        ctx = nullptr;
+    }
+};
 
 }  // namespace
 
@@ -174,6 +264,7 @@ extern "C" int kg_run_cli(int argc, const char* const* argv) {
     if (!parse_args(argc, argv, o, why)) return usage(why.c_str());
     log_info("Kestrel %s", kg_version());
     log_info("Parsing VCF \"%s\"", o.input);
+    DeviceInit dev;
     kg::VcfData vcf;
     std::string err;
     if (kg::read_vcf(o.input, o.field, o.af_info, o.threads, vcf, err)) {
@@ -203,12 +294,13 @@ extern "C" int kg_run_cli(int argc, const char* const* argv) {
     int64_t np = nsel * (nsel + 1) / 2;
     log_info("Calculating Jacquard coefficients for %s pairs", std::to_string(np));
     std::vector<kg_output> out((size_t)np);
-    kg_ctx* ctx = nullptr;
-    int st = kg_create(&ctx, 0, 0);
-    if (st) {
-        std::fprintf(stderr, "Error: no usable CUDA device (%d)\n", st);
+    dev.join();
+    if (dev.st) {
+        std::fprintf(stderr, "Error: no usable CUDA device (%d)\n", dev.st);
         return 1;
     }
+    kg_ctx* ctx = dev.ctx;
+    int st = 0;
     st = kg_load_genotypes(ctx, codes.data(), ns, nv, nv);
     if (!st && o.af_info) st = kg_set_allele_frequencies(ctx, af.data());
     int64_t nout = 0;
@@ -218,10 +310,9 @@ extern "C" int kg_run_cli(int argc, const char* const* argv) {
     }
     if (st) {
         std::fprintf(stderr, "Error: %s\n", kg_last_error(ctx));
-        kg_destroy(ctx);
         return 1;
     }
-    kg_destroy(ctx);
+    dev.release();
     uint64_t nonconv = 0;
     for (auto& r : out) nonconv += (r.iters >= o.iterations);
     if (nonconv)
@@ -234,15 +325,29 @@ extern "C" int kg_run_cli(int argc, const char* const* argv) {
     }
     std::fprintf(f, "sample1\tsample2\tkinship\tjacquard1\tjacquard2\tjacquard3\tjacquard4\tjacquard5\t"
                     "jacquard6\tjacquard7\tjacquard8\tjacquard9\titerations\tobjective\tcondition\n");
-    const double kv[9] = {1.0, 0.0, 0.5, 0.0, 0.5, 0.0, 0.5, 0.25, 0.0};
-    std::string rowbuf;
-    for (auto& r : out) {
-        double kin = 0.0;
-        for (int i = 0; i < 9; i++) kin = std::fma(r.jacquard[i], kv[i], kin);
-        rowbuf = samples[r.x] + "\t" + samples[r.y] + "\t" + fmt_f64(kin);
-        for (int i = 0; i < 9; i++) rowbuf += "\t" + fmt_f64(r.jacquard[i]);
-        rowbuf += "\t" + std::to_string(r.iters) + "\t" + fmt_f64(r.obj) + "\t" + fmt_f64(std::log10(r.cond)) + "\n";
-        std::fputs(rowbuf.c_str(), f);
+    // rows formatted in parallel blocks, written in order; a bounded number
+    // of rows is held at a time
+    const int nt = kg::host_threads(o.threads);
+    const int64_t block = 16384;
+    std::vector<std::string> text((size_t)nt);
+    bool write_failed = false;
+    for (int64_t r0 = 0; r0 < nout && !write_failed; r0 += block * nt) {
+        const int64_t r1 = std::min<int64_t>(nout, r0 + block * nt);
+        // a round with fewer blocks than threads leaves some buffers unused
+        for (auto& t : text) t.clear();
+        kg::parallel_for(nt, (r1 - r0 + block - 1) / block, [&](int t, int64_t b0, int64_t b1) {
+            std::string& dst = text[(size_t)t];
+            for (int64_t i = r0 + b0 * block; i < std::min<int64_t>(r1, r0 + b1 * block); i++)
+                append_row(dst, out[(size_t)i], samples);
+        });
+        for (int t = 0; t < nt && !write_failed; t++)
+            if (!text[(size_t)t].empty() && std::fwrite(text[(size_t)t].data(), 1, text[(size_t)t].size(), f) != text[(size_t)t].size())
+                write_failed = true;
+    }
+    if (write_failed) {
+        std::fclose(f);
+        std::fprintf(stderr, "Error: cannot write %s\n", o.output.c_str());
+        return 1;
     }
     std::fclose(f);
     double wall = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();

@@ -11,6 +11,7 @@
 #include <stdexcept>
 
 #include "kestrel_gpu.h"
+#include "kg_threads.h"
 
 #include <algorithm>
 #include <charconv>
@@ -23,22 +24,6 @@
 
 namespace kg {
 namespace {
-
-template <class F>
-void parallel_for(int n_threads, int64_t n, F&& f) {
-    if (n <= 0) return;
-    const int t = (int)std::max<int64_t>(1, std::min<int64_t>(n_threads, n));
-    if (t == 1) {
-        f(0, (int64_t)0, n);
-        return;
-    }
-    std::vector<std::thread> pool;
-    for (int i = 0; i < t; i++) {
-        const int64_t b = n * i / t, e = n * (i + 1) / t;
-        pool.emplace_back([&f, i, b, e] { f(i, b, e); });
-    }
-    for (auto& th : pool) th.join();
-}
 
 // A file's bytes: a read-only mapping of a regular file (the parse threads
 // fault its pages in parallel), else a copy read with stdio.
@@ -498,7 +483,7 @@ void parse_chunk(Chunk& c, char field, bool af_info, size_t n_samples) {
 }  // namespace
 
 int read_vcf(const std::string& path, char field, bool af_info, int threads, VcfData& out, std::string& err) {
-    if (threads <= 0) threads = (int)std::max(1u, std::thread::hardware_concurrency());
+    threads = host_threads(threads);
     Text text;
     if (!load_text(path, threads, text, err)) return 1;
     const char* b = text.data;

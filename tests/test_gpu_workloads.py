@@ -130,6 +130,32 @@ def test_cli_gt_and_pl_match_oracle(oracle):
     assert [r[0] for r in rows[:2]] == ["S0", "S0"] and [r[1] for r in rows[:2]] == ["S0", "S1"]
 
 
+@pytest.mark.parametrize("threads", [1, 2, 5])
+def test_cli_output_rows_equal_api_results(threads):
+    # 33,930 pairs: more rows than one 16,384-row block per thread, so the
+    # writer runs rounds, the last with idle threads (at -t 2)
+    co = synth.make_cohort(260, 400, seed=44, name="cli-rows")
+    cli = os.path.join(os.path.dirname(kb.__file__), "bin", "kestrel")
+    with kb.Estimator() as est:
+        est.load(co.codes)
+        api = est.relatedness()
+    with tempfile.TemporaryDirectory() as td:
+        vcf = os.path.join(td, "in.vcf")
+        tsv = os.path.join(td, "out.tsv")
+        synth.write_vcf(vcf, co.codes, field="GT")
+        r = subprocess.run([cli, vcf, tsv, "-t", str(threads)], capture_output=True, text=True, timeout=300)
+        assert r.returncode == 0, r.stderr
+        _, rows = _read_tsv(tsv)
+    assert len(rows) == len(api) == 260 * 261 // 2
+    xy = np.array([[int(r[0][1:]), int(r[1][1:])] for r in rows])
+    assert np.array_equal(xy[:, 0], api["x"]) and np.array_equal(xy[:, 1], api["y"])
+    # shortest round-trip text: parsing gives back the API's doubles exactly
+    jac = np.array([[float(v) for v in r[3:12]] for r in rows])
+    assert np.array_equal(jac, api["jacquard"])
+    assert np.array_equal(np.array([int(r[12]) for r in rows]), api["iters"].astype(np.int64))
+    assert np.array_equal(np.array([float(r[13]) for r in rows]), api["obj"])
+
+
 def test_cli_cls_estimator_matches_oracle(oracle):
     co = synth.make_cohort(24, 2500, seed=43, missing=0.0, planted={"parent_offspring": 2})
     cli = os.path.join(os.path.dirname(kb.__file__), "bin", "kestrel")
