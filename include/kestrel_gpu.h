@@ -280,8 +280,9 @@ int kg_run_cli(int argc, const char *const *argv);
 typedef struct kg_vcf kg_vcf;
 int kg_vcf_read(const char *path, const char *field, int af_info, int threads, kg_vcf **out);
 const char *kg_vcf_error(const kg_vcf *vcf);
-/* counts (optional, 4 entries): records, non-SNP records skipped,
- * multi-allelic records skipped, GL/PL rows that were not one-hot. */
+/* counts (optional, 5 entries): records, non-SNP records skipped,
+ * multi-allelic records skipped, GL/PL rows that were not one-hot, kept
+ * records with at least one missing call. */
 int kg_vcf_info(const kg_vcf *vcf, int64_t *n_samples, int64_t *n_sites, uint64_t *counts);
 /* codes: n_samples x n_sites, sample-major (the layout kg_load_genotypes takes);
  * af: n_sites x 2 [REF, ALT] from INFO/AF (KG_EINVAL if it was not read).

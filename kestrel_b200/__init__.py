@@ -287,14 +287,14 @@ def read_vcf(path, field: str = "GT", allele_freqs: str = "estimate", threads: i
             msg = L.kg_vcf_error(h) if h.value else b"out of memory"
             raise KestrelError(st, msg.decode())
         ns, nv = ctypes.c_int64(), ctypes.c_int64()
-        counts = (ctypes.c_uint64 * 4)()
+        counts = (ctypes.c_uint64 * 5)()
         _check_vcf(L.kg_vcf_info(h, ctypes.byref(ns), ctypes.byref(nv), counts), L, h)
         codes = np.empty((ns.value, nv.value), np.uint8)
         af = np.empty((nv.value, 2)) if allele_freqs == "info" else None
         _check_vcf(L.kg_vcf_codes(h, ptr(codes), ptr(af)), L, h)
         names = [L.kg_vcf_sample(h, i).decode() for i in range(ns.value)]
         return codes, af, names, {"records": counts[0], "not_snp": counts[1], "multiallelic": counts[2],
-                                  "soft_likelihoods": counts[3]}
+                                  "soft_likelihoods": counts[3], "with_missing": counts[4]}
     finally:
         if h.value:
             L.kg_vcf_free(h)

@@ -35,7 +35,8 @@ struct Options {
     uint64_t iterations = 100;
     double maf = NAN;
     int64_t samples = -1;
-    bool cls = false;  // --estimator cls: the reference's default GT estimator (CLS/Brier)
+    int estimator = -1;  // -1 unset, 0 ml, 1 cls
+    bool cls = false;    // CLS/Brier: the reference's estimator for -f GT, the default there
     int threads = 0;   // host threads for VCF reading and output writing (0 = all)
 };
 
@@ -56,8 +57,9 @@ int usage(const char* why) {
                  "  -i, --iterations <ITERATIONS>       [default: 100]\n"
                  "  -m, --minimum-allele-frequency <F>\n"
                  "  -s, --samples <N>\n"
-                 "  -e, --estimator <ml|cls>            [default: ml; cls = conditional least squares\n"
-                 "                                       with the Brier objective, GT only]\n",
+                 "  -e, --estimator <ml|cls>            [default: cls for GT, ml for GL and PL;\n"
+                 "                                       cls = conditional least squares with the\n"
+                 "                                       Brier objective, GT only]\n",
                  why);
     return 2;
 }
@@ -104,8 +106,8 @@ bool parse_args(int argc, const char* const* argv, Options& o, std::string& why)
             o.maf = std::atof(v.c_str());
         } else if (is("-e", "--estimator")) {
             if (!val(v)) { why = "missing value for -e"; return false; }
-            if (v == "ml") o.cls = false;
-            else if (v == "cls") o.cls = true;
+            if (v == "ml") o.estimator = 0;
+            else if (v == "cls") o.estimator = 1;
             else { why = "invalid value '" + v + "' for --estimator"; return false; }
         } else if (is("-s", "--samples")) {
             if (!val(v)) { why = "missing value for -s"; return false; }
@@ -126,6 +128,8 @@ bool parse_args(int argc, const char* const* argv, Options& o, std::string& why)
     }
     o.input = pos[0];
     o.output = pos[1];
+    // the reference runs CLS on GT (src/cli.rs:108-118) and ML on GL/PL
+    o.cls = o.estimator < 0 ? o.field == 'T' : o.estimator == 1;
     if (o.cls && o.field != 'T') {
         why = "--estimator cls needs hard calls (-f GT)";
         return false;
@@ -273,8 +277,14 @@ extern "C" int kg_run_cli(int argc, const char* const* argv) {
     }
     log_info("Parsed %s total sites", std::to_string(vcf.total));
     log_info("Skipped %s sites that were not SNPs", std::to_string(vcf.not_snp));
+    if (o.cls) {
+        // the CLS estimator uses the sites every sample calls (src/vcf.rs:217-221)
+        log_info("Skipped %s sites with missing data", std::to_string(vcf.incomplete));
+        log_info("Found %s di-allelic sites", std::to_string(vcf.n_sites - (int64_t)vcf.incomplete));
+    } else {
+        log_info("Found %s di-allelic sites", std::to_string(vcf.n_sites));
+    }
     log_info("Skipped %s tri- or tetra-allelic sites (biallelic sites only)", std::to_string(vcf.multi));
-    log_info("Found %s di-allelic sites", std::to_string(vcf.n_sites));
     if (vcf.soft)
         log_info("%s likelihood entries were not one-hot; their most likely genotype was used",
                  std::to_string(vcf.soft));

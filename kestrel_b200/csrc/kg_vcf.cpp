@@ -321,7 +321,7 @@ struct Chunk {
     const char* e = nullptr;
     std::vector<uint8_t> rows;   // kept records x samples
     std::vector<double> af;
-    uint64_t total = 0, not_snp = 0, multi = 0, soft = 0;
+    uint64_t total = 0, not_snp = 0, multi = 0, soft = 0, incomplete = 0;
     int64_t kept = 0;
     bool failed = false;
     uint64_t fail_rec = 0;       // 1-based record index within the chunk
@@ -453,6 +453,7 @@ void parse_chunk(Chunk& c, char field, bool af_info, size_t n_samples) {
             }
             s = t ? t + 1 : le;
         }
+        if (std::memchr(c.rows.data() + base, 3, n_samples)) c.incomplete++;
         if (af_info) {
             const std::string_view info = field_of(7);
             double a = NAN;
@@ -545,6 +546,7 @@ int read_vcf(const std::string& path, char field, bool af_info, int threads, Vcf
         out.not_snp += c.not_snp;
         out.multi += c.multi;
         out.soft += c.soft;
+        out.incomplete += c.incomplete;
         out.n_sites += c.kept;
     }
     // sample-major codes: each thread a range of samples (a multiple of 8),
@@ -635,6 +637,7 @@ extern "C" int kg_vcf_info(const kg_vcf* v, int64_t* n_samples, int64_t* n_sites
         counts[1] = v->d.not_snp;
         counts[2] = v->d.multi;
         counts[3] = v->d.soft;
+        counts[4] = v->d.incomplete;
     }
     return KG_OK;
 }

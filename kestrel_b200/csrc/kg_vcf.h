@@ -42,6 +42,7 @@ struct VcfData {
     Bytes codes;                    // sample-major: codes[s * n_sites + v]
     std::vector<double> af;         // with allele frequencies from INFO/AF: [REF, ALT] per kept site
     uint64_t total = 0, not_snp = 0, multi = 0, soft = 0;
+    uint64_t incomplete = 0;        // kept records with at least one missing call
 };
 
 // field: 'T' GT, 'L' GL, 'P' PL.  af_info: read INFO/AF (an error when absent).

@@ -109,8 +109,8 @@ def test_cli_gt_and_pl_match_oracle(oracle):
             vcf = os.path.join(td, f"in_{field}.vcf")
             tsv = os.path.join(td, f"out_{field}.tsv")
             synth.write_vcf(vcf, co.codes, field=field)
-            r = subprocess.run([cli, vcf, tsv, "-f", field, "-s", "20"], capture_output=True, text=True,
-                               timeout=300)
+            r = subprocess.run([cli, vcf, tsv, "-f", field, "-s", "20", "-e", "ml"], capture_output=True,
+                               text=True, timeout=300)
             assert r.returncode == 0, r.stderr
             with open(tsv) as fh:
                 outs[field] = fh.read()
@@ -143,7 +143,8 @@ def test_cli_output_rows_equal_api_results(threads):
         vcf = os.path.join(td, "in.vcf")
         tsv = os.path.join(td, "out.tsv")
         synth.write_vcf(vcf, co.codes, field="GT")
-        r = subprocess.run([cli, vcf, tsv, "-t", str(threads)], capture_output=True, text=True, timeout=300)
+        r = subprocess.run([cli, vcf, tsv, "-t", str(threads), "-e", "ml"], capture_output=True, text=True,
+                           timeout=300)
         assert r.returncode == 0, r.stderr
         _, rows = _read_tsv(tsv)
     assert len(rows) == len(api) == 260 * 261 // 2
@@ -168,6 +169,12 @@ def test_cli_cls_estimator_matches_oracle(oracle):
                            text=True, timeout=300)
         assert r.returncode == 0, r.stderr
         head, rows = _read_tsv(tsv)
+        # CLS is the default for GT, as in the reference's CLI
+        tsv2 = os.path.join(td, "out_default.tsv")
+        r2 = subprocess.run([cli, vcf, tsv2, "-s", "20"], capture_output=True, text=True, timeout=300)
+        assert r2.returncode == 0, r2.stderr
+        assert open(tsv).read() == open(tsv2).read()
+        assert "Skipped 0 sites with missing data" in r2.stderr
     assert len(rows) == len(ref)
     jac = np.array([[float(v) for v in r[3:12]] for r in rows])
     obj = np.array([float(r[13]) for r in rows])
@@ -189,3 +196,25 @@ def test_autotune_and_launch_shape_leave_results_unchanged():
         small = est.relatedness()
         assert est.run_stats()["slots"] == 64
     assert _bitwise_equal(base, tuned) and _bitwise_equal(base, small)
+
+
+def test_cli_gt_default_drops_records_with_missing_calls(oracle):
+    co = synth.make_cohort(24, 4000, seed=45, missing=0.002, name="cli-cls-miss")
+    incomplete = int(np.any(co.codes == synth.MISSING, 0).sum())
+    assert 0 < incomplete < co.codes.shape[1]
+    cli = os.path.join(os.path.dirname(kb.__file__), "bin", "kestrel")
+    ref = oracle.cls_relatedness(co.codes)
+    with tempfile.TemporaryDirectory() as td:
+        vcf = os.path.join(td, "in.vcf")
+        tsv = os.path.join(td, "out.tsv")
+        synth.write_vcf(vcf, co.codes, field="GT")
+        r = subprocess.run([cli, vcf, tsv], capture_output=True, text=True, timeout=300)
+        assert r.returncode == 0, r.stderr
+        _, rows = _read_tsv(tsv)
+    assert f"Skipped {incomplete} sites with missing data" in r.stderr
+    assert f"Found {co.codes.shape[1] - incomplete} di-allelic sites" in r.stderr
+    jac = np.array([[float(v) for v in r[3:12]] for r in rows])
+    lc_ref = np.log10(ref["cond"])
+    ident = np.isfinite(lc_ref) & (lc_ref <= 4)
+    assert len(rows) == len(ref)
+    assert np.abs(jac - ref["jacquard"]).max(1)[ident].max() <= 1e-5

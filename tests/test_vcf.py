@@ -21,7 +21,7 @@ def py_parse(text, field="GT", af_info=False):
     """Reference parse: returns (codes [S, V], af or None, samples, counts)."""
     key = field
     samples, rows, afs = [], [], []
-    total = not_snp = multi = soft = 0
+    total = not_snp = multi = soft = with_missing = 0
     for line in text.split("\n"):
         line = line.rstrip("\r")
         if line.startswith("#CHROM"):
@@ -83,10 +83,12 @@ def py_parse(text, field="GT", af_info=False):
             if np.isnan(a):
                 raise ValueError("No AF info found")
             afs.append([1.0 - min(max(a, 0.0), 1.0), a])
+        with_missing += 3 in row
         rows.append(row)
     codes = np.array(rows, np.uint8).T.reshape(len(samples), len(rows)) if rows else np.zeros((len(samples), 0), np.uint8)
     return codes, (np.array(afs) if af_info else None), samples, \
-        {"records": total, "not_snp": not_snp, "multiallelic": multi, "soft_likelihoods": soft}
+        {"records": total, "not_snp": not_snp, "multiallelic": multi, "soft_likelihoods": soft,
+         "with_missing": with_missing}
 
 
 def write_bgzip(path, data: bytes, block=65280):
