@@ -109,6 +109,17 @@ int kg_load_genotypes_2bit(kg_ctx *ctx, const uint32_t *codes2,
  * them from the samples (the reference's -a estimate). */
 int kg_set_allele_frequencies(kg_ctx *ctx, const double *af);
 
+/* Tri- and tetra-allelic sites for kg_relatedness_gt (the reference's gt3 and
+ * gt4, src/coefficients.rs:180-224): gidx[s * row_stride + v] is sample s's
+ * genotype at site v as its index in the VCF order (j (j + 1) / 2 + i for
+ * alleles i <= j; 255 = missing, which drops the site), n_alleles[v] the site's
+ * allele count (3 or 4), af (n_sites x 4, or NULL to count them over all
+ * samples) its allele frequencies.  n_samples must be that of the loaded
+ * genotypes; loading genotypes again clears these, as does n_sites = 0.  The ML
+ * estimator (kg_relatedness) does not use them. */
+int kg_load_multiallelic(kg_ctx *ctx, const uint8_t *gidx, int64_t n_samples, int64_t n_sites,
+                         int64_t row_stride, const uint8_t *n_alleles, const double *af);
+
 /* All pairs (x, y), 0 <= x <= y < num_samples, in the reference's row order
  * (outputs[x] then y = x..num_samples-1, src/coefficients.rs:77-136).
  * num_samples < 0 means all samples; iterations is the SQP cap (-i, default
@@ -126,7 +137,8 @@ int kg_relatedness(kg_ctx *ctx, int64_t num_samples, uint64_t iterations,
  * or those of kg_set_allele_frequencies, with no maf filter.  Rows as
  * kg_relatedness: obj is the Brier score, iters the QP iterations (at most
  * `iterations`, src/coefficients.rs:207), cond the reduced-Hessian estimate of
- * Q at the solution.  Returns KG_ENOSITES when no site is complete. */
+ * Q at the solution.  Tri- and tetra-allelic sites of kg_load_multiallelic
+ * join Q, c and M.  Returns KG_ENOSITES when no biallelic site is complete. */
 int kg_relatedness_gt(kg_ctx *ctx, int64_t num_samples, uint64_t iterations,
                       kg_output *out, int64_t out_cap, int64_t *n_out);
 
@@ -280,14 +292,20 @@ int kg_run_cli(int argc, const char *const *argv);
 typedef struct kg_vcf kg_vcf;
 int kg_vcf_read(const char *path, const char *field, int af_info, int threads, kg_vcf **out);
 const char *kg_vcf_error(const kg_vcf *vcf);
-/* counts (optional, 5 entries): records, non-SNP records skipped,
- * multi-allelic records skipped, GL/PL rows that were not one-hot, kept
- * records with at least one missing call. */
+/* counts (optional, 7 entries): records, non-SNP records skipped (a base that
+ * is not A/C/G/T, or more than four bases), tri- and tetra-allelic records,
+ * GL/PL rows that were not one-hot, SNP records with at least one missing
+ * call, and (GT) the tri- and the tetra-allelic records kept. */
 int kg_vcf_info(const kg_vcf *vcf, int64_t *n_samples, int64_t *n_sites, uint64_t *counts);
 /* codes: n_samples x n_sites, sample-major (the layout kg_load_genotypes takes);
  * af: n_sites x 2 [REF, ALT] from INFO/AF (KG_EINVAL if it was not read).
  * Either may be NULL. */
 int kg_vcf_codes(const kg_vcf *vcf, uint8_t *codes, double *af);
+/* GT: the tri- and tetra-allelic records that every sample calls (counts[5] +
+ * counts[6] of them), the input of kg_load_multiallelic: gidx n_samples x
+ * that many genotype indices (sample-major), n_alleles one per record, af (4
+ * per record, KG_EINVAL if INFO/AF was not read).  Any may be NULL. */
+int kg_vcf_multiallelic(const kg_vcf *vcf, uint8_t *gidx, uint8_t *n_alleles, double *af);
 /* Sample name i (NULL when out of range). */
 const char *kg_vcf_sample(const kg_vcf *vcf, int64_t i);
 void kg_vcf_free(kg_vcf *vcf);

@@ -15,12 +15,14 @@ import warnings
 
 import numpy as np
 
-from ._lib import (KG_ENOSITES, KG_ETIMEOUT, KG_OK, KG_PREC_FP32C, KG_PREC_FP64, MISSING,
-                   OUTPUT_DTYPE, KestrelError, KgCohort, KgRunStats, lib, ptr)
+from ._lib import (KG_ECUDA, KG_EINVAL, KG_ENOMEM, KG_ENOSITES, KG_ENOTFOUND, KG_ENOTREADY, KG_ETIMEOUT, KG_OK,
+                   KG_PREC_FP32C, KG_PREC_FP64, MISSING, OUTPUT_DTYPE, KestrelError, KgCohort, KgRunStats, lib,
+                   ptr)
 
 __all__ = ["Coefficients", "relatedness_coefficients_gt", "relatedness_coefficients_gl", "read_vcf",
            "run_cli", "Estimator", "genotype_codes", "build_arrays", "KestrelError",
-           "OUTPUT_DTYPE", "MISSING", "KINSHIP_VECTOR"]
+           "OUTPUT_DTYPE", "MISSING", "KINSHIP_VECTOR", "KG_OK", "KG_EINVAL", "KG_ENOMEM", "KG_ECUDA",
+           "KG_ETIMEOUT", "KG_ENOSITES", "KG_ENOTREADY", "KG_ENOTFOUND", "KG_PREC_FP32C", "KG_PREC_FP64"]
 
 # Kinship as a linear function of Delta (src/cli.rs:150, src/lib.rs:127).
 KINSHIP_VECTOR = np.array([1.0, 0.0, 0.5, 0.0, 0.5, 0.0, 0.5, 0.25, 0.0])
@@ -139,6 +141,26 @@ class Estimator:
                 raise ValueError("allele_frequencies must be (sites, 2)")
             _check(self._L.kg_set_allele_frequencies(self._h, ptr(af)), self._h)
             self._af = af
+        return self
+
+    def load_multiallelic(self, genotype_indices: np.ndarray, n_alleles, allele_frequencies=None):
+        """Tri- and tetra-allelic sites for relatedness_gt: genotype indices u8
+        [samples, sites] in the VCF order (j (j + 1) / 2 + i, 255 = missing),
+        allele counts [sites] (3 or 4), frequencies [sites, 4] or None."""
+        g = np.ascontiguousarray(genotype_indices, dtype=np.uint8)
+        if g.ndim != 2 or g.shape[0] != self.n_samples:
+            raise ValueError("genotype_indices must be (samples, sites) with the loaded samples")
+        na = np.ascontiguousarray(n_alleles, dtype=np.uint8)
+        if na.shape != (g.shape[1],):
+            raise ValueError("n_alleles must have one entry per site")
+        af = None
+        if allele_frequencies is not None:
+            af = np.ascontiguousarray(allele_frequencies, dtype=np.float64)
+            if af.shape != (g.shape[1], 4):
+                raise ValueError("allele_frequencies must be (sites, 4)")
+        _check(self._L.kg_load_multiallelic(self._h, ptr(g), g.shape[0], g.shape[1], g.shape[1], ptr(na), ptr(af)),
+               self._h)
+        self._multi = (g, na, af)
         return self
 
     def relatedness(self, num_samples=None, iterations: int = 100, maf=None,
@@ -271,11 +293,16 @@ def relatedness_coefficients_gt(genotypes, allele_frequencies=None, threads=None
     return Coefficients(*build_arrays(rows, codes.shape[0]))
 
 
-def read_vcf(path, field: str = "GT", allele_freqs: str = "estimate", threads: int = 0):
+def read_vcf(path, field: str = "GT", allele_freqs: str = "estimate", threads: int = 0,
+             multiallelic: bool = False):
     """Reads a plain, gzip or bgzip VCF with the library's multithreaded reader
     (the CLI's): biallelic SNP records become genotype codes.  Returns
     (codes u8 [samples, sites], allele_frequencies f64 [sites, 2] or None,
-    sample names, counts dict).  allele_freqs "info" reads INFO/AF."""
+    sample names, counts dict).  allele_freqs "info" reads INFO/AF.  With
+    multiallelic (GT), a fifth item holds the tri- and tetra-allelic records
+    every sample calls: (genotype indices u8 [samples, sites], allele counts u8
+    [sites], allele frequencies f64 [sites, 4] or None), the arguments of
+    Estimator.load_multiallelic."""
     if allele_freqs not in ("estimate", "info"):
         raise ValueError("allele_freqs must be 'estimate' or 'info'")
     L = lib()
@@ -287,14 +314,23 @@ def read_vcf(path, field: str = "GT", allele_freqs: str = "estimate", threads: i
             msg = L.kg_vcf_error(h) if h.value else b"out of memory"
             raise KestrelError(st, msg.decode())
         ns, nv = ctypes.c_int64(), ctypes.c_int64()
-        counts = (ctypes.c_uint64 * 5)()
+        counts = (ctypes.c_uint64 * 7)()
         _check_vcf(L.kg_vcf_info(h, ctypes.byref(ns), ctypes.byref(nv), counts), L, h)
         codes = np.empty((ns.value, nv.value), np.uint8)
         af = np.empty((nv.value, 2)) if allele_freqs == "info" else None
         _check_vcf(L.kg_vcf_codes(h, ptr(codes), ptr(af)), L, h)
         names = [L.kg_vcf_sample(h, i).decode() for i in range(ns.value)]
-        return codes, af, names, {"records": counts[0], "not_snp": counts[1], "multiallelic": counts[2],
-                                  "soft_likelihoods": counts[3], "with_missing": counts[4]}
+        cd = {"records": counts[0], "not_snp": counts[1], "multiallelic": counts[2],
+              "soft_likelihoods": counts[3], "with_missing": counts[4], "tri_allelic": counts[5],
+              "tetra_allelic": counts[6]}
+        if not multiallelic:
+            return codes, af, names, cd
+        nm = counts[5] + counts[6]
+        mg = np.empty((ns.value, nm), np.uint8)
+        mal = np.empty(nm, np.uint8)
+        maf = np.empty((nm, 4)) if allele_freqs == "info" else None
+        _check_vcf(L.kg_vcf_multiallelic(h, ptr(mg), ptr(mal), ptr(maf)), L, h)
+        return codes, af, names, cd, (mg, mal, maf)
     finally:
         if h.value:
             L.kg_vcf_free(h)

@@ -52,6 +52,7 @@ struct kg_ctx {
     bool loaded = false;
     std::vector<double> af;
     bool af_set = false;
+    bool multi_af = false;                // kg_load_multiallelic gave frequencies
     kg::Workspace ws;
     kg::DevBuf dout;
     kg_run_stats last{};
@@ -406,6 +407,7 @@ int kg_load_genotypes(kg_ctx* c, const uint8_t* codes, int64_t n_samples, int64_
         c->cohort.n_samples = n_samples;
         c->cohort.n_sites = n_sites;
         c->cohort.n_kept = -1;
+        c->cohort.n_multi = 0;
         c->loaded = true;
         c->af_set = false;
         return KG_OK;
@@ -424,8 +426,44 @@ int kg_load_genotypes_2bit(kg_ctx* c, const uint32_t* codes2, const uint32_t* ob
         c->cohort.n_samples = n_samples;
         c->cohort.n_sites = n_sites;
         c->cohort.n_kept = -1;
+        c->cohort.n_multi = 0;
         c->loaded = true;
         c->af_set = false;
+        return KG_OK;
+    });
+}
+
+int kg_load_multiallelic(kg_ctx* c, const uint8_t* gidx, int64_t n_samples, int64_t n_sites, int64_t row_stride,
+                         const uint8_t* n_alleles, const double* af) {
+    if (!c) return KG_EINVAL;
+    if (!c->loaded) return set_err(c, KG_EINVAL, "load genotypes first");
+    if (n_sites == 0) {
+        c->cohort.n_multi = 0;
+        return KG_OK;
+    }
+    if (!gidx || !n_alleles || n_sites < 0 || row_stride < n_sites)
+        return set_err(c, KG_EINVAL, "gidx and n_alleles must be non-NULL with n_sites > 0 and row_stride >= n_sites");
+    if (n_samples != c->cohort.n_samples)
+        return set_err(c, KG_EINVAL, "n_samples must match the loaded genotypes");
+    return guarded(c, [&]() -> int {
+        int st = use_device(c);
+        if (st) return st;
+        kg::Cohort& co = c->cohort;
+        if (!budget_ok(c, (size_t)(n_samples * n_sites)))
+            return set_err(c, KG_ENOMEM, "multi-allelic genotypes exceed the memory budget");
+        if (co.mg.reserve((size_t)(n_samples * n_sites)) != cudaSuccess || co.malleles.reserve((size_t)n_sites) != cudaSuccess ||
+            (af && co.maf.reserve(sizeof(double) * 4 * n_sites) != cudaSuccess))
+            return set_err(c, KG_ENOMEM, "cannot allocate device multi-allelic genotypes");
+        cudaError_t e = cudaMemcpy2DAsync(co.mg.p, (size_t)n_sites, gidx, (size_t)row_stride, (size_t)n_sites,
+                                          (size_t)n_samples, cudaMemcpyHostToDevice, c->stream);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(co.malleles.p, n_alleles, (size_t)n_sites, cudaMemcpyHostToDevice, c->stream);
+        if (e == cudaSuccess && af)
+            e = cudaMemcpyAsync(co.maf.p, af, sizeof(double) * 4 * n_sites, cudaMemcpyHostToDevice, c->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+        if (e != cudaSuccess) return set_err(c, KG_ECUDA, std::string("upload: ") + cudaGetErrorString(e));
+        co.n_multi = n_sites;
+        c->multi_af = af != nullptr;
         return KG_OK;
     });
 }
@@ -530,6 +568,7 @@ int kg_relatedness_gt(kg_ctx* c, int64_t num_samples, uint64_t iterations, kg_ou
         st = kg::prepare_cohort(c->cohort, c->cohort.raw.as<uint8_t>(), c->cohort.n_samples,
                                 c->cohort.n_sites, c->cohort.n_sites, true,
                                 c->af_set ? c->af.data() : nullptr, -1.0, c->stream, err, true);
+        if (!st) st = kg::prepare_multi(c->cohort, c->multi_af, ns, c->stream, err);
         if (st) {
             cudaEventDestroy(ev0);
             cudaEventDestroy(ev1);
@@ -553,6 +592,7 @@ int kg_relatedness_gt(kg_ctx* c, int64_t num_samples, uint64_t iterations, kg_ou
         cudaEventDestroy(ev0);
         cudaEventDestroy(ev1);
         stats.launches += 9;  // count, freq, two scans, compact, pad, pack, Gram, Gram total
+        if (c->cohort.n_multi > 0) stats.launches += 4;   // multi-allelic frequencies, Gram, Gram total, rows
         if (st2 && !st) st = st2;
         stats.total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
         c->last = stats;

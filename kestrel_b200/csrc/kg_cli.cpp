@@ -278,13 +278,17 @@ extern "C" int kg_run_cli(int argc, const char* const* argv) {
     log_info("Parsed %s total sites", std::to_string(vcf.total));
     log_info("Skipped %s sites that were not SNPs", std::to_string(vcf.not_snp));
     if (o.cls) {
-        // the CLS estimator uses the sites every sample calls (src/vcf.rs:217-221)
+        // the CLS estimator uses the sites every sample calls, tri- and
+        // tetra-allelic ones included (src/vcf.rs:127-181, :217-221)
+        const uint64_t bi_missing = vcf.incomplete - (vcf.multi - vcf.tri - vcf.tetra);
         log_info("Skipped %s sites with missing data", std::to_string(vcf.incomplete));
-        log_info("Found %s di-allelic sites", std::to_string(vcf.n_sites - (int64_t)vcf.incomplete));
+        log_info("Found %s di-allelic sites", std::to_string(vcf.n_sites - (int64_t)bi_missing));
+        log_info("Found %s tri-allelic sites", std::to_string(vcf.tri));
+        log_info("Found %s tetra-allelic sites", std::to_string(vcf.tetra));
     } else {
         log_info("Found %s di-allelic sites", std::to_string(vcf.n_sites));
+        log_info("Skipped %s tri- or tetra-allelic sites (biallelic sites only)", std::to_string(vcf.multi));
     }
-    log_info("Skipped %s tri- or tetra-allelic sites (biallelic sites only)", std::to_string(vcf.multi));
     if (vcf.soft)
         log_info("%s likelihood entries were not one-hot; their most likely genotype was used",
                  std::to_string(vcf.soft));
@@ -313,6 +317,9 @@ extern "C" int kg_run_cli(int argc, const char* const* argv) {
     int st = 0;
     st = kg_load_genotypes(ctx, codes.data(), ns, nv, nv);
     if (!st && o.af_info) st = kg_set_allele_frequencies(ctx, af.data());
+    if (!st && o.cls && vcf.n_multi > 0)
+        st = kg_load_multiallelic(ctx, vcf.mcodes.data(), ns, vcf.n_multi, vcf.n_multi, vcf.malleles.data(),
+                                  o.af_info ? vcf.maf.data() : nullptr);
     int64_t nout = 0;
     if (!st) {
         if (o.cls) st = kg_relatedness_gt(ctx, nsel, o.iterations, out.data(), np, &nout);

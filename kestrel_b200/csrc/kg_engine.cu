@@ -65,7 +65,8 @@ int DevBuf::reserve(size_t n) {
 size_t Cohort::device_bytes() const {
     return raw.bytes + af.bytes + rc.bytes + oc.bytes + keep.bytes + kidx.bytes + bsum.bytes +
            nkept.bytes + pfull.bytes + qfull.bytes + p32.bytes + p64.bytes + q64.bytes +
-           site_of.bytes + planes.bytes;
+           site_of.bytes + planes.bytes + cls_q.bytes + cls_part.bytes + mg.bytes + malleles.bytes + maf.bytes +
+           mfreq.bytes + mkeep.bytes + mcount.bytes + mpart.bytes + cmulti.bytes;
 }
 
 const char* engine_version() { return "kestrel-b200 0.1.0 (sm_100a)"; }
@@ -257,18 +258,152 @@ __global__ void __launch_bounds__(GRAM_THREADS) cls_gram_kernel(const double* __
     }
 }
 
+// Q from the per-block partials of the biallelic sites and, when mpart is not
+// NULL, those of the multi-allelic sites after them, divided by the sites used.
 __global__ void cls_gram_final_kernel(const double* __restrict__ part, const int32_t* __restrict__ nkept,
+                                      const double* __restrict__ mpart, const int32_t* __restrict__ mcount,
                                       double* __restrict__ Q) {
     const int a = threadIdx.x;
     if (a >= 45) return;
     double s = 0.0;
     for (int b = 0; b < GRAM_BLOCKS; b++) s += part[b * 45 + a];
+    int64_t m = nkept[0];
+    if (mpart) {
+        for (int b = 0; b < GRAM_BLOCKS; b++) s += mpart[b * 45 + a];
+        m += mcount[0];
+    }
     int i = 0, rem = a;
     while (rem >= 9 - i) { rem -= 9 - i; i++; }
     const int j = i + rem;
-    const double v = s / (double)nkept[0];
+    const double v = s / (double)m;
     Q[i * 9 + j] = v;
     Q[j * 9 + i] = v;
+}
+
+// ---- CLS: tri- and tetra-allelic sites (the reference's gt3 / gt4 of
+// src/coefficients.rs:180-224)
+
+// Per site: used when every sample has a call (an index of 255 is missing; the
+// scan stops there, as the reader drops such a record), frequencies are allele
+// counts / (2 n_samples) (src/wrapper.rs:412-428) or the caller's; an index
+// beyond the site's genotypes or an allele count other than 3 or 4 sets the
+// bad flag.
+__global__ void multi_freq_kernel(const uint8_t* __restrict__ mg, const uint8_t* __restrict__ mal,
+                                  const double* __restrict__ maf, int64_t n_samples, int64_t n_multi,
+                                  double* __restrict__ mfreq, uint8_t* __restrict__ mkeep,
+                                  int32_t* __restrict__ mcount) {
+    const int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= n_multi) return;
+    const int na = mal[v];
+    const int ng = na * (na + 1) / 2;
+    bool bad = na < 3 || na > 4, complete = true;
+    int64_t c0 = 0, c1 = 0, c2 = 0, c3 = 0;
+    for (int64_t s = 0; s < n_samples && !bad; s++) {
+        const int g = mg[s * n_multi + v];   // adjacent threads read adjacent sites
+        if (g == 255) {
+            complete = false;
+            break;
+        }
+        if (g >= ng) {
+            bad = true;
+            break;
+        }
+        int i, j;
+        genotype_alleles(g, i, j);
+        c0 += (i == 0) + (j == 0);
+        c1 += (i == 1) + (j == 1);
+        c2 += (i == 2) + (j == 2);
+        c3 += (i == 3) + (j == 3);
+    }
+    const bool use = complete && !bad;
+    const int64_t cnt[4] = {c0, c1, c2, c3};
+#pragma unroll
+    for (int a = 0; a < 4; a++)
+        mfreq[4 * v + a] = !use ? 0.0 : maf ? maf[4 * v + a] : a < na ? (double)cnt[a] / (double)(2 * n_samples) : 0.0;
+    mkeep[v] = use ? 1 : 0;
+    if (use) atomicAdd(&mcount[0], 1);
+    if (bad) atomicOr(&mcount[1], 1);
+}
+
+// Per-block partial sums of sum over used sites and all (gx, gy) of m m^T,
+// in the layout of cls_gram_kernel.
+__global__ void __launch_bounds__(GRAM_THREADS) multi_gram_kernel(const uint8_t* __restrict__ mal,
+                                                                  const double* __restrict__ mfreq,
+                                                                  const uint8_t* __restrict__ mkeep,
+                                                                  int64_t n_multi, double* __restrict__ part) {
+    __shared__ double sh[45][GRAM_THREADS];
+    double h[45];
+#pragma unroll
+    for (int a = 0; a < 45; a++) h[a] = 0.0;
+    for (int64_t k = (int64_t)blockIdx.x * GRAM_THREADS + threadIdx.x; k < n_multi;
+         k += (int64_t)GRAM_BLOCKS * GRAM_THREADS) {
+        if (!mkeep[k]) continue;
+        const int na = mal[k], ng = na * (na + 1) / 2;
+        const double f0 = mfreq[4 * k], f1 = mfreq[4 * k + 1], f2 = mfreq[4 * k + 2], f3 = mfreq[4 * k + 3];
+        for (int gx = 0; gx < ng; gx++)
+            for (int gy = 0; gy < ng; gy++) {
+                int i, j, a1, b1;
+                genotype_alleles(gx, i, j);
+                genotype_alleles(gy, a1, b1);
+                double row[9];
+                iis_row(i, j, a1, b1, f0, f1, f2, f3, row);
+                int a = 0;
+#pragma unroll
+                for (int r = 0; r < 9; r++)
+#pragma unroll
+                    for (int t = r; t < 9; t++) h[a++] += row[r] * row[t];
+            }
+    }
+#pragma unroll
+    for (int a = 0; a < 45; a++) sh[a][threadIdx.x] = h[a];
+    __syncthreads();
+    if (threadIdx.x < 45) {
+        double s = 0.0;
+        for (int t = 0; t < GRAM_THREADS; t++) s += sh[threadIdx.x][t];
+        part[(int64_t)blockIdx.x * 45 + threadIdx.x] = s;
+    }
+}
+
+// Warp per output row r of the first ns samples (x-major, y >= x, the
+// reference's order): the 9 sums over used multi-allelic sites of
+// m[gx][gy], lanes striding over the sites, then a fixed butterfly reduction.
+__global__ void multi_c_kernel(const uint8_t* __restrict__ mg, const double* __restrict__ mfreq,
+                               const uint8_t* __restrict__ mkeep, int64_t n_multi, int64_t ns, int64_t n_rows,
+                               double* __restrict__ cm) {
+    const int lane = threadIdx.x & 31;
+    const int64_t w0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t r = w0; r < n_rows; r += nw) {
+        int64_t lo = 0, hi = ns - 1;   // the largest x whose first row is <= r
+        while (lo < hi) {
+            const int64_t mid = (lo + hi + 1) / 2;
+            if (mid * ns - mid * (mid - 1) / 2 <= r) lo = mid;
+            else hi = mid - 1;
+        }
+        const int64_t x = lo, y = x + (r - (x * ns - x * (x - 1) / 2));
+        const uint8_t* gxr = mg + x * n_multi;
+        const uint8_t* gyr = mg + y * n_multi;
+        double acc[9];
+#pragma unroll
+        for (int t = 0; t < 9; t++) acc[t] = 0.0;
+        for (int64_t v = lane; v < n_multi; v += 32) {
+            if (!mkeep[v]) continue;
+            int i, j, k, l;
+            genotype_alleles(gxr[v], i, j);
+            genotype_alleles(gyr[v], k, l);
+            double row[9];
+            iis_row(i, j, k, l, mfreq[4 * v], mfreq[4 * v + 1], mfreq[4 * v + 2], mfreq[4 * v + 3], row);
+#pragma unroll
+            for (int t = 0; t < 9; t++) acc[t] += row[t];
+        }
+#pragma unroll
+        for (int t = 0; t < 9; t++)
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) acc[t] += __shfl_xor_sync(0xffffffffu, acc[t], off);
+        if (lane == 0)
+#pragma unroll
+            for (int t = 0; t < 9; t++) cm[r * 9 + t] = acc[t];
+    }
 }
 
 // Warp per (row, 32-site word): lanes fetch the codes of 32 kept sites and two
@@ -399,8 +534,8 @@ int prepare_cohort(Cohort& c, const uint8_t* codes, int64_t n_samples, int64_t n
         KG_CUDA_TRY((cudaError_t)c.cls_q.reserve(sizeof(double) * 81));
         cls_gram_kernel<<<GRAM_BLOCKS, GRAM_THREADS, 0, st>>>(c.p64.as<double>(), c.q64.as<double>(),
                                                               c.nkept.as<int32_t>(), c.cls_part.as<double>());
-        cls_gram_final_kernel<<<1, 64, 0, st>>>(c.cls_part.as<double>(), c.nkept.as<int32_t>(),
-                                                c.cls_q.as<double>());
+        cls_gram_final_kernel<<<1, 64, 0, st>>>(c.cls_part.as<double>(), c.nkept.as<int32_t>(), nullptr,
+                                                nullptr, c.cls_q.as<double>());
     }
     KG_CUDA_TRY(cudaGetLastError());
     int32_t h[4];
@@ -584,6 +719,42 @@ jacquard_pair_kernel(PairLaunch L) {
 
 static_assert(sizeof(kg_output) == 14 * 8, "kg_output must be 112 bytes");
 
+int prepare_multi(Cohort& c, bool have_af, int64_t num_samples, cudaStream_t st, std::string& err) {
+    c.n_multi_kept = 0;
+    if (c.n_multi <= 0) return KG_OK;
+    const int64_t n = c.n_multi, rows = num_samples * (num_samples + 1) / 2;
+    KG_CUDA_TRY((cudaError_t)c.mfreq.reserve(sizeof(double) * 4 * n));
+    KG_CUDA_TRY((cudaError_t)c.mkeep.reserve((size_t)n));
+    KG_CUDA_TRY((cudaError_t)c.mcount.reserve(sizeof(int32_t) * 2));
+    KG_CUDA_TRY((cudaError_t)c.mpart.reserve(sizeof(double) * GRAM_BLOCKS * 45));
+    KG_CUDA_TRY((cudaError_t)c.cmulti.reserve(sizeof(double) * 9 * rows));
+    KG_CUDA_TRY(cudaMemsetAsync(c.mcount.p, 0, sizeof(int32_t) * 2, st));
+    multi_freq_kernel<<<grid_for(n, 256), 256, 0, st>>>(c.mg.as<uint8_t>(), c.malleles.as<uint8_t>(),
+                                                         have_af ? c.maf.as<double>() : nullptr, c.n_samples, n,
+                                                         c.mfreq.as<double>(), c.mkeep.as<uint8_t>(),
+                                                         c.mcount.as<int32_t>());
+    multi_gram_kernel<<<GRAM_BLOCKS, GRAM_THREADS, 0, st>>>(c.malleles.as<uint8_t>(), c.mfreq.as<double>(),
+                                                            c.mkeep.as<uint8_t>(), n, c.mpart.as<double>());
+    cls_gram_final_kernel<<<1, 64, 0, st>>>(c.cls_part.as<double>(), c.nkept.as<int32_t>(), c.mpart.as<double>(),
+                                            c.mcount.as<int32_t>(), c.cls_q.as<double>());
+    {
+        const int blocks = (int)std::min<int64_t>(ceil_div(rows * 32, 256), 148 * 8);
+        multi_c_kernel<<<blocks, 256, 0, st>>>(c.mg.as<uint8_t>(), c.mfreq.as<double>(), c.mkeep.as<uint8_t>(), n,
+                                               num_samples, rows, c.cmulti.as<double>());
+    }
+    KG_CUDA_TRY(cudaGetLastError());
+    int32_t h[2];
+    KG_CUDA_TRY(cudaMemcpyAsync(h, c.mcount.p, sizeof(h), cudaMemcpyDeviceToHost, st));
+    KG_CUDA_TRY(cudaStreamSynchronize(st));
+    if (h[1]) {
+        err = "multi-allelic genotype indices must be below the site's genotype count (or 255, missing), "
+              "allele counts 3 or 4";
+        return KG_EINVAL;
+    }
+    c.n_multi_kept = h[0];
+    return KG_OK;
+}
+
 CohortDev make_cohort_dev(const PairJob& jb, uint64_t iterations) {
     const Cohort& pn = *jb.panel;
     CohortDev d;
@@ -604,6 +775,9 @@ CohortDev make_cohort_dev(const PairJob& jb, uint64_t iterations) {
     d.out = jb.d_out;
     d.max_iter = jb.iterations ? jb.iterations : iterations;
     d.cls_q = jb.method == ESTIMATOR_CLS ? pn.cls_q.as<double>() : nullptr;
+    const bool multi = jb.method == ESTIMATOR_CLS && pn.n_multi_kept > 0;
+    d.cls_cmulti = multi ? pn.cmulti.as<double>() : nullptr;
+    d.cls_m = (double)pn.n_kept + (multi ? (double)pn.n_multi_kept : 0.0);
     return d;
 }
 

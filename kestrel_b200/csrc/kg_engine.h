@@ -78,6 +78,17 @@ struct Cohort {
     bool cls = false;          // prepared for the CLS estimator (complete sites, counts over all samples)
     DevBuf cls_q;              // CLS: the 9 x 9 quadratic matrix Q, row-major double
     DevBuf cls_part;           // CLS: per-block partial sums of Q's upper triangle
+    // CLS: tri- and tetra-allelic sites (the reference's gt3 / gt4)
+    int64_t n_multi = 0;       // loaded sites
+    int64_t n_multi_kept = -1; // sites every sample calls (read back after preparation)
+    DevBuf mg;                 // uint8 genotype indices (VCF order, 255 = missing), n_samples x n_multi
+    DevBuf malleles;           // uint8 allele count per site (3 or 4)
+    DevBuf maf;                // caller frequencies, n_multi x 4 (optional)
+    DevBuf mfreq;              // double frequencies used, n_multi x 4
+    DevBuf mkeep;              // uint8 site used
+    DevBuf mcount;             // int32[2]: sites used, bad-index flag
+    DevBuf mpart;              // per-block partial sums of their Q terms
+    DevBuf cmulti;             // per output row, the 9 summed rows of the pair's multi-allelic sites
     size_t device_bytes() const;
 };
 
@@ -88,6 +99,13 @@ struct Cohort {
 int prepare_cohort(Cohort& c, const uint8_t* codes, int64_t n_samples, int64_t n_sites,
                    int64_t row_stride, bool codes_on_device, const double* af, double maf,
                    cudaStream_t st, std::string& err, bool cls = false);
+
+// After prepare_cohort(..., cls = true): adds the cohort's tri- and
+// tetra-allelic sites (c.mg, c.malleles, c.maf uploaded, c.n_multi set) to the
+// CLS estimator of the first num_samples samples: their frequencies (counts
+// over all samples unless c.maf), Q over all sites, and each output row's
+// summed rows (c.cmulti).  Sets c.n_multi_kept.
+int prepare_multi(Cohort& c, bool have_af, int64_t num_samples, cudaStream_t st, std::string& err);
 
 // Unpacks the VCF reader's 2-bit codes + observed mask into device byte codes.
 int unpack_2bit(DevBuf& raw, const uint32_t* codes2, const uint32_t* observed, int64_t n_samples,

@@ -103,6 +103,8 @@ __global__ void noalloc_table_kernel(kg::CohortDev* table, const uint2* planes, 
     d.out = out;
     d.max_iter = 0;   // the single-kernel engine takes the limit from its launch
     d.cls_q = nullptr;
+    d.cls_cmulti = nullptr;
+    d.cls_m = (double)nkept[0];
     *table = d;
 }
 

@@ -73,12 +73,58 @@ struct CohortDev {
     kg_output* out;          // rows in the reference's order
     uint64_t max_iter;       // SQP iteration limit of this cohort's pairs (CLS: QP iterations)
     const double* cls_q;     // CLS: the 9 x 9 quadratic matrix Q (row-major)
+    const double* cls_cmulti;  // CLS: per output row, the 9 summed rows of its tri-/tetra-allelic sites (or NULL)
+    double cls_m;            // CLS: the sites M that Q and c are divided by (biallelic + multi-allelic)
 };
 
 // The estimators: maximum likelihood (the GL/PL path, src/coefficients.rs:40-141)
 // and the hard-call conditional least squares with the Brier objective (the
 // reference's default -f GT, src/coefficients.rs:166-278).
 enum : int { ESTIMATOR_ML = 0, ESTIMATOR_CLS = 1 };
+
+// The two alleles (i <= j) of a genotype index in the VCF order, j (j + 1) / 2 + i
+// (src/coefficients.rs:19-38); indices 0..9 cover up to four alleles.
+__host__ __device__ inline void genotype_alleles(int g, int& i, int& j) {
+    j = g >= 6 ? 3 : g >= 3 ? 2 : g >= 1 ? 1 : 0;
+    i = g - j * (j + 1) / 2;
+}
+
+// m[gx][gy] of a site with any number of alleles (frequencies f): the nine
+// conditional probabilities of the joint genotypes (i, j), (k, l) given each
+// Jacquard state, the table of src/iis.rs:279-462, evaluated from its
+// definition: every ordering of each unordered genotype (x1 x2 = a1 a2, y1 y2 =
+// b1 b2) adds, per state, the product over the state's identity classes of the
+// class's allele frequency, when all of a class's members carry one allele.
+// Classes: 1 {x1 x2 y1 y2}; 2 {x1 x2}{y1 y2}; 3 {x1 x2 y1}{y2}; 4 {x1 x2}{y1}{y2};
+// 5 {x1 y1 y2}{x2}; 6 {y1 y2}{x1}{x2}; 7 {x1 y1}{x2 y2}; 8 {x1 y1}{x2}{y2};
+// 9 all apart.
+__host__ __device__ inline void iis_row(int i, int j, int k, int l, double f0, double f1, double f2, double f3,
+                                        double* row) {
+    // frequencies by allele without an indexed array (registers, not local memory)
+    auto F = [=](int a) { return a == 0 ? f0 : a == 1 ? f1 : a == 2 ? f2 : f3; };
+#pragma unroll
+    for (int s = 0; s < 9; s++) row[s] = 0.0;
+    const int nx = i == j ? 1 : 2, ny = k == l ? 1 : 2;
+    for (int u = 0; u < nx; u++) {
+        const int a1 = u ? j : i, a2 = u ? i : j;
+        const double fa1 = F(a1), fa2 = F(a2);
+        for (int w = 0; w < ny; w++) {
+            const int b1 = w ? l : k, b2 = w ? k : l;
+            const double fb1 = F(b1), fb2 = F(b2);
+            const bool xx = a1 == a2, yy = b1 == b2, s1 = a1 == b1, s2 = a2 == b2;
+            const double xy = fa1 * fa2;
+            if (xx && yy && s1) row[0] += fa1;
+            if (xx && yy) row[1] += fa1 * fb1;
+            if (xx && s1) row[2] += fa1 * fb2;
+            if (xx) row[3] += fa1 * fb1 * fb2;
+            if (yy && s1) row[4] += fb1 * fa2;
+            if (yy) row[5] += fb1 * xy;
+            if (s1 && s2) row[6] += xy;
+            if (s1) row[7] += xy * fb2;
+            row[8] += xy * fb1 * fb2;
+        }
+    }
+}
 
 // m[gx][gy] of one biallelic site for the CLS estimator: src/iis.rs:279-462
 // with the biallelic joint-genotype modes of src/conditional.rs:6-55 (allele 0

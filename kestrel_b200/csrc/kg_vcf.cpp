@@ -21,6 +21,7 @@
 #include <memory>
 #include <string_view>
 #include <thread>
+#include <utility>
 
 namespace kg {
 namespace {
@@ -276,6 +277,40 @@ bool parse_call(std::string_view v, char field, uint8_t& code, uint64_t& soft) {
     return true;
 }
 
+// Genotype index (VCF order, j (j + 1) / 2 + i for alleles i <= j) of a GT
+// value at a site with n_alleles alleles; 255 when an allele is missing.
+// False when the value is not a diploid call of the site's alleles.
+bool parse_gt_index(std::string_view v, int n_alleles, uint8_t& g) {
+    int a[2] = {0, 0};
+    int k = 0;
+    size_t b = 0;
+    bool missing = false;
+    for (size_t i = 0; i <= v.size(); i++) {
+        if (i == v.size() || v[i] == '/' || v[i] == '|') {
+            const std::string_view t = v.substr(b, i - b);
+            if (k >= 2) return false;
+            if (t == ".") {
+                missing = true;
+                a[k++] = 0;
+            } else {
+                int x = 0;
+                const auto r = std::from_chars(t.data(), t.data() + t.size(), x);
+                if (r.ec != std::errc() || r.ptr != t.data() + t.size() || x < 0 || x >= n_alleles) return false;
+                a[k++] = x;
+            }
+            b = i + 1;
+        }
+    }
+    if (missing) {
+        g = 255;
+        return true;
+    }
+    if (k != 2) return false;
+    const int lo = std::min(a[0], a[1]), hi = std::max(a[0], a[1]);
+    g = (uint8_t)(hi * (hi + 1) / 2 + lo);
+    return true;
+}
+
 // Allele digit of a three-character GT value: 0, 1, 2 for '.', -1 otherwise.
 struct AlleleTable {
     int8_t a[256];
@@ -323,6 +358,12 @@ struct Chunk {
     std::vector<double> af;
     uint64_t total = 0, not_snp = 0, multi = 0, soft = 0, incomplete = 0;
     int64_t kept = 0;
+    // GT: tri- and tetra-allelic records every sample calls
+    std::vector<uint8_t> mrows;  // kept records x samples, genotype indices
+    std::vector<uint8_t> malleles;
+    std::vector<double> maf;     // 4 per record
+    int64_t mkept = 0;
+    uint64_t tri = 0, tetra = 0;
     bool failed = false;
     uint64_t fail_rec = 0;       // 1-based record index within the chunk
     std::string fail_kind;       // message with %R for the global record number
@@ -373,13 +414,17 @@ void parse_chunk(Chunk& c, char field, bool af_info, size_t n_samples) {
                 ab = i + 1;
             }
         }
-        if (!snp) {
+        // REF and every ALT one base; more than four bases is not a SNP
+        // (src/vcf.rs:424-444 with the arms of :127-165)
+        const int n_bases = 1 + (int)n_alts;
+        if (!snp || n_bases > 4) {
             c.not_snp++;
             p = next;
             continue;
         }
-        if (n_alts != 1) {
-            c.multi++;
+        const bool multi = n_bases > 2;
+        if (multi) c.multi++;
+        if (multi && field != 'T') {
             p = next;
             continue;
         }
@@ -403,6 +448,101 @@ void parse_chunk(Chunk& c, char field, bool af_info, size_t n_samples) {
         if (fi < 0) {
             fail("No " + std::string(key) + " data found");
             return;
+        }
+        // the fi-th ':' subfield of the sample starting at s ("." when the
+        // value has fewer); s moves to the next sample
+        auto sample_value = [&](const char*& s) {
+            const char* t = static_cast<const char*>(std::memchr(s, '\t', (size_t)(le - s)));
+            const char* se = t ? t : le;
+            const char* a = s;
+            int idx = 0;
+            while (idx < fi) {
+                const char* cpos = static_cast<const char*>(std::memchr(a, ':', (size_t)(se - a)));
+                if (!cpos) break;
+                a = cpos + 1;
+                idx++;
+            }
+            std::string_view v(".");
+            if (idx == fi) {
+                const char* cpos = static_cast<const char*>(std::memchr(a, ':', (size_t)(se - a)));
+                v = std::string_view(a, (size_t)((cpos ? cpos : se) - a));
+            }
+            s = t ? t + 1 : le;
+            return v;
+        };
+        if (multi) {
+            // genotype indices; the first missing call skips the record
+            // (src/vcf.rs:196-236)
+            const size_t mb = c.mrows.size();
+            c.mrows.resize(mb + n_samples);
+            const char* s = col[9];
+            bool missing = false;
+            for (size_t k = 0; k < n_samples && !missing; k++) {
+                const std::string_view v = sample_value(s);
+                uint8_t g = 0;
+                if (!parse_gt_index(v, n_bases, g)) {
+                    fail("Value " + std::string(v) + " is not a valid GT");
+                    return;
+                }
+                missing = g == 255;
+                c.mrows[mb + k] = g;
+            }
+            if (missing) {
+                c.mrows.resize(mb);
+                c.incomplete++;
+                p = next;
+                continue;
+            }
+            if (af_info) {
+                // INFO/AF: one value per ALT; REF = 1 - clamp(sum) (src/vcf.rs:446-482)
+                const std::string_view info = field_of(7);
+                std::string_view list;
+                bool found = false;
+                size_t ib = 0;
+                for (size_t i = 0; i <= info.size(); i++) {
+                    if (i == info.size() || info[i] == ';') {
+                        const std::string_view kv = info.substr(ib, i - ib);
+                        if (kv.size() >= 3 && kv.substr(0, 3) == "AF=") {
+                            list = kv.substr(3);
+                            found = true;
+                        }
+                        ib = i + 1;
+                    }
+                }
+                if (!found) {
+                    fail("No AF info found");
+                    return;
+                }
+                double f[4] = {0.0, 0.0, 0.0, 0.0};
+                int n_af = 1;
+                double alt_sum = 0.0;
+                size_t lb = 0;
+                for (size_t i = 0; i <= list.size(); i++) {
+                    if (i == list.size() || list[i] == ',') {
+                        if (n_af >= n_bases) {
+                            fail("Too many allele frequencies!");
+                            return;
+                        }
+                        const std::string num(list.substr(lb, i - lb));
+                        f[n_af] = std::strtod(num.c_str(), nullptr);
+                        alt_sum += f[n_af];
+                        n_af++;
+                        lb = i + 1;
+                    }
+                }
+                if (n_af != n_bases) {
+                    fail("Not enough allele frequencies!");
+                    return;
+                }
+                f[0] = 1.0 - std::min(std::max(alt_sum, 0.0), 1.0);
+                c.maf.insert(c.maf.end(), f, f + 4);
+            }
+            c.malleles.push_back((uint8_t)n_bases);
+            if (n_bases == 3) c.tri++;
+            else c.tetra++;
+            c.mkept++;
+            p = next;
+            continue;
         }
         const size_t base = c.rows.size();
         if (base == 0) {
@@ -431,27 +571,11 @@ void parse_chunk(Chunk& c, char field, bool af_info, size_t n_samples) {
                     continue;
                 }
             }
-            const char* t = static_cast<const char*>(std::memchr(s, '\t', (size_t)(le - s)));
-            const char* se = t ? t : le;
-            // the fi-th ':' subfield ("." when the value has fewer)
-            const char* a = s;
-            int idx = 0;
-            while (idx < fi) {
-                const char* cpos = static_cast<const char*>(std::memchr(a, ':', (size_t)(se - a)));
-                if (!cpos) break;
-                a = cpos + 1;
-                idx++;
-            }
-            std::string_view v(".");
-            if (idx == fi) {
-                const char* cpos = static_cast<const char*>(std::memchr(a, ':', (size_t)(se - a)));
-                v = std::string_view(a, (size_t)((cpos ? cpos : se) - a));
-            }
+            const std::string_view v = sample_value(s);
             if (!parse_call(v, field, c.rows[base + k], c.soft)) {
                 fail("Value " + std::string(v) + " is not a valid " + std::string(key));
                 return;
             }
-            s = t ? t + 1 : le;
         }
         if (std::memchr(c.rows.data() + base, 3, n_samples)) c.incomplete++;
         if (af_info) {
@@ -479,6 +603,43 @@ void parse_chunk(Chunk& c, char field, bool af_info, size_t n_samples) {
         c.kept++;
         p = next;
     }
+}
+
+// Sample-major codes[s * nv + v] from the chunks' record-major rows (rows_of(c)
+// gives a chunk's rows and record count; records in chunk order): each thread
+// a range of samples (a multiple of 8), 8 x 8 tiles of records x samples
+// transposed in 64-bit words.
+template <class RowsOf>
+void transpose_chunks(int threads, size_t ns, int64_t nv, uint8_t* codes, const std::vector<Chunk>& chunks,
+                      RowsOf rows_of) {
+    const int n_chunks = (int)chunks.size();
+    std::vector<int64_t> first((size_t)n_chunks + 1, 0);
+    for (int i = 0; i < n_chunks; i++) first[i + 1] = first[i] + rows_of(chunks[i]).second;
+    const int64_t n_groups = ((int64_t)ns + 7) / 8;
+    parallel_for(threads, n_groups, [&](int, int64_t g0, int64_t g1) {
+        const int64_t s0 = g0 * 8, s1 = std::min<int64_t>((int64_t)ns, g1 * 8);
+        for (int i = 0; i < n_chunks; i++) {
+            const auto rc = rows_of(chunks[i]);
+            const uint8_t* rows = rc.first;
+            const int64_t kept = rc.second;
+            for (int64_t b0 = 0; b0 < kept; b0 += 64) {
+                const int64_t b1 = std::min<int64_t>(kept, b0 + 64);
+                for (int64_t s = s0; s < s1; s += 8) {
+                    int64_t v = b0;
+                    if (s + 8 <= s1) {
+                        for (; v + 8 <= b1; v += 8) {
+                            uint64_t r[8];
+                            for (int k = 0; k < 8; k++) std::memcpy(&r[k], rows + (v + k) * (int64_t)ns + s, 8);
+                            transpose8x8(r);
+                            for (int k = 0; k < 8; k++) std::memcpy(codes + (s + k) * nv + first[i] + v, &r[k], 8);
+                        }
+                    }
+                    for (int64_t t = s; t < std::min<int64_t>(s1, s + 8); t++)
+                        for (int64_t w = v; w < b1; w++) codes[t * nv + first[i] + w] = rows[w * (int64_t)ns + t];
+                }
+            }
+        }
+    });
 }
 
 }  // namespace
@@ -549,37 +710,22 @@ int read_vcf(const std::string& path, char field, bool af_info, int threads, Vcf
         out.incomplete += c.incomplete;
         out.n_sites += c.kept;
     }
-    // sample-major codes: each thread a range of samples (a multiple of 8),
-    // 8 x 8 tiles of sites x samples transposed in 64-bit words
+    // sample-major codes of the biallelic and of the multi-allelic records
     const int64_t nv = out.n_sites;
     out.codes.allocate((size_t)(nv * (int64_t)ns));
-    std::vector<int64_t> first((size_t)n_chunks + 1, 0);
-    for (int i = 0; i < n_chunks; i++) first[i + 1] = first[i] + chunks[i].kept;
-    const int64_t n_groups = ((int64_t)ns + 7) / 8;
-    parallel_for(threads, n_groups, [&](int, int64_t g0, int64_t g1) {
-        const int64_t s0 = g0 * 8, s1 = std::min<int64_t>((int64_t)ns, g1 * 8);
-        uint8_t* codes = out.codes.data();
-        for (int i = 0; i < n_chunks; i++) {
-            const Chunk& c = chunks[i];
-            const uint8_t* rows = c.rows.data();
-            for (int64_t b0 = 0; b0 < c.kept; b0 += 64) {
-                const int64_t b1 = std::min<int64_t>(c.kept, b0 + 64);
-                for (int64_t s = s0; s < s1; s += 8) {
-                    int64_t v = b0;
-                    if (s + 8 <= s1) {
-                        for (; v + 8 <= b1; v += 8) {
-                            uint64_t r[8];
-                            for (int k = 0; k < 8; k++) std::memcpy(&r[k], rows + (v + k) * (int64_t)ns + s, 8);
-                            transpose8x8(r);
-                            for (int k = 0; k < 8; k++) std::memcpy(codes + (s + k) * nv + first[i] + v, &r[k], 8);
-                        }
-                    }
-                    for (int64_t t = s; t < std::min<int64_t>(s1, s + 8); t++)
-                        for (int64_t w = v; w < b1; w++) codes[t * nv + first[i] + w] = rows[w * (int64_t)ns + t];
-                }
-            }
-        }
-    });
+    transpose_chunks(threads, ns, nv, out.codes.data(), chunks,
+                     [](const Chunk& c) { return std::make_pair(c.rows.data(), c.kept); });
+    out.n_multi = 0;
+    for (auto& c : chunks) out.n_multi += c.mkept;
+    out.mcodes.allocate((size_t)(out.n_multi * (int64_t)ns));
+    transpose_chunks(threads, ns, out.n_multi, out.mcodes.data(), chunks,
+                     [](const Chunk& c) { return std::make_pair(c.mrows.data(), c.mkept); });
+    for (auto& c : chunks) {
+        out.malleles.insert(out.malleles.end(), c.malleles.begin(), c.malleles.end());
+        out.maf.insert(out.maf.end(), c.maf.begin(), c.maf.end());
+        out.tri += c.tri;
+        out.tetra += c.tetra;
+    }
     if (af_info) {
         out.af.reserve((size_t)(2 * nv));
         for (auto& c : chunks) out.af.insert(out.af.end(), c.af.begin(), c.af.end());
@@ -638,6 +784,8 @@ extern "C" int kg_vcf_info(const kg_vcf* v, int64_t* n_samples, int64_t* n_sites
         counts[2] = v->d.multi;
         counts[3] = v->d.soft;
         counts[4] = v->d.incomplete;
+        counts[5] = v->d.tri;
+        counts[6] = v->d.tetra;
     }
     return KG_OK;
 }
@@ -648,6 +796,17 @@ extern "C" int kg_vcf_codes(const kg_vcf* v, uint8_t* codes, double* af) {
     if (af) {
         if (v->d.af.empty()) return KG_EINVAL;
         std::memcpy(af, v->d.af.data(), sizeof(double) * v->d.af.size());
+    }
+    return KG_OK;
+}
+
+extern "C" int kg_vcf_multiallelic(const kg_vcf* v, uint8_t* gidx, uint8_t* n_alleles, double* af) {
+    if (!v) return KG_EINVAL;
+    if (gidx && !v->d.mcodes.empty()) std::memcpy(gidx, v->d.mcodes.data(), v->d.mcodes.size());
+    if (n_alleles && !v->d.malleles.empty()) std::memcpy(n_alleles, v->d.malleles.data(), v->d.malleles.size());
+    if (af) {
+        if (v->d.maf.size() != 4 * (size_t)v->d.n_multi) return KG_EINVAL;
+        if (!v->d.maf.empty()) std::memcpy(af, v->d.maf.data(), sizeof(double) * v->d.maf.size());
     }
     return KG_OK;
 }

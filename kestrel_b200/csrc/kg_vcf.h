@@ -3,7 +3,9 @@
 // Reads biallelic SNP records of a VCF 4.x file (plain, gzip or bgzip) into
 // per-sample genotype codes (0 = 0/0, 1 = 0/1, 2 = 1/1, 3 = missing), with the
 // reference's record rules (src/vcf.rs:96-236): records whose REF or ALT is not
-// a single base are skipped, as are records with more than one ALT; GT calls
+// a single base are skipped, as are records with more than one ALT (with GT,
+// tri- and tetra-allelic records that every sample calls are kept apart as
+// genotype indices, as the reference's gt3 / gt4); GT calls
 // are diploid allele indices separated by '/' or '|' ('.' = missing); GL/PL
 // calls are three likelihoods reduced to the most likely genotype (a row that
 // is not one-hot to 25.5 log10 units is counted as soft).  BGZF blocks are
@@ -42,7 +44,13 @@ struct VcfData {
     Bytes codes;                    // sample-major: codes[s * n_sites + v]
     std::vector<double> af;         // with allele frequencies from INFO/AF: [REF, ALT] per kept site
     uint64_t total = 0, not_snp = 0, multi = 0, soft = 0;
-    uint64_t incomplete = 0;        // kept records with at least one missing call
+    uint64_t incomplete = 0;        // SNP records with at least one missing call
+    // GT only: tri- and tetra-allelic records every sample calls
+    int64_t n_multi = 0;
+    Bytes mcodes;                   // sample-major genotype indices (VCF order), mcodes[s * n_multi + v]
+    std::vector<uint8_t> malleles;  // allele count per record (3 or 4)
+    std::vector<double> maf;        // with INFO/AF: 4 per record, [REF, ALT1, ALT2, ALT3 or 0]
+    uint64_t tri = 0, tetra = 0;
 };
 
 // field: 'T' GT, 'L' GL, 'P' PL.  af_info: read INFO/AF (an error when absent).

@@ -818,17 +818,22 @@ __device__ __forceinline__ int cls_self_qp(double q00, double q01, double q10, d
 }
 
 // The CLS estimator's step after its one moment pass (src/coefficients.rs:
-// 218-268): c = (the pair's summed likelihood rows) / (-M), every pair using
-// all M kept sites; the simplex QP on the cohort's Q from 1/9, or the
+// 218-268): c = (the pair's summed likelihood rows, biallelic from the moments
+// plus the tri- and tetra-allelic sums) / (-M), every pair using all M kept
+// sites; the simplex QP on the cohort's Q from 1/9, or the
 // two-variable QP on (Delta1, Delta7) from (1/2, 1/2) for a self pair, with the
 // cohort's iteration limit; then the Brier score, the condition estimate at
 // g = Q delta + c, and the row (iters = the QP's iteration count).
 __device__ __forceinline__ void cls_finish(const WaveArgs& A, SlotState& S, int s, const double* mom_s, int lane,
                                   const HalfGrp& grp) {
     const CohortDev& co = A.cohorts[S.cohort];
-    const double m = (double)co.n_sites;
+    const double m = co.cls_m;
     double Sg = 0.0, Ht[9];
-    if (lane < 9) rebuild_row(mom_s, lane, Sg, Ht);
+    if (lane < 9) {
+        rebuild_row(mom_s, lane, Sg, Ht);
+        // the pair's tri- and tetra-allelic rows: c2 + (c3 + c4)
+        if (co.cls_cmulti) Sg += co.cls_cmulti[(S.k - co.pair_begin) * 9 + lane];
+    }
     double c[9];
     gather9(grp, Sg / -m, c);
     double Qr[9];

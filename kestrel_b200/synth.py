@@ -151,6 +151,23 @@ def make_cohort(n_samples: int, n_sites: int, seed: int, missing=0.02,
     return Cohort(codes=codes, p_true=p, planted=plan, seed=seed, name=name)
 
 
+def make_multiallelic(n_samples: int, n_sites: int, seed: int, missing: float = 0.0):
+    """Tri- and tetra-allelic sites under Hardy-Weinberg proportions:
+    (genotype indices u8 [samples, sites] in the VCF order j (j + 1) / 2 + i,
+    255 = missing; allele counts u8 [sites], 3 or 4)."""
+    rng = np.random.default_rng(seed)
+    al = rng.integers(3, 5, n_sites).astype(np.uint8)
+    g = np.zeros((n_samples, n_sites), np.uint8)
+    for v in range(n_sites):
+        f = rng.dirichlet(np.full(int(al[v]), 0.8))
+        a = rng.choice(int(al[v]), size=(n_samples, 2), p=f)
+        i, j = a.min(1), a.max(1)
+        g[:, v] = j * (j + 1) // 2 + i
+    if missing > 0:
+        g[rng.random(g.shape) < missing] = 255
+    return g, al
+
+
 def swap_xy(delta):
     """Delta of (y, x) from Delta of (x, y): D3<->D5 and D4<->D6 (src/lib.rs:138-149)."""
     d = np.array(delta, dtype=np.float64)

@@ -785,6 +785,54 @@ static void cls_row(int gx, int gy, double p, double q, double row[9]) {
     }
 }
 
+/* The two alleles (i <= j) of genotype index g in the VCF order
+ * (j (j + 1) / 2 + i, src/coefficients.rs:19-38). */
+static void genotype_alleles(int g, int *i, int *j) {
+    int b = 0;
+    while ((b + 1) * (b + 2) / 2 <= g) b++;
+    *j = b;
+    *i = g - b * (b + 1) / 2;
+}
+
+/* m[gx][gy] for any number of alleles: the nine conditional probabilities
+ * P(genotypes (i, j), (k, l) | Jacquard state), the table of src/iis.rs:
+ * 279-462 indexed by the IIS mode of src/conditional.rs:10-50, computed here by
+ * its definition.  For each ordering of each unordered genotype (one for a
+ * homozygote, two for a heterozygote), alleles x1 = a1, x2 = a2, y1 = b1,
+ * y2 = b2 add, per state, the product over the state's identity classes of the
+ * class's allele frequency when every member carries the same allele (zero
+ * otherwise).  The classes: 1 {x1 x2 y1 y2}; 2 {x1 x2}{y1 y2}; 3 {x1 x2 y1}{y2};
+ * 4 {x1 x2}{y1}{y2}; 5 {x1 y1 y2}{x2}; 6 {y1 y2}{x1}{x2}; 7 {x1 y1}{x2 y2};
+ * 8 {x1 y1}{x2}{y2}; 9 all apart. */
+static void iis_row(int i, int j, int k, int l, const double *f, double row[9]) {
+    for (int s = 0; s < 9; s++) row[s] = 0.0;
+    const int nx = i == j ? 1 : 2, ny = k == l ? 1 : 2;
+    for (int u = 0; u < nx; u++) {
+        const int a1 = u ? j : i, a2 = u ? i : j;
+        for (int w = 0; w < ny; w++) {
+            const int b1 = w ? l : k, b2 = w ? k : l;
+            const double fa1 = f[a1], fa2 = f[a2], fb1 = f[b1], fb2 = f[b2];
+            const int xx = a1 == a2, yy = b1 == b2, s1 = a1 == b1, s2 = a2 == b2;
+            if (xx && yy && s1) row[0] += fa1;
+            if (xx && yy) row[1] += fa1 * fb1;
+            if (xx && s1) row[2] += fa1 * fb2;
+            if (xx) row[3] += fa1 * fb1 * fb2;
+            if (yy && s1) row[4] += fb1 * fa2;
+            if (yy) row[5] += fb1 * fa1 * fa2;
+            if (s1 && s2) row[6] += fa1 * fa2;
+            if (s1) row[7] += fa1 * fa2 * fb2;
+            row[8] += fa1 * fa2 * fb1 * fb2;
+        }
+    }
+}
+
+void kor_iis_row(int gx, int gy, const double *freq, double row[9]) {
+    int i, j, k, l;
+    genotype_alleles(gx, &i, &j);
+    genotype_alleles(gy, &k, &l);
+    iis_row(i, j, k, l, freq, row);
+}
+
 /* The reference's default hard-call estimator (src/coefficients.rs:166-278 with
  * src/cls.rs:6-49 and the Gram matrix of src/quadratic.rs), for biallelic
  * sites:
@@ -807,8 +855,18 @@ static void cls_row(int gx, int gy, double p, double q, double row[9]) {
 int kor_cls_relatedness(const uint8_t *codes, int64_t n_samples, int64_t n_sites, int64_t stride,
                         const double *af_in, int64_t num_samples, uint64_t iterations, int threads,
                         kor_output *out, int64_t out_cap, int64_t *n_out) {
+    return kor_cls_relatedness_ma(codes, n_samples, n_sites, stride, af_in, NULL, 0, 0, NULL, NULL,
+                                  num_samples, iterations, threads, out, out_cap, n_out);
+}
+
+int kor_cls_relatedness_ma(const uint8_t *codes, int64_t n_samples, int64_t n_sites, int64_t stride,
+                           const double *af_in, const uint8_t *mg, int64_t n_multi, int64_t mstride,
+                           const uint8_t *malleles, const double *maf_in, int64_t num_samples,
+                           uint64_t iterations, int threads, kor_output *out, int64_t out_cap,
+                           int64_t *n_out) {
     if (!codes || n_samples <= 0 || n_sites <= 0 || stride < n_sites || !out || !n_out || iterations == 0)
         return KOR_EINVAL;
+    if (n_multi < 0 || (n_multi > 0 && (!mg || !malleles || mstride < n_multi))) return KOR_EINVAL;
     if (num_samples < 0) num_samples = n_samples;
     if (num_samples == 0 || num_samples > n_samples) return KOR_EINVAL;
     int64_t npairs = num_samples * (num_samples + 1) / 2;
@@ -839,8 +897,38 @@ int kor_cls_relatedness(const uint8_t *codes, int64_t n_samples, int64_t n_sites
         }
         m++;
     }
-    if (m == 0) { free(site); free(p); free(q); return KOR_ENOSITES; }
-    /* the Gram matrix, upper triangle in the reference's row-major order */
+    /* tri- and tetra-allelic sites (genotype indices, 255 = missing): those
+     * every sample calls; frequencies are allele counts / (2 n_samples)
+     * (src/wrapper.rs:412-428) unless maf_in (n_multi x 4) gives them */
+    int64_t *msite = (int64_t *)malloc(sizeof(int64_t) * (size_t)(n_multi + 1));
+    double *mf = (double *)malloc(sizeof(double) * 4 * (size_t)(n_multi + 1));
+    if (!msite || !mf) { free(site); free(p); free(q); free(msite); free(mf); return KOR_ENOMEM; }
+    int64_t mm = 0;
+    for (int64_t v = 0; v < n_multi; v++) {
+        const int na = malleles[v];
+        if (na < 3 || na > 4) { free(site); free(p); free(q); free(msite); free(mf); return KOR_EINVAL; }
+        const int ng = na * (na + 1) / 2;
+        int64_t cnt[4] = {0, 0, 0, 0};
+        int complete = 1;
+        for (int64_t s2 = 0; s2 < n_samples; s2++) {
+            const int g = mg[s2 * mstride + v];
+            if (g == 255) { complete = 0; break; }
+            if (g >= ng) { free(site); free(p); free(q); free(msite); free(mf); return KOR_EINVAL; }
+            int a, b;
+            genotype_alleles(g, &a, &b);
+            cnt[a]++;
+            cnt[b]++;
+        }
+        if (!complete) continue;
+        msite[mm] = v;
+        for (int a = 0; a < 4; a++)
+            mf[4 * mm + a] = maf_in ? maf_in[4 * v + a] : (a < na ? (double)cnt[a] / (double)(2 * n_samples) : 0.0);
+        mm++;
+    }
+    if (m + mm == 0) { free(site); free(p); free(q); free(msite); free(mf); return KOR_ENOSITES; }
+    const double m_total = (double)(m + mm);
+    /* the Gram matrix over all sites' rows (biallelic, then the others), upper
+     * triangle in the reference's row-major order (src/coefficients.rs:281-320) */
     double h[45] = {0};
     for (int64_t k = 0; k < m; k++) {
         for (int gx = 0; gx < 3; gx++)
@@ -852,12 +940,23 @@ int kor_cls_relatedness(const uint8_t *codes, int64_t n_samples, int64_t n_sites
                     for (int j = i; j < 9; j++) h[a++] += row[i] * row[j];
             }
     }
+    for (int64_t k = 0; k < mm; k++) {
+        const int na = malleles[msite[k]], ng = na * (na + 1) / 2;
+        for (int gx = 0; gx < ng; gx++)
+            for (int gy = 0; gy < ng; gy++) {
+                double row[9];
+                kor_iis_row(gx, gy, mf + 4 * k, row);
+                int a = 0;
+                for (int i = 0; i < 9; i++)
+                    for (int j = i; j < 9; j++) h[a++] += row[i] * row[j];
+            }
+    }
     double Q[9][9];
     {
         int a = 0;
         for (int i = 0; i < 9; i++)
             for (int j = i; j < 9; j++) {
-                const double v = h[a++] / (double)m;
+                const double v = h[a++] / m_total;
                 Q[i][j] = v;
                 Q[j][i] = v;
             }
@@ -881,7 +980,16 @@ int kor_cls_relatedness(const uint8_t *codes, int64_t n_samples, int64_t n_sites
                 cls_row(codes[x * stride + v], codes[y * stride + v], p[k], q[k], row);
                 for (int i = 0; i < 9; i++) c[i] = c[i] + row[i];
             }
-            for (int i = 0; i < 9; i++) c[i] = c[i] / (-(double)m);
+            /* c2 + (c3 + c4), src/coefficients.rs:220-224 */
+            double c3[9] = {0}, c4[9] = {0};
+            for (int64_t k = 0; k < mm; k++) {
+                const int64_t v = msite[k];
+                double row[9];
+                kor_iis_row(mg[x * mstride + v], mg[y * mstride + v], mf + 4 * k, row);
+                double *acc = malleles[v] == 3 ? c3 : c4;
+                for (int i = 0; i < 9; i++) acc[i] = acc[i] + row[i];
+            }
+            for (int i = 0; i < 9; i++) c[i] = (c[i] + (c3[i] + c4[i])) / -m_total;
             double delta[9] = {0};
             uint64_t its;
             if (x == y) {
@@ -913,6 +1021,6 @@ int kor_cls_relatedness(const uint8_t *codes, int64_t n_samples, int64_t n_sites
         }
     }
     *n_out = npairs;
-    free(site); free(p); free(q);
+    free(site); free(p); free(q); free(msite); free(mf);
     return KOR_OK;
 }

@@ -92,6 +92,20 @@ int kor_eval_pair(const uint8_t *codes_x, const uint8_t *codes_y, int64_t n_site
 int kor_cls_relatedness(const uint8_t *codes, int64_t n_samples, int64_t n_sites, int64_t stride,
                         const double *af_in, int64_t num_samples, uint64_t iterations, int threads,
                         kor_output *out, int64_t out_cap, int64_t *n_out);
+/* The same with tri- and tetra-allelic sites beside the biallelic ones (the
+ * reference's gt3 / gt4): mg[s * mstride + v] is sample s's genotype index at
+ * multi-allelic site v in the VCF order (j (j + 1) / 2 + i, 255 = missing),
+ * malleles[v] its allele count (3 or 4), maf_in (n_multi x 4, or NULL) its
+ * allele frequencies.  Every site any sample misses is dropped; M counts the
+ * biallelic and multi-allelic sites used. */
+int kor_cls_relatedness_ma(const uint8_t *codes, int64_t n_samples, int64_t n_sites, int64_t stride,
+                           const double *af_in, const uint8_t *mg, int64_t n_multi, int64_t mstride,
+                           const uint8_t *malleles, const double *maf_in, int64_t num_samples,
+                           uint64_t iterations, int threads, kor_output *out, int64_t out_cap,
+                           int64_t *n_out);
+/* m[gx][gy] of a site with allele frequencies freq (genotype indices in the VCF
+ * order): the nine conditional probabilities of the joint genotypes. */
+void kor_iis_row(int gx, int gy, const double *freq, double row[9]);
 /* Pass counters of the last kor_relatedness_pairs call on this thread group:
  * total grad/Hessian passes and objective passes summed over pairs. */
 void kor_pass_counts(uint64_t *gh_passes, uint64_t *obj_passes);

@@ -52,8 +52,12 @@ def lib():
         L.kor_pass_counts.argtypes = [ctypes.POINTER(u64), ctypes.POINTER(u64)]
         L.kor_cls_relatedness.argtypes = [P, i64, i64, i64, P, i64, u64, ctypes.c_int, P, i64,
                                           ctypes.POINTER(i64)]
+        L.kor_cls_relatedness_ma.argtypes = [P, i64, i64, i64, P, P, i64, i64, P, P, i64, u64,
+                                             ctypes.c_int, P, i64, ctypes.POINTER(i64)]
+        L.kor_iis_row.argtypes = [ctypes.c_int, ctypes.c_int, P, P]
+        L.kor_iis_row.restype = None
         for f in ("kor_site_frequencies", "kor_relatedness", "kor_relatedness_pairs",
-                  "kor_eval_pair", "kor_allele_counts", "kor_cls_relatedness"):
+                  "kor_eval_pair", "kor_allele_counts", "kor_cls_relatedness", "kor_cls_relatedness_ma"):
             getattr(L, f).restype = ctypes.c_int
         L.kor_pass_counts.restype = None
         _lib = L
@@ -112,21 +116,43 @@ def relatedness(codes, af=None, num_samples=None, iterations=100, maf=None, thre
     return out
 
 
-def cls_relatedness(codes, af=None, num_samples=None, iterations=100, threads=0):
+def cls_relatedness(codes, af=None, num_samples=None, iterations=100, threads=0, multi=None):
     """The reference's default hard-call estimator (conditional least squares,
     Brier objective): rows as `relatedness`, obj = Brier score, iters = QP
-    iterations."""
+    iterations.  multi: None or (genotype indices u8 [samples, sites] in the VCF
+    order with 255 = missing, allele counts u8 [sites] of 3 or 4, allele
+    frequencies f64 [sites, 4] or None) for tri- and tetra-allelic sites."""
     codes = _codes(codes)
     n, m = codes.shape
     ns = n if num_samples is None else num_samples
     out = np.zeros(ns * (ns + 1) // 2, OUTPUT_DTYPE)
     nout = ctypes.c_int64()
     afa = None if af is None else np.ascontiguousarray(af, dtype=np.float64)
-    st = lib().kor_cls_relatedness(_ptr(codes), n, m, m, _ptr(afa), ns, iterations, threads,
-                                   _ptr(out), out.size, ctypes.byref(nout))
+    if multi is None:
+        st = lib().kor_cls_relatedness(_ptr(codes), n, m, m, _ptr(afa), ns, iterations, threads,
+                                       _ptr(out), out.size, ctypes.byref(nout))
+    else:
+        mg = np.ascontiguousarray(multi[0], dtype=np.uint8)
+        mal = np.ascontiguousarray(multi[1], dtype=np.uint8)
+        maf = None if len(multi) < 3 or multi[2] is None else np.ascontiguousarray(multi[2], dtype=np.float64)
+        assert mg.shape[0] == n and mg.shape[1] == mal.shape[0]
+        vm = mg.shape[1]
+        st = lib().kor_cls_relatedness_ma(_ptr(codes), n, m, m, _ptr(afa), _ptr(mg), vm, vm, _ptr(mal),
+                                          _ptr(maf), ns, iterations, threads, _ptr(out), out.size,
+                                          ctypes.byref(nout))
     if st:
         raise RuntimeError(f"kor_cls_relatedness failed: {st}")
     return out
+
+
+def iis_row(gx, gy, freq):
+    """m[gx][gy] (9 conditional probabilities) for genotype indices in the VCF
+    order and allele frequencies freq."""
+    f = np.zeros(4)
+    f[:len(freq)] = freq
+    row = np.zeros(9)
+    lib().kor_iis_row(int(gx), int(gy), _ptr(f), _ptr(row))
+    return row
 
 
 def relatedness_pairs(codes, p, q, keep, pairs, iterations=100, threads=0):

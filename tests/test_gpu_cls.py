@@ -83,3 +83,69 @@ def test_cls_no_complete_site(est):
     with pytest.raises(kb.KestrelError) as e:
         est.relatedness_gt()
     assert e.value.status == kb.KG_ENOSITES
+
+
+# ---- tri- and tetra-allelic sites (kg_load_multiallelic)
+
+@pytest.fixture(scope="module")
+def multi(complete):
+    g, al = synth.make_multiallelic(complete.codes.shape[0], 700, 23)
+    g[5, 11] = 255                       # a missing call drops site 11
+    return g, al
+
+
+def test_cls_multiallelic_parity(est, oracle, complete, multi):
+    g, al = multi
+    ref = oracle.cls_relatedness(complete.codes, multi=(g, al, None))
+    est.load(complete.codes)
+    est.load_multiallelic(g, al)
+    gpu = est.relatedness_gt()
+    stats = compare(gpu, ref)
+    same_iters = float(np.mean(gpu["iters"] == ref["iters"]))
+    print(stats, "same QP iterations", same_iters)
+    assert same_iters > 0.95
+    # without them the result changes, and loading genotypes again clears them
+    est.load(complete.codes)
+    plain = est.relatedness_gt()
+    assert np.abs(plain["jacquard"] - gpu["jacquard"]).max() > 1e-6
+    compare(plain, oracle.cls_relatedness(complete.codes))
+
+
+def test_cls_multiallelic_supplied_frequencies_and_subset(est, oracle, complete, multi):
+    g, al = multi
+    rng = np.random.default_rng(8)
+    maf = np.zeros((g.shape[1], 4))
+    for v in range(g.shape[1]):
+        maf[v, :al[v]] = rng.dirichlet(np.ones(al[v]))
+    ref = oracle.cls_relatedness(complete.codes, num_samples=40, multi=(g, al, maf))
+    est.load(complete.codes)
+    est.load_multiallelic(g, al, maf)
+    gpu = est.relatedness_gt(num_samples=40)
+    compare(gpu, ref)
+
+
+def test_cls_tri_site_with_an_absent_allele_is_biallelic(est, complete):
+    codes = complete.codes
+    est.load(codes)
+    base = est.relatedness_gt()
+    cut = 7000
+    est.load(codes[:, :cut])
+    est.load_multiallelic(codes[:, cut:], np.full(codes.shape[1] - cut, 3, np.uint8))
+    split = est.relatedness_gt()
+    # the same estimator up to where the sums run (FP32 moments vs FP64 rows),
+    # within the parity bar: Delta on identifiable pairs (log10 cond <= 4)
+    ident = np.log10(base["cond"]) <= 4
+    assert ident.mean() > 0.9
+    assert np.abs(split["jacquard"] - base["jacquard"]).max(1)[ident].max() < 1e-5
+    assert np.all(np.abs(split["obj"] - base["obj"]) <= 1e-6 * np.abs(base["obj"]))
+
+
+def test_cls_multiallelic_bad_index(est, complete):
+    g = np.zeros((complete.codes.shape[0], 4), np.uint8)
+    g[2, 1] = 6                          # index 6 needs four alleles
+    est.load(complete.codes)
+    est.load_multiallelic(g, np.full(4, 3, np.uint8))
+    with pytest.raises(kb.KestrelError) as e:
+        est.relatedness_gt()
+    assert e.value.status == kb.KG_EINVAL
+    est.load(complete.codes)

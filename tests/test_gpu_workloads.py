@@ -218,3 +218,44 @@ def test_cli_gt_default_drops_records_with_missing_calls(oracle):
     ident = np.isfinite(lc_ref) & (lc_ref <= 4)
     assert len(rows) == len(ref)
     assert np.abs(jac - ref["jacquard"]).max(1)[ident].max() <= 1e-5
+
+
+def test_cli_gt_default_fits_tri_and_tetra_allelic_records(oracle):
+    co = synth.make_cohort(24, 3000, seed=46, missing=0.0, name="cli-multi")
+    g, al = synth.make_multiallelic(24, 400, 47)
+    g[3, 5] = 255                                        # skipped: a missing call
+    ref = oracle.cls_relatedness(co.codes, multi=(g, al, None))
+    cli = os.path.join(os.path.dirname(kb.__file__), "bin", "kestrel")
+    alts = {3: "C,G", 4: "C,G,T"}
+    lines = []
+    for v in range(g.shape[1]):
+        calls = []
+        for s in range(24):
+            if g[s, v] == 255:
+                calls.append("./.")
+                continue
+            j = 0
+            while (j + 1) * (j + 2) // 2 <= g[s, v]:
+                j += 1
+            calls.append(f"{g[s, v] - j * (j + 1) // 2}/{j}")
+        lines.append(f"2\t{v + 1}\t.\tA\t{alts[int(al[v])]}\t.\tPASS\t.\tGT\t" + "\t".join(calls))
+    with tempfile.TemporaryDirectory() as td:
+        vcf = os.path.join(td, "in.vcf")
+        tsv = os.path.join(td, "out.tsv")
+        synth.write_vcf(vcf, co.codes, field="GT")
+        with open(vcf, "a") as fh:
+            fh.write("\n".join(lines) + "\n")
+        r = subprocess.run([cli, vcf, tsv], capture_output=True, text=True, timeout=300)
+        assert r.returncode == 0, r.stderr
+        _, rows = _read_tsv(tsv)
+    n_tri = int(np.sum(al == 3)) - int(al[5] == 3)
+    assert f"Found {n_tri} tri-allelic sites" in r.stderr
+    assert f"Found {int(np.sum(al == 4)) - int(al[5] == 4)} tetra-allelic sites" in r.stderr
+    assert "Skipped 1 sites with missing data" in r.stderr
+    jac = np.array([[float(v) for v in r[3:12]] for r in rows])
+    obj = np.array([float(r[13]) for r in rows])
+    lc_ref = np.log10(ref["cond"])
+    ident = np.isfinite(lc_ref) & (lc_ref <= 4)
+    assert len(rows) == len(ref)
+    assert np.abs(jac - ref["jacquard"]).max(1)[ident].max() <= 1e-5
+    assert (np.abs(obj - ref["obj"]) / np.abs(ref["obj"])).max() <= 1e-6

@@ -122,3 +122,129 @@ def test_num_samples_and_iteration_cap(oracle, cohort):
         assert np.array_equal(r["jacquard"], ref["jacquard"])
     capped = oracle.cls_relatedness(cohort.codes, iterations=2)
     assert capped["iters"].max() <= 2
+
+
+# ---- tri- and tetra-allelic sites (the reference's gt3 / gt4)
+
+def table_row(i, j, k, l, f):
+    """The nine conditional probabilities of genotypes (i, j), (k, l) (i <= j,
+    k <= l) from the closed forms of src/iis.rs:279-462, the mode chosen by the
+    allele equalities as src/iis.rs:76-118 does."""
+    pi, pj, pk, pl = f[i], f[j], f[k], f[l]
+    eq = (i == j, i == k, i == l, j == k, j == l, k == l)
+    r = np.zeros(9)
+    if all(eq):                                           # ii-ii
+        r[:] = [pi, pi**2, pi**2, pi**3, pi**2, pi**3, pi**2, pi**3, pi**4]
+    elif eq == (1, 0, 0, 0, 0, 1):                        # ii-kk
+        r[[1, 3, 5, 8]] = [pi * pk, pi * pk**2, pi**2 * pk, pi**2 * pk**2]
+    elif eq in ((1, 1, 0, 1, 0, 0), (1, 0, 1, 0, 1, 0)):  # ii-il, ii-ki
+        o = pl if eq[1] else pk
+        r[[2, 3, 7, 8]] = [pi * o, 2 * pi**2 * o, pi**2 * o, 2 * pi**3 * o]
+    elif eq == (1, 0, 0, 0, 0, 0):                        # ii-kl
+        r[[3, 8]] = [2 * pi * pk * pl, 2 * pi**2 * pk * pl]
+    elif eq == (0, 1, 1, 0, 0, 1):                        # ij-ii
+        r[[4, 5, 7, 8]] = [pi * pj, 2 * pi**2 * pj, pi**2 * pj, 2 * pi**3 * pj]
+    elif eq == (0, 0, 0, 1, 1, 1):                        # ij-jj
+        r[[4, 5, 7, 8]] = [pi * pj, 2 * pj**2 * pi, pj**2 * pi, 2 * pj**3 * pi]
+    elif eq == (0, 0, 0, 0, 0, 1):                        # ij-kk
+        r[[5, 8]] = [2 * pi * pj * pk, 2 * pk**2 * pi * pj]
+    elif eq in ((0, 1, 0, 0, 1, 0), (0, 0, 1, 1, 0, 0)):  # ij-ij, ij-ji
+        r[[6, 7, 8]] = [2 * pi * pj, pi * pj * (pi + pj), 4 * pi**2 * pj**2]
+    elif eq == (0, 1, 0, 0, 0, 0):                        # ij-il
+        r[[7, 8]] = [pi * pj * pl, 4 * pi**2 * pj * pl]
+    elif eq == (0, 0, 1, 0, 0, 0):                        # ij-ki
+        r[[7, 8]] = [pi * pj * pk, 4 * pi**2 * pj * pk]
+    elif eq == (0, 0, 0, 1, 0, 0):                        # ij-jl
+        r[[7, 8]] = [pi * pj * pl, 4 * pi * pj**2 * pl]
+    elif eq == (0, 0, 0, 0, 1, 0):                        # ij-kj
+        r[[7, 8]] = [pi * pj * pk, 4 * pi * pj**2 * pk]
+    elif eq == (0, 0, 0, 0, 0, 0):                        # ij-kl
+        r[8] = 4 * pi * pj * pk * pl
+    else:
+        raise AssertionError(eq)
+    return r
+
+
+def alleles_of(g):
+    b = 0
+    while (b + 1) * (b + 2) // 2 <= g:
+        b += 1
+    return g - b * (b + 1) // 2, b
+
+
+def table_rows(freq, n_alleles):
+    ng = n_alleles * (n_alleles + 1) // 2
+    R = np.zeros((ng, ng, 9))
+    for gx in range(ng):
+        for gy in range(ng):
+            R[gx, gy] = table_row(*alleles_of(gx), *alleles_of(gy), freq)
+    return R
+
+
+def test_iis_rows_match_the_closed_forms(oracle):
+    rng = np.random.default_rng(3)
+    for _ in range(20):
+        f = rng.dirichlet(np.ones(4))
+        R = table_rows(f, 4)
+        for gx in range(10):
+            for gy in range(10):
+                got = oracle.iis_row(gx, gy, f)
+                assert np.allclose(got, R[gx, gy], rtol=1e-14, atol=1e-300), (gx, gy)
+    # two alleles: the biallelic rows
+    p = rng.uniform(0.05, 0.95, 50)
+    B = numpy_rows(p, 1 - p)
+    for v in range(50):
+        for gx in range(3):
+            for gy in range(3):
+                assert np.allclose(oracle.iis_row(gx, gy, [p[v], 1 - p[v]]), B[v, gx, gy], rtol=1e-14)
+
+
+def test_tri_site_with_an_absent_allele_is_biallelic(oracle, cohort):
+    codes = cohort.codes
+    n = codes.shape[0]
+    base = oracle.cls_relatedness(codes)
+    g = codes.astype(np.int64)
+    p = (2 - g).sum(0) / (2 * n)
+    cut = 3000
+    mg = codes[:, cut:].copy()        # 0/0, 0/1, 1/1 keep their index with three alleles
+    al = np.full(mg.shape[1], 3, np.uint8)
+    for maf in (None, np.stack([p[cut:], 1 - p[cut:], 0 * p[cut:], 0 * p[cut:]], 1)):
+        out = oracle.cls_relatedness(codes[:, :cut], multi=(mg, al, maf))
+        assert np.abs(out["jacquard"] - base["jacquard"]).max() < 1e-9
+        assert np.abs(out["obj"] - base["obj"]).max() < 1e-12
+        assert np.mean(out["iters"] == base["iters"]) > 0.99
+
+
+def test_multi_allelic_brier_and_kkt_against_numpy(oracle, cohort):
+    codes = cohort.codes[:, :1500]
+    n, m = codes.shape
+    mg, al = synth.make_multiallelic(n, 300, 5)
+    mg[3, 7] = 255                          # a missing call drops site 7
+    out = oracle.cls_relatedness(codes, multi=(mg, al, None))
+    g = codes.astype(np.int64)
+    p = (2 - g).sum(0) / (2 * n)
+    Rb = numpy_rows(p, 1 - p)
+    keep = [v for v in range(mg.shape[1]) if v != 7]
+    Rm = []
+    for v in keep:
+        cnt = np.zeros(4)
+        for s in range(n):
+            a, b = alleles_of(mg[s, v])
+            cnt[a] += 1
+            cnt[b] += 1
+        Rm.append(table_rows(cnt / (2 * n), al[v]))
+    M = m + len(keep)
+    Q = np.einsum("vabi,vabj->ij", Rb, Rb) + sum(np.einsum("abi,abj->ij", R, R) for R in Rm)
+    Q /= M
+    for x, y in [(0, 1), (2, 9), (7, 7), (13, 39), (20, 21)]:
+        r = out[row_index(n, x, y)]
+        c = Rb[np.arange(m), g[x], g[y]].sum(0) + sum(R[mg[x, v], mg[y, v]] for R, v in zip(Rm, keep))
+        c = -c / M
+        d = r["jacquard"]
+        brier = d @ Q @ d + 2 * c @ d + 1
+        assert abs(brier - r["obj"]) <= 1e-11 * abs(brier)
+        if x != y and r["iters"] < 100:
+            grad = Q @ d + c
+            lam = d @ grad
+            viol = np.where(d > 0, np.abs(grad - lam), np.maximum(lam - grad, 0))
+            assert viol.max() < 1e-8

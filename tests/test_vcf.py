@@ -18,10 +18,12 @@ BASES = set("ACGTacgt")
 
 
 def py_parse(text, field="GT", af_info=False):
-    """Reference parse: returns (codes [S, V], af or None, samples, counts)."""
+    """Reference parse: returns (codes [S, V], af or None, samples, counts,
+    (multi-allelic genotype indices [S, Vm], allele counts, af [Vm, 4] or None))."""
     key = field
     samples, rows, afs = [], [], []
-    total = not_snp = multi = soft = with_missing = 0
+    mrows, malleles, mafs = [], [], []
+    total = not_snp = multi = soft = with_missing = tri = tetra = 0
     for line in text.split("\n"):
         line = line.rstrip("\r")
         if line.startswith("#CHROM"):
@@ -35,20 +37,59 @@ def py_parse(text, field="GT", af_info=False):
             raise ValueError(f"malformed record {total}")
         alts = cols[4].split(",")
         snp = len(cols[3]) == 1 and cols[3] in BASES and all(len(a) == 1 and a in BASES for a in alts)
-        if not snp:
+        nb = len(alts) + 1
+        if not snp or nb > 4:
             not_snp += 1
             continue
-        if len(alts) != 1:
+        if nb > 2:
             multi += 1
-            continue
+            if field != "GT":
+                continue
         fmt = cols[8].split(":")
         fi = max([i for i, f in enumerate(fmt) if f == key], default=-1)
         if fi < 0:
             raise ValueError(f"No {key} data found")
+
+        def value(s):
+            sub = cols[9 + s].split(":")
+            return sub[fi] if fi < len(sub) else "."
+        if nb > 2:
+            row, missing = [], False
+            for s in range(len(samples)):
+                v = value(s)
+                parts = v.replace("|", "/").split("/")
+                if "." in parts and len(parts) <= 2:
+                    missing = True
+                    break
+                if len(parts) != 2 or not all(p.isdigit() and int(p) < nb for p in parts):
+                    raise ValueError(f"Value {v} is not a valid GT")
+                i, j = sorted(int(p) for p in parts)
+                row.append(j * (j + 1) // 2 + i)
+            if missing:
+                with_missing += 1
+                continue
+            if af_info:
+                vals = None
+                for kv in cols[7].split(";"):
+                    if kv.startswith("AF="):
+                        vals = [float(x) for x in kv[3:].split(",")]
+                if vals is None:
+                    raise ValueError("No AF info found")
+                if len(vals) != nb - 1:
+                    raise ValueError("allele frequencies")
+                alt_sum = 0.0
+                for x in vals:          # in order, as the reference adds them
+                    alt_sum += x
+                f = [1.0 - min(max(alt_sum, 0.0), 1.0)] + vals
+                mafs.append(f + [0.0] * (4 - len(f)))
+            mrows.append(row)
+            malleles.append(nb)
+            tri += nb == 3
+            tetra += nb == 4
+            continue
         row = []
         for s in range(len(samples)):
-            sub = cols[9 + s].split(":")
-            v = sub[fi] if fi < len(sub) else "."
+            v = value(s)
             if field == "GT":
                 parts = v.replace("|", "/").split("/")
                 if "." in parts:
@@ -85,10 +126,13 @@ def py_parse(text, field="GT", af_info=False):
             afs.append([1.0 - min(max(a, 0.0), 1.0), a])
         with_missing += 3 in row
         rows.append(row)
-    codes = np.array(rows, np.uint8).T.reshape(len(samples), len(rows)) if rows else np.zeros((len(samples), 0), np.uint8)
-    return codes, (np.array(afs) if af_info else None), samples, \
-        {"records": total, "not_snp": not_snp, "multiallelic": multi, "soft_likelihoods": soft,
-         "with_missing": with_missing}
+    ns = len(samples)
+    codes = np.array(rows, np.uint8).T.reshape(ns, len(rows)) if rows else np.zeros((ns, 0), np.uint8)
+    mg = np.array(mrows, np.uint8).T.reshape(ns, len(mrows)) if mrows else np.zeros((ns, 0), np.uint8)
+    counts = {"records": total, "not_snp": not_snp, "multiallelic": multi, "soft_likelihoods": soft,
+              "with_missing": with_missing, "tri_allelic": tri, "tetra_allelic": tetra}
+    return codes, (np.array(afs) if af_info else None), samples, counts, \
+        (mg, np.array(malleles, np.uint8), (np.array(mafs).reshape(-1, 4) if af_info else None))
 
 
 def write_bgzip(path, data: bytes, block=65280):
@@ -111,12 +155,18 @@ def write_bgzip(path, data: bytes, block=65280):
 def edge_records(n):
     def calls(txt):
         return "\t".join([txt] * n)
-    return [f"2\t1\t.\tA\tC,G\t.\tPASS\tAF=0.2\tGT\t{calls('0/1')}",      # multi-allelic
+
+    def mixed(*txt):
+        return "\t".join(txt[i % len(txt)] for i in range(n))
+    return [f"2\t1\t.\tA\tC,G\t.\tPASS\tAF=0.2,0.1\tGT\t{mixed('0/1', '2/2', '1|2', '0/0')}",  # tri-allelic
             f"2\t2\t.\tAT\tC\t.\tPASS\tAF=0.2\tGT\t{calls('0/1')}",       # not a SNP
             f"2\t3\t.\tG\t<DEL>\t.\tPASS\tAF=0.2\tGT\t{calls('1/1')}",    # symbolic ALT
             f"2\t4\t.\tT\tG\t.\tPASS\tAF=0.4;DP=9\tGT:DP\t{calls('0|1:7')}",
             f"2\t5\t.\tc\tg\t.\tPASS\tDP=3;AF=0.7\tDP:GT\t{calls('5:1/1')}",
-            f"2\t6\t.\tA\tT\t.\tPASS\tAF=0.5\tGT\t{calls('./.')}"]
+            f"2\t6\t.\tA\tT\t.\tPASS\tAF=0.5\tGT\t{calls('./.')}",
+            f"2\t7\t.\tA\tC,G,T\t.\tPASS\tAF=0.1,0.2,0.3\tGT\t{mixed('3/1', '0/3', '2/2', '1/1')}",  # tetra
+            f"2\t8\t.\tA\tC,G\t.\tPASS\tAF=0.2,0.1\tGT\t{mixed('0/1', './.', '2/9')}",  # missing: skipped
+            f"2\t9\t.\tA\tC,G,T,A\t.\tPASS\tAF=0.1,0.1,0.1,0.1\tGT\t{calls('0/1')}"]   # five bases
 
 
 @pytest.fixture(scope="module")
@@ -153,13 +203,18 @@ def test_reader_matches_python(cohort, field, compression):
         else:
             write_bgzip(p, data)
         for threads in (1, 3, 8):
-            codes, af, names, counts = kb.read_vcf(p, field, allele_freqs="info", threads=threads)
+            codes, af, names, counts, multi = kb.read_vcf(p, field, allele_freqs="info", threads=threads,
+                                                          multiallelic=True)
             assert np.array_equal(codes, ref[0])
             assert np.array_equal(af, ref[1])
             assert names == ref[2]
             assert counts == ref[3]
+            for a, b in zip(multi, ref[4]):
+                assert np.array_equal(a, b)
     if field == "GT":
-        assert counts["multiallelic"] == 1 and counts["not_snp"] == 2
+        assert counts["multiallelic"] == 3 and counts["not_snp"] == 3
+        assert counts["tri_allelic"] == 1 and counts["tetra_allelic"] == 1
+        assert multi[0][:4, 1].tolist() == [7, 6, 5, 2]   # 3/1, 0/3, 2/2, 1/1
 
 
 def test_crlf_and_gl_field(cohort):
