@@ -47,6 +47,8 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--slots", type=int, default=0, help="pairs in flight per wave (0 = automatic)")
+    ap.add_argument("--multi-sites", type=int, default=0,
+                    help="gt-cls: tri- and tetra-allelic sites beside the biallelic ones")
     ap.add_argument("--pass-bps", type=int, default=0, help="site-pass blocks per SM (0 = automatic)")
     ap.add_argument("--workload", default="allpairs", choices=["allpairs", "batch", "inbred", "serving", "gt-cls"],
                     help="allpairs: N x M all pairs (the headline); batch: 8 uneven cohorts in one "
@@ -327,8 +329,11 @@ def run_gt_cls(args, local):
                            name="gt-cls")
     codes = co.codes
     pairs = n_s * (n_s - 1) // 2
+    mg, mal = synth.make_multiallelic(n_s, args.multi_sites, 2) if args.multi_sites else (None, None)
     est = kb.Estimator(device=local, precision=args.precision)
     est.load(codes)
+    if mg is not None:
+        est.load_multiallelic(mg, mal)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")
     for _ in range(max(3, args.warmup)):
         est.relatedness_gt()
@@ -351,6 +356,8 @@ def run_gt_cls(args, local):
                           pin_memory=True).numpy().view(kb.OUTPUT_DTYPE)
     e2 = kb.Estimator(device=local, precision=args.precision)
     e2.load(codes_pin)
+    if mg is not None:
+        e2.load_multiallelic(mg, mal)
     e2.relatedness_gt(out=out_pin)
     e2e_ms = []
     for _ in range(max(1, args.steps)):
@@ -358,6 +365,8 @@ def run_gt_cls(args, local):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         e2.load(codes_pin)
+        if mg is not None:
+            e2.load_multiallelic(mg, mal)
         e2.relatedness_gt(out=out_pin)
         e2e_ms.append((time.perf_counter() - t0) * 1e3)
     e2.close()
@@ -378,7 +387,8 @@ def run_gt_cls(args, local):
     if not args.no_cpu:
         sub = min(n_s, 192)
         t0 = time.perf_counter()
-        pyoracle.cls_relatedness(codes[:, :], num_samples=sub)
+        pyoracle.cls_relatedness(codes[:, :], num_samples=sub,
+                                 multi=None if mg is None else (mg, mal, None))
         dt = time.perf_counter() - t0
         cpu = {"value": sub * (sub + 1) / 2 / dt, "unit": "pairs/s", "cores": os.cpu_count(), "kind": "port",
                "sample": f"all {sub * (sub + 1) // 2} pairs of the first {sub} samples (oracle FP64 CLS "
@@ -388,9 +398,12 @@ def run_gt_cls(args, local):
             "n_gpus": 1, "steps": args.steps, "warmup": max(3, args.warmup), "ms_per_step": t,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32" if args.precision == "fp32c" else "f64", "data": "synthetic",
-            "config": {"workload": f"all pairs of N={n_s} x M={m_s}, no missing calls (planted PO/FS/HS/FC)",
+            "config": {"workload": f"all pairs of N={n_s} x M={m_s}" +
+                                   (f" + {args.multi_sites} tri-/tetra-allelic sites" if mg is not None else "") +
+                                   ", no missing calls (planted PO/FS/HS/FC)",
                        "pairs": pairs, "l2": "256 MB buffer written between steps"},
-            "e2e": {"value": pairs / (te * 1e-3), "unit": "pairs/s", "h2d_bytes_per_step": int(codes.nbytes),
+            "e2e": {"value": pairs / (te * 1e-3), "unit": "pairs/s",
+                    "h2d_bytes_per_step": int(codes.nbytes) + (0 if mg is None else int(mg.nbytes + mal.nbytes)),
                     "d2h_bytes_per_step": int(out_pin.nbytes), "ms_per_step": te},
             "roofline": roof, "cpu_baseline": cpu, "clocks": clk,
             "gpu_launches": int(st["launches"]),

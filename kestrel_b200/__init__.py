@@ -277,19 +277,43 @@ def relatedness_coefficients_gt(genotypes, allele_frequencies=None, threads=None
     calls (the reference's signature, src/lib.rs:46-70).  genotypes: u8/int
     [variants, samples, 2] allele indices; allele_frequencies: f64 [variants, 2]
     ([REF, ALT]) or None to estimate.  `threads` is accepted and unused.
-    estimator "ml" runs the maximum-likelihood estimator on the calls; "cls"
-    runs the reference's own hard-call estimator (conditional least squares
-    with the Brier objective, src/coefficients.rs:166-278)."""
+    estimator "ml" runs the maximum-likelihood estimator on the calls (alleles
+    other than 0 and 1 count as missing); "cls" runs the reference's own
+    hard-call estimator (conditional least squares with the Brier objective,
+    src/coefficients.rs:166-278) on the sites every sample calls, sites with
+    alleles 2 or 3 as tri- or tetra-allelic sites."""
     del threads
     if estimator not in ("ml", "cls"):
         raise ValueError("estimator must be 'ml' or 'cls'")
-    codes = genotype_codes(genotypes)
+    if estimator == "ml":
+        codes = genotype_codes(genotypes)
+        with Estimator() as est:
+            est.load(codes, allele_frequencies)
+            rows = est.relatedness(iterations=iterations)
+        return Coefficients(*build_arrays(rows, codes.shape[0]))
+    # CLS: sites whose calls use allele 2 or 3 are tri- or tetra-allelic
+    # (their allele count is the largest allele + 1); allele_frequencies, when
+    # given, are [variants, 2] for the biallelic sites only
+    g = np.asarray(genotypes)
+    if g.ndim != 3 or g.shape[2] != 2:
+        raise ValueError("genotypes must have shape (variants, samples, 2)")
+    a = g.astype(np.int16)
+    if g.dtype == np.uint8:
+        a = np.where(g == 255, -1, a)
+    called = (a >= 0).all(axis=2)
+    top = np.where(called, a.max(axis=2), -1).max(axis=1)
+    if np.any(top > 3):
+        raise ValueError("at most four alleles per site")
+    multi = top >= 2
+    codes = genotype_codes(g[~multi])
     with Estimator() as est:
         est.load(codes, allele_frequencies)
-        if estimator == "cls":
-            rows = est.relatedness_gt(iterations=iterations)
-        else:
-            rows = est.relatedness(iterations=iterations)
+        if multi.any():
+            am = a[multi]
+            lo, hi = am.min(axis=2), am.max(axis=2)
+            gi = np.where((am >= 0).all(axis=2), hi * (hi + 1) // 2 + lo, 255).astype(np.uint8)
+            est.load_multiallelic(np.ascontiguousarray(gi.T), (top[multi] + 1).astype(np.uint8))
+        rows = est.relatedness_gt(iterations=iterations)
     return Coefficients(*build_arrays(rows, codes.shape[0]))
 
 

@@ -149,3 +149,26 @@ def test_cls_multiallelic_bad_index(est, complete):
         est.relatedness_gt()
     assert e.value.status == kb.KG_EINVAL
     est.load(complete.codes)
+
+
+def test_python_gt_api_routes_multiallelic_sites(oracle, complete, multi):
+    g, al = multi
+    n = complete.codes.shape[0]
+    # allele pairs: biallelic sites from the codes, the others from the indices
+    bi = np.stack([(complete.codes >= 1).astype(np.uint8), (complete.codes >= 2).astype(np.uint8)], 2)
+    mj = np.zeros(g.shape, np.int64)
+    for k in range(1, 4):
+        mj += g >= k * (k + 1) // 2
+    mi = g.astype(np.int64) - mj * (mj + 1) // 2
+    ma = np.stack([mi, mj], 2).astype(np.uint8)
+    ma[g == 255] = 255
+    # the allele count of a site is its largest called allele + 1 here
+    top = np.where(g == 255, 0, mj).max(0)
+    keep = top >= 2
+    genotypes = np.concatenate([bi.transpose(1, 0, 2), ma[:, keep].transpose(1, 0, 2)], 0)
+    co = kb.relatedness_coefficients_gt(genotypes, estimator="cls")
+    ref = oracle.cls_relatedness(complete.codes, multi=(g[:, keep], (top[keep] + 1).astype(np.uint8), None))
+    x, y = ref["x"].astype(int), ref["y"].astype(int)
+    ident = np.log10(ref["cond"]) <= 4
+    assert np.abs(co.jacquard[x, y] - ref["jacquard"]).max(1)[ident].max() <= 1e-5
+    assert co.jacquard.shape == (n, n, 9)

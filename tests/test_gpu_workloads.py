@@ -190,7 +190,7 @@ def test_autotune_and_launch_shape_leave_results_unchanged():
         est.load(co.codes)
         base = est.relatedness()
         slots, bps = est.autotune()
-        assert slots == 0 and bps in (3, 4, 5)
+        assert slots == 0 and bps in (2, 3, 4)   # the candidates kg_autotune times
         tuned = est.relatedness()
         est.set_launch(64, 2)      # few slots in flight: many more waves
         small = est.relatedness()
