@@ -66,7 +66,7 @@ size_t Cohort::device_bytes() const {
     return raw.bytes + af.bytes + rc.bytes + oc.bytes + keep.bytes + kidx.bytes + bsum.bytes +
            nkept.bytes + pfull.bytes + qfull.bytes + p32.bytes + p64.bytes + q64.bytes +
            site_of.bytes + planes.bytes + cls_q.bytes + cls_part.bytes + mg.bytes + malleles.bytes + maf.bytes +
-           mfreq.bytes + mkeep.bytes + mcount.bytes + mpart.bytes + cmulti.bytes;
+           mfreq.bytes + mkeep.bytes + mcount.bytes + mpart.bytes + cmulti.bytes + mgT.bytes;
 }
 
 const char* engine_version() { return "kestrel-b200 0.1.0 (sm_100a)"; }
@@ -364,45 +364,83 @@ __global__ void __launch_bounds__(GRAM_THREADS) multi_gram_kernel(const uint8_t*
     }
 }
 
-// Warp per output row r of the first ns samples (x-major, y >= x, the
-// reference's order): the 9 sums over used multi-allelic sites of
-// m[gx][gy], lanes striding over the sites, then a fixed butterfly reduction.
-__global__ void multi_c_kernel(const uint8_t* __restrict__ mg, const double* __restrict__ mfreq,
-                               const uint8_t* __restrict__ mkeep, int64_t n_multi, int64_t ns, int64_t n_rows,
-                               double* __restrict__ cm) {
-    const int lane = threadIdx.x & 31;
-    const int64_t w0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    for (int64_t r = w0; r < n_rows; r += nw) {
-        int64_t lo = 0, hi = ns - 1;   // the largest x whose first row is <= r
-        while (lo < hi) {
-            const int64_t mid = (lo + hi + 1) / 2;
-            if (mid * ns - mid * (mid - 1) / 2 <= r) lo = mid;
-            else hi = mid - 1;
-        }
-        const int64_t x = lo, y = x + (r - (x * ns - x * (x - 1) / 2));
-        const uint8_t* gxr = mg + x * n_multi;
-        const uint8_t* gyr = mg + y * n_multi;
+// Site-major copy of the genotype indices (out[c * rows + r] = in[r * cols + c])
+// through 32 x 32 shared-memory tiles.
+__global__ void transpose_u8_kernel(const uint8_t* __restrict__ in, int64_t rows, int64_t cols,
+                                    uint8_t* __restrict__ out) {
+    __shared__ uint8_t t[32][33];
+    const int64_t c0 = (int64_t)blockIdx.x * 32, r0 = (int64_t)blockIdx.y * 32;
+    for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+        const int64_t r = r0 + k, c = c0 + threadIdx.x;
+        if (r < rows && c < cols) t[k][threadIdx.x] = in[r * cols + c];
+    }
+    __syncthreads();
+    for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+        const int64_t c = c0 + k, r = r0 + threadIdx.x;
+        if (r < rows && c < cols) out[c * rows + r] = t[threadIdx.x][k];
+    }
+}
+
+// Per output row (x, y) of the first ns samples, the 9 sums over used
+// multi-allelic sites of m[gx][gy], in site order.  Block per x; per tile of
+// MC_SITES sites the block evaluates x's rows m[gx][.] (at most 10 genotypes,
+// rows padded to 10 doubles) into shared memory, then each thread adds, for
+// its y, the row its genotype selects (y's indices from the site-major copy,
+// adjacent threads adjacent samples).
+constexpr int MC_SITES = 48;
+constexpr int MC_THREADS = 256;
+__global__ void __launch_bounds__(MC_THREADS) multi_c_kernel(const uint8_t* __restrict__ mg,
+                                                             const uint8_t* __restrict__ mgT,
+                                                             const uint8_t* __restrict__ mal,
+                                                             const double* __restrict__ mfreq,
+                                                             const uint8_t* __restrict__ mkeep, int64_t n_samples,
+                                                             int64_t n_multi, int64_t ns, double* __restrict__ cm) {
+    __shared__ __align__(16) double tile[MC_SITES * 10 * 10];
+    __shared__ uint8_t used[MC_SITES];
+    const int64_t x = blockIdx.x;
+    const int64_t row0 = x * ns - x * (x - 1) / 2;   // the row of (x, x)
+    for (int64_t y0 = x; y0 < ns; y0 += MC_THREADS) {
+        const int64_t y = y0 + threadIdx.x;
         double acc[9];
 #pragma unroll
         for (int t = 0; t < 9; t++) acc[t] = 0.0;
-        for (int64_t v = lane; v < n_multi; v += 32) {
-            if (!mkeep[v]) continue;
-            int i, j, k, l;
-            genotype_alleles(gxr[v], i, j);
-            genotype_alleles(gyr[v], k, l);
-            double row[9];
-            iis_row(i, j, k, l, mfreq[4 * v], mfreq[4 * v + 1], mfreq[4 * v + 2], mfreq[4 * v + 3], row);
+        for (int64_t v0 = 0; v0 < n_multi; v0 += MC_SITES) {
+            const int nv = (int)(n_multi - v0 < MC_SITES ? n_multi - v0 : MC_SITES);
+            __syncthreads();   // the previous tile has been read
+            for (int e = threadIdx.x; e < nv * 10; e += MC_THREADS) {
+                const int vl = e / 10, gy = e - vl * 10;
+                const int64_t v = v0 + vl;
+                const int na = mal[v], ng = na * (na + 1) / 2;
+                const bool use = mkeep[v] != 0;
+                if (gy == 0) used[vl] = use ? 1 : 0;
+                if (use && gy < ng) {
+                    int i, j, k, l;
+                    genotype_alleles(mg[x * n_multi + v], i, j);
+                    genotype_alleles(gy, k, l);
+                    double row[9];
+                    iis_row(i, j, k, l, mfreq[4 * v], mfreq[4 * v + 1], mfreq[4 * v + 2], mfreq[4 * v + 3], row);
+                    double* dst = tile + (vl * 10 + gy) * 10;
 #pragma unroll
-            for (int t = 0; t < 9; t++) acc[t] += row[t];
+                    for (int t = 0; t < 9; t++) dst[t] = row[t];
+                }
+            }
+            __syncthreads();
+            if (y < ns) {
+                for (int vl = 0; vl < nv; vl++) {
+                    if (!used[vl]) continue;   // the same for every thread
+                    const int gy = mgT[(v0 + vl) * n_samples + y];
+                    const double2* r = reinterpret_cast<const double2*>(tile + (vl * 10 + gy) * 10);
+                    const double2 a0 = r[0], a1 = r[1], a2 = r[2], a3 = r[3];
+                    const double a8 = tile[(vl * 10 + gy) * 10 + 8];
+                    acc[0] += a0.x; acc[1] += a0.y; acc[2] += a1.x; acc[3] += a1.y;
+                    acc[4] += a2.x; acc[5] += a2.y; acc[6] += a3.x; acc[7] += a3.y;
+                    acc[8] += a8;
+                }
+            }
         }
+        if (y < ns)
 #pragma unroll
-        for (int t = 0; t < 9; t++)
-#pragma unroll
-            for (int off = 16; off > 0; off >>= 1) acc[t] += __shfl_xor_sync(0xffffffffu, acc[t], off);
-        if (lane == 0)
-#pragma unroll
-            for (int t = 0; t < 9; t++) cm[r * 9 + t] = acc[t];
+            for (int t = 0; t < 9; t++) cm[(row0 + (y - x)) * 9 + t] = acc[t];
     }
 }
 
@@ -728,6 +766,7 @@ int prepare_multi(Cohort& c, bool have_af, int64_t num_samples, cudaStream_t st,
     KG_CUDA_TRY((cudaError_t)c.mcount.reserve(sizeof(int32_t) * 2));
     KG_CUDA_TRY((cudaError_t)c.mpart.reserve(sizeof(double) * GRAM_BLOCKS * 45));
     KG_CUDA_TRY((cudaError_t)c.cmulti.reserve(sizeof(double) * 9 * rows));
+    KG_CUDA_TRY((cudaError_t)c.mgT.reserve((size_t)(n * c.n_samples)));
     KG_CUDA_TRY(cudaMemsetAsync(c.mcount.p, 0, sizeof(int32_t) * 2, st));
     multi_freq_kernel<<<grid_for(n, 256), 256, 0, st>>>(c.mg.as<uint8_t>(), c.malleles.as<uint8_t>(),
                                                          have_af ? c.maf.as<double>() : nullptr, c.n_samples, n,
@@ -738,9 +777,11 @@ int prepare_multi(Cohort& c, bool have_af, int64_t num_samples, cudaStream_t st,
     cls_gram_final_kernel<<<1, 64, 0, st>>>(c.cls_part.as<double>(), c.nkept.as<int32_t>(), c.mpart.as<double>(),
                                             c.mcount.as<int32_t>(), c.cls_q.as<double>());
     {
-        const int blocks = (int)std::min<int64_t>(ceil_div(rows * 32, 256), 148 * 8);
-        multi_c_kernel<<<blocks, 256, 0, st>>>(c.mg.as<uint8_t>(), c.mfreq.as<double>(), c.mkeep.as<uint8_t>(), n,
-                                               num_samples, rows, c.cmulti.as<double>());
+        const dim3 tg((unsigned)ceil_div(n, 32), (unsigned)ceil_div(c.n_samples, 32));
+        transpose_u8_kernel<<<tg, dim3(32, 8), 0, st>>>(c.mg.as<uint8_t>(), c.n_samples, n, c.mgT.as<uint8_t>());
+        multi_c_kernel<<<(unsigned)num_samples, MC_THREADS, 0, st>>>(
+            c.mg.as<uint8_t>(), c.mgT.as<uint8_t>(), c.malleles.as<uint8_t>(), c.mfreq.as<double>(),
+            c.mkeep.as<uint8_t>(), c.n_samples, n, num_samples, c.cmulti.as<double>());
     }
     KG_CUDA_TRY(cudaGetLastError());
     int32_t h[2];

@@ -82,6 +82,7 @@ struct Cohort {
     int64_t n_multi = 0;       // loaded sites
     int64_t n_multi_kept = -1; // sites every sample calls (read back after preparation)
     DevBuf mg;                 // uint8 genotype indices (VCF order, 255 = missing), n_samples x n_multi
+    DevBuf mgT;                // the same, site-major (n_multi x n_samples)
     DevBuf malleles;           // uint8 allele count per site (3 or 4)
     DevBuf maf;                // caller frequencies, n_multi x 4 (optional)
     DevBuf mfreq;              // double frequencies used, n_multi x 4
