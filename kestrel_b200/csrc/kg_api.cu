@@ -592,7 +592,7 @@ int kg_relatedness_gt(kg_ctx* c, int64_t num_samples, uint64_t iterations, kg_ou
         cudaEventDestroy(ev0);
         cudaEventDestroy(ev1);
         stats.launches += 9;  // count, freq, two scans, compact, pad, pack, Gram, Gram total
-        if (c->cohort.n_multi > 0) stats.launches += 4;   // multi-allelic frequencies, Gram, Gram total, rows
+        if (c->cohort.n_multi > 0) stats.launches += 5;   // multi-allelic frequencies, Gram, Gram total, transpose, rows
         if (st2 && !st) st = st2;
         stats.total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
         c->last = stats;
