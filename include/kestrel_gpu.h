@@ -301,6 +301,9 @@ int kg_vcf_info(const kg_vcf *vcf, int64_t *n_samples, int64_t *n_sites, uint64_
  * af: n_sites x 2 [REF, ALT] from INFO/AF (KG_EINVAL if it was not read).
  * Either may be NULL. */
 int kg_vcf_codes(const kg_vcf *vcf, uint8_t *codes, double *af);
+/* The same codes packed as kg_load_genotypes_2bit takes them (2-bit codes and
+ * the observed mask, rows of ceil(n_sites/16) and ceil(n_sites/32) words). */
+int kg_vcf_codes_2bit(const kg_vcf *vcf, uint32_t *codes2, uint32_t *observed);
 /* GT: the tri- and tetra-allelic records that every sample calls (counts[5] +
  * counts[6] of them), the input of kg_load_multiallelic: gidx n_samples x
  * that many genotype indices (sample-major), n_alleles one per record, af (4

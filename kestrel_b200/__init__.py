@@ -19,7 +19,7 @@ from ._lib import (KG_ECUDA, KG_EINVAL, KG_ENOMEM, KG_ENOSITES, KG_ENOTFOUND, KG
                    KG_PREC_FP32C, KG_PREC_FP64, MISSING, OUTPUT_DTYPE, KestrelError, KgCohort, KgRunStats, lib,
                    ptr)
 
-__all__ = ["Coefficients", "relatedness_coefficients_gt", "relatedness_coefficients_gl", "read_vcf",
+__all__ = ["Coefficients", "relatedness_coefficients_gt", "relatedness_coefficients_gl", "read_vcf", "pack_2bit",
            "run_cli", "Estimator", "genotype_codes", "build_arrays", "KestrelError",
            "OUTPUT_DTYPE", "MISSING", "KINSHIP_VECTOR", "KG_OK", "KG_EINVAL", "KG_ENOMEM", "KG_ECUDA",
            "KG_ETIMEOUT", "KG_ENOSITES", "KG_ENOTREADY", "KG_ENOTFOUND", "KG_PREC_FP32C", "KG_PREC_FP64"]
@@ -62,6 +62,24 @@ def genotype_codes(genotypes: np.ndarray) -> np.ndarray:
     codes = (a[..., 0] + a[..., 1]).astype(np.uint8)
     codes[miss.any(axis=2)] = MISSING
     return np.ascontiguousarray(codes.T)
+
+
+def pack_2bit(codes: np.ndarray):
+    """Sample-major codes [samples, sites] (3 = missing) -> the packed form of
+    kg_load_genotypes_2bit: (2-bit codes uint32 [samples, ceil(sites/16)], site
+    s at bits 2 (s % 16), 0 where missing; observed mask uint32 [samples,
+    ceil(sites/32)], bit s % 32)."""
+    c = np.ascontiguousarray(codes, dtype=np.uint8)
+    n, m = c.shape
+    called = c < 3
+    m16, m32 = -(-m // 16) * 16, -(-m // 32) * 32
+    cc = np.zeros((n, m16), np.uint32)
+    cc[:, :m] = np.where(called, c, 0)
+    codes2 = (cc.reshape(n, -1, 16) << (2 * np.arange(16, dtype=np.uint32))).sum(2, dtype=np.uint64).astype(np.uint32)
+    ob = np.zeros((n, m32), np.uint32)
+    ob[:, :m] = called
+    observed = (ob.reshape(n, -1, 32) << np.arange(32, dtype=np.uint32)).sum(2, dtype=np.uint64).astype(np.uint32)
+    return np.ascontiguousarray(codes2), np.ascontiguousarray(observed)
 
 
 def build_arrays(rows: np.ndarray, num_samples: int):
@@ -138,6 +156,24 @@ class Estimator:
         if allele_frequencies is not None:
             af = np.ascontiguousarray(allele_frequencies, dtype=np.float64)
             if af.shape != (m, 2):
+                raise ValueError("allele_frequencies must be (sites, 2)")
+            _check(self._L.kg_set_allele_frequencies(self._h, ptr(af)), self._h)
+            self._af = af
+        return self
+
+    def load_packed(self, codes2: np.ndarray, observed: np.ndarray, n_sites: int, allele_frequencies=None):
+        """Loads a cohort from the packed form (pack_2bit, the VCF reader's
+        read_vcf(..., packed=True)): unpacked to byte codes on the device."""
+        c2 = np.ascontiguousarray(codes2, dtype=np.uint32)
+        ob = np.ascontiguousarray(observed, dtype=np.uint32)
+        n = c2.shape[0]
+        if c2.shape != (n, -(-n_sites // 16)) or ob.shape != (n, -(-n_sites // 32)):
+            raise ValueError("codes2 must be (samples, ceil(sites/16)) and observed (samples, ceil(sites/32))")
+        _check(self._L.kg_load_genotypes_2bit(self._h, ptr(c2), ptr(ob), n, int(n_sites)), self._h)
+        self.n_samples, self.n_sites = n, int(n_sites)
+        if allele_frequencies is not None:
+            af = np.ascontiguousarray(allele_frequencies, dtype=np.float64)
+            if af.shape != (n_sites, 2):
                 raise ValueError("allele_frequencies must be (sites, 2)")
             _check(self._L.kg_set_allele_frequencies(self._h, ptr(af)), self._h)
             self._af = af
@@ -318,7 +354,7 @@ def relatedness_coefficients_gt(genotypes, allele_frequencies=None, threads=None
 
 
 def read_vcf(path, field: str = "GT", allele_freqs: str = "estimate", threads: int = 0,
-             multiallelic: bool = False):
+             multiallelic: bool = False, packed: bool = False):
     """Reads a plain, gzip or bgzip VCF with the library's multithreaded reader
     (the CLI's): biallelic SNP records become genotype codes.  Returns
     (codes u8 [samples, sites], allele_frequencies f64 [sites, 2] or None,
@@ -326,7 +362,8 @@ def read_vcf(path, field: str = "GT", allele_freqs: str = "estimate", threads: i
     multiallelic (GT), a fifth item holds the tri- and tetra-allelic records
     every sample calls: (genotype indices u8 [samples, sites], allele counts u8
     [sites], allele frequencies f64 [sites, 4] or None), the arguments of
-    Estimator.load_multiallelic."""
+    Estimator.load_multiallelic.  With packed, codes is (2-bit codes,
+    observed mask) as pack_2bit gives them, for Estimator.load_packed."""
     if allele_freqs not in ("estimate", "info"):
         raise ValueError("allele_freqs must be 'estimate' or 'info'")
     L = lib()
@@ -340,9 +377,15 @@ def read_vcf(path, field: str = "GT", allele_freqs: str = "estimate", threads: i
         ns, nv = ctypes.c_int64(), ctypes.c_int64()
         counts = (ctypes.c_uint64 * 7)()
         _check_vcf(L.kg_vcf_info(h, ctypes.byref(ns), ctypes.byref(nv), counts), L, h)
-        codes = np.empty((ns.value, nv.value), np.uint8)
         af = np.empty((nv.value, 2)) if allele_freqs == "info" else None
-        _check_vcf(L.kg_vcf_codes(h, ptr(codes), ptr(af)), L, h)
+        if packed:
+            codes = (np.empty((ns.value, -(-nv.value // 16)), np.uint32),
+                     np.empty((ns.value, -(-nv.value // 32)), np.uint32))
+            _check_vcf(L.kg_vcf_codes_2bit(h, ptr(codes[0]), ptr(codes[1])), L, h)
+            _check_vcf(L.kg_vcf_codes(h, None, ptr(af)), L, h)
+        else:
+            codes = np.empty((ns.value, nv.value), np.uint8)
+            _check_vcf(L.kg_vcf_codes(h, ptr(codes), ptr(af)), L, h)
         names = [L.kg_vcf_sample(h, i).decode() for i in range(ns.value)]
         cd = {"records": counts[0], "not_snp": counts[1], "multiallelic": counts[2],
               "soft_likelihoods": counts[3], "with_missing": counts[4], "tri_allelic": counts[5],

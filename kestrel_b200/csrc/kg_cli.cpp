@@ -299,7 +299,6 @@ extern "C" int kg_run_cli(int argc, const char* const* argv) {
         std::fprintf(stderr, "Error: Must have at least one site and one sample\n");
         return 1;
     }
-    const kg::Bytes& codes = vcf.codes;
     int64_t nsel = o.samples < 0 ? ns : o.samples;
     if (nsel > ns) {
         std::fprintf(stderr, "Error: Requested samples %lld exceeds total samples %lld\n", (long long)nsel, (long long)ns);
@@ -315,7 +314,10 @@ extern "C" int kg_run_cli(int argc, const char* const* argv) {
     }
     kg_ctx* ctx = dev.ctx;
     int st = 0;
-    st = kg_load_genotypes(ctx, codes.data(), ns, nv, nv);
+    // the reader's codes go up packed: 2 bits a call plus the observed mask
+    std::vector<uint32_t> codes2((size_t)(ns * ((nv + 15) / 16))), observed((size_t)(ns * ((nv + 31) / 32)));
+    kg::pack_2bit(vcf, o.threads, codes2.data(), observed.data());
+    st = kg_load_genotypes_2bit(ctx, codes2.data(), observed.data(), ns, nv);
     if (!st && o.af_info) st = kg_set_allele_frequencies(ctx, af.data());
     if (!st && o.cls && vcf.n_multi > 0)
         st = kg_load_multiallelic(ctx, vcf.mcodes.data(), ns, vcf.n_multi, vcf.n_multi, vcf.malleles.data(),

@@ -733,6 +733,34 @@ int read_vcf(const std::string& path, char field, bool af_info, int threads, Vcf
     return 0;
 }
 
+void pack_2bit(const VcfData& d, int threads, uint32_t* codes2, uint32_t* observed) {
+    const int64_t ns = (int64_t)d.samples.size(), nv = d.n_sites;
+    const int64_t w2 = (nv + 15) / 16, wm = (nv + 31) / 32;
+    parallel_for(host_threads(threads), ns, [&](int, int64_t s0, int64_t s1) {
+        for (int64_t s = s0; s < s1; s++) {
+            const uint8_t* row = d.codes.data() + s * nv;
+            uint32_t* c2 = codes2 + s * w2;
+            uint32_t* ob = observed + s * wm;
+            for (int64_t w = 0; w < wm; w++) {
+                uint32_t lo = 0, hi = 0, seen = 0;
+                const int64_t v0 = w * 32;
+                const int n = (int)std::min<int64_t>(32, nv - v0);
+                for (int k = 0; k < n; k++) {
+                    const uint32_t c = row[v0 + k];
+                    const uint32_t called = c < 3 ? 1u : 0u;
+                    const uint32_t cc = called ? c : 0u;
+                    seen |= called << k;
+                    if (k < 16) lo |= cc << (2 * k);
+                    else hi |= cc << (2 * (k - 16));
+                }
+                ob[w] = seen;
+                c2[2 * w] = lo;
+                if (2 * w + 1 < w2) c2[2 * w + 1] = hi;
+            }
+        }
+    });
+}
+
 }  // namespace kg
 
 // ------------------------------------------------------------------- C ABI
@@ -797,6 +825,12 @@ extern "C" int kg_vcf_codes(const kg_vcf* v, uint8_t* codes, double* af) {
         if (v->d.af.empty()) return KG_EINVAL;
         std::memcpy(af, v->d.af.data(), sizeof(double) * v->d.af.size());
     }
+    return KG_OK;
+}
+
+extern "C" int kg_vcf_codes_2bit(const kg_vcf* v, uint32_t* codes2, uint32_t* observed) {
+    if (!v || !codes2 || !observed) return KG_EINVAL;
+    kg::pack_2bit(v->d, 0, codes2, observed);
     return KG_OK;
 }
 

@@ -53,6 +53,12 @@ struct VcfData {
     uint64_t tri = 0, tetra = 0;
 };
 
+// The codes in the packed form kg_load_genotypes_2bit takes: per sample
+// ceil(n_sites / 16) words of 2-bit codes (site s at bits 2 (s % 16) of word
+// s / 16, 0 where missing) and ceil(n_sites / 32) words of the observed mask
+// (bit s % 32 of word s / 32).  Samples in parallel over `threads`.
+void pack_2bit(const VcfData& d, int threads, uint32_t* codes2, uint32_t* observed);
+
 // field: 'T' GT, 'L' GL, 'P' PL.  af_info: read INFO/AF (an error when absent).
 // threads <= 0: all hardware threads.  Returns 0, or 1 with err set (the
 // message of the first bad record in file order).

@@ -259,3 +259,14 @@ def test_cli_gt_default_fits_tri_and_tetra_allelic_records(oracle):
     assert len(rows) == len(ref)
     assert np.abs(jac - ref["jacquard"]).max(1)[ident].max() <= 1e-5
     assert (np.abs(obj - ref["obj"]) / np.abs(ref["obj"])).max() <= 1e-6
+
+
+def test_packed_load_equals_byte_load():
+    co = synth.make_cohort(70, 3001, seed=52, missing=0.02, name="packed")   # ragged last words
+    c2, ob = kb.pack_2bit(co.codes)
+    with kb.Estimator() as est:
+        est.load(co.codes)
+        ml, gt = est.relatedness(), est.relatedness_gt()
+        est.load_packed(c2, ob, co.codes.shape[1])
+        ml2, gt2 = est.relatedness(), est.relatedness_gt()
+    assert _bitwise_equal(ml, ml2) and _bitwise_equal(gt, gt2)

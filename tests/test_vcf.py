@@ -292,3 +292,20 @@ def test_fifo_input_is_read_without_mapping(cohort):
         codes, _, names, counts = kb.read_vcf(p, "GT", threads=4)
         th.join()
     assert np.array_equal(codes, ref[0]) and names == ref[2] and counts == ref[3]
+
+
+def test_packed_codes_decode_to_the_byte_codes():
+    co = synth.make_cohort(21, 3001, 63, missing=0.05, name="packed")   # ragged last words
+    text = make_text(co.codes, "GT", extra=False)
+    with tempfile.TemporaryDirectory() as td:
+        p = os.path.join(td, "x.vcf")
+        open(p, "w").write(text)
+        (c2, ob), _, _, _ = kb.read_vcf(p, "GT", packed=True, threads=3)
+        codes, _, _, _ = kb.read_vcf(p, "GT")
+    assert np.array_equal(codes, co.codes)
+    n2, nm = kb.pack_2bit(codes)
+    assert np.array_equal(c2, n2) and np.array_equal(ob, nm)
+    s = np.arange(codes.shape[1])
+    dec = (c2[:, s // 16] >> (2 * (s % 16)).astype(np.uint32)) & 3
+    obs = (ob[:, s // 32] >> (s % 32).astype(np.uint32)) & 1
+    assert np.array_equal(np.where(obs == 1, dec, 3), codes)
