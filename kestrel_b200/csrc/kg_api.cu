@@ -421,7 +421,8 @@ int kg_load_genotypes_2bit(kg_ctx* c, const uint32_t* codes2, const uint32_t* ob
         int st = use_device(c);
         if (st) return st;
         std::string err;
-        st = kg::unpack_2bit(c->cohort.raw, codes2, observed, n_samples, n_sites, c->stream, err);
+        st = kg::unpack_2bit(c->cohort.raw, c->cohort.packed2, c->cohort.packedm, codes2, observed, n_samples,
+                             n_sites, c->stream, err);
         if (st) return set_err(c, st, err);
         c->cohort.n_samples = n_samples;
         c->cohort.n_sites = n_sites;

@@ -591,14 +591,13 @@ int prepare_cohort(Cohort& c, const uint8_t* codes, int64_t n_samples, int64_t n
     return KG_OK;
 }
 
-int unpack_2bit(DevBuf& raw, const uint32_t* codes2, const uint32_t* observed, int64_t n_samples,
-                int64_t n_sites, cudaStream_t st, std::string& err) {
+int unpack_2bit(DevBuf& raw, DevBuf& d2, DevBuf& dm, const uint32_t* codes2, const uint32_t* observed,
+                int64_t n_samples, int64_t n_sites, cudaStream_t st, std::string& err) {
     if (!codes2 || !observed || n_samples <= 0 || n_sites <= 0) {
         err = "invalid packed genotype arguments";
         return KG_EINVAL;
     }
     int64_t w2 = ceil_div(n_sites, 16), wm = ceil_div(n_sites, 32);
-    DevBuf d2, dm;
     KG_CUDA_TRY((cudaError_t)d2.reserve(sizeof(uint32_t) * w2 * n_samples));
     KG_CUDA_TRY((cudaError_t)dm.reserve(sizeof(uint32_t) * wm * n_samples));
     KG_CUDA_TRY((cudaError_t)raw.reserve((size_t)(n_samples * n_sites)));

@@ -64,6 +64,7 @@ struct Cohort {
     int64_t n_seg_max = 0;     // segments for n_sites (upper bound of the kept count)
     int64_t n_kept = -1;       // read back after preparation (-1 = not yet)
     DevBuf raw;                // uint8 codes, n_samples x n_sites
+    DevBuf packed2, packedm;   // the last packed upload (2-bit codes, observed mask)
     DevBuf af;                 // caller frequencies, n_sites x 2 (optional)
     DevBuf rc, oc;             // int32 REF allele count, observed samples
     DevBuf keep;               // uint8
@@ -108,9 +109,10 @@ int prepare_cohort(Cohort& c, const uint8_t* codes, int64_t n_samples, int64_t n
 // summed rows (c.cmulti).  Sets c.n_multi_kept.
 int prepare_multi(Cohort& c, bool have_af, int64_t num_samples, cudaStream_t st, std::string& err);
 
-// Unpacks the VCF reader's 2-bit codes + observed mask into device byte codes.
-int unpack_2bit(DevBuf& raw, const uint32_t* codes2, const uint32_t* observed, int64_t n_samples,
-                int64_t n_sites, cudaStream_t st, std::string& err);
+// Unpacks the VCF reader's 2-bit codes + observed mask into device byte codes
+// (d2, dm: the packed rows' device copies, kept for the next load).
+int unpack_2bit(DevBuf& raw, DevBuf& d2, DevBuf& dm, const uint32_t* codes2, const uint32_t* observed,
+                int64_t n_samples, int64_t n_sites, cudaStream_t st, std::string& err);
 
 // Packs query rows against a prepared panel (same raw site order); sites with
 // mask[s] == 0 become missing.  Host inputs.
