@@ -387,7 +387,7 @@ def read_vcf(path, field: str = "GT", allele_freqs: str = "estimate", threads: i
             codes = np.empty((ns.value, nv.value), np.uint8)
             _check_vcf(L.kg_vcf_codes(h, ptr(codes), ptr(af)), L, h)
         names = [L.kg_vcf_sample(h, i).decode() for i in range(ns.value)]
-        cd = {"records": counts[0], "not_snp": counts[1], "multiallelic": counts[2],
+        cd = {"sites": nv.value, "records": counts[0], "not_snp": counts[1], "multiallelic": counts[2],
               "soft_likelihoods": counts[3], "with_missing": counts[4], "tri_allelic": counts[5],
               "tetra_allelic": counts[6]}
         if not multiallelic:

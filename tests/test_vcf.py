@@ -129,7 +129,7 @@ def py_parse(text, field="GT", af_info=False):
     ns = len(samples)
     codes = np.array(rows, np.uint8).T.reshape(ns, len(rows)) if rows else np.zeros((ns, 0), np.uint8)
     mg = np.array(mrows, np.uint8).T.reshape(ns, len(mrows)) if mrows else np.zeros((ns, 0), np.uint8)
-    counts = {"records": total, "not_snp": not_snp, "multiallelic": multi, "soft_likelihoods": soft,
+    counts = {"sites": len(rows), "records": total, "not_snp": not_snp, "multiallelic": multi, "soft_likelihoods": soft,
               "with_missing": with_missing, "tri_allelic": tri, "tetra_allelic": tetra}
     return codes, (np.array(afs) if af_info else None), samples, counts, \
         (mg, np.array(malleles, np.uint8), (np.array(mafs).reshape(-1, 4) if af_info else None))
