@@ -1024,3 +1024,307 @@ int kor_cls_relatedness_ma(const uint8_t *codes, int64_t n_samples, int64_t n_si
     free(site); free(p); free(q); free(msite); free(mf);
     return KOR_OK;
 }
+
+/* ---------------------------------- soft genotype likelihoods (the GL/PL path) */
+/* The reference's GL/PL estimator on likelihoods that need not be one-hot
+ * (src/wrapper.rs:89-330, src/allele/mod.rs, src/mixture.rs, src/coefficients.rs:
+ * 40-141).  Likelihoods are linear-scale, genotype-major per sample in the VCF
+ * order (G = 3, 6, 10 for 2, 3, 4 alleles); a sample whose row holds a NaN is
+ * missing (src/vcf.rs:355, src/lanevector.rs:99-104 drop such rows). */
+
+typedef struct {
+    const double *gl;  /* n_samples x g */
+    int64_t n_samples;
+    int a, g;
+} af_site_t;
+
+static int row_ok(const double *r, int g) {
+    for (int k = 0; k < g; k++)
+        if (isnan(r[k])) return 0;
+    return 1;
+}
+
+/* -(1/n) sum over called samples of log(eps + x' L x), L the symmetric matrix of
+ * the sample's likelihoods (L_ii = GL(i,i), L_ij = L_ji = GL(i,j)): the HWE
+ * mixture x_i^2 GL(i,i) + 2 x_i x_j GL(i,j) (src/allele/objective.rs). */
+static double af_objective(const void *ctx, const double *x, double eps) {
+    const af_site_t *s = (const af_site_t *)ctx;
+    double acc = 0.0;
+    int64_t n = 0;
+    for (int64_t k = 0; k < s->n_samples; k++) {
+        const double *r = s->gl + k * s->g;
+        if (!row_ok(r, s->g)) continue;
+        double p = eps;
+        for (int b = 0; b < s->a; b++)
+            for (int a = 0; a <= b; a++) {
+                const double w = a == b ? x[a] * x[a] : 2.0 * x[a] * x[b];
+                p = fma(w, r[b * (b + 1) / 2 + a], p);
+            }
+        acc += log(p);
+        n++;
+    }
+    return -acc / (double)n;
+}
+
+/* gradient -2/n sum Lx/d and Hessian 2/n sum (2 (Lx/d)(Lx/d)' - L/d), d =
+ * eps + x' L x (src/allele/grad_hess.rs:81-172). */
+static void af_grad_hess(const void *ctx, const double *x, double eps, double g[9], double H[9][9]) {
+    const af_site_t *s = (const af_site_t *)ctx;
+    const int A = s->a;
+    double zg[4] = {0, 0, 0, 0}, zh[4][4];
+    memset(zh, 0, sizeof zh);
+    int64_t n = 0;
+    for (int64_t k = 0; k < s->n_samples; k++) {
+        const double *r = s->gl + k * s->g;
+        if (!row_ok(r, s->g)) continue;
+        double L[4][4];
+        for (int b = 0; b < A; b++)
+            for (int a = 0; a <= b; a++) L[a][b] = L[b][a] = r[b * (b + 1) / 2 + a];
+        double lx[4], d = eps;
+        for (int a = 0; a < A; a++) {
+            lx[a] = 0.0;
+            for (int b = 0; b < A; b++) lx[a] = fma(L[a][b], x[b], lx[a]);
+        }
+        for (int a = 0; a < A; a++) d = fma(x[a], lx[a], d);
+        const double inv = 1.0 / d;
+        for (int a = 0; a < A; a++) {
+            zg[a] = fma(lx[a], inv, zg[a]);
+            for (int b = 0; b < A; b++) zh[a][b] += 2.0 * (lx[a] * inv) * (lx[b] * inv) - L[a][b] * inv;
+        }
+        n++;
+    }
+    for (int i = 0; i < 9; i++) {
+        g[i] = 0.0;
+        for (int j = 0; j < 9; j++) H[i][j] = 0.0;
+    }
+    for (int a = 0; a < A; a++) {
+        g[a] = -2.0 * zg[a] / (double)n;
+        for (int b = 0; b < A; b++) H[a][b] = 2.0 * zh[a][b] / (double)n;
+    }
+}
+
+static int kkt_converged_n(int n, const double *x, const double *g, double tol) {
+    const double lambda = dotn(n, x, g);
+    for (int i = 0; i < n; i++) {
+        if (x[i] == 0.0) {
+            if (!(g[i] >= lambda - tol)) return 0;
+        } else if (!(fabs(g[i] - lambda) <= tol)) {
+            return 0;
+        }
+    }
+    return 1;
+}
+
+typedef double (*sqp_obj_fn)(const void *, const double *, double);
+typedef void (*sqp_gh_fn)(const void *, const double *, double, double g[9], double H[9][9]);
+
+/* src/sqp.rs:49-93 and :270-310 for a problem of dimension n <= 9 given by its
+ * objective and gradient/Hessian; returns the iteration count. */
+static uint64_t solve_sqp_n(int n, sqp_obj_fn fo, sqp_gh_fn fgh, const void *ctx, const double *x0,
+                            const tune_t *tu, double x_out[9], double *f_out) {
+    double x[9] = {0};
+    sum_to_one_n(n, x0, x);
+    double f = fo(ctx, x, tu->epsilon);
+    for (uint64_t it = 0; it < tu->sqp_max_iter; it++) {
+        double g[9], H[9][9];
+        fgh(ctx, x, tu->epsilon, g, H);
+        if (kkt_converged_n(n, x, g, tu->sqp_conv_tol)) {
+            memcpy(x_out, x, sizeof x);
+            *f_out = f;
+            return it;
+        }
+        double hx[9] = {0}, c[9] = {0}, y[9] = {0}, p[9] = {0};
+        matvec(n, H, x, hx);
+        for (int i = 0; i < n; i++) c[i] = g[i] - hx[i];
+        qp_active_set_n(n, H, c, x, tu, y);
+        for (int i = 0; i < n; i++) p[i] = y[i] - x[i];
+        const double t = tu->bls_sufficient_decrease * dotn(n, g, p);
+        double alpha = 1.0, xs[9] = {0}, fn;
+        uint64_t ls = 0;
+        for (;;) {
+            double xn[9] = {0};
+            for (int i = 0; i < n; i++) xn[i] = x[i] + alpha * p[i];
+            sum_to_one_n(n, xn, xs);
+            fn = fo(ctx, xs, tu->epsilon);
+            if (fn <= f + alpha * t) break;
+            if (++ls == tu->bls_max_iter) break;
+            alpha *= tu->bls_step_size_reduce;
+        }
+        memcpy(x, xs, sizeof x);
+        f = fn;
+    }
+    memcpy(x_out, x, sizeof x);
+    *f_out = f;
+    return tu->sqp_max_iter;
+}
+
+/* One site's allele frequencies (src/allele/mod.rs:91-134): the SQP from 1/A
+ * (sqp_max_iter = iterations, the QP at most A + 1 iterations); frequencies in
+ * (0, maf) become 0 and the rest sum to one.  NaN when no sample is called. */
+static void af_fit(const af_site_t *s, uint64_t iterations, double maf, double f_out[4]) {
+    for (int a = 0; a < 4; a++) f_out[a] = 0.0;
+    int64_t called = 0;
+    for (int64_t k = 0; k < s->n_samples && !called; k++) called += row_ok(s->gl + k * s->g, s->g);
+    if (!called) {
+        for (int a = 0; a < s->a; a++) f_out[a] = NAN;
+        return;
+    }
+    tune_t tu = make_tune(iterations);
+    tu.qp_max_iter = (uint64_t)s->a + 1;
+    double x0[9] = {0}, x[9], f;
+    for (int a = 0; a < s->a; a++) x0[a] = 1.0 / s->a;
+    solve_sqp_n(s->a, af_objective, af_grad_hess, s, x0, &tu, x, &f);
+    for (int a = 0; a < s->a; a++)
+        if (x[a] > 0.0 && x[a] < maf) x[a] = 0.0;
+    sum_to_one_n(s->a, x, f_out);
+}
+
+int kor_gl_allele_frequencies(const double *gl, int64_t n_sites, int64_t n_samples, int n_alleles,
+                              uint64_t iterations, double maf, int threads, double *af_out) {
+    if (!gl || !af_out || n_sites < 0 || n_samples <= 0 || n_alleles < 2 || n_alleles > 4 || iterations == 0)
+        return KOR_EINVAL;
+    const int g = n_alleles * (n_alleles + 1) / 2;
+#ifdef _OPENMP
+    if (threads <= 0) threads = omp_get_max_threads();
+#pragma omp parallel for schedule(dynamic, 16) num_threads(threads)
+#endif
+    for (int64_t v = 0; v < n_sites; v++) {
+        af_site_t s = {gl + v * n_samples * g, n_samples, n_alleles, g};
+        af_fit(&s, iterations, maf, af_out + 4 * v);
+    }
+    return KOR_OK;
+}
+
+/* A site after its zero-frequency alleles are dropped (src/wrapper.rs:349-409):
+ * the kept alleles (in order), their frequencies, for each kept genotype its
+ * index in the original VCF order, and m[gx][gy] over the kept genotypes. */
+typedef struct {
+    const double *gl;  /* the original n_samples x g0 likelihoods */
+    int g0, a, g;
+    int gidx[10];
+    double *m;         /* g x g x 9 */
+} red_site_t;
+
+int kor_gl_relatedness(const double *gl2, int64_t n2, const double *gl3, int64_t n3, const double *gl4,
+                       int64_t n4, int64_t n_samples, double maf, int64_t num_samples, uint64_t iterations,
+                       int threads, kor_output *out, int64_t out_cap, int64_t *n_out, double *af_out) {
+    if (n_samples <= 0 || n2 < 0 || n3 < 0 || n4 < 0 || (n2 && !gl2) || (n3 && !gl3) || (n4 && !gl4) || !out ||
+        !n_out || iterations == 0)
+        return KOR_EINVAL;
+    if (num_samples < 0) num_samples = n_samples;
+    if (num_samples == 0 || num_samples > n_samples) return KOR_EINVAL;
+    const int64_t npairs = num_samples * (num_samples + 1) / 2;
+    if (out_cap < npairs) return KOR_EINVAL;
+    if (!(maf >= 0.0)) maf = 1.0 / (2.0 * (double)n_samples);   /* src/wrapper.rs:99-101 */
+    const int64_t nv = n2 + n3 + n4;
+    const double *gls[3] = {gl2, gl3, gl4};
+    const int64_t ns[3] = {n2, n3, n4};
+    double *af = (double *)malloc(sizeof(double) * 4 * (size_t)(nv + 1));
+    red_site_t *lists[3];
+    int64_t counts[3] = {0, 0, 0};
+    for (int k = 0; k < 3; k++) lists[k] = (red_site_t *)calloc((size_t)(nv + 1), sizeof(red_site_t));
+    if (!af || !lists[0] || !lists[1] || !lists[2]) {
+        free(af); free(lists[0]); free(lists[1]); free(lists[2]);
+        return KOR_ENOMEM;
+    }
+    /* frequencies of every site, bi-, tri- then tetra-allelic */
+    int64_t off = 0;
+    for (int k = 0; k < 3; k++) {
+        kor_gl_allele_frequencies(gls[k], ns[k], n_samples, k + 2, iterations, maf, threads, af + 4 * off);
+        off += ns[k];
+    }
+    if (af_out) memcpy(af_out, af, sizeof(double) * 4 * (size_t)nv);
+    /* drop zero-frequency alleles, in the reference's order: each group's sites
+     * go to the list of their remaining allele count */
+    off = 0;
+    for (int k = 0; k < 3; k++) {
+        const int a0 = k + 2, g0 = a0 * (a0 + 1) / 2;
+        for (int64_t v = 0; v < ns[k]; v++) {
+            const double *f = af + 4 * (off + v);
+            int keep[4], na = 0;
+            double fk[4] = {0, 0, 0, 0};
+            for (int a = 0; a < a0; a++)
+                if (f[a] > 0.0) { keep[na] = a; fk[na] = f[a]; na++; }
+            if (na < 2) continue;
+            red_site_t *r = &lists[na - 2][counts[na - 2]++];
+            r->gl = gls[k] + v * n_samples * g0;
+            r->g0 = g0;
+            r->a = na;
+            r->g = na * (na + 1) / 2;
+            int t = 0;
+            for (int j = 0; j < na; j++)
+                for (int i = 0; i <= j; i++) r->gidx[t++] = keep[j] * (keep[j] + 1) / 2 + keep[i];
+            r->m = (double *)malloc(sizeof(double) * 9 * (size_t)(r->g * r->g));
+            if (r->m)
+                for (int gx = 0; gx < r->g; gx++)
+                    for (int gy = 0; gy < r->g; gy++) kor_iis_row(gx, gy, fk, r->m + 9 * (gx * r->g + gy));
+        }
+        off += ns[k];
+    }
+    const int64_t nk = counts[0] + counts[1] + counts[2];
+    int st = nk == 0 ? KOR_ENOSITES : KOR_OK;
+    for (int k = 0; k < 3 && st == KOR_OK; k++)
+        for (int64_t v = 0; v < counts[k]; v++)
+            if (!lists[k][v].m) st = KOR_ENOMEM;
+    if (st == KOR_OK) {
+        tune_t tu = make_tune(iterations);
+#ifdef _OPENMP
+        if (threads <= 0) threads = omp_get_max_threads();
+#pragma omp parallel num_threads(threads)
+#endif
+        {
+            rowbuf_t rb;
+            rb.blocks = (v8d *)aligned_alloc(64, sizeof(v8d) * 9 * (size_t)(nk / 8 + 1));
+            pass_count_t pc = {0, 0};
+            if (rb.blocks) {
+#ifdef _OPENMP
+#pragma omp for schedule(dynamic, 1)
+#endif
+                for (int64_t x = 0; x < num_samples; x++) {
+                    const int64_t row0 = x * num_samples - x * (x - 1) / 2;
+                    for (int64_t y = x; y < num_samples; y++) {
+                        rb_reset(&rb);
+                        /* the pair's rows: sum over genotype pairs of GLx GLy m
+                         * (src/mixture.rs:9-62), bi-, tri- then tetra-allelic */
+                        for (int k = 0; k < 3; k++)
+                            for (int64_t v = 0; v < counts[k]; v++) {
+                                const red_site_t *r = &lists[k][v];
+                                const double *lx = r->gl + x * r->g0, *ly = r->gl + y * r->g0;
+                                double row[9] = {0};
+                                for (int gx = 0; gx < r->g; gx++) {
+                                    const double ax = lx[r->gidx[gx]];
+                                    for (int gy = 0; gy < r->g; gy++) {
+                                        const double gg = ax * ly[r->gidx[gy]];
+                                        const double *mm = r->m + 9 * (gx * r->g + gy);
+                                        for (int s = 0; s < 9; s++) row[s] = fma(gg, mm[s], row[s]);
+                                    }
+                                }
+                                if (row_ok(row, 9)) rb_push(&rb, row);
+                            }
+                        rb_finish(&rb);
+                        kor_output *o = out + row0 + (y - x);
+                        o->x = (uint64_t)x;
+                        o->y = (uint64_t)y;
+                        if (rb_len(&rb) == 0) {
+                            memset(o->jacquard, 0, sizeof o->jacquard);
+                            o->obj = NAN; o->iters = 0; o->cond = NAN;
+                            continue;
+                        }
+                        double x0[9] = {0};
+                        if (x == y) { x0[0] = 0.5; x0[6] = 0.5; }
+                        else for (int i = 0; i < 9; i++) x0[i] = 1.0 / 9.0;
+                        solve_sqp(&rb, x0, &tu, o, &pc);
+                    }
+                }
+                free(rb.blocks);
+            }
+        }
+        *n_out = npairs;
+    }
+    for (int k = 0; k < 3; k++) {
+        for (int64_t v = 0; v < counts[k]; v++) free(lists[k][v].m);
+        free(lists[k]);
+    }
+    free(af);
+    return st;
+}

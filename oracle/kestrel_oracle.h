@@ -103,6 +103,22 @@ int kor_cls_relatedness_ma(const uint8_t *codes, int64_t n_samples, int64_t n_si
                            const uint8_t *malleles, const double *maf_in, int64_t num_samples,
                            uint64_t iterations, int threads, kor_output *out, int64_t out_cap,
                            int64_t *n_out);
+/* The GL/PL estimator on soft genotype likelihoods (src/wrapper.rs:89-330):
+ * gl2 / gl3 / gl4 hold n2 / n3 / n4 sites of 2 / 3 / 4 alleles, each
+ * n_samples x G linear-scale likelihoods (G = 3, 6, 10, genotypes in the VCF
+ * order; a row with a NaN is a missing sample).  Allele frequencies come from
+ * the per-site HWE SQP with the maf cut (maf < 0 or NaN: 1 / (2 n_samples)),
+ * alleles of zero frequency are dropped (a site left with one allele goes), and
+ * each pair's rows are sum over genotype pairs of GLx GLy m[gx][gy].  Rows as
+ * kor_relatedness.  af_out (optional, 4 per site in input order) gets the
+ * fitted frequencies. */
+int kor_gl_relatedness(const double *gl2, int64_t n2, const double *gl3, int64_t n3, const double *gl4,
+                       int64_t n4, int64_t n_samples, double maf, int64_t num_samples, uint64_t iterations,
+                       int threads, kor_output *out, int64_t out_cap, int64_t *n_out, double *af_out);
+/* The per-site allele-frequency fit alone (src/allele/mod.rs:91-134): gl is
+ * n_sites x n_samples x G; af_out n_sites x 4. */
+int kor_gl_allele_frequencies(const double *gl, int64_t n_sites, int64_t n_samples, int n_alleles,
+                              uint64_t iterations, double maf, int threads, double *af_out);
 /* m[gx][gy] of a site with allele frequencies freq (genotype indices in the VCF
  * order): the nine conditional probabilities of the joint genotypes. */
 void kor_iis_row(int gx, int gy, const double *freq, double row[9]);

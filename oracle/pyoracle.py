@@ -55,9 +55,13 @@ def lib():
         L.kor_cls_relatedness_ma.argtypes = [P, i64, i64, i64, P, P, i64, i64, P, P, i64, u64,
                                              ctypes.c_int, P, i64, ctypes.POINTER(i64)]
         L.kor_iis_row.argtypes = [ctypes.c_int, ctypes.c_int, P, P]
+        L.kor_gl_relatedness.argtypes = [P, i64, P, i64, P, i64, i64, dbl, i64, u64, ctypes.c_int, P, i64,
+                                         ctypes.POINTER(i64), P]
+        L.kor_gl_allele_frequencies.argtypes = [P, i64, i64, ctypes.c_int, u64, dbl, ctypes.c_int, P]
         L.kor_iis_row.restype = None
         for f in ("kor_site_frequencies", "kor_relatedness", "kor_relatedness_pairs",
-                  "kor_eval_pair", "kor_allele_counts", "kor_cls_relatedness", "kor_cls_relatedness_ma"):
+                  "kor_eval_pair", "kor_allele_counts", "kor_cls_relatedness", "kor_cls_relatedness_ma",
+                  "kor_gl_relatedness", "kor_gl_allele_frequencies"):
             getattr(L, f).restype = ctypes.c_int
         L.kor_pass_counts.restype = None
         _lib = L
@@ -196,3 +200,44 @@ def eval_pair(codes_x, codes_y, p, q, keep, delta):
     if st:
         raise RuntimeError(f"kor_eval_pair failed: {st}")
     return f.value, g, h.reshape(9, 9), n.value
+
+
+def gl_relatedness(gl2, gl3=None, gl4=None, maf=None, num_samples=None, iterations=100, threads=0):
+    """The GL/PL estimator on soft likelihoods: gl2 [sites, samples, 3], gl3
+    [sites, samples, 6], gl4 [sites, samples, 10], linear scale, NaN = missing.
+    Returns (rows, allele frequencies [sites, 4] in input order)."""
+    arrs = []
+    n = None
+    for a, g in ((gl2, 3), (gl3, 6), (gl4, 10)):
+        if a is None:
+            arrs.append(None)
+            continue
+        a = np.ascontiguousarray(a, dtype=np.float64)
+        assert a.ndim == 3 and a.shape[2] == g
+        n = a.shape[1] if n is None else n
+        assert a.shape[1] == n
+        arrs.append(a)
+    counts = [0 if a is None else a.shape[0] for a in arrs]
+    ns = n if num_samples is None else num_samples
+    out = np.zeros(ns * (ns + 1) // 2, OUTPUT_DTYPE)
+    af = np.zeros((sum(counts), 4))
+    nout = ctypes.c_int64()
+    st = lib().kor_gl_relatedness(_ptr(arrs[0]), counts[0], _ptr(arrs[1]), counts[1], _ptr(arrs[2]), counts[2], n,
+                                  float("nan") if maf is None else float(maf), ns, iterations, threads, _ptr(out),
+                                  out.size, ctypes.byref(nout), _ptr(af))
+    if st:
+        raise RuntimeError(f"kor_gl_relatedness failed: {st}")
+    return out, af
+
+
+def gl_allele_frequencies(gl, maf=0.0, iterations=100, threads=0):
+    """Per-site allele frequencies from likelihoods [sites, samples, G]."""
+    gl = np.ascontiguousarray(gl, dtype=np.float64)
+    g = gl.shape[2]
+    a = {3: 2, 6: 3, 10: 4}[g]
+    af = np.zeros((gl.shape[0], 4))
+    st = lib().kor_gl_allele_frequencies(_ptr(gl), gl.shape[0], gl.shape[1], a, iterations, float(maf), threads,
+                                         _ptr(af))
+    if st:
+        raise RuntimeError(f"kor_gl_allele_frequencies failed: {st}")
+    return af
