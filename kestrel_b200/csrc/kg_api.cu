@@ -509,7 +509,7 @@ int kg_relatedness(kg_ctx* c, int64_t num_samples, uint64_t iterations, double m
         st = kg::prepare_cohort(c->cohort, c->cohort.raw.as<uint8_t>(), c->cohort.n_samples,
                                 c->cohort.n_sites, c->cohort.n_sites, true,
                                 c->af_set ? c->af.data() : nullptr, std::isnan(maf) ? -1.0 : maf,
-                                c->stream, err);
+                                c->stream, err, false, iterations);
         if (st) {
             cudaEventDestroy(ev0);
             cudaEventDestroy(ev1);
@@ -643,7 +643,8 @@ int kg_relatedness_batch(kg_ctx* c, kg_cohort* cohorts, int n_cohorts, uint64_t 
             auto co = std::make_unique<kg::Cohort>();
             std::string e1;
             int s1 = kg::prepare_cohort(*co, k.codes, k.n_samples, k.n_sites, k.row_stride, false,
-                                        k.allele_frequencies, std::isnan(maf) ? -1.0 : maf, c->stream, e1);
+                                        k.allele_frequencies, std::isnan(maf) ? -1.0 : maf, c->stream, e1, false,
+                                        iterations);
             k.status = s1;
             if (s1) {
                 if (err.empty()) err = e1;

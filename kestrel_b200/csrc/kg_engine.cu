@@ -7,6 +7,7 @@
 //   non-segregating site drop            src/wrapper.rs:352-410
 //   per-pair driver, start points        src/coefficients.rs:77-136
 #include "kg_engine.h"
+#include "kg_allele.cuh"
 
 #include <algorithm>
 #include <cmath>
@@ -63,7 +64,7 @@ int DevBuf::reserve(size_t n) {
 }
 
 size_t Cohort::device_bytes() const {
-    return raw.bytes + af.bytes + rc.bytes + oc.bytes + keep.bytes + kidx.bytes + bsum.bytes +
+    return raw.bytes + af.bytes + rc.bytes + oc.bytes + hc.bytes + keep.bytes + kidx.bytes + bsum.bytes +
            nkept.bytes + pfull.bytes + qfull.bytes + p32.bytes + p64.bytes + q64.bytes +
            site_of.bytes + planes.bytes + cls_q.bytes + cls_part.bytes + mg.bytes + malleles.bytes + maf.bytes +
            mfreq.bytes + mkeep.bytes + mcount.bytes + mpart.bytes + cmulti.bytes + mgT.bytes;
@@ -75,29 +76,33 @@ const char* engine_version() { return "kestrel-b200 0.1.0 (sm_100a)"; }
 
 constexpr int SCAN_BLOCK = 1024;
 
-// Per raw site: REF allele count and observed samples over all rows; flags any
-// code above 3.  Four sites per thread.
+// Per raw site: REF allele count, observed samples and heterozygous calls over
+// all rows; flags any code above 3.  A thread per site (adjacent threads read
+// adjacent bytes of a row).
 __global__ void count_kernel(const uint8_t* __restrict__ codes, int64_t n_samples, int64_t n_sites,
                              int64_t stride, int32_t* __restrict__ rc, int32_t* __restrict__ oc,
-                             int32_t* __restrict__ flags) {
+                             int32_t* __restrict__ hc, int32_t* __restrict__ flags) {
     int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (v >= n_sites) return;
-    int r = 0, o = 0;
+    int r = 0, o = 0, h = 0;
     bool bad = false;
     for (int64_t s = 0; s < n_samples; s++) {
         unsigned c = codes[s * stride + v];
         bad |= (c > 3u);
-        if (c < 3u) { r += 2 - (int)c; o += 1; }
+        if (c < 3u) { r += 2 - (int)c; o += 1; h += c == 1u; }
     }
     rc[v] = r;
     oc[v] = o;
+    hc[v] = h;
     if (bad) atomicOr(&flags[1], 1);
 }
 
-// Frequencies as the ML path sees them and the segregating flag.
+// Frequencies as the ML path sees them and the segregating flag: the
+// caller's, or the allele-frequency fit of the reference's GL path on the
+// site's genotype-class counts (kg_allele.cuh), capped at `iterations`.
 __global__ void freq_kernel(const int32_t* __restrict__ rc, const int32_t* __restrict__ oc,
-                            const double* __restrict__ af, int64_t n_sites, double maf,
-                            double* __restrict__ pf, double* __restrict__ qf,
+                            const int32_t* __restrict__ hc, const double* __restrict__ af, int64_t n_sites,
+                            double maf, uint64_t iterations, double* __restrict__ pf, double* __restrict__ qf,
                             uint8_t* __restrict__ keep, int cls, int64_t n_samples) {
     int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (v >= n_sites) return;
@@ -127,14 +132,8 @@ __global__ void freq_kernel(const int32_t* __restrict__ rc, const int32_t* __res
             pf[v] = 0.0; qf[v] = 0.0; keep[v] = 0;
             return;
         }
-        double tot = 2.0 * (double)oc[v];
-        x0 = (double)rc[v] / tot;
-        x1 = (double)(2 * oc[v] - rc[v]) / tot;
-        if (x0 > 0.0 && x0 < maf) x0 = 0.0;
-        if (x1 > 0.0 && x1 < maf) x1 = 0.0;
-        double s = x0 + x1;
-        x0 = x0 / s;
-        x1 = x1 / s;
+        const int32_t het = hc[v], hom_ref = (rc[v] - het) / 2;
+        allele2_frequencies((double)hom_ref, (double)het, (double)(oc[v] - hom_ref - het), iterations, maf, x0, x1);
     }
     pf[v] = x0;
     qf[v] = x1;
@@ -491,7 +490,7 @@ static int grid_for(int64_t n, int threads) { return (int)std::max<int64_t>(1, c
 
 int prepare_cohort(Cohort& c, const uint8_t* codes, int64_t n_samples, int64_t n_sites,
                    int64_t row_stride, bool codes_on_device, const double* af, double maf,
-                   cudaStream_t st, std::string& err, bool cls) {
+                   cudaStream_t st, std::string& err, bool cls, uint64_t iterations) {
     if (n_samples <= 0 || n_sites <= 0 || row_stride < n_sites) {
         err = "n_samples and n_sites must be positive and row_stride >= n_sites";
         return KG_EINVAL;
@@ -524,6 +523,7 @@ int prepare_cohort(Cohort& c, const uint8_t* codes, int64_t n_samples, int64_t n
     const uint8_t* draw = codes_on_device ? codes : c.raw.as<uint8_t>();
     KG_CUDA_TRY((cudaError_t)c.rc.reserve(sizeof(int32_t) * n_sites));
     KG_CUDA_TRY((cudaError_t)c.oc.reserve(sizeof(int32_t) * n_sites));
+    KG_CUDA_TRY((cudaError_t)c.hc.reserve(sizeof(int32_t) * n_sites));
     KG_CUDA_TRY((cudaError_t)c.keep.reserve((size_t)n_sites));
     KG_CUDA_TRY((cudaError_t)c.kidx.reserve(sizeof(int32_t) * n_sites));
     KG_CUDA_TRY((cudaError_t)c.bsum.reserve(sizeof(int32_t) * nb));
@@ -546,9 +546,10 @@ int prepare_cohort(Cohort& c, const uint8_t* codes, int64_t n_samples, int64_t n
     KG_CUDA_TRY(cudaMemsetAsync(c.nkept.p, 0, sizeof(int32_t) * 4, st));
     count_kernel<<<grid_for(n_sites, 256), 256, 0, st>>>(draw, n_samples, n_sites, stride,
                                                           c.rc.as<int32_t>(), c.oc.as<int32_t>(),
-                                                          c.nkept.as<int32_t>());
-    freq_kernel<<<grid_for(n_sites, 256), 256, 0, st>>>(c.rc.as<int32_t>(), c.oc.as<int32_t>(), daf,
-                                                         n_sites, maf, c.pfull.as<double>(),
+                                                          c.hc.as<int32_t>(), c.nkept.as<int32_t>());
+    freq_kernel<<<grid_for(n_sites, 256), 256, 0, st>>>(c.rc.as<int32_t>(), c.oc.as<int32_t>(),
+                                                         c.hc.as<int32_t>(), daf, n_sites, maf, iterations,
+                                                         c.pfull.as<double>(),
                                                          c.qfull.as<double>(), c.keep.as<uint8_t>(),
                                                          cls ? 1 : 0, n_samples);
     scan_block_kernel<<<(int)nb, SCAN_BLOCK, 0, st>>>(c.keep.as<uint8_t>(), n_sites,

@@ -66,7 +66,7 @@ struct Cohort {
     DevBuf raw;                // uint8 codes, n_samples x n_sites
     DevBuf packed2, packedm;   // the last packed upload (2-bit codes, observed mask)
     DevBuf af;                 // caller frequencies, n_sites x 2 (optional)
-    DevBuf rc, oc;             // int32 REF allele count, observed samples
+    DevBuf rc, oc, hc;         // int32 REF allele count, observed samples, heterozygous calls
     DevBuf keep;               // uint8
     DevBuf kidx;               // int32 exclusive prefix of keep
     DevBuf bsum;               // int32 block sums of the scan
@@ -95,12 +95,13 @@ struct Cohort {
 };
 
 // Enqueues the preparation of a cohort on `st`.  codes are host memory unless
-// codes_on_device; af may be NULL.  maf < 0 selects 1/(2 n_samples).  With cls
+// codes_on_device; af may be NULL.  maf < 0 selects 1/(2 n_samples);
+// iterations caps the allele-frequency fit (the estimator's own cap).  With cls
 // the sites are those every sample calls, frequencies are counts over all
 // samples (or af), nothing is filtered by frequency, and Q is computed.
 int prepare_cohort(Cohort& c, const uint8_t* codes, int64_t n_samples, int64_t n_sites,
                    int64_t row_stride, bool codes_on_device, const double* af, double maf,
-                   cudaStream_t st, std::string& err, bool cls = false);
+                   cudaStream_t st, std::string& err, bool cls = false, uint64_t iterations = 100);
 
 // After prepare_cohort(..., cls = true): adds the cohort's tri- and
 // tetra-allelic sites (c.mg, c.malleles, c.maf uploaded, c.n_multi set) to the

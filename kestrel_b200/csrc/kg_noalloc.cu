@@ -26,9 +26,9 @@
 
 namespace kg {
 // Kernels defined in kg_engine.cu.
-__global__ void count_kernel(const uint8_t*, int64_t, int64_t, int64_t, int32_t*, int32_t*, int32_t*);
-__global__ void freq_kernel(const int32_t*, const int32_t*, const double*, int64_t, double, double*,
-                            double*, uint8_t*, int, int64_t);
+__global__ void count_kernel(const uint8_t*, int64_t, int64_t, int64_t, int32_t*, int32_t*, int32_t*, int32_t*);
+__global__ void freq_kernel(const int32_t*, const int32_t*, const int32_t*, const double*, int64_t, double, uint64_t,
+                            double*, double*, uint8_t*, int, int64_t);
 __global__ void scan_block_kernel(const uint8_t*, int64_t, int32_t*, int32_t*);
 __global__ void scan_sums_kernel(int32_t*, int64_t, int32_t*);
 __global__ void compact_kernel(const uint8_t*, const int32_t*, const int32_t*, const double*,
@@ -133,6 +133,7 @@ extern "C" int kg_relatedness_noalloc(const uint8_t* d_codes, int64_t n_samples,
     Carve cv{base};
     int32_t* rc = cv.take<int32_t>(n_sites);
     int32_t* oc = cv.take<int32_t>(n_sites);
+    int32_t* hc = cv.take<int32_t>(n_sites);
     uint8_t* keep = cv.take<uint8_t>(n_sites);
     int32_t* kidx = cv.take<int32_t>(n_sites);
     int32_t* bsum = cv.take<int32_t>(nb);
@@ -158,8 +159,9 @@ extern "C" int kg_relatedness_noalloc(const uint8_t* d_codes, int64_t n_samples,
     if (e == cudaSuccess) e = cudaMemsetAsync(counters, 0, sizeof(kg::RunCounters), s);
     if (e != cudaSuccess) return KG_ECUDA;
     const int g256 = (int)((n_sites + 255) / 256);
-    kg::count_kernel<<<g256, 256, 0, s>>>(d_codes, n_samples, n_sites, row_stride, rc, oc, nkept);
-    kg::freq_kernel<<<g256, 256, 0, s>>>(rc, oc, nullptr, n_sites, maf, pfull, qfull, keep, 0, n_samples);
+    kg::count_kernel<<<g256, 256, 0, s>>>(d_codes, n_samples, n_sites, row_stride, rc, oc, hc, nkept);
+    kg::freq_kernel<<<g256, 256, 0, s>>>(rc, oc, hc, nullptr, n_sites, maf, iterations, pfull, qfull, keep, 0,
+                                         n_samples);
     kg::scan_block_kernel<<<(int)nb, 1024, 0, s>>>(keep, n_sites, kidx, bsum);
     kg::scan_sums_kernel<<<1, 1024, 0, s>>>(bsum, nb, nkept);
     kg::compact_kernel<<<g256, 256, 0, s>>>(keep, kidx, bsum, pfull, qfull, n_sites, site_of, p32, p64, q64);

@@ -732,89 +732,7 @@ __device__ inline void finish_slot(const WaveArgs& A, SlotState& S, int s, const
 // src/cholesky.rs:6-65 for one or two free variables).  One thread.
 __device__ __forceinline__ int cls_self_qp(double q00, double q01, double q10, double q11, double c0, double c1,
                                            const Tune& tq, double& y0, double& y1) {
-    const double eps = 2.220446049250313e-16;
-    y0 = 0.5;
-    y1 = 0.5;
-    bool w0 = y0 == 0.0, w1 = y1 == 0.0;
-    int it = 0;
-    while (it < tq.qp_max_iter) {
-        const double sy = (0.0 + y0) + y1;
-        y0 = y0 / sy;
-        y1 = y1 / sy;
-        const int nf = (w0 ? 0 : 1) + (w1 ? 0 : 1);
-        if (nf == 0) return it;
-        double lambda, p0 = 0.0, p1 = 0.0, m;
-        bool m_nan;
-        if (nf == 2) {
-            const double g0 = c0 + fma(q01, y1, fma(q00, y0, 0.0));
-            const double g1 = c1 + fma(q11, y1, fma(q10, y0, 0.0));
-            const double gamma = fmax(fmax(0.0, fabs(q00)), fabs(q11));
-            const double xi = fmax(0.0, fabs(q01));
-            const double delta = eps * fmax(1.0, gamma + xi);
-            const double beta2 = fmax(fmax(gamma, xi / sqrt(3.0)), eps);
-            const double theta = fmax(0.0, fabs(q10));
-            const double d0 = fmax(fmax(fabs(q00), theta * theta / beta2), delta);
-            const double l10 = q10 / d0;
-            const double pv0 = d0 * l10;
-            const double d1 = fmax(fmax(fabs(q11 - fma(pv0, l10, 0.0)), 0.0 / beta2), delta);
-            double b0 = g0, b1 = g1 - fma(b0, l10, 0.0);
-            b0 = b0 / d0;
-            b1 = b1 / d1;
-            b0 = b0 - fma(b1, l10, 0.0);
-            double o0 = 1.0, o1 = 1.0 - fma(o0, l10, 0.0);
-            o0 = o0 / d0;
-            o1 = o1 / d1;
-            o0 = o0 - fma(o1, l10, 0.0);
-            lambda = ((0.0 + b0) + b1) / ((0.0 + o0) + o1);
-            const double f0 = lambda * o0 - b0, f1 = lambda * o1 - b1;
-            m_nan = isnan(f0) || isnan(f1);
-            m = fmax(fabs(f0), fabs(f1));
-            p0 = f0;
-            p1 = f1;
-        } else {
-            // one free variable k: the 1 x 1 factor
-            const bool k0 = !w0;
-            const double a = k0 ? q00 : q11, ck = k0 ? c0 : c1, yk = k0 ? y0 : y1;
-            const double g = ck + fma(a, yk, 0.0);
-            const double gamma = fmax(0.0, fabs(a));
-            const double delta = eps * fmax(1.0, gamma + 0.0);
-            const double d0 = fmax(fmax(fabs(a), 0.0), delta);
-            const double b = g / d0, o = 1.0 / d0;
-            lambda = (0.0 + b) / (0.0 + o);
-            const double f = lambda * o - b, f_pad = lambda * 0.0 - 0.0;
-            m_nan = isnan(f) || isnan(f_pad);
-            m = fmax(fabs(f), fabs(f_pad));
-            if (k0) p0 = f;
-            else p1 = f;
-        }
-        if (!m_nan && m <= tq.qp_zero_search_tol) {
-            if (nf == 2) return it;
-            const double gq0 = c0 + fma(q01, y1, fma(q00, y0, 0.0));
-            const double gq1 = c1 + fma(q11, y1, fma(q10, y0, 0.0));
-            const int best = w0 ? ((w1 && gq1 < gq0) ? 1 : 0) : 1;
-            const double gb = best == 0 ? gq0 : gq1;
-            if (gb - lambda >= -tq.qp_conv_tol) return it;
-            if (best == 0) w0 = false;
-            else w1 = false;
-        } else {
-            double alpha = 1.0;
-            int block = -1;
-            if (p0 < 0.0) {
-                const double a = -y0 / p0;
-                if (a < alpha) { alpha = a; block = 0; }
-            }
-            if (p1 < 0.0) {
-                const double a = -y1 / p1;
-                if (a < alpha) { alpha = a; block = 1; }
-            }
-            y0 = fmax(y0 + alpha * p0, 0.0);
-            y1 = fmax(y1 + alpha * p1, 0.0);
-            if (block == 0) { w0 = true; y0 = 0.0; }
-            if (block == 1) { w1 = true; y1 = 0.0; }
-        }
-        it++;
-    }
-    return it;
+    return qp_simplex2(q00, q01, q10, q11, c0, c1, 0.5, 0.5, tq, y0, y1);
 }
 
 // The CLS estimator's step after its one moment pass (src/coefficients.rs:

@@ -22,9 +22,8 @@
  *    src/log/scalar.rs:18-58 (both within about 1 ulp);
  *  - one-hot rows are exact (zeros stay zero), whereas the reference's PL=255
  *    encoding leaves ~1e-26 residues (changes f, g, H by < 1e-18 relative);
- *  - allele frequencies use the count form count/(2 n_obs) (the closed-form ML
- *    optimum for hard calls, as src/wrapper.rs:412-428 computes for GT), not the
- *    per-site HWE SQP of src/allele/mod.rs:78-134.
+ *  - the per-site HWE SQP of the allele frequencies (src/allele/mod.rs:78-134)
+ *    sums its terms per genotype class (count x term) rather than per sample.
  */
 #include "kestrel_oracle.h"
 
@@ -572,10 +571,22 @@ int kor_allele_counts(const uint8_t *codes, int64_t n_samples, int64_t n_sites,
     return KOR_OK;
 }
 
+/* A biallelic site's frequencies from its hard calls: the reference's GL path
+ * on one-hot likelihoods, i.e. the per-site HWE SQP of src/allele/mod.rs:91-134
+ * (defined with the soft-likelihood code below) on the three genotype classes
+ * weighted by their counts, then the maf cut. */
+static void hard_call_frequencies(const int64_t cnt[3], uint64_t iterations, double maf, double f[4]);
+
 int kor_site_frequencies(const uint8_t *codes, int64_t n_samples, int64_t n_sites,
                          int64_t stride, const double *af_in, double maf,
                          double *p, double *q, uint8_t *keep, int64_t *n_kept) {
-    if (n_samples <= 0 || n_sites <= 0) return KOR_EINVAL;
+    return kor_site_frequencies_it(codes, n_samples, n_sites, stride, af_in, maf, 100, p, q, keep, n_kept);
+}
+
+int kor_site_frequencies_it(const uint8_t *codes, int64_t n_samples, int64_t n_sites,
+                            int64_t stride, const double *af_in, double maf, uint64_t iterations,
+                            double *p, double *q, uint8_t *keep, int64_t *n_kept) {
+    if (n_samples <= 0 || n_sites <= 0 || iterations == 0) return KOR_EINVAL;
     int64_t kept = 0;
     if (af_in) {
         for (int64_t s = 0; s < n_sites; s++) {
@@ -587,30 +598,23 @@ int kor_site_frequencies(const uint8_t *codes, int64_t n_samples, int64_t n_site
         *n_kept = kept;
         return KOR_OK;
     }
-    int32_t *rc = (int32_t *)malloc(sizeof(int32_t) * n_sites);
-    int32_t *oc = (int32_t *)malloc(sizeof(int32_t) * n_sites);
-    if (!rc || !oc) { free(rc); free(oc); return KOR_ENOMEM; }
-    int st = kor_allele_counts(codes, n_samples, n_sites, stride, rc, oc);
-    if (st != KOR_OK) { free(rc); free(oc); return st; }
     if (maf < 0.0) maf = 1.0 / (2.0 * (double)n_samples);
     for (int64_t s = 0; s < n_sites; s++) {
+        int64_t cnt[3] = {0, 0, 0};
+        for (int64_t i = 0; i < n_samples; i++) {
+            const uint8_t c = codes[i * stride + s];
+            if (c > 3) return KOR_EINVAL;
+            if (c < 3) cnt[c]++;
+        }
         p[s] = 0.0; q[s] = 0.0; keep[s] = 0;
-        if (oc[s] == 0) continue; /* no observed call: nothing to estimate */
-        double tot = 2.0 * (double)oc[s];
-        double x0 = (double)rc[s] / tot;
-        double x1 = (double)(2 * oc[s] - rc[s]) / tot;
-        if (x0 > 0.0 && x0 < maf) x0 = 0.0;
-        if (x1 > 0.0 && x1 < maf) x1 = 0.0;
-        double sm = x0 + x1;
-        x0 = x0 / sm;
-        x1 = x1 / sm;
-        p[s] = x0;
-        q[s] = x1;
-        keep[s] = (x0 > 0.0 && x1 > 0.0);
+        if (cnt[0] + cnt[1] + cnt[2] == 0) continue; /* no observed call: nothing to estimate */
+        double f[4];
+        hard_call_frequencies(cnt, iterations, maf, f);
+        p[s] = f[0];
+        q[s] = f[1];
+        keep[s] = (f[0] > 0.0 && f[1] > 0.0);
         kept += keep[s];
     }
-    free(rc);
-    free(oc);
     *n_kept = kept;
     return KOR_OK;
 }
@@ -715,7 +719,7 @@ int kor_relatedness(const uint8_t *codes, int64_t n_samples, int64_t n_sites,
     int st = KOR_ENOMEM;
     if (p && q && keep && px && py) {
         int64_t kept;
-        st = kor_site_frequencies(codes, n_samples, n_sites, stride, af_in, maf, p, q, keep, &kept);
+        st = kor_site_frequencies_it(codes, n_samples, n_sites, stride, af_in, maf, iterations, p, q, keep, &kept);
         if (st == KOR_OK && kept == 0) st = KOR_ENOSITES;
         if (st == KOR_OK) {
             int64_t k = 0;
@@ -1036,6 +1040,7 @@ typedef struct {
     const double *gl;  /* n_samples x g */
     int64_t n_samples;
     int a, g;
+    const double *w;   /* NULL, or a weight per row (rows standing for that many samples) */
 } af_site_t;
 
 static int row_ok(const double *r, int g) {
@@ -1060,8 +1065,9 @@ static double af_objective(const void *ctx, const double *x, double eps) {
                 const double w = a == b ? x[a] * x[a] : 2.0 * x[a] * x[b];
                 p = fma(w, r[b * (b + 1) / 2 + a], p);
             }
-        acc += log(p);
-        n++;
+        const double wk = s->w ? s->w[k] : 1.0;
+        acc = fma(wk, log(p), acc);
+        n += (int64_t)wk;
     }
     return -acc / (double)n;
 }
@@ -1087,11 +1093,12 @@ static void af_grad_hess(const void *ctx, const double *x, double eps, double g[
         }
         for (int a = 0; a < A; a++) d = fma(x[a], lx[a], d);
         const double inv = 1.0 / d;
+        const double wk = s->w ? s->w[k] : 1.0;
         for (int a = 0; a < A; a++) {
-            zg[a] = fma(lx[a], inv, zg[a]);
-            for (int b = 0; b < A; b++) zh[a][b] += 2.0 * (lx[a] * inv) * (lx[b] * inv) - L[a][b] * inv;
+            zg[a] = fma(wk, lx[a] * inv, zg[a]);
+            for (int b = 0; b < A; b++) zh[a][b] = fma(wk, 2.0 * (lx[a] * inv) * (lx[b] * inv) - L[a][b] * inv, zh[a][b]);
         }
-        n++;
+        n += (int64_t)wk;
     }
     for (int i = 0; i < 9; i++) {
         g[i] = 0.0;
@@ -1179,6 +1186,19 @@ static void af_fit(const af_site_t *s, uint64_t iterations, double maf, double f
     sum_to_one_n(s->a, x, f_out);
 }
 
+static void hard_call_frequencies(const int64_t cnt[3], uint64_t iterations, double maf, double f[4]) {
+    static const double one_hot[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+    double rows[9], w[3];
+    int n = 0;
+    for (int c = 0; c < 3; c++)
+        if (cnt[c] > 0) {
+            memcpy(rows + 3 * n, one_hot + 3 * c, sizeof(double) * 3);
+            w[n++] = (double)cnt[c];
+        }
+    af_site_t s = {rows, n, 2, 3, w};
+    af_fit(&s, iterations, maf, f);
+}
+
 int kor_gl_allele_frequencies(const double *gl, int64_t n_sites, int64_t n_samples, int n_alleles,
                               uint64_t iterations, double maf, int threads, double *af_out) {
     if (!gl || !af_out || n_sites < 0 || n_samples <= 0 || n_alleles < 2 || n_alleles > 4 || iterations == 0)
@@ -1189,7 +1209,7 @@ int kor_gl_allele_frequencies(const double *gl, int64_t n_sites, int64_t n_sampl
 #pragma omp parallel for schedule(dynamic, 16) num_threads(threads)
 #endif
     for (int64_t v = 0; v < n_sites; v++) {
-        af_site_t s = {gl + v * n_samples * g, n_samples, n_alleles, g};
+        af_site_t s = {gl + v * n_samples * g, n_samples, n_alleles, g, NULL};
         af_fit(&s, iterations, maf, af_out + 4 * v);
     }
     return KOR_OK;

@@ -49,15 +49,22 @@ enum {
 int kor_allele_counts(const uint8_t *codes, int64_t n_samples, int64_t n_sites,
                       int64_t stride, int32_t *ref_count, int32_t *obs_count);
 
-/* Allele frequencies as the ML path would see them: count form, maf zeroing
+/* Allele frequencies as the ML path sees them: the reference's GL path on
+ * one-hot likelihoods, i.e. the per-site HWE SQP of src/allele/mod.rs:91-134
+ * (on the three genotype classes weighted by their counts), maf zeroing
  * (src/allele/mod.rs:120-126), renormalisation, and the non-segregating drop
- * (src/wrapper.rs:366-383).  af_in (n_sites x 2, [ref, alt]) overrides the
- * estimate when non-NULL (then only the zero drop applies).  maf < 0 selects the
- * default 1/(2 n_samples) (src/wrapper.rs:101).  Writes p (ref) and q (alt) and
- * keep[s] = 1 for segregating sites; returns the number kept in *n_kept. */
+ * (src/wrapper.rs:366-383).  The SQP's optimum sits about 5e-9 below the count
+ * frequency (the eps inside its log), so a count frequency equal to maf is cut.
+ * af_in (n_sites x 2, [ref, alt]) overrides the estimate when non-NULL (then
+ * only the zero drop applies).  maf < 0 selects the default 1/(2 n_samples). */
 int kor_site_frequencies(const uint8_t *codes, int64_t n_samples, int64_t n_sites,
                          int64_t stride, const double *af_in, double maf,
                          double *p, double *q, uint8_t *keep, int64_t *n_kept);
+/* The same with the allele-frequency SQP's iteration cap (the estimator's
+ * `iterations`, src/wrapper.rs:103-131); kor_site_frequencies uses 100. */
+int kor_site_frequencies_it(const uint8_t *codes, int64_t n_samples, int64_t n_sites,
+                            int64_t stride, const double *af_in, double maf, uint64_t iterations,
+                            double *p, double *q, uint8_t *keep, int64_t *n_kept);
 
 /* Full all-pairs run for pairs (x, y), 0 <= x <= y < num_samples, in the
  * reference's row order.  num_samples < 0 means all.  threads <= 0 means all

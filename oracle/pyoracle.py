@@ -44,6 +44,7 @@ def lib():
         i64, u64, dbl = ctypes.c_int64, ctypes.c_uint64, ctypes.c_double
         P = ctypes.c_void_p
         L.kor_site_frequencies.argtypes = [P, i64, i64, i64, P, dbl, P, P, P, ctypes.POINTER(i64)]
+        L.kor_site_frequencies_it.argtypes = [P, i64, i64, i64, P, dbl, u64, P, P, P, ctypes.POINTER(i64)]
         L.kor_relatedness.argtypes = [P, i64, i64, i64, P, i64, u64, dbl, ctypes.c_int, P, i64,
                                       ctypes.POINTER(i64)]
         L.kor_relatedness_pairs.argtypes = [P, i64, i64, P, P, P, P, P, i64, u64, ctypes.c_int, P]
@@ -59,7 +60,7 @@ def lib():
                                          ctypes.POINTER(i64), P]
         L.kor_gl_allele_frequencies.argtypes = [P, i64, i64, ctypes.c_int, u64, dbl, ctypes.c_int, P]
         L.kor_iis_row.restype = None
-        for f in ("kor_site_frequencies", "kor_relatedness", "kor_relatedness_pairs",
+        for f in ("kor_site_frequencies", "kor_site_frequencies_it", "kor_relatedness", "kor_relatedness_pairs",
                   "kor_eval_pair", "kor_allele_counts", "kor_cls_relatedness", "kor_cls_relatedness_ma",
                   "kor_gl_relatedness", "kor_gl_allele_frequencies"):
             getattr(L, f).restype = ctypes.c_int
@@ -89,7 +90,7 @@ def allele_counts(codes):
     return rc, oc
 
 
-def site_frequencies(codes, af=None, maf=None):
+def site_frequencies(codes, af=None, maf=None, iterations=100):
     codes = _codes(codes)
     n, m = codes.shape
     p = np.zeros(m)
@@ -97,9 +98,9 @@ def site_frequencies(codes, af=None, maf=None):
     keep = np.zeros(m, np.uint8)
     kept = ctypes.c_int64()
     afa = None if af is None else np.ascontiguousarray(af, dtype=np.float64)
-    st = lib().kor_site_frequencies(_ptr(codes), n, m, m, _ptr(afa),
-                                    -1.0 if maf is None else float(maf),
-                                    _ptr(p), _ptr(q), _ptr(keep), ctypes.byref(kept))
+    st = lib().kor_site_frequencies_it(_ptr(codes), n, m, m, _ptr(afa),
+                                       -1.0 if maf is None else float(maf), iterations,
+                                       _ptr(p), _ptr(q), _ptr(keep), ctypes.byref(kept))
     if st:
         raise RuntimeError(f"kor_site_frequencies failed: {st}")
     return p, q, keep.astype(bool)

@@ -15,14 +15,23 @@ def test_allele_counts_match_numpy(oracle, cfg0):
     assert np.array_equal(rc, np.where(obs, 2 - c.astype(int), 0).sum(0))
 
 
-def test_site_frequencies_count_form(oracle, cfg0):
-    p, q, keep = oracle.site_frequencies(cfg0.codes)
+def test_site_frequencies_are_the_allele_sqp(oracle, cfg0):
+    # the reference's GL path fits each site's frequencies by an SQP
+    # (src/allele/mod.rs); on hard calls its optimum is the count frequency
+    # moved by the eps inside the log (about 5e-9), and it equals the fit on
+    # one-hot likelihoods
+    p, q, keep = oracle.site_frequencies(cfg0.codes, maf=0.0)
     rc, oc = oracle.allele_counts(cfg0.codes)
     x0 = rc / (2.0 * oc)
-    x1 = (2 * oc - rc) / (2.0 * oc)
-    s = x0 + x1
-    assert np.array_equal(p, x0 / s) and np.array_equal(q, x1 / s)
-    assert np.array_equal(keep, (x0 > 0) & (x1 > 0))
+    assert np.abs(p - x0)[keep].max() < 1e-6      # the SQP stops at KKT tolerance 1e-8
+    assert np.array_equal(keep, (x0 > 0) & (x0 < 1))
+    codes = cfg0.codes
+    gl = np.zeros(codes.T.shape + (3,))
+    for g in range(3):
+        gl[..., g] = codes.T == g
+    gl[codes.T == 3] = np.nan
+    af = oracle.gl_allele_frequencies(gl, maf=0.0)
+    assert np.abs(af[:, 0] - p)[keep].max() < 1e-8     # per class vs per sample sums: the same fit
 
 
 def test_maf_zeroing_drops_rare_sites(oracle):
@@ -32,7 +41,12 @@ def test_maf_zeroing_drops_rare_sites(oracle):
     codes[:, 3] = 2           # monomorphic ALT
     p, q, keep = oracle.site_frequencies(codes, maf=0.1)
     assert list(keep) == [False, False, True, False]
-    p, q, keep = oracle.site_frequencies(codes)      # default maf 1/(2N)
+    # default maf 1/(2N) = 0.05: the fitted q of the singleton lands about
+    # 5e-9 below its count frequency 0.05, so the cut takes it, as the
+    # reference's GL path does
+    p, q, keep = oracle.site_frequencies(codes)
+    assert list(keep) == [False, False, True, False]
+    p, q, keep = oracle.site_frequencies(codes, maf=0.04)
     assert list(keep) == [False, True, True, False]
 
 
