@@ -142,6 +142,18 @@ int kg_relatedness(kg_ctx *ctx, int64_t num_samples, uint64_t iterations,
 int kg_relatedness_gt(kg_ctx *ctx, int64_t num_samples, uint64_t iterations,
                       kg_output *out, int64_t out_cap, int64_t *n_out);
 
+/* The reference's GL/PL estimator on soft genotype likelihoods (src/wrapper.rs:
+ * 89-330), biallelic sites: gl is n_samples x n_sites x 3 doubles, sample-major,
+ * the linear-scale likelihoods of 0/0, 0/1, 1/1 (the VCF reader's 10^(GL - max)
+ * or 10^(-PL/10)); a sample with a NaN at a site is missing there.  Allele
+ * frequencies come from the per-site HWE SQP on the likelihoods (capped at
+ * `iterations`), with the maf cut (maf < 0 or NaN: 1/(2 n_samples)); each
+ * pair's rows are sum over genotype pairs of GLx GLy m(gx, gy), and the SQP is
+ * that of kg_relatedness.  The first form runs in FP64 with a warp per pair. */
+int kg_load_likelihoods(kg_ctx *ctx, const double *gl, int64_t n_samples, int64_t n_sites);
+int kg_relatedness_gl(kg_ctx *ctx, int64_t num_samples, uint64_t iterations, double maf,
+                      kg_output *out, int64_t out_cap, int64_t *n_out);
+
 /* One-shot form of the reference's
  * calculate_relatedness_coefficients_gl(genotype_likelihoods,
  * allele_frequencies, threads, iterations, minimum_allele_frequency,

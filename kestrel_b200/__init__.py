@@ -179,6 +179,28 @@ class Estimator:
             self._af = af
         return self
 
+    def load_likelihoods(self, likelihoods: np.ndarray):
+        """Soft genotype likelihoods for relatedness_gl: double [samples, sites,
+        3] (0/0, 0/1, 1/1), linear scale, NaN = missing."""
+        gl = np.ascontiguousarray(likelihoods, dtype=np.float64)
+        if gl.ndim != 3 or gl.shape[2] != 3:
+            raise ValueError("likelihoods must be (samples, sites, 3)")
+        _check(self._L.kg_load_likelihoods(self._h, ptr(gl), gl.shape[0], gl.shape[1]), self._h)
+        self.n_gl_samples = gl.shape[0]
+        return self
+
+    def relatedness_gl(self, num_samples=None, iterations: int = 100, maf=None,
+                       out: np.ndarray | None = None) -> np.ndarray:
+        """The GL/PL estimator on the loaded soft likelihoods (kg_relatedness_gl)."""
+        ns = self.n_gl_samples if num_samples is None else int(num_samples)
+        np_ = ns * (ns + 1) // 2
+        if out is None:
+            out = np.empty(np_, OUTPUT_DTYPE)
+        nout = ctypes.c_int64()
+        _check(self._L.kg_relatedness_gl(self._h, ns, iterations, float("nan") if maf is None else float(maf),
+                                         ptr(out), out.size, ctypes.byref(nout)), self._h)
+        return out
+
     def load_multiallelic(self, genotype_indices: np.ndarray, n_alleles, allele_frequencies=None):
         """Tri- and tetra-allelic sites for relatedness_gt: genotype indices u8
         [samples, sites] in the VCF order (j (j + 1) / 2 + i, 255 = missing),
@@ -410,9 +432,13 @@ def _check_vcf(st, L, h):
 
 def relatedness_coefficients_gl(genotype_likelihoods, allele_frequencies=None, threads=None,
                                 iterations=100, minimum_allele_frequency=None):
-    """The GL/PL entry point (src/lib.rs:72-109) for biallelic one-hot
-    likelihoods [variants, samples, 3] (NaN = missing).  Each call is the most
-    likely genotype; non-one-hot rows are reduced the same way with a warning."""
+    """The GL/PL entry point (src/lib.rs:72-109) for biallelic likelihoods
+    [variants, samples, 3] (linear scale, NaN = missing).  One-hot rows (to
+    25.5 log10 units) go through the hard-call estimator (kg_relatedness); any
+    other row sends the
+    cohort through the soft-likelihood estimator (kg_relatedness_gl), which
+    estimates the allele frequencies itself (the reference's GL path does not
+    take given frequencies, src/wrapper.rs:118-126)."""
     del threads
     gl = np.asarray(genotype_likelihoods, dtype=np.float64)
     if gl.ndim != 3 or gl.shape[2] != 3:
@@ -420,11 +446,18 @@ def relatedness_coefficients_gl(genotype_likelihoods, allele_frequencies=None, t
     miss = np.isnan(gl).any(axis=2)
     g = np.where(miss[..., None], 0.0, gl)
     best = np.argmax(g, axis=2)
+    # one-hot to 25.5 log10 units (the reference's PL = 255 encoding leaves
+    # 10^-25.5 residues, which move f, g and H by < 1e-18 relative)
     top = np.take_along_axis(g, best[..., None], axis=2)[..., 0]
     rest = np.sort(g, axis=2)[..., 1]
-    soft = (~miss) & (rest > top * 10 ** -25.5)
+    soft = ~miss & (rest > top * 10 ** -25.5)
     if soft.any():
-        warnings.warn(f"{int(soft.sum())} likelihood rows are not one-hot; using the most likely genotype")
+        if allele_frequencies is not None:
+            raise ValueError("allele_frequencies cannot be given with soft likelihoods")
+        with Estimator() as est:
+            est.load_likelihoods(np.ascontiguousarray(gl.transpose(1, 0, 2)))
+            rows = est.relatedness_gl(iterations=iterations, maf=minimum_allele_frequency)
+        return build_arrays(rows, gl.shape[1])
     codes = best.astype(np.uint8)
     codes[miss] = MISSING
     codes = np.ascontiguousarray(codes.T)

@@ -53,6 +53,8 @@ struct kg_ctx {
     std::vector<double> af;
     bool af_set = false;
     bool multi_af = false;                // kg_load_multiallelic gave frequencies
+    kg::DevBuf soft_gl;                   // kg_load_likelihoods: double [sample][site][3]
+    int64_t soft_ns = 0, soft_nv = 0;
     kg::Workspace ws;
     kg::DevBuf dout;
     kg_run_stats last{};
@@ -598,6 +600,66 @@ int kg_relatedness_gt(kg_ctx* c, int64_t num_samples, uint64_t iterations, kg_ou
         stats.total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
         c->last = stats;
         if (n_out) *n_out = np;
+        if (st) return set_err(c, st, err.empty() ? t_last_err : err);
+        return KG_OK;
+    });
+}
+
+int kg_load_likelihoods(kg_ctx* c, const double* gl, int64_t n_samples, int64_t n_sites) {
+    if (!c) return KG_EINVAL;
+    if (!gl || n_samples <= 0 || n_sites <= 0 || n_sites > (int64_t)INT32_MAX)
+        return set_err(c, KG_EINVAL, "gl must be non-NULL with n_samples, n_sites > 0");
+    return guarded(c, [&]() -> int {
+        int st = use_device(c);
+        if (st) return st;
+        const size_t bytes = sizeof(double) * 3 * (size_t)n_samples * (size_t)n_sites;
+        if (!budget_ok(c, bytes)) return set_err(c, KG_ENOMEM, "likelihoods exceed the memory budget");
+        if (c->soft_gl.reserve(bytes) != cudaSuccess) return set_err(c, KG_ENOMEM, "cannot allocate device likelihoods");
+        cudaError_t e = cudaMemcpyAsync(c->soft_gl.p, gl, bytes, cudaMemcpyHostToDevice, c->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+        if (e != cudaSuccess) return set_err(c, KG_ECUDA, std::string("upload: ") + cudaGetErrorString(e));
+        c->soft_ns = n_samples;
+        c->soft_nv = n_sites;
+        return KG_OK;
+    });
+}
+
+int kg_relatedness_gl(kg_ctx* c, int64_t num_samples, uint64_t iterations, double maf, kg_output* out,
+                      int64_t out_cap, int64_t* n_out) {
+    if (!c) return KG_EINVAL;
+    if (!c->soft_ns) return set_err(c, KG_EINVAL, "no likelihoods loaded");
+    if (iterations == 0) return set_err(c, KG_EINVAL, "iterations must be non-zero");
+    const int64_t ns = num_samples < 0 ? c->soft_ns : num_samples;
+    if (ns > c->soft_ns || ns == 0)
+        return set_err(c, KG_EINVAL, "Requested samples " + std::to_string(ns) + " exceeds total samples " +
+                                         std::to_string(c->soft_ns));
+    const int64_t np = ns * (ns + 1) / 2;
+    if (!out || out_cap < np) return set_err(c, KG_EINVAL, "output capacity must be at least num_samples*(num_samples+1)/2");
+    return guarded(c, [&]() -> int {
+        auto t0 = std::chrono::steady_clock::now();
+        int st = use_device(c);
+        if (st) return st;
+        if (c->dout.reserve(sizeof(kg_output) * np) != cudaSuccess)
+            return set_err(c, KG_ENOMEM, "cannot allocate device output rows");
+        std::string err;
+        cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+        cudaEventCreate(&ev0);
+        cudaEventCreate(&ev1);
+        cudaEventRecord(ev0, c->stream);
+        st = kg::soft_relatedness(c->soft_gl, c->soft_ns, c->soft_nv, ns, iterations, std::isnan(maf) ? -1.0 : maf,
+                                  c->dout.as<kg_output>(), c->stream, err);
+        cudaEventRecord(ev1, c->stream);
+        int st2 = copy_rows_out(c, c->dout, np, out, c->stream);
+        kg_run_stats stats{};
+        float dms = 0.f;
+        if (cudaEventElapsedTime(&dms, ev0, ev1) == cudaSuccess) stats.device_ms = dms;
+        cudaEventDestroy(ev0);
+        cudaEventDestroy(ev1);
+        stats.launches = 2;   // frequencies, pairs
+        stats.total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        c->last = stats;
+        if (n_out) *n_out = np;
+        if (!st && st2) st = st2;
         if (st) return set_err(c, st, err.empty() ? t_last_err : err);
         return KG_OK;
     });

@@ -110,6 +110,13 @@ int prepare_cohort(Cohort& c, const uint8_t* codes, int64_t n_samples, int64_t n
 // summed rows (c.cmulti).  Sets c.n_multi_kept.
 int prepare_multi(Cohort& c, bool have_af, int64_t num_samples, cudaStream_t st, std::string& err);
 
+// The GL/PL estimator on soft likelihoods of biallelic sites (kg_soft.cu): gl
+// is double [n_samples][n_sites][3] on the device (linear scale, NaN =
+// missing); rows of the first ns samples into d_out (device), the reference's
+// order.  maf < 0: 1 / (2 n_samples).
+int soft_relatedness(const DevBuf& gl, int64_t n_samples, int64_t n_sites, int64_t ns, uint64_t iterations,
+                     double maf, kg_output* d_out, cudaStream_t st, std::string& err);
+
 // Unpacks the VCF reader's 2-bit codes + observed mask into device byte codes
 // (d2, dm: the packed rows' device copies, kept for the next load).
 int unpack_2bit(DevBuf& raw, DevBuf& d2, DevBuf& dm, const uint32_t* codes2, const uint32_t* observed,

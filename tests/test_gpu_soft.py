@@ -1,0 +1,69 @@
+"""GPU parity of the GL/PL estimator on soft genotype likelihoods
+(kg_relatedness_gl, src/wrapper.rs:89-330) against the oracle's restatement
+(kor_gl_relatedness), with the same bar as the hard-call path."""
+import numpy as np
+import pytest
+
+import kestrel_b200 as kb
+from kestrel_b200 import synth
+
+from .parity import compare
+from .test_oracle_gl import one_hot, soft_gl
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def cohort():
+    return synth.make_cohort(40, 3000, 71, missing=0.02,
+                             planted={"parent_offspring": 3, "full_sib": 3}, name="soft")
+
+
+@pytest.fixture(scope="module")
+def est():
+    e = kb.Estimator()
+    yield e
+    e.close()
+
+
+def test_soft_likelihoods_parity(est, oracle, cohort):
+    gl = soft_gl(cohort.codes, np.random.default_rng(3), err=0.1)     # [sites, samples, 3]
+    ref, _ = oracle.gl_relatedness(gl)
+    est.load_likelihoods(np.ascontiguousarray(gl.transpose(1, 0, 2)))
+    gpu = est.relatedness_gl()
+    stats = compare(gpu, ref)
+    same = float(np.mean(gpu["iters"] == ref["iters"]))
+    print(stats, "same iterations", same)
+    assert same > 0.95
+
+
+def test_soft_subset_cap_and_maf(est, oracle, cohort):
+    gl = soft_gl(cohort.codes, np.random.default_rng(4), err=0.05)
+    ref, _ = oracle.gl_relatedness(gl, num_samples=25, iterations=5, maf=0.05)
+    est.load_likelihoods(np.ascontiguousarray(gl.transpose(1, 0, 2)))
+    gpu = est.relatedness_gl(num_samples=25, iterations=5, maf=0.05)
+    assert gpu["iters"].max() <= 5
+    assert np.mean(gpu["iters"] == ref["iters"]) > 0.95
+    ok = ref["iters"] < 5
+    d = np.abs(gpu["jacquard"] - ref["jacquard"]).max(1)
+    lc = np.log10(ref["cond"])
+    assert d[ok & np.isfinite(lc) & (lc <= 4)].max() <= 1e-5
+
+
+def test_one_hot_likelihoods_match_the_hard_call_path(est, oracle, cohort):
+    # maf off the 1/(2N) tie (see the oracle tests)
+    gl = one_hot(cohort.codes)
+    est.load_likelihoods(np.ascontiguousarray(gl.transpose(1, 0, 2)))
+    soft = est.relatedness_gl(maf=0.01)
+    hard = oracle.relatedness(cohort.codes, maf=0.01)
+    compare(soft, hard)
+
+
+def test_python_gl_api_routes_soft_input(oracle, cohort):
+    gl = soft_gl(cohort.codes, np.random.default_rng(5), err=0.1)
+    jac, kin, inb = kb.relatedness_coefficients_gl(gl)
+    ref, _ = oracle.gl_relatedness(gl)
+    x, y = ref["x"].astype(int), ref["y"].astype(int)
+    lc = np.log10(ref["cond"])
+    ident = np.isfinite(lc) & (lc <= 4)
+    assert np.abs(jac[x, y] - ref["jacquard"]).max(1)[ident].max() <= 1e-5
