@@ -50,7 +50,8 @@ def parse():
     ap.add_argument("--multi-sites", type=int, default=0,
                     help="gt-cls: tri- and tetra-allelic sites beside the biallelic ones")
     ap.add_argument("--pass-bps", type=int, default=0, help="site-pass blocks per SM (0 = automatic)")
-    ap.add_argument("--workload", default="allpairs", choices=["allpairs", "batch", "inbred", "serving", "gt-cls"],
+    ap.add_argument("--workload", default="allpairs",
+                    choices=["allpairs", "batch", "inbred", "serving", "gt-cls", "gl-soft"],
                     help="allpairs: N x M all pairs (the headline); batch: 8 uneven cohorts in one "
                          "launch; inbred: N=512 x M=50k inbred stress; serving: panel + Poisson "
                          "query stream (p50/p99 latency)")
@@ -313,6 +314,69 @@ def run_serving(args, local):
             "launches": sv["launches"]}
 
 
+def run_gl_soft(args, local):
+    """The GL/PL estimator on soft genotype likelihoods (kg_relatedness_gl): all
+    pairs of --samples x --sites, likelihoods with mass off the call (each
+    other genotype uniform in [0, 0.05) of the called one's), 2% missing."""
+    import torch
+    import kestrel_b200 as kb
+    from kestrel_b200 import synth
+    from oracle import pyoracle
+    n_s, m_s = args.samples, args.sites
+    co = synth.make_cohort(n_s, m_s, 9, missing=0.02, planted={"parent_offspring": 4, "full_sib": 4},
+                           name="gl-soft")
+    rng = np.random.default_rng(10)
+    c = co.codes                                          # [samples, sites]
+    gl = rng.uniform(0.0, 0.05, c.shape + (3,))
+    for g in range(3):
+        gl[..., g] = np.where(c == g, 1.0, gl[..., g])
+    gl[c == synth.MISSING] = np.nan
+    pairs = n_s * (n_s + 1) // 2
+    est = kb.Estimator(device=local)
+    est.load_likelihoods(gl)
+    for _ in range(max(3, args.warmup)):
+        est.relatedness_gl()
+    clocks = ClockSampler(local)
+    torch.cuda.synchronize()
+    clocks.start()
+    dev = []
+    for _ in range(max(1, args.steps)):
+        est.relatedness_gl()
+        dev.append(est.run_stats()["device_ms"])
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    t = float(np.mean(dev))
+    gl_pin = torch.from_numpy(gl).pin_memory().numpy()
+    out_pin = torch.empty(pairs * kb.OUTPUT_DTYPE.itemsize, dtype=torch.uint8,
+                          pin_memory=True).numpy().view(kb.OUTPUT_DTYPE)
+    e2e_ms = []
+    for _ in range(max(1, args.steps)):
+        t0 = time.perf_counter()
+        est.load_likelihoods(gl_pin)
+        est.relatedness_gl(out=out_pin)
+        e2e_ms.append((time.perf_counter() - t0) * 1e3)
+    te = float(np.mean(e2e_ms))
+    est.close()
+    cpu = None
+    if not args.no_cpu:
+        sub = min(n_s, 48)
+        t0 = time.perf_counter()
+        pyoracle.gl_relatedness(np.ascontiguousarray(gl[:sub].transpose(1, 0, 2)))
+        dt = time.perf_counter() - t0
+        cpu = {"value": sub * (sub + 1) / 2 / dt, "unit": "pairs/s", "cores": os.cpu_count(), "kind": "port",
+               "sample": f"all {sub * (sub + 1) // 2} pairs of the first {sub} samples (oracle FP64 GL "
+                         f"restatement, OpenMP over {os.cpu_count()} threads, {dt:.1f} s)"}
+    return {"metric": "all-pairs/s, GL/PL estimator on soft likelihoods", "value": pairs / (t * 1e-3),
+            "unit": "pairs/s", "n_gpus": 1, "steps": args.steps, "warmup": max(3, args.warmup), "ms_per_step": t,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"all pairs of N={n_s} x M={m_s} soft likelihoods (2% missing)", "pairs": pairs},
+            "e2e": {"value": pairs / (te * 1e-3), "unit": "pairs/s", "h2d_bytes_per_step": int(gl.nbytes),
+                    "d2h_bytes_per_step": int(out_pin.nbytes), "ms_per_step": te},
+            "roofline": None, "roofline_note": "first form (warp per pair, FP64, likelihoods read per pass): "
+                                               "not yet analysed against a roofline",
+            "cpu_baseline": cpu, "clocks": clk, "gpu_launches": 2 * max(1, args.steps)}
+
+
 def run_gt_cls(args, local):
     """The reference's default hard-call estimator (-f GT: conditional least
     squares, Brier objective) on all pairs of N=1024 x M=100,000 with every call
@@ -417,7 +481,8 @@ def main():
     if args.workload != "allpairs":
         import torch
         torch.cuda.set_device(local)
-        fn = {"batch": run_batch, "inbred": run_inbred, "serving": run_serving, "gt-cls": run_gt_cls}[args.workload]
+        fn = {"batch": run_batch, "inbred": run_inbred, "serving": run_serving, "gt-cls": run_gt_cls,
+              "gl-soft": run_gl_soft}[args.workload]
         if rank == 0:
             print(json.dumps(fn(args, local)), flush=True)
         return
