@@ -313,6 +313,10 @@ int kg_vcf_info(const kg_vcf *vcf, int64_t *n_samples, int64_t *n_sites, uint64_
  * af: n_sites x 2 [REF, ALT] from INFO/AF (KG_EINVAL if it was not read).
  * Either may be NULL. */
 int kg_vcf_codes(const kg_vcf *vcf, uint8_t *codes, double *af);
+/* GL/PL files with a likelihood row that is not one-hot (counts[3] > 0): the
+ * linear-scale likelihoods, n_samples x n_sites x 3 (sample-major, NaN where
+ * missing), the input of kg_load_likelihoods; KG_ENOTFOUND otherwise. */
+int kg_vcf_likelihoods(const kg_vcf *vcf, double *gl);
 /* The same codes packed as kg_load_genotypes_2bit takes them (2-bit codes and
  * the observed mask, rows of ceil(n_sites/16) and ceil(n_sites/32) words). */
 int kg_vcf_codes_2bit(const kg_vcf *vcf, uint32_t *codes2, uint32_t *observed);

@@ -20,6 +20,7 @@ from ._lib import (KG_ECUDA, KG_EINVAL, KG_ENOMEM, KG_ENOSITES, KG_ENOTFOUND, KG
                    ptr)
 
 __all__ = ["Coefficients", "relatedness_coefficients_gt", "relatedness_coefficients_gl", "read_vcf", "pack_2bit",
+           "read_vcf_likelihoods",
            "run_cli", "Estimator", "genotype_codes", "build_arrays", "KestrelError",
            "OUTPUT_DTYPE", "MISSING", "KINSHIP_VECTOR", "KG_OK", "KG_EINVAL", "KG_ENOMEM", "KG_ECUDA",
            "KG_ETIMEOUT", "KG_ENOSITES", "KG_ENOTREADY", "KG_ENOTFOUND", "KG_PREC_FP32C", "KG_PREC_FP64"]
@@ -420,6 +421,31 @@ def read_vcf(path, field: str = "GT", allele_freqs: str = "estimate", threads: i
         maf = np.empty((nm, 4)) if allele_freqs == "info" else None
         _check_vcf(L.kg_vcf_multiallelic(h, ptr(mg), ptr(mal), ptr(maf)), L, h)
         return codes, af, names, cd, (mg, mal, maf)
+    finally:
+        if h.value:
+            L.kg_vcf_free(h)
+
+
+def read_vcf_likelihoods(path, field: str = "PL", threads: int = 0):
+    """The linear-scale likelihoods of a GL/PL file's biallelic SNP records as
+    the reference's reader makes them (10^(GL - max GL), 10^(-PL/10); NaN where
+    missing), double [samples, sites, 3], the input of
+    Estimator.load_likelihoods; None when every row is one-hot."""
+    L = lib()
+    h = ctypes.c_void_p()
+    st = L.kg_vcf_read(os.fsencode(path), field.encode(), 0, int(threads), ctypes.byref(h))
+    try:
+        if st != KG_OK:
+            msg = L.kg_vcf_error(h) if h.value else b"out of memory"
+            raise KestrelError(st, msg.decode())
+        ns, nv = ctypes.c_int64(), ctypes.c_int64()
+        _check_vcf(L.kg_vcf_info(h, ctypes.byref(ns), ctypes.byref(nv), None), L, h)
+        gl = np.empty((ns.value, nv.value, 3))
+        st = L.kg_vcf_likelihoods(h, ptr(gl))
+        if st == KG_ENOTFOUND:
+            return None
+        _check_vcf(st, L, h)
+        return gl
     finally:
         if h.value:
             L.kg_vcf_free(h)

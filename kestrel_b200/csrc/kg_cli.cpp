@@ -289,9 +289,17 @@ extern "C" int kg_run_cli(int argc, const char* const* argv) {
         log_info("Found %s di-allelic sites", std::to_string(vcf.n_sites));
         log_info("Skipped %s tri- or tetra-allelic sites (biallelic sites only)", std::to_string(vcf.multi));
     }
-    if (vcf.soft)
-        log_info("%s likelihood entries were not one-hot; their most likely genotype was used",
+    // GL/PL likelihoods that are not all one-hot go to the soft-likelihood
+    // estimator, as the reference's GL path fits them (src/wrapper.rs:89-330)
+    const bool soft_path = o.field != 'T' && !vcf.gl.empty();
+    if (soft_path) {
+        log_info("%s likelihood entries are not one-hot: estimating from the soft likelihoods",
                  std::to_string(vcf.soft));
+        if (o.af_info) {
+            std::fprintf(stderr, "Error: allele frequencies from INFO/AF cannot be used with soft likelihoods\n");
+            return 1;
+        }
+    }
     const std::vector<std::string>& samples = vcf.samples;
     const std::vector<double>& af = vcf.af;
     const int64_t ns = (int64_t)samples.size(), nv = vcf.n_sites;
@@ -314,18 +322,23 @@ extern "C" int kg_run_cli(int argc, const char* const* argv) {
     }
     kg_ctx* ctx = dev.ctx;
     int st = 0;
-    // the reader's codes go up packed: 2 bits a call plus the observed mask
-    std::vector<uint32_t> codes2((size_t)(ns * ((nv + 15) / 16))), observed((size_t)(ns * ((nv + 31) / 32)));
-    kg::pack_2bit(vcf, o.threads, codes2.data(), observed.data());
-    st = kg_load_genotypes_2bit(ctx, codes2.data(), observed.data(), ns, nv);
-    if (!st && o.af_info) st = kg_set_allele_frequencies(ctx, af.data());
-    if (!st && o.cls && vcf.n_multi > 0)
-        st = kg_load_multiallelic(ctx, vcf.mcodes.data(), ns, vcf.n_multi, vcf.n_multi, vcf.malleles.data(),
-                                  o.af_info ? vcf.maf.data() : nullptr);
     int64_t nout = 0;
-    if (!st) {
-        if (o.cls) st = kg_relatedness_gt(ctx, nsel, o.iterations, out.data(), np, &nout);
-        else st = kg_relatedness(ctx, nsel, o.iterations, o.maf, out.data(), np, &nout);
+    if (soft_path) {
+        st = kg_load_likelihoods(ctx, vcf.gl.data(), ns, nv);
+        if (!st) st = kg_relatedness_gl(ctx, nsel, o.iterations, o.maf, out.data(), np, &nout);
+    } else {
+        // the reader's codes go up packed: 2 bits a call plus the observed mask
+        std::vector<uint32_t> codes2((size_t)(ns * ((nv + 15) / 16))), observed((size_t)(ns * ((nv + 31) / 32)));
+        kg::pack_2bit(vcf, o.threads, codes2.data(), observed.data());
+        st = kg_load_genotypes_2bit(ctx, codes2.data(), observed.data(), ns, nv);
+        if (!st && o.af_info) st = kg_set_allele_frequencies(ctx, af.data());
+        if (!st && o.cls && vcf.n_multi > 0)
+            st = kg_load_multiallelic(ctx, vcf.mcodes.data(), ns, vcf.n_multi, vcf.n_multi, vcf.malleles.data(),
+                                      o.af_info ? vcf.maf.data() : nullptr);
+        if (!st) {
+            if (o.cls) st = kg_relatedness_gt(ctx, nsel, o.iterations, out.data(), np, &nout);
+            else st = kg_relatedness(ctx, nsel, o.iterations, o.maf, out.data(), np, &nout);
+        }
     }
     if (st) {
         std::fprintf(stderr, "Error: %s\n", kg_last_error(ctx));

@@ -204,7 +204,10 @@ bool load_text(const std::string& path, int threads, Text& text, std::string& er
 bool is_base(std::string_view b) { return b.size() == 1 && std::strchr("ACGTacgt", b[0]) != nullptr; }
 
 // Genotype code of one sample's value of the FORMAT key; false if malformed.
-bool parse_call(std::string_view v, char field, uint8_t& code, uint64_t& soft) {
+// GL/PL: like (when not NULL) gets the call's linear-scale likelihoods as the
+// reference's reader makes them (src/vcf.rs:325-420): 10^(GL - max GL) with GL
+// read at single precision, or 10^(-PL/10); NaN when the call is missing.
+bool parse_call(std::string_view v, char field, uint8_t& code, uint64_t& soft, double* like = nullptr) {
     if (field == 'T') {
         int a[2] = {0, 0};
         int k = 0;
@@ -234,6 +237,7 @@ bool parse_call(std::string_view v, char field, uint8_t& code, uint64_t& soft) {
         code = (uint8_t)(a[0] + a[1]);
         return true;
     }
+    if (like) like[0] = like[1] = like[2] = NAN;
     if (v == ".") {
         code = 3;
         return true;
@@ -261,6 +265,18 @@ bool parse_call(std::string_view v, char field, uint8_t& code, uint64_t& soft) {
     if (any_missing) {
         code = 3;
         return true;
+    }
+    if (like) {
+        if (field == 'P') {
+            for (int i = 0; i < 3; i++) like[i] = std::pow(10.0, -val[i] / 10.0);
+        } else {
+            double g[3], mx = -INFINITY;
+            for (int i = 0; i < 3; i++) {
+                g[i] = (double)(float)val[i];
+                mx = std::max(mx, g[i]);
+            }
+            for (int i = 0; i < 3; i++) like[i] = std::pow(10.0, g[i] - mx);
+        }
     }
     // likelihood scale: PL = -10 log10 L, GL = log10 L
     double ll[3];
@@ -355,6 +371,7 @@ struct Chunk {
     const char* b = nullptr;
     const char* e = nullptr;
     std::vector<uint8_t> rows;   // kept records x samples
+    std::vector<double> lrows;   // GL/PL: kept records x samples x 3 linear-scale likelihoods
     std::vector<double> af;
     uint64_t total = 0, not_snp = 0, multi = 0, soft = 0, incomplete = 0;
     int64_t kept = 0;
@@ -369,7 +386,7 @@ struct Chunk {
     std::string fail_kind;       // message with %R for the global record number
 };
 
-void parse_chunk(Chunk& c, char field, bool af_info, size_t n_samples) {
+void parse_chunk(Chunk& c, char field, bool af_info, size_t n_samples, bool want_like) {
     const std::string_view key = field == 'T' ? "GT" : (field == 'P' ? "PL" : "GL");
     std::string_view last_fmt;
     int last_fi = -1;
@@ -572,7 +589,12 @@ void parse_chunk(Chunk& c, char field, bool af_info, size_t n_samples) {
                 }
             }
             const std::string_view v = sample_value(s);
-            if (!parse_call(v, field, c.rows[base + k], c.soft)) {
+            double* like = nullptr;
+            if (want_like) {
+                if (k == 0) c.lrows.resize((base + n_samples) * 3);
+                like = c.lrows.data() + (base + k) * 3;
+            }
+            if (!parse_call(v, field, c.rows[base + k], c.soft, like)) {
                 fail("Value " + std::string(v) + " is not a valid " + std::string(key));
                 return;
             }
@@ -689,8 +711,28 @@ int read_vcf(const std::string& path, char field, bool af_info, int threads, Vcf
     }
     const size_t ns = out.samples.size();
     parallel_for(threads, n_chunks, [&](int, int64_t cb, int64_t ce) {
-        for (int64_t i = cb; i < ce; i++) parse_chunk(chunks[i], field, af_info, ns);
+        for (int64_t i = cb; i < ce; i++) parse_chunk(chunks[i], field, af_info, ns, false);
     });
+    // a soft GL/PL row: parse again keeping the likelihoods (one-hot files
+    // never hold them)
+    if (field != 'T') {
+        bool any_soft = false, any_failed = false;
+        for (auto& c : chunks) {
+            any_soft |= c.soft > 0;
+            any_failed |= c.failed;
+        }
+        if (any_soft && !any_failed) {
+            for (auto& c : chunks) {
+                Chunk fresh;
+                fresh.b = c.b;
+                fresh.e = c.e;
+                c = std::move(fresh);
+            }
+            parallel_for(threads, n_chunks, [&](int, int64_t cb, int64_t ce) {
+                for (int64_t i = cb; i < ce; i++) parse_chunk(chunks[i], field, af_info, ns, true);
+            });
+        }
+    }
     // counts and the first failure in file order
     uint64_t before = 0;
     for (auto& c : chunks) {
@@ -715,6 +757,21 @@ int read_vcf(const std::string& path, char field, bool af_info, int threads, Vcf
     out.codes.allocate((size_t)(nv * (int64_t)ns));
     transpose_chunks(threads, ns, nv, out.codes.data(), chunks,
                      [](const Chunk& c) { return std::make_pair(c.rows.data(), c.kept); });
+    if (field != 'T' && out.soft > 0) {
+        // sample-major likelihoods [s][v][3], each thread a range of samples
+        out.gl.resize((size_t)(nv * (int64_t)ns * 3));
+        std::vector<int64_t> first((size_t)chunks.size() + 1, 0);
+        for (size_t i = 0; i < chunks.size(); i++) first[i + 1] = first[i] + chunks[i].kept;
+        parallel_for(threads, (int64_t)ns, [&](int, int64_t s0, int64_t s1) {
+            for (size_t i = 0; i < chunks.size(); i++) {
+                const double* lr = chunks[i].lrows.data();
+                for (int64_t s = s0; s < s1; s++)
+                    for (int64_t v = 0; v < chunks[i].kept; v++)
+                        std::memcpy(out.gl.data() + ((size_t)s * nv + first[i] + v) * 3,
+                                    lr + ((size_t)v * ns + s) * 3, sizeof(double) * 3);
+            }
+        });
+    }
     out.n_multi = 0;
     for (auto& c : chunks) out.n_multi += c.mkept;
     out.mcodes.allocate((size_t)(out.n_multi * (int64_t)ns));
@@ -825,6 +882,13 @@ extern "C" int kg_vcf_codes(const kg_vcf* v, uint8_t* codes, double* af) {
         if (v->d.af.empty()) return KG_EINVAL;
         std::memcpy(af, v->d.af.data(), sizeof(double) * v->d.af.size());
     }
+    return KG_OK;
+}
+
+extern "C" int kg_vcf_likelihoods(const kg_vcf* v, double* gl) {
+    if (!v || !gl) return KG_EINVAL;
+    if (v->d.gl.empty()) return KG_ENOTFOUND;
+    std::memcpy(gl, v->d.gl.data(), sizeof(double) * v->d.gl.size());
     return KG_OK;
 }
 

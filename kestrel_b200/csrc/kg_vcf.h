@@ -51,6 +51,9 @@ struct VcfData {
     std::vector<uint8_t> malleles;  // allele count per record (3 or 4)
     std::vector<double> maf;        // with INFO/AF: 4 per record, [REF, ALT1, ALT2, ALT3 or 0]
     uint64_t tri = 0, tetra = 0;
+    // GL/PL with a soft row: the linear-scale likelihoods, sample-major
+    // gl[(s * n_sites + v) * 3 + g] (NaN where missing); empty otherwise
+    std::vector<double> gl;
 };
 
 // The codes in the packed form kg_load_genotypes_2bit takes: per sample

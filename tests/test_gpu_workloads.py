@@ -270,3 +270,27 @@ def test_packed_load_equals_byte_load():
         est.load_packed(c2, ob, co.codes.shape[1])
         ml2, gt2 = est.relatedness(), est.relatedness_gt()
     assert _bitwise_equal(ml, ml2) and _bitwise_equal(gt, gt2)
+
+
+def test_cli_soft_pl_file_uses_the_soft_estimator(oracle):
+    from .test_vcf import py_likelihoods, soft_pl_text
+    co = synth.make_cohort(24, 1500, seed=48, missing=0.02, name="cli-soft")
+    text = soft_pl_text(co.codes, np.random.default_rng(2))
+    gl = py_likelihoods(text, "PL")                      # [samples, sites, 3]
+    ref, _ = oracle.gl_relatedness(np.ascontiguousarray(gl.transpose(1, 0, 2)), num_samples=20)
+    cli = os.path.join(os.path.dirname(kb.__file__), "bin", "kestrel")
+    with tempfile.TemporaryDirectory() as td:
+        vcf = os.path.join(td, "in.vcf")
+        tsv = os.path.join(td, "out.tsv")
+        open(vcf, "w").write(text)
+        r = subprocess.run([cli, vcf, tsv, "-f", "PL", "-s", "20"], capture_output=True, text=True, timeout=300)
+        assert r.returncode == 0, r.stderr
+        _, rows = _read_tsv(tsv)
+    assert "estimating from the soft likelihoods" in r.stderr
+    jac = np.array([[float(v) for v in r[3:12]] for r in rows])
+    obj = np.array([float(r[13]) for r in rows])
+    lc = np.log10(ref["cond"])
+    ident = np.isfinite(lc) & (lc <= 4)
+    assert len(rows) == len(ref)
+    assert np.abs(jac - ref["jacquard"]).max(1)[ident].max() <= 1e-5
+    assert (np.abs(obj - ref["obj"]) / np.abs(ref["obj"])).max() <= 1e-6

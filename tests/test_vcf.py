@@ -309,3 +309,66 @@ def test_packed_codes_decode_to_the_byte_codes():
     dec = (c2[:, s // 16] >> (2 * (s % 16)).astype(np.uint32)) & 3
     obs = (ob[:, s // 32] >> (s % 32).astype(np.uint32)) & 1
     assert np.array_equal(np.where(obs == 1, dec, 3), codes)
+
+
+def soft_pl_text(codes, rng):
+    """A PL VCF whose rows are not one-hot: 0 at the call, 5-40 elsewhere."""
+    n, m = codes.shape
+    lines = ["##fileformat=VCFv4.2", "#CHROM\tPOS\tID\tREF\tALT\tQUAL\tFILTER\tINFO\tFORMAT\t" +
+             "\t".join(f"S{i}" for i in range(n))]
+    for v in range(m):
+        calls = []
+        for s in range(n):
+            c = codes[s, v]
+            if c == 3:
+                calls.append(".,.,.")
+                continue
+            pl = rng.integers(5, 41, 3)
+            pl[c] = 0
+            calls.append(",".join(str(x) for x in pl))
+        lines.append(f"1\t{v + 1}\t.\tA\tC\t.\tPASS\t.\tPL\t" + "\t".join(calls))
+    return "\n".join(lines) + "\n"
+
+
+def py_likelihoods(text, field):
+    samples, rows = None, []
+    for line in text.split("\n"):
+        if line.startswith("#CHROM"):
+            samples = line.split("\t")[9:]
+        if not line or line.startswith("#"):
+            continue
+        cols = line.split("\t")
+        row = []
+        for v in cols[9:9 + len(samples)]:
+            parts = v.split(",")
+            if "." in parts:
+                row.append([np.nan] * 3)
+            elif field == "PL":
+                row.append([10.0 ** (-float(x) / 10.0) for x in parts])
+            else:
+                g = [float(np.float32(float(x))) for x in parts]
+                mx = max(g)
+                row.append([10.0 ** (x - mx) for x in g])
+        rows.append(row)
+    return np.array(rows).transpose(1, 0, 2)
+
+
+def test_soft_likelihoods_are_read_as_the_reference_makes_them():
+    co = synth.make_cohort(19, 900, 64, missing=0.03, name="soft-pl")
+    text = soft_pl_text(co.codes, np.random.default_rng(1))
+    gl_text = text.replace("\tPL\t", "\tGL\t")   # the same numbers read as GL (log10 scale)
+    with tempfile.TemporaryDirectory() as td:
+        p = os.path.join(td, "pl.vcf")
+        open(p, "w").write(text)
+        g = os.path.join(td, "gl.vcf")
+        open(g, "w").write(gl_text)
+        got = kb.read_vcf_likelihoods(p, "PL", threads=3)
+        got_gl = kb.read_vcf_likelihoods(g, "GL", threads=3)
+        hard = os.path.join(td, "hard.vcf")
+        synth.write_vcf(hard, co.codes, field="PL")
+        assert kb.read_vcf_likelihoods(hard, "PL") is None     # one-hot: no likelihoods kept
+    want = py_likelihoods(text, "PL")
+    assert np.array_equal(np.isnan(got), np.isnan(want))
+    assert np.allclose(got, want, rtol=1e-15, atol=0, equal_nan=True)
+    want_gl = py_likelihoods(gl_text, "GL")
+    assert np.allclose(got_gl, want_gl, rtol=1e-15, atol=0, equal_nan=True)
