@@ -142,7 +142,7 @@ __device__ inline int64_t soft_evaluate(const double* __restrict__ gl, int64_t n
 
 // Warp per output row of the first ns samples (x-major, y >= x), taken from a
 // counter; the Jacquard SQP of src/sqp.rs:49-93 in FP64.
-__global__ void __launch_bounds__(SOFT_WARPS * 32) soft_pairs_kernel(
+__global__ void __launch_bounds__(SOFT_WARPS * 32, 4) soft_pairs_kernel(
     const double* __restrict__ gl, int64_t n_sites, const int32_t* __restrict__ kept, const double* __restrict__ kp,
     const double* __restrict__ kq, int64_t nk, int64_t ns, int64_t n_rows, uint64_t iterations, kg_output* out,
     unsigned long long* next, int* no_rows) {
