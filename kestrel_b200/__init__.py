@@ -193,7 +193,7 @@ class Estimator:
     def relatedness_gl(self, num_samples=None, iterations: int = 100, maf=None,
                        out: np.ndarray | None = None) -> np.ndarray:
         """The GL/PL estimator on the loaded soft likelihoods (kg_relatedness_gl)."""
-        ns = self.n_gl_samples if num_samples is None else int(num_samples)
+        ns = getattr(self, "n_gl_samples", 0) if num_samples is None else int(num_samples)
         np_ = ns * (ns + 1) // 2
         if out is None:
             out = np.empty(np_, OUTPUT_DTYPE)

@@ -58,3 +58,10 @@ def test_cli_usage_error_without_gpu(L):
 def test_cli_cls_needs_hard_calls(L):
     argv = (ctypes.c_char_p * 7)(b"kestrel", b"in.vcf", b"out.tsv", b"-f", b"PL", b"-e", b"cls")
     assert L.kg_run_cli(7, argv) == 2
+
+
+def test_soft_likelihood_entry_points_check_their_arguments(L):
+    # argument checks only: no device work (kg_create is not called)
+    assert L.kg_load_likelihoods(None, None, 1, 1) == _lib.KG_EINVAL
+    assert L.kg_relatedness_gl(None, -1, 100, float("nan"), None, 0, None) == _lib.KG_EINVAL
+    assert L.kg_vcf_likelihoods(None, None) == _lib.KG_EINVAL
