@@ -45,6 +45,7 @@ def parse():
     ap.add_argument("--sites", type=int, default=100_000)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-fp64", action="store_true", help="skip the plain FP64 form's measurement")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--slots", type=int, default=0, help="pairs in flight per wave (0 = automatic)")
     ap.add_argument("--multi-sites", type=int, default=0,
@@ -149,9 +150,17 @@ def measured_hbm_peak():
         return 6650.0
 
 
-def cpu_baseline(codes, planted, seconds, threads=0):
+def workload_config(n, m):
+    """The config dict of the all-pairs workload, the same in both arms."""
+    return {"workload": f"all pairs of N={n} x M={m} (planted PO/FS/HS/FC)",
+            "samples": n, "sites": m, "pairs": n * (n - 1) // 2, "self_pairs": n,
+            "l2": "GPU arm: 256 MB buffer written between steps; the CPU arm has no GPU work"}
+
+
+def cpu_baseline(codes, planted, seconds, threads=0, keep_rows=False):
     """The oracle (the reference's ML path restated in C, FP64, all host
-    threads) on a bounded sample of this workload's pairs; pairs/s."""
+    threads) on a bounded sample of this workload's pairs; pairs/s.  With
+    keep_rows, also returns the sampled pairs and the oracle's rows for them."""
     from oracle import pyoracle
     p, q, keep = pyoracle.site_frequencies(codes)
     rng = np.random.default_rng(123)
@@ -168,12 +177,49 @@ def cpu_baseline(codes, planted, seconds, threads=0):
     pyoracle.relatedness_pairs(codes, p, q, keep, sample(k), threads=threads)
     dt = time.perf_counter() - t0
     k2 = int(max(k, min(200_000, k * max(1.0, (seconds - dt) / max(dt, 1e-3)))))
+    pairs = sample(k2)
     t0 = time.perf_counter()
-    pyoracle.relatedness_pairs(codes, p, q, keep, sample(k2), threads=threads)
+    rows = pyoracle.relatedness_pairs(codes, p, q, keep, pairs, threads=threads)
     dt2 = time.perf_counter() - t0
-    return {"value": k2 / dt2, "unit": "pairs/s", "cores": cores, "kind": "port",
-            "sample": f"{k2} random pairs of the {n} x {codes.shape[1]} cohort "
-                      f"(oracle FP64 restatement, OpenMP over {cores} threads, {dt2:.1f} s)"}
+    out = {"value": k2 / dt2, "unit": "pairs/s", "cores": cores, "kind": "port",
+           "sample": f"{k2} random pairs of the {n} x {codes.shape[1]} cohort "
+                     f"(oracle FP64 restatement, OpenMP over {cores} threads, {dt2:.1f} s)"}
+    if keep_rows:
+        return out, pairs, rows, (p, q, keep)
+    return out
+
+
+def error_vs_oracle(gpu_rows, codes, planted, pairs, ref_rows, freqs):
+    """Largest errors of the GPU rows against the FP64 oracle over the
+    sampled pairs of the CPU leg plus every planted pair (run after the timed
+    region): Delta and kinship over pairs whose oracle log10 condition
+    estimate is below 15, the objective (relative) over all of them, and the
+    pairs whose condition flag (log10 cond > 15) differs."""
+    import kestrel_b200 as kb
+    from oracle import pyoracle
+    p, q, keep = freqs
+    pl = np.array([(a, b) for a, b, _, _ in planted], dtype=np.int64).reshape(-1, 2)
+    if len(pl):
+        pairs = np.concatenate([pairs, pl])
+        ref_rows = np.concatenate([ref_rows, pyoracle.relatedness_pairs(codes, p, q, keep, pl)])
+    n = codes.shape[0]
+    x, y = pairs[:, 0].astype(np.int64), pairs[:, 1].astype(np.int64)
+    idx = x * n - x * (x - 1) // 2 + (y - x)          # row of (x, y) in the reference's order
+    g = gpu_rows[idx]
+    assert np.array_equal(g["x"].astype(np.int64), x) and np.array_equal(g["y"].astype(np.int64), y)
+    lc_ref = np.log10(ref_rows["cond"])
+    below = np.isfinite(lc_ref) & (lc_ref < 15)
+    dd = np.abs(g["jacquard"] - ref_rows["jacquard"]).max(1)
+    dk = np.abs(g["jacquard"] @ kb.KINSHIP_VECTOR - ref_rows["jacquard"] @ kb.KINSHIP_VECTOR)
+    do = np.abs(g["obj"] - ref_rows["obj"]) / np.abs(ref_rows["obj"])
+    flag = (np.log10(g["cond"]) > 15) != (lc_ref > 15)
+    return {"pairs": int(len(pairs)), "planted": int(len(pl)), "compared": int(below.sum()),
+            "max_abs_delta_err": float(dd[below].max(initial=0)),
+            "max_abs_kinship_err": float(dk[below].max(initial=0)),
+            "max_rel_objective_err": float(do.max(initial=0)),
+            "cond_flag_disagreements": int(np.sum(flag & below)),
+            "bar": "Delta and kinship <= 1e-5 absolute, objective <= 1e-6 relative, flag equal below 1e15",
+            "oracle": "FP64 C restatement of the reference's ML path"}
 
 
 def run_reference(args, codes, planted):
@@ -194,9 +240,7 @@ def run_reference(args, codes, planted):
             "warmup": args.warmup, "ms_per_step": pairs_per_step / v * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic", "impl": "reference",
-            "config": {"workload": f"all pairs of N={n} x M={codes.shape[1]}", "samples": n,
-                       "sites": int(codes.shape[1]), "pairs": pairs_per_step,
-                       "l2": "inputs larger than L2"},
+            "config": workload_config(n, int(codes.shape[1])),
             "cpu_baseline": dict(cb, value=v),
             "e2e": {"value": v, "unit": "pairs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -579,9 +623,8 @@ def main():
     list_bytes = 8.0 if fp64_form else 4.0
     roof = {"bound": "fp64" if fp64_form else "fp32", "achieved": achieved, "peak": peak,
             "unit": "TFLOP/s", "frac": achieved / peak if peak else None,
-            # DRAM bytes per pair-site-pass from the ncu capture in
-            # profiles/wave_pass_kernel_N96_M100k.md, times the pair-sites of an
-            # average pass launch of this step
+            # DRAM bytes per pair-site-pass from one ncu capture (a 96-sample
+            # cohort), times the pair-sites of an average pass launch of this step
             "traffic": (PASS_DRAM_BYTES_PER_SITE * pass_sites / launches) if not fp64_form else None,
             "traffic_unit": "bytes per launch",
             "algorithmic_bytes": list_bytes * pass_sites / launches,
@@ -603,10 +646,8 @@ def main():
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32" if args.precision == "fp32c" else "f64",
             "data": "synthetic",
-            "config": {"workload": f"all pairs of N={n} x M={m} (planted PO/FS/HS/FC)",
-                       "samples": n, "sites": m, "pairs": pairs, "self_pairs": n,
-                       "precision": args.precision, "parallelism": f"replicas x{world}",
-                       "l2": "256 MB buffer written between steps"},
+            "config": workload_config(n, m),
+            "precision": args.precision, "parallelism": f"replicas x{world}",
             "e2e": e2e, "roofline": roof, "clocks": clk,
             "gpu_launches": int(stats["launches"]) * args.steps,
             "phases_ms": dict(zip(("admit", "pass", "solve", "waves_total"),
@@ -614,8 +655,12 @@ def main():
             "stats": {k: stats[k] for k in ("gh_passes", "fp64_passes", "fp64_pairs", "pair_sites",
                                             "work_units", "shape_sites", "waves", "slots", "nonconverged",
                                             "flops_fp64")}}
+    if rank == 0 and world == 1 and args.precision == "fp32c" and not args.no_fp64:
+        line["fp64_form"] = fp64_form(est, value)
     if rank == 0 and not args.no_cpu and world == 1:
-        line["cpu_baseline"] = cpu_baseline(codes, cohort.planted, args.cpu_seconds)
+        cb, sp, sr, fr = cpu_baseline(codes, cohort.planted, args.cpu_seconds, keep_rows=True)
+        line["cpu_baseline"] = cb
+        line["error_vs_oracle"] = error_vs_oracle(rows, codes, cohort.planted, sp, sr, fr)
     if rank == 0:
         print(json.dumps(line), flush=True)
     est.close()
@@ -623,8 +668,31 @@ def main():
         pg.destroy_process_group()
 
 
-# DRAM bytes (read + write) per pair-site-pass of wave_pass_kernel, measured by
-# ncu (profiles/wave_pass_kernel_N96_M100k.md): 1.911 GB over 447,339,158.
+def fp64_form(est, fp32c_value, steps=2):
+    """The plain FP64 GPU form (every site pass in FP64, IEEE division and the
+    library log) on the same loaded cohort, after the FP32C timing: pairs/s
+    from the device time of `steps` calls after one warm-up, and the FP32C
+    form's speed-up over it."""
+    est.set_precision("fp64")
+    try:
+        est.relatedness()
+        dev = []
+        for _ in range(steps):
+            est.relatedness()
+            dev.append(est.run_stats()["device_ms"])
+    finally:
+        est.set_precision("fp32c")
+    t = float(np.mean(dev))
+    n = est.n_samples
+    v = n * (n - 1) // 2 / (t * 1e-3)
+    return {"value": v, "unit": "pairs/s", "ms_per_step": t, "steps": steps,
+            "ratio_fp32c_over_fp64": fp32c_value / v,
+            "timing": "device time (CUDA events in the library) of kg_relatedness with KG_PREC_FP64"}
+
+
+# DRAM bytes (read + write) per pair-site-pass of wave_pass_kernel: the ncu
+# capture of one launch on a 96-sample x 100,000-site cohort read and wrote
+# 1.911 GB over 447,339,158 pair-site-passes.
 PASS_DRAM_BYTES_PER_SITE = 4.27
 
 

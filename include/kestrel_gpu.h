@@ -87,6 +87,14 @@ int kg_set_precision(kg_ctx *ctx, int precision);
  * autotuner and tests; results do not depend on it. */
 int kg_set_launch(kg_ctx *ctx, int slots, int blocks_per_sm);
 
+/* Upper bound on the waves of one call (0 = automatic: a bound from the work
+ * that only stops a loop that would not end).  A call that reaches it returns
+ * KG_ETIMEOUT with its rows unfinished; the context stays usable and the next
+ * call starts afresh.  No counterpart in the reference (its SQP loop is bounded
+ * per pair by `iterations`, src/sqp.rs:60); exposed so that the bounded device
+ * loop's error path can be exercised without a fault. */
+int kg_set_wave_limit(kg_ctx *ctx, uint64_t waves);
+
 /* Runs the autotuner on a sample of the loaded cohort and keeps the fastest
  * launch shape; writes it to *slots / *blocks_per_sm if non-NULL. */
 int kg_autotune(kg_ctx *ctx, int *slots, int *blocks_per_sm);
@@ -237,15 +245,19 @@ int kg_serving_stats(kg_ctx *ctx, int64_t *requests, int64_t *pairs,
  *   d_codes: device pointer to the genotype codes (sample-major, row_stride
  *            bytes per sample, 0/1/2, 3 = missing);
  *   d_out:   device pointer to out_cap >= n_samples*(n_samples+1)/2 rows;
- *   stream:  a cudaStream_t (NULL = the default stream); the call returns once
- *            the rows are written.
+ *   stream:  a cudaStream_t (NULL = the default stream); the call is
+ *            synchronous: it waits on that stream and returns once the rows
+ *            are written.
  * Limits: n_samples <= 512 and n_sites <= 32768; larger inputs return
  * KG_ENOMEM.  Every intermediate lives in one 48 MiB file-scope __device__
  * array that each GPU loading the library holds until the process exits.  Its
  * device address is looked up on the first call on each device, so make that
- * first call before any stream capture.  All calls share the array: calls that
- * overlap on the GPU (other host threads, other streams) race and must be
- * serialised by the caller. */
+ * first call before any stream capture; the address is kept for the life of
+ * the process, so do not use this entry point across a cudaDeviceReset.  All
+ * calls share the array: calls that overlap on the GPU (other host threads,
+ * other streams) race and must be serialised by the caller.  A CUDA error the
+ * calling thread left pending makes the call return KG_ECUDA at once and is
+ * left pending. */
 int kg_relatedness_noalloc(const uint8_t *d_codes, int64_t n_samples,
                            int64_t n_sites, int64_t row_stride,
                            uint64_t iterations, double maf, kg_output *d_out,

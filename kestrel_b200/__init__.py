@@ -142,6 +142,11 @@ class Estimator:
         """Pairs in flight per wave and site-pass blocks per SM (0 = automatic)."""
         _check(self._L.kg_set_launch(self._h, slots, blocks_per_sm), self._h)
 
+    def set_wave_limit(self, waves: int = 0):
+        """Waves a call may run before it stops with KG_ETIMEOUT (0 = a bound
+        from the work, which only stops a loop that would not end)."""
+        _check(self._L.kg_set_wave_limit(self._h, int(waves)), self._h)
+
     def autotune(self):
         w, b = ctypes.c_int(), ctypes.c_int()
         _check(self._L.kg_autotune(self._h, ctypes.byref(w), ctypes.byref(b)), self._h)

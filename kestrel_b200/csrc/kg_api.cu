@@ -46,6 +46,7 @@ struct kg_ctx {
     int precision = KG_PREC_FP32C;
     int64_t wave_slots = 0;
     int pass_bps = 0;
+    uint64_t wave_limit = 0;
     cudaStream_t stream = nullptr;
     // single cohort
     kg::Cohort cohort;
@@ -126,6 +127,7 @@ kg::RunConfig run_config(const kg_ctx* c, uint64_t iterations) {
     cfg.iterations = iterations;
     cfg.slots = c->wave_slots;
     cfg.pass_blocks_per_sm = c->pass_bps;
+    cfg.max_waves = c->wave_limit;
     return cfg;
 }
 
@@ -391,6 +393,12 @@ int kg_set_launch(kg_ctx* c, int slots, int blocks_per_sm) {
     return KG_OK;
 }
 
+int kg_set_wave_limit(kg_ctx* c, uint64_t waves) {
+    if (!c) return KG_EINVAL;
+    c->wave_limit = waves;
+    return KG_OK;
+}
+
 int kg_load_genotypes(kg_ctx* c, const uint8_t* codes, int64_t n_samples, int64_t n_sites,
                       int64_t row_stride) {
     if (!c) return KG_EINVAL;
@@ -494,7 +502,8 @@ int kg_relatedness(kg_ctx* c, int64_t num_samples, uint64_t iterations, double m
     if (!(std::isnan(maf) || maf < 0.0) && maf > 1.0)
         return set_err(c, KG_EINVAL, "Minimum allele frequency must be within 0 to 1");
     int64_t ns = num_samples < 0 ? c->cohort.n_samples : num_samples;
-    if (ns > c->cohort.n_samples || ns == 0)
+    if (ns == 0) return set_err(c, KG_EINVAL, "num_samples must be positive (or negative for all samples)");
+    if (ns > c->cohort.n_samples)
         return set_err(c, KG_EINVAL, "Requested samples " + std::to_string(ns) + " exceeds total samples " +
                                          std::to_string(c->cohort.n_samples));
     int64_t np = ns * (ns + 1) / 2;
@@ -554,7 +563,8 @@ int kg_relatedness_gt(kg_ctx* c, int64_t num_samples, uint64_t iterations, kg_ou
     if (!c->loaded) return set_err(c, KG_EINVAL, "no genotypes loaded");
     if (iterations == 0) return set_err(c, KG_EINVAL, "iterations must be non-zero");
     int64_t ns = num_samples < 0 ? c->cohort.n_samples : num_samples;
-    if (ns > c->cohort.n_samples || ns == 0)
+    if (ns == 0) return set_err(c, KG_EINVAL, "num_samples must be positive (or negative for all samples)");
+    if (ns > c->cohort.n_samples)
         return set_err(c, KG_EINVAL, "Requested samples " + std::to_string(ns) + " exceeds total samples " +
                                          std::to_string(c->cohort.n_samples));
     int64_t np = ns * (ns + 1) / 2;
@@ -629,8 +639,11 @@ int kg_relatedness_gl(kg_ctx* c, int64_t num_samples, uint64_t iterations, doubl
     if (!c) return KG_EINVAL;
     if (!c->soft_ns) return set_err(c, KG_EINVAL, "no likelihoods loaded");
     if (iterations == 0) return set_err(c, KG_EINVAL, "iterations must be non-zero");
+    if (!(std::isnan(maf) || maf < 0.0) && maf > 1.0)
+        return set_err(c, KG_EINVAL, "Minimum allele frequency must be within 0 to 1");
     const int64_t ns = num_samples < 0 ? c->soft_ns : num_samples;
-    if (ns > c->soft_ns || ns == 0)
+    if (ns == 0) return set_err(c, KG_EINVAL, "num_samples must be positive (or negative for all samples)");
+    if (ns > c->soft_ns)
         return set_err(c, KG_EINVAL, "Requested samples " + std::to_string(ns) + " exceeds total samples " +
                                          std::to_string(c->soft_ns));
     const int64_t np = ns * (ns + 1) / 2;

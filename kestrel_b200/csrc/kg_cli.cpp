@@ -15,6 +15,9 @@
 #include "kg_threads.h"
 #include "kg_vcf.h"
 
+#include <sys/resource.h>
+#include <sys/time.h>
+
 #include <charconv>
 #include <chrono>
 #include <cmath>
@@ -40,11 +43,52 @@ struct Options {
     int threads = 0;   // host threads for VCF reading and output writing (0 = all)
 };
 
+// Log lines in the reference's format (env_logger without timestamp or target,
+// src/cli.rs:68-71): the level padded to five characters in brackets.
 void log_info(const char* fmt, const std::string& a = "") {
-    std::fprintf(stderr, "[INFO] ");
+    std::fprintf(stderr, "[INFO ] ");
     std::fprintf(stderr, fmt, a.c_str());
     std::fprintf(stderr, "\n");
 }
+
+// A duration as Rust's {:.2?} prints it: seconds above one second, else
+// milliseconds, microseconds or nanoseconds, two decimals.
+std::string rust_duration(double seconds) {
+    char b[64];
+    if (seconds >= 1.0) std::snprintf(b, sizeof b, "%.2fs", seconds);
+    else if (seconds >= 1e-3) std::snprintf(b, sizeof b, "%.2fms", seconds * 1e3);
+    else if (seconds >= 1e-6) std::snprintf(b, sizeof b, "%.2f\u00b5s", seconds * 1e6);
+    else std::snprintf(b, sizeof b, "%.2fns", seconds * 1e9);
+    return b;
+}
+
+// The reference's resource checkpoints (src/util.rs:9-37): wall, user and
+// kernel time since the tracker was made, and the peak resident set size, as
+// "Wall Time ..., User Time ..., Kernel Time ..., Peak Memory ..." (the peak in
+// binary units with two decimals).  The estimator calls make one tracker
+// after the VCF is read and check it where the reference's wrappers do
+// (src/wrapper.rs:84, :158, :204).
+struct ResourceTracker {
+    std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
+    struct rusage u0 {};
+    ResourceTracker() { getrusage(RUSAGE_SELF, &u0); }
+    static double tv(const timeval& t) { return (double)t.tv_sec + 1e-6 * (double)t.tv_usec; }
+    void checkpoint() const {
+        struct rusage u {};
+        getrusage(RUSAGE_SELF, &u);
+        const double wall = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        const double kib = (double)u.ru_maxrss;   // Linux: kibibytes
+        const char* unit[] = {"KiB", "MiB", "GiB", "TiB"};
+        double v = kib;
+        int k = 0;
+        while (v >= 1024.0 && k < 3) { v /= 1024.0; k++; }
+        char mem[64];
+        std::snprintf(mem, sizeof mem, "%.2f %s", v, unit[k]);
+        std::fprintf(stderr, "[INFO ] Wall Time %s, User Time %s, Kernel Time %s, Peak Memory %s\n",
+                     rust_duration(wall).c_str(), rust_duration(tv(u.ru_utime) - tv(u0.ru_utime)).c_str(),
+                     rust_duration(tv(u.ru_stime) - tv(u0.ru_stime)).c_str(), mem);
+    }
+};
 
 int usage(const char* why) {
     std::fprintf(stderr,
@@ -262,7 +306,6 @@ struct DeviceInit {
 }  // namespace
 
 extern "C" int kg_run_cli(int argc, const char* const* argv) {
-    auto t0 = std::chrono::steady_clock::now();
     Options o;
     std::string why;
     if (!parse_args(argc, argv, o, why)) return usage(why.c_str());
@@ -323,8 +366,14 @@ extern "C" int kg_run_cli(int argc, const char* const* argv) {
     kg_ctx* ctx = dev.ctx;
     int st = 0;
     int64_t nout = 0;
+    // the estimator's resource tracker starts where the reference's wrapper
+    // call does, with the VCF read; the ML path checks it once the inputs are
+    // on the device (the reference: after its allele frequencies) and again
+    // after the estimate, the CLS path once at the end
+    const ResourceTracker tracker;
     if (soft_path) {
         st = kg_load_likelihoods(ctx, vcf.gl.data(), ns, nv);
+        if (!st) tracker.checkpoint();
         if (!st) st = kg_relatedness_gl(ctx, nsel, o.iterations, o.maf, out.data(), np, &nout);
     } else {
         // the reader's codes go up packed: 2 bits a call plus the observed mask
@@ -335,6 +384,7 @@ extern "C" int kg_run_cli(int argc, const char* const* argv) {
         if (!st && o.cls && vcf.n_multi > 0)
             st = kg_load_multiallelic(ctx, vcf.mcodes.data(), ns, vcf.n_multi, vcf.n_multi, vcf.malleles.data(),
                                       o.af_info ? vcf.maf.data() : nullptr);
+        if (!st && !o.cls) tracker.checkpoint();
         if (!st) {
             if (o.cls) st = kg_relatedness_gt(ctx, nsel, o.iterations, out.data(), np, &nout);
             else st = kg_relatedness(ctx, nsel, o.iterations, o.maf, out.data(), np, &nout);
@@ -344,11 +394,12 @@ extern "C" int kg_run_cli(int argc, const char* const* argv) {
         std::fprintf(stderr, "Error: %s\n", kg_last_error(ctx));
         return 1;
     }
+    tracker.checkpoint();
     dev.release();
     uint64_t nonconv = 0;
     for (auto& r : out) nonconv += (r.iters >= o.iterations);
     if (nonconv)
-        std::fprintf(stderr, "[WARN] No convergence for %llu pairs, max iterations %llu exceeded\n",
+        std::fprintf(stderr, "[WARN ] No convergence for %llu pairs, max iterations %llu exceeded\n",
                      (unsigned long long)nonconv, (unsigned long long)o.iterations);
     FILE* f = std::fopen(o.output.c_str(), "w");
     if (!f) {
@@ -382,9 +433,5 @@ extern "C" int kg_run_cli(int argc, const char* const* argv) {
         return 1;
     }
     std::fclose(f);
-    double wall = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
-    char wb[64];
-    std::snprintf(wb, sizeof wb, "%.2fs", wall);
-    log_info("Wall Time %s", wb);
     return 0;
 }

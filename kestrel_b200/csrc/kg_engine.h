@@ -151,6 +151,7 @@ struct RunConfig {
     uint64_t iterations = 100;
     int64_t slots = 0;         // pairs in flight per wave (0 = pairs / 8 within 4096..32768, as memory allows)
     int pass_blocks_per_sm = 0;   // site-pass kernel blocks per SM (0 = occupancy limit)
+    uint64_t max_waves = 0;       // waves a call may run before it gives up (0 = a bound from the work)
     // Called between waves, on the calling thread, once per job whose pairs
     // have all finished (their rows are final in device memory).
     std::function<void(int job)> job_done;

@@ -3,9 +3,8 @@
 //
 // Some callers cannot call cudaMalloc: code that runs where the allocator is
 // off limits (inside another framework's memory pool or a custom allocator
-// that must not be bypassed, a process whose device memory is fully reserved
-// up front, or a host thread that must not touch the CUDA allocator while
-// other work is captured or in flight).  For them this entry point takes the
+// that must not be bypassed, or a process whose device memory is fully
+// reserved up front).  For them this entry point takes the
 // genotypes and the output rows as device buffers the caller already owns and
 // keeps every intermediate (allele counts, frequencies, bit-plane genotypes,
 // the per-warp shape lists, the work queue and counters) in one file-scope
@@ -14,7 +13,14 @@
 //
 // It launches the same preparation kernels and the same persistent pair
 // kernel as kg_relatedness, on a fixed grid of kWarps warps, so its rows equal
-// those of kg_relatedness on the same input.
+// those of kg_relatedness on the same input.  The call is synchronous: it
+// waits on the caller's stream for the kept-site count and the pair counters
+// before it returns.
+//
+// The array's device address is looked up once per device and kept for the
+// life of the process; after a cudaDeviceReset (or anything else that
+// recreates the device's primary context) that address is stale, so the entry
+// point must not be used across a device reset.
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -118,6 +124,9 @@ extern "C" int kg_relatedness_noalloc(const uint8_t* d_codes, int64_t n_samples,
     if (n_samples > kMaxSamples || n_sites > kMaxSites) return KG_ENOMEM;
     const int64_t np = n_samples * (n_samples + 1) / 2;
     if (out_cap < np) return KG_EINVAL;
+    // an error the caller's thread left pending is the caller's: report it
+    // and leave it in place rather than take it for one of this call's launches
+    if (cudaPeekAtLastError() != cudaSuccess) return KG_ECUDA;
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return KG_ECUDA;
     unsigned char* base = nullptr;

@@ -1524,12 +1524,17 @@ int run_waves(const std::vector<PairJob>& jobs, const RunConfig& cfg, Workspace&
         uint64_t max_iter = cfg.iterations;
         for (const CohortDev& d : table) max_iter = std::max<uint64_t>(max_iter, (uint64_t)d.max_iter);
         const unsigned long long per_pair = 2ull * (max_iter + 2) * 16ull + 64ull;
-        r = eng.run_until_idle(gens * per_pair, err);
+        r = eng.run_until_idle(cfg.max_waves ? cfg.max_waves : gens * per_pair, err);
         if (r) return r;
         return eng.stats(stats, err);
     }
     std::vector<int> fin;
+    uint64_t waves = 0;
     while (!eng.idle()) {
+        if (cfg.max_waves && waves++ >= cfg.max_waves) {
+            err = "the host wave loop reached its wave limit";
+            return KG_ETIMEOUT;
+        }
         fin.clear();
         r = eng.wave(fin, err);
         if (r) return r;

@@ -1,33 +1,54 @@
 """The parity bar shared by the GPU tests.
 
 Tolerances (the estimator's stated bar): Delta and kinship within 1e-5
-absolute, objective within 1e-6 relative, and the condition flag
-(log10 cond > 15) equal wherever the oracle's log10 cond is below 15.  The
-Delta bound applies to identifiable pairs (oracle log10 cond <= 4); beyond that
-Delta is not unique to 1e-5 even in FP64."""
+absolute and objective within 1e-6 relative on every pair whose oracle log10
+condition estimate is finite and below 15, and the condition flag
+(log10 cond > 15) equal on those pairs.  Pairs at or above 15 (or with an
+infinite estimate) are flagged as not identifiable by both sides; only their
+objective and flag are compared.
+
+Each check also reports the band 4 < log10 cond < 15 on its own (count and
+largest Delta error), the pairs where an FP32 pass is closest to its
+resolution."""
 import numpy as np
 
 import kestrel_b200 as kb
 
 KIN = kb.KINSHIP_VECTOR
+DELTA_TOL = 1e-5
+KIN_TOL = 1e-5
+OBJ_RTOL = 1e-6
+COND_FLAG = 15.0
+BAND_LO = 4.0
 
 
-def compare(gpu, ref, strict_cond=4.0, check_xy=True):
+def check_values(jac, obj, log10_cond, ref):
+    """The bar on raw arrays (rows of the API or columns of the CLI's TSV):
+    jac [n, 9], obj [n], log10_cond [n] (None to skip the flag), against the
+    oracle's rows ref."""
+    lc_ref = np.log10(ref["cond"])
+    below = np.isfinite(lc_ref) & (lc_ref < COND_FLAG)
+    band = below & (lc_ref > BAND_LO)
+    dd = np.abs(jac - ref["jacquard"]).max(1)
+    dk = np.abs(jac @ KIN - ref["jacquard"] @ KIN)
+    do = np.abs(obj - ref["obj"]) / np.abs(ref["obj"])
+    assert np.all(np.isfinite(obj))
+    assert dd[below].max(initial=0) <= DELTA_TOL, \
+        f"max Delta err {dd[below].max()} (band 4..15: {int(band.sum())} pairs, max {dd[band].max(initial=0)})"
+    assert dk[below].max(initial=0) <= KIN_TOL, f"max kinship err {dk[below].max()}"
+    assert do.max(initial=0) <= OBJ_RTOL, f"max objective rel err {do.max()}"
+    if log10_cond is not None:
+        assert np.all((log10_cond[below] > COND_FLAG) == (lc_ref[below] > COND_FLAG)), "condition flag differs"
+    return {"max_delta_err": float(dd[below].max(initial=0)),
+            "max_kin_err": float(dk[below].max(initial=0)),
+            "max_obj_rel_err": float(do.max(initial=0)),
+            "compared": int(below.sum()), "flagged": int((~below).sum()),
+            "band_4_15": int(band.sum()), "band_max_delta_err": float(dd[band].max(initial=0)),
+            "pairs": len(ref)}
+
+
+def compare(gpu, ref, check_xy=True):
+    """The bar on result rows (kestrel_b200.OUTPUT_DTYPE) in the oracle's order."""
     if check_xy:
         assert np.array_equal(gpu["x"], ref["x"]) and np.array_equal(gpu["y"], ref["y"])
-    lc_ref = np.log10(ref["cond"])
-    lc_gpu = np.log10(gpu["cond"])
-    ident = np.isfinite(lc_ref) & (lc_ref <= strict_cond)
-    dd = np.abs(gpu["jacquard"] - ref["jacquard"]).max(1)
-    dk = np.abs(gpu["jacquard"] @ KIN - ref["jacquard"] @ KIN)
-    do = np.abs(gpu["obj"] - ref["obj"]) / np.abs(ref["obj"])
-    assert np.all(np.isfinite(gpu["obj"]))
-    assert dd[ident].max(initial=0) <= 1e-5, f"max Delta err {dd[ident].max()}"
-    assert dk[ident].max(initial=0) <= 1e-5
-    assert do.max() <= 1e-6, f"max objective rel err {do.max()}"
-    below = np.isfinite(lc_ref) & (lc_ref < 15)
-    assert np.all((lc_gpu[below] > 15) == (lc_ref[below] > 15))
-    return {"max_delta_err": float(dd[ident].max(initial=0)),
-            "max_kin_err": float(dk.max(initial=0)),
-            "max_obj_rel_err": float(do.max()),
-            "identifiable": int(ident.sum()), "pairs": len(ref)}
+    return check_values(gpu["jacquard"], gpu["obj"], np.log10(gpu["cond"]), ref)

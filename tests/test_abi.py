@@ -65,3 +65,4 @@ def test_soft_likelihood_entry_points_check_their_arguments(L):
     assert L.kg_load_likelihoods(None, None, 1, 1) == _lib.KG_EINVAL
     assert L.kg_relatedness_gl(None, -1, 100, float("nan"), None, 0, None) == _lib.KG_EINVAL
     assert L.kg_vcf_likelihoods(None, None) == _lib.KG_EINVAL
+

@@ -46,7 +46,7 @@ def test_one_hot_likelihoods_give_the_hard_call_estimator(oracle, cohort):
     seg = (alt > 0) & (alt < 1)
     assert np.abs(af[seg, 1] - alt[seg]).max() < 1e-6     # the SQP stops at KKT tolerance 1e-8
     lc = np.log10(hard["cond"])
-    ident = np.isfinite(lc) & (lc <= 4)
+    ident = np.isfinite(lc) & (lc < 15)
     # the frequencies differ at the SQP's tolerance, so the estimates at the
     # parity bar (Delta 1e-5 absolute, objective 1e-6 relative) and tighter
     assert np.abs(soft["jacquard"] - hard["jacquard"]).max(1)[ident].max() < 1e-6
@@ -121,7 +121,7 @@ def test_tri_site_with_an_absent_allele_is_biallelic(oracle, cohort):
     assert np.all(af2[cut:, 2] == 0.0)
     assert np.abs(af2[cut:, :2] - af[cut:, :2]).max() < 1e-7
     lc = np.log10(base["cond"])
-    ident = np.isfinite(lc) & (lc <= 4)
+    ident = np.isfinite(lc) & (lc < 15)
     assert np.abs(split["jacquard"] - base["jacquard"]).max(1)[ident].max() < 1e-6
     assert np.all(np.abs(split["obj"] - base["obj"]) <= 1e-9 * np.abs(base["obj"]))
 

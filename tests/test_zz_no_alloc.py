@@ -55,6 +55,14 @@ def test_noalloc_matches_allocating_entry_point():
         _check_close(got2, ref)
 
 
+def test_noalloc_matches_the_oracle(oracle):
+    """The same rows against the FP64 oracle directly (the bar of the other
+    parity tests)."""
+    from .parity import compare
+    c = synth.make_cohort(32, 5000, seed=33, planted={"half_sib": 2})
+    print(compare(_noalloc_rows(c.codes), oracle.relatedness(c.codes)))
+
+
 def test_noalloc_rejects_oversized_input():
     import torch
     codes = torch.zeros((513, 10), dtype=torch.uint8, device="cuda:0")
