@@ -95,8 +95,27 @@ int kg_set_launch(kg_ctx *ctx, int slots, int blocks_per_sm);
  * loop's error path can be exercised without a fault. */
 int kg_set_wave_limit(kg_ctx *ctx, uint64_t waves);
 
-/* Runs the autotuner on a sample of the loaded cohort and keeps the fastest
- * launch shape; writes it to *slots / *blocks_per_sm if non-NULL. */
+/* Pass work unit (the site chunk one warp of the site-pass kernel streams at a
+ * time): list entries per unit, a multiple of 512 from 1024 to 65536, or 0 for
+ * the default (16384).  It sets how a pass's FP64 partial sums are grouped, so
+ * rows can change in their last bits (well inside the parity tolerances).  No
+ * counterpart in the reference (its passes stream a pair's rows in 32-row blocks,
+ * src/jacquard/grad_hess.rs:10). */
+int kg_set_work_unit(kg_ctx *ctx, int entries);
+
+/* The context's launch shape: pairs in flight (0 = automatic), site-pass blocks
+ * per SM (0 = occupancy limit), work unit (0 = default) and the divisor of the
+ * automatic pairs in flight (the job's pairs / divisor, within 4096..32768).
+ * Any pointer may be NULL. */
+int kg_get_launch(const kg_ctx *ctx, int *slots, int *blocks_per_sm, int *unit_entries, int *slot_divisor);
+
+/* Runs the autotuner on a sample of the loaded cohort (about 32,768 pairs of
+ * its first samples) and keeps the fastest launch shape: site-pass blocks per
+ * SM (occupancy limit, 4, 3), the work unit (16384, 8192, 4096 entries) and the
+ * automatic pairs in flight (an eighth, a quarter or a sixteenth of a job's
+ * pairs), by coordinate descent, a change kept only when it is more than 2%
+ * faster.  Writes *slots (0: automatic) and *blocks_per_sm if non-NULL;
+ * kg_get_launch reports the rest. */
 int kg_autotune(kg_ctx *ctx, int *slots, int *blocks_per_sm);
 
 /* ---------------------------------------------------------------- cohort */
@@ -117,14 +136,23 @@ int kg_load_genotypes_2bit(kg_ctx *ctx, const uint32_t *codes2,
  * them from the samples (the reference's -a estimate). */
 int kg_set_allele_frequencies(kg_ctx *ctx, const double *af);
 
-/* Tri- and tetra-allelic sites for kg_relatedness_gt (the reference's gt3 and
- * gt4, src/coefficients.rs:180-224): gidx[s * row_stride + v] is sample s's
- * genotype at site v as its index in the VCF order (j (j + 1) / 2 + i for
- * alleles i <= j; 255 = missing, which drops the site), n_alleles[v] the site's
- * allele count (3 or 4), af (n_sites x 4, or NULL to count them over all
- * samples) its allele frequencies.  n_samples must be that of the loaded
- * genotypes; loading genotypes again clears these, as does n_sites = 0.  The ML
- * estimator (kg_relatedness) does not use them. */
+/* Tri- and tetra-allelic sites (the reference's gt3 and gt4 for the CLS
+ * estimator, src/coefficients.rs:180-224, and its gl3 / gl4 on one-hot
+ * likelihoods for the ML estimator, src/coefficients.rs:99-106):
+ * gidx[s * row_stride + v] is sample s's genotype at site v as its index in the
+ * VCF order (j (j + 1) / 2 + i for alleles i <= j; 255 = missing), n_alleles[v]
+ * the site's allele count (3 or 4), af (n_sites x 4, or NULL) its allele
+ * frequencies.  n_samples must be that of the loaded genotypes; loading
+ * genotypes again clears these, as does n_sites = 0.
+ *   kg_relatedness_gt: a missing call drops the site; frequencies are counts
+ *   over all samples unless af is given.
+ *   kg_relatedness: a missing call drops the site for that sample's pairs;
+ *   frequencies come from the per-site fit over the called samples (capped
+ *   at the call's iterations, then the maf cut) unless af is given; alleles
+ *   left at zero frequency are dropped (src/wrapper.rs:349-409), a site with
+ *   fewer than two left is discarded, and a call that uses a dropped allele
+ *   gives its pairs a row of zeros at that site, as the reference's one-hot
+ *   likelihoods do. */
 int kg_load_multiallelic(kg_ctx *ctx, const uint8_t *gidx, int64_t n_samples, int64_t n_sites,
                          int64_t row_stride, const uint8_t *n_alleles, const double *af);
 
@@ -288,6 +316,11 @@ typedef struct {
     double pair_kernel_ms;     /* CUDA-event time of all pair-engine waves */
     double device_ms;          /* CUDA-event time of preparation + pair kernel */
     double total_ms;           /* host time of the call */
+    uint64_t sites_used[3];    /* sites the estimate used, by the alleles they keep (2, 3, 4) after the
+                                  frequency cut and the drop of zero-frequency alleles: the reference's
+                                  "Identified N di-/tri-/tetra-allelic sites" (src/wrapper.rs:321-323) */
+    uint64_t sites_discarded;  /* loaded sites left out (fewer than two alleles left, or for the CLS
+                                  estimator a missing call) */
 } kg_run_stats;
 
 int kg_last_run_stats(kg_ctx *ctx, kg_run_stats *stats);
@@ -318,8 +351,8 @@ int kg_vcf_read(const char *path, const char *field, int af_info, int threads, k
 const char *kg_vcf_error(const kg_vcf *vcf);
 /* counts (optional, 7 entries): records, non-SNP records skipped (a base that
  * is not A/C/G/T, or more than four bases), tri- and tetra-allelic records,
- * GL/PL rows that were not one-hot, SNP records with at least one missing
- * call, and (GT) the tri- and the tetra-allelic records kept. */
+ * biallelic GL/PL rows that were not one-hot, SNP records with at least one
+ * missing call, and the tri- and the tetra-allelic records kept. */
 int kg_vcf_info(const kg_vcf *vcf, int64_t *n_samples, int64_t *n_sites, uint64_t *counts);
 /* codes: n_samples x n_sites, sample-major (the layout kg_load_genotypes takes);
  * af: n_sites x 2 [REF, ALT] from INFO/AF (KG_EINVAL if it was not read).
@@ -332,10 +365,13 @@ int kg_vcf_likelihoods(const kg_vcf *vcf, double *gl);
 /* The same codes packed as kg_load_genotypes_2bit takes them (2-bit codes and
  * the observed mask, rows of ceil(n_sites/16) and ceil(n_sites/32) words). */
 int kg_vcf_codes_2bit(const kg_vcf *vcf, uint32_t *codes2, uint32_t *observed);
-/* GT: the tri- and tetra-allelic records that every sample calls (counts[5] +
- * counts[6] of them), the input of kg_load_multiallelic: gidx n_samples x
- * that many genotype indices (sample-major), n_alleles one per record, af (4
- * per record, KG_EINVAL if INFO/AF was not read).  Any may be NULL. */
+/* The tri- and tetra-allelic records (counts[5] + counts[6] of them), the
+ * input of kg_load_multiallelic: gidx n_samples x that many genotype indices
+ * (sample-major, VCF order; GL/PL rows give their most likely genotype; 255 =
+ * a missing call), n_alleles one per record, af (4 per record, KG_EINVAL if
+ * INFO/AF was not read).  Any may be NULL.  A GT record with a malformed call
+ * after a missing one is left out, as the reference's reader stops at the
+ * missing call. */
 int kg_vcf_multiallelic(const kg_vcf *vcf, uint8_t *gidx, uint8_t *n_alleles, double *af);
 /* Sample name i (NULL when out of range). */
 const char *kg_vcf_sample(const kg_vcf *vcf, int64_t i);

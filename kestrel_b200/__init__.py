@@ -147,7 +147,19 @@ class Estimator:
         from the work, which only stops a loop that would not end)."""
         _check(self._L.kg_set_wave_limit(self._h, int(waves)), self._h)
 
+    def set_work_unit(self, entries: int = 0):
+        """List entries per site-pass work unit (0 = the default, 16384)."""
+        _check(self._L.kg_set_work_unit(self._h, int(entries)), self._h)
+
+    def launch(self) -> dict:
+        """The launch shape in use (kg_get_launch; 0 = automatic / default)."""
+        v = [ctypes.c_int() for _ in range(4)]
+        _check(self._L.kg_get_launch(self._h, *[ctypes.byref(x) for x in v]), self._h)
+        return dict(zip(("slots", "blocks_per_sm", "unit_entries", "slot_divisor"), (x.value for x in v)))
+
     def autotune(self):
+        """Runs kg_autotune; returns (slots, blocks_per_sm) as the C call does
+        (launch() gives the work unit and the slot divisor it chose)."""
         w, b = ctypes.c_int(), ctypes.c_int()
         _check(self._L.kg_autotune(self._h, ctypes.byref(w), ctypes.byref(b)), self._h)
         return w.value, b.value
@@ -262,6 +274,7 @@ class Estimator:
         _check(self._L.kg_last_run_stats(self._h, ctypes.byref(s)), self._h)
         d = {f: getattr(s, f) for f, _ in KgRunStats._fields_}
         d["shape_sites"] = list(s.shape_sites)
+        d["sites_used"] = list(s.sites_used)
         return d
 
     def relatedness_batch(self, cohorts, iterations: int = 100, maf=None):
@@ -341,23 +354,16 @@ def relatedness_coefficients_gt(genotypes, allele_frequencies=None, threads=None
     calls (the reference's signature, src/lib.rs:46-70).  genotypes: u8/int
     [variants, samples, 2] allele indices; allele_frequencies: f64 [variants, 2]
     ([REF, ALT]) or None to estimate.  `threads` is accepted and unused.
-    estimator "ml" runs the maximum-likelihood estimator on the calls (alleles
-    other than 0 and 1 count as missing); "cls" runs the reference's own
-    hard-call estimator (conditional least squares with the Brier objective,
-    src/coefficients.rs:166-278) on the sites every sample calls, sites with
-    alleles 2 or 3 as tri- or tetra-allelic sites."""
+    Sites whose calls use allele 2 or 3 are tri- or tetra-allelic (their
+    allele count is the largest allele + 1); allele_frequencies, when given,
+    are [variants, 2] for the biallelic sites only.  estimator "ml" runs the
+    maximum-likelihood estimator on the calls (the reference's GL/PL path on
+    one-hot likelihoods); "cls" runs the reference's own hard-call estimator
+    (conditional least squares with the Brier objective,
+    src/coefficients.rs:166-278) on the sites every sample calls."""
     del threads
     if estimator not in ("ml", "cls"):
         raise ValueError("estimator must be 'ml' or 'cls'")
-    if estimator == "ml":
-        codes = genotype_codes(genotypes)
-        with Estimator() as est:
-            est.load(codes, allele_frequencies)
-            rows = est.relatedness(iterations=iterations)
-        return Coefficients(*build_arrays(rows, codes.shape[0]))
-    # CLS: sites whose calls use allele 2 or 3 are tri- or tetra-allelic
-    # (their allele count is the largest allele + 1); allele_frequencies, when
-    # given, are [variants, 2] for the biallelic sites only
     g = np.asarray(genotypes)
     if g.ndim != 3 or g.shape[2] != 2:
         raise ValueError("genotypes must have shape (variants, samples, 2)")
@@ -377,7 +383,10 @@ def relatedness_coefficients_gt(genotypes, allele_frequencies=None, threads=None
             lo, hi = am.min(axis=2), am.max(axis=2)
             gi = np.where((am >= 0).all(axis=2), hi * (hi + 1) // 2 + lo, 255).astype(np.uint8)
             est.load_multiallelic(np.ascontiguousarray(gi.T), (top[multi] + 1).astype(np.uint8))
-        rows = est.relatedness_gt(iterations=iterations)
+        if estimator == "ml":
+            rows = est.relatedness(iterations=iterations)
+        else:
+            rows = est.relatedness_gt(iterations=iterations)
     return Coefficients(*build_arrays(rows, codes.shape[0]))
 
 
@@ -387,10 +396,10 @@ def read_vcf(path, field: str = "GT", allele_freqs: str = "estimate", threads: i
     (the CLI's): biallelic SNP records become genotype codes.  Returns
     (codes u8 [samples, sites], allele_frequencies f64 [sites, 2] or None,
     sample names, counts dict).  allele_freqs "info" reads INFO/AF.  With
-    multiallelic (GT), a fifth item holds the tri- and tetra-allelic records
-    every sample calls: (genotype indices u8 [samples, sites], allele counts u8
-    [sites], allele frequencies f64 [sites, 4] or None), the arguments of
-    Estimator.load_multiallelic.  With packed, codes is (2-bit codes,
+    multiallelic, a fifth item holds the tri- and tetra-allelic records:
+    (genotype indices u8 [samples, sites] in the VCF order, 255 = missing,
+    allele counts u8 [sites], allele frequencies f64 [sites, 4] or None), the
+    arguments of Estimator.load_multiallelic.  With packed, codes is (2-bit codes,
     observed mask) as pack_2bit gives them, for Estimator.load_packed."""
     if allele_freqs not in ("estimate", "info"):
         raise ValueError("allele_freqs must be 'estimate' or 'info'")

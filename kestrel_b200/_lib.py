@@ -46,7 +46,8 @@ class KgRunStats(ctypes.Structure):
                 ("waves", ctypes.c_uint64), ("slots", ctypes.c_uint64),
                 ("admit_ms", ctypes.c_double), ("pass_ms", ctypes.c_double),
                 ("solve_ms", ctypes.c_double), ("pair_kernel_ms", ctypes.c_double), ("device_ms", ctypes.c_double),
-                ("total_ms", ctypes.c_double)]
+                ("total_ms", ctypes.c_double), ("sites_used", ctypes.c_uint64 * 3),
+                ("sites_discarded", ctypes.c_uint64)]
 
 
 OUTPUT_DTYPE = np.dtype([("x", np.uint64), ("y", np.uint64), ("jacquard", np.float64, 9),
@@ -55,7 +56,7 @@ assert OUTPUT_DTYPE.itemsize == ctypes.sizeof(KgOutput) == 112
 
 # Every symbol include/kestrel_gpu.h declares.
 EXPORTS = ("kg_create", "kg_destroy", "kg_last_error", "kg_version", "kg_set_precision",
-           "kg_set_launch", "kg_set_wave_limit", "kg_autotune", "kg_load_genotypes", "kg_load_genotypes_2bit",
+           "kg_set_launch", "kg_set_wave_limit", "kg_set_work_unit", "kg_get_launch", "kg_autotune", "kg_load_genotypes", "kg_load_genotypes_2bit",
            "kg_set_allele_frequencies", "kg_load_multiallelic", "kg_load_likelihoods", "kg_relatedness_gl",
            "kg_relatedness", "kg_relatedness_gt", "kg_relatedness_coefficients",
            "kg_relatedness_batch", "kg_panel_load", "kg_submit", "kg_poll", "kg_wait",
@@ -90,6 +91,9 @@ def lib():
         "kg_set_precision": ([P, i32], i32),
         "kg_set_launch": ([P, i32, i32], i32),
         "kg_set_wave_limit": ([P, u64], i32),
+        "kg_set_work_unit": ([P, i32], i32),
+        "kg_get_launch": ([P, ctypes.POINTER(i32), ctypes.POINTER(i32), ctypes.POINTER(i32), ctypes.POINTER(i32)],
+                          i32),
         "kg_autotune": ([P, ctypes.POINTER(i32), ctypes.POINTER(i32)], i32),
         "kg_load_genotypes": ([P, P, i64, i64, i64], i32),
         "kg_load_genotypes_2bit": ([P, P, P, i64, i64], i32),

@@ -19,10 +19,10 @@ LIB = os.path.join(HERE, "libkestrel_gpu.so")
 CLI = os.path.join(HERE, "bin", "kestrel")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-CUDA_SOURCES = ["kg_engine.cu", "kg_wave.cu", "kg_api.cu", "kg_noalloc.cu", "kg_soft.cu"]
+CUDA_SOURCES = ["kg_engine.cu", "kg_wave.cu", "kg_api.cu", "kg_noalloc.cu", "kg_soft.cu", "kg_multi.cu"]
 HOST_SOURCES = ["kg_cli.cpp", "kg_vcf.cpp"]
 HEADERS = ["kg_engine.h", "kg_pair.cuh", "kg_solver.cuh", "kg_rowsolve.cuh", "kg_wave.cuh", "kg_bulk.cuh",
-           "kg_vcf.h", "kg_threads.h", "kg_allele.cuh"]
+           "kg_vcf.h", "kg_threads.h", "kg_allele.cuh", "kg_alleleN.cuh"]
 
 
 def nvcc() -> str:

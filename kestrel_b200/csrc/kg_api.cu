@@ -46,6 +46,8 @@ struct kg_ctx {
     int precision = KG_PREC_FP32C;
     int64_t wave_slots = 0;
     int pass_bps = 0;
+    int unit_elems = 0;
+    int slot_divisor = 8;
     uint64_t wave_limit = 0;
     cudaStream_t stream = nullptr;
     // single cohort
@@ -128,6 +130,8 @@ kg::RunConfig run_config(const kg_ctx* c, uint64_t iterations) {
     cfg.slots = c->wave_slots;
     cfg.pass_blocks_per_sm = c->pass_bps;
     cfg.max_waves = c->wave_limit;
+    cfg.unit_elems = c->unit_elems;
+    cfg.slot_divisor = c->slot_divisor;
     return cfg;
 }
 
@@ -393,6 +397,23 @@ int kg_set_launch(kg_ctx* c, int slots, int blocks_per_sm) {
     return KG_OK;
 }
 
+int kg_set_work_unit(kg_ctx* c, int entries) {
+    if (!c) return KG_EINVAL;
+    if (entries != 0 && (entries < 1024 || entries > 65536 || entries % 512 != 0))
+        return set_err(c, KG_EINVAL, "the work unit must be 0 or a multiple of 512 from 1024 to 65536 entries");
+    c->unit_elems = entries;
+    return KG_OK;
+}
+
+int kg_get_launch(const kg_ctx* c, int* slots, int* blocks_per_sm, int* unit_entries, int* slot_divisor) {
+    if (!c) return KG_EINVAL;
+    if (slots) *slots = (int)c->wave_slots;
+    if (blocks_per_sm) *blocks_per_sm = c->pass_bps;
+    if (unit_entries) *unit_entries = c->unit_elems;
+    if (slot_divisor) *slot_divisor = c->slot_divisor;
+    return KG_OK;
+}
+
 int kg_set_wave_limit(kg_ctx* c, uint64_t waves) {
     if (!c) return KG_EINVAL;
     c->wave_limit = waves;
@@ -521,6 +542,9 @@ int kg_relatedness(kg_ctx* c, int64_t num_samples, uint64_t iterations, double m
                                 c->cohort.n_sites, c->cohort.n_sites, true,
                                 c->af_set ? c->af.data() : nullptr, std::isnan(maf) ? -1.0 : maf,
                                 c->stream, err, false, iterations);
+        if (!st)
+            st = kg::prepare_ml_multi(c->cohort, c->multi_af, std::isnan(maf) ? -1.0 : maf, iterations, c->stream,
+                                      err);
         if (st) {
             cudaEventDestroy(ev0);
             cudaEventDestroy(ev1);
@@ -543,6 +567,12 @@ int kg_relatedness(kg_ctx* c, int64_t num_samples, uint64_t iterations, double m
         cudaEventDestroy(ev0);
         cudaEventDestroy(ev1);
         stats.launches += 7;  // count, freq, two scans, compact, pad, pack
+        const kg::Cohort& co = c->cohort;
+        if (co.n_multi > 0) stats.launches += 3 + (co.ml_nk > 0 ? 2 : 0);   // fit, two scans, rows, codes
+        stats.sites_used[0] = (uint64_t)(co.n_kept + co.ml_by_alleles[0]);
+        stats.sites_used[1] = (uint64_t)co.ml_by_alleles[1];
+        stats.sites_used[2] = (uint64_t)co.ml_by_alleles[2];
+        stats.sites_discarded = (uint64_t)(co.n_sites + co.n_multi - co.n_kept - co.ml_nk);
         if (st2 && !st) st = st2;
         stats.total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
         c->last = stats;
@@ -606,6 +636,9 @@ int kg_relatedness_gt(kg_ctx* c, int64_t num_samples, uint64_t iterations, kg_ou
         cudaEventDestroy(ev1);
         stats.launches += 9;  // count, freq, two scans, compact, pad, pack, Gram, Gram total
         if (c->cohort.n_multi > 0) stats.launches += 5;   // multi-allelic frequencies, Gram, Gram total, transpose, rows
+        stats.sites_used[0] = (uint64_t)c->cohort.n_kept;
+        stats.sites_discarded = (uint64_t)(c->cohort.n_sites - c->cohort.n_kept +
+                                           (c->cohort.n_multi > 0 ? c->cohort.n_multi - c->cohort.n_multi_kept : 0));
         if (st2 && !st) st = st2;
         stats.total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
         c->last = stats;
@@ -659,8 +692,9 @@ int kg_relatedness_gl(kg_ctx* c, int64_t num_samples, uint64_t iterations, doubl
         cudaEventCreate(&ev0);
         cudaEventCreate(&ev1);
         cudaEventRecord(ev0, c->stream);
+        int64_t kept = 0;
         st = kg::soft_relatedness(c->soft_gl, c->soft_ns, c->soft_nv, ns, iterations, std::isnan(maf) ? -1.0 : maf,
-                                  c->dout.as<kg_output>(), c->stream, err);
+                                  c->dout.as<kg_output>(), c->stream, err, &kept);
         cudaEventRecord(ev1, c->stream);
         int st2 = copy_rows_out(c, c->dout, np, out, c->stream);
         kg_run_stats stats{};
@@ -669,6 +703,8 @@ int kg_relatedness_gl(kg_ctx* c, int64_t num_samples, uint64_t iterations, doubl
         cudaEventDestroy(ev0);
         cudaEventDestroy(ev1);
         stats.launches = 2;   // frequencies, pairs
+        stats.sites_used[0] = (uint64_t)kept;
+        stats.sites_discarded = (uint64_t)(c->soft_nv - kept);
         stats.total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
         c->last = stats;
         if (n_out) *n_out = np;
@@ -781,6 +817,20 @@ int kg_last_run_stats(kg_ctx* c, kg_run_stats* s) {
     return KG_OK;
 }
 
+// The autotuner: the launch shape that gives the fewest device milliseconds
+// per pair on a sample of the loaded cohort (the first samples, about 32,768
+// pairs, every site), by coordinate descent over three parameters in turn,
+// each candidate run twice and timed the second time (the first instantiates
+// its graphs):
+//   * site-pass blocks per SM: the occupancy limit (5), 4, 3;
+//   * the work unit (site chunk) of the pass kernel: 16,384, 8,192, 4,096
+//     list entries;
+//   * pairs in flight (the pair tile of a wave) as a share of the job's pairs:
+//     an eighth (the default), a quarter, a sixteenth, within 4,096..32,768.
+// A candidate is kept only when it beats the current choice by more than 2%,
+// so run-to-run noise leaves the defaults.  Slots and blocks per SM leave the
+// rows bit for bit the same; the work unit changes how a pass's FP64 partial
+// sums are grouped, so rows can move in their last bits.
 int kg_autotune(kg_ctx* c, int* slots_out, int* bps_out) {
     if (!c) return KG_EINVAL;
     if (!c->loaded) return set_err(c, KG_EINVAL, "load genotypes first");
@@ -792,35 +842,58 @@ int kg_autotune(kg_ctx* c, int* slots_out, int* bps_out) {
                                 c->cohort.n_sites, c->cohort.n_sites, true,
                                 c->af_set ? c->af.data() : nullptr, -1.0, c->stream, err);
         if (st) return set_err(c, st, err);
-        // a sample triangle of about 4096 pairs
+        c->cohort.ml_nk = 0;   // the sample runs the biallelic sites
         int64_t ns = 2;
-        while (ns < c->cohort.n_samples && ns * (ns + 1) / 2 < 4096) ns++;
-        int64_t np = ns * (ns + 1) / 2;
+        while (ns < c->cohort.n_samples && ns * (ns + 1) / 2 < 32768) ns++;
+        const int64_t np = ns * (ns + 1) / 2;
         if (c->dout.reserve(sizeof(kg_output) * np) != cudaSuccess)
             return set_err(c, KG_ENOMEM, "cannot allocate device output rows");
-        // the site-pass kernel's blocks per SM decide its latency hiding; the
-        // slot count only needs to cover the work (the default)
-        const int cand[] = {4, 3, 2};
-        double best = 1e300;
-        int bb = 0;
-        for (int cd : cand) {
-            kg::PairJob jb;
-            jb.panel = &c->cohort;
-            jb.n_x = ns;
-            jb.d_out = c->dout.as<kg_output>();
+        kg::PairJob jb;
+        jb.panel = &c->cohort;
+        jb.n_x = ns;
+        jb.d_out = c->dout.as<kg_output>();
+        int bps = 0, unit = 0, div = 8;
+        auto cost = [&](int b, int u, int d, double& ms) -> int {
             kg::RunConfig cfg = run_config(c, 100);
             cfg.slots = 0;
-            cfg.pass_blocks_per_sm = cd;
-            kg_run_stats stt{};
-            st = kg::run_pairs({jb}, cfg, c->ws, c->stream, stt, err);
-            if (st && st != KG_ENOSITES) return set_err(c, st, err);
-            double cost = stt.pass_ms / std::max<double>(1.0, (double)stt.work_units);
-            if (cost < best) { best = cost; bb = cd; }
-        }
+            cfg.pass_blocks_per_sm = b;
+            cfg.unit_elems = u;
+            cfg.slot_divisor = d;
+            for (int rep = 0; rep < 2; rep++) {
+                kg_run_stats stt{};
+                int r = kg::run_pairs({jb}, cfg, c->ws, c->stream, stt, err);
+                if (r && r != KG_ENOSITES) return r;
+                ms = stt.pair_kernel_ms;
+            }
+            return KG_OK;
+        };
+        double best = 0.0;
+        st = cost(bps, unit, div, best);
+        if (st) return set_err(c, st, err);
+        auto consider = [&](int b, int u, int d) -> int {
+            double ms = 0.0;
+            int r = cost(b, u, d, ms);
+            if (r) return r;
+            if (ms < 0.98 * best) {
+                best = ms;
+                bps = b;
+                unit = u;
+                div = d;
+            }
+            return KG_OK;
+        };
+        for (int b : {4, 3})
+            if ((st = consider(b, unit, div))) return set_err(c, st, err);
+        for (int u : {8192, 4096})
+            if ((st = consider(bps, u, div))) return set_err(c, st, err);
+        for (int d : {4, 16})
+            if ((st = consider(bps, unit, d))) return set_err(c, st, err);
         c->wave_slots = 0;
-        c->pass_bps = bb;
+        c->pass_bps = bps;
+        c->unit_elems = unit;
+        c->slot_divisor = div;
         if (slots_out) *slots_out = 0;
-        if (bps_out) *bps_out = bb;
+        if (bps_out) *bps_out = bps;
         return KG_OK;
     });
 }

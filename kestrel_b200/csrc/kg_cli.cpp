@@ -1,6 +1,5 @@
 // kg_cli.cpp — the reference-compatible command line (src/cli.rs:12-181) on
-// top of the C ABI; its VCF reader (src/vcf.rs:96-482, biallelic SNPs) is
-// kg_vcf.cpp.  The CUDA context is created while the VCF is read, and the
+// top of the C ABI; its VCF reader (src/vcf.rs:96-482) is kg_vcf.cpp.  The CUDA context is created while the VCF is read, and the
 // output rows are formatted on the host threads in blocks, written in order.
 //
 //   kestrel input.vcf[.gz] kinship.tsv [-a estimate|info] [-f GT|GL|PL]
@@ -10,8 +9,12 @@
 // most likely genotype (the reference's one-hot PL encoding, 0 at the call and
 // 255 elsewhere, maps back exactly).  Missing entries become code 3 and are
 // dropped per pair, as the reference's NaN likelihood rows are
-// (src/vcf.rs:355,397; src/lanevector.rs:99-104).  Only biallelic SNPs are
-// estimated; tri- and tetra-allelic SNPs are counted and skipped.
+// (src/vcf.rs:355,397; src/lanevector.rs:99-104).  Tri- and tetra-allelic
+// SNPs go to the estimators as genotype indices (kg_load_multiallelic): the
+// CLS estimator uses the ones every sample calls, the ML estimator all of them
+// (with the reference's frequency cut and drop of zero-frequency alleles).
+// Files with soft likelihoods run the soft-likelihood estimator on their
+// biallelic SNPs.
 #include "kg_threads.h"
 #include "kg_vcf.h"
 
@@ -323,14 +326,16 @@ extern "C" int kg_run_cli(int argc, const char* const* argv) {
     if (o.cls) {
         // the CLS estimator uses the sites every sample calls, tri- and
         // tetra-allelic ones included (src/vcf.rs:127-181, :217-221)
-        const uint64_t bi_missing = vcf.incomplete - (vcf.multi - vcf.tri - vcf.tetra);
+        const uint64_t bi_missing = vcf.incomplete - vcf.multi_incomplete;
         log_info("Skipped %s sites with missing data", std::to_string(vcf.incomplete));
         log_info("Found %s di-allelic sites", std::to_string(vcf.n_sites - (int64_t)bi_missing));
+        log_info("Found %s tri-allelic sites", std::to_string(vcf.tri_full));
+        log_info("Found %s tetra-allelic sites", std::to_string(vcf.tetra_full));
+    } else {
+        // the GL/PL reader's counts (src/vcf.rs:238-320)
+        log_info("Found %s di-allelic sites", std::to_string(vcf.n_sites));
         log_info("Found %s tri-allelic sites", std::to_string(vcf.tri));
         log_info("Found %s tetra-allelic sites", std::to_string(vcf.tetra));
-    } else {
-        log_info("Found %s di-allelic sites", std::to_string(vcf.n_sites));
-        log_info("Skipped %s tri- or tetra-allelic sites (biallelic sites only)", std::to_string(vcf.multi));
     }
     // GL/PL likelihoods that are not all one-hot go to the soft-likelihood
     // estimator, as the reference's GL path fits them (src/wrapper.rs:89-330)
@@ -338,6 +343,9 @@ extern "C" int kg_run_cli(int argc, const char* const* argv) {
     if (soft_path) {
         log_info("%s likelihood entries are not one-hot: estimating from the soft likelihoods",
                  std::to_string(vcf.soft));
+        if (vcf.n_multi > 0)
+            log_info("Skipped %s tri- or tetra-allelic sites (the soft-likelihood estimator takes biallelic sites)",
+                     std::to_string(vcf.n_multi));
         if (o.af_info) {
             std::fprintf(stderr, "Error: allele frequencies from INFO/AF cannot be used with soft likelihoods\n");
             return 1;
@@ -376,12 +384,15 @@ extern "C" int kg_run_cli(int argc, const char* const* argv) {
         if (!st) tracker.checkpoint();
         if (!st) st = kg_relatedness_gl(ctx, nsel, o.iterations, o.maf, out.data(), np, &nout);
     } else {
+        if (!o.cls && vcf.multi_soft > 0)
+            std::fprintf(stderr, "[WARN ] %llu tri- or tetra-allelic likelihood rows are not one-hot: their most "
+                                 "likely genotypes are used\n", (unsigned long long)vcf.multi_soft);
         // the reader's codes go up packed: 2 bits a call plus the observed mask
         std::vector<uint32_t> codes2((size_t)(ns * ((nv + 15) / 16))), observed((size_t)(ns * ((nv + 31) / 32)));
         kg::pack_2bit(vcf, o.threads, codes2.data(), observed.data());
         st = kg_load_genotypes_2bit(ctx, codes2.data(), observed.data(), ns, nv);
         if (!st && o.af_info) st = kg_set_allele_frequencies(ctx, af.data());
-        if (!st && o.cls && vcf.n_multi > 0)
+        if (!st && vcf.n_multi > 0)
             st = kg_load_multiallelic(ctx, vcf.mcodes.data(), ns, vcf.n_multi, vcf.n_multi, vcf.malleles.data(),
                                       o.af_info ? vcf.maf.data() : nullptr);
         if (!st && !o.cls) tracker.checkpoint();
@@ -393,6 +404,17 @@ extern "C" int kg_run_cli(int argc, const char* const* argv) {
     if (st) {
         std::fprintf(stderr, "Error: %s\n", kg_last_error(ctx));
         return 1;
+    }
+    if (!o.cls) {
+        // the sites the ML estimate used after the frequency cut and the drop
+        // of zero-frequency alleles (src/wrapper.rs:321-324)
+        kg_run_stats rs{};
+        if (kg_last_run_stats(ctx, &rs) == 0) {
+            log_info("Identified %s di-allelic sites", std::to_string(rs.sites_used[0]));
+            log_info("Identified %s tri-allelic sites", std::to_string(rs.sites_used[1]));
+            log_info("Identified %s tetra-allelic sites", std::to_string(rs.sites_used[2]));
+            log_info("Discarded %s non-segregating sites", std::to_string(rs.sites_discarded));
+        }
     }
     tracker.checkpoint();
     dev.release();

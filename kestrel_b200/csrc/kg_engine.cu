@@ -67,7 +67,9 @@ size_t Cohort::device_bytes() const {
     return raw.bytes + af.bytes + rc.bytes + oc.bytes + hc.bytes + keep.bytes + kidx.bytes + bsum.bytes +
            nkept.bytes + pfull.bytes + qfull.bytes + p32.bytes + p64.bytes + q64.bytes +
            site_of.bytes + planes.bytes + cls_q.bytes + cls_part.bytes + mg.bytes + malleles.bytes + maf.bytes +
-           mfreq.bytes + mkeep.bytes + mcount.bytes + mpart.bytes + cmulti.bytes + mgT.bytes;
+           mfreq.bytes + mkeep.bytes + mcount.bytes + mpart.bytes + cmulti.bytes + mgT.bytes + ml_keep.bytes +
+           ml_nrows.bytes + ml_kidx.bytes + ml_rbase.bytes + ml_remap.bytes + ml_redf.bytes + ml_count.bytes +
+           ml_site.bytes + ml_orig.bytes + ml_kremap.bytes + ml_rows.bytes + ml_gr.bytes + ml_obs.bytes;
 }
 
 const char* engine_version() { return "kestrel-b200 0.1.0 (sm_100a)"; }
@@ -819,6 +821,14 @@ CohortDev make_cohort_dev(const PairJob& jb, uint64_t iterations) {
     const bool multi = jb.method == ESTIMATOR_CLS && pn.n_multi_kept > 0;
     d.cls_cmulti = multi ? pn.cmulti.as<double>() : nullptr;
     d.cls_m = (double)pn.n_kept + (multi ? (double)pn.n_multi_kept : 0.0);
+    // the ML path's tri- and tetra-allelic sites (whole cohorts only)
+    const bool ml = jb.method == ESTIMATOR_ML && jb.kind == COHORT_TRIANGLE && pn.ml_nk > 0;
+    d.ml_gr = ml ? pn.ml_gr.as<uint8_t>() : nullptr;
+    d.ml_obs = ml ? pn.ml_obs.as<uint32_t>() : nullptr;
+    d.ml_site = ml ? pn.ml_site.as<int2>() : nullptr;
+    d.ml_rows = ml ? pn.ml_rows.as<double>() : nullptr;
+    d.ml_nk = ml ? (int32_t)pn.ml_nk : 0;
+    d.ml_stride = ml ? (int32_t)pn.ml_stride : 0;
     return d;
 }
 

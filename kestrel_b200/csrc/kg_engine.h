@@ -91,6 +91,18 @@ struct Cohort {
     DevBuf mcount;             // int32[2]: sites used, bad-index flag
     DevBuf mpart;              // per-block partial sums of their Q terms
     DevBuf cmulti;             // per output row, the 9 summed rows of the pair's multi-allelic sites
+    // ML: the same tri- and tetra-allelic sites after the frequency fit, the
+    // maf cut and the drop of zero-frequency alleles (kg_multi.cu)
+    int64_t ml_nk = 0;         // kept sites (two or more alleles remain)
+    int64_t ml_stride = 0;     // bytes per sample row of ml_gr (a multiple of 32)
+    int64_t ml_by_alleles[3] = {0, 0, 0};   // kept sites left with 2, 3, 4 alleles
+    DevBuf ml_keep, ml_nrows, ml_kidx, ml_rbase, ml_remap, ml_redf, ml_count;   // per loaded site
+    DevBuf ml_site;            // int2 per kept site: first row of its table, reduced genotypes G'
+    DevBuf ml_orig;            // int32 per kept site: loaded site index
+    DevBuf ml_kremap;          // uint8 [kept][10]: original genotype -> reduced genotype or ML_ZERO_ROW
+    DevBuf ml_rows;            // double [rows][9]: m[g'x][g'y] of every kept site
+    DevBuf ml_gr;              // uint8 [n_samples][ml_stride]: reduced genotype, ML_ZERO_ROW or ML_MISSING
+    DevBuf ml_obs;             // uint32 [n_samples][ml_stride / 32]: called at the kept site
     size_t device_bytes() const;
 };
 
@@ -110,12 +122,20 @@ int prepare_cohort(Cohort& c, const uint8_t* codes, int64_t n_samples, int64_t n
 // summed rows (c.cmulti).  Sets c.n_multi_kept.
 int prepare_multi(Cohort& c, bool have_af, int64_t num_samples, cudaStream_t st, std::string& err);
 
+// Before an ML estimate: the cohort's tri- and tetra-allelic sites (c.mg,
+// c.malleles, c.maf uploaded, c.n_multi set) as the reference's GL/PL path
+// takes them on one-hot likelihoods (kg_multi.cu): frequencies fitted over the
+// called samples (capped at `iterations`; the caller's when have_af), maf cut
+// (maf < 0: 1 / (2 n_samples)), zero-frequency alleles dropped, sites with
+// fewer than two alleles left discarded.  Sets c.ml_nk.
+int prepare_ml_multi(Cohort& c, bool have_af, double maf, uint64_t iterations, cudaStream_t st, std::string& err);
+
 // The GL/PL estimator on soft likelihoods of biallelic sites (kg_soft.cu): gl
 // is double [n_samples][n_sites][3] on the device (linear scale, NaN =
 // missing); rows of the first ns samples into d_out (device), the reference's
 // order.  maf < 0: 1 / (2 n_samples).
 int soft_relatedness(const DevBuf& gl, int64_t n_samples, int64_t n_sites, int64_t ns, uint64_t iterations,
-                     double maf, kg_output* d_out, cudaStream_t st, std::string& err);
+                     double maf, kg_output* d_out, cudaStream_t st, std::string& err, int64_t* n_kept = nullptr);
 
 // Unpacks the VCF reader's 2-bit codes + observed mask into device byte codes
 // (d2, dm: the packed rows' device copies, kept for the next load).
@@ -152,6 +172,9 @@ struct RunConfig {
     int64_t slots = 0;         // pairs in flight per wave (0 = pairs / 8 within 4096..32768, as memory allows)
     int pass_blocks_per_sm = 0;   // site-pass kernel blocks per SM (0 = occupancy limit)
     uint64_t max_waves = 0;       // waves a call may run before it gives up (0 = a bound from the work)
+    int ml_units = 0;             // work units per slot of the ML path's tri-/tetra-allelic sites (run_pairs sets it)
+    int unit_elems = 0;           // list entries per site-pass work unit (0 = UNIT_ELEMS, 16384)
+    int slot_divisor = 8;         // automatic slots: the job's pairs / slot_divisor within 4096..32768
     // Called between waves, on the calling thread, once per job whose pairs
     // have all finished (their rows are final in device memory).
     std::function<void(int job)> job_done;
@@ -164,6 +187,7 @@ class WaveEngine;
 struct Workspace {
     DevBuf scratch, queue, counters, table;
     DevBuf partial, slots, lists_a, lists_b, tasks, counts, done;
+    DevBuf ml_partial;   // per slot and unit, the sums of the ML path's tri-/tetra-allelic sites
     PinBuf host;   // per-wave counters read back by the host loop
     int sm_count = 0;
     // run_pairs' engine, kept between calls: a call of the same shape only

@@ -111,6 +111,12 @@ __global__ void noalloc_table_kernel(kg::CohortDev* table, const uint2* planes, 
     d.cls_q = nullptr;
     d.cls_cmulti = nullptr;
     d.cls_m = (double)nkept[0];
+    d.ml_gr = nullptr;
+    d.ml_obs = nullptr;
+    d.ml_site = nullptr;
+    d.ml_rows = nullptr;
+    d.ml_nk = 0;
+    d.ml_stride = 0;
     *table = d;
 }
 

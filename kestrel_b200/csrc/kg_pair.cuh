@@ -75,7 +75,20 @@ struct CohortDev {
     const double* cls_q;     // CLS: the 9 x 9 quadratic matrix Q (row-major)
     const double* cls_cmulti;  // CLS: per output row, the 9 summed rows of its tri-/tetra-allelic sites (or NULL)
     double cls_m;            // CLS: the sites M that Q and c are divided by (biallelic + multi-allelic)
+    // ML: tri- and tetra-allelic sites (triangle cohorts; ml_nk = 0 otherwise)
+    const uint8_t* ml_gr;    // [samples][ml_stride] reduced genotype, ML_ZERO_ROW or ML_MISSING
+    const uint32_t* ml_obs;  // [samples][ml_stride / 32] called bits
+    const int2* ml_site;     // per kept site: {first row, reduced genotypes G'}
+    const double* ml_rows;   // [rows][9] m[g'x][g'y]
+    int32_t ml_nk;           // kept sites
+    int32_t ml_stride;       // bytes per sample row of ml_gr (a multiple of 32)
 };
+
+// Reduced genotype codes of the ML path's tri- and tetra-allelic sites: a call
+// that uses a dropped allele (its likelihood row becomes all zeros) and a
+// missing call.
+constexpr uint8_t ML_ZERO_ROW = 0xFE;
+constexpr uint8_t ML_MISSING = 0xFF;
 
 // The estimators: maximum likelihood (the GL/PL path, src/coefficients.rs:40-141)
 // and the hard-call conditional least squares with the Brier objective (the

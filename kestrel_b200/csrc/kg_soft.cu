@@ -229,7 +229,7 @@ __global__ void __launch_bounds__(SOFT_WARPS * 32, 4) soft_pairs_kernel(
 }
 
 int soft_relatedness(const DevBuf& gl, int64_t n_samples, int64_t n_sites, int64_t ns, uint64_t iterations,
-                     double maf, kg_output* d_out, cudaStream_t st, std::string& err) {
+                     double maf, kg_output* d_out, cudaStream_t st, std::string& err, int64_t* n_kept) {
     if (!(maf >= 0.0)) maf = 1.0 / (2.0 * (double)n_samples);
     DevBuf pf, qf, keep, idx, kp, kq, ctr;
     KG_SOFT_TRY((cudaError_t)pf.reserve(sizeof(double) * n_sites));
@@ -255,6 +255,7 @@ int soft_relatedness(const DevBuf& gl, int64_t n_samples, int64_t n_sites, int64
             kqv.push_back(hq[(size_t)v]);
         }
     const int64_t nk = (int64_t)ki.size();
+    if (n_kept) *n_kept = nk;
     if (nk == 0) {
         err = "no segregating site left after allele-frequency filtering";
         return KG_ENOSITES;

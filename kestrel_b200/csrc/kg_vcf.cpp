@@ -293,6 +293,51 @@ bool parse_call(std::string_view v, char field, uint8_t& code, uint64_t& soft, d
     return true;
 }
 
+// Most likely genotype (VCF order) of a GL/PL value of ng likelihoods at a
+// tri- or tetra-allelic site, 255 when the value or an entry is missing; the
+// row counts as soft as in parse_call.  False when the value is not ng numbers.
+bool parse_like_index(std::string_view v, char field, int ng, uint8_t& g, uint64_t& soft) {
+    if (v == ".") {
+        g = 255;
+        return true;
+    }
+    double ll[10];
+    int k = 0;
+    bool any_missing = false;
+    size_t b = 0;
+    for (size_t i = 0; i <= v.size(); i++) {
+        if (i == v.size() || v[i] == ',') {
+            if (k >= ng) return false;
+            const std::string_view t = v.substr(b, i - b);
+            if (t == ".") {
+                any_missing = true;
+                ll[k++] = 0.0;
+            } else {
+                double x = 0.0;
+                const auto r = std::from_chars(t.data(), t.data() + t.size(), x);
+                if (r.ec != std::errc() || r.ptr == t.data()) return false;
+                ll[k++] = field == 'P' ? -x / 10.0 : x;   // PL = -10 log10 L, GL = log10 L
+            }
+            b = i + 1;
+        }
+    }
+    if (k != ng) return false;
+    if (any_missing) {
+        g = 255;
+        return true;
+    }
+    int best = 0;
+    for (int i = 1; i < ng; i++)
+        if (ll[i] > ll[best]) best = i;
+    for (int i = 0; i < ng; i++)
+        if (i != best && ll[best] - ll[i] < 25.5 - 1e-9) {
+            soft++;
+            break;
+        }
+    g = (uint8_t)best;
+    return true;
+}
+
 // Genotype index (VCF order, j (j + 1) / 2 + i for alleles i <= j) of a GT
 // value at a site with n_alleles alleles; 255 when an allele is missing.
 // False when the value is not a diploid call of the site's alleles.
@@ -375,12 +420,14 @@ struct Chunk {
     std::vector<double> af;
     uint64_t total = 0, not_snp = 0, multi = 0, soft = 0, incomplete = 0;
     int64_t kept = 0;
-    // GT: tri- and tetra-allelic records every sample calls
+    // tri- and tetra-allelic records (255 = a missing call)
     std::vector<uint8_t> mrows;  // kept records x samples, genotype indices
     std::vector<uint8_t> malleles;
     std::vector<double> maf;     // 4 per record
     int64_t mkept = 0;
-    uint64_t tri = 0, tetra = 0;
+    uint64_t tri = 0, tetra = 0, tri_full = 0, tetra_full = 0, mincomplete = 0;
+    uint64_t multi_dropped = 0;  // GT records with a malformed call after a missing one
+    uint64_t msoft = 0;          // GL/PL rows of these records that are not one-hot
     bool failed = false;
     uint64_t fail_rec = 0;       // 1-based record index within the chunk
     std::string fail_kind;       // message with %R for the global record number
@@ -441,10 +488,6 @@ void parse_chunk(Chunk& c, char field, bool af_info, size_t n_samples, bool want
         }
         const bool multi = n_bases > 2;
         if (multi) c.multi++;
-        if (multi && field != 'T') {
-            p = next;
-            continue;
-        }
         const std::string_view fmt = field_of(8);
         int fi = -1;
         if (fmt == last_fmt) {
@@ -488,25 +531,39 @@ void parse_chunk(Chunk& c, char field, bool af_info, size_t n_samples, bool want
             return v;
         };
         if (multi) {
-            // genotype indices; the first missing call skips the record
-            // (src/vcf.rs:196-236)
+            // genotype indices (GT) or the most likely genotype (GL/PL); a
+            // missing call is 255.  The CLS estimator leaves out a record with
+            // a missing call, as the reference's GT reader does
+            // (src/vcf.rs:196-236: it stops at the first missing call, so a bad
+            // value after one is not an error there, and the record is
+            // dropped here); the ML estimator drops it for that sample's pairs.
             const size_t mb = c.mrows.size();
             c.mrows.resize(mb + n_samples);
             const char* s = col[9];
-            bool missing = false;
-            for (size_t k = 0; k < n_samples && !missing; k++) {
+            const int ng = n_bases * (n_bases + 1) / 2;
+            bool missing = false, bad_after_missing = false;
+            for (size_t k = 0; k < n_samples; k++) {
                 const std::string_view v = sample_value(s);
                 uint8_t g = 0;
-                if (!parse_gt_index(v, n_bases, g)) {
-                    fail("Value " + std::string(v) + " is not a valid GT");
+                const bool ok = field == 'T' ? parse_gt_index(v, n_bases, g) : parse_like_index(v, field, ng, g, c.msoft);
+                if (!ok) {
+                    if (field == 'T' && missing) {
+                        bad_after_missing = true;
+                        break;
+                    }
+                    fail("Value " + std::string(v) + " is not a valid " + std::string(key));
                     return;
                 }
-                missing = g == 255;
+                missing = missing || g == 255;
                 c.mrows[mb + k] = g;
             }
             if (missing) {
-                c.mrows.resize(mb);
                 c.incomplete++;
+                c.mincomplete++;
+            }
+            if (bad_after_missing) {
+                c.mrows.resize(mb);
+                c.multi_dropped++;
                 p = next;
                 continue;
             }
@@ -555,8 +612,13 @@ void parse_chunk(Chunk& c, char field, bool af_info, size_t n_samples, bool want
                 c.maf.insert(c.maf.end(), f, f + 4);
             }
             c.malleles.push_back((uint8_t)n_bases);
-            if (n_bases == 3) c.tri++;
-            else c.tetra++;
+            if (n_bases == 3) {
+                c.tri++;
+                if (!missing) c.tri_full++;
+            } else {
+                c.tetra++;
+                if (!missing) c.tetra_full++;
+            }
             c.mkept++;
             p = next;
             continue;
@@ -782,6 +844,11 @@ int read_vcf(const std::string& path, char field, bool af_info, int threads, Vcf
         out.maf.insert(out.maf.end(), c.maf.begin(), c.maf.end());
         out.tri += c.tri;
         out.tetra += c.tetra;
+        out.tri_full += c.tri_full;
+        out.tetra_full += c.tetra_full;
+        out.multi_incomplete += c.mincomplete;
+        out.multi_dropped += c.multi_dropped;
+        out.multi_soft += c.msoft;
     }
     if (af_info) {
         out.af.reserve((size_t)(2 * nv));

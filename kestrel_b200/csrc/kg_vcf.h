@@ -3,12 +3,12 @@
 // Reads biallelic SNP records of a VCF 4.x file (plain, gzip or bgzip) into
 // per-sample genotype codes (0 = 0/0, 1 = 0/1, 2 = 1/1, 3 = missing), with the
 // reference's record rules (src/vcf.rs:96-236): records whose REF or ALT is not
-// a single base are skipped, as are records with more than one ALT (with GT,
-// tri- and tetra-allelic records that every sample calls are kept apart as
-// genotype indices, as the reference's gt3 / gt4); GT calls
-// are diploid allele indices separated by '/' or '|' ('.' = missing); GL/PL
-// calls are three likelihoods reduced to the most likely genotype (a row that
-// is not one-hot to 25.5 log10 units is counted as soft).  BGZF blocks are
+// a single base are skipped; tri- and tetra-allelic records are kept apart as
+// genotype indices in the VCF order (the reference's gt3 / gt4 and gl3 / gl4),
+// 255 for a missing call; GT calls are diploid allele indices separated by '/'
+// or '|' ('.' = missing); GL/PL calls are likelihoods reduced to the most
+// likely genotype (a row that is not one-hot to 25.5 log10 units is counted as
+// soft).  BGZF blocks are
 // inflated in parallel; the text is cut at line boundaries and the chunks are
 // parsed in parallel, then merged in file order.
 #pragma once
@@ -45,12 +45,16 @@ struct VcfData {
     std::vector<double> af;         // with allele frequencies from INFO/AF: [REF, ALT] per kept site
     uint64_t total = 0, not_snp = 0, multi = 0, soft = 0;
     uint64_t incomplete = 0;        // SNP records with at least one missing call
-    // GT only: tri- and tetra-allelic records every sample calls
+    // tri- and tetra-allelic records
     int64_t n_multi = 0;
-    Bytes mcodes;                   // sample-major genotype indices (VCF order), mcodes[s * n_multi + v]
+    Bytes mcodes;                   // sample-major genotype indices (VCF order, 255 = missing), mcodes[s * n_multi + v]
     std::vector<uint8_t> malleles;  // allele count per record (3 or 4)
     std::vector<double> maf;        // with INFO/AF: 4 per record, [REF, ALT1, ALT2, ALT3 or 0]
-    uint64_t tri = 0, tetra = 0;
+    uint64_t tri = 0, tetra = 0;    // kept records by allele count
+    uint64_t tri_full = 0, tetra_full = 0;   // of those, the ones every sample calls
+    uint64_t multi_incomplete = 0;  // kept records with a missing call
+    uint64_t multi_dropped = 0;     // GT records dropped: a malformed call after a missing one
+    uint64_t multi_soft = 0;        // GL/PL likelihood rows of these records that are not one-hot
     // GL/PL with a soft row: the linear-scale likelihoods, sample-major
     // gl[(s * n_sites + v) * 3 + g] (NaN where missing); empty otherwise
     std::vector<double> gl;

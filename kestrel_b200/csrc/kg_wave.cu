@@ -158,9 +158,12 @@ __device__ inline void scatter_lockstep(const CohortDev& co, int64_t x, int64_t 
 // Each warp of the block takes a contiguous eighth of the pair's 1024-site
 // units: it counts its sites per shape, the block turns the counts into write
 // offsets (so the lists stay in site order), and each warp scatters its units.
+// The returned count n also takes the pair's jointly called tri- and
+// tetra-allelic sites (ML path), whose sums the multi-allelic kernel forms
+// from the samples' reduced genotypes without a list.
 template <class T>
 __device__ inline int64_t build_lists(const CohortDev& co, int64_t x, int64_t y, T* lists, char* wsm,
-                                      unsigned (*cnt)[5], int64_t* start, int64_t* count) {
+                                      unsigned (*cnt)[6], int64_t* start, int64_t* count) {
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int u0 = (int)((int64_t)co.n_units * w / ADMIT_WARPS);
     const int u1 = (int)((int64_t)co.n_units * (w + 1) / ADMIT_WARPS);
@@ -180,6 +183,16 @@ __device__ inline int64_t build_lists(const CohortDev& co, int64_t x, int64_t y,
             for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
             if (lane == 0) cnt[w][k] = v;
         }
+        unsigned cm = 0;
+        if (co.ml_nk > 0) {
+            const int nw = co.ml_stride >> 5;
+            const uint32_t* ox = co.ml_obs + x * nw;
+            const uint32_t* oy = co.ml_obs + y * nw;
+            for (int wd = w * 32 + lane; wd < nw; wd += ADMIT_WARPS * 32) cm += __popc(ox[wd] & oy[wd]);
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) cm += __shfl_xor_sync(0xffffffffu, cm, o);
+        }
+        if (lane == 0) cnt[w][5] = cm;
     }
     __syncthreads();
     int64_t off[5], st = 0, n = 0;
@@ -197,6 +210,7 @@ __device__ inline int64_t build_lists(const CohortDev& co, int64_t x, int64_t y,
         n += tot;
     }
     if (n > 0) scatter_lockstep<T>(co, x, y, lane, u0, u1, off, lists, wsm);
+    for (int v = 0; v < ADMIT_WARPS; v++) n += cnt[v][5];
     __syncthreads();   // cnt is reused by the block's next pair
     return n;
 }
@@ -204,7 +218,7 @@ __device__ inline int64_t build_lists(const CohortDev& co, int64_t x, int64_t y,
 extern "C" __global__ void __launch_bounds__(ADMIT_WARPS * 32, 4) wave_admit_kernel(WaveArgs A) {
     __shared__ int sh_e;
     __shared__ unsigned long long sh_k;
-    __shared__ unsigned cnt[ADMIT_WARPS][5];
+    __shared__ unsigned cnt[ADMIT_WARPS][6];
     extern __shared__ __align__(16) char smem[];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     char* wsm = smem + w * ADMIT_WARP_SMEM;
@@ -231,7 +245,7 @@ extern "C" __global__ void __launch_bounds__(ADMIT_WARPS * 32, 4) wave_admit_ker
                 S.status = SLOT_PASS;
             }
             __syncthreads();
-            if (w == 0) enqueue_pass<32>(A.pass_cur, A.tasks_cur, A.task_cap, A.wc_cur, s, S, lane, 0xffffffffu);
+            if (w == 0) enqueue_pass<32>(A.pass_cur, A.tasks_cur, A.task_cap, A.wc_cur, s, S, lane, 0xffffffffu, A.unit_elems);
             continue;
         }
         // a free slot takes pairs until one has jointly observed sites
@@ -271,7 +285,7 @@ extern "C" __global__ void __launch_bounds__(ADMIT_WARPS * 32, 4) wave_admit_ker
                 S.cohort = c;
                 for (int i = 0; i < 5; i++) { S.start[i] = start[i]; S.cnt[i] = count[i]; }
                 S.n = n;
-                units_from_counts(S);
+                units_from_counts(S, A.unit_elems);
                 S.lists64 = f64 ? 1 : 0;
                 S.fp64 = f64 ? 1 : 0;
                 S.near_count = 0;
@@ -294,7 +308,7 @@ extern "C" __global__ void __launch_bounds__(ADMIT_WARPS * 32, 4) wave_admit_ker
                 S.status = SLOT_PASS;
             }
             __syncthreads();
-            if (w == 0) enqueue_pass<32>(A.pass_cur, A.tasks_cur, A.task_cap, A.wc_cur, s, S, lane, 0xffffffffu);
+            if (w == 0) enqueue_pass<32>(A.pass_cur, A.tasks_cur, A.task_cap, A.wc_cur, s, S, lane, 0xffffffffu, A.unit_elems);
             break;
         }
     }
@@ -341,11 +355,35 @@ __device__ __forceinline__ float4 lds4(uint32_t a) {
     return v;
 }
 
+// Running FP32 sums of per-stage partials, one per half, with the rounding
+// errors of both halves gathered in c (an FP32 compensated sum on the FMA
+// pipe instead of an FP32 -> FP64 conversion and an FP64 add per partial).
+// fast2sum_acc is Fast2Sum, exact while |s| >= |p|: the gradient terms of a
+// shape are all positive, so s outgrows each partial once the first stage
+// (added to s = 0, exactly) is in.  two_sum_acc is TwoSum, exact for either
+// sign: the objective terms.
+__device__ __forceinline__ void fast2sum_acc(float2& s, float& c, float2 p) {
+    const float2 t = add2(s, p);
+    const float2 e = add2(fma2(t, dup2(-1.0f), s), p);   // (s - t) + p
+    c += e.x + e.y;
+    s = t;
+}
+__device__ __forceinline__ void two_sum_acc(float2& s, float& c, float2 p) {
+    const float2 m1 = dup2(-1.0f);
+    const float2 t = add2(s, p);
+    const float2 bp = fma2(s, m1, t);                     // t - s
+    const float2 ap = fma2(bp, m1, t);                    // t - bp
+    const float2 e = add2(fma2(ap, m1, s), fma2(bp, m1, p));   // (s - ap) + (p - bp)
+    c += e.x + e.y;
+    s = t;
+}
+
 // One shape's FP32 list from the ring.  Stage i holds float4 128 i .. 128 i +
 // 127; lane l takes 128 i + 32 j + l (j = 0..3): 16 sites, in packed pairs
-// (Shape32x2), whose FP32 gradient and objective partials go to FP64 after
-// every stage (8 sites per partial) and whose Hessian partials go every
-// HESS_STAGES stages (64 sites per partial).  Only the list's last stage can
+// (Shape32x2), whose FP32 gradient and objective partials (8 sites per half)
+// join compensated FP32 running sums after every stage, promoted to FP64 once
+// per unit, and whose Hessian partials go to FP64 every HESS_STAGES stages
+// (64 sites per partial).  Only the list's last stage can
 // be partly filled; the others run without bounds tests.  L and every stage
 // start are 16-byte aligned (list starts are multiples of four entries); a
 // stage's copy rounds its size up to 16 bytes, which stays inside the slot's
@@ -361,11 +399,12 @@ __device__ __forceinline__ bool stream32_ring(const float* __restrict__ L, int64
     constexpr int NG = E::NG, NH = E::NH, GOFF = E::GOFF, HOFF = E::HOFF;
     E ev;
     ev.load(K, DIFF);
-    double G[NG], F = 0.0;
+    float2 gs[NG], fs = dup2(0.f);
+    float gc[NG], fc = 0.f;
     double* H = Hs + lane;
     float2 h[NH];
 #pragma unroll
-    for (int i = 0; i < NG; i++) G[i] = 0.0;
+    for (int i = 0; i < NG; i++) { gs[i] = dup2(0.f); gc[i] = 0.f; }
 #pragma unroll
     for (int i = 0; i < NH; i++) { H[32 * i] = 0.0; h[i] = dup2(0.f); }
     const int64_t n4 = len >> 2;
@@ -394,9 +433,8 @@ __device__ __forceinline__ bool stream32_ring(const float* __restrict__ L, int64
                 if (lane + 32 * j < rem) ev.template site4<DIFF>(lds4(b + 512 * j), g, o, h, j & 1);
         }
 #pragma unroll
-        for (int j = 0; j < NG; j++) { G[j] += (double)g[j].x; G[j] += (double)g[j].y; }
-        F += (double)o.x;
-        F += (double)o.y;
+        for (int j = 0; j < NG; j++) fast2sum_acc(gs[j], gc[j], g[j]);
+        two_sum_acc(fs, fc, o);
         if (i % HESS_STAGES == HESS_STAGES - 1) {
 #pragma unroll
             for (int j = 0; j < NH; j++) { H[32 * j] += (double)(h[j].x + h[j].y); h[j] = dup2(0.f); }
@@ -418,7 +456,10 @@ __device__ __forceinline__ bool stream32_ring(const float* __restrict__ L, int64
         }
         return false;
     }
-    double Hf[NH];
+    double G[NG], Hf[NH];
+#pragma unroll
+    for (int j = 0; j < NG; j++) G[j] = ((double)gs[j].x + (double)gs[j].y) + (double)gc[j];
+    double F = ((double)fs.x + (double)fs.y) + (double)fc;
 #pragma unroll
     for (int j = 0; j < NH; j++) Hf[j] = H[32 * j] + (double)(h[j].x + h[j].y);
     if (lane < (int)(len & 3)) {
@@ -694,6 +735,107 @@ extern "C" __global__ void __launch_bounds__(128, PASS_MIN_BLOCKS) wave_pass_ker
     }
 }
 
+// ------------------------------------------------- tri- and tetra-allelic
+
+// The sums of the ML path's tri- and tetra-allelic sites for every slot with
+// a pending ML pass, in FP64: per kept site with both samples called, the row
+// L = m[g'x][g'y] from the site's table, d = eps + L.xt, and the terms L/d
+// (gradient), (L/d)(L/d)' (Hessian) and the objective term (log d, or for a
+// difference pass log(d / d_old) with d_old = eps + L.xc); a call that uses a
+// dropped allele gives the site a row of zeros (objective term log eps, or 0
+// in a difference pass).  Work units are (slot of the pass list, ML_CHUNK
+// sites), strided over the grid's warps; lanes stride over the unit's sites,
+// and the unit's sums go to ml_partial in a fixed order.
+extern "C" __global__ void __launch_bounds__(128, 2) wave_multi_kernel(WaveArgs A) {
+    if (A.clk->stop) return;   // a device loop past its last wave
+    const int lane = threadIdx.x & 31;
+    const PhaseEnd pe{&A.clk->end[1], lane == 0};   // timed as part of the pass phase
+    const int64_t warp = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const int64_t nwarps = (int64_t)gridDim.x * (blockDim.x >> 5);
+    const int64_t ntask = (int64_t)A.wc_cur->n_pass * A.ml_units;
+    const double eps = A.tune.epsilon;
+    for (int64_t t = warp; t < ntask; t += nwarps) {
+        const int s = A.pass_cur[t / A.ml_units];
+        const int u = (int)(t % A.ml_units);
+        const SlotState& S = A.slots[s];
+        const int kind = S.kind;
+        if (kind == PASS_CLS || kind == PASS_CLS64) continue;
+        const CohortDev& co = A.cohorts[S.cohort];
+        const int64_t v0 = (int64_t)u * ML_CHUNK;
+        if (v0 >= co.ml_nk) continue;
+        const int64_t v1 = min((int64_t)co.ml_nk, v0 + ML_CHUNK);
+        const bool diff = kind == PASS_FP32_DIFF;
+        double xt[9], xc[9];
+#pragma unroll
+        for (int k = 0; k < 9; k++) { xt[k] = S.xt[k]; xc[k] = S.xc[k]; }
+        const uint8_t* grx = co.ml_gr + S.x * co.ml_stride;
+        const uint8_t* gry = co.ml_gr + S.y * co.ml_stride;
+        double g[9], H[45], ob = 0.0;
+#pragma unroll
+        for (int k = 0; k < 9; k++) g[k] = 0.0;
+#pragma unroll
+        for (int k = 0; k < 45; k++) H[k] = 0.0;
+        for (int64_t v = v0 + lane; v < v1; v += 32) {
+            const int a = grx[v], b = gry[v];
+            if (a == ML_MISSING || b == ML_MISSING) continue;
+            if (a == ML_ZERO_ROW || b == ML_ZERO_ROW) {
+                if (!diff) ob += log(eps);
+                continue;
+            }
+            const int2 si = co.ml_site[v];
+            const double* R = co.ml_rows + 9 * ((int64_t)si.x + a * si.y + b);
+            double L[9];
+#pragma unroll
+            for (int k = 0; k < 9; k++) L[k] = __ldg(R + k);
+            double d = eps;
+#pragma unroll
+            for (int k = 0; k < 9; k++) d = fma(L[k], xt[k], d);
+            const double r = 1.0 / d;
+            double q[9];
+#pragma unroll
+            for (int k = 0; k < 9; k++) {
+                q[k] = L[k] * r;
+                g[k] += q[k];
+            }
+            int h = 0;
+#pragma unroll
+            for (int i = 0; i < 9; i++)
+#pragma unroll
+                for (int j = i; j < 9; j++, h++) H[h] = fma(q[i], q[j], H[h]);
+            if (!diff) {
+                ob += log(d);
+            } else {
+                double dc = eps, dl = 0.0;
+#pragma unroll
+                for (int k = 0; k < 9; k++) {
+                    dc = fma(L[k], xc[k], dc);
+                    dl = fma(L[k], xt[k] - xc[k], dl);
+                }
+                ob += log1p(dl / dc);
+            }
+        }
+        double* P = A.ml_partial + ((int64_t)s * A.ml_units + u) * ML_VALS;
+#pragma unroll
+        for (int k = 0; k < 9; k++) {
+            const double v = warp_sum(g[k]);
+            if (lane == 0) P[k] = v;
+        }
+#pragma unroll
+        for (int k = 0; k < 45; k++) {
+            const double v = warp_sum(H[k]);
+            if (lane == 0) P[9 + k] = v;
+        }
+        const double vo = warp_sum(ob);
+        if (lane == 0) P[54] = vo;
+    }
+}
+
+// Index of Hessian entry (i, j) in the upper triangle (row-major) of 9 x 9.
+__device__ __forceinline__ int upper9(int i, int j) {
+    const int a = i < j ? i : j, b = i < j ? j : i;
+    return a * 9 - a * (a - 1) / 2 + (b - a);
+}
+
 // ------------------------------------------------------------------ solve
 
 // (lane: the lane's index in its half-warp group)
@@ -809,7 +951,7 @@ __device__ inline void schedule_pass(const WaveArgs& A, SlotState& S, int s, int
     }
     if (lane == 0) S.status = SLOT_PASS;
     grp.sync();
-    enqueue_pass<16>(A.pass_next, A.tasks_next, A.task_cap, A.wc_next, s, S, lane, grp.mask);
+    enqueue_pass<16>(A.pass_next, A.tasks_next, A.task_cap, A.wc_next, s, S, lane, grp.mask, A.unit_elems);
 }
 
 // Two slots per warp, one per half-warp (the row-parallel solver needs nine
@@ -873,11 +1015,31 @@ extern "C" __global__ void __launch_bounds__(128, 4) wave_solve_kernel(WaveArgs 
         grp.sync();
         corr = mom_s[NMOM + 1];
     }
+    // the pair's tri- and tetra-allelic sums (ML path), units in order: lane
+    // r < 9 takes gradient r and Hessian row r, lane 9 the objective term
+    double ml_obj = 0.0, ml_g = 0.0, ml_h[9];
+#pragma unroll
+    for (int j = 0; j < 9; j++) ml_h[j] = 0.0;
+    if (A.ml_units > 0) {
+        const int nml = (A.cohorts[S.cohort].ml_nk + ML_CHUNK - 1) / ML_CHUNK;
+        const double* P = A.ml_partial + (int64_t)s * A.ml_units * ML_VALS;
+        for (int u = 0; u < nml; u++) {
+            const double* Pu = P + (int64_t)u * ML_VALS;
+            if (lane < 9) {
+                ml_g += Pu[lane];
+#pragma unroll
+                for (int j = 0; j < 9; j++) ml_h[j] += Pu[9 + upper9(lane, j)];
+            } else if (lane == 9) {
+                ml_obj += Pu[54];
+            }
+        }
+        ml_obj = grp.bcast(ml_obj, 9);
+    }
     const double obj = mom_s[NMOM];
     double ft;
-    if (kind == PASS_FP64) ft = -obj / n;
-    else if (kind == PASS_FP32_DIRECT) ft = -(obj * 0.69314718055994530942 + corr) / n;
-    else ft = S.f - obj / n;
+    if (kind == PASS_FP64) ft = -(obj + ml_obj) / n;
+    else if (kind == PASS_FP32_DIRECT) ft = -((obj * 0.69314718055994530942 + corr) + ml_obj) / n;
+    else ft = S.f - (obj + ml_obj) / n;
     double gt[9], Ht[9];
     {
         double Sg = 0.0;
@@ -885,8 +1047,9 @@ extern "C" __global__ void __launch_bounds__(128, 4) wave_solve_kernel(WaveArgs 
         for (int j = 0; j < 9; j++) Ht[j] = 0.0;
         if (lane < 9) {
             rebuild_row(mom_s, lane, Sg, Ht);
+            Sg += ml_g;
 #pragma unroll
-            for (int j = 0; j < 9; j++) Ht[j] = Ht[j] / n;
+            for (int j = 0; j < 9; j++) Ht[j] = (Ht[j] + ml_h[j]) / n;
         }
         gather9(grp, -Sg / n, gt);
     }
@@ -1047,7 +1210,7 @@ struct WaveEngine::Impl {
     RunConfig cfg;
     int64_t n_slots = 0, list_cap = 0, task_cap = 0;
     int max_units = 0, max_jobs = 0;
-    int pass_blocks = 0, admit_blocks = 0, solve_blocks = 0;
+    int pass_blocks = 0, admit_blocks = 0, solve_blocks = 0, multi_blocks = 0;
     WaveArgs A{};
     WaveCounts* wc = nullptr;
     int* admit_task = nullptr;
@@ -1080,7 +1243,8 @@ struct WaveEngine::Impl {
     // what open() was last called with, and the buffers its graphs point into
     bool opened = false;
     int64_t key_list_cap = 0, key_want = 0, key_expected = 0;
-    int key_max_jobs = 0, key_precision = 0, key_bps = 0, key_dev = -1;
+    int key_max_jobs = 0, key_precision = 0, key_bps = 0, key_dev = -1, key_ml_units = 0, key_unit = 0,
+        key_divisor = 0;
     uint64_t key_iterations = 0;
     cudaStream_t key_st = nullptr;
     std::vector<void*> key_bufs;
@@ -1119,10 +1283,13 @@ int WaveEngine::open(Workspace& ws, cudaStream_t st, const RunConfig& cfg, int64
     const bool same_call = E.opened && E.key_list_cap == list_cap && E.key_want == cfg.slots &&
                            E.key_expected == expected_pairs && E.key_max_jobs == E.max_jobs &&
                            E.key_precision == cfg.precision && E.key_bps == cfg.pass_blocks_per_sm &&
-                           E.key_iterations == cfg.iterations && E.key_dev == dev && E.key_st == st;
-    // work units: per shape at most ceil(list_cap / UNIT_ELEMS), over the five
+                           E.key_iterations == cfg.iterations && E.key_dev == dev && E.key_st == st &&
+                           E.key_ml_units == cfg.ml_units && E.key_unit == cfg.unit_elems &&
+                           E.key_divisor == cfg.slot_divisor;
+    // work units: per shape at most ceil(list_cap / unit), over the five
     // shapes at most that + 5
-    const int64_t shape_units = (list_cap + UNIT_ELEMS - 1) / UNIT_ELEMS;
+    const int unit = cfg.unit_elems > 0 ? cfg.unit_elems : UNIT_ELEMS;
+    const int64_t shape_units = (list_cap + unit - 1) / unit;
     E.max_units = (int)shape_units + 5;
     // slots: as many as the work and the memory allow
     const size_t per_slot = sizeof(double) * (size_t)list_cap + sizeof(double) * E.max_units * UNIT_VALS +
@@ -1131,7 +1298,8 @@ int WaveEngine::open(Workspace& ws, cudaStream_t st, const RunConfig& cfg, int64
     // by default an eighth of the job's pairs, between 4,096 and 32,768: enough
     // to fill the waves, few enough that the last waves drain quickly
     const int64_t want = cfg.slots > 0 ? cfg.slots
-                                       : std::min<int64_t>(32768, std::max<int64_t>(4096, expected_pairs / 8));
+                                       : std::min<int64_t>(32768, std::max<int64_t>(
+                                                                      4096, expected_pairs / std::max(1, cfg.slot_divisor)));
     if (!same_call) {
         KG_WAVE_TRY(cudaMemGetInfo(&fr, &tot));
         const int64_t by_mem = (int64_t)((fr / 2) / per_slot);
@@ -1142,6 +1310,8 @@ int WaveEngine::open(Workspace& ws, cudaStream_t st, const RunConfig& cfg, int64
     // device buffers (grown and reused through the workspace)
     KG_WAVE_TRY((cudaError_t)ws.scratch.reserve(sizeof(double) * (size_t)list_cap * n_slots));
     KG_WAVE_TRY((cudaError_t)ws.partial.reserve(sizeof(double) * (size_t)E.max_units * UNIT_VALS * n_slots));
+    KG_WAVE_TRY((cudaError_t)ws.ml_partial.reserve(sizeof(double) * (size_t)std::max(1, cfg.ml_units) * ML_VALS *
+                                                   (size_t)(cfg.ml_units > 0 ? n_slots : 1)));
     KG_WAVE_TRY((cudaError_t)ws.slots.reserve(sizeof(SlotState) * n_slots));
     KG_WAVE_TRY((cudaError_t)ws.lists_a.reserve(sizeof(int) * 2 * n_slots));   // pass lists
     KG_WAVE_TRY((cudaError_t)ws.lists_b.reserve(sizeof(int) * 2 * n_slots));   // free lists
@@ -1171,8 +1341,9 @@ int WaveEngine::open(Workspace& ws, cudaStream_t st, const RunConfig& cfg, int64
     E.h_done = E.h_q + 1;
     E.live_h->total_pairs = 0;
     E.live_h->n_cohorts = 0;
-    const std::vector<void*> bufs{ws.scratch.p, ws.partial.p, ws.slots.p, ws.lists_a.p, ws.lists_b.p, ws.tasks.p,
-                                  ws.counts.p,  ws.queue.p,   ws.counters.p, ws.table.p, ws.done.p, ws.host.p};
+    const std::vector<void*> bufs{ws.scratch.p, ws.partial.p, ws.slots.p,    ws.lists_a.p, ws.lists_b.p,
+                                  ws.tasks.p,   ws.counts.p,  ws.queue.p,    ws.counters.p, ws.table.p,
+                                  ws.done.p,    ws.host.p,    ws.ml_partial.p};
     const bool reuse = same_call && bufs == E.key_bufs;
     // the job state of a fresh engine
     E.table.clear();
@@ -1218,6 +1389,12 @@ int WaveEngine::open(Workspace& ws, cudaStream_t st, const RunConfig& cfg, int64
     }
     E.admit_blocks = ws.sm_count * aocc;
     E.solve_blocks = (int)((n_slots + 2 * WAVE_WPB - 1) / (2 * WAVE_WPB));   // two slots per warp
+    E.multi_blocks = 0;
+    if (cfg.ml_units > 0) {
+        int mocc = 0;
+        KG_WAVE_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&mocc, wave_multi_kernel, 128, 0));
+        E.multi_blocks = ws.sm_count * std::max(1, mocc);
+    }
     WaveArgs& A = E.A;
     A.cohorts = ws.table.as<CohortDev>();
     A.live = E.live_d;
@@ -1236,6 +1413,9 @@ int WaveEngine::open(Workspace& ws, cudaStream_t st, const RunConfig& cfg, int64
     A.counters = ws.counters.as<RunCounters>();
     A.cohort_done = ws.done.as<unsigned long long>();
     A.clk = E.clk;
+    A.ml_partial = ws.ml_partial.as<double>();
+    A.ml_units = cfg.ml_units;
+    A.unit_elems = unit;
     E.drop_loop();
     // One wave (counter resets, admit, pass, solve, read-back) captured as a
     // CUDA graph per parity of the current/next lists, then replayed: one
@@ -1279,6 +1459,7 @@ int WaveEngine::open(Workspace& ws, cudaStream_t st, const RunConfig& cfg, int64
         }
         if (ce == cudaSuccess) {
             wave_pass_kernel<<<E.pass_blocks, 128, WAVE_WPB * PASS_WARP_SMEM, st>>>(Aw);
+            if (E.multi_blocks) wave_multi_kernel<<<E.multi_blocks, 128, 0, st>>>(Aw);
             ce = cudaEventRecordWithFlags(E.ev[par][2], st, cudaEventRecordExternal);
         }
         if (ce == cudaSuccess) {
@@ -1306,6 +1487,9 @@ int WaveEngine::open(Workspace& ws, cudaStream_t st, const RunConfig& cfg, int64
     E.key_iterations = cfg.iterations;
     E.key_dev = dev;
     E.key_st = st;
+    E.key_ml_units = cfg.ml_units;
+    E.key_unit = cfg.unit_elems;
+    E.key_divisor = cfg.slot_divisor;
     E.key_bufs = bufs;
     return KG_OK;
 }
@@ -1350,7 +1534,7 @@ int WaveEngine::wave(std::vector<int>& finished, std::string& err) {
     const cudaStream_t st = E.st;
     KG_WAVE_TRY(cudaGraphLaunch(E.x[E.cur], st));
     KG_WAVE_TRY(cudaStreamSynchronize(st));
-    E.launches += 3;
+    E.launches += E.multi_blocks ? 4 : 3;
     E.waves++;
     for (size_t k = 0; k < E.table.size(); k++)
         if (!E.reported[k] && E.h_done[k] >= (unsigned long long)E.table[k].n_pairs) {
@@ -1392,6 +1576,7 @@ int WaveEngine::run_until_idle(unsigned long long max_waves, std::string& err) {
             const WaveArgs& Aw = E.args[E.cur ^ k];
             wave_admit_kernel<<<E.admit_blocks, ADMIT_WARPS * 32, ADMIT_WARPS * ADMIT_WARP_SMEM, st>>>(Aw);
             wave_pass_kernel<<<E.pass_blocks, 128, WAVE_WPB * PASS_WARP_SMEM, st>>>(Aw);
+            if (E.multi_blocks) wave_multi_kernel<<<E.multi_blocks, 128, 0, st>>>(Aw);
             wave_solve_kernel<<<E.solve_blocks, 128, WAVE_WPB * WARP_SMEM, st>>>(Aw);
             wave_end_kernel<<<1, 32, 0, st>>>(Aw, k, h, max_waves);
         }
@@ -1420,7 +1605,7 @@ int WaveEngine::run_until_idle(unsigned long long max_waves, std::string& err) {
         E.total += (double)c.acc[i] * 1e-6;
     }
     E.waves += c.waves;
-    E.launches += 8 * c.iters;
+    E.launches += (E.multi_blocks ? 10 : 8) * c.iters;
     E.cur ^= (int)(c.waves & 1);
     E.last_q = *E.h_q;
     // the next wave's counts, as a host wave would have read them; the clock
@@ -1501,10 +1686,13 @@ int WaveEngine::stats(kg_run_stats& stats, std::string& err) {
 }
 
 // All jobs of one call through one engine, waves until every pair is done.
-int run_waves(const std::vector<PairJob>& jobs, const RunConfig& cfg, Workspace& ws,
+int run_waves(const std::vector<PairJob>& jobs, const RunConfig& cfg_in, Workspace& ws,
               cudaStream_t st, kg_run_stats& stats, std::string& err,
               const std::vector<CohortDev>& table, int64_t total_pairs, int64_t list_cap) {
     (void)jobs;
+    RunConfig cfg = cfg_in;
+    cfg.ml_units = 0;
+    for (const CohortDev& d : table) cfg.ml_units = std::max(cfg.ml_units, (d.ml_nk + ML_CHUNK - 1) / ML_CHUNK);
     if (!ws.engine) ws.engine = std::make_shared<WaveEngine>();
     WaveEngine& eng = *ws.engine;
     int r = eng.open(ws, st, cfg, list_cap, total_pairs, (int)table.size(), err);

@@ -5,8 +5,8 @@
 //   admit : free slots take the next pairs from the device work queue (an atomic
 //           counter over all cohorts' pairs) and build their shape lists;
 //   pass  : a persistent kernel over work units (slot, shape, chunk of
-//           UNIT_ELEMS list entries) streams the lists at each slot's pending
-//           point and writes per-unit partial moments;
+//           unit_elems list entries, UNIT_ELEMS by default) streams the lists at
+//           each slot's pending point and writes per-unit partial moments;
 //   solve : one warp per slot sums its units' partials in a fixed order, rebuilds
 //           f, g, H and advances the slot's SQP: KKT test, condition estimate,
 //           simplex QP, Armijo line search.  Converged slots write their output
@@ -19,7 +19,7 @@
 
 namespace kg {
 
-constexpr int UNIT_ELEMS = 16384;  // list entries per pass work unit
+constexpr int UNIT_ELEMS = 16384;  // list entries per pass work unit (the default; RunConfig::unit_elems)
 constexpr int UNIT_VALS = 14;      // partial values per unit: <= 13 moments + objective
 
 enum : int { SLOT_FREE = 0, SLOT_PASS = 1, SLOT_RESORT = 2 };
@@ -127,7 +127,16 @@ struct WaveArgs {
     RunCounters* counters;
     unsigned long long* cohort_done;   // finished pairs per cohort
     WaveClock* clk;
+    double* ml_partial;            // per slot: ml_units * ML_VALS sums of its tri-/tetra-allelic sites
+    int ml_units;                  // their work units per slot (0: no cohort has such sites)
+    int unit_elems;                // list entries per pass work unit
 };
+
+// Work units of the ML path's tri- and tetra-allelic sites: ML_CHUNK kept
+// sites each; per unit 9 gradient sums, the 45 Hessian sums of the upper
+// triangle (row-major) and the objective term.
+constexpr int ML_CHUNK = 2048;
+constexpr int ML_VALS = 56;
 
 __device__ __forceinline__ int shape_ng(int s) { return s == 0 ? 4 : s == 3 ? 4 : s == 4 ? 2 : 3; }
 __device__ __forceinline__ int shape_nh(int s) { return s == 0 ? 7 : s == 3 ? 9 : s == 4 ? 3 : 5; }
@@ -154,10 +163,9 @@ __device__ inline void set_coefficients(SlotState& S, int kind) {
     S.kind = kind;
 }
 
-__device__ inline void units_from_counts(SlotState& S) {
+__device__ inline void units_from_counts(SlotState& S, int unit) {
     S.ustart[0] = 0;
-    for (int s = 0; s < 5; s++)
-        S.ustart[s + 1] = S.ustart[s] + (int)((S.cnt[s] + UNIT_ELEMS - 1) / UNIT_ELEMS);
+    for (int s = 0; s < 5; s++) S.ustart[s + 1] = S.ustart[s] + (int)((S.cnt[s] + unit - 1) / unit);
 }
 
 __device__ __forceinline__ void decode_pair(const WaveArgs& A, int64_t k, int& c, int64_t& j,
@@ -202,7 +210,7 @@ __device__ __forceinline__ int4 make_task(int s, int u, int64_t off, int64_t len
 // lanes (a warp or a half-warp, given by mask); lane is the index among them.
 template <int W>
 __device__ inline void enqueue_pass(int* pass, int4* tasks, int64_t task_cap, WaveCounts* wc, int s,
-                                    const SlotState& S, int lane, unsigned mask) {
+                                    const SlotState& S, int lane, unsigned mask, int unit) {
 #pragma unroll 1
     for (int sh = 0; sh < 5; sh++) {
         const int u0 = S.ustart[sh], nu = S.ustart[sh + 1] - u0;
@@ -213,8 +221,8 @@ __device__ inline void enqueue_pass(int* pass, int4* tasks, int64_t task_cap, Wa
         const int64_t st = S.start[sh], cnt = S.cnt[sh];
         const int kind = S.kind;
         for (int i = lane; i < nu; i += W) {
-            const int64_t c0 = (int64_t)i * UNIT_ELEMS;
-            tasks[sh * task_cap + base + i] = make_task(s, u0 + i, st + c0, min((int64_t)UNIT_ELEMS, cnt - c0), kind);
+            const int64_t c0 = (int64_t)i * unit;
+            tasks[sh * task_cap + base + i] = make_task(s, u0 + i, st + c0, min((int64_t)unit, cnt - c0), kind);
         }
     }
     if (lane == 0) pass[atomicAdd(&wc->n_pass, 1)] = s;

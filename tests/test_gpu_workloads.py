@@ -198,19 +198,28 @@ def test_cli_cls_estimator_matches_oracle(oracle):
     print(check_values(*_tsv_values(rows), ref))
 
 
-def test_autotune_and_launch_shape_leave_results_unchanged():
-    co = synth.make_cohort(48, 4000, seed=51)
+def test_autotune_and_launch_shape_leave_results_unchanged(oracle):
+    co = synth.make_cohort(300, 4000, seed=51)
     with kb.Estimator() as est:
         est.load(co.codes)
         base = est.relatedness()
         slots, bps = est.autotune()
-        assert slots == 0 and bps in (2, 3, 4)   # the candidates kg_autotune times
+        shape = est.launch()
+        # the candidates kg_autotune times (0 = the defaults)
+        assert slots == 0 and bps in (0, 4, 3)
+        assert shape["unit_entries"] in (0, 8192, 4096) and shape["slot_divisor"] in (8, 4, 16)
         tuned = est.relatedness()
+        est.set_work_unit(0)
         est.set_launch(64, 2)      # few slots in flight: many more waves
         small = est.relatedness()
         assert est.run_stats()["slots"] == 64
-    assert _bitwise_equal(base, tuned) and _bitwise_equal(base, small)
-
+        est.set_work_unit(4096)    # other partial-sum groups: within the bar
+        units = est.relatedness()
+    assert _bitwise_equal(base, small)
+    if shape["unit_entries"] == 0:
+        assert _bitwise_equal(base, tuned)
+    compare(tuned, base)
+    compare(units, base)
 
 def test_cli_gt_default_drops_records_with_missing_calls(oracle):
     co = synth.make_cohort(24, 4000, seed=45, missing=0.002, name="cli-cls-miss")

@@ -49,12 +49,13 @@ def test_cli_counts_skipped_records(built):
         assert "Skipped 1 sites that were not SNPs" in out.stderr
     # GT runs CLS by default, on the records every sample calls (as the
     # reference's GT reader keeps), the tri-allelic one included; ML keeps the
-    # record with a missing call and skips the tri-allelic one
+    # record with a missing call and the tri-allelic one (the GL/PL reader's
+    # counts)
     assert "Skipped 1 sites with missing data" in r.stderr
     assert "Found 2 di-allelic sites" in r.stderr
     assert "Found 1 tri-allelic sites" in r.stderr and "Found 0 tetra-allelic sites" in r.stderr
     assert "Found 3 di-allelic sites" in r_ml.stderr and "missing data" not in r_ml.stderr
-    assert "Skipped 1 tri- or tetra-allelic sites" in r_ml.stderr
+    assert "Found 1 tri-allelic sites" in r_ml.stderr
     if not torch.cuda.is_available():
         assert r.returncode != 0
 

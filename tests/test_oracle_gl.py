@@ -135,3 +135,52 @@ def test_singleton_at_the_default_maf_sits_on_the_cut(oracle, cohort):
     _, af = oracle.gl_relatedness(one_hot(codes[:, :50]))
     n = codes.shape[0]
     assert af[0, 1] == 0.0 or abs(af[0, 1] - 1 / (2 * n)) < 1e-6
+
+
+def test_device_allele_fit_matches_the_oracle(oracle, tmp_path):
+    """The GPU's per-site frequency fit for 2-4 alleles (kg_alleleN.cuh, the
+    class-count form of the reference's allele SQP on one-hot likelihoods),
+    built for the host, against the oracle's fit of the same calls given as
+    per-sample one-hot rows: equal to 1e-7 (the two sum in different orders,
+    so the SQP can stop an iterate apart within its KKT tolerance of 1e-8),
+    with the same frequencies cut to zero by maf."""
+    import os
+    import shutil
+    import subprocess
+    nvcc = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+    if not os.path.exists(nvcc):
+        pytest.skip("nvcc not available")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    exe = str(tmp_path / "allele_fit_host")
+    subprocess.run([nvcc, "-O2", "-std=c++17", "-I", os.path.join(root, "kestrel_b200", "csrc"),
+                    os.path.join(root, "tests", "host", "allele_fit_host.cu"), "-o", exe], check=True)
+    rng = np.random.default_rng(5)
+    lines, cases = [], []
+    for a in (2, 3, 4):
+        ng = a * (a + 1) // 2
+        for k in range(60):
+            n = int(rng.integers(5, 200))
+            f = rng.dirichlet(np.full(a, 0.6))
+            al = rng.choice(a, size=(n, 2), p=f)
+            i, j = al.min(1), al.max(1)
+            g = j * (j + 1) // 2 + i
+            if k % 7 == 0:
+                g[rng.random(n) < 0.2] = ng                       # missing
+            cnt = np.bincount(g[g < ng], minlength=ng)
+            maf = 1.0 / (2 * n) if k % 2 else 0.02
+            lines.append(f"{a} " + " ".join(str(c) for c in cnt) + f" 100 {maf!r}")
+            gl = np.zeros((1, n, ng))
+            for c in range(ng):
+                gl[0, :, c] = g == c
+            gl[0, g == ng] = np.nan
+            cases.append((a, gl, maf))
+    out = subprocess.run([exe], input=f"{len(lines)}\n" + "\n".join(lines) + "\n", capture_output=True,
+                         text=True, check=True).stdout.split("\n")
+    worst = 0.0
+    for (a, gl, maf), line in zip(cases, out):
+        got = np.array([float(v) for v in line.split()])[:a]
+        want = oracle.gl_allele_frequencies(gl, maf=maf)[0, :a]
+        assert np.array_equal(got > 0, want > 0), (a, got, want)
+        worst = max(worst, float(np.abs(got - want).max()))
+        assert np.abs(got - want).max() <= 1e-7, (a, got, want)
+    print("largest frequency difference", worst)

@@ -43,8 +43,6 @@ def py_parse(text, field="GT", af_info=False):
             continue
         if nb > 2:
             multi += 1
-            if field != "GT":
-                continue
         fmt = cols[8].split(":")
         fi = max([i for i, f in enumerate(fmt) if f == key], default=-1)
         if fi < 0:
@@ -54,19 +52,40 @@ def py_parse(text, field="GT", af_info=False):
             sub = cols[9 + s].split(":")
             return sub[fi] if fi < len(sub) else "."
         if nb > 2:
-            row, missing = [], False
+            # every record kept, a missing call as 255; GT: a malformed call
+            # after a missing one drops the record (the reference's reader
+            # stops at the missing call); GL/PL: the most likely genotype
+            row, missing, dropped = [], False, False
+            ng = nb * (nb + 1) // 2
             for s in range(len(samples)):
                 v = value(s)
-                parts = v.replace("|", "/").split("/")
-                if "." in parts and len(parts) <= 2:
-                    missing = True
-                    break
-                if len(parts) != 2 or not all(p.isdigit() and int(p) < nb for p in parts):
-                    raise ValueError(f"Value {v} is not a valid GT")
-                i, j = sorted(int(p) for p in parts)
-                row.append(j * (j + 1) // 2 + i)
+                if field == "GT":
+                    parts = v.replace("|", "/").split("/")
+                    if "." in parts and len(parts) <= 2:
+                        missing = True
+                        row.append(255)
+                        continue
+                    if len(parts) != 2 or not all(p.isdigit() and int(p) < nb for p in parts):
+                        if missing:
+                            dropped = True
+                            break
+                        raise ValueError(f"Value {v} is not a valid GT")
+                    i, j = sorted(int(p) for p in parts)
+                    row.append(j * (j + 1) // 2 + i)
+                else:
+                    parts = v.split(",")
+                    if v != "." and len(parts) != ng:
+                        raise ValueError(f"Value {v} is not a valid {key}")
+                    if v == "." or "." in parts:
+                        missing = True
+                        row.append(255)
+                        continue
+                    val = [float(p) for p in parts]
+                    ll = [-x / 10.0 for x in val] if field == "PL" else val
+                    row.append(int(np.argmax(ll)))
             if missing:
                 with_missing += 1
+            if dropped:
                 continue
             if af_info:
                 vals = None
@@ -372,3 +391,45 @@ def test_soft_likelihoods_are_read_as_the_reference_makes_them():
     assert np.allclose(got, want, rtol=1e-15, atol=0, equal_nan=True)
     want_gl = py_likelihoods(gl_text, "GL")
     assert np.allclose(got_gl, want_gl, rtol=1e-15, atol=0, equal_nan=True)
+
+
+def test_likelihood_fields_keep_multiallelic_records():
+    """GL/PL tri- and tetra-allelic records are kept (the ML estimator's input):
+    each call becomes its most likely genotype in the VCF order, a missing value
+    or entry 255; rows that are not one-hot count apart from the biallelic ones."""
+    rng = np.random.default_rng(8)
+    n = 6
+    lines = ["##fileformat=VCFv4.2", "#CHROM\tPOS\tID\tREF\tALT\tQUAL\tFILTER\tINFO\tFORMAT\t" +
+             "\t".join(f"S{i}" for i in range(n))]
+    for v in range(40):
+        nb = int(rng.integers(2, 5))
+        ng = nb * (nb + 1) // 2
+        alt = ",".join("CGT"[:nb - 1])
+        calls = []
+        for s in range(n):
+            r = rng.random()
+            if r < 0.1:
+                calls.append(".")
+            elif r < 0.15:
+                calls.append(",".join("." if k == 1 else "0" for k in range(ng)))
+            else:
+                pl = np.full(ng, 255)
+                pl[int(rng.integers(0, ng))] = 0
+                if r > 0.9:
+                    pl[int(rng.integers(0, ng))] = 7        # not one-hot
+                calls.append(",".join(str(int(x)) for x in pl))
+        lines.append(f"3\t{v + 1}\t.\tA\t{alt}\t.\tPASS\t.\tPL\t" + "\t".join(calls))
+    text = "\n".join(lines) + "\n"
+    ref = py_parse(text, "PL")
+    with tempfile.TemporaryDirectory() as td:
+        p = os.path.join(td, "pl.vcf")
+        open(p, "w").write(text)
+        for threads in (1, 4):
+            codes, _, _, counts, multi = kb.read_vcf(p, "PL", threads=threads, multiallelic=True)
+            assert np.array_equal(codes, ref[0])
+            for a, b in zip(multi[:2], ref[4][:2]):
+                assert np.array_equal(a, b)
+            assert counts["tri_allelic"] == ref[3]["tri_allelic"] > 0
+            assert counts["tetra_allelic"] == ref[3]["tetra_allelic"] > 0
+            assert counts["with_missing"] == ref[3]["with_missing"]
+    assert np.any(ref[4][0] == 255)
