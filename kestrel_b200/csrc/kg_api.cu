@@ -693,8 +693,9 @@ int kg_relatedness_gl(kg_ctx* c, int64_t num_samples, uint64_t iterations, doubl
         cudaEventCreate(&ev1);
         cudaEventRecord(ev0, c->stream);
         int64_t kept = 0;
+        uint64_t sc[5] = {0, 0, 0, 0, 0};
         st = kg::soft_relatedness(c->soft_gl, c->soft_ns, c->soft_nv, ns, iterations, std::isnan(maf) ? -1.0 : maf,
-                                  c->dout.as<kg_output>(), c->stream, err, &kept);
+                                  c->dout.as<kg_output>(), c->stream, err, &kept, c->precision, sc);
         cudaEventRecord(ev1, c->stream);
         int st2 = copy_rows_out(c, c->dout, np, out, c->stream);
         kg_run_stats stats{};
@@ -702,7 +703,16 @@ int kg_relatedness_gl(kg_ctx* c, int64_t num_samples, uint64_t iterations, doubl
         if (cudaEventElapsedTime(&dms, ev0, ev1) == cudaSuccess) stats.device_ms = dms;
         cudaEventDestroy(ev0);
         cudaEventDestroy(ev1);
-        stats.launches = 2;   // frequencies, pairs
+        stats.launches = c->precision == KG_PREC_FP64 ? 2 : 3;   // frequencies, (FP32 packing,) pairs
+        stats.gh_passes = sc[0];
+        stats.obj_passes = sc[0];
+        stats.fp64_passes = sc[1];
+        stats.fp64_pairs = sc[2];
+        stats.work_units = sc[3];
+        // executed FP32 arithmetic at 204 FLOP per pair-site (FMA = 2): the
+        // row from the nine likelihood products, d, the gradient and the 45
+        // Hessian terms, the objective term
+        stats.flops_fp32 = (sc[3] - sc[4]) * 204ull;
         stats.sites_used[0] = (uint64_t)kept;
         stats.sites_discarded = (uint64_t)(c->soft_nv - kept);
         stats.total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();

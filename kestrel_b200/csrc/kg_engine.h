@@ -134,8 +134,12 @@ int prepare_ml_multi(Cohort& c, bool have_af, double maf, uint64_t iterations, c
 // is double [n_samples][n_sites][3] on the device (linear scale, NaN =
 // missing); rows of the first ns samples into d_out (device), the reference's
 // order.  maf < 0: 1 / (2 n_samples).
+// precision: KG_PREC_FP32C (FP32 evaluations, FP64 for pairs that need it) or
+// KG_PREC_FP64; counters (5, optional): grad-Hessian evaluations, those in
+// FP64, pairs escalated to FP64, pair-sites evaluated, those in FP64.
 int soft_relatedness(const DevBuf& gl, int64_t n_samples, int64_t n_sites, int64_t ns, uint64_t iterations,
-                     double maf, kg_output* d_out, cudaStream_t st, std::string& err, int64_t* n_kept = nullptr);
+                     double maf, kg_output* d_out, cudaStream_t st, std::string& err, int64_t* n_kept = nullptr,
+                     int precision = KG_PREC_FP32C, uint64_t* counters = nullptr);
 
 // Unpacks the VCF reader's 2-bit codes + observed mask into device byte codes
 // (d2, dm: the packed rows' device copies, kept for the next load).

@@ -5,13 +5,27 @@
 // L_s = sum over (gx, gy) of GLx(gx) GLy(gy) m(gx, gy) of its sites.
 //
 // Layout: likelihoods double [sample][site][3] (0/0, 0/1, 1/1; linear scale;
-// a NaN marks a missing sample).  First form: a warp per pair, lanes over the
-// kept sites, everything in FP64; a lane's 45 Hessian sums live in shared
-// memory.  Each pass reads both samples' likelihoods, so this form is bound by
-// those reads, not by the arithmetic.
+// a NaN marks a missing sample) as loaded; the kept sites' likelihoods are
+// also packed as FP32 [sample][kept site][3] (all three NaN when missing).
+//
+// A warp per pair, lanes over the kept sites; the SQP itself is FP64.  Its
+// evaluations (f, g and H at a point) run in one of two forms:
+//   * FP32 (the default, KG_PREC_FP32C): from the FP32 likelihoods, which stay
+//     L2-resident for cohorts of a few hundred samples, each site's row L is
+//     formed from the pair's nine likelihood products in closed form; d =
+//     eps + L.x with the FP32 hi parts of x, the sums in FP32 promoted to FP64
+//     (gradient and objective every 8 sites, Hessian every 32 into the lane's
+//     shared memory), and the lo parts of x restored to first order in FP64;
+//     near convergence the objective change is summed as log(d / d_old), as
+//     on the hard-call path.  A pair whose FP32 condition estimate exceeds
+//     COND_RECHECK, or whose KKT residual stalls below 1e-6 three times, is
+//     re-evaluated in FP64 and stays FP64 (the hard-call path's rule).
+//   * FP64 (KG_PREC_FP64, and escalated pairs): from the FP64 likelihoods,
+//     each row the sum over the nine genotype pairs of GLx GLy m(gx, gy).
 #include <cuda_runtime.h>
 #include <math_constants.h>
 
+#include <algorithm>
 #include <string>
 #include <vector>
 
@@ -60,7 +74,7 @@ constexpr int SOFT_WARPS = 4;
 // f, g and this lane's Hessian row at x over the pair's rows (-(1/n) sum log(eps
 // + L.x), -(1/n) sum L r, (1/n) sum L L' r^2, r = 1/(eps + L.x)); n = rows
 // without a NaN.  hs: the lane's 45 upper-triangle sums in shared memory.
-__device__ inline int64_t soft_evaluate(const double* __restrict__ gl, int64_t n_sites, const int32_t* __restrict__ kept,
+__device__ __noinline__ int64_t soft_evaluate(const double* __restrict__ gl, int64_t n_sites, const int32_t* __restrict__ kept,
                                         const double* __restrict__ kp, const double* __restrict__ kq, int64_t nk,
                                         int64_t x, int64_t y, const double* xv, double eps, int lane, double* hs,
                                         PairEval& ev) {
@@ -140,16 +154,180 @@ __device__ inline int64_t soft_evaluate(const double* __restrict__ gl, int64_t n
     return n;
 }
 
+// Packs the kept sites' likelihoods as FP32 [sample][kept][3], all three NaN
+// for a missing sample, and the kept frequencies as FP32.
+__global__ void soft_pack32_kernel(const double* __restrict__ gl, int64_t n_samples, int64_t n_sites,
+                                   const int32_t* __restrict__ kept, const double* __restrict__ kp,
+                                   const double* __restrict__ kq, int64_t nk, float* __restrict__ g32,
+                                   float* __restrict__ p32, float* __restrict__ q32) {
+    const int64_t total = n_samples * nk;
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t s = t / nk, k = t - s * nk;
+        const double* r = gl + (s * n_sites + kept[k]) * 3;
+        const bool miss = isnan(r[0]) || isnan(r[1]) || isnan(r[2]);
+        float* o = g32 + t * 3;
+        o[0] = miss ? CUDART_NAN_F : (float)r[0];
+        o[1] = miss ? CUDART_NAN_F : (float)r[1];
+        o[2] = miss ? CUDART_NAN_F : (float)r[2];
+        if (s == 0) {
+            p32[k] = (float)kp[k];
+            q32[k] = (float)kq[k];
+        }
+    }
+}
+
+// The FP32 evaluation (see the file comment) at xt; in a difference pass
+// (DIFF) the objective is f_old - (1/n) sum log(d / d_old) with d_old at xc.
+// hs: the lane's 45 FP64 Hessian sums in shared memory.  Returns n.  Not
+// inlined: the site loop gets the registers the pair's SQP state would hold.
+template <bool DIFF>
+__device__ __noinline__ int64_t soft_evaluate32(const float* __restrict__ g32, const float* __restrict__ p32,
+                                                const float* __restrict__ q32, int64_t nk, int64_t x, int64_t y,
+                                                const double* xt, const double* xc, double f_old, double eps,
+                                                int lane, double* hs, PairEval& ev) {
+    const bool diff = DIFF;
+    float xh[9], sd[9];
+    double lo[9];
+#pragma unroll
+    for (int i = 0; i < 9; i++) {
+        xh[i] = (float)xt[i];
+        lo[i] = xt[i] - (double)xh[i];
+        sd[i] = DIFF ? (float)(xt[i] - xc[i]) : 0.f;
+    }
+    double G[9], F = 0.0;
+    float g[9], h[45], o = 0.f;
+#pragma unroll
+    for (int i = 0; i < 9; i++) { G[i] = 0.0; g[i] = 0.f; }
+#pragma unroll
+    for (int a = 0; a < 45; a++) h[a] = 0.f;
+    for (int a = 0; a < 45; a++) hs[a * 32 + lane] = 0.0;
+    const float* lx = g32 + x * nk * 3;
+    const float* ly = g32 + y * nk * 3;
+    const float e32 = (float)eps;
+    int64_t n = 0;
+    int cnt = 0;
+    for (int64_t k = lane; k < nk; k += 32) {
+        const float X0 = lx[3 * k], X1 = lx[3 * k + 1], X2 = lx[3 * k + 2];
+        const float Y0 = ly[3 * k], Y1 = ly[3 * k + 1], Y2 = ly[3 * k + 2];
+        if (isnan(X0) || isnan(Y0)) continue;   // a missing sample has all three NaN
+        const float p = p32[k], q = q32[k];
+        // L = sum over (gx, gy) of GLx(gx) GLy(gy) m(gx, gy), the nine rows of
+        // the biallelic conditional table (cls_row) gathered by entry
+        const float A = X0 * Y0, B = X2 * Y2, C = X0 * Y2, D = X2 * Y0, E = X0 * Y1;
+        const float Fx = X2 * Y1, Gx = X1 * Y0, Hx = X1 * Y2, I = X1 * Y1;
+        const float p2 = p * p, q2 = q * q, pq = p * q;
+        const float p2q = p2 * q, pq2 = p * q2;
+        const float S2 = fmaf(A, p2, B * q2);
+        const float S3 = fmaf(A, p2 * p, B * (q2 * q));
+        float L[9];
+        L[0] = fmaf(A, p, B * q);
+        L[1] = fmaf(C + D, pq, S2);
+        L[2] = fmaf(E + Fx, pq, S2);
+        L[3] = fmaf(2.0f * E, p2q, fmaf(2.0f * Fx, pq2, fmaf(C, pq2, fmaf(D, p2q, S3))));
+        L[4] = fmaf(Gx + Hx, pq, S2);
+        L[5] = fmaf(2.0f * Gx, p2q, fmaf(2.0f * Hx, pq2, fmaf(C, p2q, fmaf(D, pq2, S3))));
+        L[6] = fmaf(2.0f * I, pq, S2);
+        L[7] = fmaf(I, p2q + pq2, fmaf(Fx + Hx, pq2, fmaf(E + Gx, p2q, S3)));
+        L[8] = fmaf(4.0f * I, p2 * q2,
+                    fmaf(2.0f * (Fx + Hx), pq2 * q,
+                         fmaf(2.0f * (E + Gx), p2q * p, fmaf(C + D, p2 * q2, fmaf(A, p2 * p2, B * (q2 * q2))))));
+        float d = e32;
+#pragma unroll
+        for (int i = 0; i < 9; i++) d = fmaf(L[i], xh[i], d);
+        const float r = rcp_approx(d);
+        float b[9];
+#pragma unroll
+        for (int i = 0; i < 9; i++) {
+            b[i] = L[i] * r;
+            g[i] += b[i];
+        }
+        int a = 0;
+#pragma unroll
+        for (int i = 0; i < 9; i++)
+#pragma unroll
+            for (int j = i; j < 9; j++, a++) h[a] = fmaf(b[i], b[j], h[a]);
+        if (!diff) {
+            o += lg2_approx(d);
+        } else {
+            float dl = 0.f;
+#pragma unroll
+            for (int i = 0; i < 9; i++) dl = fmaf(L[i], sd[i], dl);
+            o += neg_log1m(dl * r);
+        }
+        n++;
+        cnt++;
+        if ((cnt & 7) == 0) {
+#pragma unroll
+            for (int i = 0; i < 9; i++) { G[i] += (double)g[i]; g[i] = 0.f; }
+            F += (double)o;
+            o = 0.f;
+        }
+        if ((cnt & 31) == 0) {
+#pragma unroll
+            for (int a2 = 0; a2 < 45; a2++) { hs[a2 * 32 + lane] += (double)h[a2]; h[a2] = 0.f; }
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < 9; i++) G[i] += (double)g[i];
+    F += (double)o;
+#pragma unroll
+    for (int a = 0; a < 45; a++) hs[a * 32 + lane] += (double)h[a];
+    // warp sums (fixed butterfly order)
+    for (int off = 16; off > 0; off >>= 1) {
+        F += __shfl_xor_sync(0xffffffffu, F, off);
+        n += __shfl_xor_sync(0xffffffffu, n, off);
+#pragma unroll
+        for (int i = 0; i < 9; i++) G[i] += __shfl_xor_sync(0xffffffffu, G[i], off);
+    }
+    __syncwarp();
+    for (int a = 0; a < 45; a++) {
+        double hv = hs[a * 32 + lane];
+        for (int off = 16; off > 0; off >>= 1) hv += __shfl_xor_sync(0xffffffffu, hv, off);
+        if (lane == 0) hs[a * 32] = hv;
+    }
+    __syncwarp();
+    auto Hsum = [&](int i, int j) {
+        const int i0 = i < j ? i : j, j0 = i < j ? j : i;
+        return hs[(i0 * 9 - i0 * (i0 - 1) / 2 + (j0 - i0)) * 32];
+    };
+    // the lo parts of x to first order: sum log d gains sum_j lo_j G_j, and
+    // G_i loses sum_j H_ij lo_j (a difference pass uses the step's FP32 values)
+    double corr = 0.0;
+#pragma unroll
+    for (int j = 0; j < 9; j++) corr = fma(lo[j], G[j], corr);
+    double Gc[9];
+#pragma unroll
+    for (int i = 0; i < 9; i++) {
+        double s = 0.0;
+#pragma unroll
+        for (int j = 0; j < 9; j++) s = fma(Hsum(i, j), lo[j], s);
+        Gc[i] = G[i] - s;
+    }
+    const double dn = (double)n;
+    ev.f = diff ? f_old - F / dn : -(F * 0.69314718055994530942 + corr) / dn;
+#pragma unroll
+    for (int i = 0; i < 9; i++) ev.g[i] = -Gc[i] / dn;
+#pragma unroll
+    for (int j = 0; j < 9; j++) ev.Hr[j] = lane < 9 ? Hsum(lane, j) / dn : 0.0;
+    __syncwarp();
+    return n;
+}
+
 // Warp per output row of the first ns samples (x-major, y >= x), taken from a
-// counter; the Jacquard SQP of src/sqp.rs:49-93 in FP64.
-__global__ void __launch_bounds__(SOFT_WARPS * 32, 4) soft_pairs_kernel(
+// counter; the Jacquard SQP of src/sqp.rs:49-93 in FP64 on FP32 evaluations
+// (prec64 = 0) or FP64 ones.  stats: [0] grad-Hessian evaluations, [1] of them
+// in FP64, [2] pairs escalated to FP64, [3] pair-sites evaluated (summed over
+// evaluations), [4] of them in FP64.
+__global__ void __launch_bounds__(SOFT_WARPS * 32, 3) soft_pairs_kernel(
     const double* __restrict__ gl, int64_t n_sites, const int32_t* __restrict__ kept, const double* __restrict__ kp,
-    const double* __restrict__ kq, int64_t nk, int64_t ns, int64_t n_rows, uint64_t iterations, kg_output* out,
-    unsigned long long* next, int* no_rows) {
+    const double* __restrict__ kq, const float* __restrict__ g32, const float* __restrict__ p32,
+    const float* __restrict__ q32, int prec64, int64_t nk, int64_t ns, int64_t n_rows, uint64_t iterations,
+    kg_output* out, unsigned long long* next, int* no_rows, unsigned long long* stats) {
     __shared__ double hsm[SOFT_WARPS][45 * 32];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     double* hs = hsm[w];
     const Tune tu = make_tune(iterations);
+    unsigned long long c_gh = 0, c_f64 = 0, c_esc = 0, c_sites = 0, c_sites64 = 0;
     for (;;) {
         unsigned long long r = 0;
         if (lane == 0) r = atomicAdd(next, 1ull);
@@ -167,8 +345,25 @@ __global__ void __launch_bounds__(SOFT_WARPS * 32, 4) soft_pairs_kernel(
         for (int i = 0; i < 9; i++) xv[i] = x == y ? 0.0 : 1.0 / 9.0;
         if (x == y) { xv[0] = 0.5; xv[6] = 0.5; }
         normalise9(xv);
+        bool fp64 = prec64 != 0;
+        // one evaluation at xt: FP64, or FP32 (a difference pass relative to xc
+        // and the objective f_old there when diff)
         PairEval ev;
-        const int64_t n = soft_evaluate(gl, n_sites, kept, kp, kq, nk, x, y, xv, tu.epsilon, lane, hs, ev);
+        auto eval = [&](const double* xt, const double* xc, bool diff, double f_old) -> int64_t {
+            c_gh++;
+            int64_t m;
+            if (fp64) {
+                c_f64++;
+                m = soft_evaluate(gl, n_sites, kept, kp, kq, nk, x, y, xt, tu.epsilon, lane, hs, ev);
+                c_sites64 += (unsigned long long)m;
+            } else {
+                m = diff ? soft_evaluate32<true>(g32, p32, q32, nk, x, y, xt, xc, f_old, tu.epsilon, lane, hs, ev)
+                         : soft_evaluate32<false>(g32, p32, q32, nk, x, y, xt, xc, f_old, tu.epsilon, lane, hs, ev);
+            }
+            c_sites += (unsigned long long)m;
+            return m;
+        };
+        const int64_t n = eval(xv, xv, false, 0.0);
         kg_output* o = out + r;
         if (n == 0) {
             if (lane == 0) {
@@ -187,9 +382,29 @@ __global__ void __launch_bounds__(SOFT_WARPS * 32, 4) soft_pairs_kernel(
         for (int i = 0; i < 9; i++) { g[i] = ev.g[i]; Hr[i] = ev.Hr[i]; }
         uint64_t iters = tu.sqp_max_iter;
         double cond = CUDART_NAN;
+        int near_count = 0;
         for (uint64_t it = 0; it < tu.sqp_max_iter; it++) {
             double resid;
-            if (kkt_ok(xv, g, tu.sqp_conv_tol, &resid)) {
+            bool conv = kkt_ok(xv, g, tu.sqp_conv_tol, &resid);
+            if (!fp64 && (conv || resid < 1e-6)) {
+                if (!conv) near_count++;
+                const double c32 = conv ? condition_rows(xv, g, Hr, tu.sqp_conv_tol) : 0.0;
+                if (conv ? !(c32 <= COND_RECHECK) : (near_count >= 3)) {
+                    // FP64 re-evaluation at the same point; the pair stays FP64
+                    fp64 = true;
+                    c_esc++;
+                    eval(xv, xv, false, 0.0);
+                    f = ev.f;
+#pragma unroll
+                    for (int i = 0; i < 9; i++) { g[i] = ev.g[i]; Hr[i] = ev.Hr[i]; }
+                    conv = kkt_ok(xv, g, tu.sqp_conv_tol, &resid);
+                } else if (conv) {
+                    iters = it;
+                    cond = c32;
+                    break;
+                }
+            }
+            if (conv) {
                 iters = it;
                 cond = condition_rows(xv, g, Hr, tu.sqp_conv_tol);
                 break;
@@ -201,13 +416,14 @@ __global__ void __launch_bounds__(SOFT_WARPS * 32, 4) soft_pairs_kernel(
             qp_simplex_rows(WarpGrp{FULL_MASK}, Hr, c, xv, tu, lane, yv);
 #pragma unroll
             for (int i = 0; i < 9; i++) p[i] = yv[i] - xv[i];
-            const double tt = tu.bls_sufficient_decrease * dot_fma(9, g, p);
+            const double gp = dot_fma(9, g, p);
+            const double tt = tu.bls_sufficient_decrease * gp;
             double alpha = 1.0, xn[9];
             for (int bls = 0;;) {
 #pragma unroll
                 for (int i = 0; i < 9; i++) xn[i] = xv[i] + alpha * p[i];
                 normalise9(xn);
-                soft_evaluate(gl, n_sites, kept, kp, kq, nk, x, y, xn, tu.epsilon, lane, hs, ev);
+                eval(xn, xv, fabs(alpha * gp) < DIFF_BELOW, f);
                 const bool accept = ev.f <= f + alpha * tt;
                 bls++;
                 if (accept || bls == tu.bls_max_iter) break;
@@ -226,12 +442,20 @@ __global__ void __launch_bounds__(SOFT_WARPS * 32, 4) soft_pairs_kernel(
             o->cond = cond;
         }
     }
+    if (lane == 0) {
+        atomicAdd(&stats[0], c_gh);
+        atomicAdd(&stats[1], c_f64);
+        atomicAdd(&stats[2], c_esc);
+        atomicAdd(&stats[3], c_sites);
+        atomicAdd(&stats[4], c_sites64);
+    }
 }
 
 int soft_relatedness(const DevBuf& gl, int64_t n_samples, int64_t n_sites, int64_t ns, uint64_t iterations,
-                     double maf, kg_output* d_out, cudaStream_t st, std::string& err, int64_t* n_kept) {
+                     double maf, kg_output* d_out, cudaStream_t st, std::string& err, int64_t* n_kept, int precision,
+                     uint64_t* counters) {
     if (!(maf >= 0.0)) maf = 1.0 / (2.0 * (double)n_samples);
-    DevBuf pf, qf, keep, idx, kp, kq, ctr;
+    DevBuf pf, qf, keep, idx, kp, kq, ctr, g32, p32, q32;
     KG_SOFT_TRY((cudaError_t)pf.reserve(sizeof(double) * n_sites));
     KG_SOFT_TRY((cudaError_t)qf.reserve(sizeof(double) * n_sites));
     KG_SOFT_TRY((cudaError_t)keep.reserve((size_t)n_sites));
@@ -263,24 +487,42 @@ int soft_relatedness(const DevBuf& gl, int64_t n_samples, int64_t n_sites, int64
     KG_SOFT_TRY((cudaError_t)idx.reserve(sizeof(int32_t) * nk));
     KG_SOFT_TRY((cudaError_t)kp.reserve(sizeof(double) * nk));
     KG_SOFT_TRY((cudaError_t)kq.reserve(sizeof(double) * nk));
-    KG_SOFT_TRY((cudaError_t)ctr.reserve(sizeof(unsigned long long) + sizeof(int)));
+    KG_SOFT_TRY((cudaError_t)ctr.reserve(sizeof(unsigned long long) * 6 + sizeof(int)));
     KG_SOFT_TRY(cudaMemcpyAsync(idx.p, ki.data(), sizeof(int32_t) * nk, cudaMemcpyHostToDevice, st));
     KG_SOFT_TRY(cudaMemcpyAsync(kp.p, kpv.data(), sizeof(double) * nk, cudaMemcpyHostToDevice, st));
     KG_SOFT_TRY(cudaMemcpyAsync(kq.p, kqv.data(), sizeof(double) * nk, cudaMemcpyHostToDevice, st));
-    KG_SOFT_TRY(cudaMemsetAsync(ctr.p, 0, sizeof(unsigned long long) + sizeof(int), st));
+    KG_SOFT_TRY(cudaMemsetAsync(ctr.p, 0, sizeof(unsigned long long) * 6 + sizeof(int), st));
     unsigned long long* next = ctr.as<unsigned long long>();
-    int* no_rows = reinterpret_cast<int*>(next + 1);
+    unsigned long long* stats = next + 1;
+    int* no_rows = reinterpret_cast<int*>(next + 6);
+    const bool fp64 = precision == KG_PREC_FP64;
+    if (!fp64) {
+        KG_SOFT_TRY((cudaError_t)g32.reserve(sizeof(float) * 3 * (size_t)(n_samples * nk)));
+        KG_SOFT_TRY((cudaError_t)p32.reserve(sizeof(float) * nk));
+        KG_SOFT_TRY((cudaError_t)q32.reserve(sizeof(float) * nk));
+        const int64_t total = n_samples * nk;
+        const unsigned blocks = (unsigned)std::min<int64_t>((total + 255) / 256, 148 * 16);
+        soft_pack32_kernel<<<blocks, 256, 0, st>>>(gl.as<double>(), n_samples, n_sites, idx.as<int32_t>(),
+                                                   kp.as<double>(), kq.as<double>(), nk, g32.as<float>(),
+                                                   p32.as<float>(), q32.as<float>());
+    }
     const int64_t rows = ns * (ns + 1) / 2;
     int dev = 0, sms = 148;
     KG_SOFT_TRY(cudaGetDevice(&dev));
     KG_SOFT_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    soft_pairs_kernel<<<(unsigned)(sms * 4), SOFT_WARPS * 32, 0, st>>>(gl.as<double>(), n_sites, idx.as<int32_t>(),
-                                                                      kp.as<double>(), kq.as<double>(), nk, ns, rows,
-                                                                      iterations, d_out, next, no_rows);
+    int occ = 0;
+    KG_SOFT_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, soft_pairs_kernel, SOFT_WARPS * 32, 0));
+    soft_pairs_kernel<<<(unsigned)(sms * std::max(1, occ)), SOFT_WARPS * 32, 0, st>>>(
+        gl.as<double>(), n_sites, idx.as<int32_t>(), kp.as<double>(), kq.as<double>(), g32.as<float>(),
+        p32.as<float>(), q32.as<float>(), fp64 ? 1 : 0, nk, ns, rows, iterations, d_out, next, no_rows, stats);
     KG_SOFT_TRY(cudaGetLastError());
     int h_no_rows = 0;
+    unsigned long long hs[5] = {0, 0, 0, 0, 0};
     KG_SOFT_TRY(cudaMemcpyAsync(&h_no_rows, no_rows, sizeof(int), cudaMemcpyDeviceToHost, st));
+    KG_SOFT_TRY(cudaMemcpyAsync(hs, stats, sizeof(hs), cudaMemcpyDeviceToHost, st));
     KG_SOFT_TRY(cudaStreamSynchronize(st));
+    if (counters)
+        for (int i = 0; i < 5; i++) counters[i] = hs[i];
     if (h_no_rows) {
         err = "a pair shares no called segregating site";
         return KG_ENOSITES;

@@ -76,3 +76,21 @@ def test_soft_entry_point_argument_errors(est):
         with pytest.raises(kb.KestrelError) as ei:
             est.relatedness_gl(num_samples=ns if ns >= 0 else None, maf=maf)
         assert ei.value.status == kb.KG_EINVAL and msg in str(ei.value), str(ei.value)
+
+
+def test_soft_fp32_and_fp64_forms(est, oracle, cohort):
+    """Both evaluation forms against the oracle: FP32 evaluations (the default,
+    with FP64 re-evaluation of pairs that need it) and the plain FP64 form."""
+    gl = soft_gl(cohort.codes, np.random.default_rng(6), err=0.08)
+    ref, _ = oracle.gl_relatedness(gl)
+    est.load_likelihoods(np.ascontiguousarray(gl.transpose(1, 0, 2)))
+    out = {}
+    for prec in ("fp32c", "fp64"):
+        est.set_precision(prec)
+        rows = est.relatedness_gl()
+        st = est.run_stats()
+        out[prec] = (compare(rows, ref), {k: st[k] for k in ("gh_passes", "fp64_passes", "fp64_pairs", "work_units")})
+    est.set_precision("fp32c")
+    print(out)
+    assert out["fp64"][1]["fp64_passes"] == out["fp64"][1]["gh_passes"] > 0
+    assert out["fp32c"][1]["fp64_passes"] < out["fp32c"][1]["gh_passes"]
