@@ -187,6 +187,16 @@ int kg_relatedness_gt(kg_ctx *ctx, int64_t num_samples, uint64_t iterations,
  * pair's rows are sum over genotype pairs of GLx GLy m(gx, gy), and the SQP is
  * that of kg_relatedness.  The first form runs in FP64 with a warp per pair. */
 int kg_load_likelihoods(kg_ctx *ctx, const double *gl, int64_t n_samples, int64_t n_sites);
+/* Tri- or tetra-allelic sites for kg_relatedness_gl (the reference's gl3 and
+ * gl4, src/coefficients.rs:99-106): gl is n_samples x n_sites x G doubles
+ * (G = 6 for n_alleles 3, 10 for 4; genotypes in the VCF order, linear scale,
+ * a NaN marks a missing sample), n_samples that of kg_load_likelihoods, which
+ * clears both classes (as does n_sites = 0).  Their frequencies come from the
+ * same per-site fit, then the maf cut and the drop of zero-frequency alleles
+ * (src/wrapper.rs:349-409); a pair's row at such a site is the sum over its
+ * remaining genotype pairs of GLx GLy m(gx, gy), built once per pair. */
+int kg_load_likelihoods_multiallelic(kg_ctx *ctx, const double *gl, int64_t n_samples, int64_t n_sites,
+                                     int n_alleles);
 int kg_relatedness_gl(kg_ctx *ctx, int64_t num_samples, uint64_t iterations, double maf,
                       kg_output *out, int64_t out_cap, int64_t *n_out);
 

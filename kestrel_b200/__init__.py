@@ -207,6 +207,18 @@ class Estimator:
         self.n_gl_samples = gl.shape[0]
         return self
 
+    def load_likelihoods_multiallelic(self, likelihoods: np.ndarray, n_alleles: int):
+        """Tri- (G = 6) or tetra-allelic (G = 10) sites for relatedness_gl:
+        double [samples, sites, G], genotypes in the VCF order, linear scale,
+        NaN = missing; after load_likelihoods."""
+        gl = np.ascontiguousarray(likelihoods, dtype=np.float64)
+        ng = n_alleles * (n_alleles + 1) // 2
+        if gl.ndim != 3 or gl.shape[2] != ng:
+            raise ValueError(f"likelihoods must be (samples, sites, {ng})")
+        _check(self._L.kg_load_likelihoods_multiallelic(self._h, ptr(gl), gl.shape[0], gl.shape[1], int(n_alleles)),
+               self._h)
+        return self
+
     def relatedness_gl(self, num_samples=None, iterations: int = 100, maf=None,
                        out: np.ndarray | None = None) -> np.ndarray:
         """The GL/PL estimator on the loaded soft likelihoods (kg_relatedness_gl)."""

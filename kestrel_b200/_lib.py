@@ -57,7 +57,7 @@ assert OUTPUT_DTYPE.itemsize == ctypes.sizeof(KgOutput) == 112
 # Every symbol include/kestrel_gpu.h declares.
 EXPORTS = ("kg_create", "kg_destroy", "kg_last_error", "kg_version", "kg_set_precision",
            "kg_set_launch", "kg_set_wave_limit", "kg_set_work_unit", "kg_get_launch", "kg_autotune", "kg_load_genotypes", "kg_load_genotypes_2bit",
-           "kg_set_allele_frequencies", "kg_load_multiallelic", "kg_load_likelihoods", "kg_relatedness_gl",
+           "kg_set_allele_frequencies", "kg_load_multiallelic", "kg_load_likelihoods", "kg_load_likelihoods_multiallelic", "kg_relatedness_gl",
            "kg_relatedness", "kg_relatedness_gt", "kg_relatedness_coefficients",
            "kg_relatedness_batch", "kg_panel_load", "kg_submit", "kg_poll", "kg_wait",
            "kg_cancel", "kg_serving_stats", "kg_relatedness_noalloc", "kg_last_run_stats",
@@ -100,6 +100,7 @@ def lib():
         "kg_set_allele_frequencies": ([P, P], i32),
         "kg_load_multiallelic": ([P, P, i64, i64, i64, P, P], i32),
         "kg_load_likelihoods": ([P, P, i64, i64], i32),
+        "kg_load_likelihoods_multiallelic": ([P, P, i64, i64, i32], i32),
         "kg_relatedness_gl": ([P, i64, u64, ctypes.c_double, P, i64, ctypes.POINTER(i64)], i32),
         "kg_relatedness": ([P, i64, u64, dbl, P, i64, ctypes.POINTER(i64)], i32),
         "kg_relatedness_gt": ([P, i64, u64, P, i64, ctypes.POINTER(i64)], i32),

@@ -7,12 +7,12 @@
 // src/cholesky.rs:6-65 and its solves (:104-140); then frequencies in (0, maf)
 // become zero and the rest are renormalised.
 //
-// With one-hot likelihoods the objective -(1/n) sum_samples log(eps + x'Lx)
-// only depends on how many samples carry each genotype, so the sums run over
-// the site's genotype classes, each weighted by its count (the rows are the
-// classes' one-hot likelihood rows, genotype g = j (j + 1) / 2 + i for alleles
-// i <= j, the VCF order).  One thread per site: every array is at most 4 or
-// 4 x 4.
+// The sums run over weighted likelihood rows (genotype g = j (j + 1) / 2 + i
+// for alleles i <= j, the VCF order), given by a row source: with one-hot
+// likelihoods the objective -(1/n) sum_samples log(eps + x'Lx) only depends on
+// how many samples carry each genotype, so AlleleClasses gives the site's
+// genotype classes, each weighted by its count; soft likelihoods give one row
+// per called sample.  One thread per site: every array is at most 4 or 4 x 4.
 #pragma once
 
 #include <cstdint>
@@ -29,60 +29,73 @@ struct AlleleClasses {
     int n;               // classes with a non-zero count
     int cls[MAXG];       // their genotype indices
     double w[MAXG];      // their counts
+    // the row source: row k's likelihoods (one-hot at its genotype) and weight
+    __host__ __device__ int alleles() const { return a; }
+    __host__ __device__ int rows() const { return n; }
+    __host__ __device__ double weight(int k) const { return w[k]; }
+    __host__ __device__ bool row(int k, double* l) const {
+        for (int g = 0; g < MAXG; g++) l[g] = g == cls[k] ? 1.0 : 0.0;
+        return true;
+    }
 };
 
-// The one-hot likelihood matrix entry L[r][c] of genotype g (L symmetric,
-// L[i][j] = L[j][i] = 1 for g = (i, j)).
-__host__ __device__ __forceinline__ double onehot_l(int g, int r, int c) {
-    const int j = g >= 6 ? 3 : g >= 3 ? 2 : g >= 1 ? 1 : 0;
-    const int i = g - j * (j + 1) / 2;
-    return ((r == i && c == j) || (r == j && c == i)) ? 1.0 : 0.0;
+// The likelihood matrix entry L[r][c] of a row l (L symmetric: L[i][j] =
+// L[j][i] = l[genotype (i, j)]).
+__host__ __device__ __forceinline__ double lmat(const double* l, int r, int c) {
+    const int i = r < c ? r : c, j = r < c ? c : r;
+    return l[j * (j + 1) / 2 + i];
 }
 
-// -(1/n) sum over classes of count x log(eps + sum over genotypes (a <= b) of
+// -(1/n) sum over rows of weight x log(eps + sum over genotypes (a <= b) of
 // w_ab L_ab), w_aa = x_a^2, w_ab = 2 x_a x_b, fused in the reference's order
-// (src/allele/objective.rs).
-__host__ __device__ inline double allele_objective(const AlleleClasses& C, const double* x, double eps) {
+// (src/allele/objective.rs); rows with a NaN are skipped.
+template <class Src>
+__host__ __device__ inline double allele_objective(const Src& C, const double* x, double eps) {
     double acc = 0.0, tot = 0.0;
-    for (int k = 0; k < C.n; k++) {
-        const int g = C.cls[k];
+    const int A = C.alleles();
+    for (int k = 0; k < C.rows(); k++) {
+        double l[MAXG];
+        if (!C.row(k, l)) continue;
         double p = eps;
-        for (int b = 0; b < C.a; b++)
+        for (int b = 0; b < A; b++)
             for (int a = 0; a <= b; a++) {
                 const double w = a == b ? x[a] * x[a] : 2.0 * x[a] * x[b];
-                p = fma(w, (b * (b + 1) / 2 + a) == g ? 1.0 : 0.0, p);
+                p = fma(w, l[b * (b + 1) / 2 + a], p);
             }
-        acc = fma(C.w[k], log(p), acc);
-        tot += C.w[k];
+        acc = fma(C.weight(k), log(p), acc);
+        tot += C.weight(k);
     }
     return -acc / tot;
 }
 
 // gradient -2/n sum Lx/d and Hessian 2/n sum (2 (Lx/d)(Lx/d)' - L/d), d = eps
-// + x'Lx (src/allele/grad_hess.rs), per class weighted by its count.
-__host__ __device__ inline void allele_grad_hess(const AlleleClasses& C, const double* x, double eps, double* g,
+// + x'Lx (src/allele/grad_hess.rs), per row weighted.
+template <class Src>
+__host__ __device__ inline void allele_grad_hess(const Src& C, const double* x, double eps, double* g,
                                                  double (*H)[MAXA]) {
-    const int A = C.a;
+    const int A = C.alleles();
     double zg[MAXA], zh[MAXA][MAXA], tot = 0.0;
     for (int a = 0; a < MAXA; a++) {
         zg[a] = 0.0;
         for (int b = 0; b < MAXA; b++) zh[a][b] = 0.0;
     }
-    for (int k = 0; k < C.n; k++) {
-        const int gk = C.cls[k];
+    for (int k = 0; k < C.rows(); k++) {
+        double l[MAXG];
+        if (!C.row(k, l)) continue;
+        const double wk = C.weight(k);
         double lx[MAXA], d = eps;
         for (int a = 0; a < A; a++) {
             lx[a] = 0.0;
-            for (int b = 0; b < A; b++) lx[a] = fma(onehot_l(gk, a, b), x[b], lx[a]);
+            for (int b = 0; b < A; b++) lx[a] = fma(lmat(l, a, b), x[b], lx[a]);
         }
         for (int a = 0; a < A; a++) d = fma(x[a], lx[a], d);
         const double inv = 1.0 / d;
         for (int a = 0; a < A; a++) {
-            zg[a] = fma(C.w[k], lx[a] * inv, zg[a]);
+            zg[a] = fma(wk, lx[a] * inv, zg[a]);
             for (int b = 0; b < A; b++)
-                zh[a][b] = fma(C.w[k], 2.0 * (lx[a] * inv) * (lx[b] * inv) - onehot_l(gk, a, b) * inv, zh[a][b]);
+                zh[a][b] = fma(wk, 2.0 * (lx[a] * inv) * (lx[b] * inv) - lmat(l, a, b) * inv, zh[a][b]);
         }
-        tot += C.w[k];
+        tot += wk;
     }
     for (int a = 0; a < MAXA; a++) {
         g[a] = a < A ? -2.0 * zg[a] / tot : 0.0;
@@ -220,11 +233,17 @@ __host__ __device__ inline void qp_simplex4(int n, const double (*Q)[MAXA], cons
 }
 
 // The fit of one site: f gets its A frequencies (zero past A).  A site
-// without a called sample gets NaN frequencies (its sums have no term).
-__host__ __device__ inline void allele_fit(const AlleleClasses& C, uint64_t iterations, double maf, double* f) {
-    const int A = C.a;
+// without a called row gets NaN frequencies (its sums have no term).
+template <class Src>
+__host__ __device__ inline void allele_fit(const Src& C, uint64_t iterations, double maf, double* f) {
+    const int A = C.alleles();
     for (int a = 0; a < MAXA; a++) f[a] = 0.0;
-    if (C.n == 0) {
+    bool any = false;
+    for (int k = 0; k < C.rows() && !any; k++) {
+        double l[MAXG];
+        any = C.row(k, l);
+    }
+    if (!any) {
         for (int a = 0; a < A; a++) f[a] = nan("");
         return;
     }

@@ -58,6 +58,8 @@ struct kg_ctx {
     bool multi_af = false;                // kg_load_multiallelic gave frequencies
     kg::DevBuf soft_gl;                   // kg_load_likelihoods: double [sample][site][3]
     int64_t soft_ns = 0, soft_nv = 0;
+    kg::DevBuf soft_gl3, soft_gl4;        // kg_load_likelihoods_multiallelic: [sample][site][6], [..][10]
+    int64_t soft_n3 = 0, soft_n4 = 0;
     kg::Workspace ws;
     kg::DevBuf dout;
     kg_run_stats last{};
@@ -663,6 +665,37 @@ int kg_load_likelihoods(kg_ctx* c, const double* gl, int64_t n_samples, int64_t 
         if (e != cudaSuccess) return set_err(c, KG_ECUDA, std::string("upload: ") + cudaGetErrorString(e));
         c->soft_ns = n_samples;
         c->soft_nv = n_sites;
+        c->soft_n3 = 0;
+        c->soft_n4 = 0;
+        return KG_OK;
+    });
+}
+
+int kg_load_likelihoods_multiallelic(kg_ctx* c, const double* gl, int64_t n_samples, int64_t n_sites,
+                                     int n_alleles) {
+    if (!c) return KG_EINVAL;
+    if (!c->soft_ns) return set_err(c, KG_EINVAL, "load the biallelic likelihoods first");
+    if (n_alleles != 3 && n_alleles != 4) return set_err(c, KG_EINVAL, "n_alleles must be 3 or 4");
+    if (n_samples != c->soft_ns) return set_err(c, KG_EINVAL, "n_samples must match the loaded likelihoods");
+    if (n_sites < 0 || n_sites > (int64_t)INT32_MAX || (n_sites > 0 && !gl))
+        return set_err(c, KG_EINVAL, "gl must be non-NULL with n_sites >= 0");
+    int64_t& count = n_alleles == 3 ? c->soft_n3 : c->soft_n4;
+    kg::DevBuf& buf = n_alleles == 3 ? c->soft_gl3 : c->soft_gl4;
+    if (n_sites == 0) {
+        count = 0;
+        return KG_OK;
+    }
+    return guarded(c, [&]() -> int {
+        int st = use_device(c);
+        if (st) return st;
+        const int ng = n_alleles * (n_alleles + 1) / 2;
+        const size_t bytes = sizeof(double) * ng * (size_t)n_samples * (size_t)n_sites;
+        if (!budget_ok(c, bytes)) return set_err(c, KG_ENOMEM, "likelihoods exceed the memory budget");
+        if (buf.reserve(bytes) != cudaSuccess) return set_err(c, KG_ENOMEM, "cannot allocate device likelihoods");
+        cudaError_t e = cudaMemcpyAsync(buf.p, gl, bytes, cudaMemcpyHostToDevice, c->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+        if (e != cudaSuccess) return set_err(c, KG_ECUDA, std::string("upload: ") + cudaGetErrorString(e));
+        count = n_sites;
         return KG_OK;
     });
 }
@@ -692,10 +725,15 @@ int kg_relatedness_gl(kg_ctx* c, int64_t num_samples, uint64_t iterations, doubl
         cudaEventCreate(&ev0);
         cudaEventCreate(&ev1);
         cudaEventRecord(ev0, c->stream);
-        int64_t kept = 0;
+        int64_t kept = 0, used[3] = {0, 0, 0};
         uint64_t sc[5] = {0, 0, 0, 0, 0};
+        kg::SoftMultiInput mi;
+        mi.gl3 = c->soft_n3 ? c->soft_gl3.as<double>() : nullptr;
+        mi.n3 = c->soft_n3;
+        mi.gl4 = c->soft_n4 ? c->soft_gl4.as<double>() : nullptr;
+        mi.n4 = c->soft_n4;
         st = kg::soft_relatedness(c->soft_gl, c->soft_ns, c->soft_nv, ns, iterations, std::isnan(maf) ? -1.0 : maf,
-                                  c->dout.as<kg_output>(), c->stream, err, &kept, c->precision, sc);
+                                  c->dout.as<kg_output>(), c->stream, err, &kept, c->precision, sc, &mi, used);
         cudaEventRecord(ev1, c->stream);
         int st2 = copy_rows_out(c, c->dout, np, out, c->stream);
         kg_run_stats stats{};
@@ -713,8 +751,10 @@ int kg_relatedness_gl(kg_ctx* c, int64_t num_samples, uint64_t iterations, doubl
         // row from the nine likelihood products, d, the gradient and the 45
         // Hessian terms, the objective term
         stats.flops_fp32 = (sc[3] - sc[4]) * 204ull;
-        stats.sites_used[0] = (uint64_t)kept;
-        stats.sites_discarded = (uint64_t)(c->soft_nv - kept);
+        stats.sites_used[0] = (uint64_t)(kept + used[0]);
+        stats.sites_used[1] = (uint64_t)used[1];
+        stats.sites_used[2] = (uint64_t)used[2];
+        stats.sites_discarded = (uint64_t)(c->soft_nv + c->soft_n3 + c->soft_n4 - kept - used[0] - used[1] - used[2]);
         stats.total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
         c->last = stats;
         if (n_out) *n_out = np;

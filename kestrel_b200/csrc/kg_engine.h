@@ -137,9 +137,19 @@ int prepare_ml_multi(Cohort& c, bool have_af, double maf, uint64_t iterations, c
 // precision: KG_PREC_FP32C (FP32 evaluations, FP64 for pairs that need it) or
 // KG_PREC_FP64; counters (5, optional): grad-Hessian evaluations, those in
 // FP64, pairs escalated to FP64, pair-sites evaluated, those in FP64.
+// multi (optional): tri- and tetra-allelic sites' likelihoods on the device,
+// [sample][site][6] and [sample][site][10]; multi_used (3, optional): those
+// kept with 2, 3 and 4 alleles after the frequency cut.
+struct SoftMultiInput {
+    const double* gl3 = nullptr;
+    int64_t n3 = 0;
+    const double* gl4 = nullptr;
+    int64_t n4 = 0;
+};
 int soft_relatedness(const DevBuf& gl, int64_t n_samples, int64_t n_sites, int64_t ns, uint64_t iterations,
                      double maf, kg_output* d_out, cudaStream_t st, std::string& err, int64_t* n_kept = nullptr,
-                     int precision = KG_PREC_FP32C, uint64_t* counters = nullptr);
+                     int precision = KG_PREC_FP32C, uint64_t* counters = nullptr,
+                     const SoftMultiInput* multi = nullptr, int64_t* multi_used = nullptr);
 
 // Unpacks the VCF reader's 2-bit codes + observed mask into device byte codes
 // (d2, dm: the packed rows' device copies, kept for the next load).

@@ -1,15 +1,18 @@
-// kg_soft.cu — the GL/PL estimator on soft genotype likelihoods, biallelic
-// sites (src/wrapper.rs:89-330 with src/mixture.rs:67-140 and
-// src/coefficients.rs:40-141): per-site allele frequencies by the HWE SQP on
-// the samples' likelihoods, then for every pair the Jacquard SQP on the rows
-// L_s = sum over (gx, gy) of GLx(gx) GLy(gy) m(gx, gy) of its sites.
+// kg_soft.cu — the GL/PL estimator on soft genotype likelihoods
+// (src/wrapper.rs:89-330 with src/mixture.rs:9-140 and src/coefficients.rs:
+// 40-141): per-site allele frequencies by the HWE SQP on the samples'
+// likelihoods, then for every pair the Jacquard SQP on the rows L_s = sum over
+// (gx, gy) of GLx(gx) GLy(gy) m(gx, gy) of its sites.
 //
-// Layout: likelihoods double [sample][site][3] (0/0, 0/1, 1/1; linear scale;
-// a NaN marks a missing sample) as loaded; the kept sites' likelihoods are
-// also packed as FP32 [sample][kept site][3] (all three NaN when missing).
+// Layout: biallelic likelihoods double [sample][site][3] (0/0, 0/1, 1/1;
+// linear scale; a NaN marks a missing sample) as loaded; the kept sites'
+// likelihoods are also packed as FP32 [sample][kept site][3] (all three NaN
+// when missing).  Tri- and tetra-allelic sites: double [sample][site][6] and
+// [sample][site][10] in the VCF genotype order.
 //
 // A warp per pair, lanes over the kept sites; the SQP itself is FP64.  Its
-// evaluations (f, g and H at a point) run in one of two forms:
+// evaluations (f, g and H at a point) of the biallelic sites run in one of two
+// forms:
 //   * FP32 (the default, KG_PREC_FP32C): from the FP32 likelihoods, which stay
 //     L2-resident for cohorts of a few hundred samples, each site's row L is
 //     formed from the pair's nine likelihood products in closed form; d =
@@ -22,6 +25,12 @@
 //     re-evaluated in FP64 and stays FP64 (the hard-call path's rule).
 //   * FP64 (KG_PREC_FP64, and escalated pairs): from the FP64 likelihoods,
 //     each row the sum over the nine genotype pairs of GLx GLy m(gx, gy).
+// Tri- and tetra-allelic sites keep the genotypes of the alleles left after
+// the frequency cut (src/wrapper.rs:349-409); their rows (G' x G' x 9 terms
+// each) are built once per pair in FP64 into the warp's scratch, as the
+// reference builds its pair buffer once, and every evaluation adds their FP64
+// sums to the biallelic ones.  The shared-memory sums of a warp are 45 rows of
+// 33 doubles: the 32 lanes' partials and the warp's total.
 #include <cuda_runtime.h>
 #include <math_constants.h>
 
@@ -31,6 +40,7 @@
 
 #include "kestrel_gpu.h"
 #include "kg_allele.cuh"
+#include "kg_alleleN.cuh"
 #include "kg_engine.h"
 #include "kg_pair.cuh"
 #include "kg_rowsolve.cuh"
@@ -70,18 +80,231 @@ __global__ void soft_freq_kernel(const double* __restrict__ gl, int64_t n_sample
 }
 
 constexpr int SOFT_WARPS = 4;
+constexpr int HS = 33;   // shared-memory stride of the Hessian sums: 32 lane partials, then the warp total
+
+// ---------------------------------------------------------- tri / tetra
+// A loaded tri- or tetra-allelic site after its frequency fit: G' genotypes of
+// the remaining alleles (0: discarded), the original genotype index of each,
+// and the site's G' x G' rows m[g'x][g'y] (stride ML_SOFT_ROWS rows).
+constexpr int SOFT_MULTI_ROWS = 100;
+
+struct SoftMultiDev {
+    const double* gl[2];      // [sample][site][G0] of the tri- and of the tetra-allelic sites
+    int64_t n[2];             // their site counts
+    int64_t total;            // n[0] + n[1]: tri-allelic sites first
+    const int32_t* gk;        // per site: G' (0 = discarded)
+    const uint8_t* gidx;      // per site: [10] original genotype of reduced genotype g'
+    const double* rows;       // per site: SOFT_MULTI_ROWS x 9
+    double* scratch;          // per warp: total x 9, the current pair's rows (NaN first entry: no row)
+};
+
+// Per-sample likelihood rows of one multi-allelic site (a row with a NaN is a
+// missing sample), weight 1: the row source of allele_fit.
+struct SoftRows {
+    const double* gl;
+    int64_t n_samples, n_sites, v;
+    int a, g0;
+    __device__ int alleles() const { return a; }
+    __device__ int rows() const { return (int)n_samples; }
+    __device__ double weight(int) const { return 1.0; }
+    __device__ bool row(int k, double* l) const {
+        const double* r = gl + ((int64_t)k * n_sites + v) * g0;
+        bool ok = true;
+        for (int g = 0; g < MAXG; g++) {
+            l[g] = g < g0 ? r[g] : 0.0;
+            ok = ok && !(g < g0 && isnan(l[g]));
+        }
+        return ok;
+    }
+};
+
+// Thread per tri-/tetra-allelic site: the frequency fit on the samples'
+// likelihoods with the maf cut, the alleles left (in order), each reduced
+// genotype's original index and the site's rows; used[0..2] counts the sites
+// left with 2, 3, 4 alleles.
+__global__ void soft_multi_site_kernel(SoftMultiDev M, int64_t n_samples, double maf, uint64_t iterations,
+                                       int32_t* __restrict__ gk, uint8_t* __restrict__ gidx,
+                                       double* __restrict__ rows, unsigned long long* __restrict__ used) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= M.total) return;
+    const int c = t < M.n[0] ? 0 : 1;
+    const int64_t v = c == 0 ? t : t - M.n[0];
+    SoftRows src;
+    src.gl = M.gl[c];
+    src.n_samples = n_samples;
+    src.n_sites = M.n[c];
+    src.v = v;
+    src.a = c == 0 ? 3 : 4;
+    src.g0 = c == 0 ? 6 : 10;
+    double f[MAXA];
+    allele_fit(src, iterations, maf, f);
+    int keep[MAXA], na = 0;
+    double fk[MAXA] = {0.0, 0.0, 0.0, 0.0};
+    for (int a = 0; a < src.a; a++)
+        if (f[a] > 0.0) {
+            keep[na] = a;
+            fk[na] = f[a];
+            na++;
+        }
+    if (na < 2) {
+        gk[t] = 0;
+        return;
+    }
+    const int g = na * (na + 1) / 2;
+    gk[t] = g;
+    int k = 0;
+    for (int j = 0; j < na; j++)
+        for (int i = 0; i <= j; i++) gidx[MAXG * t + k++] = (uint8_t)(keep[j] * (keep[j] + 1) / 2 + keep[i]);
+    double* R = rows + (int64_t)SOFT_MULTI_ROWS * 9 * t;
+    for (int gx = 0; gx < g; gx++) {
+        int i, j;
+        genotype_alleles(gx, i, j);
+        for (int gy = 0; gy < g; gy++) {
+            int a, b;
+            genotype_alleles(gy, a, b);
+            iis_row(i, j, a, b, fk[0], fk[1], fk[2], fk[3], R + 9 * (gx * g + gy));
+        }
+    }
+    atomicAdd(&used[na - 2], 1ull);
+}
+
+// The pair's rows at the multi-allelic sites, in FP64, into the warp's
+// scratch: sum over the remaining genotypes of GLx(gx) GLy(gy) m[gx][gy]
+// (gx outer, gy inner, as src/mixture.rs:9-60 accumulates); NaN first entry
+// when a sample is missing or the site was discarded.  Returns the warp's count
+// of rows.
+__device__ __noinline__ int64_t soft_multi_build(const SoftMultiDev M, int64_t x, int64_t y, int lane, double* R) {
+    int64_t m = 0;
+    for (int64_t t = lane; t < M.total; t += 32) {
+        double* o = R + 9 * t;
+        const int g = M.gk[t];
+        bool ok = g > 0;
+        double L[9];
+#pragma unroll
+        for (int k = 0; k < 9; k++) L[k] = 0.0;
+        if (ok) {
+            const int c = t < M.n[0] ? 0 : 1;
+            const int64_t v = c == 0 ? t : t - M.n[0];
+            const int g0 = c == 0 ? 6 : 10;
+            const double* lx = M.gl[c] + (x * M.n[c] + v) * g0;
+            const double* ly = M.gl[c] + (y * M.n[c] + v) * g0;
+            const uint8_t* gi = M.gidx + MAXG * t;
+            const double* mm = M.rows + (int64_t)SOFT_MULTI_ROWS * 9 * t;
+            for (int gx = 0; gx < g && ok; gx++) {
+                const double ax = lx[gi[gx]];
+                for (int gy = 0; gy < g; gy++) {
+                    const double gg = ax * ly[gi[gy]];
+#pragma unroll
+                    for (int k = 0; k < 9; k++) L[k] = fma(gg, mm[9 * (gx * g + gy) + k], L[k]);
+                }
+            }
+#pragma unroll
+            for (int k = 0; k < 9; k++) ok = ok && !isnan(L[k]);
+        }
+        if (ok) {
+#pragma unroll
+            for (int k = 0; k < 9; k++) o[k] = L[k];
+            m++;
+        } else {
+            o[0] = CUDART_NAN;
+        }
+    }
+    for (int off = 16; off > 0; off >>= 1) m += __shfl_xor_sync(0xffffffffu, m, off);
+    __syncwarp();   // the rows are read by every lane's evaluations
+    return m;
+}
+
+// Adds the pair's multi-allelic rows at xt to the warp's totals, in FP64:
+// G (warp-uniform), the 45 Hessian totals at hs[a * HS + 32], F (sum log d, or
+// sum log(d / d_old) with d_old at xc in a difference pass) and n.
+__device__ __noinline__ void soft_multi_add(const double* R, int64_t total, const double* xt, const double* xc,
+                                            bool diff, double eps, int lane, double* hs, double* G, double& F,
+                                            int64_t& n) {
+    double g[9], f = 0.0;
+#pragma unroll
+    for (int i = 0; i < 9; i++) g[i] = 0.0;
+    int64_t m = 0;
+    for (int a = 0; a < 45; a++) hs[a * HS + lane] = 0.0;
+    for (int64_t t = lane; t < total; t += 32) {
+        const double* L = R + 9 * t;
+        if (isnan(L[0])) continue;
+        double d = eps;
+#pragma unroll
+        for (int i = 0; i < 9; i++) d = fma(xt[i], L[i], d);
+        const double r = 1.0 / d;
+        double b[9];
+#pragma unroll
+        for (int i = 0; i < 9; i++) {
+            g[i] = fma(L[i], r, g[i]);
+            b[i] = L[i] * r;
+        }
+        int a = 0;
+#pragma unroll
+        for (int i = 0; i < 9; i++)
+#pragma unroll
+            for (int j = i; j < 9; j++, a++) hs[a * HS + lane] = fma(b[i], b[j], hs[a * HS + lane]);
+        if (!diff) {
+            f += log(d);
+        } else {
+            double dc = eps, dl = 0.0;
+#pragma unroll
+            for (int i = 0; i < 9; i++) {
+                dc = fma(xc[i], L[i], dc);
+                dl = fma(xt[i] - xc[i], L[i], dl);
+            }
+            f += log1p(dl / dc);
+        }
+        m++;
+    }
+    for (int off = 16; off > 0; off >>= 1) {
+        f += __shfl_xor_sync(0xffffffffu, f, off);
+        m += __shfl_xor_sync(0xffffffffu, m, off);
+#pragma unroll
+        for (int i = 0; i < 9; i++) g[i] += __shfl_xor_sync(0xffffffffu, g[i], off);
+    }
+    __syncwarp();
+    for (int a = 0; a < 45; a++) {
+        double h = hs[a * HS + lane];
+        for (int off = 16; off > 0; off >>= 1) h += __shfl_xor_sync(0xffffffffu, h, off);
+        if (lane == 0) hs[a * HS + 32] += h;
+    }
+    __syncwarp();
+#pragma unroll
+    for (int i = 0; i < 9; i++) G[i] += g[i];
+    F += f;
+    n += m;
+}
+
+// The Hessian total (i, j) of the upper triangle, row-major.
+__device__ __forceinline__ double htotal(const double* hs, int i, int j) {
+    const int i0 = i < j ? i : j, j0 = i < j ? j : i;
+    return hs[(i0 * 9 - i0 * (i0 - 1) / 2 + (j0 - i0)) * HS + 32];
+}
+
+// The warp's 45 Hessian totals from the lanes' partials: hs[a * HS + 32].
+__device__ __forceinline__ void hessian_totals(double* hs, int lane) {
+    __syncwarp();
+    for (int a = 0; a < 45; a++) {
+        double h = hs[a * HS + lane];
+        for (int off = 16; off > 0; off >>= 1) h += __shfl_xor_sync(0xffffffffu, h, off);
+        if (lane == 0) hs[a * HS + 32] = h;
+    }
+    __syncwarp();
+}
 
 // f, g and this lane's Hessian row at x over the pair's rows (-(1/n) sum log(eps
 // + L.x), -(1/n) sum L r, (1/n) sum L L' r^2, r = 1/(eps + L.x)); n = rows
-// without a NaN.  hs: the lane's 45 upper-triangle sums in shared memory.
-__device__ __noinline__ int64_t soft_evaluate(const double* __restrict__ gl, int64_t n_sites, const int32_t* __restrict__ kept,
-                                        const double* __restrict__ kp, const double* __restrict__ kq, int64_t nk,
-                                        int64_t x, int64_t y, const double* xv, double eps, int lane, double* hs,
-                                        PairEval& ev) {
+// without a NaN.  hs: the warp's Hessian sums in shared memory; R, nm: the
+// pair's multi-allelic rows.
+__device__ __noinline__ int64_t soft_evaluate(const double* __restrict__ gl, int64_t n_sites,
+                                              const int32_t* __restrict__ kept, const double* __restrict__ kp,
+                                              const double* __restrict__ kq, int64_t nk, int64_t x, int64_t y,
+                                              const double* xv, double eps, int lane, double* hs, const double* R,
+                                              int64_t nm, PairEval& ev) {
     double f = 0.0, g[9];
 #pragma unroll
     for (int i = 0; i < 9; i++) g[i] = 0.0;
-    for (int a = 0; a < 45; a++) hs[a * 32 + lane] = 0.0;
+    for (int a = 0; a < 45; a++) hs[a * HS + lane] = 0.0;
     int64_t n = 0;
     for (int64_t k = lane; k < nk; k += 32) {
         const int64_t v = kept[k];
@@ -118,7 +341,7 @@ __device__ __noinline__ int64_t soft_evaluate(const double* __restrict__ gl, int
 #pragma unroll
         for (int i = 0; i < 9; i++)
 #pragma unroll
-            for (int j = i; j < 9; j++, a++) hs[a * 32 + lane] = fma(b[i], b[j], hs[a * 32 + lane]);
+            for (int j = i; j < 9; j++, a++) hs[a * HS + lane] = fma(b[i], b[j], hs[a * HS + lane]);
         n++;
     }
     // warp sums (fixed butterfly order)
@@ -128,28 +351,15 @@ __device__ __noinline__ int64_t soft_evaluate(const double* __restrict__ gl, int
 #pragma unroll
         for (int i = 0; i < 9; i++) g[i] += __shfl_xor_sync(0xffffffffu, g[i], off);
     }
-    __syncwarp();
-    for (int a = 0; a < 45; a++) {
-        double h = hs[a * 32 + lane];
-        for (int off = 16; off > 0; off >>= 1) h += __shfl_xor_sync(0xffffffffu, h, off);
-        if (lane == 0) hs[a * 32] = h;
-    }
-    __syncwarp();
+    hessian_totals(hs, lane);
+    if (nm > 0) soft_multi_add(R, nm, xv, xv, false, eps, lane, hs, g, f, n);
     const double dn = (double)n;
     ev.f = -f / dn;
 #pragma unroll
     for (int i = 0; i < 9; i++) ev.g[i] = -g[i] / dn;
     // lane i < 9 takes row i of H
 #pragma unroll
-    for (int j = 0; j < 9; j++) {
-        double h = 0.0;
-        if (lane < 9) {
-            const int i0 = lane < j ? lane : j, j0 = lane < j ? j : lane;
-            const int a = i0 * 9 - i0 * (i0 - 1) / 2 + (j0 - i0);
-            h = hs[a * 32] / dn;
-        }
-        ev.Hr[j] = h;
-    }
+    for (int j = 0; j < 9; j++) ev.Hr[j] = lane < 9 ? htotal(hs, lane, j) / dn : 0.0;
     __syncwarp();
     return n;
 }
@@ -178,13 +388,15 @@ __global__ void soft_pack32_kernel(const double* __restrict__ gl, int64_t n_samp
 
 // The FP32 evaluation (see the file comment) at xt; in a difference pass
 // (DIFF) the objective is f_old - (1/n) sum log(d / d_old) with d_old at xc.
-// hs: the lane's 45 FP64 Hessian sums in shared memory.  Returns n.  Not
-// inlined: the site loop gets the registers the pair's SQP state would hold.
+// hs: the warp's FP64 Hessian sums in shared memory; R, nm: the pair's
+// multi-allelic rows, added in FP64 after the lo correction of the biallelic
+// sums.  Returns n.  Not inlined: the site loop gets the registers the pair's
+// SQP state would hold.
 template <bool DIFF>
 __device__ __noinline__ int64_t soft_evaluate32(const float* __restrict__ g32, const float* __restrict__ p32,
                                                 const float* __restrict__ q32, int64_t nk, int64_t x, int64_t y,
                                                 const double* xt, const double* xc, double f_old, double eps,
-                                                int lane, double* hs, PairEval& ev) {
+                                                int lane, double* hs, const double* R, int64_t nm, PairEval& ev) {
     const bool diff = DIFF;
     float xh[9], sd[9];
     double lo[9];
@@ -200,7 +412,7 @@ __device__ __noinline__ int64_t soft_evaluate32(const float* __restrict__ g32, c
     for (int i = 0; i < 9; i++) { G[i] = 0.0; g[i] = 0.f; }
 #pragma unroll
     for (int a = 0; a < 45; a++) h[a] = 0.f;
-    for (int a = 0; a < 45; a++) hs[a * 32 + lane] = 0.0;
+    for (int a = 0; a < 45; a++) hs[a * HS + lane] = 0.0;
     const float* lx = g32 + x * nk * 3;
     const float* ly = g32 + y * nk * 3;
     const float e32 = (float)eps;
@@ -264,14 +476,14 @@ __device__ __noinline__ int64_t soft_evaluate32(const float* __restrict__ g32, c
         }
         if ((cnt & 31) == 0) {
 #pragma unroll
-            for (int a2 = 0; a2 < 45; a2++) { hs[a2 * 32 + lane] += (double)h[a2]; h[a2] = 0.f; }
+            for (int a2 = 0; a2 < 45; a2++) { hs[a2 * HS + lane] += (double)h[a2]; h[a2] = 0.f; }
         }
     }
 #pragma unroll
     for (int i = 0; i < 9; i++) G[i] += (double)g[i];
     F += (double)o;
 #pragma unroll
-    for (int a = 0; a < 45; a++) hs[a * 32 + lane] += (double)h[a];
+    for (int a = 0; a < 45; a++) hs[a * HS + lane] += (double)h[a];
     // warp sums (fixed butterfly order)
     for (int off = 16; off > 0; off >>= 1) {
         F += __shfl_xor_sync(0xffffffffu, F, off);
@@ -279,17 +491,7 @@ __device__ __noinline__ int64_t soft_evaluate32(const float* __restrict__ g32, c
 #pragma unroll
         for (int i = 0; i < 9; i++) G[i] += __shfl_xor_sync(0xffffffffu, G[i], off);
     }
-    __syncwarp();
-    for (int a = 0; a < 45; a++) {
-        double hv = hs[a * 32 + lane];
-        for (int off = 16; off > 0; off >>= 1) hv += __shfl_xor_sync(0xffffffffu, hv, off);
-        if (lane == 0) hs[a * 32] = hv;
-    }
-    __syncwarp();
-    auto Hsum = [&](int i, int j) {
-        const int i0 = i < j ? i : j, j0 = i < j ? j : i;
-        return hs[(i0 * 9 - i0 * (i0 - 1) / 2 + (j0 - i0)) * 32];
-    };
+    hessian_totals(hs, lane);
     // the lo parts of x to first order: sum log d gains sum_j lo_j G_j, and
     // G_i loses sum_j H_ij lo_j (a difference pass uses the step's FP32 values)
     double corr = 0.0;
@@ -300,15 +502,18 @@ __device__ __noinline__ int64_t soft_evaluate32(const float* __restrict__ g32, c
     for (int i = 0; i < 9; i++) {
         double s = 0.0;
 #pragma unroll
-        for (int j = 0; j < 9; j++) s = fma(Hsum(i, j), lo[j], s);
+        for (int j = 0; j < 9; j++) s = fma(htotal(hs, i, j), lo[j], s);
         Gc[i] = G[i] - s;
     }
+    // objective so far in natural-log units (direct: F counted log2 d)
+    double fsum = diff ? F : F * 0.69314718055994530942 + corr;
+    if (nm > 0) soft_multi_add(R, nm, xt, xc, diff, eps, lane, hs, Gc, fsum, n);
     const double dn = (double)n;
-    ev.f = diff ? f_old - F / dn : -(F * 0.69314718055994530942 + corr) / dn;
+    ev.f = diff ? f_old - fsum / dn : -fsum / dn;
 #pragma unroll
     for (int i = 0; i < 9; i++) ev.g[i] = -Gc[i] / dn;
 #pragma unroll
-    for (int j = 0; j < 9; j++) ev.Hr[j] = lane < 9 ? Hsum(lane, j) / dn : 0.0;
+    for (int j = 0; j < 9; j++) ev.Hr[j] = lane < 9 ? htotal(hs, lane, j) / dn : 0.0;
     __syncwarp();
     return n;
 }
@@ -322,10 +527,12 @@ __global__ void __launch_bounds__(SOFT_WARPS * 32, 3) soft_pairs_kernel(
     const double* __restrict__ gl, int64_t n_sites, const int32_t* __restrict__ kept, const double* __restrict__ kp,
     const double* __restrict__ kq, const float* __restrict__ g32, const float* __restrict__ p32,
     const float* __restrict__ q32, int prec64, int64_t nk, int64_t ns, int64_t n_rows, uint64_t iterations,
-    kg_output* out, unsigned long long* next, int* no_rows, unsigned long long* stats) {
-    __shared__ double hsm[SOFT_WARPS][45 * 32];
+    kg_output* out, unsigned long long* next, int* no_rows, unsigned long long* stats, SoftMultiDev M) {
+    __shared__ double hsm[SOFT_WARPS][45 * HS];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     double* hs = hsm[w];
+    // the warp's scratch for its pair's multi-allelic rows
+    double* R = M.total > 0 ? M.scratch + ((int64_t)blockIdx.x * SOFT_WARPS + w) * M.total * 9 : nullptr;
     const Tune tu = make_tune(iterations);
     unsigned long long c_gh = 0, c_f64 = 0, c_esc = 0, c_sites = 0, c_sites64 = 0;
     for (;;) {
@@ -346,6 +553,7 @@ __global__ void __launch_bounds__(SOFT_WARPS * 32, 3) soft_pairs_kernel(
         if (x == y) { xv[0] = 0.5; xv[6] = 0.5; }
         normalise9(xv);
         bool fp64 = prec64 != 0;
+        if (M.total > 0) soft_multi_build(M, x, y, lane, R);
         // one evaluation at xt: FP64, or FP32 (a difference pass relative to xc
         // and the objective f_old there when diff)
         PairEval ev;
@@ -354,11 +562,13 @@ __global__ void __launch_bounds__(SOFT_WARPS * 32, 3) soft_pairs_kernel(
             int64_t m;
             if (fp64) {
                 c_f64++;
-                m = soft_evaluate(gl, n_sites, kept, kp, kq, nk, x, y, xt, tu.epsilon, lane, hs, ev);
+                m = soft_evaluate(gl, n_sites, kept, kp, kq, nk, x, y, xt, tu.epsilon, lane, hs, R, M.total, ev);
                 c_sites64 += (unsigned long long)m;
             } else {
-                m = diff ? soft_evaluate32<true>(g32, p32, q32, nk, x, y, xt, xc, f_old, tu.epsilon, lane, hs, ev)
-                         : soft_evaluate32<false>(g32, p32, q32, nk, x, y, xt, xc, f_old, tu.epsilon, lane, hs, ev);
+                m = diff ? soft_evaluate32<true>(g32, p32, q32, nk, x, y, xt, xc, f_old, tu.epsilon, lane, hs, R,
+                                                 M.total, ev)
+                         : soft_evaluate32<false>(g32, p32, q32, nk, x, y, xt, xc, f_old, tu.epsilon, lane, hs, R,
+                                                  M.total, ev);
             }
             c_sites += (unsigned long long)m;
             return m;
@@ -453,9 +663,9 @@ __global__ void __launch_bounds__(SOFT_WARPS * 32, 3) soft_pairs_kernel(
 
 int soft_relatedness(const DevBuf& gl, int64_t n_samples, int64_t n_sites, int64_t ns, uint64_t iterations,
                      double maf, kg_output* d_out, cudaStream_t st, std::string& err, int64_t* n_kept, int precision,
-                     uint64_t* counters) {
+                     uint64_t* counters, const SoftMultiInput* multi, int64_t* multi_used) {
     if (!(maf >= 0.0)) maf = 1.0 / (2.0 * (double)n_samples);
-    DevBuf pf, qf, keep, idx, kp, kq, ctr, g32, p32, q32;
+    DevBuf pf, qf, keep, idx, kp, kq, ctr, g32, p32, q32, mgk, mgidx, mrows, mused, mscratch;
     KG_SOFT_TRY((cudaError_t)pf.reserve(sizeof(double) * n_sites));
     KG_SOFT_TRY((cudaError_t)qf.reserve(sizeof(double) * n_sites));
     KG_SOFT_TRY((cudaError_t)keep.reserve((size_t)n_sites));
@@ -480,13 +690,40 @@ int soft_relatedness(const DevBuf& gl, int64_t n_samples, int64_t n_sites, int64
         }
     const int64_t nk = (int64_t)ki.size();
     if (n_kept) *n_kept = nk;
-    if (nk == 0) {
+    // tri- and tetra-allelic sites: frequencies, remaining alleles, rows
+    SoftMultiDev M{};
+    M.n[0] = multi ? multi->n3 : 0;
+    M.n[1] = multi ? multi->n4 : 0;
+    M.gl[0] = multi ? multi->gl3 : nullptr;
+    M.gl[1] = multi ? multi->gl4 : nullptr;
+    M.total = M.n[0] + M.n[1];
+    unsigned long long mu[3] = {0, 0, 0};
+    if (M.total > 0) {
+        KG_SOFT_TRY((cudaError_t)mgk.reserve(sizeof(int32_t) * M.total));
+        KG_SOFT_TRY((cudaError_t)mgidx.reserve((size_t)MAXG * M.total));
+        KG_SOFT_TRY((cudaError_t)mrows.reserve(sizeof(double) * 9 * SOFT_MULTI_ROWS * (size_t)M.total));
+        KG_SOFT_TRY((cudaError_t)mused.reserve(sizeof(unsigned long long) * 3));
+        KG_SOFT_TRY(cudaMemsetAsync(mused.p, 0, sizeof(unsigned long long) * 3, st));
+        M.gk = mgk.as<int32_t>();
+        M.gidx = mgidx.as<uint8_t>();
+        M.rows = mrows.as<double>();
+        soft_multi_site_kernel<<<(unsigned)((M.total + 127) / 128), 128, 0, st>>>(
+            M, n_samples, maf, iterations, mgk.as<int32_t>(), mgidx.as<uint8_t>(), mrows.as<double>(),
+            mused.as<unsigned long long>());
+        KG_SOFT_TRY(cudaGetLastError());
+        KG_SOFT_TRY(cudaMemcpyAsync(mu, mused.p, sizeof(mu), cudaMemcpyDeviceToHost, st));
+        KG_SOFT_TRY(cudaStreamSynchronize(st));
+    }
+    if (multi_used)
+        for (int k = 0; k < 3; k++) multi_used[k] = (int64_t)mu[k];
+    if (nk == 0 && mu[0] + mu[1] + mu[2] == 0) {
         err = "no segregating site left after allele-frequency filtering";
         return KG_ENOSITES;
     }
-    KG_SOFT_TRY((cudaError_t)idx.reserve(sizeof(int32_t) * nk));
-    KG_SOFT_TRY((cudaError_t)kp.reserve(sizeof(double) * nk));
-    KG_SOFT_TRY((cudaError_t)kq.reserve(sizeof(double) * nk));
+    const int64_t nk1 = std::max<int64_t>(nk, 1);   // buffers exist even with no biallelic site
+    KG_SOFT_TRY((cudaError_t)idx.reserve(sizeof(int32_t) * nk1));
+    KG_SOFT_TRY((cudaError_t)kp.reserve(sizeof(double) * nk1));
+    KG_SOFT_TRY((cudaError_t)kq.reserve(sizeof(double) * nk1));
     KG_SOFT_TRY((cudaError_t)ctr.reserve(sizeof(unsigned long long) * 6 + sizeof(int)));
     KG_SOFT_TRY(cudaMemcpyAsync(idx.p, ki.data(), sizeof(int32_t) * nk, cudaMemcpyHostToDevice, st));
     KG_SOFT_TRY(cudaMemcpyAsync(kp.p, kpv.data(), sizeof(double) * nk, cudaMemcpyHostToDevice, st));
@@ -497,14 +734,16 @@ int soft_relatedness(const DevBuf& gl, int64_t n_samples, int64_t n_sites, int64
     int* no_rows = reinterpret_cast<int*>(next + 6);
     const bool fp64 = precision == KG_PREC_FP64;
     if (!fp64) {
-        KG_SOFT_TRY((cudaError_t)g32.reserve(sizeof(float) * 3 * (size_t)(n_samples * nk)));
-        KG_SOFT_TRY((cudaError_t)p32.reserve(sizeof(float) * nk));
-        KG_SOFT_TRY((cudaError_t)q32.reserve(sizeof(float) * nk));
+        KG_SOFT_TRY((cudaError_t)g32.reserve(sizeof(float) * 3 * (size_t)(n_samples * nk1)));
+        KG_SOFT_TRY((cudaError_t)p32.reserve(sizeof(float) * nk1));
+        KG_SOFT_TRY((cudaError_t)q32.reserve(sizeof(float) * nk1));
         const int64_t total = n_samples * nk;
-        const unsigned blocks = (unsigned)std::min<int64_t>((total + 255) / 256, 148 * 16);
-        soft_pack32_kernel<<<blocks, 256, 0, st>>>(gl.as<double>(), n_samples, n_sites, idx.as<int32_t>(),
-                                                   kp.as<double>(), kq.as<double>(), nk, g32.as<float>(),
-                                                   p32.as<float>(), q32.as<float>());
+        if (total > 0) {
+            const unsigned blocks = (unsigned)std::min<int64_t>((total + 255) / 256, 148 * 16);
+            soft_pack32_kernel<<<blocks, 256, 0, st>>>(gl.as<double>(), n_samples, n_sites, idx.as<int32_t>(),
+                                                       kp.as<double>(), kq.as<double>(), nk, g32.as<float>(),
+                                                       p32.as<float>(), q32.as<float>());
+        }
     }
     const int64_t rows = ns * (ns + 1) / 2;
     int dev = 0, sms = 148;
@@ -512,9 +751,14 @@ int soft_relatedness(const DevBuf& gl, int64_t n_samples, int64_t n_sites, int64
     KG_SOFT_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     int occ = 0;
     KG_SOFT_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, soft_pairs_kernel, SOFT_WARPS * 32, 0));
-    soft_pairs_kernel<<<(unsigned)(sms * std::max(1, occ)), SOFT_WARPS * 32, 0, st>>>(
+    const int64_t grid = (int64_t)sms * std::max(1, occ);
+    if (M.total > 0) {
+        KG_SOFT_TRY((cudaError_t)mscratch.reserve(sizeof(double) * 9 * (size_t)(grid * SOFT_WARPS * M.total)));
+        M.scratch = mscratch.as<double>();
+    }
+    soft_pairs_kernel<<<(unsigned)grid, SOFT_WARPS * 32, 0, st>>>(
         gl.as<double>(), n_sites, idx.as<int32_t>(), kp.as<double>(), kq.as<double>(), g32.as<float>(),
-        p32.as<float>(), q32.as<float>(), fp64 ? 1 : 0, nk, ns, rows, iterations, d_out, next, no_rows, stats);
+        p32.as<float>(), q32.as<float>(), fp64 ? 1 : 0, nk, ns, rows, iterations, d_out, next, no_rows, stats, M);
     KG_SOFT_TRY(cudaGetLastError());
     int h_no_rows = 0;
     unsigned long long hs[5] = {0, 0, 0, 0, 0};

@@ -94,3 +94,45 @@ def test_soft_fp32_and_fp64_forms(est, oracle, cohort):
     print(out)
     assert out["fp64"][1]["fp64_passes"] == out["fp64"][1]["gh_passes"] > 0
     assert out["fp32c"][1]["fp64_passes"] < out["fp32c"][1]["gh_passes"]
+
+
+def _soft_multi(g, al, rng, err=0.05):
+    """Tri- and tetra-allelic genotype indices (255 = missing) -> soft
+    likelihoods [samples, sites, G] per allele count (the called genotype 1,
+    the others uniform in [0, err)), NaN where missing."""
+    out = {}
+    for a in (3, 4):
+        sel = np.nonzero(al == a)[0]
+        ng = a * (a + 1) // 2
+        sub = g[:, sel]
+        gl = rng.uniform(0.0, err, sub.shape + (ng,))
+        for k in range(ng):
+            gl[..., k] = np.where(sub == k, 1.0, gl[..., k])
+        gl[sub == 255] = np.nan
+        out[a] = gl
+    return out
+
+
+def test_soft_multiallelic_sites_parity(est, oracle, cohort):
+    """Tri- and tetra-allelic sites with soft likelihoods (kg_load_likelihoods_
+    multiallelic) against the oracle's GL/PL path on the same likelihoods:
+    frequencies fitted over 2-4 alleles, maf cut, zero-frequency alleles
+    dropped, rows built from the remaining genotypes."""
+    rng = np.random.default_rng(12)
+    gl = soft_gl(cohort.codes, rng, err=0.08)                       # [sites, samples, 3]
+    g, al = synth.make_multiallelic(cohort.codes.shape[0], 300, 13, missing=0.02)
+    m = _soft_multi(g, al, rng)
+    ref, af = oracle.gl_relatedness(gl, gl3=np.ascontiguousarray(m[3].transpose(1, 0, 2)),
+                                    gl4=np.ascontiguousarray(m[4].transpose(1, 0, 2)))
+    nz = (af > 0).sum(1)
+    for prec in ("fp32c", "fp64"):
+        est.set_precision(prec)
+        est.load_likelihoods(np.ascontiguousarray(gl.transpose(1, 0, 2)))
+        est.load_likelihoods_multiallelic(m[3], 3)
+        est.load_likelihoods_multiallelic(m[4], 4)
+        rows = est.relatedness_gl()
+        st = est.run_stats()
+        print(prec, compare(rows, ref), st["sites_used"], st["fp64_pairs"])
+        assert st["sites_used"] == [int(np.sum(nz == 2)), int(np.sum(nz == 3)), int(np.sum(nz == 4))]
+    est.set_precision("fp32c")
+    assert st["sites_used"][1] > 0 and st["sites_used"][2] > 0
