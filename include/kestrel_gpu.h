@@ -372,6 +372,10 @@ int kg_vcf_codes(const kg_vcf *vcf, uint8_t *codes, double *af);
  * linear-scale likelihoods, n_samples x n_sites x 3 (sample-major, NaN where
  * missing), the input of kg_load_likelihoods; KG_ENOTFOUND otherwise. */
 int kg_vcf_likelihoods(const kg_vcf *vcf, double *gl);
+/* The same for the tri- (n_alleles 3, G = 6) or tetra-allelic (4, G = 10)
+ * records, in file order: n_samples x (counts[5] or counts[6]) x G, the input
+ * of kg_load_likelihoods_multiallelic; KG_ENOTFOUND when every row is one-hot. */
+int kg_vcf_likelihoods_multiallelic(const kg_vcf *vcf, int n_alleles, double *gl);
 /* The same codes packed as kg_load_genotypes_2bit takes them (2-bit codes and
  * the observed mask, rows of ceil(n_sites/16) and ceil(n_sites/32) words). */
 int kg_vcf_codes_2bit(const kg_vcf *vcf, uint32_t *codes2, uint32_t *observed);

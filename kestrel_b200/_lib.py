@@ -62,7 +62,7 @@ EXPORTS = ("kg_create", "kg_destroy", "kg_last_error", "kg_version", "kg_set_pre
            "kg_relatedness_batch", "kg_panel_load", "kg_submit", "kg_poll", "kg_wait",
            "kg_cancel", "kg_serving_stats", "kg_relatedness_noalloc", "kg_last_run_stats",
            "kg_fp32_peak", "kg_run_cli", "kg_vcf_read", "kg_vcf_error", "kg_vcf_info", "kg_vcf_codes",
-           "kg_vcf_codes_2bit", "kg_vcf_likelihoods", "kg_vcf_multiallelic", "kg_vcf_sample", "kg_vcf_free")
+           "kg_vcf_codes_2bit", "kg_vcf_likelihoods", "kg_vcf_likelihoods_multiallelic", "kg_vcf_multiallelic", "kg_vcf_sample", "kg_vcf_free")
 
 
 class KestrelError(RuntimeError):
@@ -124,6 +124,7 @@ def lib():
         "kg_vcf_multiallelic": ([P, P, P, P], i32),
         "kg_vcf_codes_2bit": ([P, P, P], i32),
         "kg_vcf_likelihoods": ([P, P], i32),
+        "kg_vcf_likelihoods_multiallelic": ([P, i32, P], i32),
         "kg_vcf_sample": ([P, i64], ctypes.c_char_p),
         "kg_vcf_free": ([P], None),
     }

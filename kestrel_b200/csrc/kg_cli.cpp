@@ -342,10 +342,7 @@ extern "C" int kg_run_cli(int argc, const char* const* argv) {
     const bool soft_path = o.field != 'T' && !vcf.gl.empty();
     if (soft_path) {
         log_info("%s likelihood entries are not one-hot: estimating from the soft likelihoods",
-                 std::to_string(vcf.soft));
-        if (vcf.n_multi > 0)
-            log_info("Skipped %s tri- or tetra-allelic sites (the soft-likelihood estimator takes biallelic sites)",
-                     std::to_string(vcf.n_multi));
+                 std::to_string(vcf.soft + vcf.multi_soft));
         if (o.af_info) {
             std::fprintf(stderr, "Error: allele frequencies from INFO/AF cannot be used with soft likelihoods\n");
             return 1;
@@ -381,12 +378,24 @@ extern "C" int kg_run_cli(int argc, const char* const* argv) {
     const ResourceTracker tracker;
     if (soft_path) {
         st = kg_load_likelihoods(ctx, vcf.gl.data(), ns, nv);
+        // tri- and tetra-allelic records: their likelihoods by allele count
+        for (int a = 3; a <= 4 && !st && vcf.n_multi > 0 && !vcf.mgl.empty(); a++) {
+            const int ng = a * (a + 1) / 2;
+            std::vector<int64_t> sel;
+            for (int64_t r = 0; r < vcf.n_multi; r++)
+                if (vcf.malleles[(size_t)r] == a) sel.push_back(r);
+            if (sel.empty()) continue;
+            const int64_t nk = (int64_t)sel.size();
+            std::vector<double> g((size_t)(ns * nk * ng));
+            for (int64_t s = 0; s < ns; s++)
+                for (int64_t k = 0; k < nk; k++)
+                    std::memcpy(g.data() + (s * nk + k) * ng,
+                                vcf.mgl.data() + ((size_t)s * vcf.n_multi + sel[(size_t)k]) * 10, sizeof(double) * ng);
+            st = kg_load_likelihoods_multiallelic(ctx, g.data(), ns, nk, a);
+        }
         if (!st) tracker.checkpoint();
         if (!st) st = kg_relatedness_gl(ctx, nsel, o.iterations, o.maf, out.data(), np, &nout);
     } else {
-        if (!o.cls && vcf.multi_soft > 0)
-            std::fprintf(stderr, "[WARN ] %llu tri- or tetra-allelic likelihood rows are not one-hot: their most "
-                                 "likely genotypes are used\n", (unsigned long long)vcf.multi_soft);
         // the reader's codes go up packed: 2 bits a call plus the observed mask
         std::vector<uint32_t> codes2((size_t)(ns * ((nv + 15) / 16))), observed((size_t)(ns * ((nv + 31) / 32)));
         kg::pack_2bit(vcf, o.threads, codes2.data(), observed.data());
@@ -407,7 +416,7 @@ extern "C" int kg_run_cli(int argc, const char* const* argv) {
     }
     if (!o.cls) {
         // the sites the ML estimate used after the frequency cut and the drop
-        // of zero-frequency alleles (src/wrapper.rs:321-324)
+        // of zero-frequency alleles (src/wrapper.rs:321-324; the soft path too)
         kg_run_stats rs{};
         if (kg_last_run_stats(ctx, &rs) == 0) {
             log_info("Identified %s di-allelic sites", std::to_string(rs.sites_used[0]));

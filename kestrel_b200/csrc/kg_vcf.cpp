@@ -295,13 +295,17 @@ bool parse_call(std::string_view v, char field, uint8_t& code, uint64_t& soft, d
 
 // Most likely genotype (VCF order) of a GL/PL value of ng likelihoods at a
 // tri- or tetra-allelic site, 255 when the value or an entry is missing; the
-// row counts as soft as in parse_call.  False when the value is not ng numbers.
-bool parse_like_index(std::string_view v, char field, int ng, uint8_t& g, uint64_t& soft) {
+// row counts as soft as in parse_call.  like (optional, ng values): the
+// linear-scale likelihoods as the reference's reader makes them (NaN when
+// missing).  False when the value is not ng numbers.
+bool parse_like_index(std::string_view v, char field, int ng, uint8_t& g, uint64_t& soft, double* like = nullptr) {
+    if (like)
+        for (int i = 0; i < ng; i++) like[i] = NAN;
     if (v == ".") {
         g = 255;
         return true;
     }
-    double ll[10];
+    double ll[10], raw[10];
     int k = 0;
     bool any_missing = false;
     size_t b = 0;
@@ -316,6 +320,7 @@ bool parse_like_index(std::string_view v, char field, int ng, uint8_t& g, uint64
                 double x = 0.0;
                 const auto r = std::from_chars(t.data(), t.data() + t.size(), x);
                 if (r.ec != std::errc() || r.ptr == t.data()) return false;
+                raw[k] = x;
                 ll[k++] = field == 'P' ? -x / 10.0 : x;   // PL = -10 log10 L, GL = log10 L
             }
             b = i + 1;
@@ -325,6 +330,20 @@ bool parse_like_index(std::string_view v, char field, int ng, uint8_t& g, uint64
     if (any_missing) {
         g = 255;
         return true;
+    }
+    if (like) {
+        // 10^(-PL/10); 10^(GL - max GL) with GL read at single precision
+        // (src/vcf.rs:325-420)
+        if (field == 'P') {
+            for (int i = 0; i < ng; i++) like[i] = std::pow(10.0, -raw[i] / 10.0);
+        } else {
+            double mx = -INFINITY, gv[10];
+            for (int i = 0; i < ng; i++) {
+                gv[i] = (double)(float)raw[i];
+                mx = std::max(mx, gv[i]);
+            }
+            for (int i = 0; i < ng; i++) like[i] = std::pow(10.0, gv[i] - mx);
+        }
     }
     int best = 0;
     for (int i = 1; i < ng; i++)
@@ -428,6 +447,7 @@ struct Chunk {
     uint64_t tri = 0, tetra = 0, tri_full = 0, tetra_full = 0, mincomplete = 0;
     uint64_t multi_dropped = 0;  // GT records with a malformed call after a missing one
     uint64_t msoft = 0;          // GL/PL rows of these records that are not one-hot
+    std::vector<double> mlrows;  // with likelihoods kept: records x samples x 10 (G used, NaN after)
     bool failed = false;
     uint64_t fail_rec = 0;       // 1-based record index within the chunk
     std::string fail_kind;       // message with %R for the global record number
@@ -545,7 +565,13 @@ void parse_chunk(Chunk& c, char field, bool af_info, size_t n_samples, bool want
             for (size_t k = 0; k < n_samples; k++) {
                 const std::string_view v = sample_value(s);
                 uint8_t g = 0;
-                const bool ok = field == 'T' ? parse_gt_index(v, n_bases, g) : parse_like_index(v, field, ng, g, c.msoft);
+                double* like = nullptr;
+                if (want_like && field != 'T') {
+                    if (k == 0) c.mlrows.resize(c.mlrows.size() + n_samples * 10, (double)NAN);
+                    like = c.mlrows.data() + c.mlrows.size() - (n_samples - k) * 10;
+                }
+                const bool ok = field == 'T' ? parse_gt_index(v, n_bases, g)
+                                             : parse_like_index(v, field, ng, g, c.msoft, like);
                 if (!ok) {
                     if (field == 'T' && missing) {
                         bad_after_missing = true;
@@ -780,7 +806,7 @@ int read_vcf(const std::string& path, char field, bool af_info, int threads, Vcf
     if (field != 'T') {
         bool any_soft = false, any_failed = false;
         for (auto& c : chunks) {
-            any_soft |= c.soft > 0;
+            any_soft |= c.soft > 0 || c.msoft > 0;
             any_failed |= c.failed;
         }
         if (any_soft && !any_failed) {
@@ -819,7 +845,9 @@ int read_vcf(const std::string& path, char field, bool af_info, int threads, Vcf
     out.codes.allocate((size_t)(nv * (int64_t)ns));
     transpose_chunks(threads, ns, nv, out.codes.data(), chunks,
                      [](const Chunk& c) { return std::make_pair(c.rows.data(), c.kept); });
-    if (field != 'T' && out.soft > 0) {
+    bool any_soft = out.soft > 0;
+    for (auto& c : chunks) any_soft |= c.msoft > 0;
+    if (field != 'T' && any_soft) {
         // sample-major likelihoods [s][v][3], each thread a range of samples
         out.gl.resize((size_t)(nv * (int64_t)ns * 3));
         std::vector<int64_t> first((size_t)chunks.size() + 1, 0);
@@ -849,6 +877,22 @@ int read_vcf(const std::string& path, char field, bool af_info, int threads, Vcf
         out.multi_incomplete += c.mincomplete;
         out.multi_dropped += c.multi_dropped;
         out.multi_soft += c.msoft;
+    }
+    if (field != 'T' && any_soft && out.n_multi > 0) {
+        // sample-major likelihoods [s][record][10], each thread a range of samples
+        const int64_t nm = out.n_multi;
+        out.mgl.resize((size_t)(nm * (int64_t)ns * 10));
+        std::vector<int64_t> first((size_t)chunks.size() + 1, 0);
+        for (size_t i = 0; i < chunks.size(); i++) first[i + 1] = first[i] + chunks[i].mkept;
+        parallel_for(threads, (int64_t)ns, [&](int, int64_t s0, int64_t s1) {
+            for (size_t i = 0; i < chunks.size(); i++) {
+                const double* lr = chunks[i].mlrows.data();
+                for (int64_t s = s0; s < s1; s++)
+                    for (int64_t v = 0; v < chunks[i].mkept; v++)
+                        std::memcpy(out.mgl.data() + ((size_t)s * nm + first[i] + v) * 10,
+                                    lr + ((size_t)v * ns + s) * 10, sizeof(double) * 10);
+            }
+        });
     }
     if (af_info) {
         out.af.reserve((size_t)(2 * nv));
@@ -962,6 +1006,24 @@ extern "C" int kg_vcf_likelihoods(const kg_vcf* v, double* gl) {
 extern "C" int kg_vcf_codes_2bit(const kg_vcf* v, uint32_t* codes2, uint32_t* observed) {
     if (!v || !codes2 || !observed) return KG_EINVAL;
     kg::pack_2bit(v->d, 0, codes2, observed);
+    return KG_OK;
+}
+
+extern "C" int kg_vcf_likelihoods_multiallelic(const kg_vcf* v, int n_alleles, double* gl) {
+    if (!v || (n_alleles != 3 && n_alleles != 4)) return KG_EINVAL;
+    if (v->d.mgl.empty()) return KG_ENOTFOUND;
+    if (!gl) return KG_OK;
+    const int ng = n_alleles * (n_alleles + 1) / 2;
+    const int64_t ns = (int64_t)v->d.samples.size(), nm = v->d.n_multi;
+    int64_t k = 0;
+    std::vector<int64_t> sel;
+    for (int64_t r = 0; r < nm; r++)
+        if (v->d.malleles[(size_t)r] == n_alleles) sel.push_back(r);
+    const int64_t nk = (int64_t)sel.size();
+    for (int64_t s = 0; s < ns; s++)
+        for (k = 0; k < nk; k++)
+            std::memcpy(gl + (s * nk + k) * ng, v->d.mgl.data() + ((size_t)s * nm + sel[(size_t)k]) * 10,
+                        sizeof(double) * ng);
     return KG_OK;
 }
 

@@ -55,6 +55,9 @@ struct VcfData {
     uint64_t multi_incomplete = 0;  // kept records with a missing call
     uint64_t multi_dropped = 0;     // GT records dropped: a malformed call after a missing one
     uint64_t multi_soft = 0;        // GL/PL likelihood rows of these records that are not one-hot
+    // GL/PL with a soft row: their linear-scale likelihoods, [s][record][10]
+    // (G used, NaN after and where missing); empty otherwise
+    std::vector<double> mgl;
     // GL/PL with a soft row: the linear-scale likelihoods, sample-major
     // gl[(s * n_sites + v) * 3 + g] (NaN where missing); empty otherwise
     std::vector<double> gl;

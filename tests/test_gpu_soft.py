@@ -136,3 +136,53 @@ def test_soft_multiallelic_sites_parity(est, oracle, cohort):
         assert st["sites_used"] == [int(np.sum(nz == 2)), int(np.sum(nz == 3)), int(np.sum(nz == 4))]
     est.set_precision("fp32c")
     assert st["sites_used"][1] > 0 and st["sites_used"][2] > 0
+
+
+def test_cli_soft_pl_with_multiallelic_records(oracle):
+    """The CLI on a soft PL VCF with tri- and tetra-allelic records: every
+    record's likelihoods go to the soft estimator (10^(-PL/10), as the
+    reference's reader makes them), against the oracle on the same arrays."""
+    import os
+    import subprocess
+    import tempfile
+    from .test_gpu_workloads import _read_tsv, _tsv_values
+    from .parity import check_values
+    from .test_vcf import py_likelihoods, soft_pl_text
+    rng = np.random.default_rng(21)
+    co = synth.make_cohort(22, 1200, seed=49, missing=0.02, name="cli-soft-multi")
+    text = soft_pl_text(co.codes, rng)
+    g, al = synth.make_multiallelic(22, 150, 50, missing=0.02)
+    pls = {3: [], 4: []}
+    lines = []
+    for v in range(g.shape[1]):
+        a = int(al[v])
+        ng = a * (a + 1) // 2
+        calls, row = [], []
+        for s in range(22):
+            if g[s, v] == 255:
+                calls.append(".")
+                row.append([np.nan] * ng)
+                continue
+            pl = rng.integers(5, 41, ng)
+            pl[int(g[s, v])] = 0
+            calls.append(",".join(str(int(x)) for x in pl))
+            row.append([10.0 ** (-float(x) / 10.0) for x in pl])
+        pls[a].append(row)
+        lines.append(f"2\t{v + 1}\t.\tA\t{'C,G' if a == 3 else 'C,G,T'}\t.\tPASS\t.\tPL\t" + "\t".join(calls))
+    text += "\n".join(lines) + "\n"
+    gl2 = py_likelihoods(text.split("\n2\t")[0] + "\n", "PL")          # [samples, sites, 3]
+    gl3 = np.array(pls[3])                                                # [sites, samples, 6]
+    gl4 = np.array(pls[4])
+    ref, _ = oracle.gl_relatedness(np.ascontiguousarray(gl2.transpose(1, 0, 2)), gl3=gl3, gl4=gl4)
+    cli = os.path.join(os.path.dirname(kb.__file__), "bin", "kestrel")
+    with tempfile.TemporaryDirectory() as td:
+        vcf = os.path.join(td, "in.vcf")
+        tsv = os.path.join(td, "out.tsv")
+        open(vcf, "w").write(text)
+        r = subprocess.run([cli, vcf, tsv, "-f", "PL"], capture_output=True, text=True, timeout=300)
+        assert r.returncode == 0, r.stderr
+        _, rows = _read_tsv(tsv)
+    assert "estimating from the soft likelihoods" in r.stderr
+    assert f"Found {len(pls[3])} tri-allelic sites" in r.stderr
+    assert len(rows) == len(ref)
+    print(check_values(*_tsv_values(rows), ref))
