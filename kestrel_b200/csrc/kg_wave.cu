@@ -355,35 +355,11 @@ __device__ __forceinline__ float4 lds4(uint32_t a) {
     return v;
 }
 
-// Running FP32 sums of per-stage partials, one per half, with the rounding
-// errors of both halves gathered in c (an FP32 compensated sum on the FMA
-// pipe instead of an FP32 -> FP64 conversion and an FP64 add per partial).
-// fast2sum_acc is Fast2Sum, exact while |s| >= |p|: the gradient terms of a
-// shape are all positive, so s outgrows each partial once the first stage
-// (added to s = 0, exactly) is in.  two_sum_acc is TwoSum, exact for either
-// sign: the objective terms.
-__device__ __forceinline__ void fast2sum_acc(float2& s, float& c, float2 p) {
-    const float2 t = add2(s, p);
-    const float2 e = add2(fma2(t, dup2(-1.0f), s), p);   // (s - t) + p
-    c += e.x + e.y;
-    s = t;
-}
-__device__ __forceinline__ void two_sum_acc(float2& s, float& c, float2 p) {
-    const float2 m1 = dup2(-1.0f);
-    const float2 t = add2(s, p);
-    const float2 bp = fma2(s, m1, t);                     // t - s
-    const float2 ap = fma2(bp, m1, t);                    // t - bp
-    const float2 e = add2(fma2(ap, m1, s), fma2(bp, m1, p));   // (s - ap) + (p - bp)
-    c += e.x + e.y;
-    s = t;
-}
-
 // One shape's FP32 list from the ring.  Stage i holds float4 128 i .. 128 i +
 // 127; lane l takes 128 i + 32 j + l (j = 0..3): 16 sites, in packed pairs
-// (Shape32x2), whose FP32 gradient and objective partials (8 sites per half)
-// join compensated FP32 running sums after every stage, promoted to FP64 once
-// per unit, and whose Hessian partials go to FP64 every HESS_STAGES stages
-// (64 sites per partial).  Only the list's last stage can
+// (Shape32x2), whose FP32 gradient and objective partials go to FP64 after
+// every stage (8 sites per partial) and whose Hessian partials go every
+// HESS_STAGES stages (64 sites per partial).  Only the list's last stage can
 // be partly filled; the others run without bounds tests.  L and every stage
 // start are 16-byte aligned (list starts are multiples of four entries); a
 // stage's copy rounds its size up to 16 bytes, which stays inside the slot's
@@ -399,12 +375,11 @@ __device__ __forceinline__ bool stream32_ring(const float* __restrict__ L, int64
     constexpr int NG = E::NG, NH = E::NH, GOFF = E::GOFF, HOFF = E::HOFF;
     E ev;
     ev.load(K, DIFF);
-    float2 gs[NG], fs = dup2(0.f);
-    float gc[NG], fc = 0.f;
+    double G[NG], F = 0.0;
     double* H = Hs + lane;
     float2 h[NH];
 #pragma unroll
-    for (int i = 0; i < NG; i++) { gs[i] = dup2(0.f); gc[i] = 0.f; }
+    for (int i = 0; i < NG; i++) G[i] = 0.0;
 #pragma unroll
     for (int i = 0; i < NH; i++) { H[32 * i] = 0.0; h[i] = dup2(0.f); }
     const int64_t n4 = len >> 2;
@@ -433,8 +408,9 @@ __device__ __forceinline__ bool stream32_ring(const float* __restrict__ L, int64
                 if (lane + 32 * j < rem) ev.template site4<DIFF>(lds4(b + 512 * j), g, o, h, j & 1);
         }
 #pragma unroll
-        for (int j = 0; j < NG; j++) fast2sum_acc(gs[j], gc[j], g[j]);
-        two_sum_acc(fs, fc, o);
+        for (int j = 0; j < NG; j++) { G[j] += (double)g[j].x; G[j] += (double)g[j].y; }
+        F += (double)o.x;
+        F += (double)o.y;
         if (i % HESS_STAGES == HESS_STAGES - 1) {
 #pragma unroll
             for (int j = 0; j < NH; j++) { H[32 * j] += (double)(h[j].x + h[j].y); h[j] = dup2(0.f); }
@@ -456,10 +432,7 @@ __device__ __forceinline__ bool stream32_ring(const float* __restrict__ L, int64
         }
         return false;
     }
-    double G[NG], Hf[NH];
-#pragma unroll
-    for (int j = 0; j < NG; j++) G[j] = ((double)gs[j].x + (double)gs[j].y) + (double)gc[j];
-    double F = ((double)fs.x + (double)fs.y) + (double)fc;
+    double Hf[NH];
 #pragma unroll
     for (int j = 0; j < NH; j++) Hf[j] = H[32 * j] + (double)(h[j].x + h[j].y);
     if (lane < (int)(len & 3)) {
