@@ -122,48 +122,4 @@ __host__ __device__ inline void allele2_frequencies(double n00, double n01, doub
                 iterations, maf, p, q);
 }
 
-// The same fit on soft likelihoods: l(s, g) gives sample s's likelihood of
-// genotype g (0/0, 0/1, 1/1; linear scale); a sample with a NaN is skipped.
-template <class L>
-__host__ __device__ inline void allele2_frequencies_soft(const L& l, int64_t n_samples, uint64_t iterations,
-                                                         double maf, double& p, double& q) {
-    const double eps = make_tune(iterations).epsilon;
-    auto obj = [&](double x0, double x1) {
-        double acc = 0.0, n = 0.0;
-        const double w0 = x0 * x0, w1 = 2.0 * x0 * x1, w2 = x1 * x1;
-        for (int64_t s = 0; s < n_samples; s++) {
-            const double l0 = l(s, 0), l1 = l(s, 1), l2 = l(s, 2);
-            if (isnan(l0) || isnan(l1) || isnan(l2)) continue;
-            const double d = fma(w2, l2, fma(w1, l1, fma(w0, l0, eps)));
-            acc += log(d);
-            n += 1.0;
-        }
-        return -acc / n;
-    };
-    auto gh = [&](double x0, double x1, double& g0, double& g1, double& h00, double& h01, double& h11) {
-        double zg0 = 0.0, zg1 = 0.0, z00 = 0.0, z01 = 0.0, z11 = 0.0, n = 0.0;
-        for (int64_t s = 0; s < n_samples; s++) {
-            const double l0 = l(s, 0), l1 = l(s, 1), l2 = l(s, 2);
-            if (isnan(l0) || isnan(l1) || isnan(l2)) continue;
-            const double lx0 = fma(l1, x1, fma(l0, x0, 0.0));
-            const double lx1 = fma(l2, x1, fma(l1, x0, 0.0));
-            const double d = fma(x1, lx1, fma(x0, lx0, eps));
-            const double inv = 1.0 / d;
-            const double a0 = lx0 * inv, a1 = lx1 * inv;
-            zg0 += a0;
-            zg1 += a1;
-            z00 += 2.0 * a0 * a0 - l0 * inv;
-            z01 += 2.0 * a0 * a1 - l1 * inv;
-            z11 += 2.0 * a1 * a1 - l2 * inv;
-            n += 1.0;
-        }
-        g0 = -2.0 * zg0 / n;
-        g1 = -2.0 * zg1 / n;
-        h00 = 2.0 * z00 / n;
-        h01 = 2.0 * z01 / n;
-        h11 = 2.0 * z11 / n;
-    };
-    allele2_fit(obj, gh, iterations, maf, p, q);
-}
-
 }  // namespace kg

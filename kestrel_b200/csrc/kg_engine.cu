@@ -69,7 +69,7 @@ size_t Cohort::device_bytes() const {
            site_of.bytes + planes.bytes + cls_q.bytes + cls_part.bytes + mg.bytes + malleles.bytes + maf.bytes +
            mfreq.bytes + mkeep.bytes + mcount.bytes + mpart.bytes + cmulti.bytes + mgT.bytes + ml_keep.bytes +
            ml_nrows.bytes + ml_kidx.bytes + ml_rbase.bytes + ml_remap.bytes + ml_redf.bytes + ml_count.bytes +
-           ml_site.bytes + ml_orig.bytes + ml_kremap.bytes + ml_rows.bytes + ml_gr.bytes + ml_obs.bytes;
+           ml_site.bytes + ml_orig.bytes + ml_kremap.bytes + ml_rows.bytes + ml_rows32.bytes + ml_gr.bytes + ml_obs.bytes;
 }
 
 const char* engine_version() { return "kestrel-b200 0.1.0 (sm_100a)"; }
@@ -827,6 +827,7 @@ CohortDev make_cohort_dev(const PairJob& jb, uint64_t iterations) {
     d.ml_obs = ml ? pn.ml_obs.as<uint32_t>() : nullptr;
     d.ml_site = ml ? pn.ml_site.as<int2>() : nullptr;
     d.ml_rows = ml ? pn.ml_rows.as<double>() : nullptr;
+    d.ml_rows32 = ml ? pn.ml_rows32.as<float4>() : nullptr;
     d.ml_nk = ml ? (int32_t)pn.ml_nk : 0;
     d.ml_stride = ml ? (int32_t)pn.ml_stride : 0;
     return d;

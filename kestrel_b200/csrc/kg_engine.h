@@ -101,6 +101,7 @@ struct Cohort {
     DevBuf ml_orig;            // int32 per kept site: loaded site index
     DevBuf ml_kremap;          // uint8 [kept][10]: original genotype -> reduced genotype or ML_ZERO_ROW
     DevBuf ml_rows;            // double [rows][9]: m[g'x][g'y] of every kept site
+    DevBuf ml_rows32;          // float [rows][12]: the same rows in FP32, zero-padded to three float4
     DevBuf ml_gr;              // uint8 [n_samples][ml_stride]: reduced genotype, ML_ZERO_ROW or ML_MISSING
     DevBuf ml_obs;             // uint32 [n_samples][ml_stride / 32]: called at the kept site
     size_t device_bytes() const;

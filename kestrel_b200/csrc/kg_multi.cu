@@ -19,6 +19,7 @@
 // Device layout after preparation (kept sites k = 0 .. nk - 1, in site order):
 //   ml_site[k]  = {first row of the site's table, G' genotypes}
 //   ml_rows     = FP64 rows m[g'x][g'y] (9 values), G' x G' per site
+//   ml_rows32   = the same rows in FP32, 12 floats each (three float4)
 //   ml_gr[s][k] = sample s's reduced genotype (0 .. G' - 1), ML_ZERO_ROW or
 //                 ML_MISSING, rows of ml_stride bytes
 //   ml_obs[s][w] = bit k % 32 of word k / 32 set when sample s is called at k
@@ -156,7 +157,7 @@ __global__ void ml_compact_kernel(const int32_t* __restrict__ keep, const int32_
                                   const int32_t* __restrict__ rbase, const uint8_t* __restrict__ remap,
                                   const double* __restrict__ redf, int64_t n_multi, int2* __restrict__ site,
                                   int32_t* __restrict__ orig, uint8_t* __restrict__ kremap,
-                                  double* __restrict__ rows) {
+                                  double* __restrict__ rows, float* __restrict__ rows32) {
     const int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (v >= n_multi || !keep[v]) return;
     const int k = kidx[v];
@@ -173,7 +174,9 @@ __global__ void ml_compact_kernel(const int32_t* __restrict__ keep, const int32_
         for (int gy = 0; gy < gk; gy++) {
             int a, b;
             genotype_alleles(gy, a, b);
+            const int64_t row = (int64_t)rbase[v] + gx * gk + gy;
             iis_row(i, j, a, b, f0, f1, f2, f3, R + 9 * (gx * gk + gy));
+            for (int e = 0; e < 12; e++) rows32[12 * row + e] = e < 9 ? (float)rows[9 * row + e] : 0.f;
         }
     }
 }
@@ -240,12 +243,13 @@ int prepare_ml_multi(Cohort& c, bool have_af, double maf, uint64_t iterations, c
     KG_MULTI_TRY((cudaError_t)c.ml_orig.reserve(sizeof(int32_t) * nk));
     KG_MULTI_TRY((cudaError_t)c.ml_kremap.reserve((size_t)MAXG * nk));
     KG_MULTI_TRY((cudaError_t)c.ml_rows.reserve(sizeof(double) * 9 * nrows));
+    KG_MULTI_TRY((cudaError_t)c.ml_rows32.reserve(sizeof(float) * 12 * nrows));
     KG_MULTI_TRY((cudaError_t)c.ml_gr.reserve((size_t)(ns * stride)));
     KG_MULTI_TRY((cudaError_t)c.ml_obs.reserve(sizeof(uint32_t) * ns * (stride / 32)));
     ml_compact_kernel<<<(unsigned)cdiv(n, 128), 128, 0, st>>>(
         c.ml_keep.as<int32_t>(), c.ml_kidx.as<int32_t>(), c.ml_rbase.as<int32_t>(), c.ml_remap.as<uint8_t>(),
         c.ml_redf.as<double>(), n, c.ml_site.as<int2>(), c.ml_orig.as<int32_t>(), c.ml_kremap.as<uint8_t>(),
-        c.ml_rows.as<double>());
+        c.ml_rows.as<double>(), c.ml_rows32.as<float>());
     const dim3 cg((unsigned)cdiv(stride, 256), (unsigned)std::min<int64_t>(ns, 65535));
     ml_codes_kernel<<<cg, 256, 0, st>>>(c.mg.as<uint8_t>(), ns, n, c.ml_orig.as<int32_t>(), c.ml_kremap.as<uint8_t>(),
                                         cnt + 1, stride, c.ml_gr.as<uint8_t>(), c.ml_obs.as<uint32_t>());

@@ -115,6 +115,7 @@ __global__ void noalloc_table_kernel(kg::CohortDev* table, const uint2* planes, 
     d.ml_obs = nullptr;
     d.ml_site = nullptr;
     d.ml_rows = nullptr;
+    d.ml_rows32 = nullptr;
     d.ml_nk = 0;
     d.ml_stride = 0;
     *table = d;

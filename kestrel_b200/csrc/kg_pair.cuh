@@ -80,6 +80,7 @@ struct CohortDev {
     const uint32_t* ml_obs;  // [samples][ml_stride / 32] called bits
     const int2* ml_site;     // per kept site: {first row, reduced genotypes G'}
     const double* ml_rows;   // [rows][9] m[g'x][g'y]
+    const float4* ml_rows32; // [rows][3] the same rows in FP32 (9 values and 3 zeros)
     int32_t ml_nk;           // kept sites
     int32_t ml_stride;       // bytes per sample row of ml_gr (a multiple of 32)
 };

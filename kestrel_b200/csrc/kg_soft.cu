@@ -6,8 +6,9 @@
 //
 // Layout: biallelic likelihoods double [sample][site][3] (0/0, 0/1, 1/1;
 // linear scale; a NaN marks a missing sample) as loaded; the kept sites'
-// likelihoods are also packed as FP32 [sample][kept site][3] (all three NaN
-// when missing).  Tri- and tetra-allelic sites: double [sample][site][6] and
+// likelihoods are also packed as FP32 [sample][kept site] float4 records
+// (the three likelihoods and a zero; all three NaN when missing), beside the
+// kept sites' FP32 (REF, ALT) frequency pairs.  Tri- and tetra-allelic sites: double [sample][site][6] and
 // [sample][site][10] in the VCF genotype order.
 //
 // A warp per pair, lanes over the kept sites; the SQP itself is FP64.  Its
@@ -59,24 +60,74 @@ namespace kg {
 
 // Thread per site: frequencies (REF, ALT) and the keep flag (both non-zero
 // after the maf cut).  Adjacent threads read adjacent sites of a sample.
+__device__ __forceinline__ double warp_allsum(double v) {
+    // butterfly: every lane adds the same two partials at every level, so all
+    // lanes end with the same bits
+    for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+    return v;
+}
+
+// Warp per site: the HWE SQP of the site's frequencies with the samples over
+// the lanes (the sums of src/mixture.rs's objective and derivatives reduced
+// across the warp; every lane then runs the same solver steps on the same
+// values).
 __global__ void soft_freq_kernel(const double* __restrict__ gl, int64_t n_samples, int64_t n_sites, double maf,
                                  uint64_t iterations, double* __restrict__ pf, double* __restrict__ qf,
                                  uint8_t* __restrict__ keep) {
-    const int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x & 31;
+    const int64_t v = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     if (v >= n_sites) return;
-    int64_t called = 0;
-    for (int64_t s = 0; s < n_samples; s++) {
-        const double* r = gl + (s * n_sites + v) * 3;
+    const double eps = make_tune(iterations).epsilon;
+    auto rowp = [&](int64_t s) { return gl + (s * n_sites + v) * 3; };
+    double called = 0.0;
+    for (int64_t s = lane; s < n_samples; s += 32) {
+        const double* r = rowp(s);
         called += !(isnan(r[0]) || isnan(r[1]) || isnan(r[2]));
     }
+    called = warp_allsum(called);
     double p = 0.0, q = 0.0;
-    if (called) {
-        auto l = [&](int64_t s, int g) { return gl[(s * n_sites + v) * 3 + g]; };
-        allele2_frequencies_soft(l, n_samples, iterations, maf, p, q);
+    if (called > 0.0) {
+        auto obj = [&](double x0, double x1) {
+            double acc = 0.0;
+            const double w0 = x0 * x0, w1 = 2.0 * x0 * x1, w2 = x1 * x1;
+            for (int64_t s = lane; s < n_samples; s += 32) {
+                const double* r = rowp(s);
+                const double l0 = r[0], l1 = r[1], l2 = r[2];
+                if (isnan(l0) || isnan(l1) || isnan(l2)) continue;
+                acc += log(fma(w2, l2, fma(w1, l1, fma(w0, l0, eps))));
+            }
+            return -warp_allsum(acc) / called;
+        };
+        auto gh = [&](double x0, double x1, double& g0, double& g1, double& h00, double& h01, double& h11) {
+            double zg0 = 0.0, zg1 = 0.0, z00 = 0.0, z01 = 0.0, z11 = 0.0;
+            for (int64_t s = lane; s < n_samples; s += 32) {
+                const double* r = rowp(s);
+                const double l0 = r[0], l1 = r[1], l2 = r[2];
+                if (isnan(l0) || isnan(l1) || isnan(l2)) continue;
+                const double lx0 = fma(l1, x1, fma(l0, x0, 0.0));
+                const double lx1 = fma(l2, x1, fma(l1, x0, 0.0));
+                const double d = fma(x1, lx1, fma(x0, lx0, eps));
+                const double inv = 1.0 / d;
+                const double a0 = lx0 * inv, a1 = lx1 * inv;
+                zg0 += a0;
+                zg1 += a1;
+                z00 += 2.0 * a0 * a0 - l0 * inv;
+                z01 += 2.0 * a0 * a1 - l1 * inv;
+                z11 += 2.0 * a1 * a1 - l2 * inv;
+            }
+            g0 = -2.0 * warp_allsum(zg0) / called;
+            g1 = -2.0 * warp_allsum(zg1) / called;
+            h00 = 2.0 * warp_allsum(z00) / called;
+            h01 = 2.0 * warp_allsum(z01) / called;
+            h11 = 2.0 * warp_allsum(z11) / called;
+        };
+        allele2_fit(obj, gh, iterations, maf, p, q);
     }
-    pf[v] = p;
-    qf[v] = q;
-    keep[v] = (p > 0.0 && q > 0.0) ? 1 : 0;
+    if (lane == 0) {
+        pf[v] = p;
+        qf[v] = q;
+        keep[v] = (p > 0.0 && q > 0.0) ? 1 : 0;
+    }
 }
 
 constexpr int SOFT_WARPS = 4;
@@ -368,21 +419,16 @@ __device__ __noinline__ int64_t soft_evaluate(const double* __restrict__ gl, int
 // for a missing sample, and the kept frequencies as FP32.
 __global__ void soft_pack32_kernel(const double* __restrict__ gl, int64_t n_samples, int64_t n_sites,
                                    const int32_t* __restrict__ kept, const double* __restrict__ kp,
-                                   const double* __restrict__ kq, int64_t nk, float* __restrict__ g32,
-                                   float* __restrict__ p32, float* __restrict__ q32) {
+                                   const double* __restrict__ kq, int64_t nk, float4* __restrict__ g32,
+                                   float2* __restrict__ pq32) {
     const int64_t total = n_samples * nk;
     for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
         const int64_t s = t / nk, k = t - s * nk;
         const double* r = gl + (s * n_sites + kept[k]) * 3;
         const bool miss = isnan(r[0]) || isnan(r[1]) || isnan(r[2]);
-        float* o = g32 + t * 3;
-        o[0] = miss ? CUDART_NAN_F : (float)r[0];
-        o[1] = miss ? CUDART_NAN_F : (float)r[1];
-        o[2] = miss ? CUDART_NAN_F : (float)r[2];
-        if (s == 0) {
-            p32[k] = (float)kp[k];
-            q32[k] = (float)kq[k];
-        }
+        g32[t] = miss ? make_float4(CUDART_NAN_F, CUDART_NAN_F, CUDART_NAN_F, 0.f)
+                      : make_float4((float)r[0], (float)r[1], (float)r[2], 0.f);
+        if (s == 0) pq32[k] = make_float2((float)kp[k], (float)kq[k]);
     }
 }
 
@@ -393,17 +439,15 @@ __global__ void soft_pack32_kernel(const double* __restrict__ gl, int64_t n_samp
 // sums.  Returns n.  Not inlined: the site loop gets the registers the pair's
 // SQP state would hold.
 template <bool DIFF>
-__device__ __noinline__ int64_t soft_evaluate32(const float* __restrict__ g32, const float* __restrict__ p32,
-                                                const float* __restrict__ q32, int64_t nk, int64_t x, int64_t y,
+__device__ __noinline__ int64_t soft_evaluate32(const float4* __restrict__ g32, const float2* __restrict__ pq32,
+                                                int64_t nk, int64_t x, int64_t y,
                                                 const double* xt, const double* xc, double f_old, double eps,
                                                 int lane, double* hs, const double* R, int64_t nm, PairEval& ev) {
     const bool diff = DIFF;
     float xh[9], sd[9];
-    double lo[9];
 #pragma unroll
     for (int i = 0; i < 9; i++) {
         xh[i] = (float)xt[i];
-        lo[i] = xt[i] - (double)xh[i];
         sd[i] = DIFF ? (float)(xt[i] - xc[i]) : 0.f;
     }
     double G[9], F = 0.0;
@@ -413,16 +457,21 @@ __device__ __noinline__ int64_t soft_evaluate32(const float* __restrict__ g32, c
 #pragma unroll
     for (int a = 0; a < 45; a++) h[a] = 0.f;
     for (int a = 0; a < 45; a++) hs[a * HS + lane] = 0.0;
-    const float* lx = g32 + x * nk * 3;
-    const float* ly = g32 + y * nk * 3;
+    const float4* lx = g32 + x * nk;
+    const float4* ly = g32 + y * nk;
     const float e32 = (float)eps;
+    const int nk32 = (int)nk;
     int64_t n = 0;
     int cnt = 0;
-    for (int64_t k = lane; k < nk; k += 32) {
-        const float X0 = lx[3 * k], X1 = lx[3 * k + 1], X2 = lx[3 * k + 2];
-        const float Y0 = ly[3 * k], Y1 = ly[3 * k + 1], Y2 = ly[3 * k + 2];
+    // the next site's records are loaded while this one is evaluated
+    float4 X = make_float4(0.f, 0.f, 0.f, 0.f), Y = X;
+    float2 PQ = make_float2(0.f, 0.f);
+    if (lane < nk32) { X = lx[lane]; Y = ly[lane]; PQ = pq32[lane]; }
+    for (int k = lane; k < nk32; k += 32) {
+        const float X0 = X.x, X1 = X.y, X2 = X.z, Y0 = Y.x, Y1 = Y.y, Y2 = Y.z;
+        const float p = PQ.x, q = PQ.y;
+        if (k + 32 < nk32) { X = lx[k + 32]; Y = ly[k + 32]; PQ = pq32[k + 32]; }
         if (isnan(X0) || isnan(Y0)) continue;   // a missing sample has all three NaN
-        const float p = p32[k], q = q32[k];
         // L = sum over (gx, gy) of GLx(gx) GLy(gy) m(gx, gy), the nine rows of
         // the biallelic conditional table (cls_row) gathered by entry
         const float A = X0 * Y0, B = X2 * Y2, C = X0 * Y2, D = X2 * Y0, E = X0 * Y1;
@@ -476,7 +525,11 @@ __device__ __noinline__ int64_t soft_evaluate32(const float* __restrict__ g32, c
         }
         if ((cnt & 31) == 0) {
 #pragma unroll
-            for (int a2 = 0; a2 < 45; a2++) { hs[a2 * HS + lane] += (double)h[a2]; h[a2] = 0.f; }
+            for (int a2 = 0; a2 < 45; a2++) {
+                hs[a2 * HS + lane] += (double)h[a2];
+                h[a2] = 0.f;
+                asm volatile("" ::: "memory");   // one read-modify-write at a time: no register peak
+            }
         }
     }
 #pragma unroll
@@ -494,6 +547,9 @@ __device__ __noinline__ int64_t soft_evaluate32(const float* __restrict__ g32, c
     hessian_totals(hs, lane);
     // the lo parts of x to first order: sum log d gains sum_j lo_j G_j, and
     // G_i loses sum_j H_ij lo_j (a difference pass uses the step's FP32 values)
+    double lo[9];
+#pragma unroll
+    for (int j = 0; j < 9; j++) lo[j] = xt[j] - (double)xh[j];
     double corr = 0.0;
 #pragma unroll
     for (int j = 0; j < 9; j++) corr = fma(lo[j], G[j], corr);
@@ -525,8 +581,7 @@ __device__ __noinline__ int64_t soft_evaluate32(const float* __restrict__ g32, c
 // evaluations), [4] of them in FP64.
 __global__ void __launch_bounds__(SOFT_WARPS * 32, 3) soft_pairs_kernel(
     const double* __restrict__ gl, int64_t n_sites, const int32_t* __restrict__ kept, const double* __restrict__ kp,
-    const double* __restrict__ kq, const float* __restrict__ g32, const float* __restrict__ p32,
-    const float* __restrict__ q32, int prec64, int64_t nk, int64_t ns, int64_t n_rows, uint64_t iterations,
+    const double* __restrict__ kq, const float4* __restrict__ g32, const float2* __restrict__ pq32, int prec64, int64_t nk, int64_t ns, int64_t n_rows, uint64_t iterations,
     kg_output* out, unsigned long long* next, int* no_rows, unsigned long long* stats, SoftMultiDev M) {
     __shared__ double hsm[SOFT_WARPS][45 * HS];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -565,9 +620,9 @@ __global__ void __launch_bounds__(SOFT_WARPS * 32, 3) soft_pairs_kernel(
                 m = soft_evaluate(gl, n_sites, kept, kp, kq, nk, x, y, xt, tu.epsilon, lane, hs, R, M.total, ev);
                 c_sites64 += (unsigned long long)m;
             } else {
-                m = diff ? soft_evaluate32<true>(g32, p32, q32, nk, x, y, xt, xc, f_old, tu.epsilon, lane, hs, R,
+                m = diff ? soft_evaluate32<true>(g32, pq32, nk, x, y, xt, xc, f_old, tu.epsilon, lane, hs, R,
                                                  M.total, ev)
-                         : soft_evaluate32<false>(g32, p32, q32, nk, x, y, xt, xc, f_old, tu.epsilon, lane, hs, R,
+                         : soft_evaluate32<false>(g32, pq32, nk, x, y, xt, xc, f_old, tu.epsilon, lane, hs, R,
                                                   M.total, ev);
             }
             c_sites += (unsigned long long)m;
@@ -665,11 +720,11 @@ int soft_relatedness(const DevBuf& gl, int64_t n_samples, int64_t n_sites, int64
                      double maf, kg_output* d_out, cudaStream_t st, std::string& err, int64_t* n_kept, int precision,
                      uint64_t* counters, const SoftMultiInput* multi, int64_t* multi_used) {
     if (!(maf >= 0.0)) maf = 1.0 / (2.0 * (double)n_samples);
-    DevBuf pf, qf, keep, idx, kp, kq, ctr, g32, p32, q32, mgk, mgidx, mrows, mused, mscratch;
+    DevBuf pf, qf, keep, idx, kp, kq, ctr, g32, pq32, mgk, mgidx, mrows, mused, mscratch;
     KG_SOFT_TRY((cudaError_t)pf.reserve(sizeof(double) * n_sites));
     KG_SOFT_TRY((cudaError_t)qf.reserve(sizeof(double) * n_sites));
     KG_SOFT_TRY((cudaError_t)keep.reserve((size_t)n_sites));
-    soft_freq_kernel<<<(unsigned)((n_sites + 127) / 128), 128, 0, st>>>(gl.as<double>(), n_samples, n_sites, maf,
+    soft_freq_kernel<<<(unsigned)((n_sites + 3) / 4), 128, 0, st>>>(gl.as<double>(), n_samples, n_sites, maf,
                                                                         iterations, pf.as<double>(), qf.as<double>(),
                                                                         keep.as<uint8_t>());
     KG_SOFT_TRY(cudaGetLastError());
@@ -734,15 +789,14 @@ int soft_relatedness(const DevBuf& gl, int64_t n_samples, int64_t n_sites, int64
     int* no_rows = reinterpret_cast<int*>(next + 6);
     const bool fp64 = precision == KG_PREC_FP64;
     if (!fp64) {
-        KG_SOFT_TRY((cudaError_t)g32.reserve(sizeof(float) * 3 * (size_t)(n_samples * nk1)));
-        KG_SOFT_TRY((cudaError_t)p32.reserve(sizeof(float) * nk1));
-        KG_SOFT_TRY((cudaError_t)q32.reserve(sizeof(float) * nk1));
+        KG_SOFT_TRY((cudaError_t)g32.reserve(sizeof(float4) * (size_t)(n_samples * nk1)));
+        KG_SOFT_TRY((cudaError_t)pq32.reserve(sizeof(float2) * nk1));
         const int64_t total = n_samples * nk;
         if (total > 0) {
             const unsigned blocks = (unsigned)std::min<int64_t>((total + 255) / 256, 148 * 16);
             soft_pack32_kernel<<<blocks, 256, 0, st>>>(gl.as<double>(), n_samples, n_sites, idx.as<int32_t>(),
-                                                       kp.as<double>(), kq.as<double>(), nk, g32.as<float>(),
-                                                       p32.as<float>(), q32.as<float>());
+                                                       kp.as<double>(), kq.as<double>(), nk, g32.as<float4>(),
+                                                       pq32.as<float2>());
         }
     }
     const int64_t rows = ns * (ns + 1) / 2;
@@ -757,8 +811,8 @@ int soft_relatedness(const DevBuf& gl, int64_t n_samples, int64_t n_sites, int64
         M.scratch = mscratch.as<double>();
     }
     soft_pairs_kernel<<<(unsigned)grid, SOFT_WARPS * 32, 0, st>>>(
-        gl.as<double>(), n_sites, idx.as<int32_t>(), kp.as<double>(), kq.as<double>(), g32.as<float>(),
-        p32.as<float>(), q32.as<float>(), fp64 ? 1 : 0, nk, ns, rows, iterations, d_out, next, no_rows, stats, M);
+        gl.as<double>(), n_sites, idx.as<int32_t>(), kp.as<double>(), kq.as<double>(), g32.as<float4>(),
+        pq32.as<float2>(), fp64 ? 1 : 0, nk, ns, rows, iterations, d_out, next, no_rows, stats, M);
     KG_SOFT_TRY(cudaGetLastError());
     int h_no_rows = 0;
     unsigned long long hs[5] = {0, 0, 0, 0, 0};

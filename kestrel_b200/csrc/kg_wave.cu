@@ -711,15 +711,192 @@ extern "C" __global__ void __launch_bounds__(128, PASS_MIN_BLOCKS) wave_pass_ker
 // ------------------------------------------------- tri- and tetra-allelic
 
 // The sums of the ML path's tri- and tetra-allelic sites for every slot with
-// a pending ML pass, in FP64: per kept site with both samples called, the row
-// L = m[g'x][g'y] from the site's table, d = eps + L.xt, and the terms L/d
+// a pending ML pass: per kept site with both samples called, the row L =
+// m[g'x][g'y] from the site's table, d = eps + L.xt, and the terms L/d
 // (gradient), (L/d)(L/d)' (Hessian) and the objective term (log d, or for a
-// difference pass log(d / d_old) with d_old = eps + L.xc); a call that uses a
+// difference pass log(d / d_old) with d_old at xc); a call that uses a
 // dropped allele gives the site a row of zeros (objective term log eps, or 0
 // in a difference pass).  Work units are (slot of the pass list, ML_CHUNK
 // sites), strided over the grid's warps; lanes stride over the unit's sites,
 // and the unit's sums go to ml_partial in a fixed order.
-extern "C" __global__ void __launch_bounds__(128, 2) wave_multi_kernel(WaveArgs A) {
+//
+// FP32 passes evaluate as the biallelic passes do: the FP32 rows with the FP32
+// hi parts of xt, FP32 partial sums (gradient and objective promoted to FP64
+// every 8 sites, the Hessian once per unit: at most ML_CHUNK / 32 = 64 terms),
+// and the lo parts of xt restored to first order in FP64 from the unit's own
+// sums (G_i loses sum_j H_ij lo_j, the objective gains sum_j lo_j G_j).  FP64
+// passes use the FP64 rows.  The lanes' Hessian sums go through shared memory.
+constexpr int MULTI_WARPS = 4;
+
+template <bool DIFF>
+__device__ __forceinline__ void multi_unit32(const CohortDev& co, const SlotState& S, int64_t v0, int64_t v1,
+                                             int lane, double eps, double* hs, double* P) {
+    float xh[9], sd[9];
+#pragma unroll
+    for (int k = 0; k < 9; k++) {
+        xh[k] = (float)S.xt[k];
+        sd[k] = DIFF ? (float)(S.xt[k] - S.xc[k]) : 0.f;
+    }
+    const uint8_t* grx = co.ml_gr + S.x * co.ml_stride;
+    const uint8_t* gry = co.ml_gr + S.y * co.ml_stride;
+    const float e32 = (float)eps;
+    float g[9], h[45], o = 0.f;
+    double G[9], F = 0.0;
+#pragma unroll
+    for (int k = 0; k < 9; k++) { g[k] = 0.f; G[k] = 0.0; }
+#pragma unroll
+    for (int k = 0; k < 45; k++) h[k] = 0.f;
+    int nzero = 0, cnt = 0;
+    for (int64_t v = v0 + lane; v < v1; v += 32) {
+        const int a = grx[v], b = gry[v];
+        if (a == ML_MISSING || b == ML_MISSING) continue;
+        if (a == ML_ZERO_ROW || b == ML_ZERO_ROW) {
+            nzero++;
+            continue;
+        }
+        const int2 si = co.ml_site[v];
+        const float4* R = co.ml_rows32 + 3 * ((int64_t)si.x + a * si.y + b);
+        const float4 r0 = __ldg(R), r1 = __ldg(R + 1), r2 = __ldg(R + 2);
+        const float L[9] = {r0.x, r0.y, r0.z, r0.w, r1.x, r1.y, r1.z, r1.w, r2.x};
+        float d = e32;
+#pragma unroll
+        for (int k = 0; k < 9; k++) d = fmaf(L[k], xh[k], d);
+        const float r = rcp_approx(d);
+        float q[9];
+#pragma unroll
+        for (int k = 0; k < 9; k++) {
+            q[k] = L[k] * r;
+            g[k] += q[k];
+        }
+        int hh = 0;
+#pragma unroll
+        for (int i = 0; i < 9; i++)
+#pragma unroll
+            for (int j = i; j < 9; j++, hh++) h[hh] = fmaf(q[i], q[j], h[hh]);
+        if (!DIFF) {
+            o += lg2_approx(d);
+        } else {
+            float dl = 0.f;
+#pragma unroll
+            for (int k = 0; k < 9; k++) dl = fmaf(L[k], sd[k], dl);
+            o += neg_log1m(dl * r);
+        }
+        if ((++cnt & 7) == 0) {
+#pragma unroll
+            for (int k = 0; k < 9; k++) { G[k] += (double)g[k]; g[k] = 0.f; }
+            F += (double)o;
+            o = 0.f;
+        }
+    }
+    // the Hessian partials leave the registers before the reductions
+#pragma unroll
+    for (int k = 0; k < 45; k++) hs[32 * k + lane] = (double)h[k];
+#pragma unroll
+    for (int k = 0; k < 9; k++) G[k] = warp_sum(G[k] + (double)g[k]);
+    F = warp_sum(F + (double)o);
+    double lo[9], corr[9];
+#pragma unroll
+    for (int k = 0; k < 9; k++) {
+        lo[k] = S.xt[k] - (double)xh[k];
+        corr[k] = 0.0;
+    }
+    int hh = 0;
+#pragma unroll
+    for (int i = 0; i < 9; i++)
+#pragma unroll
+        for (int j = i; j < 9; j++, hh++) {
+            const double t = warp_sum(hs[32 * hh + lane]);
+            if (lane == 0) P[9 + hh] = t;
+            corr[i] = fma(t, lo[j], corr[i]);
+            if (j != i) corr[j] = fma(t, lo[i], corr[j]);
+        }
+    double ob;
+    if (DIFF) {
+        ob = F;
+    } else {
+        double c = 0.0;
+#pragma unroll
+        for (int k = 0; k < 9; k++) c = fma(lo[k], G[k], c);
+        double z = 0.0;
+        for (int off = 16; off > 0; off >>= 1) nzero += __shfl_xor_sync(0xffffffffu, nzero, off);
+        z = (double)nzero * log(eps);
+        ob = (F * 0.69314718055994530942 + c) + z;
+    }
+    if (lane == 0) {
+#pragma unroll
+        for (int k = 0; k < 9; k++) P[k] = G[k] - corr[k];
+        P[54] = ob;
+    }
+    __syncwarp();
+}
+
+__device__ __forceinline__ void multi_unit64(const CohortDev& co, const SlotState& S, int64_t v0, int64_t v1,
+                                             int lane, double eps, double* hs, double* P) {
+    const bool diff = S.kind == PASS_FP32_DIFF;
+    double xt[9], xc[9];
+#pragma unroll
+    for (int k = 0; k < 9; k++) { xt[k] = S.xt[k]; xc[k] = S.xc[k]; }
+    const uint8_t* grx = co.ml_gr + S.x * co.ml_stride;
+    const uint8_t* gry = co.ml_gr + S.y * co.ml_stride;
+    double g[9], ob = 0.0;
+#pragma unroll
+    for (int k = 0; k < 9; k++) g[k] = 0.0;
+    for (int k = 0; k < 45; k++) hs[32 * k + lane] = 0.0;
+    for (int64_t v = v0 + lane; v < v1; v += 32) {
+        const int a = grx[v], b = gry[v];
+        if (a == ML_MISSING || b == ML_MISSING) continue;
+        if (a == ML_ZERO_ROW || b == ML_ZERO_ROW) {
+            if (!diff) ob += log(eps);
+            continue;
+        }
+        const int2 si = co.ml_site[v];
+        const double* R = co.ml_rows + 9 * ((int64_t)si.x + a * si.y + b);
+        double L[9];
+#pragma unroll
+        for (int k = 0; k < 9; k++) L[k] = __ldg(R + k);
+        double d = eps;
+#pragma unroll
+        for (int k = 0; k < 9; k++) d = fma(L[k], xt[k], d);
+        const double r = 1.0 / d;
+        double q[9];
+#pragma unroll
+        for (int k = 0; k < 9; k++) {
+            q[k] = L[k] * r;
+            g[k] += q[k];
+        }
+        int h = 0;
+#pragma unroll
+        for (int i = 0; i < 9; i++)
+#pragma unroll
+            for (int j = i; j < 9; j++, h++) hs[32 * h + lane] = fma(q[i], q[j], hs[32 * h + lane]);
+        if (!diff) {
+            ob += log(d);
+        } else {
+            double dc = eps, dl = 0.0;
+#pragma unroll
+            for (int k = 0; k < 9; k++) {
+                dc = fma(L[k], xc[k], dc);
+                dl = fma(L[k], xt[k] - xc[k], dl);
+            }
+            ob += log1p(dl / dc);
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < 9; k++) {
+        const double v = warp_sum(g[k]);
+        if (lane == 0) P[k] = v;
+    }
+    for (int k = 0; k < 45; k++) {
+        const double v = warp_sum(hs[32 * k + lane]);
+        if (lane == 0) P[9 + k] = v;
+    }
+    const double vo = warp_sum(ob);
+    if (lane == 0) P[54] = vo;
+    __syncwarp();
+}
+
+extern "C" __global__ void __launch_bounds__(MULTI_WARPS * 32, 3) wave_multi_kernel(WaveArgs A) {
+    __shared__ double hsm[MULTI_WARPS][45 * 32];   // the lanes' Hessian sums
     if (A.clk->stop) return;   // a device loop past its last wave
     const int lane = threadIdx.x & 31;
     const PhaseEnd pe{&A.clk->end[1], lane == 0};   // timed as part of the pass phase
@@ -727,6 +904,7 @@ extern "C" __global__ void __launch_bounds__(128, 2) wave_multi_kernel(WaveArgs 
     const int64_t nwarps = (int64_t)gridDim.x * (blockDim.x >> 5);
     const int64_t ntask = (int64_t)A.wc_cur->n_pass * A.ml_units;
     const double eps = A.tune.epsilon;
+    double* hs = hsm[threadIdx.x >> 5];
     for (int64_t t = warp; t < ntask; t += nwarps) {
         const int s = A.pass_cur[t / A.ml_units];
         const int u = (int)(t % A.ml_units);
@@ -737,69 +915,10 @@ extern "C" __global__ void __launch_bounds__(128, 2) wave_multi_kernel(WaveArgs 
         const int64_t v0 = (int64_t)u * ML_CHUNK;
         if (v0 >= co.ml_nk) continue;
         const int64_t v1 = min((int64_t)co.ml_nk, v0 + ML_CHUNK);
-        const bool diff = kind == PASS_FP32_DIFF;
-        double xt[9], xc[9];
-#pragma unroll
-        for (int k = 0; k < 9; k++) { xt[k] = S.xt[k]; xc[k] = S.xc[k]; }
-        const uint8_t* grx = co.ml_gr + S.x * co.ml_stride;
-        const uint8_t* gry = co.ml_gr + S.y * co.ml_stride;
-        double g[9], H[45], ob = 0.0;
-#pragma unroll
-        for (int k = 0; k < 9; k++) g[k] = 0.0;
-#pragma unroll
-        for (int k = 0; k < 45; k++) H[k] = 0.0;
-        for (int64_t v = v0 + lane; v < v1; v += 32) {
-            const int a = grx[v], b = gry[v];
-            if (a == ML_MISSING || b == ML_MISSING) continue;
-            if (a == ML_ZERO_ROW || b == ML_ZERO_ROW) {
-                if (!diff) ob += log(eps);
-                continue;
-            }
-            const int2 si = co.ml_site[v];
-            const double* R = co.ml_rows + 9 * ((int64_t)si.x + a * si.y + b);
-            double L[9];
-#pragma unroll
-            for (int k = 0; k < 9; k++) L[k] = __ldg(R + k);
-            double d = eps;
-#pragma unroll
-            for (int k = 0; k < 9; k++) d = fma(L[k], xt[k], d);
-            const double r = 1.0 / d;
-            double q[9];
-#pragma unroll
-            for (int k = 0; k < 9; k++) {
-                q[k] = L[k] * r;
-                g[k] += q[k];
-            }
-            int h = 0;
-#pragma unroll
-            for (int i = 0; i < 9; i++)
-#pragma unroll
-                for (int j = i; j < 9; j++, h++) H[h] = fma(q[i], q[j], H[h]);
-            if (!diff) {
-                ob += log(d);
-            } else {
-                double dc = eps, dl = 0.0;
-#pragma unroll
-                for (int k = 0; k < 9; k++) {
-                    dc = fma(L[k], xc[k], dc);
-                    dl = fma(L[k], xt[k] - xc[k], dl);
-                }
-                ob += log1p(dl / dc);
-            }
-        }
         double* P = A.ml_partial + ((int64_t)s * A.ml_units + u) * ML_VALS;
-#pragma unroll
-        for (int k = 0; k < 9; k++) {
-            const double v = warp_sum(g[k]);
-            if (lane == 0) P[k] = v;
-        }
-#pragma unroll
-        for (int k = 0; k < 45; k++) {
-            const double v = warp_sum(H[k]);
-            if (lane == 0) P[9 + k] = v;
-        }
-        const double vo = warp_sum(ob);
-        if (lane == 0) P[54] = vo;
+        if (kind == PASS_FP64) multi_unit64(co, S, v0, v1, lane, eps, hs, P);
+        else if (kind == PASS_FP32_DIFF) multi_unit32<true>(co, S, v0, v1, lane, eps, hs, P);
+        else multi_unit32<false>(co, S, v0, v1, lane, eps, hs, P);
     }
 }
 
@@ -1365,7 +1484,7 @@ int WaveEngine::open(Workspace& ws, cudaStream_t st, const RunConfig& cfg, int64
     E.multi_blocks = 0;
     if (cfg.ml_units > 0) {
         int mocc = 0;
-        KG_WAVE_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&mocc, wave_multi_kernel, 128, 0));
+        KG_WAVE_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&mocc, wave_multi_kernel, MULTI_WARPS * 32, 0));
         E.multi_blocks = ws.sm_count * std::max(1, mocc);
     }
     WaveArgs& A = E.A;
@@ -1432,7 +1551,7 @@ int WaveEngine::open(Workspace& ws, cudaStream_t st, const RunConfig& cfg, int64
         }
         if (ce == cudaSuccess) {
             wave_pass_kernel<<<E.pass_blocks, 128, WAVE_WPB * PASS_WARP_SMEM, st>>>(Aw);
-            if (E.multi_blocks) wave_multi_kernel<<<E.multi_blocks, 128, 0, st>>>(Aw);
+            if (E.multi_blocks) wave_multi_kernel<<<E.multi_blocks, MULTI_WARPS * 32, 0, st>>>(Aw);
             ce = cudaEventRecordWithFlags(E.ev[par][2], st, cudaEventRecordExternal);
         }
         if (ce == cudaSuccess) {
@@ -1549,7 +1668,7 @@ int WaveEngine::run_until_idle(unsigned long long max_waves, std::string& err) {
             const WaveArgs& Aw = E.args[E.cur ^ k];
             wave_admit_kernel<<<E.admit_blocks, ADMIT_WARPS * 32, ADMIT_WARPS * ADMIT_WARP_SMEM, st>>>(Aw);
             wave_pass_kernel<<<E.pass_blocks, 128, WAVE_WPB * PASS_WARP_SMEM, st>>>(Aw);
-            if (E.multi_blocks) wave_multi_kernel<<<E.multi_blocks, 128, 0, st>>>(Aw);
+            if (E.multi_blocks) wave_multi_kernel<<<E.multi_blocks, MULTI_WARPS * 32, 0, st>>>(Aw);
             wave_solve_kernel<<<E.solve_blocks, 128, WAVE_WPB * WARP_SMEM, st>>>(Aw);
             wave_end_kernel<<<1, 32, 0, st>>>(Aw, k, h, max_waves);
         }
