@@ -59,6 +59,7 @@ struct kg_ctx {
     kg::DevBuf soft_gl;                   // kg_load_likelihoods: double [sample][site][3]
     int64_t soft_ns = 0, soft_nv = 0;
     kg::DevBuf soft_gl3, soft_gl4;        // kg_load_likelihoods_multiallelic: [sample][site][6], [..][10]
+    kg::SoftWork soft_work;               // the soft estimator's buffers, kept between calls
     int64_t soft_n3 = 0, soft_n4 = 0;
     kg::Workspace ws;
     kg::DevBuf dout;
@@ -732,7 +733,7 @@ int kg_relatedness_gl(kg_ctx* c, int64_t num_samples, uint64_t iterations, doubl
         mi.n3 = c->soft_n3;
         mi.gl4 = c->soft_n4 ? c->soft_gl4.as<double>() : nullptr;
         mi.n4 = c->soft_n4;
-        st = kg::soft_relatedness(c->soft_gl, c->soft_ns, c->soft_nv, ns, iterations, std::isnan(maf) ? -1.0 : maf,
+        st = kg::soft_relatedness(c->soft_work, c->soft_gl, c->soft_ns, c->soft_nv, ns, iterations, std::isnan(maf) ? -1.0 : maf,
                                   c->dout.as<kg_output>(), c->stream, err, &kept, c->precision, sc, &mi, used);
         cudaEventRecord(ev1, c->stream);
         int st2 = copy_rows_out(c, c->dout, np, out, c->stream);

@@ -141,14 +141,20 @@ int prepare_ml_multi(Cohort& c, bool have_af, double maf, uint64_t iterations, c
 // multi (optional): tri- and tetra-allelic sites' likelihoods on the device,
 // [sample][site][6] and [sample][site][10]; multi_used (3, optional): those
 // kept with 2, 3 and 4 alleles after the frequency cut.
+// Device buffers of the soft-likelihood estimator, kept between calls (they
+// only grow, so repeated calls allocate nothing).
+struct SoftWork {
+    DevBuf pf, qf, keep, idx, kp, kq, ctr, g32, pq32, mgk, mgidx, mrows, mused, mscratch;
+};
 struct SoftMultiInput {
     const double* gl3 = nullptr;
     int64_t n3 = 0;
     const double* gl4 = nullptr;
     int64_t n4 = 0;
 };
-int soft_relatedness(const DevBuf& gl, int64_t n_samples, int64_t n_sites, int64_t ns, uint64_t iterations,
-                     double maf, kg_output* d_out, cudaStream_t st, std::string& err, int64_t* n_kept = nullptr,
+int soft_relatedness(SoftWork& w, const DevBuf& gl, int64_t n_samples, int64_t n_sites, int64_t ns,
+                     uint64_t iterations, double maf, kg_output* d_out, cudaStream_t st, std::string& err,
+                     int64_t* n_kept = nullptr,
                      int precision = KG_PREC_FP32C, uint64_t* counters = nullptr,
                      const SoftMultiInput* multi = nullptr, int64_t* multi_used = nullptr);
 
@@ -188,6 +194,7 @@ struct RunConfig {
     int pass_blocks_per_sm = 0;   // site-pass kernel blocks per SM (0 = occupancy limit)
     uint64_t max_waves = 0;       // waves a call may run before it gives up (0 = a bound from the work)
     int ml_units = 0;             // work units per slot of the ML path's tri-/tetra-allelic sites (run_pairs sets it)
+    int ml_chunk = 0;             // their kept sites per unit (run_pairs sets it)
     int unit_elems = 0;           // list entries per site-pass work unit (0 = UNIT_ELEMS, 16384)
     int slot_divisor = 8;         // automatic slots: the job's pairs / slot_divisor within 4096..32768
     // Called between waves, on the calling thread, once per job whose pairs

@@ -462,68 +462,72 @@ __device__ __noinline__ int64_t soft_evaluate32(const float4* __restrict__ g32, 
     const float e32 = (float)eps;
     const int nk32 = (int)nk;
     int64_t n = 0;
-    int cnt = 0;
     // the next site's records are loaded while this one is evaluated
     float4 X = make_float4(0.f, 0.f, 0.f, 0.f), Y = X;
     float2 PQ = make_float2(0.f, 0.f);
     if (lane < nk32) { X = lx[lane]; Y = ly[lane]; PQ = pq32[lane]; }
-    for (int k = lane; k < nk32; k += 32) {
+    // warp-uniform iterations (a lane past the end or at a missing sample
+    // skips the site), so that the FP64 flushes below run once per warp
+    const int iters = (nk32 + 31) >> 5;
+    for (int it = 0; it < iters; it++) {
+        const int k = lane + 32 * it;
         const float X0 = X.x, X1 = X.y, X2 = X.z, Y0 = Y.x, Y1 = Y.y, Y2 = Y.z;
         const float p = PQ.x, q = PQ.y;
         if (k + 32 < nk32) { X = lx[k + 32]; Y = ly[k + 32]; PQ = pq32[k + 32]; }
-        if (isnan(X0) || isnan(Y0)) continue;   // a missing sample has all three NaN
-        // L = sum over (gx, gy) of GLx(gx) GLy(gy) m(gx, gy), the nine rows of
-        // the biallelic conditional table (cls_row) gathered by entry
-        const float A = X0 * Y0, B = X2 * Y2, C = X0 * Y2, D = X2 * Y0, E = X0 * Y1;
-        const float Fx = X2 * Y1, Gx = X1 * Y0, Hx = X1 * Y2, I = X1 * Y1;
-        const float p2 = p * p, q2 = q * q, pq = p * q;
-        const float p2q = p2 * q, pq2 = p * q2;
-        const float S2 = fmaf(A, p2, B * q2);
-        const float S3 = fmaf(A, p2 * p, B * (q2 * q));
-        float L[9];
-        L[0] = fmaf(A, p, B * q);
-        L[1] = fmaf(C + D, pq, S2);
-        L[2] = fmaf(E + Fx, pq, S2);
-        L[3] = fmaf(2.0f * E, p2q, fmaf(2.0f * Fx, pq2, fmaf(C, pq2, fmaf(D, p2q, S3))));
-        L[4] = fmaf(Gx + Hx, pq, S2);
-        L[5] = fmaf(2.0f * Gx, p2q, fmaf(2.0f * Hx, pq2, fmaf(C, p2q, fmaf(D, pq2, S3))));
-        L[6] = fmaf(2.0f * I, pq, S2);
-        L[7] = fmaf(I, p2q + pq2, fmaf(Fx + Hx, pq2, fmaf(E + Gx, p2q, S3)));
-        L[8] = fmaf(4.0f * I, p2 * q2,
-                    fmaf(2.0f * (Fx + Hx), pq2 * q,
-                         fmaf(2.0f * (E + Gx), p2q * p, fmaf(C + D, p2 * q2, fmaf(A, p2 * p2, B * (q2 * q2))))));
-        float d = e32;
+        // a missing sample has all three NaN
+        if (k < nk32 && !isnan(X0) && !isnan(Y0)) {
+            // L = sum over (gx, gy) of GLx(gx) GLy(gy) m(gx, gy), the nine rows
+            // of the biallelic conditional table (cls_row) gathered by entry
+            const float A = X0 * Y0, B = X2 * Y2, C = X0 * Y2, D = X2 * Y0, E = X0 * Y1;
+            const float Fx = X2 * Y1, Gx = X1 * Y0, Hx = X1 * Y2, I = X1 * Y1;
+            const float p2 = p * p, q2 = q * q, pq = p * q;
+            const float p2q = p2 * q, pq2 = p * q2;
+            const float S2 = fmaf(A, p2, B * q2);
+            const float S3 = fmaf(A, p2 * p, B * (q2 * q));
+            float L[9];
+            L[0] = fmaf(A, p, B * q);
+            L[1] = fmaf(C + D, pq, S2);
+            L[2] = fmaf(E + Fx, pq, S2);
+            L[3] = fmaf(2.0f * E, p2q, fmaf(2.0f * Fx, pq2, fmaf(C, pq2, fmaf(D, p2q, S3))));
+            L[4] = fmaf(Gx + Hx, pq, S2);
+            L[5] = fmaf(2.0f * Gx, p2q, fmaf(2.0f * Hx, pq2, fmaf(C, p2q, fmaf(D, pq2, S3))));
+            L[6] = fmaf(2.0f * I, pq, S2);
+            L[7] = fmaf(I, p2q + pq2, fmaf(Fx + Hx, pq2, fmaf(E + Gx, p2q, S3)));
+            L[8] = fmaf(4.0f * I, p2 * q2,
+                        fmaf(2.0f * (Fx + Hx), pq2 * q,
+                             fmaf(2.0f * (E + Gx), p2q * p, fmaf(C + D, p2 * q2, fmaf(A, p2 * p2, B * (q2 * q2))))));
+            float d = e32;
 #pragma unroll
-        for (int i = 0; i < 9; i++) d = fmaf(L[i], xh[i], d);
-        const float r = rcp_approx(d);
-        float b[9];
+            for (int i = 0; i < 9; i++) d = fmaf(L[i], xh[i], d);
+            const float r = rcp_approx(d);
+            float b[9];
 #pragma unroll
-        for (int i = 0; i < 9; i++) {
-            b[i] = L[i] * r;
-            g[i] += b[i];
+            for (int i = 0; i < 9; i++) {
+                b[i] = L[i] * r;
+                g[i] += b[i];
+            }
+            int a = 0;
+#pragma unroll
+            for (int i = 0; i < 9; i++)
+#pragma unroll
+                for (int j = i; j < 9; j++, a++) h[a] = fmaf(b[i], b[j], h[a]);
+            if (!diff) {
+                o += lg2_approx(d);
+            } else {
+                float dl = 0.f;
+#pragma unroll
+                for (int i = 0; i < 9; i++) dl = fmaf(L[i], sd[i], dl);
+                o += neg_log1m(dl * r);
+            }
+            n++;
         }
-        int a = 0;
-#pragma unroll
-        for (int i = 0; i < 9; i++)
-#pragma unroll
-            for (int j = i; j < 9; j++, a++) h[a] = fmaf(b[i], b[j], h[a]);
-        if (!diff) {
-            o += lg2_approx(d);
-        } else {
-            float dl = 0.f;
-#pragma unroll
-            for (int i = 0; i < 9; i++) dl = fmaf(L[i], sd[i], dl);
-            o += neg_log1m(dl * r);
-        }
-        n++;
-        cnt++;
-        if ((cnt & 7) == 0) {
+        if ((it & 7) == 7) {
 #pragma unroll
             for (int i = 0; i < 9; i++) { G[i] += (double)g[i]; g[i] = 0.f; }
             F += (double)o;
             o = 0.f;
         }
-        if ((cnt & 31) == 0) {
+        if ((it & 31) == 31) {
 #pragma unroll
             for (int a2 = 0; a2 < 45; a2++) {
                 hs[a2 * HS + lane] += (double)h[a2];
@@ -716,11 +720,14 @@ __global__ void __launch_bounds__(SOFT_WARPS * 32, 3) soft_pairs_kernel(
     }
 }
 
-int soft_relatedness(const DevBuf& gl, int64_t n_samples, int64_t n_sites, int64_t ns, uint64_t iterations,
-                     double maf, kg_output* d_out, cudaStream_t st, std::string& err, int64_t* n_kept, int precision,
+int soft_relatedness(SoftWork& w, const DevBuf& gl, int64_t n_samples, int64_t n_sites, int64_t ns,
+                     uint64_t iterations, double maf, kg_output* d_out, cudaStream_t st, std::string& err,
+                     int64_t* n_kept, int precision,
                      uint64_t* counters, const SoftMultiInput* multi, int64_t* multi_used) {
     if (!(maf >= 0.0)) maf = 1.0 / (2.0 * (double)n_samples);
-    DevBuf pf, qf, keep, idx, kp, kq, ctr, g32, pq32, mgk, mgidx, mrows, mused, mscratch;
+    DevBuf &pf = w.pf, &qf = w.qf, &keep = w.keep, &idx = w.idx, &kp = w.kp, &kq = w.kq, &ctr = w.ctr;
+    DevBuf &g32 = w.g32, &pq32 = w.pq32, &mgk = w.mgk, &mgidx = w.mgidx, &mrows = w.mrows, &mused = w.mused;
+    DevBuf& mscratch = w.mscratch;
     KG_SOFT_TRY((cudaError_t)pf.reserve(sizeof(double) * n_sites));
     KG_SOFT_TRY((cudaError_t)qf.reserve(sizeof(double) * n_sites));
     KG_SOFT_TRY((cudaError_t)keep.reserve((size_t)n_sites));

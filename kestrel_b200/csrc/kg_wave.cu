@@ -716,17 +716,50 @@ extern "C" __global__ void __launch_bounds__(128, PASS_MIN_BLOCKS) wave_pass_ker
 // (gradient), (L/d)(L/d)' (Hessian) and the objective term (log d, or for a
 // difference pass log(d / d_old) with d_old at xc); a call that uses a
 // dropped allele gives the site a row of zeros (objective term log eps, or 0
-// in a difference pass).  Work units are (slot of the pass list, ML_CHUNK
+// in a difference pass).  Work units are (slot of the pass list, ml_chunk
 // sites), strided over the grid's warps; lanes stride over the unit's sites,
 // and the unit's sums go to ml_partial in a fixed order.
 //
 // FP32 passes evaluate as the biallelic passes do: the FP32 rows with the FP32
-// hi parts of xt, FP32 partial sums (gradient and objective promoted to FP64
-// every 8 sites, the Hessian once per unit: at most ML_CHUNK / 32 = 64 terms),
-// and the lo parts of xt restored to first order in FP64 from the unit's own
-// sums (G_i loses sum_j H_ij lo_j, the objective gains sum_j lo_j G_j).  FP64
-// passes use the FP64 rows.  The lanes' Hessian sums go through shared memory.
+// hi parts of xt, FP32 partial sums added to the lane's FP64 sums in shared
+// memory (gradient and objective every 8 sites, Hessian every 64), and the lo
+// parts of xt restored to first order in FP64 from the unit's own sums (G_i
+// loses sum_j H_ij lo_j, the objective gains sum_j lo_j G_j).  FP64 passes use
+// the FP64 rows, their Hessian sums in the same shared memory.
 constexpr int MULTI_WARPS = 4;
+// shared-memory rows of a warp's sums (32 lane partials each): the 45 Hessian
+// terms, the 9 gradient terms, the objective
+constexpr int MULTI_HS_ROWS = 55;
+constexpr int MULTI_SMEM = MULTI_WARPS * MULTI_HS_ROWS * 32 * (int)sizeof(double);
+
+// A lane's next multi-allelic site: its two codes and table entry, then its
+// row (a zero row unless both calls use kept alleles only).
+struct MultiCodes {
+    int a, b;
+    int2 si;
+};
+__device__ __forceinline__ MultiCodes multi_codes(const CohortDev& co, const uint8_t* grx, const uint8_t* gry,
+                                                  int64_t v, int64_t v1) {
+    MultiCodes c{ML_MISSING, ML_MISSING, make_int2(0, 0)};
+    if (v < v1) {
+        c.a = grx[v];
+        c.b = gry[v];
+        c.si = co.ml_site[v];
+    }
+    return c;
+}
+__device__ __forceinline__ bool multi_has_row(const MultiCodes& c) { return c.a < ML_ZERO_ROW && c.b < ML_ZERO_ROW; }
+__device__ __forceinline__ void multi_row(const CohortDev& co, const MultiCodes& c, float4& r0, float4& r1,
+                                          float4& r2) {
+    if (multi_has_row(c)) {
+        const float4* R = co.ml_rows32 + 3 * ((int64_t)c.si.x + c.a * c.si.y + c.b);
+        r0 = __ldg(R);
+        r1 = __ldg(R + 1);
+        r2 = __ldg(R + 2);
+    } else {
+        r0 = r1 = r2 = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+}
 
 template <bool DIFF>
 __device__ __forceinline__ void multi_unit32(const CohortDev& co, const SlotState& S, int64_t v0, int64_t v1,
@@ -741,65 +774,85 @@ __device__ __forceinline__ void multi_unit32(const CohortDev& co, const SlotStat
     const uint8_t* gry = co.ml_gr + S.y * co.ml_stride;
     const float e32 = (float)eps;
     float g[9], h[45], o = 0.f;
-    double G[9], F = 0.0;
 #pragma unroll
-    for (int k = 0; k < 9; k++) { g[k] = 0.f; G[k] = 0.0; }
+    for (int k = 0; k < 9; k++) g[k] = 0.f;
 #pragma unroll
     for (int k = 0; k < 45; k++) h[k] = 0.f;
-    int nzero = 0, cnt = 0;
-    for (int64_t v = v0 + lane; v < v1; v += 32) {
-        const int a = grx[v], b = gry[v];
-        if (a == ML_MISSING || b == ML_MISSING) continue;
-        if (a == ML_ZERO_ROW || b == ML_ZERO_ROW) {
-            nzero++;
-            continue;
-        }
-        const int2 si = co.ml_site[v];
-        const float4* R = co.ml_rows32 + 3 * ((int64_t)si.x + a * si.y + b);
-        const float4 r0 = __ldg(R), r1 = __ldg(R + 1), r2 = __ldg(R + 2);
+    int nzero = 0;
+    for (int k = 0; k < MULTI_HS_ROWS; k++) hs[32 * k + lane] = 0.0;
+    // Warp-uniform iterations, so that the FP64 flushes run once per warp.
+    // Loads run ahead: the codes two sites ahead, the row one site ahead (the
+    // row's address needs the codes).
+    const int iters = (int)((v1 - v0 + 31) >> 5);
+    MultiCodes c0 = multi_codes(co, grx, gry, v0 + lane, v1);
+    MultiCodes c1 = multi_codes(co, grx, gry, v0 + lane + 32, v1);
+    float4 r0, r1, r2;
+    multi_row(co, c0, r0, r1, r2);
+    for (int it = 0; it < iters; it++) {
+        const MultiCodes c = c0;
         const float L[9] = {r0.x, r0.y, r0.z, r0.w, r1.x, r1.y, r1.z, r1.w, r2.x};
-        float d = e32;
+        multi_row(co, c1, r0, r1, r2);
+        c0 = c1;
+        c1 = multi_codes(co, grx, gry, v0 + lane + 32 * (int64_t)(it + 2), v1);
+        if (multi_has_row(c)) {
+            float d = e32;
 #pragma unroll
-        for (int k = 0; k < 9; k++) d = fmaf(L[k], xh[k], d);
-        const float r = rcp_approx(d);
-        float q[9];
+            for (int k = 0; k < 9; k++) d = fmaf(L[k], xh[k], d);
+            const float r = rcp_approx(d);
+            float q[9];
 #pragma unroll
-        for (int k = 0; k < 9; k++) {
-            q[k] = L[k] * r;
-            g[k] += q[k];
+            for (int k = 0; k < 9; k++) {
+                q[k] = L[k] * r;
+                g[k] += q[k];
+            }
+            int hh = 0;
+#pragma unroll
+            for (int i = 0; i < 9; i++)
+#pragma unroll
+                for (int j = i; j < 9; j++, hh++) h[hh] = fmaf(q[i], q[j], h[hh]);
+            if (!DIFF) {
+                o += lg2_approx(d);
+            } else {
+                float dl = 0.f;
+#pragma unroll
+                for (int k = 0; k < 9; k++) dl = fmaf(L[k], sd[k], dl);
+                o += neg_log1m(dl * r);
+            }
+        } else if (c.a != ML_MISSING && c.b != ML_MISSING) {
+            nzero++;   // a call with a dropped allele: a zero row
         }
-        int hh = 0;
+        if ((it & 7) == 7) {
 #pragma unroll
-        for (int i = 0; i < 9; i++)
-#pragma unroll
-            for (int j = i; j < 9; j++, hh++) h[hh] = fmaf(q[i], q[j], h[hh]);
-        if (!DIFF) {
-            o += lg2_approx(d);
-        } else {
-            float dl = 0.f;
-#pragma unroll
-            for (int k = 0; k < 9; k++) dl = fmaf(L[k], sd[k], dl);
-            o += neg_log1m(dl * r);
-        }
-        if ((++cnt & 7) == 0) {
-#pragma unroll
-            for (int k = 0; k < 9; k++) { G[k] += (double)g[k]; g[k] = 0.f; }
-            F += (double)o;
+            for (int k = 0; k < 9; k++) {
+                hs[32 * (45 + k) + lane] += (double)g[k];
+                g[k] = 0.f;
+            }
+            hs[32 * 54 + lane] += (double)o;
             o = 0.f;
         }
+        if ((it & 63) == 63) {
+#pragma unroll
+            for (int k = 0; k < 45; k++) {
+                hs[32 * k + lane] += (double)h[k];
+                h[k] = 0.f;
+                asm volatile("" ::: "memory");   // one read-modify-write at a time: no register peak
+            }
+        }
     }
-    // the Hessian partials leave the registers before the reductions
+    // the partials leave the registers before the reductions
 #pragma unroll
-    for (int k = 0; k < 45; k++) hs[32 * k + lane] = (double)h[k];
+    for (int k = 0; k < 45; k++) hs[32 * k + lane] += (double)h[k];
 #pragma unroll
-    for (int k = 0; k < 9; k++) G[k] = warp_sum(G[k] + (double)g[k]);
-    F = warp_sum(F + (double)o);
-    double lo[9], corr[9];
+    for (int k = 0; k < 9; k++) hs[32 * (45 + k) + lane] += (double)g[k];
+    hs[32 * 54 + lane] += (double)o;
+    double G[9], lo[9], corr[9];
 #pragma unroll
     for (int k = 0; k < 9; k++) {
+        G[k] = warp_sum(hs[32 * (45 + k) + lane]);
         lo[k] = S.xt[k] - (double)xh[k];
         corr[k] = 0.0;
     }
+    const double F = warp_sum(hs[32 * 54 + lane]);
     int hh = 0;
 #pragma unroll
     for (int i = 0; i < 9; i++)
@@ -817,10 +870,8 @@ __device__ __forceinline__ void multi_unit32(const CohortDev& co, const SlotStat
         double c = 0.0;
 #pragma unroll
         for (int k = 0; k < 9; k++) c = fma(lo[k], G[k], c);
-        double z = 0.0;
         for (int off = 16; off > 0; off >>= 1) nzero += __shfl_xor_sync(0xffffffffu, nzero, off);
-        z = (double)nzero * log(eps);
-        ob = (F * 0.69314718055994530942 + c) + z;
+        ob = (F * 0.69314718055994530942 + c) + (double)nzero * log(eps);
     }
     if (lane == 0) {
 #pragma unroll
@@ -896,7 +947,7 @@ __device__ __forceinline__ void multi_unit64(const CohortDev& co, const SlotStat
 }
 
 extern "C" __global__ void __launch_bounds__(MULTI_WARPS * 32, 3) wave_multi_kernel(WaveArgs A) {
-    __shared__ double hsm[MULTI_WARPS][45 * 32];   // the lanes' Hessian sums
+    extern __shared__ double multi_smem[];   // per warp MULTI_HS_ROWS x 32 lane sums
     if (A.clk->stop) return;   // a device loop past its last wave
     const int lane = threadIdx.x & 31;
     const PhaseEnd pe{&A.clk->end[1], lane == 0};   // timed as part of the pass phase
@@ -904,7 +955,7 @@ extern "C" __global__ void __launch_bounds__(MULTI_WARPS * 32, 3) wave_multi_ker
     const int64_t nwarps = (int64_t)gridDim.x * (blockDim.x >> 5);
     const int64_t ntask = (int64_t)A.wc_cur->n_pass * A.ml_units;
     const double eps = A.tune.epsilon;
-    double* hs = hsm[threadIdx.x >> 5];
+    double* hs = multi_smem + (threadIdx.x >> 5) * (MULTI_HS_ROWS * 32);
     for (int64_t t = warp; t < ntask; t += nwarps) {
         const int s = A.pass_cur[t / A.ml_units];
         const int u = (int)(t % A.ml_units);
@@ -912,9 +963,9 @@ extern "C" __global__ void __launch_bounds__(MULTI_WARPS * 32, 3) wave_multi_ker
         const int kind = S.kind;
         if (kind == PASS_CLS || kind == PASS_CLS64) continue;
         const CohortDev& co = A.cohorts[S.cohort];
-        const int64_t v0 = (int64_t)u * ML_CHUNK;
+        const int64_t v0 = (int64_t)u * A.ml_chunk;
         if (v0 >= co.ml_nk) continue;
-        const int64_t v1 = min((int64_t)co.ml_nk, v0 + ML_CHUNK);
+        const int64_t v1 = min((int64_t)co.ml_nk, v0 + A.ml_chunk);
         double* P = A.ml_partial + ((int64_t)s * A.ml_units + u) * ML_VALS;
         if (kind == PASS_FP64) multi_unit64(co, S, v0, v1, lane, eps, hs, P);
         else if (kind == PASS_FP32_DIFF) multi_unit32<true>(co, S, v0, v1, lane, eps, hs, P);
@@ -1113,7 +1164,7 @@ extern "C" __global__ void __launch_bounds__(128, 4) wave_solve_kernel(WaveArgs 
 #pragma unroll
     for (int j = 0; j < 9; j++) ml_h[j] = 0.0;
     if (A.ml_units > 0) {
-        const int nml = (A.cohorts[S.cohort].ml_nk + ML_CHUNK - 1) / ML_CHUNK;
+        const int nml = (A.cohorts[S.cohort].ml_nk + A.ml_chunk - 1) / A.ml_chunk;
         const double* P = A.ml_partial + (int64_t)s * A.ml_units * ML_VALS;
         for (int u = 0; u < nml; u++) {
             const double* Pu = P + (int64_t)u * ML_VALS;
@@ -1335,7 +1386,8 @@ struct WaveEngine::Impl {
     // what open() was last called with, and the buffers its graphs point into
     bool opened = false;
     int64_t key_list_cap = 0, key_want = 0, key_expected = 0;
-    int key_max_jobs = 0, key_precision = 0, key_bps = 0, key_dev = -1, key_ml_units = 0, key_unit = 0,
+    int key_max_jobs = 0, key_precision = 0, key_bps = 0, key_dev = -1, key_ml_units = 0, key_ml_chunk = 0,
+        key_unit = 0,
         key_divisor = 0;
     uint64_t key_iterations = 0;
     cudaStream_t key_st = nullptr;
@@ -1376,7 +1428,8 @@ int WaveEngine::open(Workspace& ws, cudaStream_t st, const RunConfig& cfg, int64
                            E.key_expected == expected_pairs && E.key_max_jobs == E.max_jobs &&
                            E.key_precision == cfg.precision && E.key_bps == cfg.pass_blocks_per_sm &&
                            E.key_iterations == cfg.iterations && E.key_dev == dev && E.key_st == st &&
-                           E.key_ml_units == cfg.ml_units && E.key_unit == cfg.unit_elems &&
+                           E.key_ml_units == cfg.ml_units && E.key_ml_chunk == cfg.ml_chunk &&
+                           E.key_unit == cfg.unit_elems &&
                            E.key_divisor == cfg.slot_divisor;
     // work units: per shape at most ceil(list_cap / unit), over the five
     // shapes at most that + 5
@@ -1484,7 +1537,9 @@ int WaveEngine::open(Workspace& ws, cudaStream_t st, const RunConfig& cfg, int64
     E.multi_blocks = 0;
     if (cfg.ml_units > 0) {
         int mocc = 0;
-        KG_WAVE_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&mocc, wave_multi_kernel, MULTI_WARPS * 32, 0));
+        KG_WAVE_TRY(cudaFuncSetAttribute(wave_multi_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, MULTI_SMEM));
+        KG_WAVE_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&mocc, wave_multi_kernel, MULTI_WARPS * 32,
+                                                                  MULTI_SMEM));
         E.multi_blocks = ws.sm_count * std::max(1, mocc);
     }
     WaveArgs& A = E.A;
@@ -1507,6 +1562,7 @@ int WaveEngine::open(Workspace& ws, cudaStream_t st, const RunConfig& cfg, int64
     A.clk = E.clk;
     A.ml_partial = ws.ml_partial.as<double>();
     A.ml_units = cfg.ml_units;
+    A.ml_chunk = cfg.ml_chunk;
     A.unit_elems = unit;
     E.drop_loop();
     // One wave (counter resets, admit, pass, solve, read-back) captured as a
@@ -1551,7 +1607,7 @@ int WaveEngine::open(Workspace& ws, cudaStream_t st, const RunConfig& cfg, int64
         }
         if (ce == cudaSuccess) {
             wave_pass_kernel<<<E.pass_blocks, 128, WAVE_WPB * PASS_WARP_SMEM, st>>>(Aw);
-            if (E.multi_blocks) wave_multi_kernel<<<E.multi_blocks, MULTI_WARPS * 32, 0, st>>>(Aw);
+            if (E.multi_blocks) wave_multi_kernel<<<E.multi_blocks, MULTI_WARPS * 32, MULTI_SMEM, st>>>(Aw);
             ce = cudaEventRecordWithFlags(E.ev[par][2], st, cudaEventRecordExternal);
         }
         if (ce == cudaSuccess) {
@@ -1580,6 +1636,7 @@ int WaveEngine::open(Workspace& ws, cudaStream_t st, const RunConfig& cfg, int64
     E.key_dev = dev;
     E.key_st = st;
     E.key_ml_units = cfg.ml_units;
+    E.key_ml_chunk = cfg.ml_chunk;
     E.key_unit = cfg.unit_elems;
     E.key_divisor = cfg.slot_divisor;
     E.key_bufs = bufs;
@@ -1668,7 +1725,7 @@ int WaveEngine::run_until_idle(unsigned long long max_waves, std::string& err) {
             const WaveArgs& Aw = E.args[E.cur ^ k];
             wave_admit_kernel<<<E.admit_blocks, ADMIT_WARPS * 32, ADMIT_WARPS * ADMIT_WARP_SMEM, st>>>(Aw);
             wave_pass_kernel<<<E.pass_blocks, 128, WAVE_WPB * PASS_WARP_SMEM, st>>>(Aw);
-            if (E.multi_blocks) wave_multi_kernel<<<E.multi_blocks, MULTI_WARPS * 32, 0, st>>>(Aw);
+            if (E.multi_blocks) wave_multi_kernel<<<E.multi_blocks, MULTI_WARPS * 32, MULTI_SMEM, st>>>(Aw);
             wave_solve_kernel<<<E.solve_blocks, 128, WAVE_WPB * WARP_SMEM, st>>>(Aw);
             wave_end_kernel<<<1, 32, 0, st>>>(Aw, k, h, max_waves);
         }
@@ -1783,8 +1840,10 @@ int run_waves(const std::vector<PairJob>& jobs, const RunConfig& cfg_in, Workspa
               const std::vector<CohortDev>& table, int64_t total_pairs, int64_t list_cap) {
     (void)jobs;
     RunConfig cfg = cfg_in;
-    cfg.ml_units = 0;
-    for (const CohortDev& d : table) cfg.ml_units = std::max(cfg.ml_units, (d.ml_nk + ML_CHUNK - 1) / ML_CHUNK);
+    int max_nk = 0;
+    for (const CohortDev& d : table) max_nk = std::max(max_nk, (int)d.ml_nk);
+    cfg.ml_units = (max_nk + ML_CHUNK - 1) / ML_CHUNK;
+    cfg.ml_chunk = cfg.ml_units ? ((max_nk + cfg.ml_units - 1) / cfg.ml_units + 31) / 32 * 32 : 0;
     if (!ws.engine) ws.engine = std::make_shared<WaveEngine>();
     WaveEngine& eng = *ws.engine;
     int r = eng.open(ws, st, cfg, list_cap, total_pairs, (int)table.size(), err);

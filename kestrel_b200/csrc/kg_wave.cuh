@@ -129,13 +129,15 @@ struct WaveArgs {
     WaveClock* clk;
     double* ml_partial;            // per slot: ml_units * ML_VALS sums of its tri-/tetra-allelic sites
     int ml_units;                  // their work units per slot (0: no cohort has such sites)
+    int ml_chunk;                  // kept sites per such unit (a multiple of 32, at most ML_CHUNK)
     int unit_elems;                // list entries per pass work unit
 };
 
-// Work units of the ML path's tri- and tetra-allelic sites: ML_CHUNK kept
-// sites each; per unit 9 gradient sums, the 45 Hessian sums of the upper
-// triangle (row-major) and the objective term.
-constexpr int ML_CHUNK = 2048;
+// Work units of the ML path's tri- and tetra-allelic sites: at most ML_CHUNK
+// kept sites each, the largest cohort's sites split evenly; per unit 9
+// gradient sums, the 45 Hessian sums of the upper triangle (row-major) and the
+// objective term.
+constexpr int ML_CHUNK = 8192;
 constexpr int ML_VALS = 56;
 
 __device__ __forceinline__ int shape_ng(int s) { return s == 0 ? 4 : s == 3 ? 4 : s == 4 ? 2 : 3; }
