@@ -633,6 +633,15 @@ struct Shape32 {
     }
 };
 
+// eps + L.x over nine entries as three interleaved chains (five dependent
+// operations instead of nine), for the generic-row evaluations
+__device__ __forceinline__ float dot9_eps(const float* L, const float* x, float eps) {
+    const float a = fmaf(L[0], x[0], fmaf(L[3], x[3], fmaf(L[6], x[6], eps)));
+    const float b = fmaf(L[1], x[1], fmaf(L[4], x[4], L[7] * x[7]));
+    const float c = fmaf(L[2], x[2], fmaf(L[5], x[5], L[8] * x[8]));
+    return a + (b + c);
+}
+
 // ---------------------------------------------------------------- packed pairs
 // Shape32's hi-coefficient site arithmetic on two sites at once with the
 // sm_100 packed FP32 instructions (fma/mul/add .f32x2): one instruction per

@@ -42,6 +42,7 @@
 #include "kestrel_gpu.h"
 #include "kg_allele.cuh"
 #include "kg_alleleN.cuh"
+#include "kg_bulk.cuh"
 #include "kg_engine.h"
 #include "kg_pair.cuh"
 #include "kg_rowsolve.cuh"
@@ -132,6 +133,13 @@ __global__ void soft_freq_kernel(const double* __restrict__ gl, int64_t n_sample
 
 constexpr int SOFT_WARPS = 4;
 constexpr int HS = 33;   // shared-memory stride of the Hessian sums: 32 lane partials, then the warp total
+// A warp's shared memory: the Hessian sums (45 rows of HS doubles, padded to
+// 16 bytes), then per lane SOFT_STAGES slots of 48 bytes for the FP32 form's
+// prefetched site (the two samples' float4 records and the (p, q) pair).
+constexpr int SOFT_STAGES = 3;
+constexpr int SOFT_SUMS_BYTES = (45 * HS * 8 + 15) / 16 * 16;
+constexpr int SOFT_WARP_SMEM = SOFT_SUMS_BYTES + 32 * SOFT_STAGES * 48;
+constexpr int SOFT_SMEM = SOFT_WARPS * SOFT_WARP_SMEM;
 
 // ---------------------------------------------------------- tri / tetra
 // A loaded tri- or tetra-allelic site after its frequency fit: G' genotypes of
@@ -442,7 +450,8 @@ template <bool DIFF>
 __device__ __noinline__ int64_t soft_evaluate32(const float4* __restrict__ g32, const float2* __restrict__ pq32,
                                                 int64_t nk, int64_t x, int64_t y,
                                                 const double* xt, const double* xc, double f_old, double eps,
-                                                int lane, double* hs, const double* R, int64_t nm, PairEval& ev) {
+                                                int lane, double* hs, float4* slots, const double* R, int64_t nm,
+                                                PairEval& ev) {
     const bool diff = DIFF;
     float xh[9], sd[9];
 #pragma unroll
@@ -462,20 +471,41 @@ __device__ __noinline__ int64_t soft_evaluate32(const float4* __restrict__ g32, 
     const float e32 = (float)eps;
     const int nk32 = (int)nk;
     int64_t n = 0;
-    // the next site's records are loaded while this one is evaluated
-    float4 X = make_float4(0.f, 0.f, 0.f, 0.f), Y = X;
-    float2 PQ = make_float2(0.f, 0.f);
-    if (lane < nk32) { X = lx[lane]; Y = ly[lane]; PQ = pq32[lane]; }
-    // warp-uniform iterations (a lane past the end or at a missing sample
-    // skips the site), so that the FP64 flushes below run once per warp
+    // Warp-uniform iterations (a lane past the end or at a missing sample
+    // skips the site), so that the FP64 flushes below run once per warp.  The
+    // site two iterations ahead is copied by cp.async into the lane's slots:
+    // the prefetch holds no registers.
+    float4* my = slots + lane * (3 * SOFT_STAGES);
+    const uint32_t my0 = smem_u32(my);
+    auto issue = [&](int it2) {
+        const int k2 = lane + 32 * it2;
+        if (k2 < nk32) {
+            const uint32_t d = my0 + 48u * (uint32_t)(it2 % SOFT_STAGES);
+            cp_async16(d, lx + k2);
+            cp_async16(d + 16u, ly + k2);
+            cp_async8(d + 32u, pq32 + k2);
+        }
+        cp_async_commit();
+    };
     const int iters = (nk32 + 31) >> 5;
+    issue(0);
+    issue(1);
     for (int it = 0; it < iters; it++) {
+        issue(it + 2);
+        cp_async_wait<2>();   // this iteration's site has landed
         const int k = lane + 32 * it;
+        const float4* st = my + 3 * (it % SOFT_STAGES);
+        float4 X = make_float4(CUDART_NAN_F, 0.f, 0.f, 0.f), Y = X;
+        float2 PQ = make_float2(0.f, 0.f);
+        if (k < nk32) {
+            X = st[0];
+            Y = st[1];
+            PQ = *reinterpret_cast<const float2*>(st + 2);
+        }
         const float X0 = X.x, X1 = X.y, X2 = X.z, Y0 = Y.x, Y1 = Y.y, Y2 = Y.z;
         const float p = PQ.x, q = PQ.y;
-        if (k + 32 < nk32) { X = lx[k + 32]; Y = ly[k + 32]; PQ = pq32[k + 32]; }
-        // a missing sample has all three NaN
-        if (k < nk32 && !isnan(X0) && !isnan(Y0)) {
+        // a missing sample has all three NaN (and so has a lane past the end)
+        if (!isnan(X0) && !isnan(Y0)) {
             // L = sum over (gx, gy) of GLx(gx) GLy(gy) m(gx, gy), the nine rows
             // of the biallelic conditional table (cls_row) gathered by entry
             const float A = X0 * Y0, B = X2 * Y2, C = X0 * Y2, D = X2 * Y0, E = X0 * Y1;
@@ -496,9 +526,7 @@ __device__ __noinline__ int64_t soft_evaluate32(const float4* __restrict__ g32, 
             L[8] = fmaf(4.0f * I, p2 * q2,
                         fmaf(2.0f * (Fx + Hx), pq2 * q,
                              fmaf(2.0f * (E + Gx), p2q * p, fmaf(C + D, p2 * q2, fmaf(A, p2 * p2, B * (q2 * q2))))));
-            float d = e32;
-#pragma unroll
-            for (int i = 0; i < 9; i++) d = fmaf(L[i], xh[i], d);
+            const float d = dot9_eps(L, xh, e32);
             const float r = rcp_approx(d);
             float b[9];
 #pragma unroll
@@ -536,6 +564,7 @@ __device__ __noinline__ int64_t soft_evaluate32(const float4* __restrict__ g32, 
             }
         }
     }
+    cp_async_wait<0>();   // no copy outstanding into the slots (they are past the last site)
 #pragma unroll
     for (int i = 0; i < 9; i++) G[i] += (double)g[i];
     F += (double)o;
@@ -587,9 +616,10 @@ __global__ void __launch_bounds__(SOFT_WARPS * 32, 3) soft_pairs_kernel(
     const double* __restrict__ gl, int64_t n_sites, const int32_t* __restrict__ kept, const double* __restrict__ kp,
     const double* __restrict__ kq, const float4* __restrict__ g32, const float2* __restrict__ pq32, int prec64, int64_t nk, int64_t ns, int64_t n_rows, uint64_t iterations,
     kg_output* out, unsigned long long* next, int* no_rows, unsigned long long* stats, SoftMultiDev M) {
-    __shared__ double hsm[SOFT_WARPS][45 * HS];
+    extern __shared__ __align__(16) unsigned char soft_smem[];   // SOFT_WARP_SMEM per warp
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    double* hs = hsm[w];
+    double* hs = reinterpret_cast<double*>(soft_smem + w * SOFT_WARP_SMEM);
+    float4* slots = reinterpret_cast<float4*>(soft_smem + w * SOFT_WARP_SMEM + SOFT_SUMS_BYTES);
     // the warp's scratch for its pair's multi-allelic rows
     double* R = M.total > 0 ? M.scratch + ((int64_t)blockIdx.x * SOFT_WARPS + w) * M.total * 9 : nullptr;
     const Tune tu = make_tune(iterations);
@@ -624,9 +654,9 @@ __global__ void __launch_bounds__(SOFT_WARPS * 32, 3) soft_pairs_kernel(
                 m = soft_evaluate(gl, n_sites, kept, kp, kq, nk, x, y, xt, tu.epsilon, lane, hs, R, M.total, ev);
                 c_sites64 += (unsigned long long)m;
             } else {
-                m = diff ? soft_evaluate32<true>(g32, pq32, nk, x, y, xt, xc, f_old, tu.epsilon, lane, hs, R,
+                m = diff ? soft_evaluate32<true>(g32, pq32, nk, x, y, xt, xc, f_old, tu.epsilon, lane, hs, slots, R,
                                                  M.total, ev)
-                         : soft_evaluate32<false>(g32, pq32, nk, x, y, xt, xc, f_old, tu.epsilon, lane, hs, R,
+                         : soft_evaluate32<false>(g32, pq32, nk, x, y, xt, xc, f_old, tu.epsilon, lane, hs, slots, R,
                                                   M.total, ev);
             }
             c_sites += (unsigned long long)m;
@@ -811,13 +841,14 @@ int soft_relatedness(SoftWork& w, const DevBuf& gl, int64_t n_samples, int64_t n
     KG_SOFT_TRY(cudaGetDevice(&dev));
     KG_SOFT_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     int occ = 0;
-    KG_SOFT_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, soft_pairs_kernel, SOFT_WARPS * 32, 0));
+    KG_SOFT_TRY(cudaFuncSetAttribute(soft_pairs_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SOFT_SMEM));
+    KG_SOFT_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, soft_pairs_kernel, SOFT_WARPS * 32, SOFT_SMEM));
     const int64_t grid = (int64_t)sms * std::max(1, occ);
     if (M.total > 0) {
         KG_SOFT_TRY((cudaError_t)mscratch.reserve(sizeof(double) * 9 * (size_t)(grid * SOFT_WARPS * M.total)));
         M.scratch = mscratch.as<double>();
     }
-    soft_pairs_kernel<<<(unsigned)grid, SOFT_WARPS * 32, 0, st>>>(
+    soft_pairs_kernel<<<(unsigned)grid, SOFT_WARPS * 32, SOFT_SMEM, st>>>(
         gl.as<double>(), n_sites, idx.as<int32_t>(), kp.as<double>(), kq.as<double>(), g32.as<float4>(),
         pq32.as<float2>(), fp64 ? 1 : 0, nk, ns, rows, iterations, d_out, next, no_rows, stats, M);
     KG_SOFT_TRY(cudaGetLastError());

@@ -730,14 +730,19 @@ constexpr int MULTI_WARPS = 4;
 // shared-memory rows of a warp's sums (32 lane partials each): the 45 Hessian
 // terms, the 9 gradient terms, the objective
 constexpr int MULTI_HS_ROWS = 55;
-constexpr int MULTI_SMEM = MULTI_WARPS * MULTI_HS_ROWS * 32 * (int)sizeof(double);
+// per lane MULTI_STAGES row slots of 48 bytes after the sums
+constexpr int MULTI_STAGES = 3;
+constexpr int MULTI_WARP_SMEM = MULTI_HS_ROWS * 32 * (int)sizeof(double) + 32 * MULTI_STAGES * 48;
+constexpr int MULTI_SMEM = MULTI_WARPS * MULTI_WARP_SMEM;
 
-// A lane's next multi-allelic site: its two codes and table entry, then its
-// row (a zero row unless both calls use kept alleles only).
+// A lane's multi-allelic site as loaded: its two codes and table entry; then
+// its row index (ML_ROW_NONE: a missing call, ML_ROW_ZERO: a call with a
+// dropped allele, whose row is zero).
 struct MultiCodes {
     int a, b;
     int2 si;
 };
+constexpr int ML_ROW_NONE = -1, ML_ROW_ZERO = -2;
 __device__ __forceinline__ MultiCodes multi_codes(const CohortDev& co, const uint8_t* grx, const uint8_t* gry,
                                                   int64_t v, int64_t v1) {
     MultiCodes c{ML_MISSING, ML_MISSING, make_int2(0, 0)};
@@ -748,17 +753,10 @@ __device__ __forceinline__ MultiCodes multi_codes(const CohortDev& co, const uin
     }
     return c;
 }
-__device__ __forceinline__ bool multi_has_row(const MultiCodes& c) { return c.a < ML_ZERO_ROW && c.b < ML_ZERO_ROW; }
-__device__ __forceinline__ void multi_row(const CohortDev& co, const MultiCodes& c, float4& r0, float4& r1,
-                                          float4& r2) {
-    if (multi_has_row(c)) {
-        const float4* R = co.ml_rows32 + 3 * ((int64_t)c.si.x + c.a * c.si.y + c.b);
-        r0 = __ldg(R);
-        r1 = __ldg(R + 1);
-        r2 = __ldg(R + 2);
-    } else {
-        r0 = r1 = r2 = make_float4(0.f, 0.f, 0.f, 0.f);
-    }
+__device__ __forceinline__ int multi_row_index(const MultiCodes& c) {
+    if (c.a == ML_MISSING || c.b == ML_MISSING) return ML_ROW_NONE;
+    if (c.a == ML_ZERO_ROW || c.b == ML_ZERO_ROW) return ML_ROW_ZERO;
+    return c.si.x + c.a * c.si.y + c.b;
 }
 
 template <bool DIFF>
@@ -781,23 +779,37 @@ __device__ __forceinline__ void multi_unit32(const CohortDev& co, const SlotStat
     int nzero = 0;
     for (int k = 0; k < MULTI_HS_ROWS; k++) hs[32 * k + lane] = 0.0;
     // Warp-uniform iterations, so that the FP64 flushes run once per warp.
-    // Loads run ahead: the codes two sites ahead, the row one site ahead (the
-    // row's address needs the codes).
+    // Loads run ahead without holding registers: the codes three sites ahead
+    // into registers, the row two sites ahead by cp.async into the lane's
+    // MULTI_STAGES slots in shared memory (the row's address needs the codes).
     const int iters = (int)((v1 - v0 + 31) >> 5);
-    MultiCodes c0 = multi_codes(co, grx, gry, v0 + lane, v1);
-    MultiCodes c1 = multi_codes(co, grx, gry, v0 + lane + 32, v1);
-    float4 r0, r1, r2;
-    multi_row(co, c0, r0, r1, r2);
+    float4* slots = reinterpret_cast<float4*>(hs + 32 * MULTI_HS_ROWS) + lane * (3 * MULTI_STAGES);
+    const uint32_t slot0 = smem_u32(slots);
+    auto issue_row = [&](int ri, int stage) {
+        if (ri >= 0) {
+            const float4* R = co.ml_rows32 + 3 * (int64_t)ri;
+            const uint32_t d = slot0 + 48u * (uint32_t)stage;
+            cp_async16(d, R);
+            cp_async16(d + 16u, R + 1);
+            cp_async16(d + 32u, R + 2);
+        }
+        cp_async_commit();
+    };
+    int ri0 = multi_row_index(multi_codes(co, grx, gry, v0 + lane, v1));
+    int ri1 = multi_row_index(multi_codes(co, grx, gry, v0 + lane + 32, v1));
+    issue_row(ri0, 0);
+    issue_row(ri1, 1);
+    MultiCodes c2 = multi_codes(co, grx, gry, v0 + lane + 64, v1);
     for (int it = 0; it < iters; it++) {
-        const MultiCodes c = c0;
-        const float L[9] = {r0.x, r0.y, r0.z, r0.w, r1.x, r1.y, r1.z, r1.w, r2.x};
-        multi_row(co, c1, r0, r1, r2);
-        c0 = c1;
-        c1 = multi_codes(co, grx, gry, v0 + lane + 32 * (int64_t)(it + 2), v1);
-        if (multi_has_row(c)) {
-            float d = e32;
-#pragma unroll
-            for (int k = 0; k < 9; k++) d = fmaf(L[k], xh[k], d);
+        const int ri2 = multi_row_index(c2);
+        issue_row(ri2, (it + 2) % MULTI_STAGES);
+        c2 = multi_codes(co, grx, gry, v0 + lane + 32 * (int64_t)(it + 3), v1);
+        cp_async_wait<2>();   // this site's row has landed
+        if (ri0 >= 0) {
+            const float4* Rs = slots + 3 * (it % MULTI_STAGES);
+            const float4 r0 = Rs[0], r1 = Rs[1], r2 = Rs[2];
+            const float L[9] = {r0.x, r0.y, r0.z, r0.w, r1.x, r1.y, r1.z, r1.w, r2.x};
+            const float d = dot9_eps(L, xh, e32);
             const float r = rcp_approx(d);
             float q[9];
 #pragma unroll
@@ -818,9 +830,11 @@ __device__ __forceinline__ void multi_unit32(const CohortDev& co, const SlotStat
                 for (int k = 0; k < 9; k++) dl = fmaf(L[k], sd[k], dl);
                 o += neg_log1m(dl * r);
             }
-        } else if (c.a != ML_MISSING && c.b != ML_MISSING) {
-            nzero++;   // a call with a dropped allele: a zero row
+        } else if (ri0 == ML_ROW_ZERO) {
+            nzero++;
         }
+        ri0 = ri1;
+        ri1 = ri2;
         if ((it & 7) == 7) {
 #pragma unroll
             for (int k = 0; k < 9; k++) {
@@ -839,6 +853,7 @@ __device__ __forceinline__ void multi_unit32(const CohortDev& co, const SlotStat
             }
         }
     }
+    cp_async_wait<0>();   // no copy outstanding into the slots (they are past the last site)
     // the partials leave the registers before the reductions
 #pragma unroll
     for (int k = 0; k < 45; k++) hs[32 * k + lane] += (double)h[k];
@@ -955,7 +970,7 @@ extern "C" __global__ void __launch_bounds__(MULTI_WARPS * 32, 3) wave_multi_ker
     const int64_t nwarps = (int64_t)gridDim.x * (blockDim.x >> 5);
     const int64_t ntask = (int64_t)A.wc_cur->n_pass * A.ml_units;
     const double eps = A.tune.epsilon;
-    double* hs = multi_smem + (threadIdx.x >> 5) * (MULTI_HS_ROWS * 32);
+    double* hs = multi_smem + (threadIdx.x >> 5) * (MULTI_WARP_SMEM / (int)sizeof(double));
     for (int64_t t = warp; t < ntask; t += nwarps) {
         const int s = A.pass_cur[t / A.ml_units];
         const int u = (int)(t % A.ml_units);
