@@ -185,7 +185,11 @@ int kg_relatedness_gt(kg_ctx *ctx, int64_t num_samples, uint64_t iterations,
  * frequencies come from the per-site HWE SQP on the likelihoods (capped at
  * `iterations`), with the maf cut (maf < 0 or NaN: 1/(2 n_samples)); each
  * pair's rows are sum over genotype pairs of GLx GLy m(gx, gy), and the SQP is
- * that of kg_relatedness.  The first form runs in FP64 with a warp per pair. */
+ * that of kg_relatedness, a warp per pair.  Evaluations follow the context's
+ * precision (kg_set_precision): KG_PREC_FP32C evaluates in FP32 from FP32
+ * copies of the likelihoods with FP64 sums, and re-runs a pair in FP64 by the
+ * rule of kg_relatedness; KG_PREC_FP64 evaluates every pair in FP64.  The
+ * device buffers of the call stay with the context for the next call. */
 int kg_load_likelihoods(kg_ctx *ctx, const double *gl, int64_t n_samples, int64_t n_sites);
 /* Tri- or tetra-allelic sites for kg_relatedness_gl (the reference's gl3 and
  * gl4, src/coefficients.rs:99-106): gl is n_samples x n_sites x G doubles

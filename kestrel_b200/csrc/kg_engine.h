@@ -210,6 +210,7 @@ struct Workspace {
     DevBuf scratch, queue, counters, table;
     DevBuf partial, slots, lists_a, lists_b, tasks, counts, done;
     DevBuf ml_partial;   // per slot and unit, the sums of the ML path's tri-/tetra-allelic sites
+    DevBuf qp;           // per slot the QP's inputs and solution, and the wave's list of QP slots
     PinBuf host;   // per-wave counters read back by the host loop
     int sm_count = 0;
     // run_pairs' engine, kept between calls: a call of the same shape only

@@ -7,6 +7,7 @@
 
 #include "kg_engine.h"
 #include "kg_bulk.cuh"
+#include "kg_qp1.cuh"
 #include "kg_wave.cuh"
 
 namespace kg {
@@ -1292,20 +1293,70 @@ extern "C" __global__ void __launch_bounds__(128, 4) wave_solve_kernel(WaveArgs 
         finish_slot(A, S, s, x, f, it, condition_rows(grp, x, g, Hr, tu.sqp_conv_tol), lane);
         return;
     }
-    // ---- QP step (src/sqp.rs:78-83): c = g - H x, y = QP(H, c, x), p = y - x
-    double cr = 0.0;
-    if (lane < 9) cr = pick9(g, lane) - dot_fma(9, Hr, x);
-    double c[9], y[9], p[9];
-    gather9(grp, cr, c);
-    qp_simplex_rows(grp, Hr, c, x, tu, lane, y);
+    // ---- QP step (src/sqp.rs:78-83): c = g - H x, y = QP(H, c, x).  Its
+    // inputs go to the slot's QP buffer and the slot to this wave's QP list:
+    // wave_qp_kernel solves them a thread per slot, wave_step_kernel takes the
+    // step from the solution.
+    double* Qb = A.qp_buf + (int64_t)s * QP_VALS;
+    if (lane < 9) {
 #pragma unroll
-    for (int k = 0; k < 9; k++) p[k] = y[k] - x[k];
+        for (int k = 0; k < 9; k++) Qb[lane * 9 + k] = Hr[k];
+        Qb[81 + lane] = pick9(g, lane) - dot_fma(9, Hr, x);
+    }
+    if (lane == 0) A.qp_list[atomicAdd(&A.wc_cur->n_qp, 1)] = s;
+}
+
+// The QP of every slot in this wave's QP list, a thread per slot (kg_qp1.cuh,
+// the same arithmetic as the row-parallel form); the solution replaces c's
+// neighbour in the slot's QP buffer.
+extern "C" __global__ void __launch_bounds__(128) wave_qp_kernel(WaveArgs A) {
+    if (A.clk->stop) return;   // a device loop past its last wave
+    const PhaseEnd pe{&A.clk->end[2], (threadIdx.x & 31) == 0};   // timed as part of the solve phase
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= A.wc_cur->n_qp) return;
+    const int s = A.qp_list[i];
+    double* Qb = A.qp_buf + (int64_t)s * QP_VALS;
+    double Q[9][9], c[9], x[9], y[9];
+#pragma unroll
+    for (int r = 0; r < 9; r++) {
+#pragma unroll
+        for (int k = 0; k < 9; k++) Q[r][k] = Qb[r * 9 + k];
+        c[r] = Qb[81 + r];
+        x[r] = A.slots[s].xc[r];
+    }
+    qp_simplex_thread(Q, c, x, A.tune, y);
+#pragma unroll
+    for (int k = 0; k < 9; k++) Qb[90 + k] = y[k];
+}
+
+// The step after each QP (src/sqp.rs:78-90): p = y - x, the first trial point
+// x + p (normalised) and its pass.  Half-warp per slot, as the solve kernel.
+extern "C" __global__ void __launch_bounds__(128) wave_step_kernel(WaveArgs A) {
+    const int wib = threadIdx.x >> 5, half = (threadIdx.x >> 4) & 1;
+    const int lane = threadIdx.x & 15;
+    const HalfGrp grp{half ? 0xFFFF0000u : 0x0000FFFFu};
+    const int i = (blockIdx.x * WAVE_WPB + wib) * 2 + half;
+    if (A.clk->stop) return;   // a device loop past its last wave
+    const PhaseEnd pe{&A.clk->end[2], (threadIdx.x & 31) == 0};
+    if (i >= A.wc_cur->n_qp) return;
+    const int s = A.qp_list[i];
+    SlotState& S = A.slots[s];
+    const double* Qb = A.qp_buf + (int64_t)s * QP_VALS;
+    double x[9], g[9], p[9];
+#pragma unroll
+    for (int k = 0; k < 9; k++) {
+        x[k] = S.xc[k];
+        g[k] = S.g[k];
+        p[k] = Qb[90 + k] - x[k];
+    }
     const double gp = dot_fma(9, g, p);
     double xn[9];
 #pragma unroll
     for (int k = 0; k < 9; k++) xn[k] = x[k] + 1.0 * p[k];
     normalise9(xn);
+    const bool fp64 = S.fp64 != 0;
     const int nkind = fp64 ? PASS_FP64 : (fabs(gp) < DIFF_BELOW ? PASS_FP32_DIFF : PASS_FP32_DIRECT);
+    grp.sync();   // every lane has read S before lane 0 writes it
     if (lane == 0) {
         for (int k = 0; k < 9; k++) { S.p[k] = p[k]; S.xt[k] = xn[k]; }
         S.gp = gp;
@@ -1368,7 +1419,7 @@ struct WaveEngine::Impl {
     RunConfig cfg;
     int64_t n_slots = 0, list_cap = 0, task_cap = 0;
     int max_units = 0, max_jobs = 0;
-    int pass_blocks = 0, admit_blocks = 0, solve_blocks = 0, multi_blocks = 0;
+    int pass_blocks = 0, admit_blocks = 0, solve_blocks = 0, multi_blocks = 0, qp_blocks = 0;
     WaveArgs A{};
     WaveCounts* wc = nullptr;
     int* admit_task = nullptr;
@@ -1473,6 +1524,7 @@ int WaveEngine::open(Workspace& ws, cudaStream_t st, const RunConfig& cfg, int64
     KG_WAVE_TRY((cudaError_t)ws.ml_partial.reserve(sizeof(double) * (size_t)std::max(1, cfg.ml_units) * ML_VALS *
                                                    (size_t)(cfg.ml_units > 0 ? n_slots : 1)));
     KG_WAVE_TRY((cudaError_t)ws.slots.reserve(sizeof(SlotState) * n_slots));
+    KG_WAVE_TRY((cudaError_t)ws.qp.reserve((sizeof(double) * QP_VALS + sizeof(int)) * (size_t)n_slots));
     KG_WAVE_TRY((cudaError_t)ws.lists_a.reserve(sizeof(int) * 2 * n_slots));   // pass lists
     KG_WAVE_TRY((cudaError_t)ws.lists_b.reserve(sizeof(int) * 2 * n_slots));   // free lists
     KG_WAVE_TRY((cudaError_t)ws.tasks.reserve(sizeof(int4) * 2 * 5 * E.task_cap));
@@ -1503,7 +1555,7 @@ int WaveEngine::open(Workspace& ws, cudaStream_t st, const RunConfig& cfg, int64
     E.live_h->n_cohorts = 0;
     const std::vector<void*> bufs{ws.scratch.p, ws.partial.p, ws.slots.p,    ws.lists_a.p, ws.lists_b.p,
                                   ws.tasks.p,   ws.counts.p,  ws.queue.p,    ws.counters.p, ws.table.p,
-                                  ws.done.p,    ws.host.p,    ws.ml_partial.p};
+                                  ws.done.p,    ws.host.p,    ws.ml_partial.p, ws.qp.p};
     const bool reuse = same_call && bufs == E.key_bufs;
     // the job state of a fresh engine
     E.table.clear();
@@ -1549,6 +1601,7 @@ int WaveEngine::open(Workspace& ws, cudaStream_t st, const RunConfig& cfg, int64
     }
     E.admit_blocks = ws.sm_count * aocc;
     E.solve_blocks = (int)((n_slots + 2 * WAVE_WPB - 1) / (2 * WAVE_WPB));   // two slots per warp
+    E.qp_blocks = (int)((n_slots + 127) / 128);                               // a thread per slot
     E.multi_blocks = 0;
     if (cfg.ml_units > 0) {
         int mocc = 0;
@@ -1578,6 +1631,8 @@ int WaveEngine::open(Workspace& ws, cudaStream_t st, const RunConfig& cfg, int64
     A.ml_partial = ws.ml_partial.as<double>();
     A.ml_units = cfg.ml_units;
     A.ml_chunk = cfg.ml_chunk;
+    A.qp_buf = ws.qp.as<double>();
+    A.qp_list = reinterpret_cast<int*>(A.qp_buf + (size_t)QP_VALS * n_slots);
     A.unit_elems = unit;
     E.drop_loop();
     // One wave (counter resets, admit, pass, solve, read-back) captured as a
@@ -1627,6 +1682,8 @@ int WaveEngine::open(Workspace& ws, cudaStream_t st, const RunConfig& cfg, int64
         }
         if (ce == cudaSuccess) {
             wave_solve_kernel<<<E.solve_blocks, 128, wsm, st>>>(Aw);
+            wave_qp_kernel<<<E.qp_blocks, 128, 0, st>>>(Aw);
+            wave_step_kernel<<<E.solve_blocks, 128, 0, st>>>(Aw);
             ce = cudaEventRecordWithFlags(E.ev[par][3], st, cudaEventRecordExternal);
         }
         if (ce == cudaSuccess) ce = cudaMemcpyAsync(E.h_wc, wc + nxt, sizeof(WaveCounts), cudaMemcpyDeviceToHost, st);
@@ -1698,7 +1755,7 @@ int WaveEngine::wave(std::vector<int>& finished, std::string& err) {
     const cudaStream_t st = E.st;
     KG_WAVE_TRY(cudaGraphLaunch(E.x[E.cur], st));
     KG_WAVE_TRY(cudaStreamSynchronize(st));
-    E.launches += E.multi_blocks ? 4 : 3;
+    E.launches += E.multi_blocks ? 6 : 5;
     E.waves++;
     for (size_t k = 0; k < E.table.size(); k++)
         if (!E.reported[k] && E.h_done[k] >= (unsigned long long)E.table[k].n_pairs) {
@@ -1742,6 +1799,8 @@ int WaveEngine::run_until_idle(unsigned long long max_waves, std::string& err) {
             wave_pass_kernel<<<E.pass_blocks, 128, WAVE_WPB * PASS_WARP_SMEM, st>>>(Aw);
             if (E.multi_blocks) wave_multi_kernel<<<E.multi_blocks, MULTI_WARPS * 32, MULTI_SMEM, st>>>(Aw);
             wave_solve_kernel<<<E.solve_blocks, 128, WAVE_WPB * WARP_SMEM, st>>>(Aw);
+            wave_qp_kernel<<<E.qp_blocks, 128, 0, st>>>(Aw);
+            wave_step_kernel<<<E.solve_blocks, 128, 0, st>>>(Aw);
             wave_end_kernel<<<1, 32, 0, st>>>(Aw, k, h, max_waves);
         }
         cudaGraph_t captured = nullptr;
@@ -1769,7 +1828,7 @@ int WaveEngine::run_until_idle(unsigned long long max_waves, std::string& err) {
         E.total += (double)c.acc[i] * 1e-6;
     }
     E.waves += c.waves;
-    E.launches += (E.multi_blocks ? 10 : 8) * c.iters;
+    E.launches += (E.multi_blocks ? 14 : 12) * c.iters;
     E.cur ^= (int)(c.waves & 1);
     E.last_q = *E.h_q;
     // the next wave's counts, as a host wave would have read them; the clock

@@ -59,6 +59,8 @@ struct WaveCounts {
     int n_free;      // slots for the admit step: free ones and those waiting for FP64 lists
     int n_resort;    // of those, slots waiting for FP64 lists
     int units[5];    // pass work units per shape
+    int n_qp;        // slots whose SQP step needs a QP (wave_qp_kernel) this wave
+    int pad;
 };
 
 // The job table's extent, in device memory so that jobs can be appended
@@ -130,6 +132,8 @@ struct WaveArgs {
     double* ml_partial;            // per slot: ml_units * ML_VALS sums of its tri-/tetra-allelic sites
     int ml_units;                  // their work units per slot (0: no cohort has such sites)
     int ml_chunk;                  // kept sites per such unit (a multiple of 32, at most ML_CHUNK)
+    double* qp_buf;                // per slot QP_VALS: Q (9 x 9 row-major), c, the solution y
+    int* qp_list;                  // the slots of this wave's QPs (wc_cur->n_qp of them)
     int unit_elems;                // list entries per pass work unit
 };
 
@@ -139,6 +143,8 @@ struct WaveArgs {
 // objective term.
 constexpr int ML_CHUNK = 8192;
 constexpr int ML_VALS = 56;
+// a slot's QP: Q at 0, c at 81, the solution at 90
+constexpr int QP_VALS = 100;
 
 __device__ __forceinline__ int shape_ng(int s) { return s == 0 ? 4 : s == 3 ? 4 : s == 4 ? 2 : 3; }
 __device__ __forceinline__ int shape_nh(int s) { return s == 0 ? 7 : s == 3 ? 9 : s == 4 ? 3 : 5; }
