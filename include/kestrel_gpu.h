@@ -65,7 +65,7 @@ typedef enum {
 } kg_status;
 
 typedef enum {
-    KG_PREC_FP32C = 0,  /* FP32 site sums with compensation; FP64 solver (default) */
+    KG_PREC_FP32C = 0,  /* FP32 site sums promoted to FP64 every few sites; FP64 solver (default) */
     KG_PREC_FP64 = 1    /* FP64 throughout (the plain FP64 GPU form) */
 } kg_precision;
 
@@ -82,7 +82,7 @@ const char *kg_version(void);
 int kg_set_precision(kg_ctx *ctx, int precision);
 
 /* Launch shape of the pair engine: pairs in flight per wave (slots; 0 = an
- * eighth of the pairs, from 4096 to 32768, as memory allows) and blocks per SM
+ * eighth of the pairs, from 4096 to 65536, as memory allows) and blocks per SM
  * of the site-pass kernel (0 = the occupancy limit).  Exposed for the
  * autotuner and tests; results do not depend on it. */
 int kg_set_launch(kg_ctx *ctx, int slots, int blocks_per_sm);
@@ -105,7 +105,7 @@ int kg_set_work_unit(kg_ctx *ctx, int entries);
 
 /* The context's launch shape: pairs in flight (0 = automatic), site-pass blocks
  * per SM (0 = occupancy limit), work unit (0 = default) and the divisor of the
- * automatic pairs in flight (the job's pairs / divisor, within 4096..32768).
+ * automatic pairs in flight (the job's pairs / divisor, within 4096..65536).
  * Any pointer may be NULL. */
 int kg_get_launch(const kg_ctx *ctx, int *slots, int *blocks_per_sm, int *unit_entries, int *slot_divisor);
 
