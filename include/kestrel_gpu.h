@@ -109,13 +109,14 @@ int kg_set_work_unit(kg_ctx *ctx, int entries);
  * Any pointer may be NULL. */
 int kg_get_launch(const kg_ctx *ctx, int *slots, int *blocks_per_sm, int *unit_entries, int *slot_divisor);
 
-/* Runs the autotuner on a sample of the loaded cohort (about 32,768 pairs of
- * its first samples) and keeps the fastest launch shape: site-pass blocks per
- * SM (occupancy limit, 4, 3), the work unit (16384, 8192, 4096 entries) and the
- * automatic pairs in flight (an eighth, a quarter or a sixteenth of a job's
- * pairs), by coordinate descent, a change kept only when it is more than 2%
- * faster.  Writes *slots (0: automatic) and *blocks_per_sm if non-NULL;
- * kg_get_launch reports the rest. */
+/* Runs the autotuner on a sample of the loaded cohort (about 131,072 pairs of
+ * its first samples) and keeps the fastest launch shape, by coordinate descent,
+ * a change kept only when it is more than 2% faster: site-pass blocks per SM
+ * (occupancy limit, 4, 3) and the work unit (16384, 8192, 4096 entries), judged
+ * by the site passes' device time; then, for a cohort of fewer than 524,288
+ * pairs, the automatic pairs in flight (an eighth, a quarter or a sixteenth of
+ * a job's pairs), judged by the sample's whole device time.  Writes *slots (0:
+ * automatic) and *blocks_per_sm if non-NULL; kg_get_launch reports the rest. */
 int kg_autotune(kg_ctx *ctx, int *slots, int *blocks_per_sm);
 
 /* ---------------------------------------------------------------- cohort */

@@ -894,9 +894,12 @@ int kg_autotune(kg_ctx* c, int* slots_out, int* bps_out) {
                                 c->af_set ? c->af.data() : nullptr, -1.0, c->stream, err);
         if (st) return set_err(c, st, err);
         c->cohort.ml_nk = 0;   // the sample runs the biallelic sites
+        // a sample of about 131,072 pairs: enough waves of full slots that the
+        // pass kernel runs as in a large job
         int64_t ns = 2;
-        while (ns < c->cohort.n_samples && ns * (ns + 1) / 2 < 32768) ns++;
+        while (ns < c->cohort.n_samples && ns * (ns + 1) / 2 < 131072) ns++;
         const int64_t np = ns * (ns + 1) / 2;
+        const int64_t full_pairs = c->cohort.n_samples * (c->cohort.n_samples + 1) / 2;
         if (c->dout.reserve(sizeof(kg_output) * np) != cudaSuccess)
             return set_err(c, KG_ENOMEM, "cannot allocate device output rows");
         kg::PairJob jb;
@@ -904,7 +907,12 @@ int kg_autotune(kg_ctx* c, int* slots_out, int* bps_out) {
         jb.n_x = ns;
         jb.d_out = c->dout.as<kg_output>();
         int bps = 0, unit = 0, div = 8;
-        auto cost = [&](int b, int u, int d, double& ms) -> int {
+        // The site-pass shape (blocks per SM, work unit) is judged by the pass
+        // phase's device time: every shape runs the same passes, and the wave
+        // tail of a sample does not mislead it.  The share of pairs in flight
+        // only matters for jobs below 8 x 65,536 pairs; it is judged by the
+        // sample's whole device time, and only for such a cohort.
+        auto cost = [&](int b, int u, int d, bool whole, double& ms) -> int {
             kg::RunConfig cfg = run_config(c, 100);
             cfg.slots = 0;
             cfg.pass_blocks_per_sm = b;
@@ -914,16 +922,16 @@ int kg_autotune(kg_ctx* c, int* slots_out, int* bps_out) {
                 kg_run_stats stt{};
                 int r = kg::run_pairs({jb}, cfg, c->ws, c->stream, stt, err);
                 if (r && r != KG_ENOSITES) return r;
-                ms = stt.pair_kernel_ms;
+                ms = whole ? stt.pair_kernel_ms : stt.pass_ms;
             }
             return KG_OK;
         };
         double best = 0.0;
-        st = cost(bps, unit, div, best);
+        st = cost(bps, unit, div, false, best);
         if (st) return set_err(c, st, err);
-        auto consider = [&](int b, int u, int d) -> int {
+        auto consider = [&](int b, int u, int d, bool whole) -> int {
             double ms = 0.0;
-            int r = cost(b, u, d, ms);
+            int r = cost(b, u, d, whole, ms);
             if (r) return r;
             if (ms < 0.98 * best) {
                 best = ms;
@@ -934,11 +942,14 @@ int kg_autotune(kg_ctx* c, int* slots_out, int* bps_out) {
             return KG_OK;
         };
         for (int b : {4, 3})
-            if ((st = consider(b, unit, div))) return set_err(c, st, err);
+            if ((st = consider(b, unit, div, false))) return set_err(c, st, err);
         for (int u : {8192, 4096})
-            if ((st = consider(bps, u, div))) return set_err(c, st, err);
-        for (int d : {4, 16})
-            if ((st = consider(bps, unit, d))) return set_err(c, st, err);
+            if ((st = consider(bps, u, div, false))) return set_err(c, st, err);
+        if (full_pairs / 8 < 65536) {
+            if ((st = cost(bps, unit, div, true, best))) return set_err(c, st, err);
+            for (int d : {4, 16})
+                if ((st = consider(bps, unit, d, true))) return set_err(c, st, err);
+        }
         c->wave_slots = 0;
         c->pass_bps = bps;
         c->unit_elems = unit;
