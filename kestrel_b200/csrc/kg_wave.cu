@@ -26,19 +26,8 @@ constexpr int WAVE_WPB = 4;   // warps per block of the three wave kernels
 // ------------------------------------------------------------------ admit
 
 constexpr int ADMIT_WARPS = 8;   // warps that build one pair's lists together
-constexpr int ADMIT_WARP_SMEM = UNIT_SITES * 4;   // FP32 output buffer
+constexpr int ADMIT_WARP_SMEM = UNIT_SITES * 4 + 6 * 32 * 4;   // FP32 output buffer, lane write positions
 
-// 64-bit shifts as PTX defines them: an amount of 64 or more gives 0.
-__device__ __forceinline__ unsigned long long shr64(unsigned long long v, unsigned s) {
-    unsigned long long r;
-    asm("shr.b64 %0, %1, %2;" : "=l"(r) : "l"(v), "r"(s));
-    return r;
-}
-__device__ __forceinline__ unsigned long long shl64(unsigned long long v, unsigned s) {
-    unsigned long long r;
-    asm("shl.b64 %0, %1, %2;" : "=l"(r) : "l"(v), "r"(s));
-    return r;
-}
 
 // Writes the frequency value t (p or 1 - p by the site's sel bit) of every
 // jointly observed site of units [u0, u1) into its shape list, in site order,
@@ -92,27 +81,27 @@ __device__ inline void scatter_lockstep(const CohortDev& co, int64_t x, int64_t 
         __syncwarp();
         if (sizeof(T) == 4) {
             // Branch-free: each site has a field index f (A 0, B1 1, B2 2, C 3,
-            // D 4, not jointly observed 5) and the lane's position counters sit
-            // 13 bits apart in R, counting down from 1023: a site of shape f
-            // goes to 1023 - field f and decrements it.  For f = 5 the shift
-            // of 65 reads 0 and decrements nothing, so such a site writes to
-            // position 1023, which no list value of the unit uses (the unit
-            // has fewer than 1024 of them).  A counter that passes 0 only
-            // borrows from counters this lane no longer writes.
+            // D 4, not jointly observed 5) and the lane's write position for
+            // each field sits in shared memory (counters[f][lane]): a site
+            // writes at its field's position and advances it by its observed
+            // bit.  Field 5 stays at 1023, which no list value of the unit
+            // uses unless all 1,024 sites are observed, when field 5 is never
+            // taken.  (Positions kept as 13-bit fields of one 64-bit register
+            // cost 2% more admit time in 64-bit shifts.)
             const unsigned obs = sm.m[0] | sm.m[1] | sm.m[2] | sm.m[3] | sm.m[4];
             const unsigned f0 = sm.m[1] | sm.m[3] | ~obs, f1 = sm.m[2] | sm.m[3], f2 = sm.m[4] | ~obs;
             const unsigned long long pre = ust + (inc - v);
-            unsigned long long R = 0;
+            int* cnt = reinterpret_cast<int*>(wsm + UNIT_SITES * 4) + lane;
 #pragma unroll
-            for (int k = 0; k < 5; k++)
-                R += (unsigned long long)((long long)(1023 - (int)((pre >> (11 * k)) & 0x7FFull)) << (13 * k));
+            for (int k = 0; k < 5; k++) cnt[32 * k] = (int)((pre >> (11 * k)) & 0x7FFull);
+            cnt[32 * 5] = 1023;
             const float* st = reinterpret_cast<const float*>(freq);
 #pragma unroll 8
             for (int i = 0; i < 32; i++) {
                 const unsigned f = ((f0 >> i) & 1u) | (((f1 >> i) & 1u) << 1) | (((f2 >> i) & 1u) << 2);
-                const unsigned sh = 13u * f;
-                const int pos = 1023 - (int)(shr64(R, sh) & 0x3FFull);
-                R -= shl64(1ull, sh);
+                int* c = cnt + 32 * f;
+                const int pos = *c;
+                *c = pos + (int)((obs >> i) & 1u);
                 const float p = __ldg(st + i * 32 + lane);
                 obuf[pos] = ((sl >> i) & 1u) ? 1.0f - p : p;
             }
