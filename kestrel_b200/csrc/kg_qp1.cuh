@@ -8,19 +8,20 @@
 // It computes what the row-parallel form (qp_simplex_rows in kg_rowsolve.cuh)
 // computes, operation for operation and in the same order (the same FMAs,
 // divisions and sequential sums), so both give the same bits; with a thread
-// per slot a warp serves 32 pairs' QPs instead of two.  Q, L and the vectors
-// are fixed-size arrays indexed by loop counters that unroll, so they stay in
-// registers or the thread's local memory.
+// per slot a warp serves 32 pairs' QPs instead of two.  Q is read where it
+// lies (the slot's QP buffer, through L1); L and the vectors are fixed-size
+// arrays indexed by loop counters that unroll, so they stay in registers or
+// the thread's local memory.
 #pragma once
 
 #include "kg_solver.cuh"
 
 namespace kg {
 
-// GMW81-modified LDL^T of the free block (mask F, nf free) of the 9 x 9 Q;
-// L unit lower triangular with identity rows and columns for the fixed
-// variables, d their diagonal 1.
-__device__ __forceinline__ void ldl_gmw_thread(const double (&Q)[9][9], unsigned F, int nf, double (&L)[9][9],
+// GMW81-modified LDL^T of the free block (mask F, nf free) of the 9 x 9 Q,
+// which it reads inside that block only; L unit lower triangular with
+// identity rows and columns for the fixed variables, d their diagonal 1.
+__device__ __forceinline__ void ldl_gmw_thread(const double (*Q)[9], unsigned F, int nf, double (&L)[9][9],
                                                double (&d)[9]) {
     double gamma = 0.0, xi = 0.0;
 #pragma unroll
@@ -118,7 +119,7 @@ __device__ __forceinline__ void ldl_solve2_thread(const double (&L)[9][9], const
 }
 
 // The QP from y0 (y0 and y may alias).  Returns the iteration count.
-__device__ inline int qp_simplex_thread(const double (&Q)[9][9], const double (&c)[9], const double* y0,
+__device__ inline int qp_simplex_thread(const double (*Q)[9], const double (&c)[9], const double* y0,
                                         const Tune& tu, double* y) {
     unsigned work = 0;
 #pragma unroll
@@ -131,23 +132,21 @@ __device__ inline int qp_simplex_thread(const double (&Q)[9][9], const double (&
         const unsigned F = (~work) & 0x1FFu;
         const int nf = __popc(F);
         if (nf == 0) return it;
-        // the free block, its gradient c_f + Q_f y_f and the ones vector
-        double Qf[9][9], gf[9], on[9];
+        // the free block's gradient c_f + Q_f y_f and the ones vector (the
+        // factorisation below reads Q inside the free block only)
+        double gf[9], on[9];
 #pragma unroll
         for (int r = 0; r < 9; r++) {
             const bool rf = (F >> r) & 1u;
             double s = 0.0;
 #pragma unroll
-            for (int j = 0; j < 9; j++) {
-                const bool jf = (F >> j) & 1u;
-                Qf[r][j] = (rf && jf) ? Q[r][j] : 0.0;
-                if (rf && jf) s = fma(Qf[r][j], y[j], s);
-            }
+            for (int j = 0; j < 9; j++)
+                if (rf && ((F >> j) & 1u)) s = fma(Q[r][j], y[j], s);
             gf[r] = rf ? c[r] + s : 0.0;
             on[r] = rf ? 1.0 : 0.0;
         }
         double L[9][9], d[9];
-        ldl_gmw_thread(Qf, F, nf, L, d);
+        ldl_gmw_thread(Q, F, nf, L, d);
         ldl_solve2_thread(L, d, gf, on);
         double sg = 0.0, so = 0.0;
 #pragma unroll

@@ -1305,15 +1305,13 @@ extern "C" __global__ void __launch_bounds__(128) wave_qp_kernel(WaveArgs A) {
     if (i >= A.wc_cur->n_qp) return;
     const int s = A.qp_list[i];
     double* Qb = A.qp_buf + (int64_t)s * QP_VALS;
-    double Q[9][9], c[9], x[9], y[9];
+    double c[9], x[9], y[9];
 #pragma unroll
     for (int r = 0; r < 9; r++) {
-#pragma unroll
-        for (int k = 0; k < 9; k++) Q[r][k] = Qb[r * 9 + k];
         c[r] = Qb[81 + r];
         x[r] = A.slots[s].xc[r];
     }
-    qp_simplex_thread(Q, c, x, A.tune, y);
+    qp_simplex_thread(reinterpret_cast<const double (*)[9]>(Qb), c, x, A.tune, y);
 #pragma unroll
     for (int k = 0; k < 9; k++) Qb[90 + k] = y[k];
 }
