@@ -257,17 +257,21 @@ def run_batch(args, local):
     from kestrel_b200 import synth
     cohorts = synth.config2()
     pairs = sum(c.codes.shape[0] * (c.codes.shape[0] - 1) // 2 for c in cohorts)
+    import torch
     est = kb.Estimator(device=local, precision=args.precision)
     est.set_launch(args.slots, args.pass_bps)
     inputs = [(c.codes,) for c in cohorts]
+    # page-locked row buffers, reused by every call
+    outs = [torch.empty(c.codes.shape[0] * (c.codes.shape[0] + 1) // 2 * kb.OUTPUT_DTYPE.itemsize,
+                        dtype=torch.uint8, pin_memory=True).numpy().view(kb.OUTPUT_DTYPE) for c in cohorts]
 
     def timed():
         for _ in range(max(1, args.warmup)):
-            est.relatedness_batch(inputs)
+            est.relatedness_batch(inputs, out=outs)
         wall, waves = [], []
         for _ in range(max(1, args.steps)):
             t0 = time.perf_counter()
-            est.relatedness_batch(inputs)
+            est.relatedness_batch(inputs, out=outs)
             wall.append(time.perf_counter() - t0)
             waves.append(est.run_stats()["pair_kernel_ms"])
         return float(np.mean(wall)), float(np.mean(waves)), est.run_stats()
@@ -289,7 +293,8 @@ def run_batch(args, local):
             "config": {"workload": "cohorts N=" + "/".join(str(c.codes.shape[0]) for c in cohorts) +
                                    " x M=" + "/".join(str(c.codes.shape[1]) for c in cohorts) +
                                    ", per-sample missingness U(0, 0.2)", "pairs": pairs},
-            "timing": "host wall clock around kg_relatedness_batch (uploads, preparation, waves, rows back)",
+            "timing": "host wall clock around kg_relatedness_batch (uploads, preparation, waves, rows back "
+                      "into page-locked buffers)",
             "waves_ms": float(np.mean(waves_ms)), "waves_pairs_per_s": pairs / (np.mean(waves_ms) * 1e-3),
             "autotune": {"shape": shape, "tune_s": t_tune, "default_pairs_per_s": pairs / t_default,
                          "default_waves_ms": w_default, "tuned_pairs_per_s": pairs / tw, "tuned_waves_ms": w_tuned,

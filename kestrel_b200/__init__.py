@@ -289,9 +289,12 @@ class Estimator:
         d["sites_used"] = list(s.sites_used)
         return d
 
-    def relatedness_batch(self, cohorts, iterations: int = 100, maf=None):
+    def relatedness_batch(self, cohorts, iterations: int = 100, maf=None, out=None):
         """cohorts: list of (codes[S, V] u8, allele_frequencies or None, num_samples or None).
-        Returns one row array per cohort, all from a single persistent launch."""
+        Returns one row array per cohort, all from a single persistent launch.
+        out: optional list of row arrays (OUTPUT_DTYPE, at least num_samples *
+        (num_samples + 1) / 2 rows each), filled and returned in place (page-locked
+        ones avoid first-touch page faults in the copy back)."""
         arr = (KgCohort * len(cohorts))()
         keep = []
         outs = []
@@ -300,16 +303,23 @@ class Estimator:
             codes = np.ascontiguousarray(codes, dtype=np.uint8)
             n, m = codes.shape
             ns = n if ns is None else int(ns)
-            out = np.empty(ns * (ns + 1) // 2, OUTPUT_DTYPE)
+            if out is not None:
+                o = out[i]
+                if o.dtype != OUTPUT_DTYPE or o.ndim != 1 or o.size < ns * (ns + 1) // 2:
+                    raise ValueError(f"out[{i}] must be a 1-D {OUTPUT_DTYPE} array of at least "
+                                     f"{ns * (ns + 1) // 2} rows")
+                out_i = o
+            else:
+                out_i = np.empty(ns * (ns + 1) // 2, OUTPUT_DTYPE)
             afa = None if af is None else np.ascontiguousarray(af, dtype=np.float64)
-            keep += [codes, afa, out]
+            keep += [codes, afa, out_i]
             arr[i].codes = codes.ctypes.data
             arr[i].n_samples, arr[i].n_sites, arr[i].row_stride = n, m, m
             arr[i].allele_frequencies = None if afa is None else afa.ctypes.data
             arr[i].num_samples = ns
-            arr[i].out = out.ctypes.data
-            arr[i].out_cap = out.size
-            outs.append(out)
+            arr[i].out = out_i.ctypes.data
+            arr[i].out_cap = out_i.size
+            outs.append(out_i)
         st = self._L.kg_relatedness_batch(self._h, arr, len(cohorts), iterations,
                                           float("nan") if maf is None else float(maf))
         _check(st, self._h)
