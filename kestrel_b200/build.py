@@ -22,7 +22,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CUDA_SOURCES = ["kg_engine.cu", "kg_wave.cu", "kg_api.cu", "kg_noalloc.cu", "kg_soft.cu", "kg_multi.cu"]
 HOST_SOURCES = ["kg_cli.cpp", "kg_vcf.cpp"]
 HEADERS = ["kg_engine.h", "kg_pair.cuh", "kg_solver.cuh", "kg_rowsolve.cuh", "kg_wave.cuh", "kg_bulk.cuh",
-           "kg_vcf.h", "kg_threads.h", "kg_allele.cuh", "kg_alleleN.cuh"]
+           "kg_vcf.h", "kg_threads.h", "kg_allele.cuh", "kg_alleleN.cuh", "kg_qp1.cuh"]
 
 
 def nvcc() -> str:
