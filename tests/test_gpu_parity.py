@@ -108,6 +108,12 @@ def test_batch_matches_single_runs(est, oracle):
         np.testing.assert_array_equal(out["obj"], single["obj"])
     for c, out in zip(cohorts, outs):          # every cohort of the batch, every pair
         compare(out, oracle.relatedness(c.codes))
+    # the same call into caller-owned row buffers, filled in place
+    bufs = [np.zeros(len(o) + 3, kb.OUTPUT_DTYPE) for o in outs]
+    again = est.relatedness_batch([(c.codes,) for c in cohorts], out=bufs)
+    for o, a, b in zip(outs, again, bufs):
+        assert a is b
+        np.testing.assert_array_equal(b[:len(o)].view(np.uint8), o.view(np.uint8))
 
 
 def test_python_api_build_arrays(oracle, cfg0):
