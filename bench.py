@@ -252,7 +252,8 @@ def run_reference(args, codes, planted):
 def run_batch(args, local):
     """Eight cohorts of uneven N, M and missingness in one launch: timed with
     the default launch shape, then with the one kg_autotune picks on a sample
-    of the largest cohort (both reported; the line's value is the tuned one)."""
+    of the largest cohort (both reported; the line's value is the default
+    shape's, the tuned run's beside it)."""
     import kestrel_b200 as kb
     from kestrel_b200 import synth
     cohorts = synth.config2()
@@ -285,9 +286,9 @@ def run_batch(args, local):
     shape = est.launch()
     tw, w_tuned, st = timed()
     est.close()
-    waves_ms = [w_tuned]
-    return {"metric": "all-pairs/s, 8 uneven cohorts in one launch", "value": pairs / tw, "unit": "pairs/s",
-            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": tw * 1e3,
+    waves_ms = [w_default]
+    return {"metric": "all-pairs/s, 8 uneven cohorts in one launch", "value": pairs / t_default, "unit": "pairs/s",
+            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_default * 1e3,
             "higher_is_better": True, "dtype": "f32" if args.precision == "fp32c" else "f64",
             "data": "synthetic",
             "config": {"workload": "cohorts N=" + "/".join(str(c.codes.shape[0]) for c in cohorts) +
