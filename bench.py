@@ -287,7 +287,8 @@ def run_batch(args, local):
     tw, w_tuned, st = timed()
     est.close()
     waves_ms = [w_default]
-    return {"metric": "all-pairs/s, 8 uneven cohorts in one launch", "value": pairs / t_default, "unit": "pairs/s",
+    return {"metric": "all-pairs/s, 8 uneven cohorts in one launch", "value": pairs / t_default,
+            "unit": "pairs/s",
             "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_default * 1e3,
             "higher_is_better": True, "dtype": "f32" if args.precision == "fp32c" else "f64",
             "data": "synthetic",
