@@ -725,34 +725,40 @@ struct Shape32x2 {
         }
     }
 
-    // Shape32::diff_term on a pair of sites
-    __device__ __forceinline__ float2 diff_term(float2 t, float2 r, float2 c) const {
+    // z = delta / d_new of Shape32::diff_term on a pair of sites
+    __device__ __forceinline__ float2 diff_z(float2 t, float2 r, float2 c) const {
         float2 dl;
         if (S == 0) dl = mul2(t, fma2(fma2(fma2(s3, t, s2), t, s1), t, s0));
         else if (S == 1 || S == 2) dl = mul2(c, fma2(fma2(s2, t, s1), t, s0));
         else if (S == 3) dl = mul2(c, fma2(c, s3, fma2(t, s2, fma2(add2(dup2(1.0f), neg2(t)), s1, s0))));
         else dl = mul2(c, fma2(c, s1, s0));
-        const float2 z = mul2(dl, r);
-        return make_float2(neg_log1m(z.x), neg_log1m(z.y));
+        return mul2(dl, r);
     }
 
-    // four sites (one float4) as two pairs; o collects the objective terms
-    // (direct mode: one lg2 of the product of the four d, in o.y for odd
-    // float4 and o.x for even ones, so each half takes every other one)
+    // four sites (one float4) as two pairs; o collects the objective terms,
+    // one per four sites, in o.y for odd float4 and o.x for even ones, so each
+    // half takes every other one.  Direct mode: one lg2 of the product of the
+    // four d.  Difference mode: the four terms -log(1 - z_i) as one,
+    // -log(1 - w) with 1 - w = prod (1 - z_i), where the w of two sites is
+    // z0 + z1 - z0 z1 (no cancellation for small z: w carries the rounding of
+    // the z themselves, as the four separate terms would).
     template <bool DIFF>
     __device__ __forceinline__ void site4(float4 v, float2* g, float2& o, float2* h, bool odd) const {
         const float2 ta = make_float2(v.x, v.y), tb = make_float2(v.z, v.w);
         float2 da, db, ra, rb, ca, cb;
         core(ta, g, h, da, ra, ca);
         core(tb, g, h, db, rb, cb);
+        float l;
         if (!DIFF) {
             const float2 p = mul2(da, db);
-            const float l = lg2_approx(p.x * p.y);
-            if (odd) o.y += l;
-            else o.x += l;
+            l = lg2_approx(p.x * p.y);
         } else {
-            o = add2(o, add2(diff_term(ta, ra, ca), diff_term(tb, rb, cb)));
+            const float2 za = diff_z(ta, ra, ca), zb = diff_z(tb, rb, cb);
+            const float2 w2 = fma2(neg2(za), zb, add2(za, zb));
+            l = neg_log1m(fmaf(-w2.x, w2.y, w2.x + w2.y));
         }
+        if (odd) o.y += l;
+        else o.x += l;
     }
 };
 
@@ -1157,7 +1163,7 @@ __host__ __device__ constexpr int flops4_fp32_hi(int s) {
     return s == 0 ? 141 : s == 1 ? 113 : s == 2 ? 113 : s == 3 ? 165 : 77;
 }
 __host__ __device__ constexpr int flops4_diff_extra(int s) {
-    return s == 0 ? 75 : s == 1 ? 67 : s == 2 ? 67 : s == 3 ? 79 : 59;
+    return s == 0 ? 48 : s == 1 ? 40 : s == 2 ? 40 : s == 3 ? 52 : 32;
 }
 __host__ __device__ constexpr int flops_fp32_lo(int s) {
     return s == 0 ? 43 : s == 1 ? 34 : s == 2 ? 34 : s == 3 ? 49 : 23;

@@ -338,12 +338,6 @@ __device__ __forceinline__ void ring_prologue(const Ring& R, const float* L, int
     }
 }
 
-// One 16-byte read of a ring stage (a shared-memory address).
-__device__ __forceinline__ float4 lds4(uint32_t a) {
-    float4 v;
-    asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];" : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w) : "r"(a));
-    return v;
-}
 
 // One shape's FP32 list from the ring.  Stage i holds float4 128 i .. 128 i +
 // 127; lane l takes 128 i + 32 j + l (j = 0..3): 16 sites, in packed pairs
@@ -356,7 +350,11 @@ __device__ __forceinline__ float4 lds4(uint32_t a) {
 // list buffer.  The FP64 Hessian sums live in the warp's shared memory (Hs,
 // moment j of lane l at Hs[32 j + l]), which leaves registers for a fifth
 // block per SM.  The sums use the hi coefficients only (lo_correction
-// restores the rest).  Returns false if a wait ran out.
+// restores the rest).  A stage is read with plain shared-memory loads: the
+// barrier wait (a memory clobber) keeps them after the copy has landed and
+// the warp sync keeps them before the stage's next copy, and between the two
+// the compiler schedules them among the site arithmetic.  Returns false if a
+// wait ran out.
 constexpr int HESS_STAGES = 8;
 template <int S, bool DIFF>
 __device__ __forceinline__ bool stream32_ring(const float* __restrict__ L, int64_t len, const Coef32* K, int lane,
@@ -375,7 +373,6 @@ __device__ __forceinline__ bool stream32_ring(const float* __restrict__ L, int64
     const int64_t n4 = len >> 2;
     const int nst = (int)((len + STAGE_ELEMS - 1) / STAGE_ELEMS);
     const int nfull = (int)(n4 / STAGE_F4);   // stages with all 128 float4 inside the list
-    const uint32_t base = smem_u32(R.buf) + 16u * (uint32_t)lane;
     const uint32_t seq0 = R.seq;   // ring_prologue has issued the first stages
     bool ok = true;
     int done = 0;
@@ -384,18 +381,18 @@ __device__ __forceinline__ bool stream32_ring(const float* __restrict__ L, int64
         const uint32_t slot = q % RING_STAGES;
         if (!mbar_wait(&R.bar[slot], (q / RING_STAGES) & 1u)) { ok = false; break; }
         done = i + 1;
-        const uint32_t b = base + slot * (STAGE_F4 * 16);
+        const float4* B4 = R.buf + slot * STAGE_F4 + lane;
         float2 g[NG], o = dup2(0.f);
 #pragma unroll
         for (int j = 0; j < NG; j++) g[j] = dup2(0.f);
         if (i < nfull) {
 #pragma unroll
-            for (int j = 0; j < 4; j++) ev.template site4<DIFF>(lds4(b + 512 * j), g, o, h, j & 1);
+            for (int j = 0; j < 4; j++) ev.template site4<DIFF>(B4[32 * j], g, o, h, j & 1);
         } else {
             const int rem = (int)(n4 - (int64_t)i * STAGE_F4);   // float4 in this stage, 0..127
 #pragma unroll
             for (int j = 0; j < 4; j++)
-                if (lane + 32 * j < rem) ev.template site4<DIFF>(lds4(b + 512 * j), g, o, h, j & 1);
+                if (lane + 32 * j < rem) ev.template site4<DIFF>(B4[32 * j], g, o, h, j & 1);
         }
 #pragma unroll
         for (int j = 0; j < NG; j++) { G[j] += (double)g[j].x; G[j] += (double)g[j].y; }
@@ -503,7 +500,6 @@ __device__ __forceinline__ bool cls_stream32_ring(const float* __restrict__ L, i
     const int64_t n4 = len >> 2;
     const int nst = (int)((len + STAGE_ELEMS - 1) / STAGE_ELEMS);
     const int nfull = (int)(n4 / STAGE_F4);
-    const uint32_t base = smem_u32(R.buf) + 16u * (uint32_t)lane;
     const uint32_t seq0 = R.seq;
     bool ok = true;
     int done = 0;
@@ -512,7 +508,7 @@ __device__ __forceinline__ bool cls_stream32_ring(const float* __restrict__ L, i
         const uint32_t slot = q % RING_STAGES;
         if (!mbar_wait(&R.bar[slot], (q / RING_STAGES) & 1u)) { ok = false; break; }
         done = i + 1;
-        const uint32_t b = base + slot * (STAGE_F4 * 16);
+        const float4* B4 = R.buf + slot * STAGE_F4 + lane;
         float2 g[NG];
 #pragma unroll
         for (int j = 0; j < NG; j++) g[j] = dup2(0.f);
@@ -520,7 +516,7 @@ __device__ __forceinline__ bool cls_stream32_ring(const float* __restrict__ L, i
 #pragma unroll
         for (int j = 0; j < 4; j++)
             if (lane + 32 * j < rem) {
-                const float4 v = lds4(b + 512 * j);
+                const float4 v = B4[32 * j];
                 cls_pair<S>(make_float2(v.x, v.y), g);
                 cls_pair<S>(make_float2(v.z, v.w), g);
             }
