@@ -44,9 +44,9 @@ __device__ inline void scatter_lockstep(const CohortDev& co, int64_t x, int64_t 
     const uint2* px = co.planes_x + x * co.plane_stride;
     const uint2* py = co.planes_y + y * co.plane_stride;
     float* obuf = reinterpret_cast<float*>(wsm);   // FP32 only
-    int64_t off[5];
+    int off[5];
 #pragma unroll
-    for (int k = 0; k < 5; k++) off[k] = off0[k];
+    for (int k = 0; k < 5; k++) off[k] = (int)off0[k];
     for (int u = u0; u < u1; u++) {
         const uint2 X = px[u * UNIT_WORDS + lane], Y = py[u * UNIT_WORDS + lane];
         // the unit's REF frequencies, unit-transposed: site 32 lane + i at
@@ -87,7 +87,11 @@ __device__ inline void scatter_lockstep(const CohortDev& co, int64_t x, int64_t 
             // bit.  Field 5 stays at 1023, which no list value of the unit
             // uses unless all 1,024 sites are observed, when field 5 is never
             // taken.  (Positions kept as 13-bit fields of one 64-bit register
-            // cost 2% more admit time in 64-bit shifts.)
+            // cost 2% more admit time in 64-bit shifts.)  The 32 steps are
+            // unrolled, so every shift count is a constant, and the list
+            // offsets are 32-bit (a slot's lists hold far fewer than 2^31
+            // entries), which keeps the loop's registers within the four
+            // blocks per SM that the kernel needs (three ran 25% slower).
             const unsigned obs = sm.m[0] | sm.m[1] | sm.m[2] | sm.m[3] | sm.m[4];
             const unsigned f0 = sm.m[1] | sm.m[3] | ~obs, f1 = sm.m[2] | sm.m[3], f2 = sm.m[4] | ~obs;
             const unsigned long long pre = ust + (inc - v);
@@ -96,7 +100,7 @@ __device__ inline void scatter_lockstep(const CohortDev& co, int64_t x, int64_t 
             for (int k = 0; k < 5; k++) cnt[32 * k] = (int)((pre >> (11 * k)) & 0x7FFull);
             cnt[32 * 5] = 1023;
             const float* st = reinterpret_cast<const float*>(freq);
-#pragma unroll 8
+#pragma unroll
             for (int i = 0; i < 32; i++) {
                 const unsigned f = ((f0 >> i) & 1u) | (((f1 >> i) & 1u) << 1) | (((f2 >> i) & 1u) << 2);
                 int* c = cnt + 32 * f;
@@ -122,7 +126,7 @@ __device__ inline void scatter_lockstep(const CohortDev& co, int64_t x, int64_t 
                     obuf[pos] = (float)t;
                 } else {
                     const int k = code - 1;
-                    const int64_t o = k == 0 ? off[0] : k == 1 ? off[1] : k == 2 ? off[2] : k == 3 ? off[3] : off[4];
+                    const int o = k == 0 ? off[0] : k == 1 ? off[1] : k == 2 ? off[2] : k == 3 ? off[3] : off[4];
                     lists[o + pos] = t;
                 }
             }
@@ -141,7 +145,7 @@ __device__ inline void scatter_lockstep(const CohortDev& co, int64_t x, int64_t 
             __syncwarp();
         }
 #pragma unroll
-        for (int k = 0; k < 5; k++) off[k] += (int64_t)((tot >> (11 * k)) & 0x7FFull);
+        for (int k = 0; k < 5; k++) off[k] += (int)((tot >> (11 * k)) & 0x7FFull);
     }
 }
 
