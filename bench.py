@@ -302,7 +302,7 @@ def run_batch(args, local):
             "waves_ms": float(np.mean(waves_ms)), "waves_pairs_per_s": pairs / (np.mean(waves_ms) * 1e-3),
             "autotune": {"shape": shape, "tune_s": t_tune, "default_pairs_per_s": pairs / t_default,
                          "default_waves_ms": w_default, "tuned_pairs_per_s": pairs / tw, "tuned_waves_ms": w_tuned,
-                         "note": "0 = the default (occupancy limit, 16384-entry units, an eighth of the pairs in "
+                         "note": "0 = the default (occupancy limit, 16384-entry units, a fifth of the pairs in "
                                  "flight); tuned on about 131,072 pairs of the 2048 x 100000 cohort"},
             "stats": {k: st[k] for k in ("gh_passes", "fp64_pairs", "waves", "slots", "nonconverged")}}
 
@@ -316,6 +316,7 @@ def run_inbred(args, local):
     n = co.codes.shape[0]
     pairs = n * (n - 1) // 2
     est = kb.Estimator(device=local, precision=args.precision)
+    est.set_launch(args.slots, args.pass_bps)
     est.load(co.codes)
     for _ in range(max(1, args.warmup)):
         est.relatedness()
@@ -543,22 +544,21 @@ def run_gt_cls(args, local):
     codes_pin = torch.from_numpy(codes).pin_memory().numpy()
     out_pin = torch.empty(n_s * (n_s + 1) // 2 * kb.OUTPUT_DTYPE.itemsize, dtype=torch.uint8,
                           pin_memory=True).numpy().view(kb.OUTPUT_DTYPE)
-    e2 = kb.Estimator(device=local, precision=args.precision)
-    e2.load(codes_pin)
+    # (on the same context: a second one would find half the memory taken)
+    est.load(codes_pin)
     if mg is not None:
-        e2.load_multiallelic(mg, mal)
-    e2.relatedness_gt(out=out_pin)
+        est.load_multiallelic(mg, mal)
+    est.relatedness_gt(out=out_pin)
     e2e_ms = []
     for _ in range(max(1, args.steps)):
         flush.zero_()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        e2.load(codes_pin)
+        est.load(codes_pin)
         if mg is not None:
-            e2.load_multiallelic(mg, mal)
-        e2.relatedness_gt(out=out_pin)
+            est.load_multiallelic(mg, mal)
+        est.relatedness_gt(out=out_pin)
         e2e_ms.append((time.perf_counter() - t0) * 1e3)
-    e2.close()
     te = float(np.mean(e2e_ms))
     # the list-building (admit) kernel dominates: HBM-bound, 4 bytes written per
     # listed pair-site; the moment pass reads them once
@@ -664,7 +664,9 @@ def main():
     # ---- end to end through the C ABI from pinned host buffers: every step
     # uploads the genotypes in the VCF reader's packed form (2-bit codes plus
     # the observed mask, kg_load_genotypes_2bit), estimates and copies all rows
-    # back (kg_relatedness); the context is made once, as a caller would
+    # back (kg_relatedness); the context is made once, as a caller would (the
+    # same one: a second context would find half the memory taken by the
+    # first one's slots and run with fewer)
     e2e = None
     if not args.no_e2e:
         c2, ob = kb.pack_2bit(codes)
@@ -672,19 +674,16 @@ def main():
         ob_pin = torch.from_numpy(ob.view(np.int32)).pin_memory().numpy().view(np.uint32)
         out_pin = torch.empty(n * (n + 1) // 2 * kb.OUTPUT_DTYPE.itemsize, dtype=torch.uint8,
                               pin_memory=True).numpy().view(kb.OUTPUT_DTYPE)
-        e2 = kb.Estimator(device=local, precision=args.precision)
-        e2.set_launch(args.slots, args.pass_bps)
-        e2.load_packed(c2_pin, ob_pin, m)
-        e2.relatedness(out=out_pin)          # warm: workspace sized once
+        est.load_packed(c2_pin, ob_pin, m)
+        est.relatedness(out=out_pin)         # warm
         e2e_ms = []
         for i in range(max(1, args.steps)):
             flush.zero_()
             barrier()
             t0 = time.perf_counter()
-            e2.load_packed(c2_pin, ob_pin, m)
-            e2.relatedness(out=out_pin)
+            est.load_packed(c2_pin, ob_pin, m)
+            est.relatedness(out=out_pin)
             e2e_ms.append((time.perf_counter() - t0) * 1e3)
-        e2.close()
         tm = max_over_ranks(float(np.mean(e2e_ms)), pg, f"cuda:{local}")
         e2e = {"value": whole_job_rate(pairs, world, tm), "unit": "pairs/s",
                "h2d_bytes_per_step": int(c2.nbytes + ob.nbytes), "d2h_bytes_per_step": int(out_pin.nbytes),

@@ -81,8 +81,8 @@ const char *kg_version(void);
 /* Arithmetic of the per-site sums (kg_precision). */
 int kg_set_precision(kg_ctx *ctx, int precision);
 
-/* Launch shape of the pair engine: pairs in flight per wave (slots; 0 = an
- * eighth of the pairs, from 4096 to 65536, as memory allows) and blocks per SM
+/* Launch shape of the pair engine: pairs in flight per wave (slots; 0 = a
+ * fifth of the pairs, from 4096 to 131072, as memory allows) and blocks per SM
  * of the site-pass kernel (0 = the occupancy limit).  Exposed for the
  * autotuner and tests; results do not depend on it. */
 int kg_set_launch(kg_ctx *ctx, int slots, int blocks_per_sm);
@@ -105,7 +105,7 @@ int kg_set_work_unit(kg_ctx *ctx, int entries);
 
 /* The context's launch shape: pairs in flight (0 = automatic), site-pass blocks
  * per SM (0 = occupancy limit), work unit (0 = default) and the divisor of the
- * automatic pairs in flight (the job's pairs / divisor, within 4096..65536).
+ * automatic pairs in flight (the job's pairs / divisor, within 4096..131072).
  * Any pointer may be NULL. */
 int kg_get_launch(const kg_ctx *ctx, int *slots, int *blocks_per_sm, int *unit_entries, int *slot_divisor);
 
@@ -113,9 +113,9 @@ int kg_get_launch(const kg_ctx *ctx, int *slots, int *blocks_per_sm, int *unit_e
  * its first samples) and keeps the fastest launch shape, by coordinate descent,
  * a change kept only when it is more than 2% faster: site-pass blocks per SM
  * (occupancy limit, 4, 3) and the work unit (16384, 8192, 4096 entries), judged
- * by the site passes' device time; then, for a cohort of fewer than 524,288
- * pairs, the automatic pairs in flight (an eighth, a quarter or a sixteenth of
- * a job's pairs), judged by the sample's whole device time.  Writes *slots (0:
+ * by the site passes' device time; then, for a cohort of fewer than 655,360
+ * pairs, the automatic pairs in flight (a fifth, a third or an eighth of a
+ * job's pairs), judged by the sample's whole device time.  Writes *slots (0:
  * automatic) and *blocks_per_sm if non-NULL; kg_get_launch reports the rest. */
 int kg_autotune(kg_ctx *ctx, int *slots, int *blocks_per_sm);
 

@@ -47,7 +47,7 @@ struct kg_ctx {
     int64_t wave_slots = 0;
     int pass_bps = 0;
     int unit_elems = 0;
-    int slot_divisor = 8;
+    int slot_divisor = 5;
     uint64_t wave_limit = 0;
     cudaStream_t stream = nullptr;
     // single cohort
@@ -877,7 +877,7 @@ int kg_last_run_stats(kg_ctx* c, kg_run_stats* s) {
 //   * the work unit (site chunk) of the pass kernel: 16,384, 8,192, 4,096
 //     list entries;
 //   * pairs in flight (the pair tile of a wave) as a share of the job's pairs:
-//     an eighth (the default), a quarter, a sixteenth, within 4,096..32,768.
+//     a fifth (the default), a third, an eighth, within 4,096..131,072.
 // A candidate is kept only when it beats the current choice by more than 2%,
 // so run-to-run noise leaves the defaults.  Slots and blocks per SM leave the
 // rows bit for bit the same; the work unit changes how a pass's FP64 partial
@@ -906,11 +906,11 @@ int kg_autotune(kg_ctx* c, int* slots_out, int* bps_out) {
         jb.panel = &c->cohort;
         jb.n_x = ns;
         jb.d_out = c->dout.as<kg_output>();
-        int bps = 0, unit = 0, div = 8;
+        int bps = 0, unit = 0, div = 5;
         // The site-pass shape (blocks per SM, work unit) is judged by the pass
         // phase's device time: every shape runs the same passes, and the wave
         // tail of a sample does not mislead it.  The share of pairs in flight
-        // only matters for jobs below 8 x 65,536 pairs; it is judged by the
+        // only matters for jobs below 5 x 131,072 pairs; it is judged by the
         // sample's whole device time, and only for such a cohort.
         auto cost = [&](int b, int u, int d, bool whole, double& ms) -> int {
             kg::RunConfig cfg = run_config(c, 100);
@@ -945,9 +945,9 @@ int kg_autotune(kg_ctx* c, int* slots_out, int* bps_out) {
             if ((st = consider(b, unit, div, false))) return set_err(c, st, err);
         for (int u : {8192, 4096})
             if ((st = consider(bps, u, div, false))) return set_err(c, st, err);
-        if (full_pairs / 8 < 65536) {
+        if (full_pairs / 5 < 131072) {
             if ((st = cost(bps, unit, div, true, best))) return set_err(c, st, err);
-            for (int d : {4, 16})
+            for (int d : {3, 8})
                 if ((st = consider(bps, unit, d, true))) return set_err(c, st, err);
         }
         c->wave_slots = 0;

@@ -1493,10 +1493,10 @@ int WaveEngine::open(Workspace& ws, cudaStream_t st, const RunConfig& cfg, int64
     const size_t per_slot = sizeof(double) * (size_t)list_cap + sizeof(double) * E.max_units * UNIT_VALS +
                             sizeof(SlotState) + 4 * sizeof(int) + 2 * 5 * shape_units * sizeof(int4);
     size_t fr = 0, tot = 0;
-    // by default an eighth of the job's pairs, between 4,096 and 65,536: enough
+    // by default a fifth of the job's pairs, between 4,096 and 131,072: enough
     // to fill the waves, few enough that the last waves drain quickly
     const int64_t want = cfg.slots > 0 ? cfg.slots
-                                       : std::min<int64_t>(65536, std::max<int64_t>(
+                                       : std::min<int64_t>(131072, std::max<int64_t>(
                                                                       4096, expected_pairs / std::max(1, cfg.slot_divisor)));
     if (!same_call) {
         KG_WAVE_TRY(cudaMemGetInfo(&fr, &tot));
