@@ -638,7 +638,7 @@ extern "C" __global__ void __launch_bounds__(128, PASS_MIN_BLOCKS) wave_pass_ker
     int pre[6];
     pre[0] = 0;
 #pragma unroll
-    for (int k = 0; k < 5; k++) pre[k + 1] = pre[k] + A.wc_cur->units[k];
+    for (int k = 0; k < 5; k++) pre[k + 1] = pre[k] + A.wc_cur->units[k] + A.wc_cur->back[k];
     const int64_t ntask = pre[5];
     // the next task is claimed as the current one starts, so the claim's
     // latency hides behind the current task's sites
@@ -650,7 +650,8 @@ extern "C" __global__ void __launch_bounds__(128, PASS_MIN_BLOCKS) wave_pass_ker
         int sh = 0;
 #pragma unroll
         for (int k = 1; k < 5; k++) sh += ((int)t >= pre[k]) ? 1 : 0;
-        const int4 tk = A.tasks_cur[sh * A.task_cap + ((int)t - pre[sh])];
+        const int jt = (int)t - pre[sh], nfront = A.wc_cur->units[sh];
+        const int4 tk = A.tasks_cur[sh * A.task_cap + (jt < nfront ? (int64_t)jt : A.task_cap - 1 - (jt - nfront))];
         unsigned long long t_next = 0;
         if (lane == 0) t_next = atomicAdd(A.pass_task, 1ull);
         const int s = tk.x;

@@ -58,9 +58,10 @@ struct WaveCounts {
     int n_pass;      // slots with a pending pass
     int n_free;      // slots for the admit step: free ones and those waiting for FP64 lists
     int n_resort;    // of those, slots waiting for FP64 lists
-    int units[5];    // pass work units per shape
+    int units[5];    // pass work units per shape, other than difference-objective ones (from each list's start)
     int n_qp;        // slots whose SQP step needs a QP (wave_qp_kernel) this wave
     int pad;
+    int back[5];     // of the pass work units, difference-objective ones (from each list's end)
 };
 
 // The job table's extent, in device memory so that jobs can be appended
@@ -214,7 +215,10 @@ __device__ __forceinline__ int4 make_task(int s, int u, int64_t off, int64_t len
 
 // Queues slot s for a pass in the wave whose lists are (pass, tasks, wc): its
 // work units go to the shape-major task lists, so that the warps of the pass
-// kernel run one shape's code at a time.  Called after S.ustart is set by W
+// kernel run one shape's code at a time; within a shape's list, units of
+// difference-objective passes fill it from the end and the others from the
+// start, so the warps also run one pass kind's code at a time (mixing the two
+// kinds took 2.5% more pass time).  Called after S.ustart is set by W
 // lanes (a warp or a half-warp, given by mask); lane is the index among them.
 template <int W>
 __device__ inline void enqueue_pass(int* pass, int4* tasks, int64_t task_cap, WaveCounts* wc, int s,
@@ -223,14 +227,16 @@ __device__ inline void enqueue_pass(int* pass, int4* tasks, int64_t task_cap, Wa
     for (int sh = 0; sh < 5; sh++) {
         const int u0 = S.ustart[sh], nu = S.ustart[sh + 1] - u0;
         if (nu == 0) continue;
+        const int kind = S.kind;
+        const bool from_end = (kind == PASS_FP32_DIFF);
         int base = 0;
-        if (lane == 0) base = atomicAdd(&wc->units[sh], nu);
+        if (lane == 0) base = atomicAdd(from_end ? &wc->back[sh] : &wc->units[sh], nu);
         base = __shfl_sync(mask, base, 0, W);
         const int64_t st = S.start[sh], cnt = S.cnt[sh];
-        const int kind = S.kind;
         for (int i = lane; i < nu; i += W) {
             const int64_t c0 = (int64_t)i * unit;
-            tasks[sh * task_cap + base + i] = make_task(s, u0 + i, st + c0, min((int64_t)unit, cnt - c0), kind);
+            const int64_t at = from_end ? task_cap - 1 - (base + i) : base + i;
+            tasks[sh * task_cap + at] = make_task(s, u0 + i, st + c0, min((int64_t)unit, cnt - c0), kind);
         }
     }
     if (lane == 0) pass[atomicAdd(&wc->n_pass, 1)] = s;
