@@ -1298,8 +1298,10 @@ extern "C" __global__ void __launch_bounds__(128, 4) wave_solve_kernel(WaveArgs 
 
 // The QP of every slot in this wave's QP list, a thread per slot (kg_qp1.cuh,
 // the same arithmetic as the row-parallel form); the solution replaces c's
-// neighbour in the slot's QP buffer.
-extern "C" __global__ void __launch_bounds__(128) wave_qp_kernel(WaveArgs A) {
+// neighbour in the slot's QP buffer.  Three blocks per SM (168 registers, a
+// few spilled) beat two without spills: the kernel is bound by its FP64
+// dependency chains, so warps count more than registers.
+extern "C" __global__ void __launch_bounds__(128, 3) wave_qp_kernel(WaveArgs A) {
     if (A.clk->stop) return;   // a device loop past its last wave
     const PhaseEnd pe{&A.clk->end[2], (threadIdx.x & 31) == 0};   // timed as part of the solve phase
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
