@@ -1472,6 +1472,11 @@ WaveEngine::~WaveEngine() { delete d_; }
 int WaveEngine::open(Workspace& ws, cudaStream_t st, const RunConfig& cfg, int64_t list_cap,
                      int64_t expected_pairs, int max_jobs, std::string& err) {
     Impl& E = *d_;
+    // list offsets travel as 32-bit values (tasks and the admit scatter)
+    if (list_cap >= ((int64_t)1 << 31)) {
+        err = "a pair's site lists would exceed 2^31 entries";
+        return KG_EINVAL;
+    }
     E.ws = &ws;
     E.st = st;
     E.cfg = cfg;
