@@ -772,8 +772,8 @@ def measure_fp64_form(est, fp32c_value, steps=2):
 
 # DRAM bytes (read + write) per pair-site-pass of wave_pass_kernel: the ncu
 # capture of one launch on a 96-sample x 100,000-site cohort read and wrote
-# 1.913 GB over 447,339,158 pair-site-passes.
-PASS_DRAM_BYTES_PER_SITE = 4.28
+# 1.912 GB over 447,339,158 pair-site-passes.
+PASS_DRAM_BYTES_PER_SITE = 4.27
 
 
 def ctypes_peak(device):
