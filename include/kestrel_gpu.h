@@ -112,10 +112,11 @@ int kg_get_launch(const kg_ctx *ctx, int *slots, int *blocks_per_sm, int *unit_e
 /* Runs the autotuner on a sample of the loaded cohort (about 131,072 pairs of
  * its first samples) and keeps the fastest launch shape, by coordinate descent,
  * a change kept only when it is more than 2% faster: site-pass blocks per SM
- * (occupancy limit, 4, 3) and the work unit (16384, 8192, 4096 entries), judged
- * by the site passes' device time; then, for a cohort of fewer than 655,360
- * pairs, the automatic pairs in flight (a fifth, a third or an eighth of a
- * job's pairs), judged by the sample's whole device time.  Writes *slots (0:
+ * (occupancy limit, 4, 3) and the work unit (16384, 32768, 8192, 4096
+ * entries), judged by the site passes' device time; then, for a cohort of
+ * fewer than 655,360 pairs, the automatic pairs in flight (a fifth, a third
+ * or an eighth of a job's pairs), judged by the sample's whole device time.
+ * Writes *slots (0:
  * automatic) and *blocks_per_sm if non-NULL; kg_get_launch reports the rest. */
 int kg_autotune(kg_ctx *ctx, int *slots, int *blocks_per_sm);
 
