@@ -302,7 +302,7 @@ def run_batch(args, local):
             "waves_ms": float(np.mean(waves_ms)), "waves_pairs_per_s": pairs / (np.mean(waves_ms) * 1e-3),
             "autotune": {"shape": shape, "tune_s": t_tune, "default_pairs_per_s": pairs / t_default,
                          "default_waves_ms": w_default, "tuned_pairs_per_s": pairs / tw, "tuned_waves_ms": w_tuned,
-                         "note": "0 = the default (occupancy limit, 16384-entry units, a fifth of the pairs in "
+                         "note": "0 = the default (occupancy limit, 32768-entry units, a fifth of the pairs in "
                                  "flight); tuned on about 131,072 pairs of the 2048 x 100000 cohort"},
             "stats": {k: st[k] for k in ("gh_passes", "fp64_pairs", "waves", "slots", "nonconverged")}}
 

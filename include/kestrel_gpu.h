@@ -97,7 +97,7 @@ int kg_set_wave_limit(kg_ctx *ctx, uint64_t waves);
 
 /* Pass work unit (the site chunk one warp of the site-pass kernel streams at a
  * time): list entries per unit, a multiple of 512 from 1024 to 65536, or 0 for
- * the default (16384).  It sets how a pass's FP64 partial sums are grouped, so
+ * the default (32768).  It sets how a pass's FP64 partial sums are grouped, so
  * rows can change in their last bits (well inside the parity tolerances).  No
  * counterpart in the reference (its passes stream a pair's rows in 32-row blocks,
  * src/jacquard/grad_hess.rs:10). */
@@ -112,7 +112,7 @@ int kg_get_launch(const kg_ctx *ctx, int *slots, int *blocks_per_sm, int *unit_e
 /* Runs the autotuner on a sample of the loaded cohort (about 131,072 pairs of
  * its first samples) and keeps the fastest launch shape, by coordinate descent,
  * a change kept only when it is more than 2% faster: site-pass blocks per SM
- * (occupancy limit, 4, 3) and the work unit (16384, 32768, 8192, 4096
+ * (occupancy limit, 4, 3) and the work unit (32768, 65536, 16384, 8192
  * entries), judged by the site passes' device time; then, for a cohort of
  * fewer than 655,360 pairs, the automatic pairs in flight (a fifth, a third
  * or an eighth of a job's pairs), judged by the sample's whole device time.

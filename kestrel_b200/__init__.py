@@ -148,7 +148,7 @@ class Estimator:
         _check(self._L.kg_set_wave_limit(self._h, int(waves)), self._h)
 
     def set_work_unit(self, entries: int = 0):
-        """List entries per site-pass work unit (0 = the default, 16384)."""
+        """List entries per site-pass work unit (0 = the default, 32768)."""
         _check(self._L.kg_set_work_unit(self._h, int(entries)), self._h)
 
     def launch(self) -> dict:

@@ -874,7 +874,7 @@ int kg_last_run_stats(kg_ctx* c, kg_run_stats* s) {
 // each candidate run twice and timed the second time (the first instantiates
 // its graphs):
 //   * site-pass blocks per SM: the occupancy limit (5), 4, 3;
-//   * the work unit (site chunk) of the pass kernel: 16,384, 32,768, 8,192, 4,096
+//   * the work unit (site chunk) of the pass kernel: 32,768, 65,536, 16,384, 8,192
 //     list entries;
 //   * pairs in flight (the pair tile of a wave) as a share of the job's pairs:
 //     a fifth (the default), a third, an eighth, within 4,096..131,072.
@@ -943,7 +943,7 @@ int kg_autotune(kg_ctx* c, int* slots_out, int* bps_out) {
         };
         for (int b : {4, 3})
             if ((st = consider(b, unit, div, false))) return set_err(c, st, err);
-        for (int u : {32768, 8192, 4096})
+        for (int u : {65536, 16384, 8192})
             if ((st = consider(bps, u, div, false))) return set_err(c, st, err);
         if (full_pairs / 5 < 131072) {
             if ((st = cost(bps, unit, div, true, best))) return set_err(c, st, err);

@@ -195,7 +195,7 @@ struct RunConfig {
     uint64_t max_waves = 0;       // waves a call may run before it gives up (0 = a bound from the work)
     int ml_units = 0;             // work units per slot of the ML path's tri-/tetra-allelic sites (run_pairs sets it)
     int ml_chunk = 0;             // their kept sites per unit (run_pairs sets it)
-    int unit_elems = 0;           // list entries per site-pass work unit (0 = UNIT_ELEMS, 16384)
+    int unit_elems = 0;           // list entries per site-pass work unit (0 = UNIT_ELEMS, 32768)
     int slot_divisor = 5;         // automatic slots: the job's pairs / slot_divisor within 4096..131072
     // Called between waves, on the calling thread, once per job whose pairs
     // have all finished (their rows are final in device memory).

@@ -19,7 +19,7 @@
 
 namespace kg {
 
-constexpr int UNIT_ELEMS = 16384;  // list entries per pass work unit (the default; RunConfig::unit_elems)
+constexpr int UNIT_ELEMS = 32768;  // list entries per pass work unit (the default; RunConfig::unit_elems)
 constexpr int UNIT_VALS = 14;      // partial values per unit: <= 13 moments + objective
 
 enum : int { SLOT_FREE = 0, SLOT_PASS = 1, SLOT_RESORT = 2 };

@@ -207,7 +207,7 @@ def test_autotune_and_launch_shape_leave_results_unchanged(oracle):
         shape = est.launch()
         # the candidates kg_autotune times (0 = the defaults)
         assert slots == 0 and bps in (0, 4, 3)
-        assert shape["unit_entries"] in (0, 32768, 8192, 4096) and shape["slot_divisor"] in (5, 3, 8)
+        assert shape["unit_entries"] in (0, 65536, 16384, 8192) and shape["slot_divisor"] in (5, 3, 8)
         tuned = est.relatedness()
         est.set_work_unit(0)
         est.set_launch(64, 2)      # few slots in flight: many more waves
