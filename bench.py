@@ -251,9 +251,9 @@ def run_reference(args, codes, planted):
 
 def run_batch(args, local):
     """Eight cohorts of uneven N, M and missingness in one launch: timed with
-    the default launch shape, then with the one kg_autotune picks on a sample
-    of the largest cohort (both reported; the line's value is the default
-    shape's, the tuned run's beside it)."""
+    the default launch shape and with the one kg_autotune picks on a sample of
+    the largest cohort, the two alternating step by step (both reported; the
+    line's value is the default shape's, the tuned shape's beside it)."""
     import kestrel_b200 as kb
     from kestrel_b200 import synth
     cohorts = synth.config2()
@@ -261,32 +261,51 @@ def run_batch(args, local):
     import torch
     est = kb.Estimator(device=local, precision=args.precision)
     est.set_launch(args.slots, args.pass_bps)
-    inputs = [(c.codes,) for c in cohorts]
-    # page-locked row buffers, reused by every call
+    # page-locked genotypes and row buffers, reused by every call (uploads
+    # from pageable memory vary by a few hundred ms from call to call)
+    inputs = [(torch.from_numpy(c.codes).pin_memory().numpy(),) for c in cohorts]
     outs = [torch.empty(c.codes.shape[0] * (c.codes.shape[0] + 1) // 2 * kb.OUTPUT_DTYPE.itemsize,
                         dtype=torch.uint8, pin_memory=True).numpy().view(kb.OUTPUT_DTYPE) for c in cohorts]
 
-    def timed():
-        for _ in range(max(1, args.warmup)):
-            est.relatedness_batch(inputs, out=outs)
-        wall, waves = [], []
-        for _ in range(max(1, args.steps)):
-            t0 = time.perf_counter()
-            est.relatedness_batch(inputs, out=outs)
-            wall.append(time.perf_counter() - t0)
-            waves.append(est.run_stats()["pair_kernel_ms"])
-        # the median step: one host stall (page faults, another process) does
-        # not move it
-        return float(np.median(wall)), float(np.median(waves)), est.run_stats()
+    def run_once():
+        t0 = time.perf_counter()
+        est.relatedness_batch(inputs, out=outs)
+        return time.perf_counter() - t0, est.run_stats()
 
-    t_default, w_default, _ = timed()
+    # the default shape first, for the warm-up and the tuner's sample
+    for _ in range(max(1, args.warmup)):
+        est.relatedness_batch(inputs, out=outs)
+    default_shape = est.launch()
     big = max(cohorts, key=lambda c: c.codes.shape[0])
     est.load(big.codes)
     t0 = time.perf_counter()
     est.autotune()
     t_tune = time.perf_counter() - t0
     shape = est.launch()
-    tw, w_tuned, st = timed()
+
+    def apply(sh):
+        est.set_launch(args.slots, sh["blocks_per_sm"] or args.pass_bps)
+        est.set_work_unit(sh["unit_entries"])
+
+    # the two shapes alternate step by step, so that clock and power drift
+    # over the run falls on both alike (the tuner leaves the divisor of the
+    # pairs in flight alone for a cohort this large, so the two differ at
+    # most in blocks per SM and the work unit); a change of shape rebuilds
+    # the engine's buffers and graphs, so each shape's timed call follows an
+    # untimed one
+    runs = {"default": ([], []), "tuned": ([], [])}
+    st = None
+    for _ in range(max(1, args.steps)):
+        for name, sh in (("default", default_shape), ("tuned", shape)):
+            apply(sh)
+            est.relatedness_batch(inputs, out=outs)
+            dt, st = run_once()
+            runs[name][0].append(dt)
+            runs[name][1].append(st["pair_kernel_ms"])
+    # the median step: one host stall (page faults, another process) does
+    # not move it
+    t_default, w_default = float(np.median(runs["default"][0])), float(np.median(runs["default"][1]))
+    tw, w_tuned = float(np.median(runs["tuned"][0])), float(np.median(runs["tuned"][1]))
     est.close()
     waves_ms = [w_default]
     return {"metric": "all-pairs/s, 8 uneven cohorts in one launch", "value": pairs / t_default,
@@ -297,8 +316,9 @@ def run_batch(args, local):
             "config": {"workload": "cohorts N=" + "/".join(str(c.codes.shape[0]) for c in cohorts) +
                                    " x M=" + "/".join(str(c.codes.shape[1]) for c in cohorts) +
                                    ", per-sample missingness U(0, 0.2)", "pairs": pairs},
-            "timing": "host wall clock around kg_relatedness_batch (uploads, preparation, waves, rows back "
-                      "into page-locked buffers), median of the steps",
+            "timing": "host wall clock around kg_relatedness_batch (uploads from page-locked memory, "
+                      "preparation, waves, rows back into page-locked buffers), median of the steps; default and "
+                      "tuned shapes alternate",
             "waves_ms": float(np.mean(waves_ms)), "waves_pairs_per_s": pairs / (np.mean(waves_ms) * 1e-3),
             "autotune": {"shape": shape, "tune_s": t_tune, "default_pairs_per_s": pairs / t_default,
                          "default_waves_ms": w_default, "tuned_pairs_per_s": pairs / tw, "tuned_waves_ms": w_tuned,

@@ -909,12 +909,17 @@ int kg_autotune(kg_ctx* c, int* slots_out, int* bps_out) {
         int bps = 0, unit = 0, div = 5;
         // The site-pass shape (blocks per SM, work unit) is judged by the pass
         // phase's device time: every shape runs the same passes, and the wave
-        // tail of a sample does not mislead it.  The share of pairs in flight
-        // only matters for jobs below 5 x 131,072 pairs; it is judged by the
-        // sample's whole device time, and only for such a cohort.
+        // tail of a sample does not mislead it.  The sample runs with as many
+        // pairs in flight as the whole cohort would get by default (up to its
+        // own pairs): a wave's task count sets how much a unit's size costs
+        // in load balance, so a sample with fewer slots than the real job
+        // would favour small units.  The share of pairs in flight only matters
+        // for jobs below 5 x 131,072 pairs; it is judged by the sample's whole
+        // device time (automatic slots), and only for such a cohort.
+        const int64_t job_slots = std::min<int64_t>(131072, std::max<int64_t>(4096, full_pairs / 5));
         auto cost = [&](int b, int u, int d, bool whole, double& ms) -> int {
             kg::RunConfig cfg = run_config(c, 100);
-            cfg.slots = 0;
+            cfg.slots = whole ? 0 : std::min<int64_t>(job_slots, np);
             cfg.pass_blocks_per_sm = b;
             cfg.unit_elems = u;
             cfg.slot_divisor = d;

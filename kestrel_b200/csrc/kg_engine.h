@@ -190,7 +190,7 @@ struct PairJob {
 struct RunConfig {
     int precision = KG_PREC_FP32C;
     uint64_t iterations = 100;
-    int64_t slots = 0;         // pairs in flight per wave (0 = pairs / 8 within 4096..32768, as memory allows)
+    int64_t slots = 0;         // pairs in flight per wave (0 = pairs / slot_divisor within 4096..131072, as memory allows)
     int pass_blocks_per_sm = 0;   // site-pass kernel blocks per SM (0 = occupancy limit)
     uint64_t max_waves = 0;       // waves a call may run before it gives up (0 = a bound from the work)
     int ml_units = 0;             // work units per slot of the ML path's tri-/tetra-allelic sites (run_pairs sets it)
