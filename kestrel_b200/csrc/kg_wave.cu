@@ -347,7 +347,7 @@ __device__ __forceinline__ void ring_prologue(const Ring& R, const float* L, int
 // 127; lane l takes 128 i + 32 j + l (j = 0..3): 16 sites, in packed pairs
 // (Shape32x2), whose FP32 gradient and objective partials go to FP64 after
 // every stage (8 sites per partial) and whose Hessian partials go every
-// HESS_STAGES stages (64 sites per partial).  Only the list's last stage can
+// HESS_STAGES stages (128 sites per partial).  Only the list's last stage can
 // be partly filled; the others run without bounds tests.  L and every stage
 // start are 16-byte aligned (list starts are multiples of four entries); a
 // stage's copy rounds its size up to 16 bytes, which stays inside the slot's
@@ -359,7 +359,7 @@ __device__ __forceinline__ void ring_prologue(const Ring& R, const float* L, int
 // the warp sync keeps them before the stage's next copy, and between the two
 // the compiler schedules them among the site arithmetic.  Returns false if a
 // wait ran out.
-constexpr int HESS_STAGES = 8;
+constexpr int HESS_STAGES = 16;
 template <int S, bool DIFF>
 __device__ __forceinline__ bool stream32_ring(const float* __restrict__ L, int64_t len, const Coef32* K, int lane,
                                               const Ring R, double* Hs, LaneSums& out) {
